@@ -1,0 +1,375 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 walk path: RadFoam forward + backward (training
+gradient) on the 262,144-site, SH degree 3, 8 x 512^2 workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one bv_forward_backward call over the 8 views of a rank (start
+cells, walk, L2 loss, replay backward with gradient scatter), with inputs
+resident in HBM.  The gradient tables are zeroed inside the step.  L2 is
+flushed (a 256 MB write) between timed steps, outside the timed region.
+Under torchrun each rank renders its own 8 views (weak scaling) and the
+gradient tables are summed with one NCCL all-reduce per step.
+
+The JSON line also carries:
+  forward   forward-only Mrays/s (bv_radfoam_tracer_dispatch_batch)
+  e2e       the same metric through the public API with host buffers:
+            pinned target images copied in and the loss copied out per step
+  roofline  algorithmic bytes of the fused kernel / its event-timed duration
+  cpu_baseline  the CPU restatement (oracle) on the host cores, sampled
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd Mrays/s"
+UNIT = "Mrays/s"
+N_SITES = 262144
+VIEWS = 8
+WIDTH = HEIGHT = 512
+MAX_STEPS = 1024
+MAX_DT = 50.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--sites", type=int, default=N_SITES)
+    ap.add_argument("--size", type=int, default=WIDTH)
+    ap.add_argument("--views", type=int, default=VIEWS)
+    ap.add_argument("--cpu-sample", type=int, default=192,
+                    help="side of the CPU-baseline sample image (view 0)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def build_workload(args, rank):
+    from blade_volume_b200 import scenes
+
+    model = scenes.radfoam_ball(args.sites, seed=0, sh_degree=3)
+    cams = scenes.sphere_cameras(args.views, 3.0, 1 + rank, math.radians(60.0), 1.0, 100.0)
+    return model, cams
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device = device_index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.strip().split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(model, cam, side, threads=None):
+    """Oracle fwd+bwd (FP64 gradients over the FP32 walk) on view 0 at
+    side x side pixels, all host cores."""
+    from oracle import oracle as O
+
+    om = O.OracleModel.from_scene(model)
+    target = np.zeros((1, side, side, 3), np.float32)
+    nthreads = threads or os.cpu_count() or 1
+    t0 = time.perf_counter()
+    O.forward_backward(om, [cam], side, side, MAX_STEPS, 0.0, MAX_DT, target, 0,
+                       threads=nthreads)
+    dt = time.perf_counter() - t0
+    rays = side * side
+    return {"value": rays / dt / 1e6, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"view 0 of the same scene at {side}x{side} ({rays} rays), "
+                      f"fwd+bwd with FP64 gradient accumulation, {dt:.2f} s"}
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement of the reference's path
+    (trace.rs walk + training gradient), timed on the host cores."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    model, cams = build_workload(args, 0)
+    side = args.cpu_sample
+    for _ in range(args.warmup):
+        cpu_baseline(model, cams[0], max(side // 4, 8))
+    vals = []
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(model, cams[0], side))
+    wall = time.perf_counter() - t_all
+    v = statistics.median(x["value"] for x in vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall * 1000.0 / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "radfoam_train fwd+bwd", "sites": args.sites, "sh_degree": 3,
+                   "views": args.views, "width": args.size, "height": args.size,
+                   "loss": "L2", "max_steps": MAX_STEPS, "max_dt": MAX_DT},
+        "cpu_baseline": {**vals[0], "value": v},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+
+    import blade_volume_b200 as bv
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    model, cams = build_workload(args, rank)
+    from blade_volume_b200 import scenes
+
+    W = H = args.size
+    tracer = bv.RadFoamGpuTracer(model, max_steps=MAX_STEPS, weight_threshold=1e-3)
+    # targets: renders of the perturbed scene (densities x e^N(0,.1), SH + N(0,.05))
+    tgt_tracer = bv.RadFoamGpuTracer(scenes.perturbed(model, seed=2), max_steps=MAX_STEPS,
+                                     weight_threshold=1e-3)
+    rgba = tgt_tracer.render(cams, W, H)
+    target = rgba[..., :3].contiguous()
+    tgt_tracer.deinit()
+    del rgba
+    grads = tracer.new_grads()
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    stream = torch.cuda.current_stream()
+    rays = len(cams) * W * H
+
+    def step():
+        for g in grads.values():
+            g.zero_()
+        tracer.forward_backward(cams, W, H, target, grads, max_steps=MAX_STEPS,
+                                weight_threshold=0.0, max_dt=MAX_DT, loss_out=loss)
+        if dist is not None:
+            for g in grads.values():
+                dist.all_reduce(g)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    # per-launch stats of the fused kernel (device events on the launch stream)
+    tracer.enable_stats(True)
+    step()
+    st = tracer.last_stats()
+    tracer.enable_stats(False)
+    steps_per_launch, faces_per_launch = st.steps, st.faces
+
+    sampler = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    times = []
+    kernel_ms = []
+    for i in range(args.steps):
+        flush.zero_()
+        tracer.enable_stats(True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        kernel_ms.append(tracer.last_stats().kernel_ms)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    tracer.enable_stats(False)
+    total_ms = sum(times)
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = rays * world / (ms_per_step * 1e-3) / 1e6
+
+    # forward-only throughput of the same views (render path)
+    out = torch.empty((len(cams), H, W, 4), dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        tracer.dispatch_batch(out, cams, (W, H))
+    fwd_times = []
+    for _ in range(max(args.steps, 3)):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        tracer.dispatch_batch(out, cams, (W, H))
+        e1.record(stream)
+        e1.synchronize()
+        fwd_times.append(e0.elapsed_time(e1))
+    fwd_ms = sum(fwd_times) / len(fwd_times)
+
+    # end to end through the public API: pinned host targets in, loss out
+    host_target = torch.empty(target.shape, dtype=torch.float32, pin_memory=True)
+    host_target.copy_(target.cpu())
+    host_loss = torch.empty(1, dtype=torch.float32, pin_memory=True)
+    dev_target = torch.empty_like(target)
+    e2e_times = []
+    for i in range(args.steps + 1):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dev_target.copy_(host_target, non_blocking=True)
+        for g in grads.values():
+            g.zero_()
+        tracer.forward_backward(cams, W, H, dev_target, grads, max_steps=MAX_STEPS,
+                                weight_threshold=0.0, max_dt=MAX_DT, loss_out=loss)
+        if dist is not None:
+            for g in grads.values():
+                dist.all_reduce(g)
+        host_loss.copy_(loss, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        if i > 0:
+            e2e_times.append(e0.elapsed_time(e1))
+    e2e_ms = sum(e2e_times) / len(e2e_times)
+    if dist is not None:
+        t = torch.tensor([e2e_ms, fwd_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms, fwd_ms = (float(x) for x in t.tolist())
+
+    # roofline of the fused kernel: algorithmic bytes per launch
+    K = 16
+    faces_per_step = faces_per_launch / max(steps_per_launch, 1)
+    walk_step_bytes = 8 + faces_per_step * 20 + 4 + 4 * 3 * K  # offsets, idx+site, density, SH
+    atomic_bytes = 2 * (4 + 4 * 3 * K + 3 * 12)  # density, SH row, 3 site positions (r+w)
+    per_ray = 12 + 16  # target read, start-cell/loss/refill amortised
+    alg_bytes = steps_per_launch * (2 * walk_step_bytes + atomic_bytes) + rays * per_ray
+    kms = statistics.median(kernel_ms)
+    achieved = alg_bytes / (kms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "forward_backward_train.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(model, cams[0], args.cpu_sample)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "radfoam_train fwd+bwd", "sites": args.sites, "sh_degree": 3,
+                   "views_per_gpu": len(cams), "width": W, "height": H, "loss": "L2",
+                   "max_steps": MAX_STEPS, "max_dt": MAX_DT, "mean_degree": model.mean_degree(),
+                   "parallelism": f"dp{world}" if world > 1 else "single",
+                   "l2": "flushed between timed steps (256 MB write)"},
+        "forward": {"value": rays * world / (fwd_ms * 1e-3) / 1e6, "unit": UNIT,
+                    "ms_per_step": fwd_ms},
+        "e2e": {"value": rays * world / (e2e_ms * 1e-3) / 1e6, "unit": UNIT,
+                "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(target.numel() * 4),
+                "d2h_bytes_per_step": 4},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": peak_kind, "kernel": "forward_backward_kernel",
+                     "kernel_ms": kms, "alg_bytes_per_launch": alg_bytes,
+                     "steps_per_launch": steps_per_launch, "faces_per_step": faces_per_step},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    tracer.deinit()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

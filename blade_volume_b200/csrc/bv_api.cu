@@ -1,0 +1,612 @@
+// C ABI of the B200 walk path: model validation and packing, the tracer
+// handle (RadFoamGpuTracer), the path recorder and the training gradient.
+//
+// Host code only; the kernels live in bv_walk.cu and bv_start_cell.cu.
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bv_internal.h"
+
+using namespace bv;
+
+namespace {
+
+thread_local std::string g_error;
+
+bv_status fail(bv_status code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return code;
+}
+
+bv_status cuda_fail(cudaError_t e, const char *what) {
+    if (e == cudaErrorMemoryAllocation)
+        return fail(BV_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+        return fail(BV_ERR_NO_DEVICE, "%s: %s", what, cudaGetErrorString(e));
+    return fail(BV_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define BV_CUDA(call, what)                          \
+    do {                                             \
+        cudaError_t e_ = (call);                     \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+uint32_t sh_components(uint32_t degree) {
+    const uint32_t d = (degree > 3 ? 3 : degree) + 1;
+    return d * d;
+}
+
+uint16_t f32_to_bf16_rne(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40u);  // NaN
+    const uint32_t rounding = ((u >> 16) & 1u) + 0x7fffu;
+    return (uint16_t)((u + rounding) >> 16);
+}
+
+}  // namespace
+
+struct bv_tracer {
+    int device = 0;
+    uint32_t n = 0;
+    uint32_t m_edges = 0;
+    uint32_t sh_degree = 0;
+    uint32_t sh_stride = 0;
+    bool bf16 = false;
+    bool bounded = false;
+    bv_trace_settings settings{};
+    // device model
+    float4 *geom = nullptr;
+    float *density = nullptr;
+    void *sh = nullptr;
+    uint32_t *offsets = nullptr;
+    uint32_t *neighbors = nullptr;
+    // scratch
+    uint32_t *start_cells = nullptr;   // [kMaxViewsPerLaunch]
+    uint32_t *work_counter = nullptr;  // [4]
+    unsigned long long *stats = nullptr;  // [4]
+    double *partial_dist = nullptr;
+    uint32_t *partial_index = nullptr;
+    uint32_t *start_counters = nullptr;
+    int start_blocks = 1;
+    int grid_forward = 0;
+    int grid_train = 0;
+    // instrumentation
+    bool stats_enabled = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t last_stream = nullptr;
+    uint32_t last_launches = 0;
+    bool last_has_stats = false;
+    uint32_t last_start_point = 0;
+    bool start_point_pending = false;
+
+    DeviceModel model() const {
+        DeviceModel m;
+        m.geom = geom;
+        m.density = density;
+        m.sh = sh;
+        m.offsets = offsets;
+        m.neighbors = neighbors;
+        m.n = n;
+        m.sh_degree = sh_degree;
+        m.sh_stride = sh_stride;
+        m.sh_bf16 = bf16 ? 1u : 0u;
+        m.bounded = bounded ? 1u : 0u;
+        return m;
+    }
+};
+
+namespace {
+
+void free_tracer(bv_tracer *t) {
+    if (!t) return;
+    cudaFree(t->geom);
+    cudaFree(t->density);
+    cudaFree(t->sh);
+    cudaFree(t->offsets);
+    cudaFree(t->neighbors);
+    cudaFree(t->start_cells);
+    cudaFree(t->work_counter);
+    cudaFree(t->stats);
+    cudaFree(t->partial_dist);
+    cudaFree(t->partial_index);
+    cudaFree(t->start_counters);
+    for (auto &e : t->ev)
+        if (e) cudaEventDestroy(e);
+    delete t;
+}
+
+// ViewDesc for camera c of a width x height image (radfoam.wgsl:44-52).
+ViewDesc make_view(const bv_camera &c, uint32_t width, uint32_t height, uint32_t ray_begin,
+                   uint64_t pixel_begin) {
+    ViewDesc v;
+    std::memset(&v, 0, sizeof(v));
+    for (int i = 0; i < 3; ++i) v.origin[i] = c.cam_position[i];
+    v.depth = c.depth;
+    for (int i = 0; i < 4; ++i) v.q[i] = c.cam_orientation[i];
+    // tan(fov / 2): FP64 on the host, rounded to FP32 once per camera.
+    v.tan_half[0] = (float)std::tan((double)(0.5f * c.fov[0]));
+    v.tan_half[1] = (float)std::tan((double)(0.5f * c.fov[1]));
+    v.principal[0] = c.principal[0];
+    v.principal[1] = c.principal[1];
+    v.width = width;
+    v.height = height;
+    v.tiles_x = (width + kTileW - 1) / kTileW;
+    v.ray_begin = ray_begin;
+    v.pixel_begin = pixel_begin;
+    return v;
+}
+
+uint32_t padded_rays(uint32_t width, uint32_t height) {
+    const uint32_t tx = (width + kTileW - 1) / kTileW, ty = (height + kTileH - 1) / kTileH;
+    return tx * ty * kTileRays;
+}
+
+bv_status check_camera(const bv_camera &c) {
+    for (float v : c.cam_position)
+        if (!std::isfinite(v)) return fail(BV_ERR_INVALID_ARGUMENT, "camera position must be finite");
+    if (!std::isfinite(c.depth) || !(c.depth > 0.0f))
+        return fail(BV_ERR_INVALID_ARGUMENT, "camera depth must be finite and positive");
+    for (float v : c.cam_orientation)
+        if (!std::isfinite(v)) return fail(BV_ERR_INVALID_ARGUMENT, "camera orientation must be finite");
+    for (float v : c.fov)
+        if (!std::isfinite(v)) return fail(BV_ERR_INVALID_ARGUMENT, "camera fov must be finite");
+    return BV_OK;
+}
+
+// Launch the FP64 start-cell search for a chunk of cameras into
+// t->start_cells[0..count).
+bv_status launch_starts(bv_tracer *t, const bv_camera *cams, uint32_t count, cudaStream_t s) {
+    StartCellQueries q;
+    std::memset(&q, 0, sizeof(q));
+    q.count = count;
+    for (uint32_t i = 0; i < count; ++i)
+        for (int k = 0; k < 3; ++k) q.position[i][k] = cams[i].cam_position[k];
+    StartCellScratch sc{t->partial_dist, t->partial_index, t->start_counters, t->start_blocks};
+    BV_CUDA(launch_start_cells(t->geom, t->n, q, sc, t->start_cells, s), "start-cell launch");
+    return BV_OK;
+}
+
+bv_status begin_timing(bv_tracer *t, cudaStream_t s) {
+    t->last_stream = s;
+    t->last_launches = 0;
+    t->last_has_stats = t->stats_enabled;
+    if (t->stats_enabled) {
+        BV_CUDA(cudaMemsetAsync(t->stats, 0, 4 * sizeof(unsigned long long), s), "stats reset");
+        BV_CUDA(cudaEventRecord(t->ev[0], s), "event");
+    }
+    return BV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *bv_last_error(void) { return g_error.c_str(); }
+
+uint32_t bv_abi_version(void) { return BV_ABI_VERSION; }
+
+bv_status bv_model_validate(const bv_model_desc *md, char *err, size_t err_len) {
+    auto bad = [&](const char *fmt, auto... args) {
+        char buf[512];
+        snprintf(buf, sizeof(buf), fmt, args...);
+        g_error = buf;
+        if (err && err_len) {
+            strncpy(err, buf, err_len - 1);
+            err[err_len - 1] = '\0';
+        }
+        return BV_ERR_INVALID_MODEL;
+    };
+    if (!md) return bad("model descriptor is null");
+    const uint32_t n = md->num_points;
+    if (n == 0) return bad("model has no points");
+    if (!md->points || !md->sh_coefficients) return bad("points and SH coefficients are required");
+    if (md->sh_degree > 3) return bad("SH degree %u exceeds supported degree 3", md->sh_degree);
+    if (!md->adjacency_offsets || (!md->adjacency_neighbors && md->adjacency_offsets[n] != 0))
+        return bad("the cell walk requires CSR adjacency");
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *p = md->points + 4 * (size_t)i;
+        if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2]) ||
+            !std::isfinite(p[3]) || p[3] < 0.0f)
+            return bad("point %u must have finite coordinates and non-negative density/opacity", i);
+    }
+    const size_t nsh = (size_t)n * 3 * sh_components(md->sh_degree);
+    for (size_t i = 0; i < nsh; ++i)
+        if (!std::isfinite(md->sh_coefficients[i])) return bad("SH coefficients must be finite");
+    if (md->radii) {
+        for (uint32_t i = 0; i < n; ++i)
+            if (!std::isfinite(md->radii[i]) || md->radii[i] < 0.0f)
+                return bad("radii must be finite and non-negative");
+    }
+    // validate_csr_result (adjacency.rs:724-790)
+    const uint32_t *off = md->adjacency_offsets;
+    const uint32_t *nb = md->adjacency_neighbors;
+    if (off[0] != 0) return bad("Invalid adjacency_offsets[0]: expected 0, got %u", off[0]);
+    const uint32_t total = off[n];
+    for (uint32_t i = 0; i < n; ++i)
+        if (off[i + 1] < off[i] || off[i + 1] > total)
+            return bad("Invalid adjacency offset range for point %u: [%u, %u)", i, off[i], off[i + 1]);
+    for (uint32_t i = 0; i < n; ++i) {
+        for (uint32_t k = off[i]; k < off[i + 1]; ++k) {
+            if (k + 1 < off[i + 1] && nb[k] >= nb[k + 1])
+                return bad("Adjacency list for point %u must be sorted and unique", i);
+            if (nb[k] >= n)
+                return bad("Adjacency index out of bounds at entry %u: %u (num_points=%u)", k, nb[k], n);
+            if (nb[k] == i) return bad("Adjacency list for point %u contains a self-edge", i);
+        }
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        for (uint32_t k = off[i]; k < off[i + 1]; ++k) {
+            const uint32_t j = nb[k];
+            uint32_t lo = off[j], hi = off[j + 1];
+            bool found = false;
+            while (lo < hi) {
+                const uint32_t mid = lo + (hi - lo) / 2;
+                if (nb[mid] == i) {
+                    found = true;
+                    break;
+                }
+                if (nb[mid] < i)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            if (!found) return bad("Adjacency edge %u->%u has no reverse edge", i, j);
+        }
+    }
+    g_error.clear();
+    return BV_OK;
+}
+
+bv_status bv_radfoam_tracer_new(const bv_model_desc *md, const bv_trace_settings *settings,
+                                bv_tracer **out) {
+    if (!out) return fail(BV_ERR_INVALID_ARGUMENT, "out handle pointer is null");
+    *out = nullptr;
+    if (bv_model_validate(md, nullptr, 0) != BV_OK) return BV_ERR_INVALID_MODEL;
+    int device = 0;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return cuda_fail(e == cudaSuccess ? cudaErrorNoDevice : e, "cudaGetDeviceCount");
+    BV_CUDA(cudaGetDevice(&device), "cudaGetDevice");
+
+    bv_tracer *t = new bv_tracer();
+    t->device = device;
+    t->n = md->num_points;
+    t->m_edges = md->adjacency_offsets[md->num_points];
+    t->sh_degree = md->sh_degree;
+    t->bf16 = (md->flags & BV_MODEL_SH_BF16) != 0;
+    t->bounded = md->radii != nullptr;
+    if (settings) {
+        t->settings = *settings;
+    } else {
+        t->settings.max_steps = 1024;
+        t->settings.weight_threshold = 0.001f;
+    }
+    const uint32_t n = t->n;
+    const uint32_t nsh = 3 * sh_components(t->sh_degree);
+    const uint32_t align = t->bf16 ? 8u : 4u;  // 16-byte rows
+    t->sh_stride = (nsh + align - 1) / align * align;
+
+    // host packing
+    std::vector<float4> geom(n);
+    std::vector<float> dens(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *p = md->points + 4 * (size_t)i;
+        geom[i] = make_float4(p[0], p[1], p[2], md->radii ? md->radii[i] : 0.0f);
+        dens[i] = p[3];
+    }
+    auto cleanup = [&](bv_status s) {
+        free_tracer(t);
+        return s;
+    };
+#define BV_TRY(call, what)                                            \
+    do {                                                              \
+        cudaError_t e_ = (call);                                      \
+        if (e_ != cudaSuccess) return cleanup(cuda_fail(e_, what));   \
+    } while (0)
+    BV_TRY(cudaMalloc(&t->geom, sizeof(float4) * n), "cudaMalloc geom");
+    BV_TRY(cudaMalloc(&t->density, sizeof(float) * n), "cudaMalloc density");
+    BV_TRY(cudaMalloc(&t->offsets, sizeof(uint32_t) * (n + 1)), "cudaMalloc offsets");
+    BV_TRY(cudaMalloc(&t->neighbors, sizeof(uint32_t) * (t->m_edges ? t->m_edges : 1)), "cudaMalloc neighbors");
+    BV_TRY(cudaMemcpy(t->geom, geom.data(), sizeof(float4) * n, cudaMemcpyHostToDevice), "upload geom");
+    BV_TRY(cudaMemcpy(t->density, dens.data(), sizeof(float) * n, cudaMemcpyHostToDevice), "upload density");
+    BV_TRY(cudaMemcpy(t->offsets, md->adjacency_offsets, sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice), "upload offsets");
+    if (t->m_edges)
+        BV_TRY(cudaMemcpy(t->neighbors, md->adjacency_neighbors, sizeof(uint32_t) * t->m_edges, cudaMemcpyHostToDevice), "upload neighbors");
+    if (t->bf16) {
+        std::vector<uint16_t> row((size_t)n * t->sh_stride, 0);
+        for (uint32_t i = 0; i < n; ++i)
+            for (uint32_t k = 0; k < nsh; ++k)
+                row[(size_t)i * t->sh_stride + k] = f32_to_bf16_rne(md->sh_coefficients[(size_t)i * nsh + k]);
+        BV_TRY(cudaMalloc(&t->sh, row.size() * 2), "cudaMalloc sh");
+        BV_TRY(cudaMemcpy(t->sh, row.data(), row.size() * 2, cudaMemcpyHostToDevice), "upload sh");
+    } else {
+        std::vector<float> row((size_t)n * t->sh_stride, 0.0f);
+        for (uint32_t i = 0; i < n; ++i)
+            std::memcpy(&row[(size_t)i * t->sh_stride], md->sh_coefficients + (size_t)i * nsh, nsh * 4);
+        BV_TRY(cudaMalloc(&t->sh, row.size() * 4), "cudaMalloc sh");
+        BV_TRY(cudaMemcpy(t->sh, row.data(), row.size() * 4, cudaMemcpyHostToDevice), "upload sh");
+    }
+    // scratch
+    t->start_blocks = start_cell_blocks(n);
+    BV_TRY(cudaMalloc(&t->start_cells, sizeof(uint32_t) * kMaxViewsPerLaunch), "cudaMalloc start cells");
+    BV_TRY(cudaMalloc(&t->work_counter, sizeof(uint32_t) * 4), "cudaMalloc counter");
+    BV_TRY(cudaMalloc(&t->stats, sizeof(unsigned long long) * 4), "cudaMalloc stats");
+    BV_TRY(cudaMalloc(&t->partial_dist, sizeof(double) * kMaxStartQueries * t->start_blocks), "cudaMalloc partials");
+    BV_TRY(cudaMalloc(&t->partial_index, sizeof(uint32_t) * kMaxStartQueries * t->start_blocks), "cudaMalloc partials");
+    BV_TRY(cudaMalloc(&t->start_counters, sizeof(uint32_t) * kMaxStartQueries), "cudaMalloc counters");
+    BV_TRY(cudaMemset(t->start_counters, 0, sizeof(uint32_t) * kMaxStartQueries), "memset counters");
+    BV_TRY(cudaMemset(t->start_cells, 0, sizeof(uint32_t) * kMaxViewsPerLaunch), "memset start cells");
+    for (auto &ev : t->ev) BV_TRY(cudaEventCreate(&ev), "cudaEventCreate");
+    t->grid_forward = walk_grid_size(device, 0);
+    t->grid_train = walk_grid_size(device, 1);
+    BV_TRY(cudaDeviceSynchronize(), "upload");
+#undef BV_TRY
+    *out = t;
+    g_error.clear();
+    return BV_OK;
+}
+
+void bv_radfoam_tracer_destroy(bv_tracer *t) {
+    if (!t) return;
+    cudaDeviceSynchronize();
+    free_tracer(t);
+}
+
+bv_status bv_radfoam_tracer_dispatch_batch(bv_tracer *t, float *out_rgba_dev,
+                                           const bv_camera *cams, uint32_t n_cams, uint32_t width,
+                                           uint32_t height, bv_stream stream) {
+    if (!t || !out_rgba_dev || !cams) return fail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    if (width == 0 || height == 0) return fail(BV_ERR_INVALID_ARGUMENT, "render size must be non-zero");
+    if (n_cams == 0) return fail(BV_ERR_INVALID_ARGUMENT, "no cameras");
+    if ((uint64_t)padded_rays(width, height) * kMaxViewsPerLaunch >= (1ull << 32))
+        return fail(BV_ERR_INVALID_ARGUMENT, "image too large");
+    for (uint32_t i = 0; i < n_cams; ++i) {
+        bv_status s = check_camera(cams[i]);
+        if (s != BV_OK) return s;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    bv_status st = begin_timing(t, s);
+    if (st != BV_OK) return st;
+    for (uint32_t c0 = 0; c0 < n_cams; c0 += kMaxViewsPerLaunch) {
+        const uint32_t nc = std::min<uint32_t>(kMaxViewsPerLaunch, n_cams - c0);
+        st = launch_starts(t, cams + c0, nc, s);
+        if (st != BV_OK) return st;
+        if (t->stats_enabled && c0 == 0) BV_CUDA(cudaEventRecord(t->ev[1], s), "event");
+        WalkParams p;
+        std::memset(&p, 0, sizeof(p));
+        p.m = t->model();
+        p.max_steps = t->settings.max_steps;
+        p.weight_threshold = t->settings.weight_threshold;
+        p.n_views = nc;
+        uint32_t work = 0;
+        for (uint32_t v = 0; v < nc; ++v) {
+            p.views[v] = make_view(cams[c0 + v], width, height, work,
+                                   (uint64_t)v * width * height);
+            work += padded_rays(width, height);
+        }
+        p.total_work = work;
+        p.start_cells = t->start_cells;
+        p.work_counter = t->work_counter;
+        p.stats = t->stats_enabled ? t->stats : nullptr;
+        p.out_rgba = reinterpret_cast<float4 *>(out_rgba_dev) + (size_t)c0 * width * height;
+        p.debug_cell_density = t->settings.debug_cell_density;
+        BV_CUDA(cudaMemsetAsync(t->work_counter, 0, sizeof(uint32_t), s), "counter reset");
+        const int blocks_needed = (int)((work + 255) / 256);
+        const int grid = std::min(t->grid_forward, std::max(blocks_needed, 1));
+        BV_CUDA(launch_walk_forward(p, grid, s), "walk launch");
+        t->last_launches += 2;
+    }
+    if (t->stats_enabled) BV_CUDA(cudaEventRecord(t->ev[2], s), "event");
+    t->start_point_pending = true;
+    return BV_OK;
+}
+
+bv_status bv_radfoam_tracer_dispatch(bv_tracer *t, float *out_rgba_dev, const bv_camera *camera,
+                                     uint32_t width, uint32_t height, bv_stream stream) {
+    return bv_radfoam_tracer_dispatch_batch(t, out_rgba_dev, camera, 1, width, height, stream);
+}
+
+bv_status bv_radfoam_tracer_set_max_steps(bv_tracer *t, uint32_t max_steps) {
+    if (!t) return fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
+    t->settings.max_steps = max_steps;
+    return BV_OK;
+}
+
+bv_status bv_radfoam_tracer_set_weight_threshold(bv_tracer *t, float w) {
+    if (!t) return fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
+    t->settings.weight_threshold = w;
+    return BV_OK;
+}
+
+bv_status bv_radfoam_tracer_set_debug_cell_density(bv_tracer *t, uint32_t enabled) {
+    if (!t) return fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
+    t->settings.debug_cell_density = enabled ? 1u : 0u;
+    return BV_OK;
+}
+
+uint32_t bv_radfoam_tracer_max_steps(const bv_tracer *t) { return t ? t->settings.max_steps : 0; }
+float bv_radfoam_tracer_weight_threshold(const bv_tracer *t) {
+    return t ? t->settings.weight_threshold : 0.0f;
+}
+uint32_t bv_radfoam_tracer_sh_degree(const bv_tracer *t) { return t ? t->sh_degree : 0; }
+uint32_t bv_radfoam_tracer_num_points(const bv_tracer *t) { return t ? t->n : 0; }
+
+uint32_t bv_radfoam_tracer_start_point(bv_tracer *t) {
+    if (!t) return 0;
+    if (t->start_point_pending) {
+        cudaStreamSynchronize(t->last_stream);
+        cudaMemcpy(&t->last_start_point, t->start_cells, 4, cudaMemcpyDeviceToHost);
+        t->start_point_pending = false;
+    }
+    return t->last_start_point;
+}
+
+bv_status bv_containing_point(bv_tracer *t, const float position[3], uint32_t *out_index) {
+    if (!t || !position || !out_index) return fail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    if (!std::isfinite(position[0]) || !std::isfinite(position[1]) || !std::isfinite(position[2]))
+        return fail(BV_ERR_INVALID_ARGUMENT, "query position must be finite");
+    bv_camera c;
+    std::memset(&c, 0, sizeof(c));
+    for (int i = 0; i < 3; ++i) c.cam_position[i] = position[i];
+    cudaStream_t s = nullptr;
+    bv_status st = launch_starts(t, &c, 1, s);
+    if (st != BV_OK) return st;
+    BV_CUDA(cudaMemcpy(out_index, t->start_cells, 4, cudaMemcpyDeviceToHost), "read start cell");
+    t->start_point_pending = false;
+    t->last_start_point = *out_index;
+    return BV_OK;
+}
+
+bv_status bv_record_paths(bv_tracer *t, const bv_camera *cams, uint32_t n_cams, uint32_t width,
+                          uint32_t height, const bv_path_buffers *buf, bv_stream stream) {
+    if (!t || !cams || !buf) return fail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    if (width == 0 || height == 0 || n_cams == 0)
+        return fail(BV_ERR_INVALID_ARGUMENT, "render size must be non-zero");
+    if (buf->max_steps == 0 || buf->max_steps >= BV_PATH_TRUNCATED)
+        return fail(BV_ERR_INVALID_ARGUMENT, "path-record max_steps exceeds status encoding");
+    for (uint32_t i = 0; i < n_cams; ++i) {
+        bv_status s = check_camera(cams[i]);
+        if (s != BV_OK) return s;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    bv_status st = begin_timing(t, s);
+    if (st != BV_OK) return st;
+    for (uint32_t c0 = 0; c0 < n_cams; c0 += kMaxViewsPerLaunch) {
+        const uint32_t nc = std::min<uint32_t>(kMaxViewsPerLaunch, n_cams - c0);
+        st = launch_starts(t, cams + c0, nc, s);
+        if (st != BV_OK) return st;
+        RecordParams p;
+        std::memset(&p, 0, sizeof(p));
+        p.m = t->model();
+        p.max_steps = buf->max_steps;
+        p.n_views = nc;
+        uint32_t work = 0;
+        const uint64_t pix0 = (uint64_t)c0 * width * height;
+        for (uint32_t v = 0; v < nc; ++v) {
+            p.views[v] = make_view(cams[c0 + v], width, height, work, pix0 + (uint64_t)v * width * height);
+            work += padded_rays(width, height);
+        }
+        p.total_work = work;
+        p.start_cells = t->start_cells;
+        p.work_counter = t->work_counter;
+        p.buf = *buf;
+        BV_CUDA(launch_record_paths(p, 0, s), "record launch");
+        t->last_launches += 2;
+    }
+    if (t->stats_enabled) {
+        BV_CUDA(cudaEventRecord(t->ev[1], s), "event");
+        BV_CUDA(cudaEventRecord(t->ev[2], s), "event");
+    }
+    return BV_OK;
+}
+
+bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_cams,
+                              uint32_t width, uint32_t height, const float *target,
+                              const bv_train_settings *ts, const bv_grads *grads, float *loss,
+                              float *rgb_out, bv_stream stream) {
+    if (!t || !cams || !target || !ts || !grads || !loss)
+        return fail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    if (!grads->d_density_dev || !grads->d_sh_dev)
+        return fail(BV_ERR_INVALID_ARGUMENT, "density and SH gradient tables are required");
+    if (width == 0 || height == 0 || n_cams == 0)
+        return fail(BV_ERR_INVALID_ARGUMENT, "render size must be non-zero");
+    if (ts->loss != BV_LOSS_L2 && ts->loss != BV_LOSS_L1)
+        return fail(BV_ERR_INVALID_ARGUMENT, "unknown loss %u", ts->loss);
+    if (!(ts->max_dt > 0.0f)) return fail(BV_ERR_INVALID_ARGUMENT, "max_dt must be positive");
+    if (grads->d_radii_dev && !t->bounded)
+        return fail(BV_ERR_INVALID_ARGUMENT, "radius gradients need a PowerFoam model");
+    const uint32_t nsh = 3 * sh_components(t->sh_degree);
+    if ((nsh % 4) == 0 && (reinterpret_cast<uintptr_t>(grads->d_sh_dev) & 15u) != 0)
+        return fail(BV_ERR_INVALID_ARGUMENT, "d_sh table must be 16-byte aligned");
+    for (uint32_t i = 0; i < n_cams; ++i) {
+        bv_status s = check_camera(cams[i]);
+        if (s != BV_OK) return s;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    bv_status st = begin_timing(t, s);
+    if (st != BV_OK) return st;
+    BV_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), s), "loss reset");
+    const double total_rays = (double)n_cams * width * height;
+    for (uint32_t c0 = 0; c0 < n_cams; c0 += kMaxViewsPerLaunch) {
+        const uint32_t nc = std::min<uint32_t>(kMaxViewsPerLaunch, n_cams - c0);
+        st = launch_starts(t, cams + c0, nc, s);
+        if (st != BV_OK) return st;
+        if (t->stats_enabled && c0 == 0) BV_CUDA(cudaEventRecord(t->ev[1], s), "event");
+        TrainParams p;
+        std::memset(&p, 0, sizeof(p));
+        p.m = t->model();
+        p.max_steps = ts->max_steps;
+        p.weight_threshold = ts->weight_threshold;
+        p.max_dt = ts->max_dt;
+        p.loss_kind = ts->loss;
+        p.inv_count = (float)(1.0 / (3.0 * total_rays));
+        p.n_views = nc;
+        uint32_t work = 0;
+        for (uint32_t v = 0; v < nc; ++v) {
+            p.views[v] = make_view(cams[c0 + v], width, height, work, (uint64_t)v * width * height);
+            work += padded_rays(width, height);
+        }
+        const size_t off = (size_t)c0 * width * height;
+        p.total_work = work;
+        p.start_cells = t->start_cells;
+        p.work_counter = t->work_counter;
+        p.target = target + 3 * off;
+        p.rgb_out = rgb_out ? rgb_out + 3 * off : nullptr;
+        p.d_density = grads->d_density_dev;
+        p.d_sh = grads->d_sh_dev;
+        p.d_pos = grads->d_positions_dev;
+        p.d_radius = grads->d_radii_dev;
+        p.loss = loss;
+        p.stats = t->stats_enabled ? t->stats : nullptr;
+        BV_CUDA(cudaMemsetAsync(t->work_counter, 0, sizeof(uint32_t), s), "counter reset");
+        const int blocks_needed = (int)((work + 255) / 256);
+        const int grid = std::min(t->grid_train, std::max(blocks_needed, 1));
+        BV_CUDA(launch_forward_backward(p, grid, s), "forward-backward launch");
+        t->last_launches += 2;
+    }
+    if (t->stats_enabled) BV_CUDA(cudaEventRecord(t->ev[2], s), "event");
+    t->start_point_pending = true;
+    return BV_OK;
+}
+
+bv_status bv_radfoam_tracer_enable_stats(bv_tracer *t, uint32_t enabled) {
+    if (!t) return fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
+    t->stats_enabled = enabled != 0;
+    return BV_OK;
+}
+
+bv_status bv_radfoam_tracer_last_stats(bv_tracer *t, bv_launch_stats *out) {
+    if (!t || !out) return fail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    out->launches = t->last_launches;
+    if (!t->last_has_stats) return BV_OK;
+    BV_CUDA(cudaEventSynchronize(t->ev[2]), "event sync");
+    float a = 0.f, b = 0.f;
+    BV_CUDA(cudaEventElapsedTime(&a, t->ev[0], t->ev[1]), "elapsed");
+    BV_CUDA(cudaEventElapsedTime(&b, t->ev[1], t->ev[2]), "elapsed");
+    out->start_cell_ms = a;
+    out->kernel_ms = b;
+    unsigned long long h[4] = {0, 0, 0, 0};
+    BV_CUDA(cudaMemcpy(h, t->stats, sizeof(h), cudaMemcpyDeviceToHost), "stats read");
+    out->rays = h[0];
+    out->steps = h[1];
+    out->faces = h[2];
+    return BV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,121 @@
+// Internal device layout and launch descriptors of the B200 walk path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "blade_volume_b200.h"
+
+namespace bv {
+
+// Rays are handed out in tiles of 8x4 pixels so that a warp's 32 lanes start
+// on neighbouring pixels and walk mostly the same cells.
+constexpr int kTileW = 8;
+constexpr int kTileH = 4;
+constexpr int kTileRays = kTileW * kTileH;
+// Views (cameras) per launch carried in the kernel parameter block.
+constexpr int kMaxViewsPerLaunch = 32;
+
+struct ViewDesc {  // 80 bytes
+    float origin[3];
+    float depth;
+    float q[4];
+    float tan_half[2];
+    float principal[2];
+    uint32_t width, height;
+    uint32_t tiles_x;
+    uint32_t ray_begin;    // first tile-ordered work index of this view
+    uint64_t pixel_begin;  // first output pixel of this view
+    uint64_t pad;
+};
+
+// SoA device copy of a model.  geom packs the per-neighbour hot data
+// (position and power radius) into one 16-byte load; appearance lives in
+// separate tables that are read once per step.
+struct DeviceModel {
+    const float4 *geom;        // [N] x, y, z, radius (0 for plain RadFoam)
+    const float *density;      // [N]
+    const void *sh;            // [N][sh_stride] float or bf16
+    const uint32_t *offsets;   // [N+1]
+    const uint32_t *neighbors; // [M]
+    uint32_t n;
+    uint32_t sh_degree;
+    uint32_t sh_stride;        // elements per SH row (>= 3K, padded to 16 bytes)
+    uint32_t sh_bf16;
+    uint32_t bounded;          // radii present (PowerFoam)
+};
+
+struct WalkParams {
+    DeviceModel m;
+    uint32_t max_steps;
+    float weight_threshold;
+    uint32_t n_views;
+    uint32_t total_work;          // tile-ordered work items over all views
+    const uint32_t *start_cells;  // [n_views]
+    uint32_t *work_counter;       // persistent-kernel ray dispenser
+    unsigned long long *stats;    // [3] rays, steps, faces (or null)
+    float4 *out_rgba;             // [n_views][H][W]
+    uint32_t debug_cell_density;
+    ViewDesc views[kMaxViewsPerLaunch];
+};
+
+struct RecordParams {
+    DeviceModel m;
+    uint32_t max_steps;
+    uint32_t n_views;
+    uint32_t total_work;
+    const uint32_t *start_cells;
+    uint32_t *work_counter;
+    bv_path_buffers buf;
+    ViewDesc views[kMaxViewsPerLaunch];
+};
+
+struct TrainParams {
+    DeviceModel m;
+    uint32_t max_steps;
+    float weight_threshold;
+    float max_dt;
+    uint32_t loss_kind;
+    float inv_count;              // 1 / (3 * rays in the batch)
+    uint32_t n_views;
+    uint32_t total_work;
+    const uint32_t *start_cells;
+    uint32_t *work_counter;
+    const float *target;          // [views][H][W][3]
+    float *rgb_out;               // [views][H][W][3] or null
+    float *d_density;
+    float *d_sh;
+    float *d_pos;
+    float *d_radius;
+    float *loss;                  // device scalar accumulator
+    unsigned long long *stats;
+    ViewDesc views[kMaxViewsPerLaunch];
+};
+
+constexpr int kMaxStartQueries = 32;
+struct StartCellQueries {
+    float position[kMaxStartQueries][3];
+    uint32_t count;
+};
+
+// Launchers (bv_walk.cu / bv_start_cell.cu).
+cudaError_t launch_walk_forward(const WalkParams &p, int grid, cudaStream_t s);
+cudaError_t launch_record_paths(const RecordParams &p, int grid, cudaStream_t s);
+cudaError_t launch_forward_backward(const TrainParams &p, int grid, cudaStream_t s);
+int walk_grid_size(int device, int kind);
+
+// FP64 power-nearest search: out[v] = argmin_i |q_v - p_i|^2 - r_i^2, ties to
+// the lowest index.  partial/counters are scratch owned by the caller:
+// partial [n_queries * blocks_per_query] and counters [n_queries] (zeroed
+// once; the kernel leaves them zero).
+struct StartCellScratch {
+    double *partial_dist;
+    uint32_t *partial_index;
+    uint32_t *counters;
+    int blocks_per_query;
+};
+cudaError_t launch_start_cells(const float4 *geom, uint32_t n, const StartCellQueries &queries,
+                               const StartCellScratch &scratch, uint32_t *out, cudaStream_t s);
+int start_cell_blocks(uint32_t n);
+
+}  // namespace bv

@@ -1,0 +1,220 @@
+/*
+ * blade_volume_b200 — C ABI of the B200 (sm_100a) ray-tracing hot path of
+ * blade-volume: the RadFoam/PowerFoam cell walk with volumetric compositing,
+ * its path recorder, and its L2/L1 gradient.
+ *
+ * Every entry point returns a bv_status; nothing aborts across the ABI.  All
+ * pointers named *_dev are CUDA device pointers owned by the caller; host
+ * pointers are read before the call returns.  A handle is not thread-safe:
+ * one owner, one stream at a time (the reference serialises its GPU work the
+ * same way, tests/radfoam_gpu_vs_cpu.rs:41-47).
+ *
+ * Reference interfaces replaced (paths relative to the blade-volume repo):
+ *   RadFoamGpuTracer        blade-volume/src/gpu/radfoam_trace.rs:56-177
+ *   RadFoamGpuCloud         blade-volume/src/gpu/radfoam.rs:25-49, :676
+ *   PathRecorder            blade-volume/src/gpu/path_record.rs:225-595
+ *   PathRecordBuffers       blade-volume/src/gpu/path_record.rs:614-1364
+ *   training gradient       blade-volume-train/src/diff_render.rs:943-1923, :7181-7226
+ */
+#ifndef BLADE_VOLUME_B200_H
+#define BLADE_VOLUME_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BV_ABI_VERSION 1u
+
+typedef enum bv_status {
+    BV_OK = 0,
+    /* bad argument (null handle, zero size, ...): radfoam_trace.rs:113 asserts */
+    BV_ERR_INVALID_ARGUMENT = 1,
+    /* model rejected by validation: PointCloudModel::validate, lib.rs:246-483 */
+    BV_ERR_INVALID_MODEL = 2,
+    /* a CUDA runtime call failed; bv_last_error() has the text */
+    BV_ERR_CUDA = 3,
+    /* device allocation failed */
+    BV_ERR_OUT_OF_MEMORY = 4,
+    /* a per-ray candidate list overflowed: powerfoam_splat.rs:321 */
+    BV_ERR_CANDIDATE_OVERFLOW = 5,
+    /* a feature the model carries that this path does not implement */
+    BV_ERR_NOT_SUPPORTED = 6,
+    /* no CUDA device is available */
+    BV_ERR_NO_DEVICE = 7,
+} bv_status;
+
+/* cudaStream_t; NULL selects the legacy default stream. */
+typedef void *bv_stream;
+
+/* CameraParams (blade-volume/src/camera.rs:9-18): 48 bytes, same layout. */
+typedef struct bv_camera {
+    float cam_position[3];
+    float depth;
+    float cam_orientation[4]; /* unit quaternion x, y, z, w */
+    float fov[2];             /* local_dir = ((ndc - principal) * tan(fov / 2), 1) */
+    float principal[2];
+} bv_camera;
+
+/* Store SH coefficients as BF16 on the device (FP32 arithmetic). */
+#define BV_MODEL_SH_BF16 0x1u
+
+/* PointCloudModel (blade-volume/src/lib.rs:174-239), walk subset.  The
+ * arrays are the reference's own layouts, so a Rust caller passes
+ * model.points.as_ptr() etc. directly. */
+typedef struct bv_model_desc {
+    uint32_t num_points;
+    uint32_t sh_degree;                  /* 0..3 */
+    const float *points;                 /* [N*4] x, y, z, density (lib.rs:176) */
+    const float *sh_coefficients;        /* [N*3*K] [point][component][rgb] (lib.rs:185) */
+    const float *radii;                  /* [N] PowerFoam radii, or NULL (lib.rs:195) */
+    const uint32_t *adjacency_offsets;   /* CSR [N+1] */
+    const uint32_t *adjacency_neighbors; /* CSR [offsets[N]] sorted, symmetric, no self */
+    uint32_t flags;                      /* BV_MODEL_* */
+    uint32_t reserved;
+} bv_model_desc;
+
+/* RadFoamTraceSettings (blade-volume/src/gpu/radfoam_trace.rs:4-23). */
+typedef struct bv_trace_settings {
+    uint32_t max_steps;                    /* default 1024 */
+    uint32_t powerfoam_candidate_capacity; /* 0 = automatic */
+    float weight_threshold;                /* default 0.001 */
+    uint32_t debug_cell_density;           /* 1: output cells_visited/100 heat map */
+} bv_trace_settings;
+
+typedef struct bv_tracer bv_tracer;
+
+/* Last error message of the calling thread (valid until the next call). */
+const char *bv_last_error(void);
+uint32_t bv_abi_version(void);
+
+/* Host-side model validation, PointCloudModel::validate (lib.rs:246-483)
+ * and validate_csr (adjacency.rs:717-790).  Needs no GPU.  On failure the
+ * message (if err != NULL) names the first problem. */
+bv_status bv_model_validate(const bv_model_desc *model, char *err, size_t err_len);
+
+/* RadFoamGpuTracer::new (radfoam_trace.rs:63-104) + RadFoamGpuCloud::new
+ * (radfoam.rs:119-533): validates the model, packs it into the device layout
+ * and uploads it.  The tracer owns its device copy. */
+bv_status bv_radfoam_tracer_new(const bv_model_desc *model, const bv_trace_settings *settings,
+                                bv_tracer **out);
+
+/* RadFoamGpuTracer::deinit (radfoam_trace.rs:173-176). */
+void bv_radfoam_tracer_destroy(bv_tracer *tracer);
+
+/* RadFoamGpuTracer::dispatch (radfoam_trace.rs:106-135).  Renders one image
+ * of width x height into out_rgba_dev ([height][width][4] float32, RGB plus
+ * alpha = 1 - transmittance; the reference writes an rgba16f texture).  The
+ * start cell is the power-nearest site of the camera position, found on the
+ * device in FP64 (radfoam.rs:77-112 uses a host kd-tree in FP32). */
+bv_status bv_radfoam_tracer_dispatch(bv_tracer *tracer, float *out_rgba_dev,
+                                     const bv_camera *camera, uint32_t width, uint32_t height,
+                                     bv_stream stream);
+
+/* Several cameras of one size in one launch: out is [n][height][width][4]. */
+bv_status bv_radfoam_tracer_dispatch_batch(bv_tracer *tracer, float *out_rgba_dev,
+                                           const bv_camera *cameras, uint32_t n_cameras,
+                                           uint32_t width, uint32_t height, bv_stream stream);
+
+/* Settings accessors (radfoam_trace.rs:137-171). */
+bv_status bv_radfoam_tracer_set_max_steps(bv_tracer *tracer, uint32_t max_steps);
+bv_status bv_radfoam_tracer_set_weight_threshold(bv_tracer *tracer, float weight_threshold);
+bv_status bv_radfoam_tracer_set_debug_cell_density(bv_tracer *tracer, uint32_t enabled);
+uint32_t bv_radfoam_tracer_max_steps(const bv_tracer *tracer);
+float bv_radfoam_tracer_weight_threshold(const bv_tracer *tracer);
+uint32_t bv_radfoam_tracer_sh_degree(const bv_tracer *tracer);
+/* Start cell of the last dispatch (radfoam_trace.rs:169-171); synchronises
+ * the tracer's last stream. */
+uint32_t bv_radfoam_tracer_start_point(bv_tracer *tracer);
+uint32_t bv_radfoam_tracer_num_points(const bv_tracer *tracer);
+
+/* RadFoamGpuCloud::containing_point (radfoam.rs:676): power-nearest site of
+ * a position, FP64 on the device, ties to the lowest index.  Synchronous. */
+bv_status bv_containing_point(bv_tracer *tracer, const float position[3], uint32_t *out_index);
+
+/* ---- path recorder -------------------------------------------------------
+ * PathRecordBuffers (path_record.rs:614-1364), row-major [pixels, max_steps].
+ * Any stream pointer may be NULL to skip it.  Rows are written for recorded
+ * steps only; path_status[p] = steps | BV_PATH_TRUNCATED (bit 31) when the
+ * step cap stopped the ray (path_record.rs:41, :1248-1267). */
+#define BV_PATH_TRUNCATED 0x80000000u
+
+typedef struct bv_path_buffers {
+    uint32_t *previous_cells_dev; /* [P*L] */
+    uint32_t *cells_dev;          /* [P*L] */
+    uint32_t *next_cells_dev;     /* [P*L] */
+    float *dts_dev;               /* [P*L] */
+    float *dt_grad_previous_dev;  /* [P*L*4] d dt / d (x, y, z, r) of the entry site */
+    float *dt_grad_current_dev;   /* [P*L*4] of the cell's own site */
+    float *dt_grad_next_dev;      /* [P*L*4] of the exit site */
+    uint32_t *path_status_dev;    /* [P] */
+    uint32_t max_steps;           /* L */
+    uint32_t reserved;
+} bv_path_buffers;
+
+/* PathRecorder::dispatch_batch (path_record.rs:519-594) for the walk:
+ * record_path_jacobians (trace.rs:1573-1676) per pixel, cameras of one size,
+ * pixel p = view * height * width + y * width + x. */
+bv_status bv_record_paths(bv_tracer *tracer, const bv_camera *cameras, uint32_t n_cameras,
+                          uint32_t width, uint32_t height, const bv_path_buffers *buffers,
+                          bv_stream stream);
+
+/* ---- training gradient ---------------------------------------------------
+ * The differentiable forward of diff_render.rs:943-1923 on the recorded walk:
+ * dt clamped to max_dt (MAX_PATH_DT = 50, diff_render.rs:2510), raw =
+ * sigma * dt, T = exp(-exclusive cumsum), alpha = 1 - exp(-raw), per-cell
+ * ReLU colour (:2301-2303), per-pixel sum, then the loss over every channel
+ * of every pixel of the batch (metrics.rs:7): L2 = mean squared error,
+ * L1 = mean absolute error.  Gradients w.r.t. density, SH coefficients and
+ * site positions (and radii for PowerFoam) are ADDED to the caller's tables
+ * (zero them first), like the reference's scatter-add backward. */
+typedef enum bv_loss { BV_LOSS_L2 = 0, BV_LOSS_L1 = 1 } bv_loss;
+
+typedef struct bv_train_settings {
+    uint32_t max_steps;     /* rows per pixel (L) */
+    float weight_threshold; /* transmittance cut; 0 walks every recorded step */
+    float max_dt;           /* segment clamp, 50 in the reference */
+    uint32_t loss;          /* bv_loss */
+} bv_train_settings;
+
+typedef struct bv_grads {
+    float *d_density_dev;   /* [N] */
+    float *d_sh_dev;        /* [N*3*K], model layout */
+    float *d_positions_dev; /* [N*3], or NULL to skip position gradients */
+    float *d_radii_dev;     /* [N], PowerFoam only, or NULL */
+} bv_grads;
+
+/* Forward + loss + backward for a batch of cameras of one size.
+ * target_rgb_dev [n][height][width][3]; loss_dev receives the scalar loss
+ * (float, overwritten); rgb_out_dev (may be NULL) the rendered colours
+ * [n][height][width][3].  One fused launch: every ray is walked, its loss
+ * gradient formed, and its path replayed to scatter parameter gradients;
+ * no per-sample state is stored. */
+bv_status bv_forward_backward(bv_tracer *tracer, const bv_camera *cameras, uint32_t n_cameras,
+                              uint32_t width, uint32_t height, const float *target_rgb_dev,
+                              const bv_train_settings *settings, const bv_grads *grads,
+                              float *loss_dev, float *rgb_out_dev, bv_stream stream);
+
+/* ---- instrumentation -----------------------------------------------------
+ * Device time (ms, CUDA events on the launch stream) and work counters of
+ * the last dispatch / record / forward_backward call on this tracer.
+ * Synchronises that stream. */
+typedef struct bv_launch_stats {
+    float kernel_ms;        /* main traversal kernel */
+    float start_cell_ms;    /* start-cell search */
+    uint64_t rays;
+    uint64_t steps;         /* walk loop iterations over all rays */
+    uint64_t faces;         /* neighbour faces tested */
+    uint32_t launches;      /* kernels launched by the call */
+    uint32_t reserved;
+} bv_launch_stats;
+
+bv_status bv_radfoam_tracer_enable_stats(bv_tracer *tracer, uint32_t enabled);
+bv_status bv_radfoam_tracer_last_stats(bv_tracer *tracer, bv_launch_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BLADE_VOLUME_B200_H */

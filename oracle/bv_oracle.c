@@ -1,0 +1,1164 @@
+/*
+ * CPU oracle for the blade-volume ray-tracing hot path.  TEST INFRASTRUCTURE:
+ * the checker for the CUDA kernels, never part of the shipped library.
+ *
+ * Restates blade-volume/src/trace.rs (walk, recorder, Jacobians, splats),
+ * blade-volume/src/lib.rs:526-541 (containing cell) and the training
+ * gradient contract of blade-volume-train/src/diff_render.rs.  Build with
+ * -ffp-contract=off: every FP32 expression below is evaluated in the order
+ * the reference writes it (glam's Vec3::dot is ((x*x' + y*y') + z*z')).
+ */
+#include "bv_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------ */
+/* small vector helpers in glam's operation order                      */
+/* ------------------------------------------------------------------ */
+static inline float dot3f(const float a[3], const float b[3]) {
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+static inline double dot3d(const double a[3], const double b[3]) {
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+/*
+ * exp(x) for FP32, written from Cody & Waite's argument reduction
+ * (x = k*ln2 + r, ln2 split into a 12-bit-short high part and a low part)
+ * followed by the degree-7 Taylor polynomial of e^r on |r| <= ln2/2 in
+ * Horner form with fused multiply-adds, and an exact scaling by 2^k.
+ * The CUDA kernels evaluate the identical operation sequence, so α and T
+ * agree bit for bit between the oracle and the device.  The reference's
+ * f32::exp is the platform libm; both are within 2 ulp of exp (checked in
+ * tests/test_oracle_golden.py).
+ */
+float bvo_expf(float x) {
+    if (x != x) return x;
+    if (x > 88.72283935546875f) return INFINITY;
+    if (x < -103.972084045410156f) return 0.0f;
+    const float k = rintf(x * 1.44269502162933349609375f);
+    float r = fmaf(k, -0.693115234375f, x);
+    r = fmaf(k, -3.19461832987144589424133e-05f, r);
+    float p = 1.98412701138295233249664e-04f;
+    p = fmaf(p, r, 1.38888892251998186111450e-03f);
+    p = fmaf(p, r, 8.33333376795053482055664e-03f);
+    p = fmaf(p, r, 4.16666679084300994873047e-02f);
+    p = fmaf(p, r, 1.66666671633720397949219e-01f);
+    p = fmaf(p, r, 0.5f);
+    p = fmaf(p, r, 1.0f);
+    p = fmaf(p, r, 1.0f);
+    int ki = (int)k;
+    if (ki > 127) {
+        p = p * 2.0f;
+        ki -= 1;
+    }
+    if (ki < -126) {
+        /* subnormal result: scale by 2^(ki+64), then by 2^-64 */
+        union { uint32_t u; float f; } s = {(uint32_t)(ki + 64 + 127) << 23};
+        p = p * s.f;
+        return p * 5.42101086242752217004e-20f;
+    }
+    union { uint32_t u; float f; } s = {(uint32_t)(ki + 127) << 23};
+    return p * s.f;
+}
+
+/* tan(fov/2) for the ray mapping (radfoam.wgsl:268).  Computed once per
+ * camera on the host in FP64 and rounded to FP32; the product library uses
+ * the same expression and hands the result to the kernels. */
+float bvo_tan_half(float fov) { return (float)tan((double)(0.5f * fov)); }
+
+/* Pixel -> world ray, radfoam.wgsl:44-52 with qrot (common.wgsl:386-390)
+ * and glam's normalize (v * (1/|v|)). */
+void bvo_camera_ray(const bvo_camera *cam, uint32_t width, uint32_t height, uint32_t x,
+                    uint32_t y, float origin[3], float dir[3]) {
+    const float tx = bvo_tan_half(cam->fov[0]);
+    const float ty = bvo_tan_half(cam->fov[1]);
+    const float px = ((float)x + 0.5f) / (float)width;
+    const float py = ((float)y + 0.5f) / (float)height;
+    const float ndc_x = px * 2.0f - 1.0f;
+    const float ndc_y = py * 2.0f - 1.0f;
+    const float v[3] = {(ndc_x - cam->principal[0]) * tx, (ndc_y - cam->principal[1]) * ty, 1.0f};
+    const float *q = cam->orientation;
+    /* t = 2 * cross(q.xyz, v) */
+    const float c0 = q[1] * v[2] - q[2] * v[1];
+    const float c1 = q[2] * v[0] - q[0] * v[2];
+    const float c2 = q[0] * v[1] - q[1] * v[0];
+    const float t[3] = {2.0f * c0, 2.0f * c1, 2.0f * c2};
+    /* v + q.w * t + cross(q.xyz, t) */
+    const float e0 = q[1] * t[2] - q[2] * t[1];
+    const float e1 = q[2] * t[0] - q[0] * t[2];
+    const float e2 = q[0] * t[1] - q[1] * t[0];
+    const float r[3] = {(v[0] + q[3] * t[0]) + e0, (v[1] + q[3] * t[1]) + e1,
+                        (v[2] + q[3] * t[2]) + e2};
+    const float len = sqrtf(dot3f(r, r));
+    const float inv = 1.0f / len;
+    dir[0] = r[0] * inv;
+    dir[1] = r[1] * inv;
+    dir[2] = r[2] * inv;
+    origin[0] = cam->position[0];
+    origin[1] = cam->position[1];
+    origin[2] = cam->position[2];
+}
+
+/* ------------------------------------------------------------------ */
+/* SH evaluation (trace.rs:242-402)                                    */
+/* ------------------------------------------------------------------ */
+static const float SH_C[16] = {
+    0.2820948f,  -0.48860252f, 0.48860252f, -0.48860252f, 1.0925485f,  -1.0925485f,
+    0.31539157f, -1.0925485f,  0.54627424f, -0.5900436f,  2.8906114f,  -0.4570458f,
+    0.37317634f, -0.4570458f,  1.4453057f,  -0.5900436f,
+};
+
+static inline uint32_t sh_comps(uint32_t degree) {
+    uint32_t d = (degree > 3 ? 3 : degree) + 1;
+    return d * d;
+}
+
+/* SH basis values in the order and with the products that trace.rs uses;
+ * y[m] multiplies the coefficient after the constant: color += (C_m*coef)*y[m]
+ * for degree 1, ((C_m*coef)*a)*b for the two-factor degree-2 terms. */
+void bvo_eval_rgb_sh(const bvo_model *m, uint32_t point, const float dir[3], float out[3],
+                     float unclamped[3]) {
+    const uint32_t deg = m->sh_degree > 3 ? 3 : m->sh_degree;
+    const uint32_t comps = sh_comps(deg);
+    const float *c = m->sh + (size_t)point * 3u * comps;
+    const float x = dir[0], y = dir[1], z = dir[2];
+    const float xx = x * x, yy = y * y, zz = z * z;
+    float r = 0.0f, g = 0.0f, b = 0.0f;
+    r += SH_C[0] * c[0];
+    g += SH_C[0] * c[1];
+    b += SH_C[0] * c[2];
+    if (deg >= 1) {
+        r += SH_C[1] * c[3] * y;  g += SH_C[1] * c[4] * y;  b += SH_C[1] * c[5] * y;
+        r += SH_C[2] * c[6] * z;  g += SH_C[2] * c[7] * z;  b += SH_C[2] * c[8] * z;
+        r += SH_C[3] * c[9] * x;  g += SH_C[3] * c[10] * x; b += SH_C[3] * c[11] * x;
+    }
+    if (deg >= 2) {
+        r += SH_C[4] * c[12] * x * y; g += SH_C[4] * c[13] * x * y; b += SH_C[4] * c[14] * x * y;
+        r += SH_C[5] * c[15] * y * z; g += SH_C[5] * c[16] * y * z; b += SH_C[5] * c[17] * y * z;
+        const float t6 = 3.0f * zz - 1.0f;
+        r += SH_C[6] * c[18] * t6; g += SH_C[6] * c[19] * t6; b += SH_C[6] * c[20] * t6;
+        r += SH_C[7] * c[21] * x * z; g += SH_C[7] * c[22] * x * z; b += SH_C[7] * c[23] * x * z;
+        const float t8 = xx - yy;
+        r += SH_C[8] * c[24] * t8; g += SH_C[8] * c[25] * t8; b += SH_C[8] * c[26] * t8;
+    }
+    if (deg >= 3) {
+        const float t9 = y * (3.0f * xx - yy);
+        r += SH_C[9] * c[27] * t9; g += SH_C[9] * c[28] * t9; b += SH_C[9] * c[29] * t9;
+        const float t10 = x * y * z;
+        r += SH_C[10] * c[30] * t10; g += SH_C[10] * c[31] * t10; b += SH_C[10] * c[32] * t10;
+        const float t11 = y * (5.0f * zz - 1.0f);
+        r += SH_C[11] * c[33] * t11; g += SH_C[11] * c[34] * t11; b += SH_C[11] * c[35] * t11;
+        const float t12 = z * (5.0f * zz - 3.0f);
+        r += SH_C[12] * c[36] * t12; g += SH_C[12] * c[37] * t12; b += SH_C[12] * c[38] * t12;
+        const float t13 = x * (5.0f * zz - 1.0f);
+        r += SH_C[13] * c[39] * t13; g += SH_C[13] * c[40] * t13; b += SH_C[13] * c[41] * t13;
+        const float t14 = z * (xx - yy);
+        r += SH_C[14] * c[42] * t14; g += SH_C[14] * c[43] * t14; b += SH_C[14] * c[44] * t14;
+        const float t15 = x * (xx - 3.0f * yy);
+        r += SH_C[15] * c[45] * t15; g += SH_C[15] * c[46] * t15; b += SH_C[15] * c[47] * t15;
+    }
+    r = 0.5f + r;
+    g = 0.5f + g;
+    b = 0.5f + b;
+    if (unclamped) {
+        unclamped[0] = r;
+        unclamped[1] = g;
+        unclamped[2] = b;
+    }
+    out[0] = fmaxf(r, 0.0f);
+    out[1] = fmaxf(g, 0.0f);
+    out[2] = fmaxf(b, 0.0f);
+}
+
+/* SH basis Y_m(dir) in FP64 for the gradient oracle (same polynomials). */
+static void sh_basis_d(uint32_t deg, const double d[3], double Y[16]) {
+    const double x = d[0], y = d[1], z = d[2];
+    const double xx = x * x, yy = y * y, zz = z * z;
+    for (int i = 0; i < 16; ++i) Y[i] = 0.0;
+    Y[0] = (double)SH_C[0];
+    if (deg >= 1) {
+        Y[1] = (double)SH_C[1] * y;
+        Y[2] = (double)SH_C[2] * z;
+        Y[3] = (double)SH_C[3] * x;
+    }
+    if (deg >= 2) {
+        Y[4] = (double)SH_C[4] * x * y;
+        Y[5] = (double)SH_C[5] * y * z;
+        Y[6] = (double)SH_C[6] * (3.0 * zz - 1.0);
+        Y[7] = (double)SH_C[7] * x * z;
+        Y[8] = (double)SH_C[8] * (xx - yy);
+    }
+    if (deg >= 3) {
+        Y[9] = (double)SH_C[9] * y * (3.0 * xx - yy);
+        Y[10] = (double)SH_C[10] * x * y * z;
+        Y[11] = (double)SH_C[11] * y * (5.0 * zz - 1.0);
+        Y[12] = (double)SH_C[12] * z * (5.0 * zz - 3.0);
+        Y[13] = (double)SH_C[13] * x * (5.0 * zz - 1.0);
+        Y[14] = (double)SH_C[14] * z * (xx - yy);
+        Y[15] = (double)SH_C[15] * x * (xx - 3.0 * yy);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* geometry kernels of the walk                                        */
+/* ------------------------------------------------------------------ */
+static inline float read_radius(const bvo_model *m, uint32_t i) {
+    return m->radii ? m->radii[i] : 0.0f;
+}
+
+/* find_exit_face (trace.rs:170-205). Returns face index or -1. */
+static int find_exit_face(const bvo_model *m, uint32_t cell, const float cp[3], float cr,
+                          const float o[3], const float d[3], float t0, float depth,
+                          float *best_out) {
+    const uint32_t begin = m->offsets[cell], end = m->offsets[cell + 1];
+    float best = depth;
+    int face = -1;
+    const float ri2 = cr * cr;
+    for (uint32_t k = begin; k < end; ++k) {
+        const uint32_t j = m->neighbors[k];
+        const float *np = m->points + 4 * (size_t)j;
+        const float off[3] = {np[0] - cp[0], np[1] - cp[1], np[2] - cp[2]};
+        float shift;
+        if (m->radii) {
+            const float rj = m->radii[j];
+            const float dsq = fmaxf(dot3f(off, off), 1e-20f);
+            shift = 0.5f + 0.5f * (ri2 - rj * rj) / dsq;
+        } else {
+            shift = 0.5f;
+        }
+        const float fo[3] = {cp[0] + shift * off[0], cp[1] + shift * off[1], cp[2] + shift * off[2]};
+        const float dp = dot3f(off, d);
+        if (dp > 0.0f) {
+            const float rel[3] = {fo[0] - o[0], fo[1] - o[1], fo[2] - o[2]};
+            const float t = dot3f(rel, off) / dp;
+            if (isfinite(t) && t > t0 && t < best) {
+                best = t;
+                face = (int)(k - begin);
+            }
+        }
+    }
+    *best_out = best;
+    return face;
+}
+
+/* support_interval (trace.rs:209-238). Returns 1 when non-empty. */
+static int support_interval(int bounded, const float o[3], const float d[3], const float c[3],
+                            float radius, float t0, float t1, float *s, float *e) {
+    if (!bounded) {
+        if (t1 > t0) {
+            *s = t0;
+            *e = t1;
+            return 1;
+        }
+        return 0;
+    }
+    const float oc[3] = {o[0] - c[0], o[1] - c[1], o[2] - c[2]};
+    const float a = dot3f(d, d);
+    if (!isfinite(a) || a <= 0.0f) return 0;
+    const float b = dot3f(oc, d);
+    const float cc = dot3f(oc, oc) - radius * radius;
+    const float disc = b * b - a * cc;
+    if (disc <= 0.0f) return 0;
+    const float root = sqrtf(disc);
+    const float near_t = (-b - root) / a;
+    const float far_t = (-b + root) / a;
+    const float cs = fmaxf(t0, near_t);
+    const float ce = fminf(t1, far_t);
+    if (ce > cs) {
+        *s = cs;
+        *e = ce;
+        return 1;
+    }
+    return 0;
+}
+
+int bvo_support_interval(int bounded, const float o[3], const float d[3], const float c[3],
+                         float radius, float t0, float t1, float out[2]) {
+    return support_interval(bounded, o, d, c, radius, t0, t1, &out[0], &out[1]);
+}
+
+/* sphere_intersection_jacobians (trace.rs:1101-1124); dir normalized. */
+static int sphere_jac(const float o[3], const float d[3], const float c[3], float radius,
+                      float *near_t, float *far_t, float nj[4], float fj[4]) {
+    const float oc[3] = {o[0] - c[0], o[1] - c[1], o[2] - c[2]};
+    const float b = dot3f(oc, d);
+    const float disc = b * b - (dot3f(oc, oc) - radius * radius);
+    if (disc <= 0.0f || !isfinite(disc)) return 0;
+    const float root = sqrtf(disc);
+    const float perp[3] = {oc[0] - b * d[0], oc[1] - b * d[1], oc[2] - b * d[2]};
+    const float rdc[3] = {perp[0] / root, perp[1] / root, perp[2] / root};
+    const float rdr = radius / root;
+    *near_t = -b - root;
+    *far_t = -b + root;
+    if (nj) {
+        nj[0] = d[0] - rdc[0]; nj[1] = d[1] - rdc[1]; nj[2] = d[2] - rdc[2]; nj[3] = -rdr;
+        fj[0] = d[0] + rdc[0]; fj[1] = d[1] + rdc[1]; fj[2] = d[2] + rdc[2]; fj[3] = rdr;
+    }
+    return 1;
+}
+
+/* face_intersection_jacobians (trace.rs:1077-1097). */
+static void face_jac(const float o[3], const float d[3], const float cp[3], float cr,
+                     const float ap[3], float ar, float t, float cj[4], float aj[4]) {
+    const float n[3] = {ap[0] - cp[0], ap[1] - cp[1], ap[2] - cp[2]};
+    const float den = dot3f(d, n);
+    if (!isfinite(den) || fabsf(den) <= 1e-20f) {
+        memset(cj, 0, 16);
+        memset(aj, 0, 16);
+        return;
+    }
+    for (int i = 0; i < 3; ++i) {
+        cj[i] = (o[i] - cp[i] + t * d[i]) / den;
+        aj[i] = (ap[i] - o[i] - t * d[i]) / den;
+    }
+    cj[3] = cr / den;
+    aj[3] = -ar / den;
+}
+
+/* path_interval_jacobian (trace.rs:1199-1325) without oriented surfaces.
+ * Returns 1 and fills *e when the clipped interval is non-empty. */
+static int path_interval_jacobian(const bvo_model *m, const float o[3], const float d[3],
+                                  int bounded, uint32_t prev, uint32_t cell, uint32_t next,
+                                  float t0, float t1, bvo_path_entry *e) {
+    const float *cpp = m->points + 4 * (size_t)cell;
+    const float cp[3] = {cpp[0], cpp[1], cpp[2]};
+    const float cr = read_radius(m, cell);
+    float start = t0, end = t1;
+    int start_sphere = 0, end_sphere = 0;
+    float nj[4] = {0}, fj[4] = {0};
+    float qd_prev[4] = {0}, qd_cur[4] = {0};
+    if (bounded) {
+        float sn, sf;
+        if (!sphere_jac(o, d, cp, cr, &sn, &sf, nj, fj)) return 0;
+        if (sn > start) {
+            start = sn;
+            start_sphere = 1;
+        }
+        if (sf < end) {
+            end = sf;
+            end_sphere = 1;
+        }
+    }
+    if (start_sphere) {
+        memcpy(qd_cur, nj, 16);
+    } else if (prev != cell) {
+        const float *pp = m->points + 4 * (size_t)prev;
+        const float ppos[3] = {pp[0], pp[1], pp[2]};
+        face_jac(o, d, cp, cr, ppos, read_radius(m, prev), t0, qd_cur, qd_prev);
+    }
+    const float query_near = start;
+    if (end <= start || !isfinite(start) || !isfinite(end)) return 0;
+    float dprev[4] = {0}, dcur[4] = {0}, dnext[4] = {0};
+    for (int i = 0; i < 4; ++i) {
+        dcur[i] -= qd_cur[i];
+        dprev[i] -= qd_prev[i];
+    }
+    if (end_sphere) {
+        for (int i = 0; i < 4; ++i) dcur[i] += fj[i];
+    } else if (next != cell) {
+        const float *np = m->points + 4 * (size_t)next;
+        const float npos[3] = {np[0], np[1], np[2]};
+        float cj[4], aj[4];
+        face_jac(o, d, cp, cr, npos, read_radius(m, next), t1, cj, aj);
+        for (int i = 0; i < 4; ++i) {
+            dcur[i] += cj[i];
+            dnext[i] += aj[i];
+        }
+    }
+    e->previous_cell = prev;
+    e->cell = cell;
+    e->next_cell = next;
+    e->dt = end - start;
+    memcpy(e->dt_d_previous, dprev, 16);
+    memcpy(e->dt_d_current, dcur, 16);
+    memcpy(e->dt_d_next, dnext, 16);
+    e->surface_query_near = query_near;
+    memcpy(e->surface_query_d_previous, qd_prev, 16);
+    memcpy(e->surface_query_d_current, qd_cur, 16);
+    e->t_start = start;
+    return 1;
+}
+
+static int normalize_direction(const float in[3], float out[3]) {
+    const float len = sqrtf(dot3f(in, in));
+    if (len <= 0.0f || !isfinite(len)) return 0;
+    out[0] = in[0] / len;
+    out[1] = in[1] / len;
+    out[2] = in[2] / len;
+    return 1;
+}
+
+/* ------------------------------------------------------------------ */
+/* trace_one_ray (trace.rs:1680-1820)                                  */
+/* ------------------------------------------------------------------ */
+static bvo_trace_result trace_one_ray_impl(const bvo_model *m, const float origin[3],
+                                           const float direction[3],
+                                           const bvo_trace_settings *s, uint32_t *cells,
+                                           uint32_t cap, uint32_t *cell_count) {
+    bvo_trace_result res;
+    memset(&res, 0, sizeof(res));
+    res.last_point = s->start_point;
+    res.peak_point = -1;
+    if (cell_count) *cell_count = 0;
+    float d[3];
+    if (!normalize_direction(direction, d)) return res;
+    const float *o = origin;
+    float t0 = 0.0f, T = 1.0f;
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+    float depth_mode = 0.0f, peak_weight = 0.0f;
+    int32_t peak_point = -1;
+    uint32_t current = s->start_point;
+    const float *p = m->points + 4 * (size_t)current;
+    float cp[3] = {p[0], p[1], p[2]};
+    float cr = read_radius(m, current);
+    const int bounded = m->radii != NULL;
+    uint32_t steps = 0, visited = 0;
+    while (steps < s->max_steps) {
+        steps += 1;
+        if (T <= s->weight_threshold || t0 > s->depth) break;
+        if (cells && visited < cap) cells[visited] = current;
+        visited += 1;
+        float best;
+        const int face = find_exit_face(m, current, cp, cr, o, d, t0, s->depth, &best);
+        float ss, se;
+        if (support_interval(bounded, o, d, cp, cr, t0, best, &ss, &se)) {
+            const float dens = m->points[4 * (size_t)current + 3] * 1.0f;
+            if (dens > 1e-6f) {
+                const float dt = se - ss;
+                const float alpha = 1.0f - bvo_expf(-dens * dt);
+                const float w = T * alpha;
+                if (s->eval_mode == BVO_EVAL_CONSTANT) {
+                    acc[0] += w * s->constant_rgb[0];
+                    acc[1] += w * s->constant_rgb[1];
+                    acc[2] += w * s->constant_rgb[2];
+                } else if (s->eval_mode == BVO_EVAL_SH) {
+                    float c[3];
+                    bvo_eval_rgb_sh(m, current, d, c, NULL);
+                    acc[0] += w * c[0];
+                    acc[1] += w * c[1];
+                    acc[2] += w * c[2];
+                }
+                if (w > peak_weight) {
+                    peak_weight = w;
+                    depth_mode = 0.5f * (ss + se);
+                    peak_point = (int32_t)current;
+                }
+                T *= 1.0f - alpha;
+            }
+        }
+        if (face < 0) {
+            t0 = best;
+            break;
+        }
+        const uint32_t next = m->neighbors[m->offsets[current] + (uint32_t)face];
+        const float *np = m->points + 4 * (size_t)next;
+        t0 = fmaxf(t0, best);
+        current = next;
+        cp[0] = np[0];
+        cp[1] = np[1];
+        cp[2] = np[2];
+        cr = read_radius(m, next);
+    }
+    res.rgba[0] = acc[0];
+    res.rgba[1] = acc[1];
+    res.rgba[2] = acc[2];
+    res.rgba[3] = 1.0f - T;
+    res.steps = steps;
+    res.last_point = current;
+    res.t_end = t0;
+    res.depth_mode = depth_mode;
+    res.peak_weight = peak_weight;
+    res.peak_point = peak_point;
+    if (cell_count) *cell_count = visited;
+    return res;
+}
+
+bvo_trace_result bvo_trace_one_ray(const bvo_model *m, const float origin[3],
+                                   const float direction[3], const bvo_trace_settings *s) {
+    return trace_one_ray_impl(m, origin, direction, s, NULL, 0, NULL);
+}
+
+void bvo_render_walk(const bvo_model *m, const bvo_camera *cam, uint32_t width, uint32_t height,
+                     uint32_t max_steps, float weight_threshold, uint32_t start_point,
+                     float *out_rgba, uint32_t *out_steps, uint32_t *cells, uint32_t cap,
+                     uint32_t *cell_count, int threads) {
+    bvo_trace_settings s;
+    memset(&s, 0, sizeof(s));
+    s.weight_threshold = weight_threshold;
+    s.max_steps = max_steps;
+    s.start_point = start_point;
+    s.depth = cam->depth;
+    s.eval_mode = BVO_EVAL_SH;
+    const long total = (long)width * (long)height;
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+#endif
+    for (long i = 0; i < total; ++i) {
+        const uint32_t x = (uint32_t)(i % width), y = (uint32_t)(i / width);
+        float o[3], d[3];
+        bvo_camera_ray(cam, width, height, x, y, o, d);
+        bvo_trace_result r = trace_one_ray_impl(m, o, d, &s, cells ? cells + (size_t)i * cap : NULL,
+                                                cap, cell_count ? cell_count + i : NULL);
+        memcpy(out_rgba + 4 * (size_t)i, r.rgba, 16);
+        if (out_steps) out_steps[i] = r.steps;
+    }
+    (void)threads;
+}
+
+/* ------------------------------------------------------------------ */
+/* record_path_jacobians (trace.rs:1573-1676)                          */
+/* ------------------------------------------------------------------ */
+static int record_walk(const bvo_model *m, const float origin[3], const float direction[3],
+                       const bvo_trace_settings *s, bvo_path_entry *out, int capacity,
+                       int *truncated) {
+    float d[3];
+    *truncated = 0;
+    if (!normalize_direction(direction, d)) return 0;
+    float t0 = 0.0f;
+    uint32_t current = s->start_point, previous = current;
+    const float *p = m->points + 4 * (size_t)current;
+    float cp[3] = {p[0], p[1], p[2]};
+    float cr = read_radius(m, current);
+    const int bounded = m->radii != NULL;
+    int count = 0, finished = 0;
+    uint32_t steps = 0;
+    while (steps < s->max_steps) {
+        steps += 1;
+        if (t0 > s->depth) {
+            finished = 1;
+            break;
+        }
+        float best;
+        const int face = find_exit_face(m, current, cp, cr, origin, d, t0, s->depth, &best);
+        const uint32_t next =
+            face >= 0 ? m->neighbors[m->offsets[current] + (uint32_t)face] : current;
+        bvo_path_entry e;
+        if (path_interval_jacobian(m, origin, d, bounded, previous, current, next, t0, best, &e)) {
+            if (count < capacity) out[count] = e;
+            count += 1;
+        }
+        if (face < 0) {
+            finished = 1;
+            break;
+        }
+        t0 = fmaxf(t0, best);
+        previous = current;
+        current = next;
+        const float *np = m->points + 4 * (size_t)next;
+        cp[0] = np[0];
+        cp[1] = np[1];
+        cp[2] = np[2];
+        cr = read_radius(m, next);
+    }
+    *truncated = !finished;
+    return count;
+}
+
+int bvo_record_path_jacobians(const bvo_model *m, const float origin[3],
+                              const float direction[3], const bvo_trace_settings *s,
+                              bvo_path_entry *out, int capacity) {
+    int truncated;
+    return record_walk(m, origin, direction, s, out, capacity, &truncated);
+}
+
+/* Path recorder over whole images (PathRecorder::dispatch_batch,
+ * path_record.rs:519-594): rows [pixel][max_steps]; status = count | bit 31
+ * when the step cap stopped the walk (path_record.rs:41). */
+
+void bvo_record_image(const bvo_model *m, const bvo_camera *cams, uint32_t n_cams,
+                      uint32_t width, uint32_t height, uint32_t max_steps,
+                      const uint32_t *start_points, uint32_t *prev, uint32_t *cell,
+                      uint32_t *next, float *dt, float *jp, float *jc, float *jn,
+                      uint32_t *status, int threads) {
+    const long per_view = (long)width * (long)height;
+    const long total = per_view * (long)n_cams;
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel num_threads(threads)
+#endif
+    {
+        bvo_path_entry *buf = (bvo_path_entry *)malloc(sizeof(bvo_path_entry) * (max_steps + 1));
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 64)
+#endif
+        for (long i = 0; i < total; ++i) {
+            const uint32_t v = (uint32_t)(i / per_view);
+            const long pix = i % per_view;
+            float o[3], d[3];
+            bvo_camera_ray(&cams[v], width, height, (uint32_t)(pix % width),
+                           (uint32_t)(pix / width), o, d);
+            bvo_trace_settings s;
+            memset(&s, 0, sizeof(s));
+            s.max_steps = max_steps;
+            s.start_point = start_points[v];
+            s.depth = cams[v].depth;
+            int truncated = 0;
+            const int count = record_walk(m, o, d, &s, buf, (int)max_steps, &truncated);
+            const size_t row = (size_t)i * max_steps;
+            for (int k = 0; k < count && k < (int)max_steps; ++k) {
+                prev[row + k] = buf[k].previous_cell;
+                cell[row + k] = buf[k].cell;
+                next[row + k] = buf[k].next_cell;
+                dt[row + k] = buf[k].dt;
+                memcpy(jp + 4 * (row + k), buf[k].dt_d_previous, 16);
+                memcpy(jc + 4 * (row + k), buf[k].dt_d_current, 16);
+                memcpy(jn + 4 * (row + k), buf[k].dt_d_next, 16);
+            }
+            status[i] = (uint32_t)(count < (int)max_steps ? count : (int)max_steps) |
+                        (truncated ? 0x80000000u : 0u);
+        }
+        free(buf);
+    }
+    (void)threads;
+}
+
+/* ------------------------------------------------------------------ */
+/* PowerFoam splats (trace.rs:1327-1546)                               */
+/* ------------------------------------------------------------------ */
+static int powerfoam_splat_interval(const bvo_model *m, const float o[3], const float d[3],
+                                    float depth, uint32_t cell, bvo_path_entry *e) {
+    const float *cpp = m->points + 4 * (size_t)cell;
+    const float cur[3] = {cpp[0], cpp[1], cpp[2]};
+    const float cr = read_radius(m, cell);
+    const float cam[3] = {cur[0] - o[0], cur[1] - o[1], cur[2] - o[2]};
+    const float excl = 4.0f * cr;
+    if (dot3f(cam, cam) < excl * excl) return 0;
+    float sn, sf;
+    if (!sphere_jac(o, d, cur, cr, &sn, &sf, NULL, NULL)) return 0;
+    if (sf <= 0.0f || sn >= depth) return 0;
+    float face_near = 0.0f, face_far = depth;
+    uint32_t previous = cell, next = cell;
+    for (uint32_t k = m->offsets[cell]; k < m->offsets[cell + 1]; ++k) {
+        const uint32_t a = m->neighbors[k];
+        const float *ap = m->points + 4 * (size_t)a;
+        const float ar = read_radius(m, a);
+        const float n[3] = {ap[0] - cur[0], ap[1] - cur[1], ap[2] - cur[2]};
+        const float dsq = fmaxf(dot3f(n, n), 1.0e-20f);
+        const float shift = 0.5f + 0.5f * (cr * cr - ar * ar) / dsq;
+        const float fo[3] = {cur[0] + shift * n[0], cur[1] + shift * n[1], cur[2] + shift * n[2]};
+        const float rel[3] = {fo[0] - o[0], fo[1] - o[1], fo[2] - o[2]};
+        const float num = dot3f(rel, n);
+        const float den = dot3f(d, n);
+        if (den > 1.0e-20f) {
+            const float t = num / den;
+            if (t < face_far) {
+                face_far = t;
+                next = a;
+            }
+        } else if (den < -1.0e-20f) {
+            const float t = num / den;
+            if (t > face_near) {
+                face_near = t;
+                previous = a;
+            }
+        } else if (num < 0.0f) {
+            return 0;
+        }
+    }
+    return path_interval_jacobian(m, o, d, 1, previous, cell, next, face_near, face_far, e);
+}
+
+static int cmp_entry(const void *a, const void *b) {
+    const bvo_path_entry *x = (const bvo_path_entry *)a, *y = (const bvo_path_entry *)b;
+    /* total_cmp on the entry depth, then cell index (trace.rs:1404-1408). */
+    if (x->t_start < y->t_start) return -1;
+    if (x->t_start > y->t_start) return 1;
+    if (x->cell < y->cell) return -1;
+    if (x->cell > y->cell) return 1;
+    return 0;
+}
+
+static int sorted_splats(const bvo_model *m, const float o[3], const float d[3], float depth,
+                         uint32_t max_steps, bvo_path_entry **out) {
+    int cap = 64, count = 0;
+    bvo_path_entry *buf = (bvo_path_entry *)malloc(sizeof(bvo_path_entry) * (size_t)cap);
+    for (uint32_t cell = 0; cell < m->n; ++cell) {
+        bvo_path_entry e;
+        if (powerfoam_splat_interval(m, o, d, depth, cell, &e)) {
+            if (count == cap) {
+                cap *= 2;
+                buf = (bvo_path_entry *)realloc(buf, sizeof(bvo_path_entry) * (size_t)cap);
+            }
+            buf[count++] = e;
+        }
+    }
+    qsort(buf, (size_t)count, sizeof(bvo_path_entry), cmp_entry);
+    if ((uint32_t)count > max_steps) count = (int)max_steps;
+    *out = buf;
+    return count;
+}
+
+int bvo_record_powerfoam_splats(const bvo_model *m, const float origin[3],
+                                const float direction[3], const bvo_trace_settings *s,
+                                bvo_path_entry *out, int capacity) {
+    float d[3];
+    if (!normalize_direction(direction, d)) return 0;
+    bvo_path_entry *buf = NULL;
+    const int count = sorted_splats(m, origin, d, s->depth, s->max_steps, &buf);
+    for (int i = 0; i < count && i < capacity; ++i) out[i] = buf[i];
+    free(buf);
+    return count;
+}
+
+bvo_trace_result bvo_trace_powerfoam_splats(const bvo_model *m, const float origin[3],
+                                            const float direction[3],
+                                            const bvo_trace_settings *s) {
+    bvo_trace_result res;
+    memset(&res, 0, sizeof(res));
+    res.last_point = s->start_point;
+    res.peak_point = -1;
+    float d[3];
+    if (!normalize_direction(direction, d)) return res;
+    bvo_path_entry *buf = NULL;
+    const int count = sorted_splats(m, origin, d, s->depth, s->max_steps, &buf);
+    float T = 1.0f, acc[3] = {0, 0, 0}, depth_mode = 0.0f, peak_weight = 0.0f, t_end = 0.0f;
+    int32_t peak_point = -1;
+    uint32_t steps = 0, last = s->start_point;
+    for (int i = 0; i < count; ++i) {
+        if (T <= s->weight_threshold) break;
+        const bvo_path_entry *e = &buf[i];
+        steps += 1;
+        last = e->cell;
+        t_end = e->t_start + e->dt;
+        const float dens = m->points[4 * (size_t)e->cell + 3] * 1.0f;
+        if (dens <= 1.0e-6f) continue;
+        const float alpha = 1.0f - bvo_expf(-dens * e->dt);
+        const float w = T * alpha;
+        if (s->eval_mode == BVO_EVAL_CONSTANT) {
+            acc[0] += w * s->constant_rgb[0];
+            acc[1] += w * s->constant_rgb[1];
+            acc[2] += w * s->constant_rgb[2];
+        } else if (s->eval_mode == BVO_EVAL_SH) {
+            float c[3];
+            bvo_eval_rgb_sh(m, e->cell, d, c, NULL);
+            acc[0] += w * c[0];
+            acc[1] += w * c[1];
+            acc[2] += w * c[2];
+        }
+        if (w > peak_weight) {
+            peak_weight = w;
+            depth_mode = e->t_start + 0.5f * e->dt;
+            peak_point = (int32_t)e->cell;
+        }
+        T *= 1.0f - alpha;
+    }
+    free(buf);
+    res.rgba[0] = acc[0];
+    res.rgba[1] = acc[1];
+    res.rgba[2] = acc[2];
+    res.rgba[3] = 1.0f - T;
+    res.steps = steps;
+    res.last_point = last;
+    res.t_end = t_end;
+    res.depth_mode = depth_mode;
+    res.peak_weight = peak_weight;
+    res.peak_point = peak_point;
+    return res;
+}
+
+void bvo_render_splats(const bvo_model *m, const bvo_camera *cam, uint32_t width,
+                       uint32_t height, uint32_t max_steps, float weight_threshold,
+                       float *out_rgba, uint32_t *out_steps, int threads) {
+    bvo_trace_settings s;
+    memset(&s, 0, sizeof(s));
+    s.weight_threshold = weight_threshold;
+    s.max_steps = max_steps;
+    s.depth = cam->depth;
+    s.eval_mode = BVO_EVAL_SH;
+    const long total = (long)width * (long)height;
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads)
+#endif
+    for (long i = 0; i < total; ++i) {
+        const uint32_t x = (uint32_t)(i % width), y = (uint32_t)(i / width);
+        float o[3], d[3];
+        bvo_camera_ray(cam, width, height, x, y, o, d);
+        bvo_trace_result r = bvo_trace_powerfoam_splats(m, o, d, &s);
+        memcpy(out_rgba + 4 * (size_t)i, r.rgba, 16);
+        if (out_steps) out_steps[i] = r.steps;
+    }
+    (void)threads;
+}
+
+/* ------------------------------------------------------------------ */
+/* start cell                                                          */
+/* ------------------------------------------------------------------ */
+/* Exact power-nearest site in FP64, ties to the lowest index; the FP32
+ * restatement of lib.rs:526-541 is bvo_containing_cell_f32 below. */
+uint32_t bvo_containing_cell_f64(const bvo_model *m, const float position[3]) {
+    uint32_t best = 0;
+    double best_d = INFINITY;
+    for (uint32_t i = 0; i < m->n; ++i) {
+        const float *p = m->points + 4 * (size_t)i;
+        const double dx = (double)position[0] - (double)p[0];
+        const double dy = (double)position[1] - (double)p[1];
+        const double dz = (double)position[2] - (double)p[2];
+        const double r = m->radii ? (double)m->radii[i] : 0.0;
+        const double dist = (dx * dx + dy * dy + dz * dz) - r * r;
+        if (dist < best_d) {
+            best_d = dist;
+            best = i;
+        }
+    }
+    return best;
+}
+
+uint32_t bvo_containing_cell_f32(const bvo_model *m, const float position[3]) {
+    uint32_t best = 0;
+    float best_d = INFINITY;
+    for (uint32_t i = 0; i < m->n; ++i) {
+        const float *p = m->points + 4 * (size_t)i;
+        const float dv[3] = {position[0] - p[0], position[1] - p[1], position[2] - p[2]};
+        const float r = read_radius(m, i);
+        const float dist = dot3f(dv, dv) - r * r;
+        if (dist < best_d) {
+            best_d = dist;
+            best = i;
+        }
+    }
+    return best;
+}
+
+/* ------------------------------------------------------------------ */
+/* gradient oracle                                                     */
+/* ------------------------------------------------------------------ */
+enum { ROLE_FIXED = 0, ROLE_FACE = 1, ROLE_SPHERE = 2 };
+
+typedef struct {
+    uint32_t prev, cell, next;
+    uint8_t start_role, end_role;
+} seg_t;
+
+/* Recorded walk of the training contract: record_path_jacobians' loop
+ * (trace.rs:1573-1676) with the FP32 transmittance cut of trace_one_ray
+ * (trace.rs:1724) evaluated on dt clamped to max_dt (diff_render.rs:2484).
+ * Identical, operation for operation, to the device fwd+bwd walk. */
+static int record_training_walk(const bvo_model *m, const float o[3], const float d[3],
+                                uint32_t start, uint32_t max_steps, float depth, float thr,
+                                float max_dt, seg_t *segs) {
+    float t0 = 0.0f, T = 1.0f;
+    uint32_t current = start, previous = start;
+    const float *p = m->points + 4 * (size_t)current;
+    float cp[3] = {p[0], p[1], p[2]};
+    float cr = read_radius(m, current);
+    const int bounded = m->radii != NULL;
+    int count = 0;
+    uint32_t steps = 0;
+    while (steps < max_steps) {
+        steps += 1;
+        if (T <= thr || t0 > depth) break;
+        float best;
+        const int face = find_exit_face(m, current, cp, cr, o, d, t0, depth, &best);
+        const uint32_t next =
+            face >= 0 ? m->neighbors[m->offsets[current] + (uint32_t)face] : current;
+        float start_t = t0, end_t = best;
+        uint8_t srole = previous != current ? ROLE_FACE : ROLE_FIXED;
+        uint8_t erole = next != current ? ROLE_FACE : ROLE_FIXED;
+        int ok = 1;
+        if (bounded) {
+            float sn, sf;
+            if (!sphere_jac(o, d, cp, cr, &sn, &sf, NULL, NULL)) {
+                ok = 0;
+            } else {
+                if (sn > start_t) {
+                    start_t = sn;
+                    srole = ROLE_SPHERE;
+                }
+                if (sf < end_t) {
+                    end_t = sf;
+                    erole = ROLE_SPHERE;
+                }
+            }
+        }
+        if (ok && end_t > start_t && isfinite(start_t) && isfinite(end_t)) {
+            seg_t sg = {previous, current, next, srole, erole};
+            segs[count++] = sg;
+            const float dens = m->points[4 * (size_t)current + 3];
+            if (dens > 1e-6f) {
+                const float dt = fminf(end_t - start_t, max_dt);
+                const float alpha = 1.0f - bvo_expf(-dens * dt);
+                T *= 1.0f - alpha;
+            }
+        }
+        if (face < 0) break;
+        t0 = fmaxf(t0, best);
+        previous = current;
+        current = next;
+        const float *np = m->points + 4 * (size_t)next;
+        cp[0] = np[0];
+        cp[1] = np[1];
+        cp[2] = np[2];
+        cr = read_radius(m, next);
+    }
+    return count;
+}
+
+typedef struct {
+    const double *pts; /* [n*4] */
+    const double *sh;  /* [n*3K] */
+    const double *rad; /* [n] or NULL */
+} dparams;
+
+static inline double drad(const dparams *P, uint32_t i) { return P->rad ? P->rad[i] : 0.0; }
+
+/* Radical-plane hit t of face (c -> a) and its Jacobian (trace.rs:1077). */
+static double face_t_d(const dparams *P, const double o[3], const double d[3], uint32_t c,
+                       uint32_t a, double jc[4], double ja[4]) {
+    const double *cp = P->pts + 4 * (size_t)c, *ap = P->pts + 4 * (size_t)a;
+    const double rc = drad(P, c), ra = drad(P, a);
+    const double n[3] = {ap[0] - cp[0], ap[1] - cp[1], ap[2] - cp[2]};
+    double dsq = dot3d(n, n);
+    if (dsq < 1e-20) dsq = 1e-20;
+    const double shift = 0.5 + 0.5 * (rc * rc - ra * ra) / dsq;
+    const double rel[3] = {cp[0] + shift * n[0] - o[0], cp[1] + shift * n[1] - o[1],
+                           cp[2] + shift * n[2] - o[2]};
+    const double den = dot3d(n, d);
+    const double t = dot3d(rel, n) / den;
+    if (fabs(den) <= 1e-20) {
+        memset(jc, 0, 32);
+        memset(ja, 0, 32);
+        return t;
+    }
+    for (int i = 0; i < 3; ++i) {
+        jc[i] = (o[i] - cp[i] + t * d[i]) / den;
+        ja[i] = (ap[i] - o[i] - t * d[i]) / den;
+    }
+    jc[3] = rc / den;
+    ja[3] = -ra / den;
+    return t;
+}
+
+static int sphere_t_d(const dparams *P, const double o[3], const double d[3], uint32_t c,
+                      int far_side, double *t, double j[4]) {
+    const double *cp = P->pts + 4 * (size_t)c;
+    const double r = drad(P, c);
+    const double oc[3] = {o[0] - cp[0], o[1] - cp[1], o[2] - cp[2]};
+    const double b = dot3d(oc, d);
+    const double disc = b * b - (dot3d(oc, oc) - r * r);
+    if (disc <= 0.0) return 0;
+    const double root = sqrt(disc);
+    const double sgn = far_side ? 1.0 : -1.0;
+    *t = -b + sgn * root;
+    for (int i = 0; i < 3; ++i) j[i] = d[i] + sgn * (oc[i] - b * d[i]) / root;
+    j[3] = sgn * r / root;
+    return 1;
+}
+
+typedef struct {
+    double dt_raw, dt, sigma, alpha, T, w;
+    double c[3], cu[3];
+    double j_prev[4], j_cur[4], j_next[4];
+} seg_eval_t;
+
+static void eval_segment(const dparams *P, uint32_t K, const double o[3], const double d[3],
+                         const double Y[16], const seg_t *sg, double depth, seg_eval_t *ev) {
+    memset(ev, 0, sizeof(*ev));
+    double t_start = 0.0, t_end = 0.0;
+    double jc[4], ja[4];
+    /* start boundary */
+    if (sg->start_role == ROLE_FACE) {
+        t_start = face_t_d(P, o, d, sg->cell, sg->prev, jc, ja);
+        for (int i = 0; i < 4; ++i) {
+            ev->j_cur[i] -= jc[i];
+            ev->j_prev[i] -= ja[i];
+        }
+    } else if (sg->start_role == ROLE_SPHERE) {
+        double j[4];
+        sphere_t_d(P, o, d, sg->cell, 0, &t_start, j);
+        for (int i = 0; i < 4; ++i) ev->j_cur[i] -= j[i];
+    } else {
+        t_start = 0.0;
+    }
+    /* end boundary */
+    if (sg->end_role == ROLE_FACE) {
+        t_end = face_t_d(P, o, d, sg->cell, sg->next, jc, ja);
+        for (int i = 0; i < 4; ++i) {
+            ev->j_cur[i] += jc[i];
+            ev->j_next[i] += ja[i];
+        }
+    } else if (sg->end_role == ROLE_SPHERE) {
+        double j[4];
+        sphere_t_d(P, o, d, sg->cell, 1, &t_end, j);
+        for (int i = 0; i < 4; ++i) ev->j_cur[i] += j[i];
+    } else {
+        t_end = depth; /* no exit face: the fixed far plane */
+    }
+    ev->dt_raw = t_end - t_start;
+    const double *c = P->sh + (size_t)sg->cell * 3u * K;
+    for (int ch = 0; ch < 3; ++ch) {
+        double acc = 0.0;
+        for (uint32_t k = 0; k < K; ++k) acc += Y[k] * c[3 * k + ch];
+        ev->cu[ch] = 0.5 + acc;
+        ev->c[ch] = ev->cu[ch] > 0.0 ? ev->cu[ch] : 0.0;
+    }
+    ev->sigma = P->pts[4 * (size_t)sg->cell + 3];
+}
+
+double bvo_forward_backward(const bvo_model *m, const bvo_camera *cams, uint32_t n_cams,
+                            uint32_t width, uint32_t height, uint32_t max_steps,
+                            float weight_threshold, float max_dt, const float *target,
+                            int loss_kind, const bvo_params_f64 *override_params,
+                            double *out_rgb, double *d_density, double *d_sh, double *d_pos,
+                            double *d_radius, int threads) {
+    const uint32_t deg = m->sh_degree > 3 ? 3 : m->sh_degree;
+    const uint32_t K = sh_comps(deg);
+    /* FP64 parameter view */
+    double *own_pts = NULL, *own_sh = NULL, *own_rad = NULL;
+    dparams P;
+    if (override_params) {
+        P.pts = override_params->points;
+        P.sh = override_params->sh;
+        P.rad = override_params->radii;
+    } else {
+        own_pts = (double *)malloc(sizeof(double) * 4 * (size_t)m->n);
+        own_sh = (double *)malloc(sizeof(double) * 3 * K * (size_t)m->n);
+        for (size_t i = 0; i < 4 * (size_t)m->n; ++i) own_pts[i] = m->points[i];
+        for (size_t i = 0; i < 3 * (size_t)K * m->n; ++i) own_sh[i] = m->sh[i];
+        if (m->radii) {
+            own_rad = (double *)malloc(sizeof(double) * (size_t)m->n);
+            for (size_t i = 0; i < m->n; ++i) own_rad[i] = m->radii[i];
+        }
+        P.pts = own_pts;
+        P.sh = own_sh;
+        P.rad = own_rad;
+    }
+    const long per_view = (long)width * (long)height;
+    const long total = per_view * (long)n_cams;
+    const double M = 3.0 * (double)total;
+    double loss = 0.0;
+    uint32_t *starts = (uint32_t *)malloc(sizeof(uint32_t) * n_cams);
+    for (uint32_t v = 0; v < n_cams; ++v) starts[v] = bvo_containing_cell_f64(m, cams[v].position);
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel num_threads(threads)
+#endif
+    {
+        seg_t *segs = (seg_t *)malloc(sizeof(seg_t) * (max_steps + 1));
+        seg_eval_t *evs = (seg_eval_t *)malloc(sizeof(seg_eval_t) * (max_steps + 1));
+        double local_loss = 0.0;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 32)
+#endif
+        for (long i = 0; i < total; ++i) {
+            const uint32_t v = (uint32_t)(i / per_view);
+            const long pix = i % per_view;
+            const uint32_t x = (uint32_t)(pix % width), y = (uint32_t)(pix / width);
+            float of[3], df[3], dn[3];
+            bvo_camera_ray(&cams[v], width, height, x, y, of, df);
+            double C[3] = {0, 0, 0};
+            int nseg = 0;
+            double o[3] = {of[0], of[1], of[2]}, d[3] = {0, 0, 0}, Y[16];
+            if (normalize_direction(df, dn)) {
+                d[0] = dn[0];
+                d[1] = dn[1];
+                d[2] = dn[2];
+                nseg = record_training_walk(m, of, dn, starts[v], max_steps, cams[v].depth,
+                                            weight_threshold, max_dt, segs);
+            }
+            sh_basis_d(deg, d, Y);
+            double T = 1.0;
+            for (int k = 0; k < nseg; ++k) {
+                seg_eval_t *ev = &evs[k];
+                eval_segment(&P, K, o, d, Y, &segs[k], (double)cams[v].depth, ev);
+                double dt = ev->dt_raw;
+                if (dt < 0.0) dt = 0.0;
+                if (dt > (double)max_dt) dt = (double)max_dt;
+                ev->dt = dt;
+                ev->T = T;
+                if (ev->sigma > 1e-6) {
+                    ev->alpha = 1.0 - exp(-ev->sigma * dt);
+                    ev->w = T * ev->alpha;
+                    for (int ch = 0; ch < 3; ++ch) C[ch] += ev->w * ev->c[ch];
+                    T *= 1.0 - ev->alpha;
+                } else {
+                    ev->alpha = 0.0;
+                    ev->w = 0.0;
+                }
+            }
+            double g[3];
+            const float *tg = target ? target + 3 * (size_t)i : NULL;
+            for (int ch = 0; ch < 3; ++ch) {
+                const double diff = C[ch] - (tg ? (double)tg[ch] : 0.0);
+                if (loss_kind == 0) {
+                    local_loss += diff * diff / M;
+                    g[ch] = 2.0 * diff / M;
+                } else {
+                    local_loss += fabs(diff) / M;
+                    g[ch] = (diff > 0.0 ? 1.0 : (diff < 0.0 ? -1.0 : 0.0)) / M;
+                }
+                if (out_rgb) out_rgb[3 * (size_t)i + ch] = C[ch];
+            }
+            if (!d_density) continue;
+            double S[3] = {0, 0, 0};
+            for (int k = nseg - 1; k >= 0; --k) {
+                const seg_eval_t *ev = &evs[k];
+                if (ev->sigma <= 1e-6) continue;
+                const double Tn = ev->T * (1.0 - ev->alpha);
+                double gs = 0.0;
+                for (int ch = 0; ch < 3; ++ch) gs += g[ch] * (Tn * ev->c[ch] - S[ch]);
+                const uint32_t cell = segs[k].cell;
+#ifdef _OPENMP
+#pragma omp atomic update
+#endif
+                d_density[cell] += ev->dt * gs;
+                for (int ch = 0; ch < 3; ++ch) {
+                    if (ev->cu[ch] > 0.0) {
+                        for (uint32_t mm = 0; mm < K; ++mm) {
+                            const double val = g[ch] * ev->w * Y[mm];
+#ifdef _OPENMP
+#pragma omp atomic update
+#endif
+                            d_sh[(size_t)cell * 3 * K + 3 * mm + ch] += val;
+                        }
+                    }
+                }
+                const int dt_active = ev->dt_raw > 0.0 && ev->dt_raw < (double)max_dt;
+                if (dt_active && d_pos) {
+                    const double gdt = ev->sigma * gs;
+                    const uint32_t who[3] = {segs[k].prev, cell, segs[k].next};
+                    const double *js[3] = {ev->j_prev, ev->j_cur, ev->j_next};
+                    for (int r = 0; r < 3; ++r) {
+                        for (int a = 0; a < 3; ++a) {
+                            const double val = gdt * js[r][a];
+                            if (val != 0.0) {
+#ifdef _OPENMP
+#pragma omp atomic update
+#endif
+                                d_pos[3 * (size_t)who[r] + a] += val;
+                            }
+                        }
+                        if (d_radius && js[r][3] != 0.0) {
+                            const double val = gdt * js[r][3];
+#ifdef _OPENMP
+#pragma omp atomic update
+#endif
+                            d_radius[who[r]] += val;
+                        }
+                    }
+                }
+                for (int ch = 0; ch < 3; ++ch) S[ch] += ev->w * ev->c[ch];
+            }
+        }
+#ifdef _OPENMP
+#pragma omp atomic update
+#endif
+        loss += local_loss;
+        free(segs);
+        free(evs);
+    }
+    free(starts);
+    free(own_pts);
+    free(own_sh);
+    free(own_rad);
+    (void)threads;
+    return loss;
+}

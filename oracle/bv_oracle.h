@@ -1,0 +1,169 @@
+/*
+ * CPU oracle for the blade-volume ray-tracing hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker that the CUDA path
+ * is compared against; nothing in the shipped library links or calls it.
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
+ *
+ * It restates, in plain C, the reference crate's CPU tracer
+ * (blade-volume/src/trace.rs) and shading code (blade-volume/src/relight.rs,
+ * blade-volume/shaders/relight.wgsl).  Every function cites the reference
+ * lines it follows.  FP32 arithmetic is kept in the reference's operation
+ * order and compiled with -ffp-contract=off so that no multiply-add is fused
+ * behind the code's back; the few fused operations that the product kernels
+ * also use are written as explicit fmaf() calls.
+ *
+ * Parity is pinned against the reference's own known-answer tests
+ * (trace.rs tests, gpu/radfoam.rs point-index tests, relight.rs tests);
+ * tests/test_oracle_golden.py replays them.  The reference itself (Rust +
+ * WGSL) cannot be compiled or run on this machine.
+ */
+#ifndef BV_ORACLE_H
+#define BV_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* PointCloudModel (blade-volume/src/lib.rs:174-239), walk subset. */
+typedef struct {
+    const float *points;       /* [n*4] x, y, z, density (lib.rs:176) */
+    const float *radii;        /* [n] or NULL for plain RadFoam (lib.rs:195) */
+    const float *sh;           /* [n*3*K], [point][component][rgb] (lib.rs:178-185) */
+    uint32_t sh_degree;        /* 0..3 */
+    const uint32_t *offsets;   /* CSR [n+1] */
+    const uint32_t *neighbors; /* CSR [offsets[n]] */
+    uint32_t n;
+} bvo_model;
+
+/* CameraParams (blade-volume/src/camera.rs:9-18), 48 bytes. */
+typedef struct {
+    float position[3];
+    float depth;
+    float orientation[4]; /* quaternion x, y, z, w */
+    float fov[2];
+    float principal[2];
+} bvo_camera;
+
+enum { BVO_EVAL_OPACITY = 0, BVO_EVAL_CONSTANT = 1, BVO_EVAL_SH = 2 };
+
+/* TraceSettings (trace.rs:50-69). */
+typedef struct {
+    float weight_threshold;
+    uint32_t max_steps;
+    uint32_t start_point;
+    float depth;
+    int eval_mode;
+    float constant_rgb[3];
+} bvo_trace_settings;
+
+/* TraceResult (trace.rs:71-103). peak_point = -1 for None. */
+typedef struct {
+    float rgba[4];
+    uint32_t steps;
+    uint32_t last_point;
+    float t_end;
+    float depth_mode;
+    float peak_weight;
+    int32_t peak_point;
+} bvo_trace_result;
+
+/* PathJacobianEntry (trace.rs:1021-1041), geometry subset. */
+typedef struct {
+    uint32_t previous_cell, cell, next_cell;
+    float dt;
+    float dt_d_previous[4];
+    float dt_d_current[4];
+    float dt_d_next[4];
+    float surface_query_near;
+    float surface_query_d_previous[4];
+    float surface_query_d_current[4];
+    float t_start; /* entry depth of the interval (splat sort key) */
+} bvo_path_entry;
+
+/* ---- arithmetic shared bit-for-bit with the CUDA kernels ---- */
+float bvo_expf(float x);
+float bvo_tan_half(float fov);
+void bvo_camera_ray(const bvo_camera *cam, uint32_t width, uint32_t height, uint32_t x,
+                    uint32_t y, float origin[3], float dir[3]);
+void bvo_eval_rgb_sh(const bvo_model *m, uint32_t point, const float dir[3], float out[3],
+                     float unclamped[3]);
+
+/* support_interval (trace.rs:209-238): returns 1 and out = (start, end). */
+int bvo_support_interval(int bounded, const float o[3], const float d[3], const float c[3],
+                         float radius, float t0, float t1, float out[2]);
+
+/* ---- forward walk (trace.rs:1680-1820) ---- */
+bvo_trace_result bvo_trace_one_ray(const bvo_model *m, const float origin[3],
+                                   const float direction[3], const bvo_trace_settings *s);
+
+/* Image loop (blade-volume-train/src/render.rs:113-160) with the GPU ray
+ * mapping (radfoam.wgsl:44-52); start_point is used as given.
+ * out_rgba [h*w*4]; out_steps [h*w] may be NULL; cells [h*w*cap] (may be NULL)
+ * receives the visited cell of every loop iteration, cell_count [h*w] the
+ * number written (not truncated by cap). */
+void bvo_render_walk(const bvo_model *m, const bvo_camera *cam, uint32_t width, uint32_t height,
+                     uint32_t max_steps, float weight_threshold, uint32_t start_point,
+                     float *out_rgba, uint32_t *out_steps, uint32_t *cells, uint32_t cap,
+                     uint32_t *cell_count, int threads);
+
+/* ---- path recorder (trace.rs:1548-1676) ---- */
+int bvo_record_path_jacobians(const bvo_model *m, const float origin[3],
+                              const float direction[3], const bvo_trace_settings *s,
+                              bvo_path_entry *out, int capacity);
+
+/* Path recorder over images of n_cams cameras: rows [P][max_steps] of the
+ * recorded entries; jp/jc/jn are [P*max_steps*4]; status [P] = count | bit 31
+ * when truncated by the step cap.  Unwritten slots are left untouched. */
+void bvo_record_image(const bvo_model *m, const bvo_camera *cams, uint32_t n_cams,
+                      uint32_t width, uint32_t height, uint32_t max_steps,
+                      const uint32_t *start_points, uint32_t *prev, uint32_t *cell,
+                      uint32_t *next, float *dt, float *jp, float *jc, float *jn,
+                      uint32_t *status, int threads);
+
+/* ---- PowerFoam splats (trace.rs:1327-1546) ---- */
+int bvo_record_powerfoam_splats(const bvo_model *m, const float origin[3],
+                                const float direction[3], const bvo_trace_settings *s,
+                                bvo_path_entry *out, int capacity);
+bvo_trace_result bvo_trace_powerfoam_splats(const bvo_model *m, const float origin[3],
+                                            const float direction[3],
+                                            const bvo_trace_settings *s);
+void bvo_render_splats(const bvo_model *m, const bvo_camera *cam, uint32_t width,
+                       uint32_t height, uint32_t max_steps, float weight_threshold,
+                       float *out_rgba, uint32_t *out_steps, int threads);
+
+/* ---- start cell (lib.rs:526-541; gpu/radfoam.rs:77-112) ---- */
+uint32_t bvo_containing_cell_f64(const bvo_model *m, const float position[3]);
+uint32_t bvo_containing_cell_f32(const bvo_model *m, const float position[3]);
+
+/* ---- gradient oracle (FP64 over the FP32 walk's fixed path) ----
+ * The training contract of blade-volume-train/src/diff_render.rs:943-1923:
+ * recorded walk, dt clamped to max_dt (MAX_PATH_DT, :2510), raw = sigma*dt,
+ * T = exp(-exclusive_cumsum), alpha = 1-exp(-raw), per-cell ReLU colour
+ * (:2301-2303), per-pixel sum, loss over all pixel channels of the batch.
+ * loss_kind 0 = L2 (mean squared error, metrics.rs:7), 1 = L1 (mean abs).
+ * Gradients are accumulated (+=) into caller-zeroed FP64 tables:
+ * d_density [n], d_sh [n*3K], d_pos [n*3], d_radius [n] (may be NULL).
+ * params_override: if non-NULL, [n*4] FP64 positions+density and
+ * [n*3K] FP64 SH and [n] FP64 radii replace the model values in the
+ * integration (cells and boundary roles stay those of the FP32 walk), which
+ * is what central finite differences on a fixed path need. */
+typedef struct {
+    const double *points; /* [n*4] */
+    const double *sh;     /* [n*3K] */
+    const double *radii;  /* [n] or NULL */
+} bvo_params_f64;
+
+double bvo_forward_backward(const bvo_model *m, const bvo_camera *cams, uint32_t n_cams,
+                            uint32_t width, uint32_t height, uint32_t max_steps,
+                            float weight_threshold, float max_dt, const float *target,
+                            int loss_kind, const bvo_params_f64 *override_params,
+                            double *out_rgb, double *d_density, double *d_sh, double *d_pos,
+                            double *d_radius, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

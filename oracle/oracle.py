@@ -1,0 +1,325 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+Wraps oracle/_build/libbv_oracle.so (built by oracle/build.py) with numpy in
+and out.  Every function here is a checker: tests compare the CUDA library's
+results against these.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import build as _build
+
+_lib = None
+
+f32p = C.POINTER(C.c_float)
+f64p = C.POINTER(C.c_double)
+u32p = C.POINTER(C.c_uint32)
+
+
+class Model(C.Structure):
+    _fields_ = [("points", f32p), ("radii", f32p), ("sh", f32p), ("sh_degree", C.c_uint32),
+                ("offsets", u32p), ("neighbors", u32p), ("n", C.c_uint32)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("depth", C.c_float), ("orientation", C.c_float * 4),
+                ("fov", C.c_float * 2), ("principal", C.c_float * 2)]
+
+
+class Settings(C.Structure):
+    _fields_ = [("weight_threshold", C.c_float), ("max_steps", C.c_uint32),
+                ("start_point", C.c_uint32), ("depth", C.c_float), ("eval_mode", C.c_int),
+                ("constant_rgb", C.c_float * 3)]
+
+
+class TraceResult(C.Structure):
+    _fields_ = [("rgba", C.c_float * 4), ("steps", C.c_uint32), ("last_point", C.c_uint32),
+                ("t_end", C.c_float), ("depth_mode", C.c_float), ("peak_weight", C.c_float),
+                ("peak_point", C.c_int32)]
+
+
+class PathEntry(C.Structure):
+    _fields_ = [("previous_cell", C.c_uint32), ("cell", C.c_uint32), ("next_cell", C.c_uint32),
+                ("dt", C.c_float), ("dt_d_previous", C.c_float * 4),
+                ("dt_d_current", C.c_float * 4), ("dt_d_next", C.c_float * 4),
+                ("surface_query_near", C.c_float), ("surface_query_d_previous", C.c_float * 4),
+                ("surface_query_d_current", C.c_float * 4), ("t_start", C.c_float)]
+
+
+class ParamsF64(C.Structure):
+    _fields_ = [("points", f64p), ("sh", f64p), ("radii", f64p)]
+
+
+EVAL_OPACITY, EVAL_CONSTANT, EVAL_SH = 0, 1, 2
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = _build.build()
+        L = C.CDLL(path)
+        L.bvo_expf.restype = C.c_float
+        L.bvo_expf.argtypes = [C.c_float]
+        L.bvo_tan_half.restype = C.c_float
+        L.bvo_tan_half.argtypes = [C.c_float]
+        L.bvo_camera_ray.argtypes = [C.POINTER(Camera), C.c_uint32, C.c_uint32, C.c_uint32,
+                                     C.c_uint32, f32p, f32p]
+        L.bvo_eval_rgb_sh.argtypes = [C.POINTER(Model), C.c_uint32, f32p, f32p, f32p]
+        L.bvo_trace_one_ray.restype = TraceResult
+        L.bvo_trace_one_ray.argtypes = [C.POINTER(Model), f32p, f32p, C.POINTER(Settings)]
+        L.bvo_render_walk.argtypes = [C.POINTER(Model), C.POINTER(Camera), C.c_uint32, C.c_uint32,
+                                      C.c_uint32, C.c_float, C.c_uint32, f32p, u32p, u32p,
+                                      C.c_uint32, u32p, C.c_int]
+        L.bvo_record_path_jacobians.restype = C.c_int
+        L.bvo_record_path_jacobians.argtypes = [C.POINTER(Model), f32p, f32p, C.POINTER(Settings),
+                                                C.POINTER(PathEntry), C.c_int]
+        L.bvo_record_powerfoam_splats.restype = C.c_int
+        L.bvo_record_powerfoam_splats.argtypes = [C.POINTER(Model), f32p, f32p,
+                                                  C.POINTER(Settings), C.POINTER(PathEntry),
+                                                  C.c_int]
+        L.bvo_trace_powerfoam_splats.restype = TraceResult
+        L.bvo_trace_powerfoam_splats.argtypes = [C.POINTER(Model), f32p, f32p,
+                                                 C.POINTER(Settings)]
+        L.bvo_render_splats.argtypes = [C.POINTER(Model), C.POINTER(Camera), C.c_uint32,
+                                        C.c_uint32, C.c_uint32, C.c_float, f32p, u32p, C.c_int]
+        L.bvo_record_image.argtypes = [C.POINTER(Model), C.POINTER(Camera), C.c_uint32,
+                                       C.c_uint32, C.c_uint32, C.c_uint32, u32p, u32p, u32p,
+                                       u32p, f32p, f32p, f32p, f32p, u32p, C.c_int]
+        L.bvo_support_interval.restype = C.c_int
+        L.bvo_support_interval.argtypes = [C.c_int, f32p, f32p, f32p, C.c_float, C.c_float,
+                                           C.c_float, f32p]
+        L.bvo_containing_cell_f64.restype = C.c_uint32
+        L.bvo_containing_cell_f64.argtypes = [C.POINTER(Model), f32p]
+        L.bvo_containing_cell_f32.restype = C.c_uint32
+        L.bvo_containing_cell_f32.argtypes = [C.POINTER(Model), f32p]
+        L.bvo_forward_backward.restype = C.c_double
+        L.bvo_forward_backward.argtypes = [C.POINTER(Model), C.POINTER(Camera), C.c_uint32,
+                                           C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
+                                           C.c_float, f32p, C.c_int, C.POINTER(ParamsF64), f64p,
+                                           f64p, f64p, f64p, f64p, C.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a, t):
+    if a is None:
+        return C.cast(None, t)
+    return a.ctypes.data_as(t)
+
+
+class OracleModel:
+    """Holds contiguous copies of a PointCloudModel's arrays for the C side."""
+
+    def __init__(self, points, sh, sh_degree, offsets, neighbors, radii=None):
+        self.points = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 4)
+        self.sh = np.ascontiguousarray(sh, dtype=np.float32).reshape(-1)
+        self.offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+        self.neighbors = np.ascontiguousarray(neighbors, dtype=np.uint32)
+        if len(self.neighbors) == 0:
+            self.neighbors = np.zeros(1, dtype=np.uint32)
+        self.radii = None if radii is None else np.ascontiguousarray(radii, dtype=np.float32)
+        self.sh_degree = int(sh_degree)
+        self.c = Model(_ptr(self.points, f32p), _ptr(self.radii, f32p), _ptr(self.sh, f32p),
+                       self.sh_degree, _ptr(self.offsets, u32p), _ptr(self.neighbors, u32p),
+                       len(self.points))
+
+    @classmethod
+    def from_scene(cls, m):
+        return cls(m.points, m.sh, m.sh_degree, m.offsets, m.neighbors, m.radii)
+
+    @property
+    def n(self):
+        return len(self.points)
+
+
+def camera_struct(cam) -> Camera:
+    c = Camera()
+    c.position[:] = [float(v) for v in cam.position]
+    c.depth = float(cam.depth)
+    c.orientation[:] = [float(v) for v in cam.orientation]
+    c.fov[:] = [float(v) for v in cam.fov]
+    c.principal[:] = [float(v) for v in cam.principal]
+    return c
+
+
+def settings(max_steps=1024, weight_threshold=1e-3, start_point=0, depth=1e4, eval_mode=EVAL_SH,
+             constant_rgb=(1.0, 1.0, 1.0)) -> Settings:
+    s = Settings()
+    s.weight_threshold = weight_threshold
+    s.max_steps = max_steps
+    s.start_point = start_point
+    s.depth = depth
+    s.eval_mode = eval_mode
+    s.constant_rgb[:] = list(constant_rgb)
+    return s
+
+
+def expf(x: float) -> float:
+    return float(lib().bvo_expf(float(x)))
+
+
+def tan_half(fov: float) -> float:
+    return float(lib().bvo_tan_half(float(fov)))
+
+
+def camera_ray(cam, width, height, x, y):
+    o = np.zeros(3, dtype=np.float32)
+    d = np.zeros(3, dtype=np.float32)
+    cs = camera_struct(cam)
+    lib().bvo_camera_ray(C.byref(cs), width, height, x, y, _ptr(o, f32p), _ptr(d, f32p))
+    return o, d
+
+
+def eval_rgb_sh(model: OracleModel, point: int, direction):
+    d = np.ascontiguousarray(direction, dtype=np.float32)
+    out = np.zeros(3, dtype=np.float32)
+    unc = np.zeros(3, dtype=np.float32)
+    lib().bvo_eval_rgb_sh(C.byref(model.c), point, _ptr(d, f32p), _ptr(out, f32p),
+                          _ptr(unc, f32p))
+    return out, unc
+
+
+def trace_one_ray(model: OracleModel, origin, direction, s: Settings) -> TraceResult:
+    o = np.ascontiguousarray(origin, dtype=np.float32)
+    d = np.ascontiguousarray(direction, dtype=np.float32)
+    return lib().bvo_trace_one_ray(C.byref(model.c), _ptr(o, f32p), _ptr(d, f32p), C.byref(s))
+
+
+def trace_powerfoam_splats(model: OracleModel, origin, direction, s: Settings) -> TraceResult:
+    o = np.ascontiguousarray(origin, dtype=np.float32)
+    d = np.ascontiguousarray(direction, dtype=np.float32)
+    return lib().bvo_trace_powerfoam_splats(C.byref(model.c), _ptr(o, f32p), _ptr(d, f32p),
+                                            C.byref(s))
+
+
+def _entries(fn, model, origin, direction, s, capacity):
+    o = np.ascontiguousarray(origin, dtype=np.float32)
+    d = np.ascontiguousarray(direction, dtype=np.float32)
+    buf = (PathEntry * capacity)()
+    n = fn(C.byref(model.c), _ptr(o, f32p), _ptr(d, f32p), C.byref(s), buf, capacity)
+    return [buf[i] for i in range(min(n, capacity))]
+
+
+def record_path_jacobians(model, origin, direction, s, capacity=4096):
+    return _entries(lib().bvo_record_path_jacobians, model, origin, direction, s, capacity)
+
+
+def record_powerfoam_splats(model, origin, direction, s, capacity=4096):
+    return _entries(lib().bvo_record_powerfoam_splats, model, origin, direction, s, capacity)
+
+
+def support_interval(bounded, origin, direction, center, radius, t0, t1):
+    o = np.ascontiguousarray(origin, dtype=np.float32)
+    d = np.ascontiguousarray(direction, dtype=np.float32)
+    c = np.ascontiguousarray(center, dtype=np.float32)
+    out = np.zeros(2, dtype=np.float32)
+    ok = lib().bvo_support_interval(int(bounded), _ptr(o, f32p), _ptr(d, f32p), _ptr(c, f32p),
+                                    float(radius), float(t0), float(t1), _ptr(out, f32p))
+    return (float(out[0]), float(out[1])) if ok else None
+
+
+def containing_cell_f64(model: OracleModel, position) -> int:
+    p = np.ascontiguousarray(position, dtype=np.float32)
+    return int(lib().bvo_containing_cell_f64(C.byref(model.c), _ptr(p, f32p)))
+
+
+def containing_cell_f32(model: OracleModel, position) -> int:
+    p = np.ascontiguousarray(position, dtype=np.float32)
+    return int(lib().bvo_containing_cell_f32(C.byref(model.c), _ptr(p, f32p)))
+
+
+def render_walk(model: OracleModel, cam, width, height, max_steps=1024, weight_threshold=1e-3,
+                start_point=None, cell_capacity=0, threads=0):
+    """Image of the walk forward; returns rgba [H, W, 4], steps [H, W] and
+    (if cell_capacity > 0) the visited cells [H, W, cap] and counts [H, W]."""
+    if start_point is None:
+        start_point = containing_cell_f64(model, cam.position)
+    rgba = np.zeros((height, width, 4), dtype=np.float32)
+    steps = np.zeros((height, width), dtype=np.uint32)
+    cells = counts = None
+    if cell_capacity > 0:
+        cells = np.zeros((height, width, cell_capacity), dtype=np.uint32)
+        counts = np.zeros((height, width), dtype=np.uint32)
+    cs = camera_struct(cam)
+    lib().bvo_render_walk(C.byref(model.c), C.byref(cs), width, height, max_steps,
+                          weight_threshold, start_point, _ptr(rgba, f32p), _ptr(steps, u32p),
+                          _ptr(cells, u32p), cell_capacity, _ptr(counts, u32p), threads)
+    return rgba, steps, cells, counts
+
+
+def record_image(model: OracleModel, cams: Sequence, width, height, max_steps, starts=None,
+                 threads=0):
+    """Path-recorder rows for every pixel of every camera (PathRecordBuffers
+    layout [P, max_steps]); unwritten slots hold the fill values -1 / NaN."""
+    if starts is None:
+        starts = [containing_cell_f64(model, c.position) for c in cams]
+    P = len(cams) * width * height
+    L = max_steps
+    out = dict(previous_cells=np.full((P, L), 0xFFFFFFFF, np.uint32),
+               cells=np.full((P, L), 0xFFFFFFFF, np.uint32),
+               next_cells=np.full((P, L), 0xFFFFFFFF, np.uint32),
+               dts=np.full((P, L), np.nan, np.float32),
+               dt_grad_previous=np.full((P, L, 4), np.nan, np.float32),
+               dt_grad_current=np.full((P, L, 4), np.nan, np.float32),
+               dt_grad_next=np.full((P, L, 4), np.nan, np.float32),
+               path_status=np.zeros(P, np.uint32))
+    cam_arr = (Camera * len(cams))(*[camera_struct(c) for c in cams])
+    st = np.ascontiguousarray(starts, dtype=np.uint32)
+    lib().bvo_record_image(C.byref(model.c), cam_arr, len(cams), width, height, L, _ptr(st, u32p),
+                           _ptr(out["previous_cells"], u32p), _ptr(out["cells"], u32p),
+                           _ptr(out["next_cells"], u32p), _ptr(out["dts"], f32p),
+                           _ptr(out["dt_grad_previous"], f32p), _ptr(out["dt_grad_current"], f32p),
+                           _ptr(out["dt_grad_next"], f32p), _ptr(out["path_status"], u32p),
+                           threads)
+    return out
+
+
+def render_splats(model: OracleModel, cam, width, height, max_steps=1024, weight_threshold=1e-3,
+                  threads=0):
+    rgba = np.zeros((height, width, 4), dtype=np.float32)
+    steps = np.zeros((height, width), dtype=np.uint32)
+    cs = camera_struct(cam)
+    lib().bvo_render_splats(C.byref(model.c), C.byref(cs), width, height, max_steps,
+                            weight_threshold, _ptr(rgba, f32p), _ptr(steps, u32p), threads)
+    return rgba, steps
+
+
+def forward_backward(model: OracleModel, cams: Sequence, width, height, max_steps=1024,
+                     weight_threshold=0.0, max_dt=50.0, target=None, loss_kind=0,
+                     override=None, want_grads=True, threads=0):
+    """FP64 training-contract oracle.  Returns dict(loss, rgb, d_density,
+    d_sh, d_pos, d_radius)."""
+    n = model.n
+    K3 = model.sh.size // max(n, 1)
+    cam_arr = (Camera * len(cams))(*[camera_struct(c) for c in cams])
+    rgb = np.zeros((len(cams), height, width, 3), dtype=np.float64)
+    tgt = None if target is None else np.ascontiguousarray(target, dtype=np.float32)
+    dd = dsh = dpos = drad = None
+    if want_grads:
+        dd = np.zeros(n, dtype=np.float64)
+        dsh = np.zeros(n * K3, dtype=np.float64)
+        dpos = np.zeros(n * 3, dtype=np.float64)
+        drad = np.zeros(n, dtype=np.float64) if model.radii is not None else None
+    ov = None
+    keep = []
+    if override is not None:
+        pts, sh, rad = override
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1)
+        sh = np.ascontiguousarray(sh, dtype=np.float64).reshape(-1)
+        rad = None if rad is None else np.ascontiguousarray(rad, dtype=np.float64)
+        keep = [pts, sh, rad]
+        ov = ParamsF64(_ptr(pts, f64p), _ptr(sh, f64p), _ptr(rad, f64p))
+    loss = lib().bvo_forward_backward(
+        C.byref(model.c), cam_arr, len(cams), width, height, max_steps, weight_threshold,
+        max_dt, _ptr(tgt, f32p), loss_kind, C.byref(ov) if ov is not None else None,
+        _ptr(rgb, f64p), _ptr(dd, f64p), _ptr(dsh, f64p), _ptr(dpos, f64p), _ptr(drad, f64p),
+        threads)
+    del keep
+    return dict(loss=loss, rgb=rgb, d_density=dd, d_sh=dsh,
+                d_pos=None if dpos is None else dpos.reshape(n, 3), d_radius=drad)
