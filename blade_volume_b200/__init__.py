@@ -24,7 +24,8 @@ import numpy as np
 from .scenes import Camera, PointCloudModel  # noqa: F401
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libbv_b200.so")
+# BV_B200_LIBRARY selects another build of the same library (tuning sweeps).
+LIB_PATH = os.environ.get("BV_B200_LIBRARY", os.path.join(HERE, "libbv_b200.so"))
 
 BV_OK = 0
 STATUS_NAMES = {0: "BV_OK", 1: "BV_ERR_INVALID_ARGUMENT", 2: "BV_ERR_INVALID_MODEL",
@@ -91,7 +92,8 @@ class Grads(C.Structure):
 
 
 class LaunchStats(C.Structure):
-    _fields_ = [("kernel_ms", C.c_float), ("start_cell_ms", C.c_float), ("rays", C.c_uint64),
+    _fields_ = [("kernel_ms", C.c_float), ("start_cell_ms", C.c_float),
+                ("forward_ms", C.c_float), ("backward_ms", C.c_float), ("rays", C.c_uint64),
                 ("steps", C.c_uint64), ("faces", C.c_uint64), ("launches", C.c_uint32),
                 ("reserved", C.c_uint32)]
 

@@ -51,27 +51,33 @@ def stale() -> bool:
     return any(os.path.getmtime(p) > t for p in sources() + headers() + [__file__])
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
-    if not force and not stale():
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False,
+          out: str = LIB, defines=()) -> str:
+    """Compile every csrc/*.cu for sm_100a and link ``out``.  ``defines``
+    (e.g. ``["BV_FACE_UNROLL=2"]``) override the kernels' tuning knobs."""
+    if out == LIB and not defines and not force and not stale():
         return LIB
-    os.makedirs(BUILD_DIR, exist_ok=True)
+    bdir = BUILD_DIR if not defines else BUILD_DIR + "_" + "_".join(
+        d.replace("=", "") for d in defines)
+    os.makedirs(bdir, exist_ok=True)
     objs = []
     extra = ["-Xptxas", "-v"] if ptxas_info else []
+    extra += ["-D" + d for d in defines]
     for src in sources():
-        obj = os.path.join(BUILD_DIR, os.path.basename(src) + ".o")
+        obj = os.path.join(bdir, os.path.basename(src) + ".o")
         cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-dc" if False else "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.check_call(cmd)
         objs.append(obj)
-    tmp = LIB + ".tmp"
+    tmp = out + ".tmp"
     cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs, "-lcudart_static",
            "-lrt", "-ldl", "-lpthread"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.check_call(cmd)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, out)
+    return out
 
 
 if __name__ == "__main__":

@@ -6,6 +6,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -74,7 +75,7 @@ struct bv_tracer {
     float *density = nullptr;
     void *sh = nullptr;
     uint32_t *offsets = nullptr;
-    uint32_t *neighbors = nullptr;
+    FaceEntry *faces = nullptr;
     // scratch
     uint32_t *start_cells = nullptr;   // [kMaxViewsPerLaunch]
     uint32_t *work_counter = nullptr;  // [4]
@@ -83,13 +84,18 @@ struct bv_tracer {
     uint32_t *partial_index = nullptr;
     uint32_t *start_counters = nullptr;
     int start_blocks = 1;
+    RayState *ray_state = nullptr;     // per-ray training state
+    size_t ray_state_capacity = 0;
+    float4 *site_grads = nullptr;      // [N] site gradient accumulator (kept zero)
     int grid_forward = 0;
-    int grid_train = 0;
+    int grid_train_fwd = 0;
+    int grid_train_bwd = 0;
     // instrumentation
     bool stats_enabled = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaStream_t last_stream = nullptr;
     uint32_t last_launches = 0;
+    bool last_train = false;
     bool last_has_stats = false;
     uint32_t last_start_point = 0;
     bool start_point_pending = false;
@@ -100,7 +106,7 @@ struct bv_tracer {
         m.density = density;
         m.sh = sh;
         m.offsets = offsets;
-        m.neighbors = neighbors;
+        m.faces = faces;
         m.n = n;
         m.sh_degree = sh_degree;
         m.sh_stride = sh_stride;
@@ -118,7 +124,9 @@ void free_tracer(bv_tracer *t) {
     cudaFree(t->density);
     cudaFree(t->sh);
     cudaFree(t->offsets);
-    cudaFree(t->neighbors);
+    cudaFree(t->faces);
+    cudaFree(t->ray_state);
+    cudaFree(t->site_grads);
     cudaFree(t->start_cells);
     cudaFree(t->work_counter);
     cudaFree(t->stats);
@@ -184,6 +192,7 @@ bv_status launch_starts(bv_tracer *t, const bv_camera *cams, uint32_t count, cud
 bv_status begin_timing(bv_tracer *t, cudaStream_t s) {
     t->last_stream = s;
     t->last_launches = 0;
+    t->last_train = false;
     t->last_has_stats = t->stats_enabled;
     if (t->stats_enabled) {
         BV_CUDA(cudaMemsetAsync(t->stats, 0, 4 * sizeof(unsigned long long), s), "stats reset");
@@ -211,13 +220,13 @@ bv_status bv_model_validate(const bv_model_desc *md, char *err, size_t err_len) 
         }
         return BV_ERR_INVALID_MODEL;
     };
-    if (!md) return bad("model descriptor is null");
+    if (!md) return bad("%s", "model descriptor is null");
     const uint32_t n = md->num_points;
-    if (n == 0) return bad("model has no points");
-    if (!md->points || !md->sh_coefficients) return bad("points and SH coefficients are required");
+    if (n == 0) return bad("%s", "model has no points");
+    if (!md->points || !md->sh_coefficients) return bad("%s", "points and SH coefficients are required");
     if (md->sh_degree > 3) return bad("SH degree %u exceeds supported degree 3", md->sh_degree);
     if (!md->adjacency_offsets || (!md->adjacency_neighbors && md->adjacency_offsets[n] != 0))
-        return bad("the cell walk requires CSR adjacency");
+        return bad("%s", "the cell walk requires CSR adjacency");
     for (uint32_t i = 0; i < n; ++i) {
         const float *p = md->points + 4 * (size_t)i;
         if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2]) ||
@@ -226,11 +235,11 @@ bv_status bv_model_validate(const bv_model_desc *md, char *err, size_t err_len) 
     }
     const size_t nsh = (size_t)n * 3 * sh_components(md->sh_degree);
     for (size_t i = 0; i < nsh; ++i)
-        if (!std::isfinite(md->sh_coefficients[i])) return bad("SH coefficients must be finite");
+        if (!std::isfinite(md->sh_coefficients[i])) return bad("%s", "SH coefficients must be finite");
     if (md->radii) {
         for (uint32_t i = 0; i < n; ++i)
             if (!std::isfinite(md->radii[i]) || md->radii[i] < 0.0f)
-                return bad("radii must be finite and non-negative");
+                return bad("%s", "radii must be finite and non-negative");
     }
     // validate_csr_result (adjacency.rs:724-790)
     const uint32_t *off = md->adjacency_offsets;
@@ -321,12 +330,23 @@ bv_status bv_radfoam_tracer_new(const bv_model_desc *md, const bv_trace_settings
     BV_TRY(cudaMalloc(&t->geom, sizeof(float4) * n), "cudaMalloc geom");
     BV_TRY(cudaMalloc(&t->density, sizeof(float) * n), "cudaMalloc density");
     BV_TRY(cudaMalloc(&t->offsets, sizeof(uint32_t) * (n + 1)), "cudaMalloc offsets");
-    BV_TRY(cudaMalloc(&t->neighbors, sizeof(uint32_t) * (t->m_edges ? t->m_edges : 1)), "cudaMalloc neighbors");
+    BV_TRY(cudaMalloc(&t->faces, sizeof(FaceEntry) * (t->m_edges ? t->m_edges : 1)), "cudaMalloc faces");
     BV_TRY(cudaMemcpy(t->geom, geom.data(), sizeof(float4) * n, cudaMemcpyHostToDevice), "upload geom");
     BV_TRY(cudaMemcpy(t->density, dens.data(), sizeof(float) * n, cudaMemcpyHostToDevice), "upload density");
     BV_TRY(cudaMemcpy(t->offsets, md->adjacency_offsets, sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice), "upload offsets");
-    if (t->m_edges)
-        BV_TRY(cudaMemcpy(t->neighbors, md->adjacency_neighbors, sizeof(uint32_t) * t->m_edges, cudaMemcpyHostToDevice), "upload neighbors");
+    if (t->m_edges) {
+        // face table: per CSR entry the neighbour's site and its own CSR range
+        // and density, in CSR order
+        std::vector<FaceEntry> faces(t->m_edges);
+        for (uint32_t k = 0; k < t->m_edges; ++k) {
+            const uint32_t j = md->adjacency_neighbors[k];
+            uint32_t dbits;
+            std::memcpy(&dbits, &dens[j], 4);
+            faces[k].site = geom[j];
+            faces[k].link = make_uint4(j, md->adjacency_offsets[j], md->adjacency_offsets[j + 1], dbits);
+        }
+        BV_TRY(cudaMemcpy(t->faces, faces.data(), sizeof(FaceEntry) * t->m_edges, cudaMemcpyHostToDevice), "upload faces");
+    }
     if (t->bf16) {
         std::vector<uint16_t> row((size_t)n * t->sh_stride, 0);
         for (uint32_t i = 0; i < n; ++i)
@@ -351,9 +371,12 @@ bv_status bv_radfoam_tracer_new(const bv_model_desc *md, const bv_trace_settings
     BV_TRY(cudaMalloc(&t->start_counters, sizeof(uint32_t) * kMaxStartQueries), "cudaMalloc counters");
     BV_TRY(cudaMemset(t->start_counters, 0, sizeof(uint32_t) * kMaxStartQueries), "memset counters");
     BV_TRY(cudaMemset(t->start_cells, 0, sizeof(uint32_t) * kMaxViewsPerLaunch), "memset start cells");
+    BV_TRY(cudaMalloc(&t->site_grads, sizeof(float4) * n), "cudaMalloc site grads");
+    BV_TRY(cudaMemset(t->site_grads, 0, sizeof(float4) * n), "memset site grads");
     for (auto &ev : t->ev) BV_TRY(cudaEventCreate(&ev), "cudaEventCreate");
     t->grid_forward = walk_grid_size(device, 0);
-    t->grid_train = walk_grid_size(device, 1);
+    t->grid_train_fwd = walk_grid_size(device, 1);
+    t->grid_train_bwd = walk_grid_size(device, 2);
     BV_TRY(cudaDeviceSynchronize(), "upload");
 #undef BV_TRY
     *out = t;
@@ -531,6 +554,8 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
     if (grads->d_radii_dev && !t->bounded)
         return fail(BV_ERR_INVALID_ARGUMENT, "radius gradients need a PowerFoam model");
     const uint32_t nsh = 3 * sh_components(t->sh_degree);
+    if ((size_t)std::min<uint32_t>(n_cams, kMaxViewsPerLaunch) * width * height >= (1ull << 31))
+        return fail(BV_ERR_INVALID_ARGUMENT, "batch too large");
     if ((nsh % 4) == 0 && (reinterpret_cast<uintptr_t>(grads->d_sh_dev) & 15u) != 0)
         return fail(BV_ERR_INVALID_ARGUMENT, "d_sh table must be 16-byte aligned");
     for (uint32_t i = 0; i < n_cams; ++i) {
@@ -538,6 +563,15 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         if (s != BV_OK) return s;
     }
     cudaStream_t s = (cudaStream_t)stream;
+    // per-ray state scratch for the largest chunk of this call
+    const size_t chunk_rays = (size_t)std::min<uint32_t>(n_cams, kMaxViewsPerLaunch) * width * height;
+    if (chunk_rays > t->ray_state_capacity) {
+        cudaFree(t->ray_state);
+        t->ray_state = nullptr;
+        t->ray_state_capacity = 0;
+        BV_CUDA(cudaMalloc(&t->ray_state, sizeof(RayState) * chunk_rays), "cudaMalloc ray state");
+        t->ray_state_capacity = chunk_rays;
+    }
     bv_status st = begin_timing(t, s);
     if (st != BV_OK) return st;
     BV_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), s), "loss reset");
@@ -567,20 +601,29 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         p.work_counter = t->work_counter;
         p.target = target + 3 * off;
         p.rgb_out = rgb_out ? rgb_out + 3 * off : nullptr;
+        p.ray_state = t->ray_state;
         p.d_density = grads->d_density_dev;
         p.d_sh = grads->d_sh_dev;
-        p.d_pos = grads->d_positions_dev;
-        p.d_radius = grads->d_radii_dev;
+        p.d_site = (grads->d_positions_dev || grads->d_radii_dev) ? t->site_grads : nullptr;
         p.loss = loss;
         p.stats = t->stats_enabled ? t->stats : nullptr;
-        BV_CUDA(cudaMemsetAsync(t->work_counter, 0, sizeof(uint32_t), s), "counter reset");
-        const int blocks_needed = (int)((work + 255) / 256);
-        const int grid = std::min(t->grid_train, std::max(blocks_needed, 1));
-        BV_CUDA(launch_forward_backward(p, grid, s), "forward-backward launch");
-        t->last_launches += 2;
+        BV_CUDA(cudaMemsetAsync(t->work_counter, 0, 2 * sizeof(uint32_t), s), "counter reset");
+        const int blocks_needed = std::max((int)((work + 255) / 256), 1);
+        BV_CUDA(launch_train_forward(p, std::min(t->grid_train_fwd, blocks_needed), s),
+                "training forward launch");
+        if (t->stats_enabled && c0 == 0) BV_CUDA(cudaEventRecord(t->ev[3], s), "event");
+        BV_CUDA(launch_train_backward(p, std::min(t->grid_train_bwd, blocks_needed), s),
+                "training backward launch");
+        t->last_launches += 3;
+    }
+    if (grads->d_positions_dev || grads->d_radii_dev) {
+        BV_CUDA(launch_fold_site_grads(t->site_grads, t->n, grads->d_positions_dev,
+                                       grads->d_radii_dev, s), "site gradient fold");
+        t->last_launches += 1;
     }
     if (t->stats_enabled) BV_CUDA(cudaEventRecord(t->ev[2], s), "event");
     t->start_point_pending = true;
+    t->last_train = true;
     return BV_OK;
 }
 
@@ -601,6 +644,12 @@ bv_status bv_radfoam_tracer_last_stats(bv_tracer *t, bv_launch_stats *out) {
     BV_CUDA(cudaEventElapsedTime(&b, t->ev[1], t->ev[2]), "elapsed");
     out->start_cell_ms = a;
     out->kernel_ms = b;
+    if (t->last_train) {
+        float f = 0.f;
+        BV_CUDA(cudaEventElapsedTime(&f, t->ev[1], t->ev[3]), "elapsed");
+        out->forward_ms = f;
+        out->backward_ms = b - f;
+    }
     unsigned long long h[4] = {0, 0, 0, 0};
     BV_CUDA(cudaMemcpy(h, t->stats, sizeof(h), cudaMemcpyDeviceToHost), "stats read");
     out->rays = h[0];

@@ -29,15 +29,24 @@ struct ViewDesc {  // 80 bytes
     uint64_t pad;
 };
 
-// SoA device copy of a model.  geom packs the per-neighbour hot data
-// (position and power radius) into one 16-byte load; appearance lives in
-// separate tables that are read once per step.
+// One CSR entry (face) of the walk, 32 bytes: the neighbour's site record
+// and everything the walk needs once it steps into that neighbour, so that a
+// walk step costs one dependent round trip to memory (the current cell's
+// face entries) instead of three (offsets -> neighbour index -> site).
+struct __align__(16) FaceEntry {
+    float4 site;  // neighbour j: x, y, z, power radius (0 for plain RadFoam)
+    uint4 link;   // j, offsets[j], offsets[j+1], density[j] (float bits)
+};
+
+// SoA device copy of a model.  Appearance (SH rows) lives in its own table
+// read once per step; geometry the walk reads per face lives in the face
+// table; geom/density/offsets serve the start cell and the Jacobians.
 struct DeviceModel {
     const float4 *geom;        // [N] x, y, z, radius (0 for plain RadFoam)
     const float *density;      // [N]
     const void *sh;            // [N][sh_stride] float or bf16
     const uint32_t *offsets;   // [N+1]
-    const uint32_t *neighbors; // [M]
+    const FaceEntry *faces;    // [M] CSR order
     uint32_t n;
     uint32_t sh_degree;
     uint32_t sh_stride;        // elements per SH row (>= 3K, padded to 16 bytes)
@@ -70,6 +79,15 @@ struct RecordParams {
     ViewDesc views[kMaxViewsPerLaunch];
 };
 
+// Per-ray state handed from the training forward kernel to the replay
+// kernel: the compensated colour (hi, lo) and dL/dC.  48 bytes per ray; no
+// per-sample state is stored.
+struct RayState {
+    float4 c_hi;  // colour hi, dL/dC.r
+    float4 c_lo;  // colour lo, dL/dC.g
+    float4 g;     // dL/dC.b, unused x3
+};
+
 struct TrainParams {
     DeviceModel m;
     uint32_t max_steps;
@@ -80,13 +98,13 @@ struct TrainParams {
     uint32_t n_views;
     uint32_t total_work;
     const uint32_t *start_cells;
-    uint32_t *work_counter;
+    uint32_t *work_counter;       // [2]: forward, replay dispensers
     const float *target;          // [views][H][W][3]
     float *rgb_out;               // [views][H][W][3] or null
+    RayState *ray_state;          // [views][H][W] scratch
     float *d_density;
     float *d_sh;
-    float *d_pos;
-    float *d_radius;
+    float4 *d_site;               // [N] x, y, z, radius gradients (scratch) or null
     float *loss;                  // device scalar accumulator
     unsigned long long *stats;
     ViewDesc views[kMaxViewsPerLaunch];
@@ -101,7 +119,11 @@ struct StartCellQueries {
 // Launchers (bv_walk.cu / bv_start_cell.cu).
 cudaError_t launch_walk_forward(const WalkParams &p, int grid, cudaStream_t s);
 cudaError_t launch_record_paths(const RecordParams &p, int grid, cudaStream_t s);
-cudaError_t launch_forward_backward(const TrainParams &p, int grid, cudaStream_t s);
+cudaError_t launch_train_forward(const TrainParams &p, int grid, cudaStream_t s);
+cudaError_t launch_train_backward(const TrainParams &p, int grid, cudaStream_t s);
+cudaError_t launch_fold_site_grads(float4 *site, uint32_t n, float *d_pos, float *d_radius,
+                                   cudaStream_t s);
+// kind: 0 render, 1 training forward, 2 replay backward
 int walk_grid_size(int device, int kind);
 
 // FP64 power-nearest search: out[v] = argmin_i |q_v - p_i|^2 - r_i^2, ties to

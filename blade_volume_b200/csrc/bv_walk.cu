@@ -23,9 +23,28 @@ namespace bv {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr uint32_t kNone = 0xffffffffu;
 constexpr int kWalkBlock = 256;
-constexpr int kRefillMin = 8;
+
+// Tuning knobs (measured on B200; see the profiles): face entries in flight
+// per lane, idle lanes that trigger a refill, and resident blocks per SM
+// requested from the register allocator for each kernel.
+#ifndef BV_FACE_UNROLL
+#define BV_FACE_UNROLL 4
+#endif
+#ifndef BV_REFILL_MIN
+#define BV_REFILL_MIN 32
+#endif
+#ifndef BV_MINB_RENDER
+#define BV_MINB_RENDER 4
+#endif
+#ifndef BV_MINB_TRAIN_FWD
+#define BV_MINB_TRAIN_FWD 4
+#endif
+#ifndef BV_MINB_TRAIN_BWD
+#define BV_MINB_TRAIN_BWD 3
+#endif
+constexpr int kFaceUnroll = BV_FACE_UNROLL;
+constexpr int kRefillMin = BV_REFILL_MIN;
 
 // ---------------------------------------------------------------------------
 // exp(x): Cody & Waite reduction x = k ln2 + r (ln2 split into a high part
@@ -250,57 +269,90 @@ __device__ __forceinline__ size_t pixel_index(const Params &P, uint32_t view, ui
 }
 
 // ---------------------------------------------------------------------------
+// The walk's current cell: its site, CSR range and density.
+// ---------------------------------------------------------------------------
+struct Cell {
+    uint32_t id, begin, end;
+    float x, y, z, r, density;
+};
+
+__device__ __forceinline__ Cell load_cell(const DeviceModel &m, uint32_t id) {
+    const float4 g = __ldg(m.geom + id);
+    Cell c;
+    c.id = id;
+    c.begin = __ldg(m.offsets + id);
+    c.end = __ldg(m.offsets + id + 1);
+    c.x = g.x;
+    c.y = g.y;
+    c.z = g.z;
+    c.r = g.w;
+    c.density = __ldg(m.density + id);
+    return c;
+}
+
+__device__ __forceinline__ Cell cell_from_face(const FaceEntry &f) {
+    Cell c;
+    c.id = f.link.x;
+    c.begin = f.link.y;
+    c.end = f.link.z;
+    c.x = f.site.x;
+    c.y = f.site.y;
+    c.z = f.site.z;
+    c.r = f.site.w;
+    c.density = __uint_as_float(f.link.w);
+    return c;
+}
+
+// ---------------------------------------------------------------------------
 // find_exit_face (trace.rs:170-205): the first face in CSR order with the
-// smallest t in (t0, best).  Neighbour indices and site records are fetched
-// four at a time so that four independent gathers are in flight.
+// smallest t in (t0, best).  The face entries of the current cell are read
+// four at a time so that four independent loads are in flight; the winner's
+// entry already carries the next cell's site, CSR range and density.
 // ---------------------------------------------------------------------------
 template <bool BOUNDED>
-__device__ __forceinline__ void find_exit(const DeviceModel &m, uint32_t cur, float cpx, float cpy,
-                                          float cpz, float cr, const Ray &ray, float t0,
-                                          float depth, float &best, uint32_t &best_j,
-                                          float4 &best_g, uint32_t &faces) {
-    const uint32_t begin = __ldg(m.offsets + cur);
-    const uint32_t end = __ldg(m.offsets + cur + 1);
+__device__ __forceinline__ bool find_exit(const DeviceModel &m, const Cell &c, const Ray &ray,
+                                          float t0, float depth, float &best, FaceEntry &win) {
     best = depth;
-    best_j = kNone;
-    best_g = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float ri2 = cr * cr;
-    for (uint32_t k = begin; k < end; k += 4) {
-        uint32_t j[4];
-        float4 g[4];
+    uint32_t best_k = 0xffffffffu;
+    float4 best_site = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float ri2 = c.r * c.r;
+    for (uint32_t k = c.begin; k < c.end; k += kFaceUnroll) {
+        float4 site[kFaceUnroll];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) j[u] = (k + u < end) ? __ldg(m.neighbors + k + u) : cur;
+        for (int u = 0; u < kFaceUnroll; ++u) site[u] = __ldg(&m.faces[min(k + u, c.end - 1)].site);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) g[u] = __ldg(m.geom + j[u]);
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            if (k + u < end) {
-                const float offx = g[u].x - cpx, offy = g[u].y - cpy, offz = g[u].z - cpz;
+        for (int u = 0; u < kFaceUnroll; ++u) {
+            if (k + u < c.end) {
+                const float offx = site[u].x - c.x, offy = site[u].y - c.y, offz = site[u].z - c.z;
                 float shift;
                 if (BOUNDED) {
-                    const float rj = g[u].w;
+                    const float rj = site[u].w;
                     const float dsq = fmaxf(dot3(offx, offy, offz, offx, offy, offz), 1e-20f);
                     shift = 0.5f + 0.5f * (ri2 - rj * rj) / dsq;
                 } else {
                     shift = 0.5f;
                 }
-                const float fox = cpx + shift * offx;
-                const float foy = cpy + shift * offy;
-                const float foz = cpz + shift * offz;
+                const float fox = c.x + shift * offx;
+                const float foy = c.y + shift * offy;
+                const float foz = c.z + shift * offz;
                 const float dp = dot3(offx, offy, offz, ray.dx, ray.dy, ray.dz);
                 if (dp > 0.0f) {
                     const float t =
                         dot3(fox - ray.ox, foy - ray.oy, foz - ray.oz, offx, offy, offz) / dp;
                     if (isfinite(t) && t > t0 && t < best) {
                         best = t;
-                        best_j = j[u];
-                        best_g = g[u];
+                        best_k = k + u;
+                        best_site = site[u];
                     }
                 }
             }
         }
     }
-    faces = end - begin;
+    if (best_k == 0xffffffffu) return false;
+    // The winner's link shares the 32-byte sector of the site just read.
+    win.site = best_site;
+    win.link = __ldg(&m.faces[best_k].link);
+    return true;
 }
 
 // support_interval (trace.rs:209-238).
@@ -373,16 +425,16 @@ __device__ __forceinline__ bool refill(uint32_t *counter, uint32_t total, bool a
 // forward render: trace_one_ray per pixel
 // ---------------------------------------------------------------------------
 template <int DEG, bool BOUNDED, bool BF16>
-__global__ void __launch_bounds__(kWalkBlock)
+__global__ void __launch_bounds__(kWalkBlock, BV_MINB_RENDER)
 walk_forward_kernel(const __grid_constant__ WalkParams P) {
     const DeviceModel &m = P.m;
     bool drained = false, active = false;
     Ray ray;
+    Cell c;
     float t0 = 0.f, T = 1.f, ar = 0.f, ag = 0.f, ab = 0.f, depth = 0.f;
-    float cpx = 0.f, cpy = 0.f, cpz = 0.f, cr = 0.f;
-    uint32_t cur = 0, steps = 0, visited = 0;
+    uint32_t steps = 0, visited = 0;
     size_t out_index = 0;
-    unsigned long long n_rays = 0, n_steps = 0, n_faces = 0;
+    uint32_t n_rays = 0, n_steps = 0, n_faces = 0;
     for (;;) {
         uint32_t w;
         if (refill(P.work_counter, P.total_work, active, drained, w)) {
@@ -390,14 +442,8 @@ walk_forward_kernel(const __grid_constant__ WalkParams P) {
             if (work_item(P, w, view, x, y)) {
                 const ViewDesc &vd = P.views[view];
                 out_index = pixel_index(P, view, x, y);
-                const uint32_t start = P.start_cells[view];
                 const bool ok = make_ray(vd, x, y, ray);
-                cur = start;
-                const float4 g = __ldg(m.geom + cur);
-                cpx = g.x;
-                cpy = g.y;
-                cpz = g.z;
-                cr = g.w;
+                c = load_cell(m, P.start_cells[view]);
                 t0 = 0.f;
                 T = 1.f;
                 ar = ag = ab = 0.f;
@@ -427,39 +473,34 @@ walk_forward_kernel(const __grid_constant__ WalkParams P) {
                 done = true;
             } else {
                 float best;
-                uint32_t nj, faces;
-                float4 ng;
-                find_exit<BOUNDED>(m, cur, cpx, cpy, cpz, cr, ray, t0, depth, best, nj, ng, faces);
+                FaceEntry win;
+                const bool has_exit = find_exit<BOUNDED>(m, c, ray, t0, depth, best, win);
                 n_steps += 1;
-                n_faces += faces;
+                n_faces += c.end - c.begin;
                 float ss, se;
-                if (support<BOUNDED>(ray, cpx, cpy, cpz, cr, t0, best, ss, se)) {
+                if (support<BOUNDED>(ray, c.x, c.y, c.z, c.r, t0, best, ss, se)) {
                     visited += 1;
-                    const float dens = __ldg(m.density + cur) * 1.0f;
+                    const float dens = c.density * 1.0f;
                     if (dens > 1e-6f) {
                         const float dt = se - ss;
                         const float alpha = 1.0f - bv_expf(-dens * dt);
                         const float wgt = T * alpha;
-                        float c[ShDims<DEG>::N];
-                        load_sh_row<DEG, BF16>(m, cur, c);
+                        float coef[ShDims<DEG>::N];
+                        load_sh_row<DEG, BF16>(m, c.id, coef);
                         float r, g, b;
-                        eval_sh<DEG>(c, ray.dx, ray.dy, ray.dz, r, g, b);
+                        eval_sh<DEG>(coef, ray.dx, ray.dy, ray.dz, r, g, b);
                         ar += wgt * fmaxf(r, 0.0f);
                         ag += wgt * fmaxf(g, 0.0f);
                         ab += wgt * fmaxf(b, 0.0f);
                         T *= 1.0f - alpha;
                     }
                 }
-                if (nj == kNone) {
+                if (!has_exit) {
                     t0 = best;
                     done = true;
                 } else {
                     t0 = fmaxf(t0, best);
-                    cur = nj;
-                    cpx = ng.x;
-                    cpy = ng.y;
-                    cpz = ng.z;
-                    cr = ng.w;
+                    c = cell_from_face(win);
                 }
             }
         }
@@ -481,9 +522,9 @@ walk_forward_kernel(const __grid_constant__ WalkParams P) {
             n_faces += __shfl_xor_sync(kFull, n_faces, s);
         }
         if ((threadIdx.x & 31u) == 0) {
-            atomicAdd(P.stats + 0, n_rays);
-            atomicAdd(P.stats + 1, n_steps);
-            atomicAdd(P.stats + 2, n_faces);
+            atomicAdd(P.stats + 0, (unsigned long long)n_rays);
+            atomicAdd(P.stats + 1, (unsigned long long)n_steps);
+            atomicAdd(P.stats + 2, (unsigned long long)n_faces);
         }
     }
 }
@@ -514,67 +555,78 @@ __device__ __forceinline__ float4 f4sub(float4 a, float4 b) {
     return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
 }
 
-// One recorded segment with its dt Jacobians (path_interval_jacobian,
-// trace.rs:1199-1325, without oriented surfaces).
-struct Segment {
+// The clipped interval of one recorded segment (path_interval_jacobian,
+// trace.rs:1199-1325 without oriented surfaces) and which boundary is a
+// sphere clip.
+struct Interval {
     float start, end;
-    float4 jp, jc, jn;  // d dt / d (x, y, z, r) of previous, current, next
+    bool start_sphere, end_sphere;
 };
 
 template <bool BOUNDED>
-__device__ __forceinline__ bool interval_jacobian(const Ray &ray, uint32_t prev, uint32_t cur,
-                                                  uint32_t next, float ppx, float ppy, float ppz,
-                                                  float pr, float cpx, float cpy, float cpz,
-                                                  float cr, float4 ng, float t0, float t1,
-                                                  bool want_jac, Segment &sg) {
-    float start = t0, end = t1;
-    bool start_sphere = false, end_sphere = false;
-    float4 nj = make_float4(0.f, 0.f, 0.f, 0.f), fj = nj;
-    float4 qprev = nj, qcur = nj;
+__device__ __forceinline__ bool record_interval(const Ray &ray, const Cell &c, float t0, float t1,
+                                                Interval &iv) {
+    iv.start = t0;
+    iv.end = t1;
+    iv.start_sphere = iv.end_sphere = false;
     if (BOUNDED) {
         float nt, ft, root, b;
-        if (!sphere_hit(ray, cpx, cpy, cpz, cr, nt, ft, root, b)) return false;
-        if (nt > start) {
-            start = nt;
-            start_sphere = true;
+        if (!sphere_hit(ray, c.x, c.y, c.z, c.r, nt, ft, root, b)) return false;
+        if (nt > iv.start) {
+            iv.start = nt;
+            iv.start_sphere = true;
         }
-        if (ft < end) {
-            end = ft;
-            end_sphere = true;
-        }
-        if (want_jac) {
-            const float ocx = ray.ox - cpx, ocy = ray.oy - cpy, ocz = ray.oz - cpz;
-            const float px = ocx - b * ray.dx, py = ocy - b * ray.dy, pz = ocz - b * ray.dz;
-            const float rx = px / root, ry = py / root, rz = pz / root;
-            const float rr = cr / root;
-            nj = make_float4(ray.dx - rx, ray.dy - ry, ray.dz - rz, -rr);
-            fj = make_float4(ray.dx + rx, ray.dy + ry, ray.dz + rz, rr);
+        if (ft < iv.end) {
+            iv.end = ft;
+            iv.end_sphere = true;
         }
     }
-    if (end <= start || !isfinite(start) || !isfinite(end)) return false;
-    sg.start = start;
-    sg.end = end;
-    if (!want_jac) return true;
-    if (start_sphere) {
+    return !(iv.end <= iv.start || !isfinite(iv.start) || !isfinite(iv.end));
+}
+
+// d dt / d (x, y, z, r) of the previous, current and next site for a
+// recorded segment; prev/next equal to the current cell mean a fixed
+// boundary (t = 0 or the far plane).
+struct Jacobians {
+    float4 jp, jc, jn;
+};
+
+__device__ __forceinline__ Jacobians interval_jacobians(const Ray &ray, const Interval &iv,
+                                                        uint32_t prev, float4 pp, const Cell &c,
+                                                        bool has_next, float4 np, float t0,
+                                                        float t1) {
+    Jacobians J;
+    float4 qprev = make_float4(0.f, 0.f, 0.f, 0.f), qcur = qprev;
+    float4 nj = qprev, fj = qprev;
+    if (iv.start_sphere || iv.end_sphere) {
+        float nt, ft, root, b;
+        sphere_hit(ray, c.x, c.y, c.z, c.r, nt, ft, root, b);
+        const float ocx = ray.ox - c.x, ocy = ray.oy - c.y, ocz = ray.oz - c.z;
+        const float px = ocx - b * ray.dx, py = ocy - b * ray.dy, pz = ocz - b * ray.dz;
+        const float rx = px / root, ry = py / root, rz = pz / root;
+        const float rr = c.r / root;
+        nj = make_float4(ray.dx - rx, ray.dy - ry, ray.dz - rz, -rr);
+        fj = make_float4(ray.dx + rx, ray.dy + ry, ray.dz + rz, rr);
+    }
+    if (iv.start_sphere) {
         qcur = nj;
-    } else if (prev != cur) {
-        face_jacobian(ray, cpx, cpy, cpz, cr, ppx, ppy, ppz, pr, t0, qcur, qprev);
+    } else if (prev != c.id) {
+        face_jacobian(ray, c.x, c.y, c.z, c.r, pp.x, pp.y, pp.z, pp.w, t0, qcur, qprev);
     }
-    float4 jp = make_float4(0.f, 0.f, 0.f, 0.f), jc = jp, jn = jp;
-    jc = f4sub(jc, qcur);
-    jp = f4sub(jp, qprev);
-    if (end_sphere) {
-        jc = f4add(jc, fj);
-    } else if (next != cur) {
+    J.jp = make_float4(0.f, 0.f, 0.f, 0.f);
+    J.jc = J.jp;
+    J.jn = J.jp;
+    J.jc = f4sub(J.jc, qcur);
+    J.jp = f4sub(J.jp, qprev);
+    if (iv.end_sphere) {
+        J.jc = f4add(J.jc, fj);
+    } else if (has_next) {
         float4 cj, aj;
-        face_jacobian(ray, cpx, cpy, cpz, cr, ng.x, ng.y, ng.z, ng.w, t1, cj, aj);
-        jc = f4add(jc, cj);
-        jn = f4add(jn, aj);
+        face_jacobian(ray, c.x, c.y, c.z, c.r, np.x, np.y, np.z, np.w, t1, cj, aj);
+        J.jc = f4add(J.jc, cj);
+        J.jn = f4add(J.jn, aj);
     }
-    sg.jp = jp;
-    sg.jc = jc;
-    sg.jn = jn;
-    return true;
+    return J;
 }
 
 template <bool BOUNDED>
@@ -592,10 +644,9 @@ record_paths_kernel(const __grid_constant__ RecordParams P) {
     uint32_t count = 0, status = 0;
     if (make_ray(vd, x, y, ray)) {
         float t0 = 0.0f;
-        uint32_t cur = P.start_cells[view], prev = cur;
-        float4 g = __ldg(m.geom + cur);
-        float cpx = g.x, cpy = g.y, cpz = g.z, cr = g.w;
-        float ppx = cpx, ppy = cpy, ppz = cpz, pr = cr;
+        Cell c = load_cell(m, P.start_cells[view]);
+        uint32_t prev = c.id;
+        float4 pp = make_float4(c.x, c.y, c.z, c.r);
         const bool want_jac = P.buf.dt_grad_current_dev || P.buf.dt_grad_previous_dev ||
                               P.buf.dt_grad_next_dev;
         uint32_t steps = 0;
@@ -607,43 +658,38 @@ record_paths_kernel(const __grid_constant__ RecordParams P) {
                 break;
             }
             float best;
-            uint32_t nj, faces;
-            float4 ng;
-            find_exit<BOUNDED>(m, cur, cpx, cpy, cpz, cr, ray, t0, vd.depth, best, nj, ng, faces);
-            const uint32_t next = nj == kNone ? cur : nj;
-            Segment sg;
-            if (interval_jacobian<BOUNDED>(ray, prev, cur, next, ppx, ppy, ppz, pr, cpx, cpy, cpz,
-                                           cr, ng, t0, best, want_jac, sg)) {
+            FaceEntry win;
+            const bool has_exit = find_exit<BOUNDED>(m, c, ray, t0, vd.depth, best, win);
+            const uint32_t next = has_exit ? win.link.x : c.id;
+            Interval iv;
+            if (record_interval<BOUNDED>(ray, c, t0, best, iv)) {
                 if (count < P.buf.max_steps) {
                     const size_t k = row + count;
                     if (P.buf.previous_cells_dev) P.buf.previous_cells_dev[k] = prev;
-                    if (P.buf.cells_dev) P.buf.cells_dev[k] = cur;
+                    if (P.buf.cells_dev) P.buf.cells_dev[k] = c.id;
                     if (P.buf.next_cells_dev) P.buf.next_cells_dev[k] = next;
-                    if (P.buf.dts_dev) P.buf.dts_dev[k] = sg.end - sg.start;
-                    if (P.buf.dt_grad_previous_dev)
-                        reinterpret_cast<float4 *>(P.buf.dt_grad_previous_dev)[k] = sg.jp;
-                    if (P.buf.dt_grad_current_dev)
-                        reinterpret_cast<float4 *>(P.buf.dt_grad_current_dev)[k] = sg.jc;
-                    if (P.buf.dt_grad_next_dev)
-                        reinterpret_cast<float4 *>(P.buf.dt_grad_next_dev)[k] = sg.jn;
+                    if (P.buf.dts_dev) P.buf.dts_dev[k] = iv.end - iv.start;
+                    if (want_jac) {
+                        const Jacobians J = interval_jacobians(ray, iv, prev, pp, c, has_exit,
+                                                               win.site, t0, best);
+                        if (P.buf.dt_grad_previous_dev)
+                            reinterpret_cast<float4 *>(P.buf.dt_grad_previous_dev)[k] = J.jp;
+                        if (P.buf.dt_grad_current_dev)
+                            reinterpret_cast<float4 *>(P.buf.dt_grad_current_dev)[k] = J.jc;
+                        if (P.buf.dt_grad_next_dev)
+                            reinterpret_cast<float4 *>(P.buf.dt_grad_next_dev)[k] = J.jn;
+                    }
                 }
                 count += 1;
             }
-            if (nj == kNone) {
+            if (!has_exit) {
                 finished = true;
                 break;
             }
             t0 = fmaxf(t0, best);
-            prev = cur;
-            ppx = cpx;
-            ppy = cpy;
-            ppz = cpz;
-            pr = cr;
-            cur = nj;
-            cpx = ng.x;
-            cpy = ng.y;
-            cpz = ng.z;
-            cr = ng.w;
+            prev = c.id;
+            pp = make_float4(c.x, c.y, c.z, c.r);
+            c = cell_from_face(win);
         }
         if (!finished) status = BV_PATH_TRUNCATED;
     }
@@ -652,7 +698,7 @@ record_paths_kernel(const __grid_constant__ RecordParams P) {
 }
 
 // ---------------------------------------------------------------------------
-// fused forward + loss + replay backward
+// training: forward + loss kernel, then the replay backward kernel
 // ---------------------------------------------------------------------------
 // Error-free sum a + b = s + e (Knuth's two-sum).
 __device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
@@ -670,63 +716,35 @@ __device__ __forceinline__ void acc_add(float &hi, float &lo, float v) {
     lo = lo + e;
 }
 
-template <int DEG>
-__device__ __forceinline__ void scatter_sh(float *d_sh, uint32_t cell, float gw0, float gw1,
-                                           float gw2, const float (&Y)[ShDims<DEG>::K],
-                                           bool m0, bool m1, bool m2) {
-    constexpr int K = ShDims<DEG>::K;
-    constexpr int N = 3 * K;
-    float *row = d_sh + (size_t)cell * N;
-    const float gw[3] = {m0 ? gw0 : 0.f, m1 ? gw1 : 0.f, m2 ? gw2 : 0.f};
-    if (N % 4 == 0) {
-        float4 *row4 = reinterpret_cast<float4 *>(row);
-#pragma unroll
-        for (int q = 0; q < N / 4; ++q) {
-            float v[4];
-#pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                const int i = q * 4 + h;
-                v[h] = gw[i % 3] * Y[i / 3];
-            }
-            atomicAdd(row4 + q, make_float4(v[0], v[1], v[2], v[3]));
-        }
-    } else {
-#pragma unroll
-        for (int i = 0; i < N; ++i) {
-            const float v = gw[i % 3] * Y[i / 3];
-            if (v != 0.0f) atomicAdd(row + i, v);
-        }
-    }
-}
+// The walk of the training contract: record_path_jacobians' loop
+// (trace.rs:1573-1676) with trace_one_ray's transmittance cut (trace.rs:1724)
+// evaluated on dt clamped to max_dt (MAX_PATH_DT, diff_render.rs:2484).
+// Shared operation for operation by the forward and the replay kernels.
+struct TrainWalk {
+    Ray ray;
+    Cell c;
+    uint32_t prev;
+    float4 pp;
+    float t0, T, depth;
+    uint32_t steps;
+};
 
-__device__ __forceinline__ void scatter_pos(float *d_pos, float *d_radius, uint32_t cell,
-                                            float gdt, float4 j) {
-    if (d_pos) {
-        float *p = d_pos + 3 * (size_t)cell;
-        atomicAdd(p + 0, gdt * j.x);
-        atomicAdd(p + 1, gdt * j.y);
-        atomicAdd(p + 2, gdt * j.z);
-    }
-    if (d_radius && j.w != 0.0f) atomicAdd(d_radius + cell, gdt * j.w);
+// Site gradients (x, y, z, radius) go to a float4-per-site table with one
+// vector atomic; fold_site_grads_kernel adds it to the caller's tables.
+__device__ __forceinline__ void scatter_site(float4 *d_site, uint32_t cell, float gdt, float4 j) {
+    atomicAdd(d_site + cell, make_float4(gdt * j.x, gdt * j.y, gdt * j.z, gdt * j.w));
 }
 
 template <int DEG, bool BOUNDED, bool BF16>
-__global__ void __launch_bounds__(kWalkBlock)
-forward_backward_kernel(const __grid_constant__ TrainParams P) {
+__global__ void __launch_bounds__(kWalkBlock, BV_MINB_TRAIN_FWD)
+train_forward_kernel(const __grid_constant__ TrainParams P) {
     const DeviceModel &m = P.m;
-    constexpr int K = ShDims<DEG>::K;
     bool drained = false, active = false;
-    bool replay = false;
-    Ray ray;
-    float t0 = 0.f, T = 1.f, depth = 0.f;
-    uint32_t cur = 0, prev = 0, steps = 0, start_cell = 0;
-    float cpx = 0.f, cpy = 0.f, cpz = 0.f, cr = 0.f, ppx = 0.f, ppy = 0.f, ppz = 0.f, pr = 0.f;
-    float Ch[3] = {0.f, 0.f, 0.f}, Cl[3] = {0.f, 0.f, 0.f};  // forward colour
-    float Ph[3] = {0.f, 0.f, 0.f}, Pl[3] = {0.f, 0.f, 0.f};  // replay prefix
-    float gC[3] = {0.f, 0.f, 0.f};                          // dL/dC
+    TrainWalk W = {};
+    float Ch[3] = {0.f, 0.f, 0.f}, Cl[3] = {0.f, 0.f, 0.f};
     size_t pix = 0;
     float loss_acc = 0.f;
-    unsigned long long n_rays = 0, n_steps = 0, n_faces = 0;
+    uint32_t n_rays = 0, n_steps = 0, n_faces = 0;
     for (;;) {
         uint32_t w;
         if (refill(P.work_counter, P.total_work, active, drained, w)) {
@@ -734,18 +752,17 @@ forward_backward_kernel(const __grid_constant__ TrainParams P) {
             if (work_item(P, w, view, x, y)) {
                 const ViewDesc &vd = P.views[view];
                 pix = pixel_index(P, view, x, y);
-                make_ray(vd, x, y, ray);
-                start_cell = P.start_cells[view];
-                depth = vd.depth;
-                replay = false;
+                const bool ok = make_ray(vd, x, y, W.ray);
+                W.c = load_cell(m, P.start_cells[view]);
+                W.prev = W.c.id;
+                W.t0 = 0.f;
+                W.T = 1.f;
+                W.depth = ok ? vd.depth : -1.0f;  // a failed direction records nothing
+                W.steps = 0;
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) Ch[ch] = Cl[ch] = 0.f;
                 active = true;
                 n_rays += 1;
-                for (int c = 0; c < 3; ++c) {
-                    Ch[c] = Cl[c] = Ph[c] = Pl[c] = 0.f;
-                }
-                // (re)start of the walk is done below when steps == 0
-                steps = 0;
-                cur = kNone;
             }
         }
         if (__ballot_sync(kFull, active) == 0) {
@@ -753,118 +770,67 @@ forward_backward_kernel(const __grid_constant__ TrainParams P) {
             continue;
         }
         if (!active) continue;
-        if (cur == kNone) {
-            cur = start_cell;
-            prev = cur;
-            const float4 g = __ldg(m.geom + cur);
-            cpx = ppx = g.x;
-            cpy = ppy = g.y;
-            cpz = ppz = g.z;
-            cr = pr = g.w;
-            t0 = 0.f;
-            T = 1.f;
-            steps = 0;
-        }
         bool done = false;
-        const bool dir_ok = ray.dx != 0.f || ray.dy != 0.f || ray.dz != 0.f;
-        if (!dir_ok || steps >= P.max_steps) {
+        if (W.steps >= P.max_steps) {
             done = true;
         } else {
-            steps += 1;
-            if (T <= P.weight_threshold || t0 > depth) {
+            W.steps += 1;
+            if (W.T <= P.weight_threshold || W.t0 > W.depth) {
                 done = true;
             } else {
                 float best;
-                uint32_t nj, faces;
-                float4 ng;
-                find_exit<BOUNDED>(m, cur, cpx, cpy, cpz, cr, ray, t0, depth, best, nj, ng, faces);
-                if (!replay) {
-                    n_steps += 1;
-                    n_faces += faces;
-                }
-                const uint32_t next = nj == kNone ? cur : nj;
-                Segment sg;
-                if (interval_jacobian<BOUNDED>(ray, prev, cur, next, ppx, ppy, ppz, pr, cpx, cpy,
-                                               cpz, cr, ng, t0, best, replay, sg)) {
-                    const float dens = __ldg(m.density + cur);
+                FaceEntry win;
+                const bool has_exit = find_exit<BOUNDED>(m, W.c, W.ray, W.t0, W.depth, best, win);
+                n_steps += 1;
+                n_faces += W.c.end - W.c.begin;
+                Interval iv;
+                if (record_interval<BOUNDED>(W.ray, W.c, W.t0, best, iv)) {
+                    const float dens = W.c.density;
                     if (dens > 1e-6f) {
-                        const float dt_raw = sg.end - sg.start;
-                        const float dt = fminf(dt_raw, P.max_dt);
+                        const float dt = fminf(iv.end - iv.start, P.max_dt);
                         const float alpha = 1.0f - bv_expf(-dens * dt);
-                        const float wgt = T * alpha;
-                        const float Tn = T * (1.0f - alpha);
-                        float c[ShDims<DEG>::N];
-                        load_sh_row<DEG, BF16>(m, cur, c);
+                        const float wgt = W.T * alpha;
+                        float coef[ShDims<DEG>::N];
+                        load_sh_row<DEG, BF16>(m, W.c.id, coef);
                         float cu[3];
-                        eval_sh<DEG>(c, ray.dx, ray.dy, ray.dz, cu[0], cu[1], cu[2]);
-                        const float cc[3] = {fmaxf(cu[0], 0.f), fmaxf(cu[1], 0.f),
-                                             fmaxf(cu[2], 0.f)};
-                        if (!replay) {
+                        eval_sh<DEG>(coef, W.ray.dx, W.ray.dy, W.ray.dz, cu[0], cu[1], cu[2]);
 #pragma unroll
-                            for (int ch = 0; ch < 3; ++ch) acc_add(Ch[ch], Cl[ch], wgt * cc[ch]);
-                        } else {
-                            float gs = 0.f;
-#pragma unroll
-                            for (int ch = 0; ch < 3; ++ch) {
-                                acc_add(Ph[ch], Pl[ch], wgt * cc[ch]);
-                                const float suffix = (Ch[ch] - Ph[ch]) + (Cl[ch] - Pl[ch]);
-                                gs += gC[ch] * (Tn * cc[ch] - suffix);
-                            }
-                            atomicAdd(P.d_density + cur, dt * gs);
-                            float Y[K];
-                            sh_basis<DEG>(ray.dx, ray.dy, ray.dz, Y);
-                            scatter_sh<DEG>(P.d_sh, cur, gC[0] * wgt, gC[1] * wgt, gC[2] * wgt, Y,
-                                            cu[0] > 0.f, cu[1] > 0.f, cu[2] > 0.f);
-                            if ((P.d_pos || P.d_radius) && dt_raw < P.max_dt) {
-                                const float gdt = dens * gs;
-                                if (prev != cur) scatter_pos(P.d_pos, P.d_radius, prev, gdt, sg.jp);
-                                scatter_pos(P.d_pos, P.d_radius, cur, gdt, sg.jc);
-                                if (next != cur) scatter_pos(P.d_pos, P.d_radius, next, gdt, sg.jn);
-                            }
-                        }
-                        T = Tn;
+                        for (int ch = 0; ch < 3; ++ch)
+                            acc_add(Ch[ch], Cl[ch], wgt * fmaxf(cu[ch], 0.f));
+                        W.T = W.T * (1.0f - alpha);
                     }
                 }
-                if (nj == kNone) {
+                if (!has_exit) {
                     done = true;
                 } else {
-                    t0 = fmaxf(t0, best);
-                    prev = cur;
-                    ppx = cpx;
-                    ppy = cpy;
-                    ppz = cpz;
-                    pr = cr;
-                    cur = nj;
-                    cpx = ng.x;
-                    cpy = ng.y;
-                    cpz = ng.z;
-                    cr = ng.w;
+                    W.t0 = fmaxf(W.t0, best);
+                    W.c = cell_from_face(win);
                 }
             }
         }
         if (done) {
-            if (!replay) {
-                const float *tg = P.target + 3 * pix;
-                float l = 0.f;
+            const float *tg = P.target + 3 * pix;
+            float l = 0.f, gC[3];
 #pragma unroll
-                for (int ch = 0; ch < 3; ++ch) {
-                    const float col = Ch[ch] + Cl[ch];
-                    const float diff = col - __ldg(tg + ch);
-                    if (P.loss_kind == BV_LOSS_L2) {
-                        l += diff * diff;
-                        gC[ch] = 2.0f * diff * P.inv_count;
-                    } else {
-                        l += fabsf(diff);
-                        gC[ch] = (diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f)) * P.inv_count;
-                    }
-                    if (P.rgb_out) P.rgb_out[3 * pix + ch] = col;
+            for (int ch = 0; ch < 3; ++ch) {
+                const float col = Ch[ch] + Cl[ch];
+                const float diff = col - __ldg(tg + ch);
+                if (P.loss_kind == BV_LOSS_L2) {
+                    l += diff * diff;
+                    gC[ch] = 2.0f * diff * P.inv_count;
+                } else {
+                    l += fabsf(diff);
+                    gC[ch] = (diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f)) * P.inv_count;
                 }
-                loss_acc += l;
-                replay = true;
-                cur = kNone;  // restart the same ray for the replay
-            } else {
-                active = false;
+                if (P.rgb_out) P.rgb_out[3 * pix + ch] = col;
             }
+            loss_acc += l;
+            RayState st;
+            st.c_hi = make_float4(Ch[0], Ch[1], Ch[2], gC[0]);
+            st.c_lo = make_float4(Cl[0], Cl[1], Cl[2], gC[1]);
+            st.g = make_float4(gC[2], 0.f, 0.f, 0.f);
+            P.ray_state[pix] = st;
+            active = false;
         }
     }
 #pragma unroll
@@ -878,14 +844,234 @@ forward_backward_kernel(const __grid_constant__ TrainParams P) {
             n_faces += __shfl_xor_sync(kFull, n_faces, s);
         }
         if ((threadIdx.x & 31u) == 0) {
-            atomicAdd(P.stats + 0, n_rays);
-            atomicAdd(P.stats + 1, n_steps);
-            atomicAdd(P.stats + 2, n_faces);
+            atomicAdd(P.stats + 0, (unsigned long long)n_rays);
+            atomicAdd(P.stats + 1, (unsigned long long)n_steps);
+            atomicAdd(P.stats + 2, (unsigned long long)n_faces);
         }
     }
 }
 
+// Lanes of a warp that scatter into the same cell at the same replay step
+// (coherent rays walk the same cells) are reduced first: __match_any_sync
+// groups them, a binary tree over their ranks sums the values (the partner at
+// rank r + 2^l is found with __fns), and the rank-0 lane issues one vector
+// atomic per float4.  All 32 lanes must call these together.
+struct PeerTree {
+    int levels;          // warp-uniform tree depth
+    bool leader;         // rank 0 of its group
+    int src[5];          // partner lane per level
+    bool recv[5];        // adds the partner's value at that level
+};
+
+__device__ __forceinline__ PeerTree peer_tree(bool valid, uint32_t key) {
+    PeerTree t;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned peers = __match_any_sync(kFull, valid ? key : 0xffffffffu);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    const int n = __popc(peers);
+    const unsigned maxn = __reduce_max_sync(kFull, valid ? (unsigned)n : 1u);
+    t.levels = maxn <= 1 ? 0 : 32 - __clz(maxn - 1);
+    t.leader = rank == 0;
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+        const int off = 1 << l;
+        const bool r = (rank & ((off << 1) - 1)) == 0 && rank + off < n;
+        t.recv[l] = r;
+        t.src[l] = r ? (int)__fns(peers, 0, rank + off + 1) : (int)lane;
+    }
+    return t;
+}
+
+__device__ __forceinline__ float group_sum(const PeerTree &t, float v) {
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+        if (l < t.levels) {
+            const float o = __shfl_sync(kFull, v, t.src[l]);
+            if (t.recv[l]) v += o;
+        }
+    }
+    return v;
+}
+
+__device__ __forceinline__ float4 group_sum4(const PeerTree &t, float4 v) {
+    return make_float4(group_sum(t, v.x), group_sum(t, v.y), group_sum(t, v.z), group_sum(t, v.w));
+}
+
+// Replay: walk each ray again front to back, recompute T, w and the colour
+// of every segment, form the suffix S_{k+1} = C - P_k from the compensated
+// prefix, and scatter
+//   dL/dsigma_k = dt_k sum_c g_c (T_{k+1} c_kc - S_{k+1,c})
+//   dL/dSH_kmc  = g_c w_k Y_m(d) [c_kc unclamped > 0]
+//   dL/ddt_k    = sigma_k sum_c g_c (T_{k+1} c_kc - S_{k+1,c})  -> sites
+// through the exact dt Jacobians of the fixed path (trace.rs:1077-1124).
+template <int DEG, bool BOUNDED, bool BF16>
+__global__ void __launch_bounds__(kWalkBlock, BV_MINB_TRAIN_BWD)
+train_backward_kernel(const __grid_constant__ TrainParams P) {
+    const DeviceModel &m = P.m;
+    constexpr int K = ShDims<DEG>::K;
+    constexpr int N = 3 * K;
+    bool drained = false, active = false;
+    TrainWalk W = {};
+    float Ch[3] = {0.f, 0.f, 0.f}, Cl[3] = {0.f, 0.f, 0.f};
+    float Ph[3] = {0.f, 0.f, 0.f}, Pl[3] = {0.f, 0.f, 0.f};
+    float gC[3] = {0.f, 0.f, 0.f};
+    for (;;) {
+        uint32_t w;
+        if (refill(P.work_counter + 1, P.total_work, active, drained, w)) {
+            uint32_t view, x, y;
+            if (work_item(P, w, view, x, y)) {
+                const ViewDesc &vd = P.views[view];
+                const size_t pix = pixel_index(P, view, x, y);
+                const bool ok = make_ray(vd, x, y, W.ray);
+                W.c = load_cell(m, P.start_cells[view]);
+                W.prev = W.c.id;
+                W.pp = make_float4(W.c.x, W.c.y, W.c.z, W.c.r);
+                W.t0 = 0.f;
+                W.T = 1.f;
+                W.depth = ok ? vd.depth : -1.0f;
+                W.steps = 0;
+                const RayState st = P.ray_state[pix];
+                Ch[0] = st.c_hi.x;
+                Ch[1] = st.c_hi.y;
+                Ch[2] = st.c_hi.z;
+                Cl[0] = st.c_lo.x;
+                Cl[1] = st.c_lo.y;
+                Cl[2] = st.c_lo.z;
+                gC[0] = st.c_hi.w;
+                gC[1] = st.c_lo.w;
+                gC[2] = st.g.x;
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) Ph[ch] = Pl[ch] = 0.f;
+                active = (gC[0] != 0.f || gC[1] != 0.f || gC[2] != 0.f);
+            }
+        }
+        if (__ballot_sync(kFull, active) == 0) {
+            if (drained) break;
+            continue;
+        }
+        // one replay step per active lane; the current cell's contribution
+        // is scattered below at a point all 32 lanes reach
+        bool done = false, contrib = false;
+        uint32_t cell = 0;
+        float g_density = 0.f, gw[3] = {0.f, 0.f, 0.f};
+        float4 g_site = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (active) {
+            if (W.steps >= P.max_steps) {
+                done = true;
+            } else {
+                W.steps += 1;
+                if (W.T <= P.weight_threshold || W.t0 > W.depth) {
+                    done = true;
+                } else {
+                    float best;
+                    FaceEntry win;
+                    const bool has_exit =
+                        find_exit<BOUNDED>(m, W.c, W.ray, W.t0, W.depth, best, win);
+                    Interval iv;
+                    if (record_interval<BOUNDED>(W.ray, W.c, W.t0, best, iv)) {
+                        const float dens = W.c.density;
+                        if (dens > 1e-6f) {
+                            const float dt_raw = iv.end - iv.start;
+                            const float dt = fminf(dt_raw, P.max_dt);
+                            const float alpha = 1.0f - bv_expf(-dens * dt);
+                            const float wgt = W.T * alpha;
+                            const float Tn = W.T * (1.0f - alpha);
+                            float coef[ShDims<DEG>::N];
+                            load_sh_row<DEG, BF16>(m, W.c.id, coef);
+                            float cu[3];
+                            eval_sh<DEG>(coef, W.ray.dx, W.ray.dy, W.ray.dz, cu[0], cu[1], cu[2]);
+                            float gs = 0.f;
+#pragma unroll
+                            for (int ch = 0; ch < 3; ++ch) {
+                                const float cc = fmaxf(cu[ch], 0.f);
+                                acc_add(Ph[ch], Pl[ch], wgt * cc);
+                                const float suffix = (Ch[ch] - Ph[ch]) + (Cl[ch] - Pl[ch]);
+                                gs += gC[ch] * (Tn * cc - suffix);
+                                gw[ch] = cu[ch] > 0.f ? gC[ch] * wgt : 0.f;
+                            }
+                            contrib = true;
+                            cell = W.c.id;
+                            g_density = dt * gs;
+                            if (P.d_site && dt_raw < P.max_dt) {
+                                const float gdt = dens * gs;
+                                const Jacobians J = interval_jacobians(
+                                    W.ray, iv, W.prev, W.pp, W.c, has_exit, win.site, W.t0, best);
+                                g_site = make_float4(gdt * J.jc.x, gdt * J.jc.y, gdt * J.jc.z,
+                                                     gdt * J.jc.w);
+                                if (W.prev != W.c.id && !iv.start_sphere)
+                                    scatter_site(P.d_site, W.prev, gdt, J.jp);
+                                if (has_exit && !iv.end_sphere)
+                                    scatter_site(P.d_site, win.link.x, gdt, J.jn);
+                            }
+                            W.T = Tn;
+                        }
+                    }
+                    if (!has_exit) {
+                        done = true;
+                    } else {
+                        W.t0 = fmaxf(W.t0, best);
+                        W.prev = W.c.id;
+                        W.pp = make_float4(W.c.x, W.c.y, W.c.z, W.c.r);
+                        W.c = cell_from_face(win);
+                    }
+                }
+            }
+        }
+        // warp-aggregated scatter of the current cells' gradients
+        const PeerTree tree = peer_tree(contrib, cell);
+        float Y[K];
+        sh_basis<DEG>(W.ray.dx, W.ray.dy, W.ray.dz, Y);
+        const float gd = group_sum(tree, g_density);
+        if (contrib && tree.leader) atomicAdd(P.d_density + cell, gd);
+        if (N % 4 == 0) {
+            float4 *row4 = reinterpret_cast<float4 *>(P.d_sh + (size_t)cell * N);
+#pragma unroll
+            for (int q = 0; q < N / 4; ++q) {
+                float v[4];
+#pragma unroll
+                for (int h = 0; h < 4; ++h) v[h] = gw[(q * 4 + h) % 3] * Y[(q * 4 + h) / 3];
+                const float4 s4 = group_sum4(tree, make_float4(v[0], v[1], v[2], v[3]));
+                if (contrib && tree.leader) atomicAdd(row4 + q, s4);
+            }
+        } else {
+            float *row = P.d_sh + (size_t)cell * N;
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const float sv = group_sum(tree, gw[i % 3] * Y[i / 3]);
+                if (contrib && tree.leader && sv != 0.0f) atomicAdd(row + i, sv);
+            }
+        }
+        if (P.d_site) {
+            const float4 s4 = group_sum4(tree, g_site);
+            if (contrib && tree.leader) atomicAdd(P.d_site + cell, s4);
+        }
+        if (done) active = false;
+    }
+}
+
+// d_pos[i] += site[i].xyz, d_radius[i] += site[i].w (scatter-add semantics
+// of the caller's tables), then clears the site table for the next call.
+__global__ void fold_site_grads_kernel(float4 *site, uint32_t n, float *d_pos, float *d_radius) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 g = site[i];
+    if (d_pos) {
+        d_pos[3 * (size_t)i + 0] += g.x;
+        d_pos[3 * (size_t)i + 1] += g.y;
+        d_pos[3 * (size_t)i + 2] += g.z;
+    }
+    if (d_radius) d_radius[i] += g.w;
+    site[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
 }  // namespace
+
+cudaError_t launch_fold_site_grads(float4 *site, uint32_t n, float *d_pos, float *d_radius,
+                                   cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    fold_site_grads_kernel<<<(n + 255) / 256, 256, 0, s>>>(site, n, d_pos, d_radius);
+    return cudaGetLastError();
+}
 
 // ---------------------------------------------------------------------------
 // launchers: pick the instantiation for (SH degree, bounded, bf16)
@@ -920,8 +1106,13 @@ cudaError_t launch_walk_forward(const WalkParams &p, int grid, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_forward_backward(const TrainParams &p, int grid, cudaStream_t s) {
-    BV_SELECT(forward_backward_kernel, p, grid, s);
+cudaError_t launch_train_forward(const TrainParams &p, int grid, cudaStream_t s) {
+    BV_SELECT(train_forward_kernel, p, grid, s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_train_backward(const TrainParams &p, int grid, cudaStream_t s) {
+    BV_SELECT(train_backward_kernel, p, grid, s);
     return cudaGetLastError();
 }
 
@@ -944,9 +1135,11 @@ int walk_grid_size(int device, int kind) {
     if (kind == 0)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, walk_forward_kernel<3, false, false>,
                                                       kWalkBlock, 0);
+    else if (kind == 1)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, train_forward_kernel<3, false, false>,
+                                                      kWalkBlock, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-                                                      forward_backward_kernel<3, false, false>,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, train_backward_kernel<3, false, false>,
                                                       kWalkBlock, 0);
     if (per_sm < 1) per_sm = 1;
     return sms * per_sm;

@@ -189,9 +189,11 @@ typedef struct bv_grads {
 /* Forward + loss + backward for a batch of cameras of one size.
  * target_rgb_dev [n][height][width][3]; loss_dev receives the scalar loss
  * (float, overwritten); rgb_out_dev (may be NULL) the rendered colours
- * [n][height][width][3].  One fused launch: every ray is walked, its loss
- * gradient formed, and its path replayed to scatter parameter gradients;
- * no per-sample state is stored. */
+ * [n][height][width][3].  Two walk launches: the forward kernel walks
+ * every ray and forms its loss gradient dL/dC; the replay kernel walks the
+ * same path again, recomputing transmittance, and scatters the parameter
+ * gradients.  Only per-ray state (colour and dL/dC, 48 bytes) passes between
+ * them; no per-sample state is stored. */
 bv_status bv_forward_backward(bv_tracer *tracer, const bv_camera *cameras, uint32_t n_cameras,
                               uint32_t width, uint32_t height, const float *target_rgb_dev,
                               const bv_train_settings *settings, const bv_grads *grads,
@@ -202,8 +204,10 @@ bv_status bv_forward_backward(bv_tracer *tracer, const bv_camera *cameras, uint3
  * the last dispatch / record / forward_backward call on this tracer.
  * Synchronises that stream. */
 typedef struct bv_launch_stats {
-    float kernel_ms;        /* main traversal kernel */
+    float kernel_ms;        /* traversal kernels (training: forward + replay) */
     float start_cell_ms;    /* start-cell search */
+    float forward_ms;       /* training: forward + loss kernel */
+    float backward_ms;      /* training: replay backward kernel */
     uint64_t rays;
     uint64_t steps;         /* walk loop iterations over all rays */
     uint64_t faces;         /* neighbour faces tested */

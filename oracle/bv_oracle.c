@@ -836,15 +836,24 @@ enum { ROLE_FIXED = 0, ROLE_FACE = 1, ROLE_SPHERE = 2 };
 typedef struct {
     uint32_t prev, cell, next;
     uint8_t start_role, end_role;
+    float start32, end32; /* the FP32 walk's interval */
+    float jp32[4], jc32[4], jn32[4]; /* its FP32 dt Jacobians (the recorder's) */
 } seg_t;
 
 /* Recorded walk of the training contract: record_path_jacobians' loop
  * (trace.rs:1573-1676) with the FP32 transmittance cut of trace_one_ray
  * (trace.rs:1724) evaluated on dt clamped to max_dt (diff_render.rs:2484).
  * Identical, operation for operation, to the device fwd+bwd walk. */
+static inline void two_sum_f(float a, float b, float *s, float *e) {
+    *s = a + b;
+    const float bb = *s - a;
+    *e = (a - (*s - bb)) + (b - bb);
+}
+
 static int record_training_walk(const bvo_model *m, const float o[3], const float d[3],
                                 uint32_t start, uint32_t max_steps, float depth, float thr,
-                                float max_dt, seg_t *segs) {
+                                float max_dt, seg_t *segs, float rgb32[3]) {
+    float ch[3] = {0.0f, 0.0f, 0.0f}, cl[3] = {0.0f, 0.0f, 0.0f};
     float t0 = 0.0f, T = 1.0f;
     uint32_t current = start, previous = start;
     const float *p = m->points + 4 * (size_t)current;
@@ -880,13 +889,29 @@ static int record_training_walk(const bvo_model *m, const float o[3], const floa
             }
         }
         if (ok && end_t > start_t && isfinite(start_t) && isfinite(end_t)) {
-            seg_t sg = {previous, current, next, srole, erole};
+            seg_t sg = {previous, current, next, srole, erole, start_t, end_t,
+                        {0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+            bvo_path_entry e;
+            if (path_interval_jacobian(m, o, d, bounded, previous, current, next, t0, best, &e)) {
+                memcpy(sg.jp32, e.dt_d_previous, 16);
+                memcpy(sg.jc32, e.dt_d_current, 16);
+                memcpy(sg.jn32, e.dt_d_next, 16);
+            }
             segs[count++] = sg;
             const float dens = m->points[4 * (size_t)current + 3];
             if (dens > 1e-6f) {
                 const float dt = fminf(end_t - start_t, max_dt);
                 const float alpha = 1.0f - bvo_expf(-dens * dt);
-                T *= 1.0f - alpha;
+                const float w = T * alpha;
+                float c[3];
+                bvo_eval_rgb_sh(m, current, d, c, NULL);
+                for (int ch_i = 0; ch_i < 3; ++ch_i) {
+                    float sum, err;
+                    two_sum_f(ch[ch_i], w * c[ch_i], &sum, &err);
+                    ch[ch_i] = sum;
+                    cl[ch_i] = cl[ch_i] + err;
+                }
+                T = T * (1.0f - alpha);
             }
         }
         if (face < 0) break;
@@ -899,6 +924,7 @@ static int record_training_walk(const bvo_model *m, const float o[3], const floa
         cp[2] = np[2];
         cr = read_radius(m, next);
     }
+    for (int i = 0; i < 3; ++i) rgb32[i] = ch[i] + cl[i];
     return count;
 }
 
@@ -960,7 +986,8 @@ typedef struct {
 } seg_eval_t;
 
 static void eval_segment(const dparams *P, uint32_t K, const double o[3], const double d[3],
-                         const double Y[16], const seg_t *sg, double depth, seg_eval_t *ev) {
+                         const double Y[16], const seg_t *sg, double depth, int use_f32_interval,
+                         seg_eval_t *ev) {
     memset(ev, 0, sizeof(*ev));
     double t_start = 0.0, t_end = 0.0;
     double jc[4], ja[4];
@@ -993,6 +1020,17 @@ static void eval_segment(const dparams *P, uint32_t K, const double o[3], const 
         t_end = depth; /* no exit face: the fixed far plane */
     }
     ev->dt_raw = t_end - t_start;
+    /* Without perturbed parameters the segment length is the FP32 walk's own
+     * (what the device integrates and differentiates); the Jacobians above
+     * are evaluated in FP64 at the same geometry. */
+    if (use_f32_interval) {
+        ev->dt_raw = (double)sg->end32 - (double)sg->start32;
+        for (int i = 0; i < 4; ++i) {
+            ev->j_prev[i] = sg->jp32[i];
+            ev->j_cur[i] = sg->jc32[i];
+            ev->j_next[i] = sg->jn32[i];
+        }
+    }
     const double *c = P->sh + (size_t)sg->cell * 3u * K;
     for (int ch = 0; ch < 3; ++ch) {
         double acc = 0.0;
@@ -1007,8 +1045,8 @@ double bvo_forward_backward(const bvo_model *m, const bvo_camera *cams, uint32_t
                             uint32_t width, uint32_t height, uint32_t max_steps,
                             float weight_threshold, float max_dt, const float *target,
                             int loss_kind, const bvo_params_f64 *override_params,
-                            double *out_rgb, double *d_density, double *d_sh, double *d_pos,
-                            double *d_radius, int threads) {
+                            double *out_rgb, float *out_rgb32, double *d_density, double *d_sh,
+                            double *d_pos, double *d_radius, int threads) {
     const uint32_t deg = m->sh_degree > 3 ? 3 : m->sh_degree;
     const uint32_t K = sh_comps(deg);
     /* FP64 parameter view */
@@ -1057,18 +1095,22 @@ double bvo_forward_backward(const bvo_model *m, const bvo_camera *cams, uint32_t
             double C[3] = {0, 0, 0};
             int nseg = 0;
             double o[3] = {of[0], of[1], of[2]}, d[3] = {0, 0, 0}, Y[16];
+            float rgb32[3] = {0.0f, 0.0f, 0.0f};
             if (normalize_direction(df, dn)) {
                 d[0] = dn[0];
                 d[1] = dn[1];
                 d[2] = dn[2];
                 nseg = record_training_walk(m, of, dn, starts[v], max_steps, cams[v].depth,
-                                            weight_threshold, max_dt, segs);
+                                            weight_threshold, max_dt, segs, rgb32);
             }
+            if (out_rgb32)
+                for (int ch = 0; ch < 3; ++ch) out_rgb32[3 * (size_t)i + ch] = rgb32[ch];
             sh_basis_d(deg, d, Y);
             double T = 1.0;
             for (int k = 0; k < nseg; ++k) {
                 seg_eval_t *ev = &evs[k];
-                eval_segment(&P, K, o, d, Y, &segs[k], (double)cams[v].depth, ev);
+                eval_segment(&P, K, o, d, Y, &segs[k], (double)cams[v].depth,
+                             override_params == NULL, ev);
                 double dt = ev->dt_raw;
                 if (dt < 0.0) dt = 0.0;
                 if (dt > (double)max_dt) dt = (double)max_dt;

@@ -146,10 +146,17 @@ uint32_t bvo_containing_cell_f32(const bvo_model *m, const float position[3]);
  * loss_kind 0 = L2 (mean squared error, metrics.rs:7), 1 = L1 (mean abs).
  * Gradients are accumulated (+=) into caller-zeroed FP64 tables:
  * d_density [n], d_sh [n*3K], d_pos [n*3], d_radius [n] (may be NULL).
+ * Without params_override the segment lengths and their dt Jacobians are
+ * those of the FP32 walk and recorder (the quantities the device integrates
+ * and differentiates, as the reference's recorder hands FP32 Jacobians to
+ * its graph) and everything downstream is FP64.
  * params_override: if non-NULL, [n*4] FP64 positions+density and
- * [n*3K] FP64 SH and [n] FP64 radii replace the model values in the
- * integration (cells and boundary roles stay those of the FP32 walk), which
- * is what central finite differences on a fixed path need. */
+ * [n*3K] FP64 SH and [n] FP64 radii replace the model values and every
+ * segment length is re-derived in FP64 from them (cells and boundary roles
+ * stay those of the FP32 walk), which is what central finite differences on
+ * a fixed path need.  out_rgb32
+ * ([P*3], may be NULL) receives the FP32 colour of the walk, accumulated with
+ * the same compensated (two-sum) sum the device forward kernel uses. */
 typedef struct {
     const double *points; /* [n*4] */
     const double *sh;     /* [n*3K] */
@@ -160,8 +167,8 @@ double bvo_forward_backward(const bvo_model *m, const bvo_camera *cams, uint32_t
                             uint32_t width, uint32_t height, uint32_t max_steps,
                             float weight_threshold, float max_dt, const float *target,
                             int loss_kind, const bvo_params_f64 *override_params,
-                            double *out_rgb, double *d_density, double *d_sh, double *d_pos,
-                            double *d_radius, int threads);
+                            double *out_rgb, float *out_rgb32, double *d_density, double *d_sh,
+                            double *d_pos, double *d_radius, int threads);
 
 #ifdef __cplusplus
 }

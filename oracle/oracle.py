@@ -102,7 +102,7 @@ def lib():
         L.bvo_forward_backward.argtypes = [C.POINTER(Model), C.POINTER(Camera), C.c_uint32,
                                            C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
                                            C.c_float, f32p, C.c_int, C.POINTER(ParamsF64), f64p,
-                                           f64p, f64p, f64p, f64p, C.c_int]
+                                           f32p, f64p, f64p, f64p, f64p, C.c_int]
         _lib = L
     return _lib
 
@@ -299,6 +299,7 @@ def forward_backward(model: OracleModel, cams: Sequence, width, height, max_step
     K3 = model.sh.size // max(n, 1)
     cam_arr = (Camera * len(cams))(*[camera_struct(c) for c in cams])
     rgb = np.zeros((len(cams), height, width, 3), dtype=np.float64)
+    rgb32 = np.zeros((len(cams), height, width, 3), dtype=np.float32)
     tgt = None if target is None else np.ascontiguousarray(target, dtype=np.float32)
     dd = dsh = dpos = drad = None
     if want_grads:
@@ -318,8 +319,8 @@ def forward_backward(model: OracleModel, cams: Sequence, width, height, max_step
     loss = lib().bvo_forward_backward(
         C.byref(model.c), cam_arr, len(cams), width, height, max_steps, weight_threshold,
         max_dt, _ptr(tgt, f32p), loss_kind, C.byref(ov) if ov is not None else None,
-        _ptr(rgb, f64p), _ptr(dd, f64p), _ptr(dsh, f64p), _ptr(dpos, f64p), _ptr(drad, f64p),
-        threads)
+        _ptr(rgb, f64p), _ptr(rgb32, f32p), _ptr(dd, f64p), _ptr(dsh, f64p), _ptr(dpos, f64p),
+        _ptr(drad, f64p), threads)
     del keep
-    return dict(loss=loss, rgb=rgb, d_density=dd, d_sh=dsh,
+    return dict(loss=loss, rgb=rgb, rgb32=rgb32, d_density=dd, d_sh=dsh,
                 d_pos=None if dpos is None else dpos.reshape(n, 3), d_radius=drad)

@@ -101,11 +101,12 @@ def test_record_paths_bit_exact_cells_dt_and_jacobians(tiny):
 
 def test_visited_cell_sequences_bit_exact(tiny):
     """The render walk's per-ray visited cells equal the recorder's cells
-    (plain RadFoam emits one segment per visited cell)."""
+    (plain RadFoam emits one segment per visited cell).  The threshold -1
+    disables the transmittance cut (T <= 0 happens once T underflows)."""
     m, cam = tiny.model, tiny.cameras[0]
     om = O.OracleModel.from_scene(m)
     start = O.containing_cell_f64(om, cam.position)
-    _, _, cells, counts = O.render_walk(om, cam, 32, 32, 1024, 0.0, start, cell_capacity=512)
+    _, _, cells, counts = O.render_walk(om, cam, 32, 32, 1024, -1.0, start, cell_capacity=512)
     t = bv.RadFoamGpuTracer(m)
     gpu = t.record_paths([cam], 32, 32, 512, jacobians=False)
     torch.cuda.synchronize()
