@@ -44,7 +44,7 @@ EXPORTED_SYMBOLS = [
     "bv_radfoam_tracer_weight_threshold", "bv_radfoam_tracer_sh_degree",
     "bv_radfoam_tracer_start_point", "bv_radfoam_tracer_num_points", "bv_containing_point",
     "bv_record_paths", "bv_forward_backward", "bv_radfoam_tracer_enable_stats",
-    "bv_radfoam_tracer_last_stats",
+    "bv_radfoam_tracer_last_stats", "bv_containing_points_noalloc",
 ]
 
 
@@ -142,6 +142,8 @@ def load_library(path: str = LIB_PATH):
                                       C.POINTER(Grads), C.c_void_p, C.c_void_p, C.c_void_p]
     L.bv_radfoam_tracer_enable_stats.argtypes = [C.c_void_p, C.c_uint32]
     L.bv_radfoam_tracer_last_stats.argtypes = [C.c_void_p, C.POINTER(LaunchStats)]
+    L.bv_containing_points_noalloc.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_float),
+                                               C.c_uint32, C.c_void_p, C.c_void_p]
     _lib = L
     return L
 
@@ -199,6 +201,17 @@ def validate_model(model: PointCloudModel) -> Optional[str]:
     buf = C.create_string_buffer(512)
     st = load_library().bv_model_validate(C.byref(h.desc), buf, 512)
     return None if st == BV_OK else buf.value.decode()
+
+
+def containing_points_noalloc(sites, positions, out, stream=None):
+    """bv_containing_points_noalloc: power-nearest site of up to 32 query
+    positions without any device allocation.  ``sites`` is a CUDA float32
+    tensor [N, 4] (x, y, z, power radius), ``out`` a CUDA int32 tensor with
+    room for the indices; ``positions`` host floats [Q, 3]."""
+    p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+    _check(load_library().bv_containing_points_noalloc(
+        C.c_void_p(sites.data_ptr()), sites.shape[0], _fptr(p), p.shape[0],
+        C.c_void_p(out.data_ptr()), _stream_handle(stream)))
 
 
 def _stream_handle(stream) -> C.c_void_p:

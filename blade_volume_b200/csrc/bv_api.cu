@@ -61,6 +61,8 @@ uint16_t f32_to_bf16_rne(float f) {
 
 }  // namespace
 
+void bv::set_last_error(const char *message) { g_error = message; }
+
 struct bv_tracer {
     int device = 0;
     uint32_t n = 0;

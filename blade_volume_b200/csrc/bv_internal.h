@@ -136,6 +136,9 @@ struct StartCellScratch {
     uint32_t *counters;
     int blocks_per_query;
 };
+// Sets the calling thread's bv_last_error() message.
+void set_last_error(const char *message);
+
 cudaError_t launch_start_cells(const float4 *geom, uint32_t n, const StartCellQueries &queries,
                                const StartCellScratch &scratch, uint32_t *out, cudaStream_t s);
 int start_cell_blocks(uint32_t n);

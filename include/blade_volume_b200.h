@@ -218,6 +218,28 @@ typedef struct bv_launch_stats {
 bv_status bv_radfoam_tracer_enable_stats(bv_tracer *tracer, uint32_t enabled);
 bv_status bv_radfoam_tracer_last_stats(bv_tracer *tracer, bv_launch_stats *out);
 
+/* ---- allocation-free start-cell search -----------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * hosts whose device memory is owned by their own pool (a renderer's frame
+ * arena, a framework's caching allocator, a hard memory budget), where an
+ * allocation behind the pool's back breaks its accounting and cudaMalloc or
+ * cudaFree may synchronise the device mid-frame.  Same FP64 power-nearest
+ * search as bv_containing_point, without a tracer and without allocating:
+ *   sites_dev      [num_sites] float4 (x, y, z, power radius; 0 for plain
+ *                  RadFoam), 16-byte aligned, device memory
+ *   positions      [n_queries * 3] host floats, n_queries <= 32
+ *   out_index_dev  [n_queries] device uint32, receives the site indices
+ * Its scratch (per-block partials and counters, 113,792 bytes) is a fixed
+ * device array that every GPU loading the library holds until exit; every
+ * call shares it, so calls that overlap on the GPU (other streams, other
+ * threads) race.  More than 32 queries is rejected with
+ * BV_ERR_INVALID_ARGUMENT.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture. */
+bv_status bv_containing_points_noalloc(const float *sites_dev, uint32_t num_sites,
+                                       const float *positions, uint32_t n_queries,
+                                       uint32_t *out_index_dev, bv_stream stream);
+
 #ifdef __cplusplus
 }
 #endif
