@@ -360,3 +360,90 @@ def powerfoam_mix(n_sites: int = 1048576, views: int = 4, width: int = 1024, hei
     model = powerfoam_mixture(n_sites, seed=seed)
     cams = sphere_cameras(views, 3.0, 1, math.radians(60.0), width / height, 100.0)
     return Workload("powerfoam_mixture", model, cams, width, height, 1024, 1e-3)
+
+
+# --------------------------------------------------------------------------
+# relightable Gaussians
+# --------------------------------------------------------------------------
+@dataclasses.dataclass
+class GaussianModel:
+    """Gaussian PointCloudModel with explicit PBR attributes (lib.rs:174-239,
+    Transforms + PbrAttributes): mean + opacity, rotation (xyzw), scale,
+    unit normal, material index, and the material table (relight.rs:77-86:
+    albedo[3], roughness, specular_f0[3], pad)."""
+
+    points: np.ndarray  # float32 [N, 4]
+    rotations: np.ndarray  # float32 [N, 4]
+    scales: np.ndarray  # float32 [N, 3]
+    normals: np.ndarray  # float32 [N, 3]
+    material_indices: np.ndarray  # uint32 [N]
+    materials: np.ndarray  # float32 [M, 8]
+
+    @property
+    def n(self) -> int:
+        return int(self.points.shape[0])
+
+
+def quat_to_matrix(q: np.ndarray) -> np.ndarray:
+    """Rotation matrices [N, 3, 3] of unit quaternions (x, y, z, w)."""
+    x, y, z, w = (q[:, i].astype(np.float64) for i in range(4))
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1),
+    ], axis=1)
+
+
+def make_material(albedo, roughness, f0=(0.04, 0.04, 0.04)) -> np.ndarray:
+    return np.array([*albedo, roughness, *f0, 0.0], dtype=np.float32)
+
+
+def relight_gaussians(n: int = 1_000_000, seed: int = 0) -> GaussianModel:
+    """1M anisotropic Gaussians: means from the 3-component mixture,
+    log-scales N(-4, 0.5), rotations normalised N(0, 1)^4, opacity
+    sigmoid(N(0, 1)), albedo U[0, 1], GGX roughness U[0.2, 0.9], F0 0.04,
+    normal = the rotation's column of the smallest scale."""
+    rng = np.random.default_rng(seed)
+    means = mixture_points(rng, n).astype(np.float32)
+    scales = np.exp(rng.normal(-4.0, 0.5, (n, 3))).astype(np.float32)
+    q = rng.standard_normal((n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    q = q.astype(np.float32)
+    opacity = (1.0 / (1.0 + np.exp(-rng.standard_normal(n)))).astype(np.float32)
+    albedo = rng.random((n, 3)).astype(np.float32)
+    roughness = rng.uniform(0.2, 0.9, n).astype(np.float32)
+    R = quat_to_matrix(q)
+    smallest = np.argmin(scales, axis=1)
+    normals = R[np.arange(n), :, smallest]
+    normals /= np.linalg.norm(normals, axis=1, keepdims=True)
+    materials = np.zeros((n, 8), np.float32)
+    materials[:, 0:3] = albedo
+    materials[:, 3] = roughness
+    materials[:, 4:7] = 0.04
+    points = np.concatenate([means, opacity[:, None]], axis=1).astype(np.float32)
+    return GaussianModel(points, q, scales, normals.astype(np.float32),
+                         np.arange(n, dtype=np.uint32), materials)
+
+
+def sphere_lights(count: int = 16, radius: float = 2.0, intensity: float = 5.0, seed: int = 3):
+    """Isotropic point lights on a sphere (Fibonacci directions), as
+    PointLight fields (position, direction, intensity, exponent)."""
+    rng = np.random.default_rng(seed)
+    golden = math.pi * (3.0 - math.sqrt(5.0))
+    a = rng.standard_normal((3, 3))
+    qm, rm = np.linalg.qr(a)
+    qm = qm * np.sign(np.diag(rm))
+    out = []
+    for i in range(count):
+        y = 1.0 - 2.0 * (i + 0.5) / count
+        r = math.sqrt(max(0.0, 1.0 - y * y))
+        d = np.array([math.cos(golden * i) * r, y, math.sin(golden * i) * r]) @ qm.T
+        out.append((tuple((radius * d).astype(np.float32)), (0.0, 0.0, 1.0),
+                    (intensity, intensity, intensity), 0.0))
+    return out
+
+
+def relight_workload(n: int = 1_000_000, width: int = 1024, height: int = 768, seed: int = 0):
+    g = relight_gaussians(n, seed)
+    cam = sphere_cameras(1, 3.0, 1, math.radians(60.0), width / height, 100.0)[0]
+    return g, cam, sphere_lights()

@@ -1204,3 +1204,359 @@ double bvo_forward_backward(const bvo_model *m, const bvo_camera *cams, uint32_t
     (void)threads;
     return loss;
 }
+
+/* ------------------------------------------------------------------ */
+/* relightable Gaussians (relight.wgsl kernel 2, point light)          */
+/* ------------------------------------------------------------------ */
+
+/*
+ * log(x) for FP32 from the mathematics: x = m 2^e with m in [sqrt(1/2),
+ * sqrt(2)), f = m - 1, s = f / (2 + f), and log(1 + f) = 2 atanh(s) written
+ * as f - (f^2/2 - s (f^2/2 + R)) with R = z (2/3 + z (2/5 + ... + z 2/13)),
+ * z = s^2 (the atanh series; the exact leading term f carries the result so
+ * the rounding of the small correction stays below an ulp), plus e ln2 in
+ * the same hi/lo split as bvo_expf.  The device evaluates the identical
+ * sequence.
+ */
+float bvo_logf(float x) {
+    if (x != x || x < 0.0f) return NAN;
+    if (x == 0.0f) return -INFINITY;
+    if (x == INFINITY) return INFINITY;
+    union { float f; uint32_t u; } v = {x};
+    int e = 0;
+    if (v.u < 0x00800000u) { /* subnormal: scale by 2^24 */
+        v.f = x * 16777216.0f;
+        e = -24;
+    }
+    e += (int)((v.u >> 23) & 0xffu) - 127;
+    v.u = (v.u & 0x007fffffu) | 0x3f800000u; /* m in [1, 2) */
+    float m = v.f;
+    if (m > 1.41421353816986083984375f) {
+        m = m * 0.5f;
+        e += 1;
+    }
+    const float f = m - 1.0f;
+    const float s = f / (2.0f + f);
+    const float z = s * s;
+    float p = 0.1538461595773697f;
+    p = fmaf(p, z, 0.1818181872367859f);
+    p = fmaf(p, z, 0.2222222238779068f);
+    p = fmaf(p, z, 0.2857142984867096f);
+    p = fmaf(p, z, 0.4000000059604645f);
+    p = fmaf(p, z, 0.6666666865348816f);
+    const float R = z * p;
+    const float hfsq = 0.5f * f * f;
+    const float ef = (float)e;
+    return ef * 0.693115234375f -
+           ((hfsq - (s * (hfsq + R) + ef * 3.19461832987144589424133e-05f)) - f);
+}
+
+/* x^y = exp(y log x) for x >= 0. */
+float bvo_powf(float x, float y) {
+    if (x == 0.0f) return y > 0.0f ? 0.0f : (y == 0.0f ? 1.0f : INFINITY);
+    return bvo_expf(y * bvo_logf(x));
+}
+
+static inline void sub3f(const float a[3], const float b[3], float o[3]) {
+    o[0] = a[0] - b[0];
+    o[1] = a[1] - b[1];
+    o[2] = a[2] - b[2];
+}
+
+/* qrot (common.wgsl:386-390): v + q.w * t + cross(q.xyz, t), t = 2 cross(q.xyz, v) */
+static void qrot_f(const float q[4], const float v[3], float out[3]) {
+    const float t0 = 2.0f * (q[1] * v[2] - q[2] * v[1]);
+    const float t1 = 2.0f * (q[2] * v[0] - q[0] * v[2]);
+    const float t2 = 2.0f * (q[0] * v[1] - q[1] * v[0]);
+    out[0] = (v[0] + q[3] * t0) + (q[1] * t2 - q[2] * t1);
+    out[1] = (v[1] + q[3] * t1) + (q[2] * t0 - q[0] * t2);
+    out[2] = (v[2] + q[3] * t2) + (q[0] * t1 - q[1] * t0);
+}
+
+uint32_t bvo_relight_prepare(uint32_t n, const float *points, const float *rotations,
+                             const float *scales, const float *normals,
+                             const uint32_t *material_indices, uint32_t *kept_index,
+                             float *center, float *rotation, float *scale, float *opacity,
+                             float *normal, float *radius, float *support_sq,
+                             uint32_t *material) {
+    uint32_t k = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float o = points[4 * (size_t)i + 3];
+        if (o <= 0.03f) continue; /* GAUSSIAN_MIN_ALPHA, gpu/relight.rs:211-213 */
+        const float *s = scales + 3 * (size_t)i;
+        kept_index[k] = i;
+        memcpy(center + 3 * (size_t)k, points + 4 * (size_t)i, 12);
+        memcpy(rotation + 4 * (size_t)k, rotations + 4 * (size_t)i, 16);
+        memcpy(scale + 3 * (size_t)k, s, 12);
+        opacity[k] = o;
+        memcpy(normal + 3 * (size_t)k, normals + 3 * (size_t)i, 12);
+        radius[k] = 3.0f * cbrtf(s[0] * s[1] * s[2]);
+        support_sq[k] = 2.0f * logf(o / 0.03f);
+        material[k] = material_indices[i];
+        k += 1;
+    }
+    return k;
+}
+
+/* point_light_shade (relight.wgsl:190-261), diffuse_samples = 0. */
+void bvo_point_light_shade(const bvo_point_light *L, const float position[3],
+                           const float normal[3], const float view[3], const bvo_material *m,
+                           float out[3]) {
+    out[0] = out[1] = out[2] = 0.0f;
+    float fl[3];
+    sub3f(position, L->position, fl);
+    const float d2 = dot3f(fl, fl);
+    if (d2 <= 1.1920929e-7f) return;
+    const float inv = 1.0f / sqrtf(d2);
+    const float away[3] = {fl[0] * inv, fl[1] * inv, fl[2] * inv};
+    float angular = 1.0f;
+    if (L->exponent != 0.0f) angular = bvo_powf(fmaxf(dot3f(L->direction, away), 0.0f), L->exponent);
+    const float towards[3] = {-away[0], -away[1], -away[2]};
+    const float ndl = fmaxf(dot3f(normal, towards), 0.0f);
+    if (ndl == 0.0f) return;
+    const float a_d2 = angular / d2;
+    const float rad[3] = {L->intensity[0] * a_d2, L->intensity[1] * a_d2, L->intensity[2] * a_d2};
+    for (int c = 0; c < 3; ++c) out[c] = m->albedo[c] * rad[c] * ndl;
+    if (m->specular_f0[0] == 0.0f && m->specular_f0[1] == 0.0f && m->specular_f0[2] == 0.0f) return;
+    const float ndv = fmaxf(dot3f(normal, view), 0.0f);
+    const float hs[3] = {towards[0] + view[0], towards[1] + view[1], towards[2] + view[2]};
+    const float hs2 = dot3f(hs, hs);
+    if (ndv == 0.0f || hs2 <= 1.1920929e-7f) return;
+    const float hinv = 1.0f / sqrtf(hs2);
+    const float h[3] = {hs[0] * hinv, hs[1] * hinv, hs[2] * hinv};
+    const float ndh = fmaxf(dot3f(normal, h), 0.0f);
+    const float vdh = fminf(fmaxf(dot3f(view, h), 0.0f), 1.0f);
+    const float rc = fminf(fmaxf(m->roughness, 0.045f), 1.0f);
+    const float alpha = rc * rc;
+    const float a2 = alpha * alpha;
+    const float den = ndh * ndh * (a2 - 1.0f) + 1.0f;
+    const float pi = 3.14159265f;
+    const float dist = a2 / fmaxf(pi * den * den, 1.1754944e-38f);
+    const float sl = 2.0f * ndl / (ndl + sqrtf(a2 + (1.0f - a2) * ndl * ndl));
+    const float sv = 2.0f * ndv / (ndv + sqrtf(a2 + (1.0f - a2) * ndv * ndv));
+    const float g1 = 1.0f - vdh;
+    const float g2 = g1 * g1;
+    const float grazing = (g2 * g2) * g1;
+    const float scale = pi * dist * sl * sv / (4.0f * ndv);
+    for (int c = 0; c < 3; ++c) {
+        const float fres = m->specular_f0[c] + (1.0f - m->specular_f0[c]) * grazing;
+        out[c] += rad[c] * scale * fres;
+    }
+}
+
+/* relight.rs:204-323: PointLight::sample + point_light_specular +
+ * shade_point_light (the reference's CPU shading twin). */
+void bvo_shade_point_light_cpu(const bvo_point_light *L, const float point[3],
+                               const float normal_in[3], const float view_in[3],
+                               const bvo_material *m, float out[3]) {
+    out[0] = out[1] = out[2] = 0.0f;
+    float fl[3];
+    sub3f(point, L->position, fl);
+    const float d2 = dot3f(fl, fl);
+    if (!isfinite(d2) || d2 <= 1.1920929e-7f || !isfinite(L->exponent) || L->exponent < 0.0f)
+        return;
+    const float dl = sqrtf(d2);
+    const float away[3] = {fl[0] / dl, fl[1] / dl, fl[2] / dl};
+    float angular = 1.0f;
+    if (L->exponent != 0.0f) {
+        const float ln = sqrtf(dot3f(L->direction, L->direction));
+        const float r = 1.0f / ln;
+        if (!isfinite(r) || r <= 0.0f) return;
+        const float dn[3] = {L->direction[0] * r, L->direction[1] * r, L->direction[2] * r};
+        angular = powf(fmaxf(dot3f(dn, away), 0.0f), L->exponent);
+    }
+    const float towards[3] = {-away[0], -away[1], -away[2]};
+    float rad[3];
+    for (int c = 0; c < 3; ++c) rad[c] = L->intensity[c] * angular / d2;
+    float cosine = 0.0f, n[3] = {0, 0, 0};
+    {
+        const float r = 1.0f / sqrtf(dot3f(normal_in, normal_in));
+        if (isfinite(r) && r > 0.0f) {
+            n[0] = normal_in[0] * r;
+            n[1] = normal_in[1] * r;
+            n[2] = normal_in[2] * r;
+            cosine = fmaxf(dot3f(n, towards), 0.0f);
+        }
+    }
+    for (int c = 0; c < 3; ++c) out[c] = m->albedo[c] * rad[c] * cosine;
+    if (m->specular_f0[0] == 0.0f && m->specular_f0[1] == 0.0f && m->specular_f0[2] == 0.0f) return;
+    const float rn = 1.0f / sqrtf(dot3f(normal_in, normal_in));
+    const float rv = 1.0f / sqrtf(dot3f(view_in, view_in));
+    if (!isfinite(rn) || !(rn > 0.0f) || !isfinite(rv) || !(rv > 0.0f)) return;
+    const float nn[3] = {normal_in[0] * rn, normal_in[1] * rn, normal_in[2] * rn};
+    const float v[3] = {view_in[0] * rv, view_in[1] * rv, view_in[2] * rv};
+    const float ndl = fmaxf(dot3f(nn, towards), 0.0f);
+    const float ndv = fmaxf(dot3f(nn, v), 0.0f);
+    const float hs[3] = {towards[0] + v[0], towards[1] + v[1], towards[2] + v[2]};
+    const float rh = 1.0f / sqrtf(dot3f(hs, hs));
+    if (!isfinite(rh) || !(rh > 0.0f)) return;
+    const float h[3] = {hs[0] * rh, hs[1] * rh, hs[2] * rh};
+    if (ndl == 0.0f || ndv == 0.0f) return;
+    const float ndh = fmaxf(dot3f(nn, h), 0.0f);
+    const float vdh = fminf(fmaxf(dot3f(v, h), 0.0f), 1.0f);
+    const float rc = fminf(fmaxf(m->roughness, 0.045f), 1.0f);
+    const float alpha = rc * rc;
+    const float a2 = alpha * alpha;
+    const float den = ndh * ndh * (a2 - 1.0f) + 1.0f;
+    const float pi = 3.14159265358979f;
+    const float dist = a2 / fmaxf(pi * den * den, 1.17549435e-38f);
+    const float sl = 2.0f * ndl / (ndl + sqrtf(a2 + (1.0f - a2) * ndl * ndl));
+    const float sv = 2.0f * ndv / (ndv + sqrtf(a2 + (1.0f - a2) * ndv * ndv));
+    const float g1 = 1.0f - vdh;
+    const float g2 = g1 * g1;
+    const float grazing = (g2 * g2) * g1;
+    const float scale = pi * dist * (sl * sv) / (4.0f * ndv);
+    for (int c = 0; c < 3; ++c) {
+        const float fres = m->specular_f0[c] + (1.0f - m->specular_f0[c]) * grazing;
+        out[c] += rad[c] * scale * fres;
+    }
+}
+
+/* intersect_surfel, kernel 2 (relight.wgsl:419-441). */
+int bvo_intersect_gaussian(const bvo_relight_scene *s, uint32_t i, const float o[3],
+                           const float d[3], float t_end, float *t_out, float *alpha_out) {
+    const float *q = s->rotation + 4 * (size_t)i;
+    const float qi[4] = {-q[0], -q[1], -q[2], q[3]};
+    const float *c = s->center + 3 * (size_t)i;
+    const float *sc = s->scale + 3 * (size_t)i;
+    float oc[3], lo[3], ld[3];
+    sub3f(o, c, oc);
+    qrot_f(qi, oc, lo);
+    qrot_f(qi, d, ld);
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = lo[k] / sc[k];
+        ld[k] = ld[k] / sc[k];
+    }
+    const float t = -dot3f(lo, ld) / dot3f(ld, ld);
+    if (t <= 0.0f || t >= t_end) return 0;
+    const float lp[3] = {lo[0] + t * ld[0], lo[1] + t * ld[1], lo[2] + t * ld[2]};
+    const float sq = dot3f(lp, lp);
+    if (sq > s->support_sq[i]) return 0;
+    const float response = fminf(0.999f, s->opacity[i] * bvo_expf(-0.5f * sq));
+    *t_out = t;
+    *alpha_out = 1.0f - bvo_powf(1.0f - response, 1.1f);
+    return 1;
+}
+
+typedef struct {
+    float t;
+    uint32_t index;
+    float alpha;
+} relight_hit;
+
+static int cmp_hit(const void *a, const void *b) {
+    const relight_hit *x = (const relight_hit *)a, *y = (const relight_hit *)b;
+    if (x->t < y->t) return -1;
+    if (x->t > y->t) return 1;
+    return (x->index > y->index) - (x->index < y->index);
+}
+
+/* trace_blended (relight.wgsl:626-744) over every hit in (t, index) order:
+ * the reference's windowed traversal gives the same result for any window
+ * (groups carry across windows; tests/relight_gpu_vs_cpu.rs:543-915). */
+void bvo_relight_ray(const bvo_relight_scene *s, const bvo_point_light *lights,
+                     uint32_t n_lights, const float o[3], const float d[3], float depth,
+                     const float background[3], float rgba[4], uint32_t *hits_out) {
+    relight_hit *hits = NULL;
+    size_t nh = 0, cap = 0;
+    for (uint32_t i = 0; i < s->n; ++i) {
+        float t, a;
+        if (!bvo_intersect_gaussian(s, i, o, d, depth, &t, &a)) continue;
+        if (!(a > 0.0f)) continue;
+        if (nh == cap) {
+            cap = cap ? cap * 2 : 64;
+            hits = (relight_hit *)realloc(hits, cap * sizeof(relight_hit));
+        }
+        hits[nh].t = t;
+        hits[nh].index = i;
+        hits[nh].alpha = a;
+        nh += 1;
+    }
+    qsort(hits, nh, sizeof(relight_hit), cmp_hit);
+    float radiance[3] = {0, 0, 0}, T = 1.0f;
+    int active = 0;
+    float limit = 0.0f, sum_c[3] = {0, 0, 0}, sum_w = 0.0f, group_T = 1.0f;
+    uint32_t used = 0;
+    int stopped = 0;
+    for (size_t k = 0; k < nh; ++k) {
+        const relight_hit *h = &hits[k];
+        if (!active || h->t > limit) {
+            if (active) {
+                const float a_sum = fminf(1.0f, sum_w);
+                const float a_union = 1.0f - group_T;
+                const float alpha = a_union * (1.0f - 0.75f) + a_sum * 0.75f;
+                const float wmax = fmaxf(sum_w, 1.0e-6f);
+                for (int c = 0; c < 3; ++c) radiance[c] += T * (alpha * sum_c[c] / wmax);
+                T *= 1.0f - alpha;
+                active = 0;
+                if (T <= 0.003f) {
+                    stopped = 1;
+                    break;
+                }
+            }
+            active = 1;
+            limit = h->t + 0.5f * s->radius[h->index];
+            sum_c[0] = sum_c[1] = sum_c[2] = 0.0f;
+            sum_w = 0.0f;
+            group_T = 1.0f;
+        }
+        used += 1;
+        const float point[3] = {o[0] + h->t * d[0], o[1] + h->t * d[1], o[2] + h->t * d[2]};
+        const float *nrm = s->normal + 3 * (size_t)h->index;
+        float n[3] = {nrm[0], nrm[1], nrm[2]};
+        if (dot3f(n, d) > 0.0f) {
+            n[0] = -n[0];
+            n[1] = -n[1];
+            n[2] = -n[2];
+        }
+        const float view[3] = {-d[0], -d[1], -d[2]};
+        const bvo_material *mat = &s->materials[s->material[h->index]];
+        float shade[3] = {0, 0, 0};
+        for (uint32_t l = 0; l < n_lights; ++l) {
+            float one[3];
+            bvo_point_light_shade(&lights[l], point, n, view, mat, one);
+            shade[0] += one[0];
+            shade[1] += one[1];
+            shade[2] += one[2];
+        }
+        for (int c = 0; c < 3; ++c) sum_c[c] += h->alpha * shade[c];
+        sum_w += h->alpha;
+        group_T *= 1.0f - h->alpha;
+    }
+    if (active && !stopped) {
+        const float a_sum = fminf(1.0f, sum_w);
+        const float a_union = 1.0f - group_T;
+        const float alpha = a_union * (1.0f - 0.75f) + a_sum * 0.75f;
+        const float wmax = fmaxf(sum_w, 1.0e-6f);
+        for (int c = 0; c < 3; ++c) radiance[c] += T * (alpha * sum_c[c] / wmax);
+        T *= 1.0f - alpha;
+    }
+    free(hits);
+    for (int c = 0; c < 3; ++c) rgba[c] = radiance[c] + T * background[c];
+    rgba[3] = 1.0f - T;
+    if (hits_out) *hits_out = used;
+}
+
+/* trace_main (relight.wgsl:747-780): single normalisation of the ray. */
+static void relight_camera_ray(const bvo_camera *cam, uint32_t width, uint32_t height,
+                               uint32_t x, uint32_t y, float o[3], float d[3]) {
+    bvo_camera_ray(cam, width, height, x, y, o, d);
+}
+
+void bvo_relight_render(const bvo_relight_scene *s, const bvo_point_light *lights,
+                        uint32_t n_lights, const bvo_camera *cam, uint32_t width,
+                        uint32_t height, const float background[3], float *out_rgba,
+                        uint32_t *out_hits, int threads) {
+    const long total = (long)width * (long)height;
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threads)
+#endif
+    for (long i = 0; i < total; ++i) {
+        float o[3], d[3];
+        relight_camera_ray(cam, width, height, (uint32_t)(i % width), (uint32_t)(i / width), o, d);
+        bvo_relight_ray(s, lights, n_lights, o, d, cam->depth, background,
+                        out_rgba + 4 * (size_t)i, out_hits ? out_hits + i : NULL);
+    }
+    (void)threads;
+}

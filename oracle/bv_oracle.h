@@ -170,6 +170,69 @@ double bvo_forward_backward(const bvo_model *m, const bvo_camera *cams, uint32_t
                             double *out_rgb, float *out_rgb32, double *d_density, double *d_sh,
                             double *d_pos, double *d_radius, int threads);
 
+/* ---- relightable Gaussians with finite point lights ----
+ * blade-volume/shaders/relight.wgsl (kernel 2 = learned volumetric
+ * Gaussian, point light enabled, diffuse_samples = 0) and
+ * blade-volume/src/relight.rs.  Material / PointLight are the reference's
+ * #[repr(C)] layouts (relight.rs:77-86, :176-181). */
+typedef struct {
+    float albedo[3];
+    float roughness;
+    float specular_f0[3];
+    float pad;
+} bvo_material;
+
+typedef struct {
+    float position[3];
+    float direction[3];
+    float intensity[3];
+    float exponent;
+} bvo_point_light;
+
+/* Prepared particles (gpu/relight.rs:178-253): opacity > 0.03 only,
+ * index = position in this filtered list. */
+typedef struct {
+    uint32_t n;
+    const float *center;     /* [n*3] */
+    const float *rotation;   /* [n*4] x, y, z, w */
+    const float *scale;      /* [n*3] */
+    const float *opacity;    /* [n] */
+    const float *normal;     /* [n*3] */
+    const float *radius;     /* [n] 3 * cbrt(sx sy sz) */
+    const float *support_sq; /* [n] 2 * ln(opacity / 0.03) */
+    const uint32_t *material;
+    const bvo_material *materials;
+} bvo_relight_scene;
+
+float bvo_logf(float x);
+float bvo_powf(float x, float y);
+/* Fills the prepared arrays from a Gaussian PointCloudModel; returns the
+ * number kept.  Output arrays must hold n entries. */
+uint32_t bvo_relight_prepare(uint32_t n, const float *points, const float *rotations,
+                             const float *scales, const float *normals,
+                             const uint32_t *material_indices, uint32_t *kept_index,
+                             float *center, float *rotation, float *scale, float *opacity,
+                             float *normal, float *radius, float *support_sq,
+                             uint32_t *material);
+void bvo_point_light_shade(const bvo_point_light *light, const float position[3],
+                           const float normal[3], const float view[3], const bvo_material *m,
+                           float out[3]);
+/* relight.rs shade_point_light (:295-323), CPU twin of the shader's. */
+void bvo_shade_point_light_cpu(const bvo_point_light *light, const float point[3],
+                               const float normal[3], const float view[3],
+                               const bvo_material *m, float out[3]);
+int bvo_intersect_gaussian(const bvo_relight_scene *s, uint32_t i, const float o[3],
+                           const float d[3], float t_end, float *t, float *alpha);
+/* One camera ray of trace_main + trace_blended: rgba = (radiance +
+ * T * background, 1 - T); lights are summed (alpha is light-independent). */
+void bvo_relight_ray(const bvo_relight_scene *s, const bvo_point_light *lights,
+                     uint32_t n_lights, const float o[3], const float d[3], float depth,
+                     const float background[3], float rgba[4], uint32_t *hits);
+void bvo_relight_render(const bvo_relight_scene *s, const bvo_point_light *lights,
+                        uint32_t n_lights, const bvo_camera *cam, uint32_t width,
+                        uint32_t height, const float background[3], float *out_rgba,
+                        uint32_t *out_hits, int threads);
+
 #ifdef __cplusplus
 }
 #endif

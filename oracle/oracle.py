@@ -52,6 +52,22 @@ class PathEntry(C.Structure):
                 ("surface_query_d_current", C.c_float * 4), ("t_start", C.c_float)]
 
 
+class Material(C.Structure):
+    _fields_ = [("albedo", C.c_float * 3), ("roughness", C.c_float),
+                ("specular_f0", C.c_float * 3), ("pad", C.c_float)]
+
+
+class PointLight(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("direction", C.c_float * 3),
+                ("intensity", C.c_float * 3), ("exponent", C.c_float)]
+
+
+class RelightScene(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("center", f32p), ("rotation", f32p), ("scale", f32p),
+                ("opacity", f32p), ("normal", f32p), ("radius", f32p), ("support_sq", f32p),
+                ("material", u32p), ("materials", C.POINTER(Material))]
+
+
 class ParamsF64(C.Structure):
     _fields_ = [("points", f64p), ("sh", f64p), ("radii", f64p)]
 
@@ -103,6 +119,25 @@ def lib():
                                            C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
                                            C.c_float, f32p, C.c_int, C.POINTER(ParamsF64), f64p,
                                            f32p, f64p, f64p, f64p, f64p, C.c_int]
+        L.bvo_logf.restype = C.c_float
+        L.bvo_logf.argtypes = [C.c_float]
+        L.bvo_powf.restype = C.c_float
+        L.bvo_powf.argtypes = [C.c_float, C.c_float]
+        L.bvo_relight_prepare.restype = C.c_uint32
+        L.bvo_relight_prepare.argtypes = [C.c_uint32, f32p, f32p, f32p, f32p, u32p, u32p, f32p,
+                                          f32p, f32p, f32p, f32p, f32p, f32p, u32p]
+        L.bvo_point_light_shade.argtypes = [C.POINTER(PointLight), f32p, f32p, f32p,
+                                            C.POINTER(Material), f32p]
+        L.bvo_shade_point_light_cpu.argtypes = [C.POINTER(PointLight), f32p, f32p, f32p,
+                                                C.POINTER(Material), f32p]
+        L.bvo_intersect_gaussian.restype = C.c_int
+        L.bvo_intersect_gaussian.argtypes = [C.POINTER(RelightScene), C.c_uint32, f32p, f32p,
+                                             C.c_float, f32p, f32p]
+        L.bvo_relight_ray.argtypes = [C.POINTER(RelightScene), C.POINTER(PointLight), C.c_uint32,
+                                      f32p, f32p, C.c_float, f32p, f32p, u32p]
+        L.bvo_relight_render.argtypes = [C.POINTER(RelightScene), C.POINTER(PointLight),
+                                         C.c_uint32, C.POINTER(Camera), C.c_uint32, C.c_uint32,
+                                         f32p, f32p, u32p, C.c_int]
         _lib = L
     return _lib
 
@@ -324,3 +359,113 @@ def forward_backward(model: OracleModel, cams: Sequence, width, height, max_step
     del keep
     return dict(loss=loss, rgb=rgb, rgb32=rgb32, d_density=dd, d_sh=dsh,
                 d_pos=None if dpos is None else dpos.reshape(n, 3), d_radius=drad)
+
+
+# --------------------------------------------------------------------------
+# relight
+# --------------------------------------------------------------------------
+def logf(x: float) -> float:
+    return float(lib().bvo_logf(float(x)))
+
+
+def powf(x: float, y: float) -> float:
+    return float(lib().bvo_powf(float(x), float(y)))
+
+
+def material_struct(albedo, roughness, f0):
+    m = Material()
+    m.albedo[:] = [float(v) for v in albedo]
+    m.roughness = float(roughness)
+    m.specular_f0[:] = [float(v) for v in f0]
+    m.pad = 0.0
+    return m
+
+
+def light_struct(position, direction, intensity, exponent):
+    L = PointLight()
+    L.position[:] = [float(v) for v in position]
+    L.direction[:] = [float(v) for v in direction]
+    L.intensity[:] = [float(v) for v in intensity]
+    L.exponent = float(exponent)
+    return L
+
+
+def point_light_shade(light, position, normal, view, material, cpu=False):
+    out = np.zeros(3, np.float32)
+    args = [np.ascontiguousarray(a, np.float32) for a in (position, normal, view)]
+    fn = lib().bvo_shade_point_light_cpu if cpu else lib().bvo_point_light_shade
+    fn(C.byref(light), *[_ptr(a, f32p) for a in args], C.byref(material), _ptr(out, f32p))
+    return out
+
+
+class RelightOracleScene:
+    """Prepared relightable Gaussians (gpu/relight.rs:178-253) for the C side."""
+
+    def __init__(self, points, rotations, scales, normals, material_indices, materials):
+        points = np.ascontiguousarray(points, np.float32).reshape(-1, 4)
+        n = len(points)
+        self.kept = np.zeros(n, np.uint32)
+        self.center = np.zeros((n, 3), np.float32)
+        self.rotation = np.zeros((n, 4), np.float32)
+        self.scale = np.zeros((n, 3), np.float32)
+        self.opacity = np.zeros(n, np.float32)
+        self.normal = np.zeros((n, 3), np.float32)
+        self.radius = np.zeros(n, np.float32)
+        self.support_sq = np.zeros(n, np.float32)
+        self.material = np.zeros(n, np.uint32)
+        rot = np.ascontiguousarray(rotations, np.float32).reshape(-1, 4)
+        sc = np.ascontiguousarray(scales, np.float32).reshape(-1, 3)
+        nr = np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+        mi = np.ascontiguousarray(material_indices, np.uint32)
+        k = lib().bvo_relight_prepare(n, _ptr(points, f32p), _ptr(rot, f32p), _ptr(sc, f32p),
+                                      _ptr(nr, f32p), _ptr(mi, u32p), _ptr(self.kept, u32p),
+                                      _ptr(self.center, f32p), _ptr(self.rotation, f32p),
+                                      _ptr(self.scale, f32p), _ptr(self.opacity, f32p),
+                                      _ptr(self.normal, f32p), _ptr(self.radius, f32p),
+                                      _ptr(self.support_sq, f32p), _ptr(self.material, u32p))
+        self.n = int(k)
+        mats = np.ascontiguousarray(materials, np.float32).reshape(-1, 8)
+        self.materials = (Material * len(mats))()
+        for i, row in enumerate(mats):
+            self.materials[i] = material_struct(row[0:3], row[3], row[4:7])
+        self.c = RelightScene(self.n, _ptr(self.center, f32p), _ptr(self.rotation, f32p),
+                              _ptr(self.scale, f32p), _ptr(self.opacity, f32p),
+                              _ptr(self.normal, f32p), _ptr(self.radius, f32p),
+                              _ptr(self.support_sq, f32p), _ptr(self.material, u32p),
+                              self.materials)
+
+    @classmethod
+    def from_scene(cls, g):
+        return cls(g.points, g.rotations, g.scales, g.normals, g.material_indices, g.materials)
+
+
+def _lights(lights):
+    arr = (PointLight * len(lights))()
+    for i, L in enumerate(lights):
+        arr[i] = L if isinstance(L, PointLight) else light_struct(*L)
+    return arr
+
+
+def relight_ray(scene: RelightOracleScene, lights, origin, direction, depth,
+                background=(0.0, 0.0, 0.0)):
+    out = np.zeros(4, np.float32)
+    hits = np.zeros(1, np.uint32)
+    o = np.ascontiguousarray(origin, np.float32)
+    d = np.ascontiguousarray(direction, np.float32)
+    bg = np.ascontiguousarray(background, np.float32)
+    arr = _lights(lights)
+    lib().bvo_relight_ray(C.byref(scene.c), arr, len(arr), _ptr(o, f32p), _ptr(d, f32p),
+                          float(depth), _ptr(bg, f32p), _ptr(out, f32p), _ptr(hits, u32p))
+    return out, int(hits[0])
+
+
+def relight_render(scene: RelightOracleScene, lights, cam, width, height,
+                   background=(0.0, 0.0, 0.0), threads=0):
+    out = np.zeros((height, width, 4), np.float32)
+    hits = np.zeros((height, width), np.uint32)
+    bg = np.ascontiguousarray(background, np.float32)
+    arr = _lights(lights)
+    cs = camera_struct(cam)
+    lib().bvo_relight_render(C.byref(scene.c), arr, len(arr), C.byref(cs), width, height,
+                             _ptr(bg, f32p), _ptr(out, f32p), _ptr(hits, u32p), threads)
+    return out, hits
