@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=192,
                     help="side of the CPU-baseline sample image (view 0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="train", choices=["train", "relight", "render"],
+                    help="train: the headline fwd+bwd line; relight / render: secondary "
+                         "lines for the Gaussian relight and forward-render paths")
     return ap.parse_args()
 
 
@@ -185,10 +188,106 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def timed_events(fn, steps, flush, stream):
+    import torch
+
+    out = []
+    for _ in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def run_secondary(args):
+    """Relight (1M Gaussians, 1024x768, 16 lights) or forward render
+    (16,384-site ball, 128^2 and the 262,144-site scene at 8 x 512^2)."""
+    import torch
+
+    import blade_volume_b200 as bv
+    from blade_volume_b200 import scenes
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    sampler = ClockSampler(0)
+    if args.workload == "relight":
+        g, cam, lights = scenes.relight_workload()
+        W, H = 1024, 768
+        tr = bv.RelightTracer(g)
+        tr.set_point_lights(lights)
+        out = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+        for _ in range(max(args.warmup, 3)):
+            tr.dispatch(out, cam, (W, H))
+        tr.enable_stats(True)
+        tr.dispatch(out, cam, (W, H))
+        st = tr.last_stats()
+        tr.enable_stats(False)
+        sampler.start()
+        ts = timed_events(lambda: tr.dispatch(out, cam, (W, H)), args.steps, flush, stream)
+        clocks = sampler.stop()
+        ms = statistics.median(ts)
+        hits = st.steps
+        # 96 B per composited hit (particle 80 B + material 32 B read once,
+        # counted as the reference's 96 B) + 16 B per ray out
+        alg = hits * 96 + W * H * 16
+        peak, kind = peaks()
+        line = {"metric": "relight Mrays/s", "value": W * H / (ms * 1e-3) / 1e6, "unit": "Mrays/s",
+                "ms_per_step": ms, "steps": args.steps, "warmup": max(args.warmup, 3),
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "gaussian relight", "gaussians": g.n,
+                           "kept": tr.num_particles, "width": W, "height": H,
+                           "lights": len(lights), "window": 16},
+                "hits_per_ray": hits / (W * H), "nodes_per_ray": st.faces / (W * H),
+                "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak,
+                             "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
+                             "traffic": None, "peak_source": kind},
+                "gpu_launches": args.steps, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+        return
+    w = scenes.radfoam_tiny()
+    t = bv.RadFoamGpuTracer(w.model, max_steps=w.max_steps, weight_threshold=w.weight_threshold)
+    out = torch.empty((1, w.height, w.width, 4), dtype=torch.float32, device="cuda")
+    for _ in range(max(args.warmup, 3)):
+        t.dispatch_batch(out, w.cameras, (w.width, w.height))
+    t.enable_stats(True)
+    t.dispatch_batch(out, w.cameras, (w.width, w.height))
+    st = t.last_stats()
+    t.enable_stats(False)
+    sampler.start()
+    ts = timed_events(lambda: t.dispatch_batch(out, w.cameras, (w.width, w.height)), args.steps,
+                      flush, stream)
+    clocks = sampler.stop()
+    ms = statistics.median(ts)
+    deg = st.faces / max(st.steps, 1)
+    b_step = 8 + deg * 20 + 4 * (3 * 1 + 1)
+    alg = st.steps * b_step + w.width * w.height * 16
+    peak, kind = peaks()
+    line = {"metric": "forward Mrays/s", "value": w.width * w.height / (ms * 1e-3) / 1e6,
+            "unit": "Mrays/s", "ms_per_step": ms, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "radfoam_tiny forward", "sites": w.model.n, "width": w.width,
+                       "height": w.height, "steps_per_ray": st.steps / (w.width * w.height),
+                       "faces_per_step": deg},
+            "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
+                         "traffic": None, "peak_source": kind},
+            "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload != "train":
+        run_secondary(args)
         return
     import torch
 

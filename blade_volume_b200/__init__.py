@@ -45,6 +45,10 @@ EXPORTED_SYMBOLS = [
     "bv_radfoam_tracer_start_point", "bv_radfoam_tracer_num_points", "bv_containing_point",
     "bv_record_paths", "bv_forward_backward", "bv_radfoam_tracer_enable_stats",
     "bv_radfoam_tracer_last_stats", "bv_containing_points_noalloc",
+    "bv_relight_tracer_new_gaussian", "bv_relight_tracer_destroy",
+    "bv_relight_tracer_set_point_lights", "bv_relight_tracer_set_background",
+    "bv_relight_tracer_dispatch", "bv_relight_tracer_num_particles",
+    "bv_relight_tracer_enable_stats", "bv_relight_tracer_last_stats",
 ]
 
 
@@ -98,6 +102,27 @@ class LaunchStats(C.Structure):
                 ("reserved", C.c_uint32)]
 
 
+class MaterialC(C.Structure):
+    _fields_ = [("albedo", C.c_float * 3), ("roughness", C.c_float),
+                ("specular_f0", C.c_float * 3), ("pad", C.c_float)]
+
+
+class PointLightC(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("direction", C.c_float * 3),
+                ("intensity", C.c_float * 3), ("exponent", C.c_float)]
+
+
+class GaussianDesc(C.Structure):
+    _fields_ = [("num_points", C.c_uint32), ("num_materials", C.c_uint32),
+                ("points", C.POINTER(C.c_float)), ("rotations", C.POINTER(C.c_float)),
+                ("scales", C.POINTER(C.c_float)), ("normals", C.POINTER(C.c_float)),
+                ("material_indices", C.POINTER(C.c_uint32)), ("materials", C.c_void_p)]
+
+
+class RelightSettings(C.Structure):
+    _fields_ = [("background", C.c_float * 3), ("diffuse_samples", C.c_uint32)]
+
+
 _lib = None
 
 
@@ -144,6 +169,19 @@ def load_library(path: str = LIB_PATH):
     L.bv_radfoam_tracer_last_stats.argtypes = [C.c_void_p, C.POINTER(LaunchStats)]
     L.bv_containing_points_noalloc.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_float),
                                                C.c_uint32, C.c_void_p, C.c_void_p]
+    L.bv_relight_tracer_new_gaussian.argtypes = [C.POINTER(GaussianDesc),
+                                                 C.POINTER(RelightSettings), C.POINTER(C.c_void_p)]
+    L.bv_relight_tracer_destroy.argtypes = [C.c_void_p]
+    L.bv_relight_tracer_destroy.restype = None
+    L.bv_relight_tracer_set_point_lights.argtypes = [C.c_void_p, C.POINTER(PointLightC),
+                                                     C.c_uint32]
+    L.bv_relight_tracer_set_background.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
+    L.bv_relight_tracer_dispatch.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(CameraC),
+                                             C.c_uint32, C.c_uint32, C.c_void_p]
+    L.bv_relight_tracer_num_particles.argtypes = [C.c_void_p]
+    L.bv_relight_tracer_num_particles.restype = C.c_uint32
+    L.bv_relight_tracer_enable_stats.argtypes = [C.c_void_p, C.c_uint32]
+    L.bv_relight_tracer_last_stats.argtypes = [C.c_void_p, C.POINTER(LaunchStats)]
     _lib = L
     return L
 
@@ -371,4 +409,79 @@ class RadFoamGpuTracer:
     def last_stats(self) -> LaunchStats:
         s = LaunchStats()
         _check(load_library().bv_radfoam_tracer_last_stats(self._h, C.byref(s)))
+        return s
+
+
+class RelightTracer:
+    """RelightTracer::new_gaussian / set_point_light / dispatch
+    (gpu/relight.rs:313, :841, :905) over the C ABI."""
+
+    def __init__(self, model, background=(0.0, 0.0, 0.0)):
+        L = load_library()
+        self.points = np.ascontiguousarray(model.points, np.float32)
+        self.rotations = np.ascontiguousarray(model.rotations, np.float32)
+        self.scales = np.ascontiguousarray(model.scales, np.float32)
+        self.normals = np.ascontiguousarray(model.normals, np.float32)
+        self.material_indices = np.ascontiguousarray(model.material_indices, np.uint32)
+        self.materials = np.ascontiguousarray(model.materials, np.float32).reshape(-1, 8)
+        d = GaussianDesc(len(self.points), len(self.materials), _fptr(self.points),
+                         _fptr(self.rotations), _fptr(self.scales), _fptr(self.normals),
+                         _uptr(self.material_indices), self.materials.ctypes.data)
+        st = RelightSettings()
+        st.background[:] = [float(v) for v in background]
+        st.diffuse_samples = 0
+        h = C.c_void_p()
+        _check(L.bv_relight_tracer_new_gaussian(C.byref(d), C.byref(st), C.byref(h)))
+        self._h = h
+
+    def deinit(self):
+        if getattr(self, "_h", None):
+            load_library().bv_relight_tracer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.deinit()
+        except Exception:
+            pass
+
+    @property
+    def num_particles(self) -> int:
+        return load_library().bv_relight_tracer_num_particles(self._h)
+
+    def set_point_lights(self, lights):
+        arr = (PointLightC * len(lights))()
+        for i, (pos, direction, intensity, exponent) in enumerate(lights):
+            arr[i].position[:] = [float(v) for v in pos]
+            arr[i].direction[:] = [float(v) for v in direction]
+            arr[i].intensity[:] = [float(v) for v in intensity]
+            arr[i].exponent = float(exponent)
+        _check(load_library().bv_relight_tracer_set_point_lights(self._h, arr, len(lights)))
+
+    def set_point_light(self, light):
+        self.set_point_lights([light])
+
+    def set_background(self, rgb):
+        a = np.ascontiguousarray(rgb, np.float32)
+        _check(load_library().bv_relight_tracer_set_background(self._h, _fptr(a)))
+
+    def dispatch(self, output, camera: Camera, size, stream=None):
+        w, h = size
+        cam = camera_c(camera)
+        _check(load_library().bv_relight_tracer_dispatch(
+            self._h, C.c_void_p(output.data_ptr()), C.byref(cam), w, h, _stream_handle(stream)))
+
+    def render(self, camera: Camera, width: int, height: int):
+        import torch
+
+        out = torch.empty((height, width, 4), dtype=torch.float32, device="cuda")
+        self.dispatch(out, camera, (width, height))
+        return out
+
+    def enable_stats(self, enabled: bool = True):
+        _check(load_library().bv_relight_tracer_enable_stats(self._h, int(enabled)))
+
+    def last_stats(self) -> LaunchStats:
+        s = LaunchStats()
+        _check(load_library().bv_relight_tracer_last_stats(self._h, C.byref(s)))
         return s

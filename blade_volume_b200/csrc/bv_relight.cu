@@ -1,0 +1,411 @@
+// Relightable Gaussians with finite point lights on sm_100a: per-ray gather
+// of every particle whose support ellipsoid the ray crosses, strict
+// (depth, index) order, surface-band grouping and GGX point-light shading.
+//
+// Restates blade-volume/shaders/relight.wgsl (kernel 2 = learned volumetric
+// Gaussian, point light, no visibility ray): intersect_surfel :419-441,
+// point_light_shade :190-261, surface_group_response :606-624,
+// trace_blended :626-744, trace_main :747-780.  The reference enumerates
+// candidates with hardware ray queries over icosahedron proxies; here a BVH
+// over the support ellipsoids' boxes is traversed front to back in windows
+// of kWindow hits: a pass keeps the kWindow smallest (t, index) keys above
+// the cursor, pruning boxes that end before the cursor or start after the
+// window's last key, so every pass touches only a thin slab of the tree.
+// The result does not depend on the window size (groups carry across
+// windows), which is what the reference's own tests establish.
+//
+// Compiled with -fmad=false: the arithmetic is the CPU oracle's, operation
+// for operation, so images are bit-identical.
+
+#include "bv_relight.h"
+
+namespace bv {
+namespace {
+
+constexpr int kRelightBlock = 128;
+constexpr int kWindow = 16;
+constexpr int kStack = 64;
+
+__device__ __forceinline__ float r_expf(float x) {
+    if (x != x) return x;
+    if (x > 88.72283935546875f) return __int_as_float(0x7f800000);
+    if (x < -103.972084045410156f) return 0.0f;
+    const float k = rintf(x * 1.44269502162933349609375f);
+    float r = __fmaf_rn(k, -0.693115234375f, x);
+    r = __fmaf_rn(k, -3.19461832987144589424133e-05f, r);
+    float p = 1.98412701138295233249664e-04f;
+    p = __fmaf_rn(p, r, 1.38888892251998186111450e-03f);
+    p = __fmaf_rn(p, r, 8.33333376795053482055664e-03f);
+    p = __fmaf_rn(p, r, 4.16666679084300994873047e-02f);
+    p = __fmaf_rn(p, r, 1.66666671633720397949219e-01f);
+    p = __fmaf_rn(p, r, 0.5f);
+    p = __fmaf_rn(p, r, 1.0f);
+    p = __fmaf_rn(p, r, 1.0f);
+    int ki = (int)k;
+    if (ki > 127) {
+        p = p * 2.0f;
+        ki -= 1;
+    }
+    if (ki < -126) {
+        p = p * __int_as_float((ki + 64 + 127) << 23);
+        return p * 5.42101086242752217004e-20f;
+    }
+    return p * __int_as_float((ki + 127) << 23);
+}
+
+// log(x): x = m 2^e, m in [sqrt(1/2), sqrt(2)), log(1+f) = 2 atanh(f/(2+f))
+// arranged as f - (f^2/2 - s (f^2/2 + R)); same sequence as the oracle.
+__device__ __forceinline__ float r_logf(float x) {
+    if (x != x || x < 0.0f) return __int_as_float(0x7fc00000);
+    if (x == 0.0f) return __int_as_float(0xff800000);
+    if (x == __int_as_float(0x7f800000)) return x;
+    uint32_t u = __float_as_uint(x);
+    int e = 0;
+    if (u < 0x00800000u) {
+        u = __float_as_uint(x * 16777216.0f);
+        e = -24;
+    }
+    e += (int)((u >> 23) & 0xffu) - 127;
+    float m = __uint_as_float((u & 0x007fffffu) | 0x3f800000u);
+    if (m > 1.41421353816986083984375f) {
+        m = m * 0.5f;
+        e += 1;
+    }
+    const float f = m - 1.0f;
+    const float s = f / (2.0f + f);
+    const float z = s * s;
+    float p = 0.1538461595773697f;
+    p = __fmaf_rn(p, z, 0.1818181872367859f);
+    p = __fmaf_rn(p, z, 0.2222222238779068f);
+    p = __fmaf_rn(p, z, 0.2857142984867096f);
+    p = __fmaf_rn(p, z, 0.4000000059604645f);
+    p = __fmaf_rn(p, z, 0.6666666865348816f);
+    const float R = z * p;
+    const float hfsq = 0.5f * f * f;
+    const float ef = (float)e;
+    return ef * 0.693115234375f -
+           ((hfsq - (s * (hfsq + R) + ef * 3.19461832987144589424133e-05f)) - f);
+}
+
+__device__ __forceinline__ float r_powf(float x, float y) {
+    if (x == 0.0f) return y > 0.0f ? 0.0f : (y == 0.0f ? 1.0f : __int_as_float(0x7f800000));
+    return r_expf(y * r_logf(x));
+}
+
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+    return ax * bx + ay * by + az * bz;
+}
+
+// qrot (common.wgsl:386-390)
+__device__ __forceinline__ float3 qrot(float4 q, float vx, float vy, float vz) {
+    const float t0 = 2.0f * (q.y * vz - q.z * vy);
+    const float t1 = 2.0f * (q.z * vx - q.x * vz);
+    const float t2 = 2.0f * (q.x * vy - q.y * vx);
+    return make_float3((vx + q.w * t0) + (q.y * t2 - q.z * t1),
+                       (vy + q.w * t1) + (q.z * t0 - q.x * t2),
+                       (vz + q.w * t2) + (q.x * t1 - q.y * t0));
+}
+
+struct RRay {
+    float ox, oy, oz, dx, dy, dz;
+};
+
+// intersect_surfel, kernel 2 (relight.wgsl:419-441).
+__device__ __forceinline__ bool intersect(const GaussPrim *__restrict__ prims, uint32_t pos,
+                                          const RRay &r, float t_end, float &t_out,
+                                          float &alpha_out) {
+    const float4 co = __ldg(&prims[pos].center_opacity);
+    const float4 qi = __ldg(&prims[pos].qinv);
+    const float4 ss = __ldg(&prims[pos].scale_support);
+    const float3 lo0 = qrot(qi, r.ox - co.x, r.oy - co.y, r.oz - co.z);
+    const float3 ld0 = qrot(qi, r.dx, r.dy, r.dz);
+    const float lox = lo0.x / ss.x, loy = lo0.y / ss.y, loz = lo0.z / ss.z;
+    const float ldx = ld0.x / ss.x, ldy = ld0.y / ss.y, ldz = ld0.z / ss.z;
+    const float t = -dot3(lox, loy, loz, ldx, ldy, ldz) / dot3(ldx, ldy, ldz, ldx, ldy, ldz);
+    if (t <= 0.0f || t >= t_end) return false;
+    const float px = lox + t * ldx, py = loy + t * ldy, pz = loz + t * ldz;
+    const float sq = dot3(px, py, pz, px, py, pz);
+    if (sq > ss.w) return false;
+    const float response = fminf(0.999f, co.w * r_expf(-0.5f * sq));
+    t_out = t;
+    alpha_out = 1.0f - r_powf(1.0f - response, 1.1f);
+    return true;
+}
+
+// point_light_shade (relight.wgsl:190-261), diffuse_samples = 0; result is
+// added to acc.
+__device__ __forceinline__ void shade_light(const RelightLight &L, float px, float py, float pz,
+                                            float nx, float ny, float nz, float vx, float vy,
+                                            float vz, const float4 &m0, const float4 &m1,
+                                            float &ar, float &ag, float &ab) {
+    const float flx = px - L.position[0], fly = py - L.position[1], flz = pz - L.position[2];
+    const float d2 = dot3(flx, fly, flz, flx, fly, flz);
+    if (d2 <= 1.1920929e-7f) return;
+    const float inv = 1.0f / sqrtf(d2);
+    const float awx = flx * inv, awy = fly * inv, awz = flz * inv;
+    float angular = 1.0f;
+    if (L.exponent != 0.0f)
+        angular = r_powf(fmaxf(dot3(L.direction[0], L.direction[1], L.direction[2], awx, awy, awz),
+                               0.0f),
+                         L.exponent);
+    const float tx = -awx, ty = -awy, tz = -awz;
+    const float ndl = fmaxf(dot3(nx, ny, nz, tx, ty, tz), 0.0f);
+    if (ndl == 0.0f) return;
+    const float a_d2 = angular / d2;
+    const float rr = L.intensity[0] * a_d2, rg = L.intensity[1] * a_d2, rb = L.intensity[2] * a_d2;
+    float outr = m0.x * rr * ndl, outg = m0.y * rg * ndl, outb = m0.z * rb * ndl;
+    if (!(m1.x == 0.0f && m1.y == 0.0f && m1.z == 0.0f)) {
+        const float ndv = fmaxf(dot3(nx, ny, nz, vx, vy, vz), 0.0f);
+        const float hx = tx + vx, hy = ty + vy, hz = tz + vz;
+        const float hs2 = dot3(hx, hy, hz, hx, hy, hz);
+        if (!(ndv == 0.0f || hs2 <= 1.1920929e-7f)) {
+            const float hinv = 1.0f / sqrtf(hs2);
+            const float ux = hx * hinv, uy = hy * hinv, uz = hz * hinv;
+            const float ndh = fmaxf(dot3(nx, ny, nz, ux, uy, uz), 0.0f);
+            const float vdh = fminf(fmaxf(dot3(vx, vy, vz, ux, uy, uz), 0.0f), 1.0f);
+            const float rc = fminf(fmaxf(m0.w, 0.045f), 1.0f);
+            const float alpha = rc * rc;
+            const float a2 = alpha * alpha;
+            const float den = ndh * ndh * (a2 - 1.0f) + 1.0f;
+            const float pi = 3.14159265f;
+            const float dist = a2 / fmaxf(pi * den * den, 1.1754944e-38f);
+            const float sl = 2.0f * ndl / (ndl + sqrtf(a2 + (1.0f - a2) * ndl * ndl));
+            const float sv = 2.0f * ndv / (ndv + sqrtf(a2 + (1.0f - a2) * ndv * ndv));
+            const float g1 = 1.0f - vdh;
+            const float g2 = g1 * g1;
+            const float grazing = (g2 * g2) * g1;
+            const float scale = pi * dist * sl * sv / (4.0f * ndv);
+            outr += rr * scale * (m1.x + (1.0f - m1.x) * grazing);
+            outg += rg * scale * (m1.y + (1.0f - m1.y) * grazing);
+            outb += rb * scale * (m1.z + (1.0f - m1.z) * grazing);
+        }
+    }
+    ar += outr;
+    ag += outg;
+    ab += outb;
+}
+
+struct Key {
+    float t;
+    uint32_t idx;  // filtered particle index (the reference's instance index)
+    uint32_t pos;  // position in the BVH-ordered particle table
+};
+
+__device__ __forceinline__ bool key_less(float ta, uint32_t ia, float tb, uint32_t ib) {
+    return ta < tb || (ta == tb && ia < ib);
+}
+
+// Slab test of a box against the ray, conservative by a small margin.
+__device__ __forceinline__ bool slab(const float4 &lo, const float4 &hi, const RRay &r, float ix,
+                                     float iy, float iz, float t_end, float &tn, float &tf) {
+    const float ax = (lo.x - r.ox) * ix, bx = (hi.x - r.ox) * ix;
+    const float ay = (lo.y - r.oy) * iy, by = (hi.y - r.oy) * iy;
+    const float az = (lo.z - r.oz) * iz, bz = (hi.z - r.oz) * iz;
+    tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
+    tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), t_end));
+    tn = tn - (1e-5f * fabsf(tn) + 1e-6f);
+    tf = tf + (1e-5f * fabsf(tf) + 1e-6f);
+    return tn <= tf;
+}
+
+__global__ void __launch_bounds__(kRelightBlock)
+relight_kernel(const __grid_constant__ RelightParams P) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= P.total_work) return;
+    const uint32_t tile = w / 32u, in = w % 32u;
+    const uint32_t x = (tile % P.tiles_x) * 8u + in % 8u;
+    const uint32_t y = (tile / P.tiles_x) * 4u + in / 8u;
+    if (x >= P.width || y >= P.height) return;
+
+    // trace_main ray mapping (relight.wgsl:760-766): one normalisation
+    RRay ray;
+    {
+        const float px = ((float)x + 0.5f) / (float)P.width;
+        const float py = ((float)y + 0.5f) / (float)P.height;
+        const float vx = (px * 2.0f - 1.0f - P.principal[0]) * P.tan_half[0];
+        const float vy = (py * 2.0f - 1.0f - P.principal[1]) * P.tan_half[1];
+        const float4 q = make_float4(P.q[0], P.q[1], P.q[2], P.q[3]);
+        const float3 rv = qrot(q, vx, vy, 1.0f);
+        const float len = sqrtf(dot3(rv.x, rv.y, rv.z, rv.x, rv.y, rv.z));
+        const float inv = 1.0f / len;
+        ray.dx = rv.x * inv;
+        ray.dy = rv.y * inv;
+        ray.dz = rv.z * inv;
+        ray.ox = P.origin[0];
+        ray.oy = P.origin[1];
+        ray.oz = P.origin[2];
+    }
+    const float ix = 1.0f / ray.dx, iy = 1.0f / ray.dy, iz = 1.0f / ray.dz;
+    const float t_end = P.depth;
+
+    float rad_r = 0.f, rad_g = 0.f, rad_b = 0.f, T = 1.0f;
+    bool group = false, stopped = false;
+    float limit = 0.f, sc_r = 0.f, sc_g = 0.f, sc_b = 0.f, sum_w = 0.f, group_T = 1.f;
+    bool cursor_valid = false;
+    float cur_t = 0.f;
+    uint32_t cur_idx = 0;
+    uint32_t hits_used = 0, nodes_visited = 0;
+
+    for (;;) {
+        // ---- gather the next window of keys above the cursor
+        Key buf[kWindow];
+        int count = 0;
+        uint32_t stack[kStack];
+        int sp = 0;
+        stack[sp++] = 0u;
+        while (sp > 0) {
+            const uint32_t ni = stack[--sp];
+            const BvhNode nd = P.nodes[ni];
+            nodes_visited += 1;
+            float tn[2], tf[2];
+            bool ok[2];
+            const float4 lo[2] = {nd.l_lo, nd.r_lo}, hi[2] = {nd.l_hi, nd.r_hi};
+            const uint32_t cnts[2] = {__float_as_uint(nd.l_hi.w), __float_as_uint(nd.r_hi.w)};
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                ok[c] = cnts[c] != 0xffffffffu &&
+                        slab(lo[c], hi[c], ray, ix, iy, iz, t_end, tn[c], tf[c]);
+                if (ok[c] && cursor_valid && tf[c] < cur_t) ok[c] = false;
+                if (ok[c] && count == kWindow && tn[c] > buf[kWindow - 1].t) ok[c] = false;
+            }
+            // push the farther child first so the nearer one is visited next
+            const int first = (ok[0] && ok[1] && tn[1] < tn[0]) ? 1 : 0;
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int c = k == 0 ? 1 - first : first;
+                if (!ok[c]) continue;
+                const uint32_t ref = __float_as_uint(c == 0 ? nd.l_lo.w : nd.r_lo.w);
+                const uint32_t cnt = cnts[c];
+                if (cnt == 0u) {
+                    if (sp < kStack) stack[sp++] = ref;
+                    continue;
+                }
+                for (uint32_t p = ref; p < ref + cnt; ++p) {
+                    float t, a;
+                    if (!intersect(P.prims, p, ray, t_end, t, a)) continue;
+                    if (!(a > 0.0f)) continue;
+                    const uint32_t id = __ldg(&P.prims[p].ids.x);
+                    if (cursor_valid && !key_less(cur_t, cur_idx, t, id)) continue;
+                    if (count == kWindow && !key_less(t, id, buf[kWindow - 1].t, buf[kWindow - 1].idx))
+                        continue;
+                    // insertion into the sorted window
+                    Key nk{t, id, p};
+#pragma unroll
+                    for (int i = 0; i < kWindow; ++i) {
+                        if (i < count && key_less(nk.t, nk.idx, buf[i].t, buf[i].idx)) {
+                            const Key tmp = buf[i];
+                            buf[i] = nk;
+                            nk = tmp;
+                        }
+                    }
+#pragma unroll
+                    for (int i = 0; i < kWindow; ++i)
+                        if (i == count) buf[i] = nk;
+                    if (count < kWindow) count += 1;
+                }
+            }
+        }
+        if (count == 0) break;
+        // ---- composite the window in order (trace_blended :693-728)
+#pragma unroll 1
+        for (int i = 0; i < count; ++i) {
+            Key h = buf[0];
+#pragma unroll
+            for (int j = 0; j < kWindow; ++j)
+                if (j == i) h = buf[j];
+            if (!group || h.t > limit) {
+                if (group) {
+                    const float a_sum = fminf(1.0f, sum_w);
+                    const float a_union = 1.0f - group_T;
+                    const float alpha = a_union * (1.0f - 0.75f) + a_sum * 0.75f;
+                    const float wmax = fmaxf(sum_w, 1.0e-6f);
+                    rad_r += T * (alpha * sc_r / wmax);
+                    rad_g += T * (alpha * sc_g / wmax);
+                    rad_b += T * (alpha * sc_b / wmax);
+                    T *= 1.0f - alpha;
+                    group = false;
+                    if (T <= 0.003f) {
+                        stopped = true;
+                        break;
+                    }
+                }
+                group = true;
+                limit = h.t + 0.5f * __ldg(&P.prims[h.pos].normal_radius.w);
+                sc_r = sc_g = sc_b = 0.f;
+                sum_w = 0.f;
+                group_T = 1.f;
+            }
+            float tt, a;
+            intersect(P.prims, h.pos, ray, t_end, tt, a);
+            hits_used += 1;
+            const float ptx = ray.ox + h.t * ray.dx, pty = ray.oy + h.t * ray.dy,
+                        ptz = ray.oz + h.t * ray.dz;
+            const float4 nr = __ldg(&P.prims[h.pos].normal_radius);
+            float nx = nr.x, ny = nr.y, nz = nr.z;
+            if (dot3(nx, ny, nz, ray.dx, ray.dy, ray.dz) > 0.0f) {
+                nx = -nx;
+                ny = -ny;
+                nz = -nz;
+            }
+            const uint32_t mat = __ldg(&P.prims[h.pos].ids.y);
+            const float4 m0 = __ldg(&P.materials[mat].a);
+            const float4 m1 = __ldg(&P.materials[mat].b);
+            float sr = 0.f, sg = 0.f, sb = 0.f;
+            for (uint32_t l = 0; l < P.n_lights; ++l)
+                shade_light(P.lights[l], ptx, pty, ptz, nx, ny, nz, -ray.dx, -ray.dy, -ray.dz, m0,
+                            m1, sr, sg, sb);
+            sc_r += a * sr;
+            sc_g += a * sg;
+            sc_b += a * sb;
+            sum_w += a;
+            group_T *= 1.0f - a;
+        }
+        if (stopped) break;
+        if (count < kWindow) {
+            if (group) {
+                const float a_sum = fminf(1.0f, sum_w);
+                const float a_union = 1.0f - group_T;
+                const float alpha = a_union * (1.0f - 0.75f) + a_sum * 0.75f;
+                const float wmax = fmaxf(sum_w, 1.0e-6f);
+                rad_r += T * (alpha * sc_r / wmax);
+                rad_g += T * (alpha * sc_g / wmax);
+                rad_b += T * (alpha * sc_b / wmax);
+                T *= 1.0f - alpha;
+                group = false;
+            }
+            break;
+        }
+        cursor_valid = true;
+        cur_t = buf[kWindow - 1].t;
+        cur_idx = buf[kWindow - 1].idx;
+    }
+    if (group && !stopped) {
+        const float a_sum = fminf(1.0f, sum_w);
+        const float a_union = 1.0f - group_T;
+        const float alpha = a_union * (1.0f - 0.75f) + a_sum * 0.75f;
+        const float wmax = fmaxf(sum_w, 1.0e-6f);
+        rad_r += T * (alpha * sc_r / wmax);
+        rad_g += T * (alpha * sc_g / wmax);
+        rad_b += T * (alpha * sc_b / wmax);
+        T *= 1.0f - alpha;
+    }
+    const size_t o = (size_t)y * P.width + x;
+    P.out[o] = make_float4(rad_r + T * P.background[0], rad_g + T * P.background[1],
+                           rad_b + T * P.background[2], 1.0f - T);
+    if (P.stats) {
+        atomicAdd(P.stats + 0, 1ull);
+        atomicAdd(P.stats + 1, (unsigned long long)hits_used);
+        atomicAdd(P.stats + 2, (unsigned long long)nodes_visited);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_relight(const RelightParams &p, cudaStream_t s) {
+    const int blocks = (int)((p.total_work + kRelightBlock - 1) / kRelightBlock);
+    if (blocks == 0) return cudaSuccess;
+    relight_kernel<<<blocks, kRelightBlock, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace bv

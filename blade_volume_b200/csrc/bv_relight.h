@@ -1,0 +1,61 @@
+// Device layout and launch descriptor of the relightable-Gaussian tracer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "blade_volume_b200.h"
+
+namespace bv {
+
+// One prepared particle (gpu/relight.rs:178-253), in BVH leaf order, 80 B.
+// The first three vectors are all the candidate test reads.
+struct __align__(16) GaussPrim {
+    float4 center_opacity;  // mean, opacity
+    float4 qinv;            // inverse rotation (-x, -y, -z, w)
+    float4 scale_support;   // scale, support^2 = 2 ln(opacity / 0.03)
+    float4 normal_radius;   // PBR normal, surfel radius 3 cbrt(sx sy sz)
+    uint4 ids;              // filtered index, material, 0, 0
+};
+
+// Two child boxes per node (64 B).  .w of lo = child reference (node index
+// or first particle), .w of hi = particle count (0: internal node,
+// 0xffffffff: no child).
+struct __align__(16) BvhNode {
+    float4 l_lo, l_hi, r_lo, r_hi;
+};
+
+struct RelightLight {  // PointLight (relight.rs:176-181)
+    float position[3];
+    float direction[3];  // unit, used when exponent != 0
+    float intensity[3];
+    float exponent;
+};
+
+struct __align__(16) RelightMaterial {  // Material (relight.rs:77-86)
+    float4 a;  // albedo, roughness
+    float4 b;  // specular_f0, pad
+};
+
+constexpr int kMaxRelightLights = 64;
+
+struct RelightParams {
+    const GaussPrim *prims;
+    const BvhNode *nodes;
+    const RelightMaterial *materials;
+    float4 *out;
+    unsigned long long *stats;  // [3] rays, composited hits, nodes visited (or null)
+    float origin[3];
+    float depth;
+    float q[4];
+    float tan_half[2];
+    float principal[2];
+    uint32_t width, height, tiles_x, total_work;
+    float background[3];
+    uint32_t n_lights;
+    RelightLight lights[kMaxRelightLights];
+};
+
+cudaError_t launch_relight(const RelightParams &p, cudaStream_t s);
+
+}  // namespace bv

@@ -218,6 +218,68 @@ typedef struct bv_launch_stats {
 bv_status bv_radfoam_tracer_enable_stats(bv_tracer *tracer, uint32_t enabled);
 bv_status bv_radfoam_tracer_last_stats(bv_tracer *tracer, bv_launch_stats *out);
 
+/* ---- relightable Gaussians with finite point lights ------------------------
+ * RelightTracer for learned volumetric Gaussians (gpu/relight.rs:313
+ * new_gaussian, :841 set_point_light, :893 set_background, :905 dispatch;
+ * shaders/relight.wgsl kernel 2).  Environment lighting and visibility rays
+ * are not part of this path. */
+typedef struct bv_material {   /* Material (relight.rs:77-86), 32 bytes */
+    float albedo[3];
+    float roughness;           /* GGX, clamped to [0.045, 1] in shading */
+    float specular_f0[3];      /* all zero: diffuse only */
+    float pad;
+} bv_material;
+
+typedef struct bv_point_light { /* PointLight (relight.rs:176-181) */
+    float position[3];
+    float direction[3];         /* brightest axis, used when exponent != 0 */
+    float intensity[3];         /* unit-albedo diffuse response at distance 1 */
+    float exponent;             /* 0: isotropic */
+} bv_point_light;
+
+/* Gaussian PointCloudModel with Transforms + PbrAttributes (lib.rs:174-239). */
+typedef struct bv_gaussian_desc {
+    uint32_t num_points;
+    uint32_t num_materials;
+    const float *points;              /* [N*4] mean xyz, opacity */
+    const float *rotations;           /* [N*4] unit quaternion x, y, z, w */
+    const float *scales;              /* [N*3] */
+    const float *normals;             /* [N*3] unit PBR normals */
+    const uint32_t *material_indices; /* [N] */
+    const bv_material *materials;     /* [num_materials] */
+} bv_gaussian_desc;
+
+typedef struct bv_relight_settings { /* RelightSettings (gpu/relight.rs) subset */
+    float background[3];             /* radiance behind uncovered pixels */
+    uint32_t diffuse_samples;        /* must be 0 (no visibility ray) */
+} bv_relight_settings;
+
+typedef struct bv_relight_tracer bv_relight_tracer;
+
+/* Validates (lib.rs:246-340), keeps particles with opacity > 0.03
+ * (gpu/relight.rs:211), builds the device particle table and a BVH over
+ * the support ellipsoids (sqrt(2 ln(opacity/0.03)) standard deviations). */
+bv_status bv_relight_tracer_new_gaussian(const bv_gaussian_desc *model,
+                                         const bv_relight_settings *settings,
+                                         bv_relight_tracer **out);
+void bv_relight_tracer_destroy(bv_relight_tracer *tracer);
+/* set_point_light for each light; the reference holds one light per
+ * dispatch, several lights here shade every hit with their sum (alpha does
+ * not depend on the light, so this equals the sum of single-light renders
+ * with a zero background).  At most 64. */
+bv_status bv_relight_tracer_set_point_lights(bv_relight_tracer *tracer,
+                                             const bv_point_light *lights, uint32_t n_lights);
+bv_status bv_relight_tracer_set_background(bv_relight_tracer *tracer, const float rgb[3]);
+/* Renders width x height into out_rgba_dev ([h][w][4] float32): radiance +
+ * transmittance * background, alpha = 1 - transmittance (relight.wgsl:747-780). */
+bv_status bv_relight_tracer_dispatch(bv_relight_tracer *tracer, float *out_rgba_dev,
+                                     const bv_camera *camera, uint32_t width, uint32_t height,
+                                     bv_stream stream);
+uint32_t bv_relight_tracer_num_particles(const bv_relight_tracer *tracer);
+/* rays, composited hits (steps) and BVH nodes visited (faces) of the last dispatch */
+bv_status bv_relight_tracer_enable_stats(bv_relight_tracer *tracer, uint32_t enabled);
+bv_status bv_relight_tracer_last_stats(bv_relight_tracer *tracer, bv_launch_stats *out);
+
 /* ---- allocation-free start-cell search -----------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
  * hosts whose device memory is owned by their own pool (a renderer's frame
