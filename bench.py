@@ -57,9 +57,19 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=192,
                     help="side of the CPU-baseline sample image (view 0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="train", choices=["train", "relight", "render"],
+    ap.add_argument("--workload", default="train",
+                    choices=["train", "relight", "render", "serving"],
                     help="train: the headline fwd+bwd line; relight / render: secondary "
-                         "lines for the Gaussian relight and forward-render paths")
+                         "lines for the Gaussian relight and forward-render paths; serving: "
+                         "the request loop, batched against plain")
+    ap.add_argument("--rates", default="5,10,25,50,200,2000",
+                    help="serving: Poisson arrival rates (requests/s)")
+    ap.add_argument("--requests", type=int, default=60, help="serving: requests per rate")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget (GB)")
+    ap.add_argument("--serve-sites", default="65536,262144,524288,1048576",
+                    help="serving: sites of the resident scenes (seeds 1, 2, ...)")
+    ap.add_argument("--batch-rays", type=int, default=0, help="serving: rays per batch (0: default)")
+    ap.add_argument("--slots", type=int, default=0, help="serving: batches in flight (0: default)")
     return ap.parse_args()
 
 
@@ -281,10 +291,74 @@ def run_secondary(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args):
+    """Serving loop: resident RadFoam scenes, Poisson request streams (mixed
+    resolution, 1-16 views, 10% forward+backward with L2 loss), batched
+    engine against the plain one-request-at-a-time engine on the same
+    streams.  Latency runs from each request's scheduled arrival to its
+    outputs on the host."""
+    from blade_volume_b200 import serving
+
+    sites = [int(x) for x in args.serve_sites.split(",")]
+    t_build = time.time()
+    models = serving.serving_scenes(sites)  # spawned workers, before CUDA starts
+    t_build = time.time() - t_build
+    import torch
+
+    import blade_volume_b200 as bv
+
+    torch.cuda.set_device(0)
+    bufs = serving.HostBuffers()
+    rates = [float(r) for r in args.rates.split(",")]
+    sampler = ClockSampler(0)
+    out = {}
+    stats = {}
+    sampler.start()
+    for mode in ("plain", "plain_batch", "batched"):
+        srv = bv.Server(int(args.budget_gb * 1e9), mode=mode, max_batch_rays=args.batch_rays,
+                        slots=args.slots)
+        for m in models:
+            srv.add_scene(m, gradients=True)
+        srv.start()
+        serving.run_stream(srv, serving.poisson_stream(1000.0, max(args.warmup, 3) * 4,
+                                                       len(models), seed=99), bufs)
+        st0 = srv.stats()
+        out[mode] = {}
+        for rate in rates:
+            specs = serving.poisson_stream(rate, args.requests, len(models), seed=int(rate) + 1)
+            out[mode][f"{rate:g}"] = serving.run_stream(srv, specs, bufs)
+        st = srv.stats()
+        stats[mode] = {k: st[k] - st0[k] if k in ("requests_done", "frames_done", "rays_done",
+                                                   "batches", "graph_launches", "kernel_launches",
+                                                   "admission_waits") else st[k]
+                       for k in st}
+        srv.close()
+    clocks = sampler.stop()
+    top = f"{rates[-1]:g}"
+    b, p = out["batched"][top], out["plain"][top]
+    line = {"metric": "serving Mrays/s", "value": b["mrays_per_s"], "unit": "Mrays/s",
+            "higher_is_better": True, "n_gpus": 1, "dtype": "f32", "data": "synthetic",
+            "plain_value": p["mrays_per_s"],
+            "plain_batch_value": out["plain_batch"][top]["mrays_per_s"],
+            "vs_plain": b["mrays_per_s"] / p["mrays_per_s"] if p["mrays_per_s"] else None,
+            "config": {"workload": "serving", "scene_sites": sites, "sh_degree": 3,
+                       "resolutions": ["256x256", "512x512", "1280x720", "1920x1080"],
+                       "views": "1-16", "fwdbwd_fraction": 0.1, "rates": rates,
+                       "requests_per_rate": args.requests, "hbm_budget_gb": args.budget_gb,
+                       "scene_build_s": t_build},
+            "batched": out["batched"], "plain": out["plain"],
+            "plain_batch": out["plain_batch"], "server_stats": stats,
+            "gpu_launches": stats["batched"]["kernel_launches"], "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "serving":
+        run_serving(args)
         return
     if args.workload != "train":
         run_secondary(args)

@@ -30,7 +30,7 @@ LIB_PATH = os.environ.get("BV_B200_LIBRARY", os.path.join(HERE, "libbv_b200.so")
 BV_OK = 0
 STATUS_NAMES = {0: "BV_OK", 1: "BV_ERR_INVALID_ARGUMENT", 2: "BV_ERR_INVALID_MODEL",
                 3: "BV_ERR_CUDA", 4: "BV_ERR_OUT_OF_MEMORY", 5: "BV_ERR_CANDIDATE_OVERFLOW",
-                6: "BV_ERR_NOT_SUPPORTED", 7: "BV_ERR_NO_DEVICE"}
+                6: "BV_ERR_NOT_SUPPORTED", 7: "BV_ERR_NO_DEVICE", 8: "BV_ERR_TIMEOUT"}
 MODEL_SH_BF16 = 0x1
 PATH_TRUNCATED = 0x80000000
 LOSS_L2, LOSS_L1 = 0, 1
@@ -49,7 +49,14 @@ EXPORTED_SYMBOLS = [
     "bv_relight_tracer_set_point_lights", "bv_relight_tracer_set_background",
     "bv_relight_tracer_dispatch", "bv_relight_tracer_num_particles",
     "bv_relight_tracer_enable_stats", "bv_relight_tracer_last_stats",
+    "bv_server_new", "bv_server_add_scene", "bv_server_scene_grads", "bv_server_start",
+    "bv_server_submit", "bv_server_wait", "bv_server_stats_get", "bv_server_clock",
+    "bv_server_destroy",
 ]
+SERVE_BATCHED, SERVE_PLAIN, SERVE_PLAIN_BATCH = 0, 1, 2
+REQUEST_RENDER, REQUEST_FORWARD_BACKWARD = 0, 1
+SCENE_GRADIENTS = 0x1
+BV_ERR_TIMEOUT = 8
 
 
 class BvError(RuntimeError):
@@ -123,6 +130,37 @@ class RelightSettings(C.Structure):
     _fields_ = [("background", C.c_float * 3), ("diffuse_samples", C.c_uint32)]
 
 
+class ServerSettings(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("mode", C.c_uint32),
+                ("max_batch_rays", C.c_uint32), ("max_batch_views", C.c_uint32),
+                ("slots", C.c_uint32), ("max_steps", C.c_uint32), ("weight_threshold", C.c_float),
+                ("max_train_rays", C.c_uint64), ("use_graphs", C.c_uint32),
+                ("reserved", C.c_uint32 * 3)]
+
+
+class RequestC(C.Structure):
+    _fields_ = [("scene", C.c_uint32), ("kind", C.c_uint32), ("n_views", C.c_uint32),
+                ("width", C.c_uint32), ("height", C.c_uint32), ("reserved", C.c_uint32),
+                ("cameras", C.POINTER(CameraC)), ("out_host", C.c_void_p),
+                ("target_host", C.c_void_p), ("loss_host", C.c_void_p),
+                ("train", TrainSettings), ("grads", Grads), ("frame_done_host", C.c_void_p)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("status", C.c_int32), ("kind", C.c_uint32),
+                ("submit_s", C.c_double), ("admit_s", C.c_double), ("start_s", C.c_double),
+                ("done_s", C.c_double), ("rays", C.c_uint64), ("message", C.c_char * 128)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("requests_done", C.c_uint64), ("frames_done", C.c_uint64),
+                ("rays_done", C.c_uint64), ("batches", C.c_uint64),
+                ("graph_launches", C.c_uint64), ("kernel_launches", C.c_uint64),
+                ("arena_bytes", C.c_uint64), ("arena_peak_bytes", C.c_uint64),
+                ("resident_bytes", C.c_uint64), ("admission_waits", C.c_uint64),
+                ("busy_s", C.c_double)]
+
+
 _lib = None
 
 
@@ -182,6 +220,18 @@ def load_library(path: str = LIB_PATH):
     L.bv_relight_tracer_num_particles.restype = C.c_uint32
     L.bv_relight_tracer_enable_stats.argtypes = [C.c_void_p, C.c_uint32]
     L.bv_relight_tracer_last_stats.argtypes = [C.c_void_p, C.POINTER(LaunchStats)]
+    L.bv_server_new.argtypes = [C.POINTER(ServerSettings), C.POINTER(C.c_void_p)]
+    L.bv_server_add_scene.argtypes = [C.c_void_p, C.POINTER(ModelDesc), C.c_uint32,
+                                      C.POINTER(C.c_uint32)]
+    L.bv_server_scene_grads.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(Grads)]
+    L.bv_server_start.argtypes = [C.c_void_p]
+    L.bv_server_submit.argtypes = [C.c_void_p, C.POINTER(RequestC), C.POINTER(C.c_uint64)]
+    L.bv_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(RequestResult)]
+    L.bv_server_stats_get.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+    L.bv_server_clock.argtypes = [C.c_void_p]
+    L.bv_server_clock.restype = C.c_double
+    L.bv_server_destroy.argtypes = [C.c_void_p]
+    L.bv_server_destroy.restype = None
     _lib = L
     return L
 
@@ -485,3 +535,133 @@ class RelightTracer:
         s = LaunchStats()
         _check(load_library().bv_relight_tracer_last_stats(self._h, C.byref(s)))
         return s
+
+
+def _host_ptr(a) -> int:
+    """Address of a C-contiguous float32/float64 host buffer (numpy array or
+    torch CPU tensor, pinned for overlapped copies)."""
+    if hasattr(a, "data_ptr"):
+        if a.is_cuda or not a.is_contiguous():
+            raise ValueError("host buffers must be contiguous CPU tensors")
+        return a.data_ptr()
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("host buffers must be C-contiguous")
+    return a.ctypes.data
+
+
+class Server:
+    """Serving loop over the C ABI (bv_server_*): resident scenes, admission
+    under an HBM budget, continuous batching of render frames into one
+    persistent traversal launch per batch (replayed CUDA graphs), or the
+    plain one-request-at-a-time modes ("plain": one dispatch per view,
+    "plain_batch": one dispatch over the request's views).  Host buffers passed to :meth:`submit`
+    are kept alive here until :meth:`wait` returns their request."""
+
+    def __init__(self, hbm_budget_bytes: int, mode: str = "batched", max_batch_rays: int = 0,
+                 max_batch_views: int = 0, slots: int = 0, max_steps: int = 1024,
+                 weight_threshold: float = 0.001, max_train_rays: int = 0,
+                 use_graphs: bool = True):
+        L = load_library()
+        s = ServerSettings()
+        s.hbm_budget_bytes = int(hbm_budget_bytes)
+        s.mode = {"batched": SERVE_BATCHED, "plain": SERVE_PLAIN,
+                  "plain_batch": SERVE_PLAIN_BATCH}[mode]
+        s.max_batch_rays = max_batch_rays
+        s.max_batch_views = max_batch_views
+        s.slots = slots
+        s.max_steps = max_steps
+        s.weight_threshold = weight_threshold
+        s.max_train_rays = max_train_rays
+        s.use_graphs = 1 if use_graphs else 0
+        h = C.c_void_p()
+        _check(L.bv_server_new(C.byref(s), C.byref(h)))
+        self._h = h
+        self._keep = {}
+        self.scenes = []
+
+    def add_scene(self, model: PointCloudModel, gradients: bool = False) -> int:
+        d = _DescHolder(model)
+        sid = C.c_uint32()
+        _check(load_library().bv_server_add_scene(self._h, C.byref(d.desc),
+                                                  SCENE_GRADIENTS if gradients else 0,
+                                                  C.byref(sid)))
+        self.scenes.append(model)
+        return sid.value
+
+    def scene_grads(self, scene: int) -> Grads:
+        g = Grads()
+        _check(load_library().bv_server_scene_grads(self._h, scene, C.byref(g)))
+        return g
+
+    def start(self):
+        _check(load_library().bv_server_start(self._h))
+
+    def submit(self, scene: int, cameras: Sequence[Camera], width: int, height: int,
+               out=None, target=None, loss=None, grads: Optional[dict] = None,
+               max_steps: int = 1024, weight_threshold: float = 0.0, max_dt: float = 50.0,
+               loss_kind: int = LOSS_L2, frame_done=None) -> int:
+        """Queue a render request (``out`` [views, H, W, 4] float32 host) or,
+        with ``target`` ([views, H, W, 3] float32 host) and ``loss`` (float32
+        host [1]), a forward+backward request (``out`` then [views, H, W, 3]
+        or None; ``grads`` a dict of CUDA tables as from
+        RadFoamGpuTracer.new_grads, or None for the scene's own tables)."""
+        r = RequestC()
+        r.scene = scene
+        r.n_views = len(cameras)
+        r.width, r.height = width, height
+        cams = (CameraC * len(cameras))(*[camera_c(c) for c in cameras])
+        r.cameras = cams
+        keep = [cams, out, target, loss, grads, frame_done]
+        if target is None:
+            r.kind = REQUEST_RENDER
+            r.out_host = _host_ptr(out) if out is not None else None
+        else:
+            r.kind = REQUEST_FORWARD_BACKWARD
+            r.out_host = _host_ptr(out) if out is not None else None
+            r.target_host = _host_ptr(target)
+            r.loss_host = _host_ptr(loss) if loss is not None else None
+            r.train.max_steps = max_steps
+            r.train.weight_threshold = weight_threshold
+            r.train.max_dt = max_dt
+            r.train.loss = loss_kind
+            if grads is not None:
+                r.grads.d_density_dev = grads["d_density"].data_ptr()
+                r.grads.d_sh_dev = grads["d_sh"].data_ptr()
+                if "d_pos" in grads:
+                    r.grads.d_positions_dev = grads["d_pos"].data_ptr()
+                if "d_radius" in grads:
+                    r.grads.d_radii_dev = grads["d_radius"].data_ptr()
+        if frame_done is not None:
+            r.frame_done_host = _host_ptr(frame_done)
+        rid = C.c_uint64()
+        _check(load_library().bv_server_submit(self._h, C.byref(r), C.byref(rid)))
+        self._keep[rid.value] = keep
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = 120.0) -> dict:
+        res = RequestResult()
+        _check(load_library().bv_server_wait(self._h, rid, timeout, C.byref(res)))
+        self._keep.pop(rid, None)
+        return dict(id=res.id, status=res.status, kind=res.kind, submit_s=res.submit_s,
+                    admit_s=res.admit_s, start_s=res.start_s, done_s=res.done_s, rays=res.rays,
+                    message=res.message.decode(errors="replace"))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(load_library().bv_server_stats_get(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def clock(self) -> float:
+        return load_library().bv_server_clock(self._h)
+
+    def close(self):
+        if self._h:
+            load_library().bv_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -88,6 +88,7 @@ struct bv_tracer {
     int start_blocks = 1;
     RayState *ray_state = nullptr;     // per-ray training state
     size_t ray_state_capacity = 0;
+    bool ray_state_owned = true;       // false: lent by a serving engine
     float4 *site_grads = nullptr;      // [N] site gradient accumulator (kept zero)
     int grid_forward = 0;
     int grid_train_fwd = 0;
@@ -127,7 +128,7 @@ void free_tracer(bv_tracer *t) {
     cudaFree(t->sh);
     cudaFree(t->offsets);
     cudaFree(t->faces);
-    cudaFree(t->ray_state);
+    if (t->ray_state_owned) cudaFree(t->ray_state);
     cudaFree(t->site_grads);
     cudaFree(t->start_cells);
     cudaFree(t->work_counter);
@@ -204,6 +205,32 @@ bv_status begin_timing(bv_tracer *t, cudaStream_t s) {
 }
 
 }  // namespace
+
+DeviceModel bv::tracer_device_model(const bv_tracer *t) { return t->model(); }
+
+ViewDesc bv::view_desc(const bv_camera &c, uint32_t width, uint32_t height, uint32_t ray_begin,
+                       uint64_t pixel_begin) {
+    return make_view(c, width, height, ray_begin, pixel_begin);
+}
+
+uint32_t bv::tile_padded_rays(uint32_t width, uint32_t height) { return padded_rays(width, height); }
+
+bv_status bv::validate_camera(const bv_camera &c) { return check_camera(c); }
+
+size_t bv::tracer_device_bytes(const bv_tracer *t) {
+    const size_t n = t->n;
+    const size_t sh_bytes = n * t->sh_stride * (t->bf16 ? 2 : 4);
+    return n * (sizeof(float4) + sizeof(float) + sizeof(float4)) + (n + 1) * sizeof(uint32_t) +
+           (size_t)std::max<uint32_t>(t->m_edges, 1) * sizeof(FaceEntry) + sh_bytes +
+           (size_t)kMaxStartQueries * t->start_blocks * (sizeof(double) + sizeof(uint32_t));
+}
+
+void bv::tracer_lend_ray_state(bv_tracer *t, RayState *buffer, size_t capacity) {
+    if (t->ray_state_owned) cudaFree(t->ray_state);
+    t->ray_state = buffer;
+    t->ray_state_capacity = capacity;
+    t->ray_state_owned = false;
+}
 
 extern "C" {
 
@@ -567,6 +594,9 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
     cudaStream_t s = (cudaStream_t)stream;
     // per-ray state scratch for the largest chunk of this call
     const size_t chunk_rays = (size_t)std::min<uint32_t>(n_cams, kMaxViewsPerLaunch) * width * height;
+    if (chunk_rays > t->ray_state_capacity && !t->ray_state_owned)
+        return fail(BV_ERR_INVALID_ARGUMENT, "batch exceeds the lent ray-state scratch (%zu rays)",
+                    t->ray_state_capacity);
     if (chunk_rays > t->ray_state_capacity) {
         cudaFree(t->ray_state);
         t->ray_state = nullptr;

@@ -116,6 +116,45 @@ struct StartCellQueries {
     uint32_t count;
 };
 
+// ---- serving: one traversal launch over the frames (views) of many
+// requests, any resident scene and any resolution.  The batch is described
+// by a table in device memory, so one captured CUDA graph serves every batch.
+constexpr int kMaxServeScenes = 8;
+constexpr int kMaxServeViews = 1024;
+constexpr int kServeStartBlocks = 16;  // start-cell blocks per frame
+constexpr int kServeStartRows = 64;    // frames searched concurrently
+
+struct ServeView {  // 96 bytes
+    ViewDesc v;           // ray_begin: first work item in the batch; pixel_begin unused
+    uint32_t scene;
+    uint32_t start_cell;  // written by the start-cell kernel of the batch
+    uint64_t out;         // float4 * [height][width] of this frame
+};
+
+struct ServeHeader {  // 16 bytes, followed by the ServeView rows
+    uint32_t n_views;
+    uint32_t total_work;
+    uint32_t pad[2];
+};
+
+struct ServeParams {
+    DeviceModel scenes[kMaxServeScenes];
+    uint32_t n_scenes;
+    uint32_t max_steps;
+    float weight_threshold;
+    uint32_t pad;
+    const ServeHeader *header;
+    ServeView *views;
+    uint32_t *work_counter;
+    double *partial_dist;     // [kMaxServeViews][kServeStartBlocks]
+    uint32_t *partial_index;  // [kMaxServeViews][kServeStartBlocks]
+    uint32_t *counters;       // [kMaxServeViews], zero between launches
+};
+
+cudaError_t launch_serve_start_cells(const ServeParams &p, cudaStream_t s);
+cudaError_t launch_serve_walk(const ServeParams &p, int grid, cudaStream_t s);
+int serve_grid_size(int device);
+
 // Launchers (bv_walk.cu / bv_start_cell.cu).
 cudaError_t launch_walk_forward(const WalkParams &p, int grid, cudaStream_t s);
 cudaError_t launch_record_paths(const RecordParams &p, int grid, cudaStream_t s);
@@ -142,5 +181,20 @@ void set_last_error(const char *message);
 cudaError_t launch_start_cells(const float4 *geom, uint32_t n, const StartCellQueries &queries,
                                const StartCellScratch &scratch, uint32_t *out, cudaStream_t s);
 int start_cell_blocks(uint32_t n);
+
+// Camera helpers shared by the tracer calls and the serving engine
+// (bv_api.cu): the view record of a camera, work items of a tile-padded
+// image, camera validation (sets bv_last_error on failure).
+ViewDesc view_desc(const bv_camera &c, uint32_t width, uint32_t height, uint32_t ray_begin,
+                   uint64_t pixel_begin);
+uint32_t tile_padded_rays(uint32_t width, uint32_t height);
+bv_status validate_camera(const bv_camera &c);
+
+// Accessors the serving engine uses on tracers it owns (bv_api.cu).
+DeviceModel tracer_device_model(const bv_tracer *t);
+size_t tracer_device_bytes(const bv_tracer *t);
+// Hand the tracer a caller-owned ray-state buffer for bv_forward_backward
+// (chunks larger than capacity are refused instead of growing it).
+void tracer_lend_ray_state(bv_tracer *t, RayState *buffer, size_t capacity);
 
 }  // namespace bv

@@ -107,7 +107,73 @@ start_cell_kernel(const float4 *__restrict__ geom, uint32_t n,
     }
 }
 
+// Start cells of a served batch: blockIdx.y strides over the frames of the
+// batch (the frame count is read from the device table, so the grid is
+// fixed and the launch can live in a captured graph); kServeStartBlocks
+// blocks search each frame's scene.  Same scoring and tie rule as above.
+__global__ void __launch_bounds__(kStartBlock) serve_start_cells_kernel(const __grid_constant__ ServeParams P) {
+    const uint32_t n_views = P.header->n_views;
+    __shared__ bool last;
+    for (uint32_t v = blockIdx.y; v < n_views; v += gridDim.y) {
+        ServeView *sv = P.views + v;
+        const uint32_t scene = sv->scene;
+        const float4 *geom = P.scenes[scene].geom;
+        const uint32_t n = P.scenes[scene].n;
+        const double qx = sv->v.origin[0], qy = sv->v.origin[1], qz = sv->v.origin[2];
+        double best = DBL_MAX;
+        uint32_t best_i = 0xffffffffu;
+        const uint32_t stride = gridDim.x * blockDim.x;
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+            const float4 g = __ldg(geom + i);
+            const double dx = qx - (double)g.x;
+            const double dy = qy - (double)g.y;
+            const double dz = qz - (double)g.z;
+            const double r = (double)g.w;
+            const double dist = (dx * dx + dy * dy + dz * dz) - r * r;
+            if (dist < best) {
+                best = dist;
+                best_i = i;
+            }
+        }
+        block_argmin(best, best_i);
+        double *pd = P.partial_dist + (size_t)v * gridDim.x;
+        uint32_t *pi = P.partial_index + (size_t)v * gridDim.x;
+        if (threadIdx.x == 0) {
+            pd[blockIdx.x] = best;
+            pi[blockIdx.x] = best_i;
+            __threadfence();
+            last = atomicAdd(P.counters + v, 1u) == gridDim.x - 1;
+        }
+        __syncthreads();
+        if (last) {
+            __threadfence();
+            double d = DBL_MAX;
+            uint32_t i = 0xffffffffu;
+            for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+                const double od = __ldcg(pd + b);
+                const uint32_t oi = __ldcg(pi + b);
+                if (better(od, oi, d, i)) {
+                    d = od;
+                    i = oi;
+                }
+            }
+            block_argmin(d, i);
+            if (threadIdx.x == 0) {
+                sv->start_cell = i == 0xffffffffu ? 0u : i;
+                P.counters[v] = 0u;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_serve_start_cells(const ServeParams &p, cudaStream_t s) {
+    dim3 grid(kServeStartBlocks, kServeStartRows);
+    serve_start_cells_kernel<<<grid, kStartBlock, 0, s>>>(p);
+    return cudaGetLastError();
+}
 
 int start_cell_blocks(uint32_t n) {
     const uint32_t per_block = kStartBlock * 8u;

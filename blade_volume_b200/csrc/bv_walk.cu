@@ -1049,6 +1049,115 @@ train_backward_kernel(const __grid_constant__ TrainParams P) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// serving: one persistent traversal over the frames of many requests (any
+// resident scene, any resolution) listed in a device-side table.  Per ray
+// the arithmetic is walk_forward_kernel's, so a frame renders bit for bit
+// the same in any batch.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t serve_view_of(const ServeView *views, uint32_t n,
+                                                  uint32_t w) {
+    uint32_t lo = 0, hi = n - 1;  // last frame with ray_begin <= w
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) / 2;
+        if (__ldg(&views[mid].v.ray_begin) <= w)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int DEG, bool BOUNDED, bool BF16>
+__global__ void __launch_bounds__(kWalkBlock, BV_MINB_RENDER)
+serve_walk_kernel(const __grid_constant__ ServeParams P) {
+    __shared__ DeviceModel s_scenes[kMaxServeScenes];
+    if (threadIdx.x < P.n_scenes) s_scenes[threadIdx.x] = P.scenes[threadIdx.x];
+    __syncthreads();
+    const uint32_t n_views = P.header->n_views;
+    const uint32_t total = P.header->total_work;
+    bool drained = n_views == 0, active = false;
+    Ray ray;
+    Cell c;
+    uint32_t scene = 0;
+    float t0 = 0.f, T = 1.f, ar = 0.f, ag = 0.f, ab = 0.f, depth = 0.f;
+    uint32_t steps = 0;
+    float4 *out = nullptr;
+    for (;;) {
+        uint32_t w;
+        if (refill(P.work_counter, total, active, drained, w)) {
+            const ServeView *sv = P.views + serve_view_of(P.views, n_views, w);
+            const ViewDesc vd = sv->v;
+            const uint32_t local = w - vd.ray_begin;
+            const uint32_t tile = local / kTileRays, in = local % kTileRays;
+            const uint32_t x = (tile % vd.tiles_x) * kTileW + in % kTileW;
+            const uint32_t y = (tile / vd.tiles_x) * kTileH + in / kTileW;
+            if (x < vd.width && y < vd.height) {
+                scene = sv->scene;
+                out = reinterpret_cast<float4 *>(sv->out) + (size_t)y * vd.width + x;
+                const bool ok = make_ray(vd, x, y, ray);
+                c = load_cell(s_scenes[scene], sv->start_cell);
+                t0 = 0.f;
+                T = 1.f;
+                ar = ag = ab = 0.f;
+                depth = vd.depth;
+                steps = 0;
+                if (ok)
+                    active = true;
+                else
+                    *out = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+        if (__ballot_sync(kFull, active) == 0) {
+            if (drained) break;
+            continue;
+        }
+        if (!active) continue;
+        const DeviceModel &m = s_scenes[scene];
+        bool done = false;
+        if (steps >= P.max_steps) {
+            done = true;
+        } else {
+            steps += 1;
+            if (T <= P.weight_threshold || t0 > depth) {
+                done = true;
+            } else {
+                float best;
+                FaceEntry win;
+                const bool has_exit = find_exit<BOUNDED>(m, c, ray, t0, depth, best, win);
+                float ss, se;
+                if (support<BOUNDED>(ray, c.x, c.y, c.z, c.r, t0, best, ss, se)) {
+                    const float dens = c.density * 1.0f;
+                    if (dens > 1e-6f) {
+                        const float dt = se - ss;
+                        const float alpha = 1.0f - bv_expf(-dens * dt);
+                        const float wgt = T * alpha;
+                        float coef[ShDims<DEG>::N];
+                        load_sh_row<DEG, BF16>(m, c.id, coef);
+                        float r, g, b;
+                        eval_sh<DEG>(coef, ray.dx, ray.dy, ray.dz, r, g, b);
+                        ar += wgt * fmaxf(r, 0.0f);
+                        ag += wgt * fmaxf(g, 0.0f);
+                        ab += wgt * fmaxf(b, 0.0f);
+                        T *= 1.0f - alpha;
+                    }
+                }
+                if (!has_exit) {
+                    t0 = best;
+                    done = true;
+                } else {
+                    t0 = fmaxf(t0, best);
+                    c = cell_from_face(win);
+                }
+            }
+        }
+        if (done) {
+            *out = make_float4(ar, ag, ab, 1.0f - T);
+            active = false;
+        }
+    }
+}
+
 // d_pos[i] += site[i].xyz, d_radius[i] += site[i].w (scatter-add semantics
 // of the caller's tables), then clears the site table for the next call.
 __global__ void fold_site_grads_kernel(float4 *site, uint32_t n, float *d_pos, float *d_radius) {
@@ -1076,9 +1185,10 @@ cudaError_t launch_fold_site_grads(float4 *site, uint32_t n, float *d_pos, float
 // ---------------------------------------------------------------------------
 // launchers: pick the instantiation for (SH degree, bounded, bf16)
 // ---------------------------------------------------------------------------
-#define BV_SELECT(KERNEL, PARAMS, GRID, STREAM)                                                 \
+#define BV_SELECT(KERNEL, PARAMS, GRID, STREAM) BV_SELECT_M(KERNEL, (PARAMS).m, PARAMS, GRID, STREAM)
+#define BV_SELECT_M(KERNEL, MODEL, PARAMS, GRID, STREAM)                                        \
     do {                                                                                        \
-        const DeviceModel &mm = (PARAMS).m;                                                     \
+        const DeviceModel &mm = (MODEL);                                                        \
         const int key = (int)mm.sh_degree * 4 + (mm.bounded ? 2 : 0) + (mm.sh_bf16 ? 1 : 0);    \
         switch (key) {                                                                          \
             case 0: KERNEL<0, false, false><<<GRID, kWalkBlock, 0, STREAM>>>(PARAMS); break;     \
@@ -1114,6 +1224,22 @@ cudaError_t launch_train_forward(const TrainParams &p, int grid, cudaStream_t s)
 cudaError_t launch_train_backward(const TrainParams &p, int grid, cudaStream_t s) {
     BV_SELECT(train_backward_kernel, p, grid, s);
     return cudaGetLastError();
+}
+
+// Every scene of a served batch shares (SH degree, bounded, bf16): the
+// instantiation is picked from scene 0.
+cudaError_t launch_serve_walk(const ServeParams &p, int grid, cudaStream_t s) {
+    if (p.n_scenes == 0 || p.n_scenes > (uint32_t)kMaxServeScenes) return cudaErrorInvalidValue;
+    BV_SELECT_M(serve_walk_kernel, p.scenes[0], p, grid, s);
+    return cudaGetLastError();
+}
+
+int serve_grid_size(int device) {
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_walk_kernel<3, false, false>,
+                                                  kWalkBlock, 0);
+    return sms * (per_sm < 1 ? 1 : per_sm);
 }
 
 cudaError_t launch_record_paths(const RecordParams &p, int grid, cudaStream_t s) {

@@ -44,6 +44,8 @@ typedef enum bv_status {
     BV_ERR_NOT_SUPPORTED = 6,
     /* no CUDA device is available */
     BV_ERR_NO_DEVICE = 7,
+    /* bv_server_wait: the request has not finished within the timeout */
+    BV_ERR_TIMEOUT = 8,
 } bv_status;
 
 /* cudaStream_t; NULL selects the legacy default stream. */
@@ -301,6 +303,111 @@ bv_status bv_relight_tracer_last_stats(bv_relight_tracer *tracer, bv_launch_stat
 bv_status bv_containing_points_noalloc(const float *sites_dev, uint32_t num_sites,
                                        const float *positions, uint32_t n_queries,
                                        uint32_t *out_index_dev, bv_stream stream);
+
+/* ---- serving loop ----------------------------------------------------------
+ * No counterpart in the reference (its viewer renders one camera per frame,
+ * blade-volume-view/src/render.rs:145-567).  A server keeps several scenes
+ * resident on the device and serves render and forward+backward requests
+ * of mixed resolution and view count from any host thread:
+ *   - a request is admitted when its device buffers fit in the HBM budget
+ *     left after the scenes and fixed scratch (first in, first admitted);
+ *   - BV_SERVE_BATCHED: the frames (views) of all admitted render requests
+ *     are packed into batches, each ONE start-cell launch plus ONE persistent
+ *     traversal launch over every frame in it (any scene, any size), replayed
+ *     from a captured CUDA graph; up to `slots` batches run concurrently on
+ *     their own streams, and each frame is copied to the host as soon as its
+ *     batch finishes.  Forward+backward requests run on a stream of their own
+ *     beside the batches;
+ *   - BV_SERVE_PLAIN: one request at a time through the tracer calls, one
+ *     bv_radfoam_tracer_dispatch per view (the reference's tracer takes one
+ *     camera per dispatch), or bv_forward_backward, then a synchronize: the
+ *     per-request baseline.  BV_SERVE_PLAIN_BATCH: the same with one
+ *     bv_radfoam_tracer_dispatch_batch over the request's views.
+ * Every scene of a server has the same SH degree, radii presence and SH
+ * storage.  Frames render bit for bit as bv_radfoam_tracer_dispatch_batch
+ * renders them, in any batch. */
+typedef struct bv_server bv_server;
+
+typedef enum bv_serve_mode {
+    BV_SERVE_BATCHED = 0,
+    BV_SERVE_PLAIN = 1,       /* per request, one dispatch per view */
+    BV_SERVE_PLAIN_BATCH = 2, /* per request, one dispatch_batch over its views */
+} bv_serve_mode;
+typedef enum bv_request_kind { BV_REQUEST_RENDER = 0, BV_REQUEST_FORWARD_BACKWARD = 1 } bv_request_kind;
+
+typedef struct bv_server_settings {
+    uint64_t hbm_budget_bytes;  /* scenes + gradient tables + scratch + request buffers */
+    uint32_t mode;              /* bv_serve_mode */
+    uint32_t max_batch_rays;    /* rays per batch; 0 = 4,194,304; >= the largest frame */
+    uint32_t max_batch_views;   /* frames per batch, 1..1024; 0 = 256 */
+    uint32_t slots;             /* batches in flight, 1..4; 0 = 2 */
+    uint32_t max_steps;         /* 0 = 1024 */
+    float weight_threshold;     /* transmittance cut, e.g. 0.001 */
+    uint64_t max_train_rays;    /* largest forward+backward chunk (<= 32 views); 0 = 16 x 1920 x 1080 */
+    uint32_t use_graphs;        /* 1: replay captured graphs, 0: launch directly */
+    uint32_t reserved[3];
+} bv_server_settings;
+
+/* Scene flag: the server keeps gradient tables for the scene, into which
+ * forward+backward requests that name no tables of their own accumulate. */
+#define BV_SCENE_GRADIENTS 0x1u
+
+typedef struct bv_request {
+    uint32_t scene;
+    uint32_t kind;                /* bv_request_kind */
+    uint32_t n_views;             /* 1..1024 */
+    uint32_t width, height;
+    uint32_t reserved;
+    const bv_camera *cameras;     /* host [n_views], copied by bv_server_submit */
+    float *out_host;              /* render: [views][h][w][4]; fwd+bwd: [views][h][w][3] or NULL */
+    const float *target_host;     /* fwd+bwd: [views][h][w][3], read once admitted */
+    float *loss_host;             /* fwd+bwd: receives the loss */
+    bv_train_settings train;      /* fwd+bwd */
+    bv_grads grads;               /* fwd+bwd device tables; all NULL: the scene's own */
+    double *frame_done_host;      /* optional [n_views]: server-clock time each frame landed */
+} bv_request;
+
+typedef struct bv_request_result {
+    uint64_t id;
+    int32_t status;               /* bv_status of the request */
+    uint32_t kind;
+    double submit_s;              /* server clock (seconds since bv_server_new) */
+    double admit_s;               /* device buffers granted */
+    double start_s;               /* first work enqueued on the GPU */
+    double done_s;                /* every output on the host */
+    uint64_t rays;
+    char message[128];
+} bv_request_result;
+
+typedef struct bv_server_stats {
+    uint64_t requests_done, frames_done, rays_done;
+    uint64_t batches, graph_launches, kernel_launches;
+    uint64_t arena_bytes, arena_peak_bytes, resident_bytes;
+    uint64_t admission_waits;     /* times the head request did not fit */
+    double busy_s;                /* wall time with work on the device */
+} bv_server_stats;
+
+bv_status bv_server_new(const bv_server_settings *settings, bv_server **out);
+/* Uploads a scene (tracer packing); only before bv_server_start. */
+bv_status bv_server_add_scene(bv_server *server, const bv_model_desc *model, uint32_t flags,
+                              uint32_t *scene_id);
+/* Device gradient tables of a BV_SCENE_GRADIENTS scene. */
+bv_status bv_server_scene_grads(bv_server *server, uint32_t scene, bv_grads *out);
+/* Reserves the request arena (budget minus resident), captures the batch
+ * graphs and starts the scheduler thread. */
+bv_status bv_server_start(bv_server *server);
+/* Validates and queues a request; host buffers stay valid until it is done.
+ * A request whose buffers can never fit the arena is refused here. */
+bv_status bv_server_submit(bv_server *server, const bv_request *request, uint64_t *id);
+/* Waits up to timeout_s for request id.  BV_OK once it has finished: out
+ * holds its result (out->status is the request's own status) and the id is
+ * forgotten.  BV_ERR_TIMEOUT if it has not finished, BV_ERR_INVALID_ARGUMENT
+ * for an unknown id. */
+bv_status bv_server_wait(bv_server *server, uint64_t id, double timeout_s, bv_request_result *out);
+bv_status bv_server_stats_get(bv_server *server, bv_server_stats *out);
+double bv_server_clock(const bv_server *server);
+/* Finishes queued work, stops the scheduler, frees everything. */
+void bv_server_destroy(bv_server *server);
 
 #ifdef __cplusplus
 }
