@@ -58,10 +58,12 @@ def parse():
                     help="side of the CPU-baseline sample image (view 0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="train",
-                    choices=["train", "relight", "render", "serving"],
+                    choices=["train", "relight", "render", "serving", "splat"],
                     help="train: the headline fwd+bwd line; relight / render: secondary "
                          "lines for the Gaussian relight and forward-render paths; serving: "
                          "the request loop, batched against plain")
+    ap.add_argument("--splat-sites", type=int, default=1048576,
+                    help="splat: sites of the PowerFoam mixture")
     ap.add_argument("--rates", default="5,10,25,50,200,2000",
                     help="serving: Poisson arrival rates (requests/s)")
     ap.add_argument("--requests", type=int, default=60, help="serving: requests per rate")
@@ -254,6 +256,49 @@ def run_secondary(args):
                            "kept": tr.num_particles, "width": W, "height": H,
                            "lights": len(lights), "window": 16},
                 "hits_per_ray": hits / (W * H), "nodes_per_ray": st.faces / (W * H),
+                "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak,
+                             "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
+                             "traffic": None, "peak_source": kind},
+                "gpu_launches": args.steps, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+        return
+    if args.workload == "splat":
+        t_build = time.time()
+        w = scenes.powerfoam_mix(n_sites=args.splat_sites)
+        t_build = time.time() - t_build
+        W, H, V = w.width, w.height, len(w.cameras)
+        tr = bv.PowerFoamSplatTracer(w.model, max_steps=w.max_steps,
+                                     weight_threshold=w.weight_threshold)
+        out = torch.empty((V, H, W, 4), dtype=torch.float32, device="cuda")
+        for _ in range(max(args.warmup, 3)):
+            tr.dispatch_batch(out, w.cameras, (W, H))
+        tr.enable_stats(True)
+        tr.dispatch_batch(out, w.cameras, (W, H))
+        st = tr.last_stats()
+        tr.enable_stats(False)
+        max_hits, hits, entries = tr.candidate_stats()
+        sampler.start()
+        ts = timed_events(lambda: tr.dispatch_batch(out, w.cameras, (W, H)), args.steps, flush,
+                          stream)
+        clocks = sampler.stop()
+        ms = statistics.median(ts)
+        rays = V * W * H
+        K = 16
+        # per support hit: its site (16 B) + its Cech row at 20 B an entry;
+        # per composited interval: the BF16 attribute row (2*3K + 4 B);
+        # 16 B out per ray
+        alg = hits * 16 + entries * 20 + st.steps * (2 * 3 * K + 4) + rays * 16
+        peak, kind = peaks()
+        line = {"metric": "splat Mrays/s", "value": rays / (ms * 1e-3) / 1e6, "unit": "Mrays/s",
+                "ms_per_step": ms, "steps": args.steps, "warmup": max(args.warmup, 3),
+                "dtype": "f32 (SH bf16)", "data": "synthetic",
+                "config": {"workload": "powerfoam splat", "sites": w.model.n,
+                           "cech_mean_degree": w.model.mean_degree(), "views": V, "width": W,
+                           "height": H, "max_steps": w.max_steps, "scene_build_s": t_build},
+                "support_hits_per_ray": hits / rays, "max_hits_per_ray": max_hits,
+                "intervals_per_ray": st.steps / rays,
+                "cech_entries_clipped_per_ray": st.faces / rays,
+                "cech_entries_per_hit": entries / max(hits, 1),
                 "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak,
                              "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
                              "traffic": None, "peak_source": kind},

@@ -52,6 +52,14 @@ EXPORTED_SYMBOLS = [
     "bv_server_new", "bv_server_add_scene", "bv_server_scene_grads", "bv_server_start",
     "bv_server_submit", "bv_server_wait", "bv_server_stats_get", "bv_server_clock",
     "bv_server_destroy",
+    "bv_powerfoam_splat_tracer_new", "bv_powerfoam_splat_tracer_destroy",
+    "bv_powerfoam_splat_tracer_dispatch", "bv_powerfoam_splat_tracer_dispatch_batch",
+    "bv_powerfoam_splat_tracer_validate_candidate_counts",
+    "bv_powerfoam_splat_tracer_candidate_stats",
+    "bv_powerfoam_splat_tracer_candidate_capacity", "bv_powerfoam_splat_tracer_max_steps",
+    "bv_powerfoam_splat_tracer_weight_threshold",
+    "bv_powerfoam_splat_tracer_set_weight_threshold", "bv_powerfoam_splat_tracer_enable_stats",
+    "bv_powerfoam_splat_tracer_last_stats",
 ]
 SERVE_BATCHED, SERVE_PLAIN, SERVE_PLAIN_BATCH = 0, 1, 2
 REQUEST_RENDER, REQUEST_FORWARD_BACKWARD = 0, 1
@@ -232,6 +240,28 @@ def load_library(path: str = LIB_PATH):
     L.bv_server_clock.restype = C.c_double
     L.bv_server_destroy.argtypes = [C.c_void_p]
     L.bv_server_destroy.restype = None
+    L.bv_powerfoam_splat_tracer_new.argtypes = [C.POINTER(ModelDesc), C.POINTER(TraceSettings),
+                                                C.POINTER(C.c_void_p)]
+    L.bv_powerfoam_splat_tracer_destroy.argtypes = [C.c_void_p]
+    L.bv_powerfoam_splat_tracer_destroy.restype = None
+    L.bv_powerfoam_splat_tracer_dispatch.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(CameraC),
+                                                     C.c_uint32, C.c_uint32, C.c_void_p]
+    L.bv_powerfoam_splat_tracer_dispatch_batch.argtypes = [C.c_void_p, C.c_void_p,
+                                                           C.POINTER(CameraC), C.c_uint32,
+                                                           C.c_uint32, C.c_uint32, C.c_void_p]
+    L.bv_powerfoam_splat_tracer_validate_candidate_counts.argtypes = [C.c_void_p,
+                                                                      C.POINTER(C.c_uint32)]
+    L.bv_powerfoam_splat_tracer_candidate_stats.argtypes = [
+        C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    for name in ("candidate_capacity", "max_steps"):
+        f = getattr(L, "bv_powerfoam_splat_tracer_" + name)
+        f.argtypes = [C.c_void_p]
+        f.restype = C.c_uint32
+    L.bv_powerfoam_splat_tracer_weight_threshold.argtypes = [C.c_void_p]
+    L.bv_powerfoam_splat_tracer_weight_threshold.restype = C.c_float
+    L.bv_powerfoam_splat_tracer_set_weight_threshold.argtypes = [C.c_void_p, C.c_float]
+    L.bv_powerfoam_splat_tracer_enable_stats.argtypes = [C.c_void_p, C.c_uint32]
+    L.bv_powerfoam_splat_tracer_last_stats.argtypes = [C.c_void_p, C.POINTER(LaunchStats)]
     _lib = L
     return L
 
@@ -535,6 +565,92 @@ class RelightTracer:
         s = LaunchStats()
         _check(load_library().bv_relight_tracer_last_stats(self._h, C.byref(s)))
         return s
+
+
+class PowerFoamSplatTracer:
+    """PowerFoamGpuSplatTracer (gpu/powerfoam_splat.rs:38-370) over the C ABI:
+    the order-exact splat render of a PowerFoam model (radii required; the
+    CSR is the Cech overlap graph)."""
+
+    def __init__(self, model: PointCloudModel, max_steps: int = 1024,
+                 weight_threshold: float = 0.001, candidate_capacity: int = 0):
+        L = load_library()
+        self.model = model
+        d = _DescHolder(model)
+        s = TraceSettings(max_steps, candidate_capacity, weight_threshold, 0)
+        h = C.c_void_p()
+        _check(L.bv_powerfoam_splat_tracer_new(C.byref(d.desc), C.byref(s), C.byref(h)))
+        self._h = h
+
+    def deinit(self):
+        if self._h:
+            load_library().bv_powerfoam_splat_tracer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.deinit()
+        except Exception:
+            pass
+
+    @property
+    def candidate_capacity(self) -> int:
+        return load_library().bv_powerfoam_splat_tracer_candidate_capacity(self._h)
+
+    @property
+    def max_steps(self) -> int:
+        return load_library().bv_powerfoam_splat_tracer_max_steps(self._h)
+
+    @property
+    def weight_threshold(self) -> float:
+        return load_library().bv_powerfoam_splat_tracer_weight_threshold(self._h)
+
+    def set_weight_threshold(self, v: float):
+        _check(load_library().bv_powerfoam_splat_tracer_set_weight_threshold(self._h, v))
+
+    def dispatch(self, output, camera: Camera, size, stream=None):
+        w, h = size
+        cam = camera_c(camera)
+        _check(load_library().bv_powerfoam_splat_tracer_dispatch(
+            self._h, C.c_void_p(output.data_ptr()), C.byref(cam), w, h, _stream_handle(stream)))
+
+    def dispatch_batch(self, output, cameras: Sequence[Camera], size, stream=None):
+        w, h = size
+        arr = (CameraC * len(cameras))(*[camera_c(c) for c in cameras])
+        _check(load_library().bv_powerfoam_splat_tracer_dispatch_batch(
+            self._h, C.c_void_p(output.data_ptr()), arr, len(cameras), w, h,
+            _stream_handle(stream)))
+
+    def render(self, cameras: Sequence[Camera], width: int, height: int):
+        import torch
+
+        out = torch.empty((len(cameras), height, width, 4), dtype=torch.float32, device="cuda")
+        self.dispatch_batch(out, cameras, (width, height))
+        return out
+
+    def validate_candidate_counts(self) -> int:
+        """Largest support-hit count of one ray in the last dispatch; raises
+        BvError (BV_ERR_CANDIDATE_OVERFLOW) above the capacity."""
+        v = C.c_uint32()
+        _check(load_library().bv_powerfoam_splat_tracer_validate_candidate_counts(self._h,
+                                                                                 C.byref(v)))
+        return v.value
+
+    def candidate_stats(self):
+        """(max support hits of one ray, total hits, Cech row entries of the
+        hit supports) over the last dispatch's rays."""
+        mx, tot, ent = C.c_uint32(), C.c_uint64(), C.c_uint64()
+        _check(load_library().bv_powerfoam_splat_tracer_candidate_stats(
+            self._h, C.byref(mx), C.byref(tot), C.byref(ent)))
+        return mx.value, tot.value, ent.value
+
+    def enable_stats(self, enabled: bool = True):
+        _check(load_library().bv_powerfoam_splat_tracer_enable_stats(self._h, 1 if enabled else 0))
+
+    def last_stats(self) -> LaunchStats:
+        st = LaunchStats()
+        _check(load_library().bv_powerfoam_splat_tracer_last_stats(self._h, C.byref(st)))
+        return st
 
 
 def _host_ptr(a) -> int:

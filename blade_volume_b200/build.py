@@ -41,7 +41,8 @@ def sources():
 
 
 def headers():
-    return sorted(glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(INCLUDE, "*.h")))
+    return sorted(glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
+                  glob.glob(os.path.join(INCLUDE, "*.h")))
 
 
 def stale() -> bool:

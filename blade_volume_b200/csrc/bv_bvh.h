@@ -1,0 +1,169 @@
+// Host-built bounding volume hierarchy shared by the Gaussian relight tracer
+// and the PowerFoam splat tracer: primitives are sorted by the 30-bit Morton
+// code of their centres, then split top-down where the highest differing
+// code bit flips (median split when all codes agree or past depth 40).
+// Leaves hold at most kBvhLeaf consecutive primitives of the sorted order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace bv {
+
+// Two child boxes per node (64 B).  .w of lo = child reference (node index
+// or first primitive), .w of hi = primitive count (0: internal node,
+// 0xffffffff: no child).
+struct __align__(16) BvhNode {
+    float4 l_lo, l_hi, r_lo, r_hi;
+};
+
+constexpr uint32_t kBvhLeaf = 4;
+constexpr uint32_t kBvhNoChild = 0xffffffffu;
+
+struct BvhBox {
+    float lo[3], hi[3];
+};
+
+inline void bvh_grow(BvhBox &b, const BvhBox &o) {
+    for (int k = 0; k < 3; ++k) {
+        b.lo[k] = std::min(b.lo[k], o.lo[k]);
+        b.hi[k] = std::max(b.hi[k], o.hi[k]);
+    }
+}
+
+// The result of a build: nodes (root first) and the primitive order the
+// leaves refer to (order[i] = input index of the i-th sorted primitive).
+struct BvhBuild {
+    std::vector<BvhNode> nodes;
+    std::vector<uint32_t> order;
+};
+
+namespace bvh_detail {
+
+inline uint32_t spread10(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+struct Builder {
+    const std::vector<uint32_t> &codes;
+    const std::vector<BvhBox> &boxes;  // in sorted order
+    std::vector<BvhNode> nodes;
+
+    Builder(const std::vector<uint32_t> &c, const std::vector<BvhBox> &b) : codes(c), boxes(b) {}
+
+    BvhBox range_box(uint32_t b, uint32_t e) const {
+        BvhBox r = boxes[b];
+        for (uint32_t i = b + 1; i < e; ++i) bvh_grow(r, boxes[i]);
+        return r;
+    }
+
+    uint32_t split(uint32_t b, uint32_t e, int depth) const {
+        const uint32_t first = codes[b], last = codes[e - 1];
+        if (first == last || depth > 40) return b + (e - b) / 2;
+        const int bit = 31 - __builtin_clz(first ^ last);
+        const uint32_t mask = 1u << bit;
+        uint32_t lo = b, hi = e - 1;  // first index whose code has the bit set
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            if (codes[mid] & mask)
+                hi = mid;
+            else
+                lo = mid + 1;
+        }
+        return lo;
+    }
+
+    static void set_child(float4 &lo, float4 &hi, const BvhBox &bx, uint32_t ref, uint32_t count) {
+        float rf, cf;
+        std::memcpy(&rf, &ref, 4);
+        std::memcpy(&cf, &count, 4);
+        lo = make_float4(bx.lo[0], bx.lo[1], bx.lo[2], rf);
+        hi = make_float4(bx.hi[0], bx.hi[1], bx.hi[2], cf);
+    }
+
+    // Node for range [b, e) with e - b > kBvhLeaf; returns its index.
+    uint32_t build(uint32_t b, uint32_t e, int depth) {
+        const uint32_t me = (uint32_t)nodes.size();
+        nodes.push_back(BvhNode{});
+        uint32_t m = split(b, e, depth);
+        if (m <= b || m >= e) m = b + (e - b) / 2;
+        const uint32_t rb[2] = {b, m}, re[2] = {m, e};
+        for (int c = 0; c < 2; ++c) {
+            const BvhBox bx = range_box(rb[c], re[c]);
+            float4 lo, hi;
+            if (re[c] - rb[c] <= kBvhLeaf) {
+                set_child(lo, hi, bx, rb[c], re[c] - rb[c]);
+            } else {
+                const uint32_t child = build(rb[c], re[c], depth + 1);
+                set_child(lo, hi, bx, child, 0u);
+            }
+            if (c == 0) {
+                nodes[me].l_lo = lo;
+                nodes[me].l_hi = hi;
+            } else {
+                nodes[me].r_lo = lo;
+                nodes[me].r_hi = hi;
+            }
+        }
+        return me;
+    }
+};
+
+}  // namespace bvh_detail
+
+// Builds the hierarchy over `boxes` (one per primitive, n >= 1) with Morton
+// codes of `centers` ([n][3]) quantised to 1024 steps per axis of the scene
+// box.
+inline BvhBuild build_bvh(const std::vector<BvhBox> &boxes, const std::vector<float> &centers) {
+    const uint32_t n = (uint32_t)boxes.size();
+    BvhBox scene = boxes[0];
+    for (uint32_t i = 1; i < n; ++i) bvh_grow(scene, boxes[i]);
+    const float ext[3] = {std::max(scene.hi[0] - scene.lo[0], 1e-20f),
+                          std::max(scene.hi[1] - scene.lo[1], 1e-20f),
+                          std::max(scene.hi[2] - scene.lo[2], 1e-20f)};
+    std::vector<uint64_t> keyed(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t c[3];
+        for (int k = 0; k < 3; ++k) {
+            const float u = (centers[3 * (size_t)i + k] - scene.lo[k]) / ext[k];
+            c[k] = (uint32_t)std::min(std::max(u * 1024.0f, 0.0f), 1023.0f);
+        }
+        const uint32_t code = (bvh_detail::spread10(c[0]) << 2) | (bvh_detail::spread10(c[1]) << 1) |
+                              bvh_detail::spread10(c[2]);
+        keyed[i] = ((uint64_t)code << 32) | i;
+    }
+    std::sort(keyed.begin(), keyed.end());
+    BvhBuild out;
+    out.order.resize(n);
+    std::vector<uint32_t> codes(n);
+    std::vector<BvhBox> sorted(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        out.order[i] = (uint32_t)(keyed[i] & 0xffffffffu);
+        codes[i] = (uint32_t)(keyed[i] >> 32);
+        sorted[i] = boxes[out.order[i]];
+    }
+    bvh_detail::Builder b(codes, sorted);
+    if (n <= kBvhLeaf) {
+        BvhNode root;
+        bvh_detail::Builder::set_child(root.l_lo, root.l_hi, b.range_box(0, n), 0u, n);
+        const BvhBox empty{{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        bvh_detail::Builder::set_child(root.r_lo, root.r_hi, empty, 0u, kBvhNoChild);
+        b.nodes.push_back(root);
+    } else {
+        b.build(0, n, 0);
+    }
+    out.nodes = std::move(b.nodes);
+    return out;
+}
+
+}  // namespace bv

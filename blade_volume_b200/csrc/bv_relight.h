@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include "blade_volume_b200.h"
+#include "bv_bvh.h"
 
 namespace bv {
 
@@ -16,13 +17,6 @@ struct __align__(16) GaussPrim {
     float4 scale_support;   // scale, support^2 = 2 ln(opacity / 0.03)
     float4 normal_radius;   // PBR normal, surfel radius 3 cbrt(sx sy sz)
     uint4 ids;              // filtered index, material, 0, 0
-};
-
-// Two child boxes per node (64 B).  .w of lo = child reference (node index
-// or first particle), .w of hi = particle count (0: internal node,
-// 0xffffffff: no child).
-struct __align__(16) BvhNode {
-    float4 l_lo, l_hi, r_lo, r_hi;
 };
 
 struct RelightLight {  // PointLight (relight.rs:176-181)

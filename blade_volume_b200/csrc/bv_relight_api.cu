@@ -90,97 +90,6 @@ bv_status validate_gaussians(const bv_gaussian_desc *g) {
     return BV_OK;
 }
 
-struct Box {
-    float lo[3], hi[3];
-};
-
-inline void grow(Box &b, const Box &o) {
-    for (int k = 0; k < 3; ++k) {
-        b.lo[k] = std::min(b.lo[k], o.lo[k]);
-        b.hi[k] = std::max(b.hi[k], o.hi[k]);
-    }
-}
-
-inline uint32_t spread10(uint32_t v) {
-    v &= 0x3ffu;
-    v = (v | (v << 16)) & 0x030000FFu;
-    v = (v | (v << 8)) & 0x0300F00Fu;
-    v = (v | (v << 4)) & 0x030C30C3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
-}
-
-// Top-down build over Morton-sorted particles: split where the highest bit
-// differing across the range flips (median split when all codes agree or
-// the tree gets deep).  Leaves hold at most kLeaf particles.
-struct BvhBuilder {
-    static constexpr uint32_t kLeaf = 4;
-    const std::vector<uint32_t> &codes;
-    const std::vector<Box> &boxes;  // in sorted order
-    std::vector<BvhNode> nodes;
-
-    BvhBuilder(const std::vector<uint32_t> &c, const std::vector<Box> &b) : codes(c), boxes(b) {}
-
-    Box range_box(uint32_t b, uint32_t e) const {
-        Box r = boxes[b];
-        for (uint32_t i = b + 1; i < e; ++i) grow(r, boxes[i]);
-        return r;
-    }
-
-    uint32_t split(uint32_t b, uint32_t e, int depth) const {
-        const uint32_t first = codes[b], last = codes[e - 1];
-        if (first == last || depth > 40) return b + (e - b) / 2;
-        const int bit = 31 - __builtin_clz(first ^ last);
-        const uint32_t mask = 1u << bit;
-        // first index whose code has the bit set
-        uint32_t lo = b, hi = e - 1;
-        while (lo < hi) {
-            const uint32_t mid = lo + (hi - lo) / 2;
-            if (codes[mid] & mask)
-                hi = mid;
-            else
-                lo = mid + 1;
-        }
-        return lo;
-    }
-
-    static void set_child(float4 &lo, float4 &hi, const Box &bx, uint32_t ref, uint32_t count) {
-        uint32_t r = ref, c = count;
-        float rf, cf;
-        std::memcpy(&rf, &r, 4);
-        std::memcpy(&cf, &c, 4);
-        lo = make_float4(bx.lo[0], bx.lo[1], bx.lo[2], rf);
-        hi = make_float4(bx.hi[0], bx.hi[1], bx.hi[2], cf);
-    }
-
-    // Builds the node for range [b, e) (e - b > kLeaf) and returns its index.
-    uint32_t build(uint32_t b, uint32_t e, int depth) {
-        const uint32_t me = (uint32_t)nodes.size();
-        nodes.push_back(BvhNode{});
-        uint32_t m = split(b, e, depth);
-        if (m <= b || m >= e) m = b + (e - b) / 2;
-        const uint32_t rb[2] = {b, m}, re[2] = {m, e};
-        for (int c = 0; c < 2; ++c) {
-            const Box bx = range_box(rb[c], re[c]);
-            float4 lo, hi;
-            if (re[c] - rb[c] <= kLeaf) {
-                set_child(lo, hi, bx, rb[c], re[c] - rb[c]);
-            } else {
-                const uint32_t child = build(rb[c], re[c], depth + 1);
-                set_child(lo, hi, bx, child, 0u);
-            }
-            if (c == 0) {
-                nodes[me].l_lo = lo;
-                nodes[me].l_hi = hi;
-            } else {
-                nodes[me].r_lo = lo;
-                nodes[me].r_hi = hi;
-            }
-        }
-        return me;
-    }
-};
-
 }  // namespace
 
 extern "C" {
@@ -201,10 +110,10 @@ bv_status bv_relight_tracer_new_gaussian(const bv_gaussian_desc *g,
 
     // prepare_geometry (gpu/relight.rs:205-246): opacity > 0.03 only
     std::vector<GaussPrim> prims;
-    std::vector<Box> boxes;
+    std::vector<BvhBox> boxes;
+    std::vector<float> centers;
     prims.reserve(g->num_points);
     boxes.reserve(g->num_points);
-    Box scene{{INFINITY, INFINITY, INFINITY}, {-INFINITY, -INFINITY, -INFINITY}};
     uint32_t kept = 0;
     for (uint32_t i = 0; i < g->num_points; ++i) {
         const float *p = g->points + 4 * (size_t)i;
@@ -227,7 +136,7 @@ bv_status bv_relight_tracer_new_gaussian(const bv_gaussian_desc *g,
                                 {2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)},
                                 {2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)}};
         const double sup = std::sqrt(std::max((double)support_sq, 0.0));
-        Box bx;
+        BvhBox bx;
         for (int k = 0; k < 3; ++k) {
             double e2 = 0.0;
             for (int j = 0; j < 3; ++j) {
@@ -239,53 +148,21 @@ bv_status bv_relight_tracer_new_gaussian(const bv_gaussian_desc *g,
             bx.hi[k] = std::nextafter((float)((double)p[k] + ext), INFINITY);
         }
         boxes.push_back(bx);
-        grow(scene, bx);
+        centers.insert(centers.end(), {p[0], p[1], p[2]});
         kept += 1;
     }
     if (kept == 0)
         return rfail(BV_ERR_INVALID_MODEL, "PBR Gaussian geometry has no particles above alpha 0.03");
 
-    // Morton order of the particle centres
-    std::vector<uint64_t> keyed(kept);
-    const float ext[3] = {std::max(scene.hi[0] - scene.lo[0], 1e-20f),
-                          std::max(scene.hi[1] - scene.lo[1], 1e-20f),
-                          std::max(scene.hi[2] - scene.lo[2], 1e-20f)};
-    for (uint32_t i = 0; i < kept; ++i) {
-        uint32_t c[3];
-        for (int k = 0; k < 3; ++k) {
-            const float u = (prims[i].center_opacity.x * (k == 0) + prims[i].center_opacity.y * (k == 1) +
-                             prims[i].center_opacity.z * (k == 2) - scene.lo[k]) / ext[k];
-            c[k] = (uint32_t)std::min(std::max(u * 1024.0f, 0.0f), 1023.0f);
-        }
-        const uint32_t code = (spread10(c[0]) << 2) | (spread10(c[1]) << 1) | spread10(c[2]);
-        keyed[i] = ((uint64_t)code << 32) | i;
-    }
-    std::sort(keyed.begin(), keyed.end());
-    std::vector<uint32_t> codes(kept);
-    std::vector<Box> sorted_boxes(kept);
+    // BVH over the support boxes, particles stored in leaf order
+    BvhBuild bvh = build_bvh(boxes, centers);
     std::vector<GaussPrim> sorted_prims(kept);
-    for (uint32_t i = 0; i < kept; ++i) {
-        const uint32_t src = (uint32_t)(keyed[i] & 0xffffffffu);
-        codes[i] = (uint32_t)(keyed[i] >> 32);
-        sorted_boxes[i] = boxes[src];
-        sorted_prims[i] = prims[src];
-    }
-    BvhBuilder builder(codes, sorted_boxes);
-    if (kept <= BvhBuilder::kLeaf) {
-        BvhNode root;
-        const Box bx = builder.range_box(0, kept);
-        BvhBuilder::set_child(root.l_lo, root.l_hi, bx, 0u, kept);
-        const Box empty{{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-        BvhBuilder::set_child(root.r_lo, root.r_hi, empty, 0u, 0xffffffffu);  // empty child
-        builder.nodes.push_back(root);
-    } else {
-        builder.build(0, kept, 0);
-    }
+    for (uint32_t i = 0; i < kept; ++i) sorted_prims[i] = prims[bvh.order[i]];
 
     bv_relight_tracer *t = new bv_relight_tracer();
     t->n_input = g->num_points;
     t->n_kept = kept;
-    t->n_nodes = (uint32_t)builder.nodes.size();
+    t->n_nodes = (uint32_t)bvh.nodes.size();
     t->n_materials = g->num_materials;
     std::vector<RelightMaterial> mats(g->num_materials);
     for (uint32_t m = 0; m < g->num_materials; ++m) {
@@ -309,7 +186,7 @@ bv_status bv_relight_tracer_new_gaussian(const bv_gaussian_desc *g,
     BV_RTRY(cudaMalloc(&t->stats, sizeof(unsigned long long) * 4), "cudaMalloc stats");
     BV_RTRY(cudaMemcpy(t->prims, sorted_prims.data(), sizeof(GaussPrim) * kept, cudaMemcpyHostToDevice),
             "upload particles");
-    BV_RTRY(cudaMemcpy(t->nodes, builder.nodes.data(), sizeof(BvhNode) * t->n_nodes,
+    BV_RTRY(cudaMemcpy(t->nodes, bvh.nodes.data(), sizeof(BvhNode) * t->n_nodes,
                        cudaMemcpyHostToDevice), "upload nodes");
     BV_RTRY(cudaMemcpy(t->materials, mats.data(), sizeof(RelightMaterial) * mats.size(),
                        cudaMemcpyHostToDevice), "upload materials");

@@ -46,7 +46,7 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 constexpr size_t kGranule = 256;
-constexpr uint32_t kDefaultBatchRays = 4u << 20;
+constexpr uint32_t kDefaultBatchRays = 1u << 21;  // one 1920x1080 frame (2,073,600 rays)
 constexpr uint32_t kDefaultBatchViews = 256;
 constexpr uint64_t kDefaultTrainRays = 16ull * 1920 * 1080;
 

@@ -1,0 +1,675 @@
+// PowerFoam splat render on sm_100a: per ray, every support sphere the ray
+// crosses (spheres within 4 r of the camera excluded) is clipped by its Cech
+// row into [face_near, face_far] intersected with the sphere, the clipped
+// intervals are taken in (entry depth, cell) order, truncated to max_steps
+// and composited front to back.
+//
+// Restates blade-volume/src/trace.rs: powerfoam_splat_interval :1331-1389,
+// sorted_powerfoam_splat_intervals :1391-1411, trace_powerfoam_splats
+// :1456-1546 (the reference's GPU path, gpu/powerfoam_splat.rs:51-343,
+// records bounded candidate rows and sorts them).  Here a BVH over the
+// support spheres is walked front to back in windows of kSplatWindow
+// intervals: a pass keeps the kSplatWindow smallest (t, cell) keys above the
+// cursor, pruning boxes and spheres that end at or before the cursor or
+// start after the window's last key, so there is no per-ray candidate
+// scratch and no capacity to overflow.  The order equals the full sort, so
+// the image is the oracle's bit for bit (-fmad=false; every expression is
+// the CPU restatement's sequence of IEEE-rounded operations).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "bv_bvh.h"
+#include "bv_device.cuh"
+#include "bv_internal.h"
+
+namespace bv {
+namespace {
+
+constexpr int kSplatBlock = 128;
+constexpr int kSplatWindow = 16;
+constexpr int kSplatStack = 80;  // > BVH depth (40 + log2(N / 4))
+
+// One support sphere in BVH leaf order, 32 B.
+struct __align__(16) SplatPrim {
+    float4 site;  // x, y, z, power radius
+    uint4 link;   // cell (model index), Cech row begin, row end, 0
+};
+
+struct SplatParams {
+    DeviceModel m;                 // density, SH rows (model order)
+    const SplatPrim *prims;        // [N] leaf order
+    const BvhNode *nodes;
+    const float4 *row_sites;       // [M] CSR order: the neighbour's x, y, z, radius
+    uint32_t max_steps;
+    float weight_threshold;
+    uint32_t n_views;
+    uint32_t total_work;
+    float4 *out;                   // [n_views][H][W]
+    unsigned long long *stats;     // [3] rays, composited intervals, Cech entries clipped (or null)
+    uint32_t *max_candidates;      // counting pass: max over rays of the support hits
+    unsigned long long *count_totals;  // counting pass: [2] support hits, their Cech row entries
+    uint32_t count_only;
+    ViewDesc views[kMaxViewsPerLaunch];
+};
+
+struct SplatKey {
+    float t;
+    float dt;
+    uint32_t cell;
+};
+
+__device__ __forceinline__ bool key_less(float ta, uint32_t ia, float tb, uint32_t ib) {
+    return ta < tb || (ta == tb && ia < ib);
+}
+
+// 1/d with |d| raised to at least 1e-30, so that a box face through the ray
+// origin gives 0 * finite rather than 0 * inf = NaN in the slab test.
+__device__ __forceinline__ float safe_inverse(float d) {
+    return 1.0f / (fabsf(d) < 1e-30f ? copysignf(1e-30f, d) : d);
+}
+
+// Slab test of a box against the ray within [0, t_end], widened by a small
+// relative margin so that FP32 rounding can only keep a box, never drop one.
+__device__ __forceinline__ bool slab(const float4 &lo, const float4 &hi, const Ray &r, float ix,
+                                     float iy, float iz, float t_end, float &tn, float &tf) {
+    const float ax = (lo.x - r.ox) * ix, bx = (hi.x - r.ox) * ix;
+    const float ay = (lo.y - r.oy) * iy, by = (hi.y - r.oy) * iy;
+    const float az = (lo.z - r.oz) * iz, bz = (hi.z - r.oz) * iz;
+    tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
+    tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), t_end));
+    tn = tn - (1e-5f * fabsf(tn) + 1e-6f);
+    tf = tf + (1e-5f * fabsf(tf) + 1e-6f);
+    return tn <= tf;
+}
+
+// Support-sphere test of powerfoam_splat_interval (trace.rs:1331-1350):
+// false when the camera is within 4 r of the site, the ray misses the sphere,
+// or the sphere lies behind the camera or beyond depth.
+__device__ __forceinline__ bool splat_sphere(const Ray &ray, const float4 &s, float depth,
+                                             float &sn, float &sf) {
+    const float cx = s.x - ray.ox, cy = s.y - ray.oy, cz = s.z - ray.oz;
+    const float excl = 4.0f * s.w;
+    if (dot3(cx, cy, cz, cx, cy, cz) < excl * excl) return false;
+    const float ocx = ray.ox - s.x, ocy = ray.oy - s.y, ocz = ray.oz - s.z;
+    const float b = dot3(ocx, ocy, ocz, ray.dx, ray.dy, ray.dz);
+    const float disc = b * b - (dot3(ocx, ocy, ocz, ocx, ocy, ocz) - s.w * s.w);
+    if (disc <= 0.0f || !isfinite(disc)) return false;
+    const float root = sqrtf(disc);
+    sn = -b - root;
+    sf = -b + root;
+    return !(sf <= 0.0f || sn >= depth);
+}
+
+// Cech-row clip of one support (trace.rs:1351-1389, path_interval_jacobian
+// :1199-1325 for the bounded clip).  False when the interval is empty.
+__device__ __forceinline__ bool splat_clip(const SplatParams &P, const Ray &ray, const float4 &s,
+                                           uint32_t begin, uint32_t end, float depth, float sn,
+                                           float sf, float &start, float &dt) {
+    float face_near = 0.0f, face_far = depth;
+    for (uint32_t k = begin; k < end; ++k) {
+        const float4 a = __ldg(P.row_sites + k);
+        const float nx = a.x - s.x, ny = a.y - s.y, nz = a.z - s.z;
+        const float dsq = fmaxf(dot3(nx, ny, nz, nx, ny, nz), 1.0e-20f);
+        const float shift = 0.5f + 0.5f * (s.w * s.w - a.w * a.w) / dsq;
+        const float fx = s.x + shift * nx, fy = s.y + shift * ny, fz = s.z + shift * nz;
+        const float rx = fx - ray.ox, ry = fy - ray.oy, rz = fz - ray.oz;
+        const float num = dot3(rx, ry, rz, nx, ny, nz);
+        const float den = dot3(ray.dx, ray.dy, ray.dz, nx, ny, nz);
+        if (den > 1.0e-20f) {
+            const float t = num / den;
+            if (t < face_far) face_far = t;
+        } else if (den < -1.0e-20f) {
+            const float t = num / den;
+            if (t > face_near) face_near = t;
+        } else if (num < 0.0f) {
+            return false;
+        }
+    }
+    float st = face_near, en = face_far;
+    if (sn > st) st = sn;
+    if (sf < en) en = sf;
+    if (en <= st || !isfinite(st) || !isfinite(en)) return false;
+    start = st;
+    dt = en - st;
+    return true;
+}
+
+template <int DEG, bool BF16>
+__global__ void __launch_bounds__(kSplatBlock)
+splat_kernel(const __grid_constant__ SplatParams P) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= P.total_work) return;
+    uint32_t view = 0;
+    while (view + 1 < P.n_views && w >= P.views[view + 1].ray_begin) ++view;
+    const ViewDesc &vd = P.views[view];
+    const uint32_t local = w - vd.ray_begin;
+    const uint32_t tile = local / kTileRays, in = local % kTileRays;
+    const uint32_t x = (tile % vd.tiles_x) * kTileW + in % kTileW;
+    const uint32_t y = (tile / vd.tiles_x) * kTileH + in / kTileW;
+    if (x >= vd.width || y >= vd.height) return;
+    float4 *out = P.out + (size_t)vd.pixel_begin + (size_t)y * vd.width + x;
+    Ray ray;
+    if (!make_ray(vd, x, y, ray)) {
+        if (!P.count_only) *out = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const float ix = safe_inverse(ray.dx), iy = safe_inverse(ray.dy), iz = safe_inverse(ray.dz);
+    const float depth = vd.depth;
+    uint32_t clipped = 0;
+
+    if (P.count_only) {
+        // every support hit, no window pruning
+        uint32_t hits = 0, entries = 0;
+        uint32_t stack[kSplatStack];
+        int sp = 0;
+        stack[sp++] = 0u;
+        while (sp > 0) {
+            const BvhNode nd = P.nodes[stack[--sp]];
+            const float4 lo[2] = {nd.l_lo, nd.r_lo}, hi[2] = {nd.l_hi, nd.r_hi};
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const uint32_t cnt = __float_as_uint(hi[c].w);
+                float tn, tf;
+                if (cnt == kBvhNoChild || !slab(lo[c], hi[c], ray, ix, iy, iz, depth, tn, tf)) continue;
+                const uint32_t ref = __float_as_uint(lo[c].w);
+                if (cnt == 0u) {
+                    if (sp < kSplatStack) stack[sp++] = ref;
+                    continue;
+                }
+                for (uint32_t p = ref; p < ref + cnt; ++p) {
+                    float sn, sf;
+                    if (!splat_sphere(ray, __ldg(&P.prims[p].site), depth, sn, sf)) continue;
+                    const uint4 link = __ldg(&P.prims[p].link);
+                    hits += 1;
+                    entries += link.z - link.y;
+                }
+            }
+        }
+        atomicMax(P.max_candidates, hits);
+        atomicAdd(P.count_totals + 0, (unsigned long long)hits);
+        atomicAdd(P.count_totals + 1, (unsigned long long)entries);
+        return;
+    }
+
+    float T = 1.0f, ar = 0.f, ag = 0.f, ab = 0.f;
+    uint32_t steps = 0;
+    bool cursor_valid = false, done = false;
+    float cur_t = 0.f;
+    uint32_t cur_cell = 0;
+    while (!done) {
+        // ---- the next window of keys above the cursor
+        SplatKey buf[kSplatWindow];
+        int count = 0;
+        uint32_t stack[kSplatStack];
+        int sp = 0;
+        stack[sp++] = 0u;
+        while (sp > 0) {
+            const BvhNode nd = P.nodes[stack[--sp]];
+            const float4 lo[2] = {nd.l_lo, nd.r_lo}, hi[2] = {nd.l_hi, nd.r_hi};
+            float tn[2], tf[2];
+            bool ok[2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                ok[c] = __float_as_uint(hi[c].w) != kBvhNoChild &&
+                        slab(lo[c], hi[c], ray, ix, iy, iz, depth, tn[c], tf[c]);
+                if (ok[c] && cursor_valid && tf[c] < cur_t) ok[c] = false;
+                if (ok[c] && count == kSplatWindow && tn[c] > buf[kSplatWindow - 1].t) ok[c] = false;
+            }
+            const int first = (ok[0] && ok[1] && tn[1] < tn[0]) ? 1 : 0;
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int c = k == 0 ? 1 - first : first;
+                if (!ok[c]) continue;
+                const uint32_t ref = __float_as_uint(lo[c].w);
+                const uint32_t cnt = __float_as_uint(hi[c].w);
+                if (cnt == 0u) {
+                    if (sp < kSplatStack) stack[sp++] = ref;
+                    continue;
+                }
+                for (uint32_t p = ref; p < ref + cnt; ++p) {
+                    const float4 s = __ldg(&P.prims[p].site);
+                    float sn, sf;
+                    if (!splat_sphere(ray, s, depth, sn, sf)) continue;
+                    // the clipped start lies in [sn, sf): skip supports whose
+                    // every key is at or below the cursor or above the window
+                    if (cursor_valid && sf <= cur_t) continue;
+                    if (count == kSplatWindow && sn > buf[kSplatWindow - 1].t) continue;
+                    const uint4 link = __ldg(&P.prims[p].link);
+                    clipped += link.z - link.y;
+                    float st, dt;
+                    if (!splat_clip(P, ray, s, link.y, link.z, depth, sn, sf, st, dt)) continue;
+                    if (cursor_valid && !key_less(cur_t, cur_cell, st, link.x)) continue;
+                    if (count == kSplatWindow &&
+                        !key_less(st, link.x, buf[kSplatWindow - 1].t, buf[kSplatWindow - 1].cell))
+                        continue;
+                    SplatKey nk{st, dt, link.x};
+#pragma unroll
+                    for (int i = 0; i < kSplatWindow; ++i) {
+                        if (i < count && key_less(nk.t, nk.cell, buf[i].t, buf[i].cell)) {
+                            const SplatKey tmp = buf[i];
+                            buf[i] = nk;
+                            nk = tmp;
+                        }
+                    }
+#pragma unroll
+                    for (int i = 0; i < kSplatWindow; ++i)
+                        if (i == count) buf[i] = nk;
+                    if (count < kSplatWindow) count += 1;
+                }
+            }
+        }
+        // ---- composite the window in order (trace.rs:1490-1530)
+#pragma unroll 1
+        for (int i = 0; i < count; ++i) {
+            SplatKey e = buf[0];
+#pragma unroll
+            for (int j = 0; j < kSplatWindow; ++j)
+                if (j == i) e = buf[j];
+            if (T <= P.weight_threshold || steps >= P.max_steps) {
+                done = true;
+                break;
+            }
+            steps += 1;
+            const float dens = __ldg(P.m.density + e.cell) * 1.0f;
+            if (dens <= 1.0e-6f) continue;
+            const float alpha = 1.0f - bv_expf(-dens * e.dt);
+            const float wgt = T * alpha;
+            float coef[ShDims<DEG>::N];
+            load_sh_row<DEG, BF16>(P.m, e.cell, coef);
+            float r, g, b;
+            eval_sh<DEG>(coef, ray.dx, ray.dy, ray.dz, r, g, b);
+            ar += wgt * fmaxf(r, 0.0f);
+            ag += wgt * fmaxf(g, 0.0f);
+            ab += wgt * fmaxf(b, 0.0f);
+            T *= 1.0f - alpha;
+        }
+        if (count < kSplatWindow) break;
+        cursor_valid = true;
+        cur_t = buf[kSplatWindow - 1].t;
+        cur_cell = buf[kSplatWindow - 1].cell;
+    }
+    *out = make_float4(ar, ag, ab, 1.0f - T);
+    if (P.stats) {
+        atomicAdd(P.stats + 0, 1ull);
+        atomicAdd(P.stats + 1, (unsigned long long)steps);
+        atomicAdd(P.stats + 2, (unsigned long long)clipped);
+    }
+}
+
+cudaError_t launch_splat(const SplatParams &p, cudaStream_t s) {
+    const int blocks = (int)((p.total_work + kSplatBlock - 1) / kSplatBlock);
+    if (blocks == 0) return cudaSuccess;
+    const int key = (int)p.m.sh_degree * 2 + (p.m.sh_bf16 ? 1 : 0);
+    switch (key) {
+        case 0: splat_kernel<0, false><<<blocks, kSplatBlock, 0, s>>>(p); break;
+        case 1: splat_kernel<0, true><<<blocks, kSplatBlock, 0, s>>>(p); break;
+        case 2: splat_kernel<1, false><<<blocks, kSplatBlock, 0, s>>>(p); break;
+        case 3: splat_kernel<1, true><<<blocks, kSplatBlock, 0, s>>>(p); break;
+        case 4: splat_kernel<2, false><<<blocks, kSplatBlock, 0, s>>>(p); break;
+        case 5: splat_kernel<2, true><<<blocks, kSplatBlock, 0, s>>>(p); break;
+        case 6: splat_kernel<3, false><<<blocks, kSplatBlock, 0, s>>>(p); break;
+        case 7: splat_kernel<3, true><<<blocks, kSplatBlock, 0, s>>>(p); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+bv_status sp_fail(bv_status code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    set_last_error(buf);
+    return code;
+}
+
+bv_status sp_cuda(cudaError_t e, const char *what) {
+    return sp_fail(e == cudaErrorMemoryAllocation ? BV_ERR_OUT_OF_MEMORY : BV_ERR_CUDA, "%s: %s",
+                   what, cudaGetErrorString(e));
+}
+
+#define SP_CUDA(call, what)                              \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return sp_cuda(e_, what); \
+    } while (0)
+
+}  // namespace
+}  // namespace bv
+
+using namespace bv;
+
+struct bv_splat_tracer {
+    uint32_t n = 0, m_edges = 0, sh_degree = 0, sh_stride = 0, n_nodes = 0;
+    bool bf16 = false;
+    bv_trace_settings settings{};
+    uint32_t capacity = 0;
+    // device
+    SplatPrim *prims = nullptr;
+    BvhNode *nodes = nullptr;
+    float4 *row_sites = nullptr;
+    float *density = nullptr;
+    void *sh = nullptr;
+    unsigned long long *stats = nullptr;
+    uint32_t *max_candidates = nullptr;
+    unsigned long long *count_totals = nullptr;
+    // last dispatch (for the candidate count and stats)
+    std::vector<bv_camera> last_cams;
+    uint32_t last_w = 0, last_h = 0;
+    cudaStream_t last_stream = nullptr;
+    bool stats_enabled = false, last_has_stats = false;
+    uint32_t last_launches = 0;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+
+    DeviceModel model() const {
+        DeviceModel m;
+        std::memset(&m, 0, sizeof(m));
+        m.density = density;
+        m.sh = sh;
+        m.n = n;
+        m.sh_degree = sh_degree;
+        m.sh_stride = sh_stride;
+        m.sh_bf16 = bf16 ? 1u : 0u;
+        m.bounded = 1u;
+        return m;
+    }
+};
+
+namespace {
+
+void free_splat(bv_splat_tracer *t) {
+    if (!t) return;
+    cudaFree(t->prims);
+    cudaFree(t->nodes);
+    cudaFree(t->row_sites);
+    cudaFree(t->density);
+    cudaFree(t->sh);
+    cudaFree(t->stats);
+    cudaFree(t->max_candidates);
+    cudaFree(t->count_totals);
+    for (auto &e : t->ev)
+        if (e) cudaEventDestroy(e);
+    delete t;
+}
+
+uint16_t bf16_rne(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40u);
+    return (uint16_t)((u + ((u >> 16) & 1u) + 0x7fffu) >> 16);
+}
+
+// Enqueues the splat kernel for the cameras (chunks of kMaxViewsPerLaunch).
+bv_status enqueue_splats(bv_splat_tracer *t, float4 *out, const bv_camera *cams, uint32_t n,
+                         uint32_t w, uint32_t h, bool count_only, cudaStream_t s) {
+    for (uint32_t c0 = 0; c0 < n; c0 += kMaxViewsPerLaunch) {
+        const uint32_t nc = std::min<uint32_t>(kMaxViewsPerLaunch, n - c0);
+        SplatParams p;
+        std::memset(&p, 0, sizeof(p));
+        p.m = t->model();
+        p.prims = t->prims;
+        p.nodes = t->nodes;
+        p.row_sites = t->row_sites;
+        p.max_steps = t->settings.max_steps;
+        p.weight_threshold = t->settings.weight_threshold;
+        p.n_views = nc;
+        uint32_t work = 0;
+        for (uint32_t v = 0; v < nc; ++v) {
+            p.views[v] = view_desc(cams[c0 + v], w, h, work, (uint64_t)v * w * h);
+            work += tile_padded_rays(w, h);
+        }
+        p.total_work = work;
+        p.out = out ? out + (size_t)c0 * w * h : nullptr;
+        p.stats = (t->stats_enabled && !count_only) ? t->stats : nullptr;
+        p.max_candidates = t->max_candidates;
+        p.count_totals = t->count_totals;
+        p.count_only = count_only ? 1u : 0u;
+        SP_CUDA(launch_splat(p, s), "splat launch");
+        t->last_launches += 1;
+    }
+    return BV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *md, const bv_trace_settings *settings,
+                                        bv_splat_tracer **out) {
+    if (!out) return sp_fail(BV_ERR_INVALID_ARGUMENT, "out handle pointer is null");
+    *out = nullptr;
+    if (!md) return sp_fail(BV_ERR_INVALID_ARGUMENT, "null model");
+    if (!md->radii) return sp_fail(BV_ERR_INVALID_ARGUMENT, "PowerFoam splat tracer requires radii");
+    bv_trace_settings ts{};
+    if (settings) {
+        ts = *settings;
+    } else {
+        ts.max_steps = 1024;
+        ts.weight_threshold = 0.001f;
+    }
+    if (ts.max_steps == 0) return sp_fail(BV_ERR_INVALID_ARGUMENT, "PowerFoam splat max_steps must be non-zero");
+    if (ts.debug_cell_density)
+        return sp_fail(BV_ERR_INVALID_ARGUMENT, "PowerFoam splat tracer has no cell-density debug mode");
+    if (bv_model_validate(md, nullptr, 0) != BV_OK) return BV_ERR_INVALID_MODEL;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return sp_fail(BV_ERR_NO_DEVICE, "no CUDA device");
+
+    const uint32_t n = md->num_points, m_edges = md->adjacency_offsets[n];
+    const uint32_t deg = md->sh_degree > 3 ? 3 : md->sh_degree;
+    const uint32_t nsh = 3 * (deg + 1) * (deg + 1);
+    const bool bf16 = (md->flags & BV_MODEL_SH_BF16) != 0;
+    const uint32_t align = bf16 ? 8u : 4u;
+    const uint32_t stride = (nsh + align - 1) / align * align;
+
+    // supports: conservative boxes, Morton-ordered BVH
+    std::vector<BvhBox> boxes(n);
+    std::vector<float> centers(3 * (size_t)n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *p = md->points + 4 * (size_t)i;
+        const double r = std::max((double)md->radii[i], 0.0);
+        for (int k = 0; k < 3; ++k) {
+            const double ext = r * (1.0 + 1e-4) + 1e-6 * (1.0 + std::fabs((double)p[k]));
+            boxes[i].lo[k] = std::nextafter((float)((double)p[k] - ext), -INFINITY);
+            boxes[i].hi[k] = std::nextafter((float)((double)p[k] + ext), INFINITY);
+            centers[3 * (size_t)i + k] = p[k];
+        }
+    }
+    BvhBuild bvh = build_bvh(boxes, centers);
+    std::vector<SplatPrim> prims(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t c = bvh.order[i];
+        const float *p = md->points + 4 * (size_t)c;
+        prims[i].site = make_float4(p[0], p[1], p[2], md->radii[c]);
+        prims[i].link = make_uint4(c, md->adjacency_offsets[c], md->adjacency_offsets[c + 1], 0u);
+    }
+    std::vector<float4> rows(std::max<uint32_t>(m_edges, 1));
+    for (uint32_t k = 0; k < m_edges; ++k) {
+        const uint32_t j = md->adjacency_neighbors[k];
+        const float *p = md->points + 4 * (size_t)j;
+        rows[k] = make_float4(p[0], p[1], p[2], md->radii[j]);
+    }
+    std::vector<float> dens(n);
+    for (uint32_t i = 0; i < n; ++i) dens[i] = md->points[4 * (size_t)i + 3];
+
+    bv_splat_tracer *t = new bv_splat_tracer();
+    t->n = n;
+    t->m_edges = m_edges;
+    t->sh_degree = deg;
+    t->sh_stride = stride;
+    t->bf16 = bf16;
+    t->settings = ts;
+    t->capacity = std::max(std::max(ts.max_steps > 0x3fffffffu ? 0xffffffffu : ts.max_steps * 4u, 1024u),
+                           ts.powerfoam_candidate_capacity);
+    t->n_nodes = (uint32_t)bvh.nodes.size();
+    auto cleanup = [&](cudaError_t e, const char *what) {
+        free_splat(t);
+        return sp_cuda(e, what);
+    };
+#define SP_TRY(call, what)                                \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cleanup(e_, what);  \
+    } while (0)
+    SP_TRY(cudaMalloc(&t->prims, sizeof(SplatPrim) * n), "cudaMalloc supports");
+    SP_TRY(cudaMalloc(&t->nodes, sizeof(BvhNode) * t->n_nodes), "cudaMalloc nodes");
+    SP_TRY(cudaMalloc(&t->row_sites, sizeof(float4) * rows.size()), "cudaMalloc rows");
+    SP_TRY(cudaMalloc(&t->density, sizeof(float) * n), "cudaMalloc density");
+    SP_TRY(cudaMalloc(&t->stats, sizeof(unsigned long long) * 4), "cudaMalloc stats");
+    SP_TRY(cudaMalloc(&t->max_candidates, sizeof(uint32_t)), "cudaMalloc counter");
+    SP_TRY(cudaMalloc(&t->count_totals, 2 * sizeof(unsigned long long)), "cudaMalloc counters");
+    SP_TRY(cudaMemcpy(t->prims, prims.data(), sizeof(SplatPrim) * n, cudaMemcpyHostToDevice), "upload supports");
+    SP_TRY(cudaMemcpy(t->nodes, bvh.nodes.data(), sizeof(BvhNode) * t->n_nodes, cudaMemcpyHostToDevice),
+           "upload nodes");
+    SP_TRY(cudaMemcpy(t->row_sites, rows.data(), sizeof(float4) * rows.size(), cudaMemcpyHostToDevice),
+           "upload rows");
+    SP_TRY(cudaMemcpy(t->density, dens.data(), sizeof(float) * n, cudaMemcpyHostToDevice), "upload density");
+    if (bf16) {
+        std::vector<uint16_t> row((size_t)n * stride, 0);
+        for (uint32_t i = 0; i < n; ++i)
+            for (uint32_t k = 0; k < nsh; ++k)
+                row[(size_t)i * stride + k] = bf16_rne(md->sh_coefficients[(size_t)i * nsh + k]);
+        SP_TRY(cudaMalloc(&t->sh, row.size() * 2), "cudaMalloc sh");
+        SP_TRY(cudaMemcpy(t->sh, row.data(), row.size() * 2, cudaMemcpyHostToDevice), "upload sh");
+    } else {
+        std::vector<float> row((size_t)n * stride, 0.0f);
+        for (uint32_t i = 0; i < n; ++i)
+            std::memcpy(&row[(size_t)i * stride], md->sh_coefficients + (size_t)i * nsh, nsh * 4);
+        SP_TRY(cudaMalloc(&t->sh, row.size() * 4), "cudaMalloc sh");
+        SP_TRY(cudaMemcpy(t->sh, row.data(), row.size() * 4, cudaMemcpyHostToDevice), "upload sh");
+    }
+    for (auto &e : t->ev) SP_TRY(cudaEventCreate(&e), "cudaEventCreate");
+#undef SP_TRY
+    *out = t;
+    return BV_OK;
+}
+
+void bv_powerfoam_splat_tracer_destroy(bv_splat_tracer *t) {
+    if (!t) return;
+    cudaDeviceSynchronize();
+    free_splat(t);
+}
+
+bv_status bv_powerfoam_splat_tracer_dispatch_batch(bv_splat_tracer *t, float *out_rgba_dev,
+                                                   const bv_camera *cams, uint32_t n_cams,
+                                                   uint32_t width, uint32_t height, bv_stream stream) {
+    if (!t || !out_rgba_dev || !cams) return sp_fail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    if (width == 0 || height == 0) return sp_fail(BV_ERR_INVALID_ARGUMENT, "render size must be non-zero");
+    if (n_cams == 0) return sp_fail(BV_ERR_INVALID_ARGUMENT, "no cameras");
+    if ((uint64_t)tile_padded_rays(width, height) * kMaxViewsPerLaunch >= (1ull << 32))
+        return sp_fail(BV_ERR_INVALID_ARGUMENT, "image too large");
+    for (uint32_t i = 0; i < n_cams; ++i) {
+        const bv_status st = validate_camera(cams[i]);
+        if (st != BV_OK) return st;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    t->last_cams.assign(cams, cams + n_cams);
+    t->last_w = width;
+    t->last_h = height;
+    t->last_stream = s;
+    t->last_launches = 0;
+    t->last_has_stats = t->stats_enabled;
+    if (t->stats_enabled) {
+        SP_CUDA(cudaMemsetAsync(t->stats, 0, 4 * sizeof(unsigned long long), s), "stats reset");
+        SP_CUDA(cudaEventRecord(t->ev[0], s), "event");
+    }
+    const bv_status st = enqueue_splats(t, reinterpret_cast<float4 *>(out_rgba_dev), cams, n_cams,
+                                        width, height, false, s);
+    if (st != BV_OK) return st;
+    if (t->stats_enabled) SP_CUDA(cudaEventRecord(t->ev[1], s), "event");
+    return BV_OK;
+}
+
+bv_status bv_powerfoam_splat_tracer_dispatch(bv_splat_tracer *t, float *out_rgba_dev,
+                                             const bv_camera *camera, uint32_t width, uint32_t height,
+                                             bv_stream stream) {
+    return bv_powerfoam_splat_tracer_dispatch_batch(t, out_rgba_dev, camera, 1, width, height, stream);
+}
+
+bv_status bv_powerfoam_splat_tracer_candidate_stats(bv_splat_tracer *t, uint32_t *max_hits,
+                                                    uint64_t *total_hits, uint64_t *row_entries) {
+    if (!t || !max_hits) return sp_fail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    if (t->last_cams.empty()) return sp_fail(BV_ERR_INVALID_ARGUMENT, "no dispatch to count");
+    cudaStream_t s = t->last_stream;
+    SP_CUDA(cudaMemsetAsync(t->max_candidates, 0, sizeof(uint32_t), s), "counter reset");
+    SP_CUDA(cudaMemsetAsync(t->count_totals, 0, 2 * sizeof(unsigned long long), s), "counter reset");
+    const uint32_t launches = t->last_launches;
+    const bv_status st = enqueue_splats(t, nullptr, t->last_cams.data(), (uint32_t)t->last_cams.size(),
+                                        t->last_w, t->last_h, true, s);
+    t->last_launches = launches;
+    if (st != BV_OK) return st;
+    uint32_t h = 0;
+    unsigned long long tot[2] = {0, 0};
+    SP_CUDA(cudaMemcpyAsync(&h, t->max_candidates, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "read");
+    SP_CUDA(cudaMemcpyAsync(tot, t->count_totals, sizeof(tot), cudaMemcpyDeviceToHost, s), "read");
+    SP_CUDA(cudaStreamSynchronize(s), "synchronize");
+    *max_hits = h;
+    if (total_hits) *total_hits = tot[0];
+    if (row_entries) *row_entries = tot[1];
+    return BV_OK;
+}
+
+bv_status bv_powerfoam_splat_tracer_validate_candidate_counts(bv_splat_tracer *t, uint32_t *observed) {
+    if (!t || !observed) return sp_fail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    uint32_t h = 0;
+    const bv_status st = bv_powerfoam_splat_tracer_candidate_stats(t, &h, nullptr, nullptr);
+    if (st != BV_OK) return st;
+    *observed = h;
+    if (h > t->capacity)
+        return sp_fail(BV_ERR_CANDIDATE_OVERFLOW,
+                       "PowerFoam render needs %u candidates for one ray, but scratch capacity is %u", h,
+                       t->capacity);
+    return BV_OK;
+}
+
+uint32_t bv_powerfoam_splat_tracer_candidate_capacity(const bv_splat_tracer *t) {
+    return t ? t->capacity : 0;
+}
+uint32_t bv_powerfoam_splat_tracer_max_steps(const bv_splat_tracer *t) {
+    return t ? t->settings.max_steps : 0;
+}
+float bv_powerfoam_splat_tracer_weight_threshold(const bv_splat_tracer *t) {
+    return t ? t->settings.weight_threshold : 0.0f;
+}
+bv_status bv_powerfoam_splat_tracer_set_weight_threshold(bv_splat_tracer *t, float w) {
+    if (!t) return sp_fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
+    if (!(w >= 0.0f)) return sp_fail(BV_ERR_INVALID_ARGUMENT, "weight threshold must be >= 0");
+    t->settings.weight_threshold = w;
+    return BV_OK;
+}
+
+bv_status bv_powerfoam_splat_tracer_enable_stats(bv_splat_tracer *t, uint32_t enabled) {
+    if (!t) return sp_fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
+    t->stats_enabled = enabled != 0;
+    return BV_OK;
+}
+
+bv_status bv_powerfoam_splat_tracer_last_stats(bv_splat_tracer *t, bv_launch_stats *out) {
+    if (!t || !out) return sp_fail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    out->launches = t->last_launches;
+    if (!t->last_has_stats) return BV_OK;
+    SP_CUDA(cudaEventSynchronize(t->ev[1]), "event sync");
+    float ms = 0.f;
+    SP_CUDA(cudaEventElapsedTime(&ms, t->ev[0], t->ev[1]), "elapsed");
+    out->kernel_ms = ms;
+    unsigned long long h[4] = {0, 0, 0, 0};
+    SP_CUDA(cudaMemcpy(h, t->stats, sizeof(h), cudaMemcpyDeviceToHost), "stats read");
+    out->rays = h[0];
+    out->steps = h[1];
+    out->faces = h[2];
+    return BV_OK;
+}
+
+}  // extern "C"

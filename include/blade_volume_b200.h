@@ -282,6 +282,49 @@ uint32_t bv_relight_tracer_num_particles(const bv_relight_tracer *tracer);
 bv_status bv_relight_tracer_enable_stats(bv_relight_tracer *tracer, uint32_t enabled);
 bv_status bv_relight_tracer_last_stats(bv_relight_tracer *tracer, bv_launch_stats *out);
 
+/* ---- PowerFoam splat render ----------------------------------------------
+ * PowerFoamGpuSplatTracer (blade-volume/src/gpu/powerfoam_splat.rs:38-370):
+ * per ray every support sphere it crosses (spheres within 4 r of the camera
+ * excluded), each clipped by its Cech row into [face_near, face_far] and the
+ * sphere, taken in (entry depth, cell) order, truncated to max_steps and
+ * composited (trace_powerfoam_splats, trace.rs:1456-1546).  Unlike the walk
+ * it stays correct when the overlap graph is disconnected.  The model must
+ * carry radii; its CSR is the Cech overlap graph.  There is no per-ray
+ * candidate scratch on this path, so a render never overflows; the
+ * reference's capacity check is kept: validate_candidate_counts recounts
+ * the support hits of the last dispatch's rays and returns
+ * BV_ERR_CANDIDATE_OVERFLOW when one ray has more than the capacity
+ * max(4 max_steps, 1024, settings.powerfoam_candidate_capacity)
+ * (path_record.rs:58-63). */
+typedef struct bv_splat_tracer bv_splat_tracer;
+
+bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *model, const bv_trace_settings *settings,
+                                        bv_splat_tracer **out);
+void bv_powerfoam_splat_tracer_destroy(bv_splat_tracer *tracer);
+/* Renders [height][width][4] float32 (RGB, alpha = 1 - transmittance). */
+bv_status bv_powerfoam_splat_tracer_dispatch(bv_splat_tracer *tracer, float *out_rgba_dev,
+                                             const bv_camera *camera, uint32_t width, uint32_t height,
+                                             bv_stream stream);
+bv_status bv_powerfoam_splat_tracer_dispatch_batch(bv_splat_tracer *tracer, float *out_rgba_dev,
+                                                   const bv_camera *cameras, uint32_t n_cameras,
+                                                   uint32_t width, uint32_t height, bv_stream stream);
+/* Synchronous; *observed = the largest support-hit count of one ray. */
+bv_status bv_powerfoam_splat_tracer_validate_candidate_counts(bv_splat_tracer *tracer,
+                                                              uint32_t *observed);
+/* Synchronous recount of the last dispatch's rays: the largest support-hit
+ * count of one ray, the total over all rays and the Cech row entries of
+ * those supports (either total pointer may be NULL). */
+bv_status bv_powerfoam_splat_tracer_candidate_stats(bv_splat_tracer *tracer, uint32_t *max_hits,
+                                                    uint64_t *total_hits, uint64_t *row_entries);
+uint32_t bv_powerfoam_splat_tracer_candidate_capacity(const bv_splat_tracer *tracer);
+uint32_t bv_powerfoam_splat_tracer_max_steps(const bv_splat_tracer *tracer);
+float bv_powerfoam_splat_tracer_weight_threshold(const bv_splat_tracer *tracer);
+bv_status bv_powerfoam_splat_tracer_set_weight_threshold(bv_splat_tracer *tracer, float weight_threshold);
+/* rays, composited intervals (steps) and Cech row entries clipped (faces,
+ * counting re-clips in later windows) of the last dispatch */
+bv_status bv_powerfoam_splat_tracer_enable_stats(bv_splat_tracer *tracer, uint32_t enabled);
+bv_status bv_powerfoam_splat_tracer_last_stats(bv_splat_tracer *tracer, bv_launch_stats *out);
+
 /* ---- allocation-free start-cell search -----------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
  * hosts whose device memory is owned by their own pool (a renderer's frame
@@ -338,7 +381,7 @@ typedef enum bv_request_kind { BV_REQUEST_RENDER = 0, BV_REQUEST_FORWARD_BACKWAR
 typedef struct bv_server_settings {
     uint64_t hbm_budget_bytes;  /* scenes + gradient tables + scratch + request buffers */
     uint32_t mode;              /* bv_serve_mode */
-    uint32_t max_batch_rays;    /* rays per batch; 0 = 4,194,304; >= the largest frame */
+    uint32_t max_batch_rays;    /* rays per batch; 0 = 2,097,152; >= the largest frame */
     uint32_t max_batch_views;   /* frames per batch, 1..1024; 0 = 256 */
     uint32_t slots;             /* batches in flight, 1..4; 0 = 2 */
     uint32_t max_steps;         /* 0 = 1024 */
