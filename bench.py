@@ -52,18 +52,21 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--sites", type=int, default=N_SITES)
-    ap.add_argument("--size", type=int, default=WIDTH)
-    ap.add_argument("--views", type=int, default=VIEWS)
+    ap.add_argument("--size", type=int, default=None,
+                    help="image side (train: 512, splat: 1024)")
+    ap.add_argument("--views", type=int, default=None, help="views (train: 8, splat: 4)")
     ap.add_argument("--cpu-sample", type=int, default=192,
                     help="side of the CPU-baseline sample image (view 0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="train",
-                    choices=["train", "relight", "render", "serving", "splat"],
+                    choices=["train", "relight", "render", "serving", "splat", "gaussian"],
                     help="train: the headline fwd+bwd line; relight / render: secondary "
                          "lines for the Gaussian relight and forward-render paths; serving: "
                          "the request loop, batched against plain")
     ap.add_argument("--splat-sites", type=int, default=1048576,
                     help="splat: sites of the PowerFoam mixture")
+    ap.add_argument("--gaussians", type=int, default=1000000,
+                    help="relight / gaussian: particles of the Gaussian mixture scene")
     ap.add_argument("--rates", default="5,10,25,50,200,2000",
                     help="serving: Poisson arrival rates (requests/s)")
     ap.add_argument("--requests", type=int, default=60, help="serving: requests per rate")
@@ -72,7 +75,13 @@ def parse():
                     help="serving: sites of the resident scenes (seeds 1, 2, ...)")
     ap.add_argument("--batch-rays", type=int, default=0, help="serving: rays per batch (0: default)")
     ap.add_argument("--slots", type=int, default=0, help="serving: batches in flight (0: default)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    splat = args.workload == "splat"
+    if args.size is None:
+        args.size = 1024 if splat else WIDTH
+    if args.views is None:
+        args.views = 4 if splat else VIEWS
+    return args
 
 
 def dist_env():
@@ -229,7 +238,7 @@ def run_secondary(args):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     sampler = ClockSampler(0)
     if args.workload == "relight":
-        g, cam, lights = scenes.relight_workload()
+        g, cam, lights = scenes.relight_workload(args.gaussians)
         W, H = 1024, 768
         tr = bv.RelightTracer(g)
         tr.set_point_lights(lights)
@@ -262,9 +271,43 @@ def run_secondary(args):
                 "gpu_launches": args.steps, "clocks": clocks}
         print(json.dumps(line), flush=True)
         return
+    if args.workload == "gaussian":
+        g = scenes.gaussian_sh(args.gaussians, seed=0, sh_degree=3)
+        W, H = 1024, 768
+        cam = scenes.sphere_cameras(1, 3.0, 1, math.radians(60.0), W / H, 100.0)[0]
+        tr = bv.GaussianTracer(g)
+        out = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+        for _ in range(max(args.warmup, 3)):
+            tr.dispatch(out, cam, (W, H))
+        tr.enable_stats(True)
+        tr.dispatch(out, cam, (W, H))
+        st = tr.last_stats()
+        tr.enable_stats(False)
+        sampler.start()
+        ts = timed_events(lambda: tr.dispatch(out, cam, (W, H)), args.steps, flush, stream)
+        clocks = sampler.stop()
+        ms = statistics.median(ts)
+        hits = st.steps
+        # per composited hit: particle 48 B + id 4 B + SH row 192 B; 16 B per ray out
+        alg = hits * (48 + 4 + 192) + W * H * 16
+        peak, kind = peaks()
+        line = {"metric": "gaussian Mrays/s", "value": W * H / (ms * 1e-3) / 1e6,
+                "unit": "Mrays/s", "ms_per_step": ms, "steps": args.steps,
+                "warmup": max(args.warmup, 3), "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "gaussian sh trace", "gaussians": g.n,
+                           "kept": tr.num_points, "sh_degree": 3, "width": W, "height": H,
+                           "min_opacity": 0.01, "min_transmittance": 0.01, "window": 16},
+                "hits_per_ray": hits / (W * H), "nodes_per_ray": st.faces / (W * H),
+                "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak,
+                             "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
+                             "traffic": None, "peak_source": kind},
+                "gpu_launches": args.steps, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+        return
     if args.workload == "splat":
         t_build = time.time()
-        w = scenes.powerfoam_mix(n_sites=args.splat_sites)
+        w = scenes.powerfoam_mix(n_sites=args.splat_sites, views=args.views, width=args.size,
+                                 height=args.size)
         t_build = time.time() - t_build
         W, H, V = w.width, w.height, len(w.cameras)
         tr = bv.PowerFoamSplatTracer(w.model, max_steps=w.max_steps,

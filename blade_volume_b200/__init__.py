@@ -7,6 +7,10 @@ libbv_b200.so (include/blade_volume_b200.h):
 * :meth:`RadFoamGpuTracer.record_paths`   gpu/path_record.rs:519-594
 * :meth:`RadFoamGpuTracer.forward_backward`   the trainer's gradient
   (blade-volume-train/src/diff_render.rs:943-1923, :7181-7226)
+* :class:`PowerFoamSplatTracer`   gpu/powerfoam_splat.rs:38-370
+* :class:`GaussianTracer`   gpu/gaussian.rs:94-280 + shaders/gaussian.wgsl
+* :class:`RelightTracer`   gpu/relight.rs:313-934
+* :class:`Server`   the serving loop (no counterpart in the reference)
 
 Device buffers are torch CUDA tensors (torch is only the allocator and the
 stream provider here).  There is no CPU fallback: constructing a tracer
@@ -60,6 +64,10 @@ EXPORTED_SYMBOLS = [
     "bv_powerfoam_splat_tracer_weight_threshold",
     "bv_powerfoam_splat_tracer_set_weight_threshold", "bv_powerfoam_splat_tracer_enable_stats",
     "bv_powerfoam_splat_tracer_last_stats",
+    "bv_gaussian_tracer_new", "bv_gaussian_tracer_destroy",
+    "bv_gaussian_tracer_set_min_transmittance", "bv_gaussian_tracer_set_background",
+    "bv_gaussian_tracer_num_points", "bv_gaussian_tracer_dispatch",
+    "bv_gaussian_tracer_enable_stats", "bv_gaussian_tracer_last_stats",
 ]
 SERVE_BATCHED, SERVE_PLAIN, SERVE_PLAIN_BATCH = 0, 1, 2
 REQUEST_RENDER, REQUEST_FORWARD_BACKWARD = 0, 1
@@ -132,6 +140,17 @@ class GaussianDesc(C.Structure):
                 ("points", C.POINTER(C.c_float)), ("rotations", C.POINTER(C.c_float)),
                 ("scales", C.POINTER(C.c_float)), ("normals", C.POINTER(C.c_float)),
                 ("material_indices", C.POINTER(C.c_uint32)), ("materials", C.c_void_p)]
+
+
+class GaussianShDesc(C.Structure):
+    _fields_ = [("num_points", C.c_uint32), ("sh_degree", C.c_uint32),
+                ("points", C.POINTER(C.c_float)), ("rotations", C.POINTER(C.c_float)),
+                ("scales", C.POINTER(C.c_float)), ("sh_coefficients", C.POINTER(C.c_float))]
+
+
+class GaussianTraceSettingsC(C.Structure):
+    _fields_ = [("min_opacity", C.c_float), ("min_transmittance", C.c_float),
+                ("background", C.c_float * 3)]
 
 
 class RelightSettings(C.Structure):
@@ -262,6 +281,18 @@ def load_library(path: str = LIB_PATH):
     L.bv_powerfoam_splat_tracer_set_weight_threshold.argtypes = [C.c_void_p, C.c_float]
     L.bv_powerfoam_splat_tracer_enable_stats.argtypes = [C.c_void_p, C.c_uint32]
     L.bv_powerfoam_splat_tracer_last_stats.argtypes = [C.c_void_p, C.POINTER(LaunchStats)]
+    L.bv_gaussian_tracer_new.argtypes = [C.POINTER(GaussianShDesc),
+                                         C.POINTER(GaussianTraceSettingsC), C.POINTER(C.c_void_p)]
+    L.bv_gaussian_tracer_destroy.argtypes = [C.c_void_p]
+    L.bv_gaussian_tracer_destroy.restype = None
+    L.bv_gaussian_tracer_set_min_transmittance.argtypes = [C.c_void_p, C.c_float]
+    L.bv_gaussian_tracer_set_background.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
+    L.bv_gaussian_tracer_num_points.argtypes = [C.c_void_p]
+    L.bv_gaussian_tracer_num_points.restype = C.c_uint32
+    L.bv_gaussian_tracer_dispatch.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(CameraC),
+                                              C.c_uint32, C.c_uint32, C.c_void_p]
+    L.bv_gaussian_tracer_enable_stats.argtypes = [C.c_void_p, C.c_uint32]
+    L.bv_gaussian_tracer_last_stats.argtypes = [C.c_void_p, C.POINTER(LaunchStats)]
     _lib = L
     return L
 
@@ -564,6 +595,74 @@ class RelightTracer:
     def last_stats(self) -> LaunchStats:
         s = LaunchStats()
         _check(load_library().bv_relight_tracer_last_stats(self._h, C.byref(s)))
+        return s
+
+
+class GaussianTracer:
+    """GaussianGpuCloud::new (gpu/gaussian.rs:94-280) plus its ray-traced
+    draw pass (shaders/gaussian.wgsl) over the C ABI: SH-coloured Gaussians
+    composited in maximum-response order (trace_gaussians, trace.rs:695-773).
+    ``model`` carries points [N, 4] (mean, opacity), rotations [N, 4] (x, y,
+    z, w), scales [N, 3], sh [N, 3K] and sh_degree."""
+
+    def __init__(self, model, min_opacity: float = 0.01, min_transmittance: float = 0.01,
+                 background=(0.0, 0.0, 0.0)):
+        L = load_library()
+        self.points = np.ascontiguousarray(model.points, np.float32)
+        self.rotations = np.ascontiguousarray(model.rotations, np.float32)
+        self.scales = np.ascontiguousarray(model.scales, np.float32)
+        self.sh = np.ascontiguousarray(model.sh, np.float32)
+        d = GaussianShDesc(len(self.points), int(model.sh_degree), _fptr(self.points),
+                           _fptr(self.rotations), _fptr(self.scales), _fptr(self.sh))
+        st = GaussianTraceSettingsC()
+        st.min_opacity = float(min_opacity)
+        st.min_transmittance = float(min_transmittance)
+        st.background[:] = [float(v) for v in background]
+        h = C.c_void_p()
+        _check(L.bv_gaussian_tracer_new(C.byref(d), C.byref(st), C.byref(h)))
+        self._h = h
+
+    def deinit(self):
+        if getattr(self, "_h", None):
+            load_library().bv_gaussian_tracer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.deinit()
+        except Exception:
+            pass
+
+    @property
+    def num_points(self) -> int:
+        return load_library().bv_gaussian_tracer_num_points(self._h)
+
+    def set_min_transmittance(self, v: float):
+        _check(load_library().bv_gaussian_tracer_set_min_transmittance(self._h, float(v)))
+
+    def set_background(self, rgb):
+        a = np.ascontiguousarray(rgb, np.float32)
+        _check(load_library().bv_gaussian_tracer_set_background(self._h, _fptr(a)))
+
+    def dispatch(self, output, camera: Camera, size, stream=None):
+        w, h = size
+        cam = camera_c(camera)
+        _check(load_library().bv_gaussian_tracer_dispatch(
+            self._h, C.c_void_p(output.data_ptr()), C.byref(cam), w, h, _stream_handle(stream)))
+
+    def render(self, camera: Camera, width: int, height: int):
+        import torch
+
+        out = torch.empty((height, width, 4), dtype=torch.float32, device="cuda")
+        self.dispatch(out, camera, (width, height))
+        return out
+
+    def enable_stats(self, enabled: bool = True):
+        _check(load_library().bv_gaussian_tracer_enable_stats(self._h, int(enabled)))
+
+    def last_stats(self) -> LaunchStats:
+        s = LaunchStats()
+        _check(load_library().bv_gaussian_tracer_last_stats(self._h, C.byref(s)))
         return s
 
 

@@ -166,4 +166,22 @@ inline BvhBuild build_bvh(const std::vector<BvhBox> &boxes, const std::vector<fl
     return out;
 }
 
+// Levels below node ni (a node whose children are both leaves is 1).  A
+// front-to-back traversal that pushes both children keeps at most depth + 1
+// entries on its stack.  Morton splits consume at least one code bit per
+// level (<= 30) and equal-code ranges split at the median, so the depth stays
+// near 30 + log2(n / kBvhLeaf).
+inline uint32_t bvh_depth(const std::vector<BvhNode> &nodes, uint32_t ni = 0) {
+    uint32_t d = 0;
+    const BvhNode &n = nodes[ni];
+    const float4 *lo[2] = {&n.l_lo, &n.r_lo}, *hi[2] = {&n.l_hi, &n.r_hi};
+    for (int c = 0; c < 2; ++c) {
+        uint32_t cnt, ref;
+        std::memcpy(&cnt, &hi[c]->w, 4);
+        std::memcpy(&ref, &lo[c]->w, 4);
+        if (cnt == 0u) d = std::max(d, bvh_depth(nodes, ref));
+    }
+    return d + 1;
+}
+
 }  // namespace bv

@@ -1,0 +1,497 @@
+// Gaussian ray tracing with SH colour on sm_100a: per ray, every particle
+// whose maximum response along the ray reaches min_opacity, composited
+// front to back in strict (depth, index) order until the transmittance
+// falls to min_transmittance.
+//
+// Restates trace_gaussians (blade-volume/src/trace.rs:695-773), the CPU
+// oracle of the reference's hardware-ray-query tracer
+// (shaders/gaussian_trace.wgsl:66-177 under shaders/gaussian.wgsl), with the
+// local ray formed as the shader forms it (qrot of the inverse rotation,
+// then a per-axis division by the scale, gaussian_trace.wgsl:147-151).
+// Candidates come from a BVH over the support ellipsoids (the proxies of
+// gpu/gaussian.rs:175-200 scale the unit sphere by sqrt(2 ln(opacity /
+// min_opacity))), gathered in windows of kWindow keys (bv_window.cuh).
+//
+// Host side: GaussianGpuCloud::new (gpu/gaussian.rs:94-280) — validation,
+// the opacity filter, the particle table in BVH leaf order — and the draw
+// pass as one dispatch per camera.
+//
+// Compiled with -fmad=false: the arithmetic is the CPU oracle's, operation
+// for operation, so images are bit-identical to it.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "bv_device.cuh"
+#include "bv_internal.h"
+#include "bv_window.cuh"
+
+namespace bv {
+namespace {
+
+constexpr int kGaussBlock = 128;
+constexpr int kWindow = 16;
+constexpr int kStack = 64;
+
+// One particle in BVH leaf order, 48 B: all a candidate test reads.
+struct __align__(16) GaussShPrim {
+    float4 center_opacity;  // mean, opacity
+    float4 qinv;            // inverse rotation (-x, -y, -z, w)
+    float4 scale_cut;       // scale, |local hit|^2 bound past which alpha < min_opacity
+};
+
+struct GaussianParams {
+    const GaussShPrim *prims;
+    const uint32_t *ids;  // filtered model index per table position
+    const BvhNode *nodes;
+    const float *sh;      // [n][sh_stride] in table order
+    float4 *out;
+    unsigned long long *stats;  // [3] rays, composited hits, nodes visited (or null)
+    uint32_t sh_stride;
+    float origin[3];
+    float depth;
+    float q[4];
+    float tan_half[2];
+    float principal[2];
+    uint32_t width, height, tiles_x, total_work;
+    float min_opacity, min_transmittance;
+    float background[3];
+};
+
+__device__ __forceinline__ float gdot(float ax, float ay, float az, float bx, float by, float bz) {
+    return ax * bx + ay * by + az * bz;
+}
+
+// qrot (common.wgsl:386-390)
+__device__ __forceinline__ float3 gqrot(float4 q, float vx, float vy, float vz) {
+    const float t0 = 2.0f * (q.y * vz - q.z * vy);
+    const float t1 = 2.0f * (q.z * vx - q.x * vz);
+    const float t2 = 2.0f * (q.x * vy - q.y * vx);
+    return make_float3((vx + q.w * t0) + (q.y * t2 - q.z * t1),
+                       (vy + q.w * t1) + (q.z * t0 - q.x * t2),
+                       (vz + q.w * t2) + (q.x * t1 - q.y * t0));
+}
+
+// Maximum-response depth and alpha (trace.rs:731-747); false when the
+// depth is outside (0, t_end) or alpha < min_opacity.
+__device__ __forceinline__ bool response(const GaussianParams &P, uint32_t pos, const WinRay &r,
+                                         float &t_out, float &alpha_out) {
+    const float4 co = __ldg(&P.prims[pos].center_opacity);
+    const float4 qi = __ldg(&P.prims[pos].qinv);
+    const float4 sc = __ldg(&P.prims[pos].scale_cut);
+    const float3 lo0 = gqrot(qi, r.ox - co.x, r.oy - co.y, r.oz - co.z);
+    const float3 ld0 = gqrot(qi, r.dx, r.dy, r.dz);
+    const float lox = lo0.x / sc.x, loy = lo0.y / sc.y, loz = lo0.z / sc.z;
+    const float ldx = ld0.x / sc.x, ldy = ld0.y / sc.y, ldz = ld0.z / sc.z;
+    const float t = -gdot(lox, loy, loz, ldx, ldy, ldz) / gdot(ldx, ldy, ldz, ldx, ldy, ldz);
+    if (!(t > 0.0f && t < P.depth)) return false;
+    const float px = lox + t * ldx, py = loy + t * ldy, pz = loz + t * ldz;
+    const float sq = gdot(px, py, pz, px, py, pz);
+    if (sq > sc.w) return false;  // alpha would be below min_opacity by a margin
+    const float alpha = co.w * bv_expf(-0.5f * sq);
+    if (!(alpha >= P.min_opacity)) return false;
+    t_out = t;
+    alpha_out = alpha;
+    return true;
+}
+
+template <int DEG>
+__global__ void __launch_bounds__(kGaussBlock) gaussian_kernel(const __grid_constant__ GaussianParams P) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= P.total_work) return;
+    const uint32_t tile = w / 32u, in = w % 32u;
+    const uint32_t x = (tile % P.tiles_x) * 8u + in % 8u;
+    const uint32_t y = (tile / P.tiles_x) * 4u + in / 8u;
+    if (x >= P.width || y >= P.height) return;
+
+    // pixel -> ray: radfoam.wgsl:44-52 mapping, one normalisation
+    WinRay ray;
+    {
+        const float px = ((float)x + 0.5f) / (float)P.width;
+        const float py = ((float)y + 0.5f) / (float)P.height;
+        const float vx = (px * 2.0f - 1.0f - P.principal[0]) * P.tan_half[0];
+        const float vy = (py * 2.0f - 1.0f - P.principal[1]) * P.tan_half[1];
+        const float4 q = make_float4(P.q[0], P.q[1], P.q[2], P.q[3]);
+        const float3 rv = gqrot(q, vx, vy, 1.0f);
+        const float len = sqrtf(gdot(rv.x, rv.y, rv.z, rv.x, rv.y, rv.z));
+        const float inv = 1.0f / len;
+        ray.dx = rv.x * inv;
+        ray.dy = rv.y * inv;
+        ray.dz = rv.z * inv;
+        ray.ox = P.origin[0];
+        ray.oy = P.origin[1];
+        ray.oz = P.origin[2];
+        ray.ix = 1.0f / ray.dx;
+        ray.iy = 1.0f / ray.dy;
+        ray.iz = 1.0f / ray.dz;
+    }
+
+    float rad_r = 0.f, rad_g = 0.f, rad_b = 0.f, T = 1.0f;
+    bool cursor_valid = false;
+    float cur_t = 0.f;
+    uint32_t cur_idx = 0, hits_used = 0, nodes_visited = 0;
+    auto hit = [&](uint32_t p, float &t, uint32_t &id) -> bool {
+        float a;
+        if (!response(P, p, ray, t, a)) return false;
+        id = __ldg(&P.ids[p]);
+        return true;
+    };
+    while (T > P.min_transmittance) {
+        WinKey buf[kWindow];
+        const int count = win_gather<kWindow, kStack>(P.nodes, ray, P.depth, cursor_valid, cur_t,
+                                                      cur_idx, buf, nodes_visited, hit);
+        if (count == 0) break;
+#pragma unroll 1
+        for (int i = 0; i < count; ++i) {
+            if (T <= P.min_transmittance) break;
+            const WinKey h = win_at(buf, i);
+            float tt, a;
+            response(P, h.pos, ray, tt, a);
+            float coef[ShDims<DEG>::N];
+            const float4 *row = reinterpret_cast<const float4 *>(P.sh + (size_t)h.pos * P.sh_stride);
+#pragma unroll
+            for (int qd = 0; qd < (ShDims<DEG>::N + 3) / 4; ++qd) {
+                const float4 v = __ldg(row + qd);
+                const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    if (qd * 4 + e < ShDims<DEG>::N) coef[qd * 4 + e] = vv[e];
+            }
+            float cr, cg, cb;
+            eval_sh<DEG>(coef, ray.dx, ray.dy, ray.dz, cr, cg, cb);
+            cr = fmaxf(cr, 0.0f);
+            cg = fmaxf(cg, 0.0f);
+            cb = fmaxf(cb, 0.0f);
+            const float wt = a * T;
+            rad_r += wt * cr;
+            rad_g += wt * cg;
+            rad_b += wt * cb;
+            T *= 1.0f - a;
+            hits_used += 1;
+        }
+        if (count < kWindow) break;
+        cursor_valid = true;
+        cur_t = buf[kWindow - 1].t;
+        cur_idx = buf[kWindow - 1].idx;
+    }
+    const size_t o = (size_t)y * P.width + x;
+    P.out[o] = make_float4(rad_r + T * P.background[0], rad_g + T * P.background[1],
+                           rad_b + T * P.background[2], 1.0f - T);
+    if (P.stats) {
+        atomicAdd(P.stats + 0, 1ull);
+        atomicAdd(P.stats + 1, (unsigned long long)hits_used);
+        atomicAdd(P.stats + 2, (unsigned long long)nodes_visited);
+    }
+}
+
+cudaError_t launch_gaussian(const GaussianParams &p, uint32_t deg, cudaStream_t s) {
+    const int blocks = (int)((p.total_work + kGaussBlock - 1) / kGaussBlock);
+    if (blocks == 0) return cudaSuccess;
+    switch (deg) {
+        case 0: gaussian_kernel<0><<<blocks, kGaussBlock, 0, s>>>(p); break;
+        case 1: gaussian_kernel<1><<<blocks, kGaussBlock, 0, s>>>(p); break;
+        case 2: gaussian_kernel<2><<<blocks, kGaussBlock, 0, s>>>(p); break;
+        default: gaussian_kernel<3><<<blocks, kGaussBlock, 0, s>>>(p); break;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+}  // namespace bv
+
+using namespace bv;
+
+struct bv_gaussian_tracer {
+    uint32_t n_input = 0, n_kept = 0, n_nodes = 0, sh_degree = 0, sh_stride = 0;
+    float min_opacity = 0.01f, min_transmittance = 0.01f;
+    float background[3] = {0.f, 0.f, 0.f};
+    GaussShPrim *prims = nullptr;
+    uint32_t *ids = nullptr;
+    BvhNode *nodes = nullptr;
+    float *sh = nullptr;
+    unsigned long long *stats = nullptr;
+    bool stats_enabled = false, last_has_stats = false;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+bv_status gfail(bv_status code, const char *msg) {
+    set_last_error(msg);
+    return code;
+}
+
+void free_gaussian(bv_gaussian_tracer *t) {
+    if (!t) return;
+    cudaFree(t->prims);
+    cudaFree(t->ids);
+    cudaFree(t->nodes);
+    cudaFree(t->sh);
+    cudaFree(t->stats);
+    for (auto &e : t->ev)
+        if (e) cudaEventDestroy(e);
+    delete t;
+}
+
+inline bool gfinite3(const float *v) {
+    return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]);
+}
+
+// PointCloudModel::validate for a Gaussian model (lib.rs:246-340) and the
+// asserts of GaussianGpuCloud::new / trace_gaussians (gpu/gaussian.rs:100-112,
+// trace.rs:704-727).
+bv_status validate_gaussian_sh(const bv_gaussian_sh_desc *g, const bv_gaussian_trace_settings *s) {
+    if (!g || !g->points || !g->rotations || !g->scales || !g->sh_coefficients)
+        return gfail(BV_ERR_INVALID_MODEL, "Gaussian model arrays are required");
+    if (g->num_points == 0) return gfail(BV_ERR_INVALID_MODEL, "model has no points");
+    if (g->sh_degree > 3) return gfail(BV_ERR_INVALID_MODEL, "sh_degree must be at most 3");
+    if (!(std::isfinite(s->min_opacity) && s->min_opacity > 0.0f))
+        return gfail(BV_ERR_INVALID_ARGUMENT, "Gaussian min_opacity must be finite and positive");
+    if (!(std::isfinite(s->min_transmittance) && s->min_transmittance >= 0.0f &&
+          s->min_transmittance <= 1.0f))
+        return gfail(BV_ERR_INVALID_ARGUMENT, "min_transmittance must be finite and in [0, 1]");
+    if (!gfinite3(s->background))
+        return gfail(BV_ERR_INVALID_ARGUMENT, "background must be finite");
+    const uint32_t n3k = 3u * (g->sh_degree + 1) * (g->sh_degree + 1);
+    for (uint32_t i = 0; i < g->num_points; ++i) {
+        const float *p = g->points + 4 * (size_t)i;
+        if (!gfinite3(p) || !std::isfinite(p[3]) || p[3] < 0.0f)
+            return gfail(BV_ERR_INVALID_MODEL,
+                         "points must have finite coordinates and non-negative opacity");
+        const float *q = g->rotations + 4 * (size_t)i;
+        const float ql = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        if (!gfinite3(q) || !std::isfinite(q[3]) || std::fabs(ql - 1.0f) > 1.0e-3f)
+            return gfail(BV_ERR_INVALID_MODEL, "transform rotations must be finite and unit length");
+        const float *sc = g->scales + 3 * (size_t)i;
+        if (!gfinite3(sc) || std::min(std::min(sc[0], sc[1]), sc[2]) <= 0.0f)
+            return gfail(BV_ERR_INVALID_MODEL, "transform scales must be finite and positive");
+        const float *c = g->sh_coefficients + (size_t)n3k * i;
+        for (uint32_t k = 0; k < n3k; ++k)
+            if (!std::isfinite(c[k]))
+                return gfail(BV_ERR_INVALID_MODEL, "SH coefficients must be finite");
+    }
+    return BV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+bv_status bv_gaussian_tracer_new(const bv_gaussian_sh_desc *g,
+                                 const bv_gaussian_trace_settings *settings,
+                                 bv_gaussian_tracer **out) {
+    if (!out) return gfail(BV_ERR_INVALID_ARGUMENT, "out handle pointer is null");
+    *out = nullptr;
+    bv_gaussian_trace_settings st;
+    if (settings) {
+        st = *settings;
+    } else {
+        st.min_opacity = 0.01f;
+        st.min_transmittance = 0.01f;
+        st.background[0] = st.background[1] = st.background[2] = 0.0f;
+    }
+    bv_status vs = validate_gaussian_sh(g, &st);
+    if (vs != BV_OK) return vs;
+    // visible_point_indices (gpu/gaussian.rs:19-27): opacity > min_opacity
+    const uint32_t K = (g->sh_degree + 1) * (g->sh_degree + 1);
+    const uint32_t n3k = 3 * K;
+    const uint32_t stride = (n3k + 3) & ~3u;
+    std::vector<GaussShPrim> prims;
+    std::vector<uint32_t> kept_model;
+    std::vector<BvhBox> boxes;
+    std::vector<float> centers;
+    for (uint32_t i = 0; i < g->num_points; ++i) {
+        const float *p = g->points + 4 * (size_t)i;
+        if (!(p[3] > st.min_opacity)) continue;
+        const float *q = g->rotations + 4 * (size_t)i;
+        const float *s = g->scales + 3 * (size_t)i;
+        // alpha >= min_opacity  <=>  |local|^2 <= 2 ln(opacity / min_opacity);
+        // the cut is widened so that rounding never rejects a hit
+        const double support = 2.0 * std::log((double)p[3] / (double)st.min_opacity);
+        GaussShPrim gp;
+        gp.center_opacity = make_float4(p[0], p[1], p[2], p[3]);
+        gp.qinv = make_float4(-q[0], -q[1], -q[2], q[3]);
+        gp.scale_cut = make_float4(s[0], s[1], s[2], (float)(support * (1.0 + 1e-3) + 1e-5));
+        prims.push_back(gp);
+        const double x = q[0], y = q[1], z = q[2], w = q[3];
+        const double R[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)},
+                                {2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)},
+                                {2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)}};
+        const double sup = std::sqrt(support * (1.0 + 1e-3) + 1e-5);
+        BvhBox bx;
+        for (int k = 0; k < 3; ++k) {
+            double e2 = 0.0;
+            for (int j = 0; j < 3; ++j) {
+                const double a = R[k][j] * (double)s[j];
+                e2 += a * a;
+            }
+            const double ext = sup * std::sqrt(e2) * (1.0 + 1e-4) + 1e-6 * (1.0 + std::fabs(p[k]));
+            bx.lo[k] = std::nextafter((float)((double)p[k] - ext), -INFINITY);
+            bx.hi[k] = std::nextafter((float)((double)p[k] + ext), INFINITY);
+        }
+        boxes.push_back(bx);
+        centers.insert(centers.end(), {p[0], p[1], p[2]});
+        kept_model.push_back(i);
+    }
+    const uint32_t kept = (uint32_t)prims.size();
+    if (kept == 0)
+        return gfail(BV_ERR_INVALID_MODEL, "Gaussian model has no points above min_opacity");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return gfail(BV_ERR_NO_DEVICE, "no CUDA device");
+
+    BvhBuild bvh = build_bvh(boxes, centers);
+    if (bvh_depth(bvh.nodes) >= (uint32_t)kStack)
+        return gfail(BV_ERR_NOT_SUPPORTED, "BVH deeper than the traversal stack");
+    std::vector<GaussShPrim> sorted(kept);
+    std::vector<uint32_t> ids(kept);
+    std::vector<float> sh((size_t)kept * stride, 0.0f);
+    for (uint32_t i = 0; i < kept; ++i) {
+        const uint32_t f = bvh.order[i];  // filtered index
+        sorted[i] = prims[f];
+        ids[i] = f;
+        std::memcpy(&sh[(size_t)i * stride], g->sh_coefficients + (size_t)n3k * kept_model[f],
+                    sizeof(float) * n3k);
+    }
+
+    bv_gaussian_tracer *t = new bv_gaussian_tracer();
+    t->n_input = g->num_points;
+    t->n_kept = kept;
+    t->n_nodes = (uint32_t)bvh.nodes.size();
+    t->sh_degree = g->sh_degree;
+    t->sh_stride = stride;
+    t->min_opacity = st.min_opacity;
+    t->min_transmittance = st.min_transmittance;
+    std::memcpy(t->background, st.background, sizeof(t->background));
+    auto cleanup = [&](cudaError_t e, const char *what) {
+        free_gaussian(t);
+        set_last_error(what);
+        return e == cudaErrorMemoryAllocation ? BV_ERR_OUT_OF_MEMORY : BV_ERR_CUDA;
+    };
+#define BV_GTRY(call, what)                              \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cleanup(e_, what); \
+    } while (0)
+    BV_GTRY(cudaMalloc(&t->prims, sizeof(GaussShPrim) * kept), "cudaMalloc particles");
+    BV_GTRY(cudaMalloc(&t->ids, sizeof(uint32_t) * kept), "cudaMalloc ids");
+    BV_GTRY(cudaMalloc(&t->nodes, sizeof(BvhNode) * t->n_nodes), "cudaMalloc nodes");
+    BV_GTRY(cudaMalloc(&t->sh, sizeof(float) * sh.size()), "cudaMalloc SH");
+    BV_GTRY(cudaMalloc(&t->stats, sizeof(unsigned long long) * 4), "cudaMalloc stats");
+    BV_GTRY(cudaMemcpy(t->prims, sorted.data(), sizeof(GaussShPrim) * kept, cudaMemcpyHostToDevice),
+            "upload particles");
+    BV_GTRY(cudaMemcpy(t->ids, ids.data(), sizeof(uint32_t) * kept, cudaMemcpyHostToDevice),
+            "upload ids");
+    BV_GTRY(cudaMemcpy(t->nodes, bvh.nodes.data(), sizeof(BvhNode) * t->n_nodes,
+                       cudaMemcpyHostToDevice), "upload nodes");
+    BV_GTRY(cudaMemcpy(t->sh, sh.data(), sizeof(float) * sh.size(), cudaMemcpyHostToDevice),
+            "upload SH");
+    for (auto &e : t->ev) BV_GTRY(cudaEventCreate(&e), "cudaEventCreate");
+#undef BV_GTRY
+    *out = t;
+    return BV_OK;
+}
+
+void bv_gaussian_tracer_destroy(bv_gaussian_tracer *t) {
+    if (!t) return;
+    cudaDeviceSynchronize();
+    free_gaussian(t);
+}
+
+bv_status bv_gaussian_tracer_set_min_transmittance(bv_gaussian_tracer *t, float v) {
+    if (!t) return gfail(BV_ERR_INVALID_ARGUMENT, "null tracer");
+    if (!(std::isfinite(v) && v >= 0.0f && v <= 1.0f))
+        return gfail(BV_ERR_INVALID_ARGUMENT, "min_transmittance must be finite and in [0, 1]");
+    t->min_transmittance = v;
+    return BV_OK;
+}
+
+bv_status bv_gaussian_tracer_set_background(bv_gaussian_tracer *t, const float rgb[3]) {
+    if (!t || !rgb) return gfail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    if (!gfinite3(rgb)) return gfail(BV_ERR_INVALID_ARGUMENT, "background must be finite");
+    std::memcpy(t->background, rgb, sizeof(t->background));
+    return BV_OK;
+}
+
+uint32_t bv_gaussian_tracer_num_points(const bv_gaussian_tracer *t) { return t ? t->n_kept : 0; }
+
+bv_status bv_gaussian_tracer_dispatch(bv_gaussian_tracer *t, float *out_rgba_dev,
+                                      const bv_camera *c, uint32_t width, uint32_t height,
+                                      bv_stream stream) {
+    if (!t || !out_rgba_dev || !c) return gfail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    if (width == 0 || height == 0)
+        return gfail(BV_ERR_INVALID_ARGUMENT, "render size must be non-zero");
+    if (!gfinite3(c->cam_position) || !std::isfinite(c->depth) || !(c->depth > 0.f))
+        return gfail(BV_ERR_INVALID_ARGUMENT, "camera must be finite with positive depth");
+    GaussianParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.prims = t->prims;
+    p.ids = t->ids;
+    p.nodes = t->nodes;
+    p.sh = t->sh;
+    p.sh_stride = t->sh_stride;
+    p.out = reinterpret_cast<float4 *>(out_rgba_dev);
+    p.stats = t->stats_enabled ? t->stats : nullptr;
+    for (int k = 0; k < 3; ++k) p.origin[k] = c->cam_position[k];
+    p.depth = c->depth;
+    for (int k = 0; k < 4; ++k) p.q[k] = c->cam_orientation[k];
+    p.tan_half[0] = (float)std::tan((double)(0.5f * c->fov[0]));
+    p.tan_half[1] = (float)std::tan((double)(0.5f * c->fov[1]));
+    p.principal[0] = c->principal[0];
+    p.principal[1] = c->principal[1];
+    p.width = width;
+    p.height = height;
+    p.tiles_x = (width + 7) / 8;
+    const uint64_t work = (uint64_t)p.tiles_x * ((height + 3) / 4) * 32u;
+    if (work >= (1ull << 31)) return gfail(BV_ERR_INVALID_ARGUMENT, "image too large");
+    p.total_work = (uint32_t)work;
+    p.min_opacity = t->min_opacity;
+    p.min_transmittance = t->min_transmittance;
+    std::memcpy(p.background, t->background, sizeof(p.background));
+    cudaStream_t s = (cudaStream_t)stream;
+    t->last_has_stats = t->stats_enabled;
+    if (t->stats_enabled) {
+        if (cudaMemsetAsync(t->stats, 0, sizeof(unsigned long long) * 4, s) != cudaSuccess ||
+            cudaEventRecord(t->ev[0], s) != cudaSuccess)
+            return gfail(BV_ERR_CUDA, "stats setup failed");
+    }
+    cudaError_t e = launch_gaussian(p, t->sh_degree, s);
+    if (e != cudaSuccess) {
+        set_last_error(cudaGetErrorString(e));
+        return BV_ERR_CUDA;
+    }
+    if (t->stats_enabled && cudaEventRecord(t->ev[1], s) != cudaSuccess)
+        return gfail(BV_ERR_CUDA, "event record failed");
+    return BV_OK;
+}
+
+bv_status bv_gaussian_tracer_enable_stats(bv_gaussian_tracer *t, uint32_t enabled) {
+    if (!t) return gfail(BV_ERR_INVALID_ARGUMENT, "null tracer");
+    t->stats_enabled = enabled != 0;
+    return BV_OK;
+}
+
+bv_status bv_gaussian_tracer_last_stats(bv_gaussian_tracer *t, bv_launch_stats *out) {
+    if (!t || !out) return gfail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    out->launches = 1;
+    if (!t->last_has_stats) return BV_OK;
+    if (cudaEventSynchronize(t->ev[1]) != cudaSuccess)
+        return gfail(BV_ERR_CUDA, "event sync failed");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t->ev[0], t->ev[1]);
+    out->kernel_ms = ms;
+    unsigned long long h[4] = {0, 0, 0, 0};
+    if (cudaMemcpy(h, t->stats, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return gfail(BV_ERR_CUDA, "stats read failed");
+    out->rays = h[0];
+    out->steps = h[1];  // composited hits
+    out->faces = h[2];  // BVH nodes visited
+    return BV_OK;
+}
+
+}  // extern "C"

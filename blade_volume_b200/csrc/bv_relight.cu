@@ -18,13 +18,13 @@
 // for operation, so images are bit-identical.
 
 #include "bv_relight.h"
+#include "bv_window.cuh"
 
 namespace bv {
 namespace {
 
 constexpr int kRelightBlock = 128;
 constexpr int kWindow = 16;
-constexpr int kStack = 64;
 
 __device__ __forceinline__ float r_expf(float x) {
     if (x != x) return x;
@@ -106,13 +106,9 @@ __device__ __forceinline__ float3 qrot(float4 q, float vx, float vy, float vz) {
                        (vz + q.w * t2) + (q.x * t1 - q.y * t0));
 }
 
-struct RRay {
-    float ox, oy, oz, dx, dy, dz;
-};
-
 // intersect_surfel, kernel 2 (relight.wgsl:419-441).
 __device__ __forceinline__ bool intersect(const GaussPrim *__restrict__ prims, uint32_t pos,
-                                          const RRay &r, float t_end, float &t_out,
+                                          const WinRay &r, float t_end, float &t_out,
                                           float &alpha_out) {
     const float4 co = __ldg(&prims[pos].center_opacity);
     const float4 qi = __ldg(&prims[pos].qinv);
@@ -185,29 +181,6 @@ __device__ __forceinline__ void shade_light(const RelightLight &L, float px, flo
     ab += outb;
 }
 
-struct Key {
-    float t;
-    uint32_t idx;  // filtered particle index (the reference's instance index)
-    uint32_t pos;  // position in the BVH-ordered particle table
-};
-
-__device__ __forceinline__ bool key_less(float ta, uint32_t ia, float tb, uint32_t ib) {
-    return ta < tb || (ta == tb && ia < ib);
-}
-
-// Slab test of a box against the ray, conservative by a small margin.
-__device__ __forceinline__ bool slab(const float4 &lo, const float4 &hi, const RRay &r, float ix,
-                                     float iy, float iz, float t_end, float &tn, float &tf) {
-    const float ax = (lo.x - r.ox) * ix, bx = (hi.x - r.ox) * ix;
-    const float ay = (lo.y - r.oy) * iy, by = (hi.y - r.oy) * iy;
-    const float az = (lo.z - r.oz) * iz, bz = (hi.z - r.oz) * iz;
-    tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
-    tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), t_end));
-    tn = tn - (1e-5f * fabsf(tn) + 1e-6f);
-    tf = tf + (1e-5f * fabsf(tf) + 1e-6f);
-    return tn <= tf;
-}
-
 __global__ void __launch_bounds__(kRelightBlock)
 relight_kernel(const __grid_constant__ RelightParams P) {
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
@@ -218,7 +191,7 @@ relight_kernel(const __grid_constant__ RelightParams P) {
     if (x >= P.width || y >= P.height) return;
 
     // trace_main ray mapping (relight.wgsl:760-766): one normalisation
-    RRay ray;
+    WinRay ray;
     {
         const float px = ((float)x + 0.5f) / (float)P.width;
         const float py = ((float)y + 0.5f) / (float)P.height;
@@ -234,8 +207,10 @@ relight_kernel(const __grid_constant__ RelightParams P) {
         ray.ox = P.origin[0];
         ray.oy = P.origin[1];
         ray.oz = P.origin[2];
+        ray.ix = 1.0f / ray.dx;
+        ray.iy = 1.0f / ray.dy;
+        ray.iz = 1.0f / ray.dz;
     }
-    const float ix = 1.0f / ray.dx, iy = 1.0f / ray.dy, iz = 1.0f / ray.dz;
     const float t_end = P.depth;
 
     float rad_r = 0.f, rad_g = 0.f, rad_b = 0.f, T = 1.0f;
@@ -245,74 +220,23 @@ relight_kernel(const __grid_constant__ RelightParams P) {
     float cur_t = 0.f;
     uint32_t cur_idx = 0;
     uint32_t hits_used = 0, nodes_visited = 0;
+    auto hit = [&](uint32_t p, float &t, uint32_t &id) -> bool {
+        float a;
+        if (!intersect(P.prims, p, ray, t_end, t, a) || !(a > 0.0f)) return false;
+        id = __ldg(&P.prims[p].ids.x);
+        return true;
+    };
 
     for (;;) {
         // ---- gather the next window of keys above the cursor
-        Key buf[kWindow];
-        int count = 0;
-        uint32_t stack[kStack];
-        int sp = 0;
-        stack[sp++] = 0u;
-        while (sp > 0) {
-            const uint32_t ni = stack[--sp];
-            const BvhNode nd = P.nodes[ni];
-            nodes_visited += 1;
-            float tn[2], tf[2];
-            bool ok[2];
-            const float4 lo[2] = {nd.l_lo, nd.r_lo}, hi[2] = {nd.l_hi, nd.r_hi};
-            const uint32_t cnts[2] = {__float_as_uint(nd.l_hi.w), __float_as_uint(nd.r_hi.w)};
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                ok[c] = cnts[c] != 0xffffffffu &&
-                        slab(lo[c], hi[c], ray, ix, iy, iz, t_end, tn[c], tf[c]);
-                if (ok[c] && cursor_valid && tf[c] < cur_t) ok[c] = false;
-                if (ok[c] && count == kWindow && tn[c] > buf[kWindow - 1].t) ok[c] = false;
-            }
-            // push the farther child first so the nearer one is visited next
-            const int first = (ok[0] && ok[1] && tn[1] < tn[0]) ? 1 : 0;
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int c = k == 0 ? 1 - first : first;
-                if (!ok[c]) continue;
-                const uint32_t ref = __float_as_uint(c == 0 ? nd.l_lo.w : nd.r_lo.w);
-                const uint32_t cnt = cnts[c];
-                if (cnt == 0u) {
-                    if (sp < kStack) stack[sp++] = ref;
-                    continue;
-                }
-                for (uint32_t p = ref; p < ref + cnt; ++p) {
-                    float t, a;
-                    if (!intersect(P.prims, p, ray, t_end, t, a)) continue;
-                    if (!(a > 0.0f)) continue;
-                    const uint32_t id = __ldg(&P.prims[p].ids.x);
-                    if (cursor_valid && !key_less(cur_t, cur_idx, t, id)) continue;
-                    if (count == kWindow && !key_less(t, id, buf[kWindow - 1].t, buf[kWindow - 1].idx))
-                        continue;
-                    // insertion into the sorted window
-                    Key nk{t, id, p};
-#pragma unroll
-                    for (int i = 0; i < kWindow; ++i) {
-                        if (i < count && key_less(nk.t, nk.idx, buf[i].t, buf[i].idx)) {
-                            const Key tmp = buf[i];
-                            buf[i] = nk;
-                            nk = tmp;
-                        }
-                    }
-#pragma unroll
-                    for (int i = 0; i < kWindow; ++i)
-                        if (i == count) buf[i] = nk;
-                    if (count < kWindow) count += 1;
-                }
-            }
-        }
+        WinKey buf[kWindow];
+        const int count = win_gather<kWindow, kRelightStack>(P.nodes, ray, t_end, cursor_valid, cur_t,
+                                                      cur_idx, buf, nodes_visited, hit);
         if (count == 0) break;
         // ---- composite the window in order (trace_blended :693-728)
 #pragma unroll 1
         for (int i = 0; i < count; ++i) {
-            Key h = buf[0];
-#pragma unroll
-            for (int j = 0; j < kWindow; ++j)
-                if (j == i) h = buf[j];
+            const WinKey h = win_at(buf, i);
             if (!group || h.t > limit) {
                 if (group) {
                     const float a_sum = fminf(1.0f, sum_w);

@@ -32,6 +32,8 @@ struct __align__(16) RelightMaterial {  // Material (relight.rs:77-86)
 };
 
 constexpr int kMaxRelightLights = 64;
+// Traversal stack entries per ray; the BVH depth must stay below it.
+constexpr int kRelightStack = 64;
 
 struct RelightParams {
     const GaussPrim *prims;

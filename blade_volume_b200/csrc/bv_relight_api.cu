@@ -156,6 +156,8 @@ bv_status bv_relight_tracer_new_gaussian(const bv_gaussian_desc *g,
 
     // BVH over the support boxes, particles stored in leaf order
     BvhBuild bvh = build_bvh(boxes, centers);
+    if (bvh_depth(bvh.nodes) >= (uint32_t)kRelightStack)
+        return rfail(BV_ERR_NOT_SUPPORTED, "BVH deeper than the traversal stack");
     std::vector<GaussPrim> sorted_prims(kept);
     for (uint32_t i = 0; i < kept; ++i) sorted_prims[i] = prims[bvh.order[i]];
 

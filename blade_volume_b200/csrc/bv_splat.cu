@@ -34,7 +34,7 @@ namespace {
 
 constexpr int kSplatBlock = 128;
 constexpr int kSplatWindow = 16;
-constexpr int kSplatStack = 80;  // > BVH depth (40 + log2(N / 4))
+constexpr int kSplatStack = 80;  // > BVH depth, checked at tracer creation
 
 // One support sphere in BVH leaf order, 32 B.
 struct __align__(16) SplatPrim {
@@ -487,6 +487,8 @@ bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *md, const bv_trace_
         }
     }
     BvhBuild bvh = build_bvh(boxes, centers);
+    if (bvh_depth(bvh.nodes) >= (uint32_t)kSplatStack)
+        return sp_fail(BV_ERR_NOT_SUPPORTED, "BVH deeper than the traversal stack");
     std::vector<SplatPrim> prims(n);
     for (uint32_t i = 0; i < n; ++i) {
         const uint32_t c = bvh.order[i];

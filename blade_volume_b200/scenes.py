@@ -447,3 +447,41 @@ def relight_workload(n: int = 1_000_000, width: int = 1024, height: int = 768, s
     g = relight_gaussians(n, seed)
     cam = sphere_cameras(1, 3.0, 1, math.radians(60.0), width / height, 100.0)[0]
     return g, cam, sphere_lights()
+
+
+# --------------------------------------------------------------------------
+# SH-coloured Gaussians (GaussianGpuCloud input)
+# --------------------------------------------------------------------------
+@dataclasses.dataclass
+class GaussianShModel:
+    """Gaussian PointCloudModel with Transforms and SH colour (lib.rs:174-239):
+    mean + opacity, rotation (x, y, z, w), scale, SH rows [N, 3K]."""
+
+    points: np.ndarray  # float32 [N, 4]
+    rotations: np.ndarray  # float32 [N, 4]
+    scales: np.ndarray  # float32 [N, 3]
+    sh: np.ndarray  # float32 [N, 3K]
+    sh_degree: int
+
+    @property
+    def n(self) -> int:
+        return int(self.points.shape[0])
+
+
+def gaussian_sh(n: int = 1_000_000, seed: int = 0, sh_degree: int = 3,
+                log_scale_mean: float = -4.0) -> GaussianShModel:
+    """Anisotropic Gaussians with the relight scene's geometry distribution
+    (means from the 3-component mixture, log-scales N(log_scale_mean, 0.5),
+    rotations normalised N(0, 1)^4, opacity sigmoid(N(0, 1))) and SH colour:
+    DC from a uniform [0, 1] colour, higher coefficients N(0, 0.2)."""
+    rng = np.random.default_rng(seed)
+    means = mixture_points(rng, n).astype(np.float32)
+    scales = np.exp(rng.normal(log_scale_mean, 0.5, (n, 3))).astype(np.float32)
+    q = rng.standard_normal((n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    opacity = (1.0 / (1.0 + np.exp(-rng.standard_normal(n)))).astype(np.float32)
+    k = (sh_degree + 1) ** 2
+    sh = rng.normal(0.0, 0.2, (n, 3 * k)).astype(np.float32)
+    sh[:, 0:3] = _dc_from_color(rng.random((n, 3)))
+    points = np.concatenate([means, opacity[:, None]], axis=1).astype(np.float32)
+    return GaussianShModel(points, q.astype(np.float32), scales, sh, sh_degree)

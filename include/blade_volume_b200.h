@@ -325,6 +325,52 @@ bv_status bv_powerfoam_splat_tracer_set_weight_threshold(bv_splat_tracer *tracer
 bv_status bv_powerfoam_splat_tracer_enable_stats(bv_splat_tracer *tracer, uint32_t enabled);
 bv_status bv_powerfoam_splat_tracer_last_stats(bv_splat_tracer *tracer, bv_launch_stats *out);
 
+/* ---- Gaussian ray tracing with SH colour ---------------------------------
+ * GaussianGpuCloud (blade-volume/src/gpu/gaussian.rs:94-280) and its draw
+ * pass (shaders/gaussian.wgsl, gaussian_trace.wgsl:66-177) with the hit rule
+ * of the CPU oracle trace_gaussians (trace.rs:695-773): particles with
+ * opacity > min_opacity; per ray every particle whose maximum response
+ * alpha = opacity * exp(-|R^-1 (o + t d - mean) / scale|^2 / 2) at its
+ * maximum-response depth t in (0, camera depth) reaches min_opacity,
+ * composited in strict (t, model index) order, colour max(0, 0.5 + SH(d)),
+ * until the transmittance is at most min_transmittance. */
+typedef struct bv_gaussian_sh_desc { /* Gaussian PointCloudModel (lib.rs:174-239) */
+    uint32_t num_points;
+    uint32_t sh_degree;              /* 0..3 */
+    const float *points;             /* [N*4] mean xyz, opacity */
+    const float *rotations;          /* [N*4] unit quaternion x, y, z, w */
+    const float *scales;             /* [N*3] */
+    const float *sh_coefficients;    /* [N*3*K] [point][component][rgb] */
+} bv_gaussian_sh_desc;
+
+typedef struct bv_gaussian_trace_settings { /* GaussianTraceSettings (trace.rs:106-126) */
+    float min_opacity;        /* default 0.01; also InitParameters::min_opacity */
+    float min_transmittance;  /* default 0.01 */
+    float background[3];      /* radiance behind the last hit (gaussian.wgsl BACKGROUND) */
+} bv_gaussian_trace_settings;
+
+typedef struct bv_gaussian_tracer bv_gaussian_tracer;
+
+/* Validates the model, keeps particles above min_opacity, builds the device
+ * particle table and a BVH over the support ellipsoids.  settings may be
+ * NULL (defaults). */
+bv_status bv_gaussian_tracer_new(const bv_gaussian_sh_desc *model,
+                                 const bv_gaussian_trace_settings *settings,
+                                 bv_gaussian_tracer **out);
+void bv_gaussian_tracer_destroy(bv_gaussian_tracer *tracer);
+bv_status bv_gaussian_tracer_set_min_transmittance(bv_gaussian_tracer *tracer, float value);
+bv_status bv_gaussian_tracer_set_background(bv_gaussian_tracer *tracer, const float rgb[3]);
+/* particles kept (GaussianGpuCloud::num_points) */
+uint32_t bv_gaussian_tracer_num_points(const bv_gaussian_tracer *tracer);
+/* Renders width x height into out_rgba_dev ([h][w][4] float32):
+ * (radiance + T * background, 1 - T). */
+bv_status bv_gaussian_tracer_dispatch(bv_gaussian_tracer *tracer, float *out_rgba_dev,
+                                      const bv_camera *camera, uint32_t width, uint32_t height,
+                                      bv_stream stream);
+/* rays, composited hits (steps) and BVH nodes visited (faces) of the last dispatch */
+bv_status bv_gaussian_tracer_enable_stats(bv_gaussian_tracer *tracer, uint32_t enabled);
+bv_status bv_gaussian_tracer_last_stats(bv_gaussian_tracer *tracer, bv_launch_stats *out);
+
 /* ---- allocation-free start-cell search -----------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
  * hosts whose device memory is owned by their own pool (a renderer's frame

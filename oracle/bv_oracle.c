@@ -1560,3 +1560,91 @@ void bvo_relight_render(const bvo_relight_scene *s, const bvo_point_light *light
     }
     (void)threads;
 }
+
+/* ------------------------------------------------------------------ */
+/* Gaussian ray tracing with SH colour (trace.rs:695-773)              */
+/* ------------------------------------------------------------------ */
+
+/* Maximum-response depth and alpha of particle i (trace.rs:731-747), the
+ * local ray formed with qrot of the inverse rotation and a per-axis
+ * division by the scale (gaussian_trace.wgsl:147-151). */
+int bvo_gaussian_response(const bvo_gaussian_scene *s, uint32_t i, const float o[3],
+                          const float d[3], const bvo_gaussian_settings *st, float *t_out,
+                          float *alpha_out) {
+    const float *q = s->rotation + 4 * (size_t)i;
+    const float qi[4] = {-q[0], -q[1], -q[2], q[3]};
+    const float *c = s->center + 3 * (size_t)i;
+    const float *sc = s->scale + 3 * (size_t)i;
+    float oc[3], lo[3], ld[3];
+    sub3f(o, c, oc);
+    qrot_f(qi, oc, lo);
+    qrot_f(qi, d, ld);
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = lo[k] / sc[k];
+        ld[k] = ld[k] / sc[k];
+    }
+    const float t = -dot3f(lo, ld) / dot3f(ld, ld);
+    if (!(t > st->t_start && t < st->t_end)) return 0;
+    const float p[3] = {lo[0] + t * ld[0], lo[1] + t * ld[1], lo[2] + t * ld[2]};
+    const float alpha = s->opacity[i] * bvo_expf(-0.5f * dot3f(p, p));
+    if (!(alpha >= st->min_opacity)) return 0;
+    *t_out = t;
+    *alpha_out = alpha;
+    return 1;
+}
+
+void bvo_trace_gaussians(const bvo_gaussian_scene *s, const float o[3], const float d[3],
+                         const bvo_gaussian_settings *st, const float background[3],
+                         float rgba[4], uint32_t *hits_out) {
+    relight_hit *hits = NULL;
+    size_t nh = 0, cap = 0;
+    for (uint32_t i = 0; i < s->n; ++i) {
+        float t, a;
+        if (!bvo_gaussian_response(s, i, o, d, st, &t, &a)) continue;
+        if (nh == cap) {
+            cap = cap ? cap * 2 : 64;
+            hits = (relight_hit *)realloc(hits, cap * sizeof(relight_hit));
+        }
+        hits[nh].t = t;
+        hits[nh].index = i;
+        hits[nh].alpha = a;
+        nh += 1;
+    }
+    /* hits.sort_by(t.total_cmp, then index) (trace.rs:750): t is finite here */
+    qsort(hits, nh, sizeof(relight_hit), cmp_hit);
+    const bvo_model m = {NULL, NULL, s->sh, s->sh_degree, NULL, NULL, s->n};
+    float radiance[3] = {0.0f, 0.0f, 0.0f}, T = 1.0f;
+    uint32_t used = 0;
+    for (size_t k = 0; k < nh; ++k) {
+        if (T <= st->min_transmittance) break;
+        float color[3], unclamped[3];
+        bvo_eval_rgb_sh(&m, hits[k].index, d, color, unclamped);
+        const float w = hits[k].alpha * T;
+        for (int c = 0; c < 3; ++c) radiance[c] += w * color[c];
+        T *= 1.0f - hits[k].alpha;
+        used += 1;
+    }
+    free(hits);
+    for (int c = 0; c < 3; ++c) rgba[c] = radiance[c] + T * background[c];
+    rgba[3] = 1.0f - T;
+    if (hits_out) *hits_out = used;
+}
+
+void bvo_gaussian_render(const bvo_gaussian_scene *s, const bvo_camera *cam, uint32_t width,
+                         uint32_t height, float min_opacity, float min_transmittance,
+                         const float background[3], float *out_rgba, uint32_t *out_hits,
+                         int threads) {
+    const bvo_gaussian_settings st = {min_opacity, min_transmittance, 0.0f, cam->depth};
+    const long total = (long)width * (long)height;
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threads)
+#endif
+    for (long i = 0; i < total; ++i) {
+        float o[3], d[3];
+        relight_camera_ray(cam, width, height, (uint32_t)(i % width), (uint32_t)(i / width), o, d);
+        bvo_trace_gaussians(s, o, d, &st, background, out_rgba + 4 * (size_t)i,
+                            out_hits ? out_hits + i : NULL);
+    }
+    (void)threads;
+}

@@ -233,6 +233,45 @@ void bvo_relight_render(const bvo_relight_scene *s, const bvo_point_light *light
                         uint32_t height, const float background[3], float *out_rgba,
                         uint32_t *out_hits, int threads);
 
+/* ---- Gaussian ray tracing with SH colour (trace.rs:695-773) ----
+ * Particles with opacity > min_opacity only (GaussianGpuCloud::new,
+ * gpu/gaussian.rs:19-27); index = position in this filtered list, which
+ * keeps the model's order.  A hit is the point of maximum response along
+ * the ray: local ray R^-1 (o - mean) / scale (qrot of the inverse rotation,
+ * common.wgsl:386-390, as gaussian_trace.wgsl:147-148 evaluates it),
+ * t = -<o', d'> / |d'|^2 in (t_start, t_end), alpha = opacity *
+ * exp(-|o' + t d'|^2 / 2) >= min_opacity; hits are composited in strict
+ * (t, index) order until transmittance <= min_transmittance. */
+typedef struct {
+    uint32_t n;
+    const float *center;   /* [n*3] */
+    const float *rotation; /* [n*4] x, y, z, w */
+    const float *scale;    /* [n*3] */
+    const float *opacity;  /* [n] */
+    const float *sh;       /* [n*3K] */
+    uint32_t sh_degree;
+} bvo_gaussian_scene;
+
+typedef struct { /* GaussianTraceSettings (trace.rs:106-126) */
+    float min_opacity;
+    float min_transmittance;
+    float t_start;
+    float t_end;
+} bvo_gaussian_settings;
+
+int bvo_gaussian_response(const bvo_gaussian_scene *s, uint32_t i, const float o[3],
+                          const float d[3], const bvo_gaussian_settings *st, float *t,
+                          float *alpha);
+/* One ray: rgba = (radiance + T * background, 1 - T); hits = composited. */
+void bvo_trace_gaussians(const bvo_gaussian_scene *s, const float o[3], const float d[3],
+                         const bvo_gaussian_settings *st, const float background[3],
+                         float rgba[4], uint32_t *hits);
+/* Image of one camera with the relight/trace_main ray mapping, t in (0, depth). */
+void bvo_gaussian_render(const bvo_gaussian_scene *s, const bvo_camera *cam, uint32_t width,
+                         uint32_t height, float min_opacity, float min_transmittance,
+                         const float background[3], float *out_rgba, uint32_t *out_hits,
+                         int threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,6 +68,16 @@ class RelightScene(C.Structure):
                 ("material", u32p), ("materials", C.POINTER(Material))]
 
 
+class GaussianScene(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("center", f32p), ("rotation", f32p), ("scale", f32p),
+                ("opacity", f32p), ("sh", f32p), ("sh_degree", C.c_uint32)]
+
+
+class GaussianSettings(C.Structure):
+    _fields_ = [("min_opacity", C.c_float), ("min_transmittance", C.c_float),
+                ("t_start", C.c_float), ("t_end", C.c_float)]
+
+
 class ParamsF64(C.Structure):
     _fields_ = [("points", f64p), ("sh", f64p), ("radii", f64p)]
 
@@ -138,6 +148,14 @@ def lib():
         L.bvo_relight_render.argtypes = [C.POINTER(RelightScene), C.POINTER(PointLight),
                                          C.c_uint32, C.POINTER(Camera), C.c_uint32, C.c_uint32,
                                          f32p, f32p, u32p, C.c_int]
+        L.bvo_gaussian_response.restype = C.c_int
+        L.bvo_gaussian_response.argtypes = [C.POINTER(GaussianScene), C.c_uint32, f32p, f32p,
+                                            C.POINTER(GaussianSettings), f32p, f32p]
+        L.bvo_trace_gaussians.argtypes = [C.POINTER(GaussianScene), f32p, f32p,
+                                          C.POINTER(GaussianSettings), f32p, f32p, u32p]
+        L.bvo_gaussian_render.argtypes = [C.POINTER(GaussianScene), C.POINTER(Camera), C.c_uint32,
+                                          C.c_uint32, C.c_float, C.c_float, f32p, f32p, u32p,
+                                          C.c_int]
         _lib = L
     return _lib
 
@@ -468,4 +486,61 @@ def relight_render(scene: RelightOracleScene, lights, cam, width, height,
     cs = camera_struct(cam)
     lib().bvo_relight_render(C.byref(scene.c), arr, len(arr), C.byref(cs), width, height,
                              _ptr(bg, f32p), _ptr(out, f32p), _ptr(hits, u32p), threads)
+    return out, hits
+
+
+# --------------------------------------------------------------------------
+# Gaussian ray tracing with SH colour (trace.rs:695-773)
+# --------------------------------------------------------------------------
+class GaussianOracleScene:
+    """Particles with opacity > min_opacity (gpu/gaussian.rs:19-27), in model
+    order, for the C side."""
+
+    def __init__(self, points, rotations, scales, sh, sh_degree, min_opacity=0.01):
+        points = np.ascontiguousarray(points, np.float32).reshape(-1, 4)
+        keep = points[:, 3] > np.float32(min_opacity)
+        self.kept = np.nonzero(keep)[0].astype(np.uint32)
+        self.center = np.ascontiguousarray(points[keep, :3])
+        self.opacity = np.ascontiguousarray(points[keep, 3])
+        self.rotation = np.ascontiguousarray(
+            np.asarray(rotations, np.float32).reshape(-1, 4)[keep])
+        self.scale = np.ascontiguousarray(np.asarray(scales, np.float32).reshape(-1, 3)[keep])
+        k = (int(sh_degree) + 1) ** 2
+        self.sh = np.ascontiguousarray(np.asarray(sh, np.float32).reshape(-1, 3 * k)[keep])
+        self.n = int(keep.sum())
+        self.min_opacity = float(min_opacity)
+        self.c = GaussianScene(self.n, _ptr(self.center, f32p), _ptr(self.rotation, f32p),
+                               _ptr(self.scale, f32p), _ptr(self.opacity, f32p),
+                               _ptr(self.sh, f32p), int(sh_degree))
+
+    @classmethod
+    def from_scene(cls, g, min_opacity=0.01):
+        return cls(g.points, g.rotations, g.scales, g.sh, g.sh_degree, min_opacity)
+
+
+def trace_gaussians(scene: GaussianOracleScene, origin, direction, min_transmittance=0.01,
+                    t_start=0.0, t_end=10000.0, background=(0.0, 0.0, 0.0)):
+    """One ray; returns (rgba, composited hits).  ``direction`` is used as
+    given (normalise it first, as trace_gaussians does)."""
+    out = np.zeros(4, np.float32)
+    hits = np.zeros(1, np.uint32)
+    o = np.ascontiguousarray(origin, np.float32)
+    d = np.ascontiguousarray(direction, np.float32)
+    bg = np.ascontiguousarray(background, np.float32)
+    st = GaussianSettings(scene.min_opacity, float(min_transmittance), float(t_start),
+                          float(t_end))
+    lib().bvo_trace_gaussians(C.byref(scene.c), _ptr(o, f32p), _ptr(d, f32p), C.byref(st),
+                              _ptr(bg, f32p), _ptr(out, f32p), _ptr(hits, u32p))
+    return out, int(hits[0])
+
+
+def gaussian_render(scene: GaussianOracleScene, cam, width, height, min_transmittance=0.01,
+                    background=(0.0, 0.0, 0.0), threads=0):
+    out = np.zeros((height, width, 4), np.float32)
+    hits = np.zeros((height, width), np.uint32)
+    bg = np.ascontiguousarray(background, np.float32)
+    cs = camera_struct(cam)
+    lib().bvo_gaussian_render(C.byref(scene.c), C.byref(cs), width, height, scene.min_opacity,
+                              float(min_transmittance), _ptr(bg, f32p), _ptr(out, f32p),
+                              _ptr(hits, u32p), threads)
     return out, hits
