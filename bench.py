@@ -94,9 +94,10 @@ def dist_env():
 def build_workload(args, rank):
     from blade_volume_b200 import scenes
 
+    from blade_volume_b200 import dist as bvdist
+
     model = scenes.radfoam_ball(args.sites, seed=0, sh_degree=3)
-    cams = scenes.sphere_cameras(args.views, 3.0, 1 + rank, math.radians(60.0), 1.0, 100.0)
-    return model, cams
+    return model, bvdist.rank_cameras(args.views, rank)
 
 
 def peaks():
@@ -454,6 +455,7 @@ def main():
     import torch
 
     import blade_volume_b200 as bv
+    from blade_volume_b200 import dist as bvdist
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -489,8 +491,7 @@ def main():
         tracer.forward_backward(cams, W, H, target, grads, max_steps=MAX_STEPS,
                                 weight_threshold=0.0, max_dt=MAX_DT, loss_out=loss)
         if dist is not None:
-            for g in grads.values():
-                dist.all_reduce(g)
+            bvdist.allreduce_grads(grads, dist)
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -530,9 +531,7 @@ def main():
     tracer.enable_stats(False)
     total_ms = sum(times)
     if dist is not None:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = bvdist.max_over_ranks([total_ms], dist, "cuda")[0]
     ms_per_step = total_ms / args.steps
     value = rays * world / (ms_per_step * 1e-3) / 1e6
 
@@ -569,8 +568,7 @@ def main():
         tracer.forward_backward(cams, W, H, dev_target, grads, max_steps=MAX_STEPS,
                                 weight_threshold=0.0, max_dt=MAX_DT, loss_out=loss)
         if dist is not None:
-            for g in grads.values():
-                dist.all_reduce(g)
+            bvdist.allreduce_grads(grads, dist)
         host_loss.copy_(loss, non_blocking=True)
         e1.record(stream)
         e1.synchronize()
@@ -578,9 +576,7 @@ def main():
             e2e_times.append(e0.elapsed_time(e1))
     e2e_ms = sum(e2e_times) / len(e2e_times)
     if dist is not None:
-        t = torch.tensor([e2e_ms, fwd_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms, fwd_ms = (float(x) for x in t.tolist())
+        e2e_ms, fwd_ms = bvdist.max_over_ranks([e2e_ms, fwd_ms], dist, "cuda")
 
     # roofline of the dominant kernel (the replay backward), with the
     # per-step byte model of the reference's FP32 AoS layout:

@@ -44,7 +44,8 @@ EXPORTED_SYMBOLS = [
     "bv_last_error", "bv_abi_version", "bv_model_validate", "bv_radfoam_tracer_new",
     "bv_radfoam_tracer_destroy", "bv_radfoam_tracer_dispatch", "bv_radfoam_tracer_dispatch_batch",
     "bv_radfoam_tracer_set_max_steps", "bv_radfoam_tracer_set_weight_threshold",
-    "bv_radfoam_tracer_set_debug_cell_density", "bv_radfoam_tracer_max_steps",
+    "bv_radfoam_tracer_set_debug_cell_density", "bv_radfoam_tracer_set_tie_break",
+    "bv_radfoam_tracer_max_steps",
     "bv_radfoam_tracer_weight_threshold", "bv_radfoam_tracer_sh_degree",
     "bv_radfoam_tracer_start_point", "bv_radfoam_tracer_num_points", "bv_containing_point",
     "bv_record_paths", "bv_forward_backward", "bv_radfoam_tracer_enable_stats",
@@ -214,6 +215,7 @@ def load_library(path: str = LIB_PATH):
     L.bv_radfoam_tracer_set_max_steps.argtypes = [C.c_void_p, C.c_uint32]
     L.bv_radfoam_tracer_set_weight_threshold.argtypes = [C.c_void_p, C.c_float]
     L.bv_radfoam_tracer_set_debug_cell_density.argtypes = [C.c_void_p, C.c_uint32]
+    L.bv_radfoam_tracer_set_tie_break.argtypes = [C.c_void_p, C.c_uint32]
     L.bv_radfoam_tracer_max_steps.argtypes = [C.c_void_p]
     L.bv_radfoam_tracer_max_steps.restype = C.c_uint32
     L.bv_radfoam_tracer_weight_threshold.argtypes = [C.c_void_p]
@@ -408,6 +410,11 @@ class RadFoamGpuTracer:
 
     def set_debug_cell_density(self, enabled: bool):
         _check(load_library().bv_radfoam_tracer_set_debug_cell_density(self._h, int(enabled)))
+
+    def set_tie_break(self, enabled: bool):
+        """Render walk: FP64 re-evaluation of exit faces tied within 4 FP32 ulps
+        (False: the reference's first-minimum rule)."""
+        _check(load_library().bv_radfoam_tracer_set_tie_break(self._h, int(enabled)))
 
     @property
     def max_steps(self) -> int:

@@ -72,6 +72,7 @@ struct bv_tracer {
     bool bf16 = false;
     bool bounded = false;
     bv_trace_settings settings{};
+    uint32_t tie_break = 0;            // render walk: FP64 exit-face tie-break
     // device model
     float4 *geom = nullptr;
     float *density = nullptr;
@@ -457,6 +458,7 @@ bv_status bv_radfoam_tracer_dispatch_batch(bv_tracer *t, float *out_rgba_dev,
         p.stats = t->stats_enabled ? t->stats : nullptr;
         p.out_rgba = reinterpret_cast<float4 *>(out_rgba_dev) + (size_t)c0 * width * height;
         p.debug_cell_density = t->settings.debug_cell_density;
+        p.tie_break = t->tie_break;
         BV_CUDA(cudaMemsetAsync(t->work_counter, 0, sizeof(uint32_t), s), "counter reset");
         const int blocks_needed = (int)((work + 255) / 256);
         const int grid = std::min(t->grid_forward, std::max(blocks_needed, 1));
@@ -488,6 +490,13 @@ bv_status bv_radfoam_tracer_set_weight_threshold(bv_tracer *t, float w) {
 bv_status bv_radfoam_tracer_set_debug_cell_density(bv_tracer *t, uint32_t enabled) {
     if (!t) return fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
     t->settings.debug_cell_density = enabled ? 1u : 0u;
+    return BV_OK;
+}
+
+bv_status bv_radfoam_tracer_set_tie_break(bv_tracer *t, uint32_t mode) {
+    if (!t) return fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
+    if (mode > BV_TIE_BREAK_F64) return fail(BV_ERR_INVALID_ARGUMENT, "unknown tie-break mode");
+    t->tie_break = mode;
     return BV_OK;
 }
 

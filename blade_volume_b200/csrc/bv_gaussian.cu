@@ -101,12 +101,14 @@ __device__ __forceinline__ bool response(const GaussianParams &P, uint32_t pos, 
 
 template <int DEG>
 __global__ void __launch_bounds__(kGaussBlock) gaussian_kernel(const __grid_constant__ GaussianParams P) {
+    // whole warps past the last tile leave together; lanes of a partial edge
+    // tile stay (inactive) because the traversal is warp-cooperative
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= P.total_work) return;
+    if ((w & ~31u) >= P.total_work) return;
     const uint32_t tile = w / 32u, in = w % 32u;
     const uint32_t x = (tile % P.tiles_x) * 8u + in % 8u;
     const uint32_t y = (tile / P.tiles_x) * 4u + in / 8u;
-    if (x >= P.width || y >= P.height) return;
+    const bool active = x < P.width && y < P.height;
 
     // pixel -> ray: radfoam.wgsl:44-52 mapping, one normalisation
     WinRay ray;
@@ -125,26 +127,29 @@ __global__ void __launch_bounds__(kGaussBlock) gaussian_kernel(const __grid_cons
         ray.ox = P.origin[0];
         ray.oy = P.origin[1];
         ray.oz = P.origin[2];
-        ray.ix = 1.0f / ray.dx;
-        ray.iy = 1.0f / ray.dy;
-        ray.iz = 1.0f / ray.dz;
+        ray.ix = win_inverse(ray.dx);
+        ray.iy = win_inverse(ray.dy);
+        ray.iz = win_inverse(ray.dz);
     }
 
     float rad_r = 0.f, rad_g = 0.f, rad_b = 0.f, T = 1.0f;
-    bool cursor_valid = false;
+    bool cursor_valid = false, finished = !active;
     float cur_t = 0.f;
     uint32_t cur_idx = 0, hits_used = 0, nodes_visited = 0;
-    auto hit = [&](uint32_t p, float &t, uint32_t &id) -> bool {
+    auto hit = [&](uint32_t p, bool mine, float, float &t, uint32_t &id, uint32_t &) -> bool {
         float a;
-        if (!response(P, p, ray, t, a)) return false;
+        if (!mine || !response(P, p, ray, t, a)) return false;
         id = __ldg(&P.ids[p]);
         return true;
     };
-    while (T > P.min_transmittance) {
+    for (;;) {
+        const bool want = !finished && T > P.min_transmittance;
+        if (!__any_sync(0xffffffffu, want)) break;
         WinKey buf[kWindow];
-        const int count = win_gather<kWindow, kStack>(P.nodes, ray, P.depth, cursor_valid, cur_t,
-                                                      cur_idx, buf, nodes_visited, hit);
-        if (count == 0) break;
+        const int count = win_gather_warp<kWindow, kStack>(P.nodes, ray, P.depth, want,
+                                                           cursor_valid, cur_t, cur_idx, buf,
+                                                           nodes_visited, hit);
+        if (!want) continue;
 #pragma unroll 1
         for (int i = 0; i < count; ++i) {
             if (T <= P.min_transmittance) break;
@@ -173,11 +178,15 @@ __global__ void __launch_bounds__(kGaussBlock) gaussian_kernel(const __grid_cons
             T *= 1.0f - a;
             hits_used += 1;
         }
-        if (count < kWindow) break;
-        cursor_valid = true;
-        cur_t = buf[kWindow - 1].t;
-        cur_idx = buf[kWindow - 1].idx;
+        if (count < kWindow) {
+            finished = true;
+        } else {
+            cursor_valid = true;
+            cur_t = buf[kWindow - 1].t;
+            cur_idx = buf[kWindow - 1].idx;
+        }
     }
+    if (!active) return;
     const size_t o = (size_t)y * P.width + x;
     P.out[o] = make_float4(rad_r + T * P.background[0], rad_g + T * P.background[1],
                            rad_b + T * P.background[2], 1.0f - T);

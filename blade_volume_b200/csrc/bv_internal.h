@@ -65,6 +65,7 @@ struct WalkParams {
     unsigned long long *stats;    // [3] rays, steps, faces (or null)
     float4 *out_rgba;             // [n_views][H][W]
     uint32_t debug_cell_density;
+    uint32_t tie_break;           // FP64 re-evaluation of near-tied exit faces
     ViewDesc views[kMaxViewsPerLaunch];
 };
 

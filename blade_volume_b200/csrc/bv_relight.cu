@@ -183,12 +183,14 @@ __device__ __forceinline__ void shade_light(const RelightLight &L, float px, flo
 
 __global__ void __launch_bounds__(kRelightBlock)
 relight_kernel(const __grid_constant__ RelightParams P) {
+    // whole warps past the last tile leave together; lanes of a partial edge
+    // tile stay (inactive) because the traversal is warp-cooperative
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= P.total_work) return;
+    if ((w & ~31u) >= P.total_work) return;
     const uint32_t tile = w / 32u, in = w % 32u;
     const uint32_t x = (tile % P.tiles_x) * 8u + in % 8u;
     const uint32_t y = (tile / P.tiles_x) * 4u + in / 8u;
-    if (x >= P.width || y >= P.height) return;
+    const bool active = x < P.width && y < P.height;
 
     // trace_main ray mapping (relight.wgsl:760-766): one normalisation
     WinRay ray;
@@ -207,9 +209,9 @@ relight_kernel(const __grid_constant__ RelightParams P) {
         ray.ox = P.origin[0];
         ray.oy = P.origin[1];
         ray.oz = P.origin[2];
-        ray.ix = 1.0f / ray.dx;
-        ray.iy = 1.0f / ray.dy;
-        ray.iz = 1.0f / ray.dz;
+        ray.ix = win_inverse(ray.dx);
+        ray.iy = win_inverse(ray.dy);
+        ray.iz = win_inverse(ray.dz);
     }
     const float t_end = P.depth;
 
@@ -220,19 +222,26 @@ relight_kernel(const __grid_constant__ RelightParams P) {
     float cur_t = 0.f;
     uint32_t cur_idx = 0;
     uint32_t hits_used = 0, nodes_visited = 0;
-    auto hit = [&](uint32_t p, float &t, uint32_t &id) -> bool {
+    auto hit = [&](uint32_t p, bool mine, float, float &t, uint32_t &id, uint32_t &) -> bool {
         float a;
-        if (!intersect(P.prims, p, ray, t_end, t, a) || !(a > 0.0f)) return false;
+        if (!mine || !intersect(P.prims, p, ray, t_end, t, a) || !(a > 0.0f)) return false;
         id = __ldg(&P.prims[p].ids.x);
         return true;
     };
 
+    bool finished = !active;
     for (;;) {
-        // ---- gather the next window of keys above the cursor
+        // ---- gather the next window of keys above the cursor (whole warp)
+        const bool want = !finished;
+        if (!__any_sync(0xffffffffu, want)) break;
         WinKey buf[kWindow];
-        const int count = win_gather<kWindow, kRelightStack>(P.nodes, ray, t_end, cursor_valid, cur_t,
-                                                      cur_idx, buf, nodes_visited, hit);
-        if (count == 0) break;
+        const int count = win_gather_warp<kWindow, kRelightStack>(
+            P.nodes, ray, t_end, want, cursor_valid, cur_t, cur_idx, buf, nodes_visited, hit);
+        if (!want) continue;
+        if (count == 0) {
+            finished = true;
+            continue;
+        }
         // ---- composite the window in order (trace_blended :693-728)
 #pragma unroll 1
         for (int i = 0; i < count; ++i) {
@@ -284,7 +293,10 @@ relight_kernel(const __grid_constant__ RelightParams P) {
             sum_w += a;
             group_T *= 1.0f - a;
         }
-        if (stopped) break;
+        if (stopped) {
+            finished = true;
+            continue;
+        }
         if (count < kWindow) {
             if (group) {
                 const float a_sum = fminf(1.0f, sum_w);
@@ -297,7 +309,8 @@ relight_kernel(const __grid_constant__ RelightParams P) {
                 T *= 1.0f - alpha;
                 group = false;
             }
-            break;
+            finished = true;
+            continue;
         }
         cursor_valid = true;
         cur_t = buf[kWindow - 1].t;
@@ -313,6 +326,7 @@ relight_kernel(const __grid_constant__ RelightParams P) {
         rad_b += T * (alpha * sc_b / wmax);
         T *= 1.0f - alpha;
     }
+    if (!active) return;
     const size_t o = (size_t)y * P.width + x;
     P.out[o] = make_float4(rad_r + T * P.background[0], rad_g + T * P.background[1],
                            rad_b + T * P.background[2], 1.0f - T);

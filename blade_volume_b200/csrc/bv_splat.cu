@@ -28,6 +28,7 @@
 #include "bv_bvh.h"
 #include "bv_device.cuh"
 #include "bv_internal.h"
+#include "bv_window.cuh"
 
 namespace bv {
 namespace {
@@ -59,40 +60,16 @@ struct SplatParams {
     ViewDesc views[kMaxViewsPerLaunch];
 };
 
-struct SplatKey {
-    float t;
-    float dt;
-    uint32_t cell;
-};
-
-__device__ __forceinline__ bool key_less(float ta, uint32_t ia, float tb, uint32_t ib) {
-    return ta < tb || (ta == tb && ia < ib);
-}
-
-// 1/d with |d| raised to at least 1e-30, so that a box face through the ray
-// origin gives 0 * finite rather than 0 * inf = NaN in the slab test.
-__device__ __forceinline__ float safe_inverse(float d) {
-    return 1.0f / (fabsf(d) < 1e-30f ? copysignf(1e-30f, d) : d);
-}
-
-// Slab test of a box against the ray within [0, t_end], widened by a small
-// relative margin so that FP32 rounding can only keep a box, never drop one.
-__device__ __forceinline__ bool slab(const float4 &lo, const float4 &hi, const Ray &r, float ix,
-                                     float iy, float iz, float t_end, float &tn, float &tf) {
-    const float ax = (lo.x - r.ox) * ix, bx = (hi.x - r.ox) * ix;
-    const float ay = (lo.y - r.oy) * iy, by = (hi.y - r.oy) * iy;
-    const float az = (lo.z - r.oz) * iz, bz = (hi.z - r.oz) * iz;
-    tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
-    tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), t_end));
-    tn = tn - (1e-5f * fabsf(tn) + 1e-6f);
-    tf = tf + (1e-5f * fabsf(tf) + 1e-6f);
-    return tn <= tf;
+// Slab test for the counting pass (per-lane traversal).
+__device__ __forceinline__ bool slab(const float4 &lo, const float4 &hi, const WinRay &r, float t_end,
+                                     float &tn, float &tf) {
+    return win_slab(lo, hi, r, t_end, tn, tf);
 }
 
 // Support-sphere test of powerfoam_splat_interval (trace.rs:1331-1350):
 // false when the camera is within 4 r of the site, the ray misses the sphere,
 // or the sphere lies behind the camera or beyond depth.
-__device__ __forceinline__ bool splat_sphere(const Ray &ray, const float4 &s, float depth,
+__device__ __forceinline__ bool splat_sphere(const WinRay &ray, const float4 &s, float depth,
                                              float &sn, float &sf) {
     const float cx = s.x - ray.ox, cy = s.y - ray.oy, cz = s.z - ray.oz;
     const float excl = 4.0f * s.w;
@@ -108,30 +85,49 @@ __device__ __forceinline__ bool splat_sphere(const Ray &ray, const float4 &s, fl
 }
 
 // Cech-row clip of one support (trace.rs:1351-1389, path_interval_jacobian
-// :1199-1325 for the bounded clip).  False when the interval is empty.
-__device__ __forceinline__ bool splat_clip(const SplatParams &P, const Ray &ray, const float4 &s,
-                                           uint32_t begin, uint32_t end, float depth, float sn,
-                                           float sf, float &start, float &dt) {
+// :1199-1325 for the bounded clip), warp-cooperative: every lane calls it
+// for the same support; the row is read 32 entries at a time (one coalesced
+// load per chunk) and each entry is broadcast to the lanes that clip (need).
+// face_near / face_far are a max / min over the row and a parallel face
+// with num < 0 empties the interval, so the result does not depend on the
+// order the entries are taken in.  False for lanes whose interval is empty.
+__device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinRay &ray,
+                                                const float4 &s, uint32_t begin, uint32_t end,
+                                                float depth, float sn, float sf, bool need,
+                                                float &start, float &dt) {
+    const uint32_t lane = threadIdx.x & 31u;
     float face_near = 0.0f, face_far = depth;
-    for (uint32_t k = begin; k < end; ++k) {
-        const float4 a = __ldg(P.row_sites + k);
-        const float nx = a.x - s.x, ny = a.y - s.y, nz = a.z - s.z;
-        const float dsq = fmaxf(dot3(nx, ny, nz, nx, ny, nz), 1.0e-20f);
-        const float shift = 0.5f + 0.5f * (s.w * s.w - a.w * a.w) / dsq;
-        const float fx = s.x + shift * nx, fy = s.y + shift * ny, fz = s.z + shift * nz;
-        const float rx = fx - ray.ox, ry = fy - ray.oy, rz = fz - ray.oz;
-        const float num = dot3(rx, ry, rz, nx, ny, nz);
-        const float den = dot3(ray.dx, ray.dy, ray.dz, nx, ny, nz);
-        if (den > 1.0e-20f) {
-            const float t = num / den;
-            if (t < face_far) face_far = t;
-        } else if (den < -1.0e-20f) {
-            const float t = num / den;
-            if (t > face_near) face_near = t;
-        } else if (num < 0.0f) {
-            return false;
+    bool empty = !need;
+    for (uint32_t base = begin; base < end; base += 32u) {
+        const uint32_t n = min(32u, end - base);
+        const float4 mine = base + lane < end ? __ldg(P.row_sites + base + lane)
+                                              : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (uint32_t j = 0; j < n; ++j) {
+            float4 a;
+            a.x = __shfl_sync(0xffffffffu, mine.x, j);
+            a.y = __shfl_sync(0xffffffffu, mine.y, j);
+            a.z = __shfl_sync(0xffffffffu, mine.z, j);
+            a.w = __shfl_sync(0xffffffffu, mine.w, j);
+            if (empty) continue;
+            const float nx = a.x - s.x, ny = a.y - s.y, nz = a.z - s.z;
+            const float dsq = fmaxf(dot3(nx, ny, nz, nx, ny, nz), 1.0e-20f);
+            const float shift = 0.5f + 0.5f * (s.w * s.w - a.w * a.w) / dsq;
+            const float fx = s.x + shift * nx, fy = s.y + shift * ny, fz = s.z + shift * nz;
+            const float rx = fx - ray.ox, ry = fy - ray.oy, rz = fz - ray.oz;
+            const float num = dot3(rx, ry, rz, nx, ny, nz);
+            const float den = dot3(ray.dx, ray.dy, ray.dz, nx, ny, nz);
+            if (den > 1.0e-20f) {
+                const float t = num / den;
+                if (t < face_far) face_far = t;
+            } else if (den < -1.0e-20f) {
+                const float t = num / den;
+                if (t > face_near) face_near = t;
+            } else if (num < 0.0f) {
+                empty = true;
+            }
         }
     }
+    if (empty) return false;
     float st = face_near, en = face_far;
     if (sn > st) st = sn;
     if (sf < en) en = sf;
@@ -144,8 +140,11 @@ __device__ __forceinline__ bool splat_clip(const SplatParams &P, const Ray &ray,
 template <int DEG, bool BF16>
 __global__ void __launch_bounds__(kSplatBlock)
 splat_kernel(const __grid_constant__ SplatParams P) {
+    // A view's work is whole 8x4 tiles, so a warp is one tile of one view;
+    // whole warps past the end leave together, lanes of a partial edge tile
+    // stay (inactive) because the main pass is warp-cooperative.
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= P.total_work) return;
+    if ((w & ~31u) >= P.total_work) return;
     uint32_t view = 0;
     while (view + 1 < P.n_views && w >= P.views[view + 1].ray_begin) ++view;
     const ViewDesc &vd = P.views[view];
@@ -153,19 +152,26 @@ splat_kernel(const __grid_constant__ SplatParams P) {
     const uint32_t tile = local / kTileRays, in = local % kTileRays;
     const uint32_t x = (tile % vd.tiles_x) * kTileW + in % kTileW;
     const uint32_t y = (tile / vd.tiles_x) * kTileH + in / kTileW;
-    if (x >= vd.width || y >= vd.height) return;
+    const bool inside = x < vd.width && y < vd.height;
     float4 *out = P.out + (size_t)vd.pixel_begin + (size_t)y * vd.width + x;
-    Ray ray;
-    if (!make_ray(vd, x, y, ray)) {
-        if (!P.count_only) *out = make_float4(0.f, 0.f, 0.f, 0.f);
-        return;
-    }
-    const float ix = safe_inverse(ray.dx), iy = safe_inverse(ray.dy), iz = safe_inverse(ray.dz);
+    Ray r0{0.f, 0.f, 0.f, 1.f, 0.f, 0.f};
+    const bool active = inside && make_ray(vd, x, y, r0);
+    if (inside && !active && !P.count_only) *out = make_float4(0.f, 0.f, 0.f, 0.f);
+    WinRay ray;
+    ray.ox = r0.ox;
+    ray.oy = r0.oy;
+    ray.oz = r0.oz;
+    ray.dx = active ? r0.dx : 1.0f;
+    ray.dy = active ? r0.dy : 0.0f;
+    ray.dz = active ? r0.dz : 0.0f;
+    ray.ix = win_inverse(ray.dx);
+    ray.iy = win_inverse(ray.dy);
+    ray.iz = win_inverse(ray.dz);
     const float depth = vd.depth;
-    uint32_t clipped = 0;
 
     if (P.count_only) {
-        // every support hit, no window pruning
+        // every support hit, no window pruning, one ray per thread
+        if (!active) return;
         uint32_t hits = 0, entries = 0;
         uint32_t stack[kSplatStack];
         int sp = 0;
@@ -177,7 +183,7 @@ splat_kernel(const __grid_constant__ SplatParams P) {
             for (int c = 0; c < 2; ++c) {
                 const uint32_t cnt = __float_as_uint(hi[c].w);
                 float tn, tf;
-                if (cnt == kBvhNoChild || !slab(lo[c], hi[c], ray, ix, iy, iz, depth, tn, tf)) continue;
+                if (cnt == kBvhNoChild || !slab(lo[c], hi[c], ray, depth, tn, tf)) continue;
                 const uint32_t ref = __float_as_uint(lo[c].w);
                 if (cnt == 0u) {
                     if (sp < kSplatStack) stack[sp++] = ref;
@@ -199,90 +205,53 @@ splat_kernel(const __grid_constant__ SplatParams P) {
     }
 
     float T = 1.0f, ar = 0.f, ag = 0.f, ab = 0.f;
-    uint32_t steps = 0;
-    bool cursor_valid = false, done = false;
+    uint32_t steps = 0, clipped = 0, nodes_visited = 0;
+    bool cursor_valid = false, finished = !active;
     float cur_t = 0.f;
     uint32_t cur_cell = 0;
-    while (!done) {
-        // ---- the next window of keys above the cursor
-        SplatKey buf[kSplatWindow];
-        int count = 0;
-        uint32_t stack[kSplatStack];
-        int sp = 0;
-        stack[sp++] = 0u;
-        while (sp > 0) {
-            const BvhNode nd = P.nodes[stack[--sp]];
-            const float4 lo[2] = {nd.l_lo, nd.r_lo}, hi[2] = {nd.l_hi, nd.r_hi};
-            float tn[2], tf[2];
-            bool ok[2];
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                ok[c] = __float_as_uint(hi[c].w) != kBvhNoChild &&
-                        slab(lo[c], hi[c], ray, ix, iy, iz, depth, tn[c], tf[c]);
-                if (ok[c] && cursor_valid && tf[c] < cur_t) ok[c] = false;
-                if (ok[c] && count == kSplatWindow && tn[c] > buf[kSplatWindow - 1].t) ok[c] = false;
-            }
-            const int first = (ok[0] && ok[1] && tn[1] < tn[0]) ? 1 : 0;
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int c = k == 0 ? 1 - first : first;
-                if (!ok[c]) continue;
-                const uint32_t ref = __float_as_uint(lo[c].w);
-                const uint32_t cnt = __float_as_uint(hi[c].w);
-                if (cnt == 0u) {
-                    if (sp < kSplatStack) stack[sp++] = ref;
-                    continue;
-                }
-                for (uint32_t p = ref; p < ref + cnt; ++p) {
-                    const float4 s = __ldg(&P.prims[p].site);
-                    float sn, sf;
-                    if (!splat_sphere(ray, s, depth, sn, sf)) continue;
-                    // the clipped start lies in [sn, sf): skip supports whose
-                    // every key is at or below the cursor or above the window
-                    if (cursor_valid && sf <= cur_t) continue;
-                    if (count == kSplatWindow && sn > buf[kSplatWindow - 1].t) continue;
-                    const uint4 link = __ldg(&P.prims[p].link);
-                    clipped += link.z - link.y;
-                    float st, dt;
-                    if (!splat_clip(P, ray, s, link.y, link.z, depth, sn, sf, st, dt)) continue;
-                    if (cursor_valid && !key_less(cur_t, cur_cell, st, link.x)) continue;
-                    if (count == kSplatWindow &&
-                        !key_less(st, link.x, buf[kSplatWindow - 1].t, buf[kSplatWindow - 1].cell))
-                        continue;
-                    SplatKey nk{st, dt, link.x};
-#pragma unroll
-                    for (int i = 0; i < kSplatWindow; ++i) {
-                        if (i < count && key_less(nk.t, nk.cell, buf[i].t, buf[i].cell)) {
-                            const SplatKey tmp = buf[i];
-                            buf[i] = nk;
-                            nk = tmp;
-                        }
-                    }
-#pragma unroll
-                    for (int i = 0; i < kSplatWindow; ++i)
-                        if (i == count) buf[i] = nk;
-                    if (count < kSplatWindow) count += 1;
-                }
-            }
-        }
+    // support p: sphere test per lane, then the warp clips its Cech row for
+    // the lanes whose sphere interval can still enter their window
+    auto hit = [&](uint32_t p, bool mine, float limit, float &t, uint32_t &cell,
+                   uint32_t &aux) -> bool {
+        const float4 s = __ldg(&P.prims[p].site);
+        float sn = 0.f, sf = 0.f;
+        bool need = mine && splat_sphere(ray, s, depth, sn, sf);
+        // the clipped start lies in [sn, sf): skip supports whose every key is
+        // at or below the cursor or past the window end
+        if (need && cursor_valid && sf <= cur_t) need = false;
+        if (need && sn > limit) need = false;
+        if (!__any_sync(0xffffffffu, need)) return false;
+        const uint4 link = __ldg(&P.prims[p].link);
+        if (need) clipped += link.z - link.y;
+        float st, dt;
+        if (!splat_clip_warp(P, ray, s, link.y, link.z, depth, sn, sf, need, st, dt)) return false;
+        t = st;
+        cell = link.x;
+        aux = __float_as_uint(dt);
+        return true;
+    };
+    for (;;) {
+        const bool want = !finished;
+        if (!__any_sync(0xffffffffu, want)) break;
+        WinKey buf[kSplatWindow];
+        const int count = win_gather_warp<kSplatWindow, kSplatStack>(
+            P.nodes, ray, depth, want, cursor_valid, cur_t, cur_cell, buf, nodes_visited, hit);
+        if (!want) continue;
         // ---- composite the window in order (trace.rs:1490-1530)
 #pragma unroll 1
         for (int i = 0; i < count; ++i) {
-            SplatKey e = buf[0];
-#pragma unroll
-            for (int j = 0; j < kSplatWindow; ++j)
-                if (j == i) e = buf[j];
+            const WinKey e = win_at(buf, i);
             if (T <= P.weight_threshold || steps >= P.max_steps) {
-                done = true;
+                finished = true;
                 break;
             }
             steps += 1;
-            const float dens = __ldg(P.m.density + e.cell) * 1.0f;
+            const float dens = __ldg(P.m.density + e.idx) * 1.0f;
             if (dens <= 1.0e-6f) continue;
-            const float alpha = 1.0f - bv_expf(-dens * e.dt);
+            const float alpha = 1.0f - bv_expf(-dens * __uint_as_float(e.pos));
             const float wgt = T * alpha;
             float coef[ShDims<DEG>::N];
-            load_sh_row<DEG, BF16>(P.m, e.cell, coef);
+            load_sh_row<DEG, BF16>(P.m, e.idx, coef);
             float r, g, b;
             eval_sh<DEG>(coef, ray.dx, ray.dy, ray.dz, r, g, b);
             ar += wgt * fmaxf(r, 0.0f);
@@ -290,11 +259,16 @@ splat_kernel(const __grid_constant__ SplatParams P) {
             ab += wgt * fmaxf(b, 0.0f);
             T *= 1.0f - alpha;
         }
-        if (count < kSplatWindow) break;
-        cursor_valid = true;
-        cur_t = buf[kSplatWindow - 1].t;
-        cur_cell = buf[kSplatWindow - 1].cell;
+        if (finished) continue;
+        if (count < kSplatWindow) {
+            finished = true;
+        } else {
+            cursor_valid = true;
+            cur_t = buf[kSplatWindow - 1].t;
+            cur_cell = buf[kSplatWindow - 1].idx;
+        }
     }
+    if (!active) return;
     *out = make_float4(ar, ag, ab, 1.0f - T);
     if (P.stats) {
         atomicAdd(P.stats + 0, 1ull);

@@ -100,18 +100,45 @@ __device__ __forceinline__ Cell cell_from_face(const FaceEntry &f) {
     return c;
 }
 
+// Exit distance through a face (neighbour site s) of cell c in FP64 from the
+// FP32 inputs: the re-evaluation of the exit-face tie-break.
+template <bool BOUNDED>
+__device__ __noinline__ double face_t_f64(const Cell &c, const float4 &s, const Ray &ray) {
+    const double offx = (double)s.x - (double)c.x, offy = (double)s.y - (double)c.y,
+                 offz = (double)s.z - (double)c.z;
+    double shift = 0.5;
+    if (BOUNDED) {
+        const double ri = c.r, rj = s.w;
+        shift = 0.5 + 0.5 * (ri * ri - rj * rj) / fmax(offx * offx + offy * offy + offz * offz, 1e-20);
+    }
+    const double rx = ((double)c.x + shift * offx) - (double)ray.ox;
+    const double ry = ((double)c.y + shift * offy) - (double)ray.oy;
+    const double rz = ((double)c.z + shift * offz) - (double)ray.oz;
+    return (rx * offx + ry * offy + rz * offz) /
+           (offx * (double)ray.dx + offy * (double)ray.dy + offz * (double)ray.dz);
+}
+
+// Runner-up distances within this many FP32 ulps of the winner are re-evaluated.
+constexpr float kTieUlps = 4.0f;
+
 // ---------------------------------------------------------------------------
 // find_exit_face (trace.rs:170-205): the first face in CSR order with the
 // smallest t in (t0, best).  The face entries of the current cell are read
 // four at a time so that four independent loads are in flight; the winner's
 // entry already carries the next cell's site, CSR range and density.
+// TIE: the runner-up is tracked too, and when its FP32 distance is within
+// kTieUlps ulps of the winner's both are re-evaluated in FP64 and the smaller
+// wins (equal: the earlier face in CSR order, the reference's own rule).
 // ---------------------------------------------------------------------------
-template <bool BOUNDED>
+template <bool BOUNDED, bool TIE = false>
 __device__ __forceinline__ bool find_exit(const DeviceModel &m, const Cell &c, const Ray &ray,
                                           float t0, float depth, float &best, FaceEntry &win) {
     best = depth;
     uint32_t best_k = 0xffffffffu;
     float4 best_site = make_float4(0.f, 0.f, 0.f, 0.f);
+    float second = depth;
+    uint32_t second_k = 0xffffffffu;
+    float4 second_site = best_site;
     const float ri2 = c.r * c.r;
     for (uint32_t k = c.begin; k < c.end; k += kFaceUnroll) {
         float4 site[kFaceUnroll];
@@ -137,15 +164,37 @@ __device__ __forceinline__ bool find_exit(const DeviceModel &m, const Cell &c, c
                     const float t =
                         dot3(fox - ray.ox, foy - ray.oy, foz - ray.oz, offx, offy, offz) / dp;
                     if (isfinite(t) && t > t0 && t < best) {
+                        if (TIE) {
+                            second = best;
+                            second_k = best_k;
+                            second_site = best_site;
+                        }
                         best = t;
                         best_k = k + u;
                         best_site = site[u];
+                    } else if (TIE && isfinite(t) && t > t0 && t < second && t < depth) {
+                        second = t;
+                        second_k = k + u;
+                        second_site = site[u];
                     }
                 }
             }
         }
     }
     if (best_k == 0xffffffffu) return false;
+    if (TIE && second_k != 0xffffffffu) {
+        const float ab = fabsf(best);
+        const float ulp = __uint_as_float(__float_as_uint(ab) + 1u) - ab;
+        if (second - best <= kTieUlps * ulp) {
+            const double tb = face_t_f64<BOUNDED>(c, best_site, ray);
+            const double t2 = face_t_f64<BOUNDED>(c, second_site, ray);
+            if (t2 < tb || (t2 == tb && second_k < best_k)) {
+                best = second;
+                best_k = second_k;
+                best_site = second_site;
+            }
+        }
+    }
     // The winner's link shares the 32-byte sector of the site just read.
     win.site = best_site;
     win.link = __ldg(&m.faces[best_k].link);
@@ -202,9 +251,8 @@ __device__ __forceinline__ float3 heatmap(float t) {
 // ---------------------------------------------------------------------------
 // forward render: trace_one_ray per pixel
 // ---------------------------------------------------------------------------
-template <int DEG, bool BOUNDED, bool BF16>
-__global__ void __launch_bounds__(kWalkBlock, BV_MINB_RENDER)
-walk_forward_kernel(const __grid_constant__ WalkParams P) {
+template <int DEG, bool BOUNDED, bool BF16, bool TIE>
+__device__ __forceinline__ void walk_forward_body(const WalkParams &P) {
     const DeviceModel &m = P.m;
     bool drained = false, active = false;
     Ray ray;
@@ -252,7 +300,7 @@ walk_forward_kernel(const __grid_constant__ WalkParams P) {
             } else {
                 float best;
                 FaceEntry win;
-                const bool has_exit = find_exit<BOUNDED>(m, c, ray, t0, depth, best, win);
+                const bool has_exit = find_exit<BOUNDED, TIE>(m, c, ray, t0, depth, best, win);
                 n_steps += 1;
                 n_faces += c.end - c.begin;
                 float ss, se;
@@ -305,6 +353,19 @@ walk_forward_kernel(const __grid_constant__ WalkParams P) {
             atomicAdd(P.stats + 2, (unsigned long long)n_faces);
         }
     }
+}
+
+template <int DEG, bool BOUNDED, bool BF16>
+__global__ void __launch_bounds__(kWalkBlock, BV_MINB_RENDER)
+walk_forward_kernel(const __grid_constant__ WalkParams P) {
+    walk_forward_body<DEG, BOUNDED, BF16, false>(P);
+}
+
+// The render walk with the FP64 exit-face tie-break.
+template <int DEG, bool BOUNDED, bool BF16>
+__global__ void __launch_bounds__(kWalkBlock, BV_MINB_RENDER)
+walk_forward_tb_kernel(const __grid_constant__ WalkParams P) {
+    walk_forward_body<DEG, BOUNDED, BF16, true>(P);
 }
 
 // ---------------------------------------------------------------------------
@@ -990,7 +1051,10 @@ cudaError_t launch_fold_site_grads(float4 *site, uint32_t n, float *d_pos, float
     } while (0)
 
 cudaError_t launch_walk_forward(const WalkParams &p, int grid, cudaStream_t s) {
-    BV_SELECT(walk_forward_kernel, p, grid, s);
+    if (p.tie_break)
+        BV_SELECT(walk_forward_tb_kernel, p, grid, s);
+    else
+        BV_SELECT(walk_forward_kernel, p, grid, s);
     return cudaGetLastError();
 }
 

@@ -1,5 +1,5 @@
 // Windowed front-to-back gather over a BVH of particle support boxes, shared
-// by the Gaussian tracers (SH colour and relight).
+// by the Gaussian tracers (SH colour and relight) and the PowerFoam splat.
 //
 // The reference enumerates candidates with hardware ray queries over proxy
 // meshes and keeps, per batch, the next K hits above a cursor in strict
@@ -34,6 +34,12 @@ __device__ __forceinline__ bool win_less(float ta, uint32_t ia, float tb, uint32
     return ta < tb || (ta == tb && ia < ib);
 }
 
+// 1/d with |d| raised to at least 1e-30, so that a box face through the ray
+// origin gives 0 * finite rather than 0 * inf = NaN in the slab test.
+__device__ __forceinline__ float win_inverse(float d) {
+    return 1.0f / (fabsf(d) < 1e-30f ? copysignf(1e-30f, d) : d);
+}
+
 // Slab test of a box against the ray over [0, t_end], widened by a relative
 // margin so that rounding can only keep a box, never drop one.
 __device__ __forceinline__ bool win_slab(const float4 &lo, const float4 &hi, const WinRay &r,
@@ -48,56 +54,106 @@ __device__ __forceinline__ bool win_slab(const float4 &lo, const float4 &hi, con
     return tn <= tf;
 }
 
-// One pass: fills buf[0..count) with the W smallest keys above the cursor
-// (all keys when !cursor_valid) in ascending order and returns count.
-// `hit(pos, t, idx)` tests the particle at table position pos and returns
-// its key when the ray hits it; every hit's depth must lie inside its leaf
-// box's slab interval.  S bounds the traversal stack (the BVH depth plus
-// one).
-template <int W, int S, class Hit>
-__device__ __forceinline__ int win_gather(const BvhNode *__restrict__ nodes, const WinRay &ray,
-                                          float t_end, bool cursor_valid, float cur_t,
-                                          uint32_t cur_idx, WinKey (&buf)[W],
-                                          uint32_t &nodes_visited, Hit hit) {
-    int count = 0;
-    uint32_t stack[S];
+// A traversal stack shared by the 32 lanes of a warp, held across their
+// registers: entry i lives in lane i % 32, slot i / 32.  Every lane calls
+// push/pop with the same arguments (the stack pointer is warp-uniform).
+template <int S>
+struct WarpStack {
+    static_assert(S <= 96, "at most three register slots per lane");
+    uint32_t slot[(S + 31) / 32] = {};
     int sp = 0;
-    stack[sp++] = 0u;
-    while (sp > 0) {
-        const uint32_t ni = stack[--sp];
+
+    __device__ __forceinline__ void push(uint32_t v, uint32_t lane) {
+        if (sp >= S) return;
+        if ((uint32_t)(sp & 31) == lane) {
+#pragma unroll
+            for (int k = 0; k < (S + 31) / 32; ++k)
+                if (k == (sp >> 5)) slot[k] = v;
+        }
+        ++sp;
+    }
+    __device__ __forceinline__ uint32_t pop() {
+        --sp;
+        uint32_t mine = slot[0];
+#pragma unroll
+        for (int k = 1; k < (S + 31) / 32; ++k)
+            if (k == (sp >> 5)) mine = slot[k];
+        return __shfl_sync(0xffffffffu, mine, sp & 31);
+    }
+};
+
+// One pass fills a lane's buf[0..count) with the W smallest keys above its
+// cursor (all keys when !cursor_valid) in ascending order and returns count.
+// Every hit's depth must lie inside its leaf box's slab interval.  S bounds
+// the traversal stack (the BVH depth plus one).
+//
+// The pass is warp-cooperative: all 32 lanes of the warp call it together,
+// each with its own ray, cursor and window; lanes that need no pass (no ray,
+// or done) pass want = false.  The warp walks one BVH traversal: a child is
+// entered when any wanting lane's ray overlaps it and is not pruned for that
+// lane, and each lane tests the primitives of entered leaves against its own
+// ray only where the leaf is live for it.  Camera rays of an 8x4 pixel tile
+// are coherent, so the union of their traversals is close to each one, and
+// node and primitive loads are warp-uniform (one broadcast transaction).
+// The window a lane ends with is the W smallest keys above its cursor,
+// whatever the traversal order, because pruning only drops boxes that cannot
+// hold such a key.
+// `hit(pos, mine, limit, t, idx, aux)` is called by every lane for every
+// primitive of an entered leaf and must return false where mine is false (it
+// may use warp collectives).  limit is the lane's current window end (+inf
+// while the window has room): a key at or past it cannot enter.  aux is
+// stored in the key's pos field.
+template <int W, int S, class Hit>
+__device__ __forceinline__ int win_gather_warp(const BvhNode *__restrict__ nodes,
+                                               const WinRay &ray, float t_end, bool want,
+                                               bool cursor_valid, float cur_t, uint32_t cur_idx,
+                                               WinKey (&buf)[W], uint32_t &nodes_visited,
+                                               Hit hit) {
+    const uint32_t lane = threadIdx.x & 31u;
+    int count = 0;
+    WarpStack<S> stack;
+    stack.push(0u, lane);
+    while (stack.sp > 0) {
+        const uint32_t ni = stack.pop();
         const BvhNode nd = nodes[ni];
-        nodes_visited += 1;
+        if (want) nodes_visited += 1;
         float tn[2], tf[2];
         bool ok[2];
         const float4 lo[2] = {nd.l_lo, nd.r_lo}, hi[2] = {nd.l_hi, nd.r_hi};
         const uint32_t cnts[2] = {__float_as_uint(nd.l_hi.w), __float_as_uint(nd.r_hi.w)};
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-            ok[c] = cnts[c] != kBvhNoChild && win_slab(lo[c], hi[c], ray, t_end, tn[c], tf[c]);
+            ok[c] = want && cnts[c] != kBvhNoChild &&
+                    win_slab(lo[c], hi[c], ray, t_end, tn[c], tf[c]);
             if (ok[c] && cursor_valid && tf[c] < cur_t) ok[c] = false;
             if (ok[c] && count == W && tn[c] > buf[W - 1].t) ok[c] = false;
         }
-        // push the farther child first so that the nearer one is visited next
-        const int first = (ok[0] && ok[1] && tn[1] < tn[0]) ? 1 : 0;
+        const uint32_t live0 = __ballot_sync(0xffffffffu, ok[0]);
+        const uint32_t live1 = __ballot_sync(0xffffffffu, ok[1]);
+        // nearer child (by the lanes that enter both) is handled last, so
+        // that it is popped first / its hits fill the windows first
+        const uint32_t near1 = __ballot_sync(0xffffffffu, ok[0] && ok[1] && tn[1] < tn[0]);
+        const uint32_t near0 = __ballot_sync(0xffffffffu, ok[0] && ok[1] && !(tn[1] < tn[0]));
+        const int first = __popc(near1) > __popc(near0) ? 1 : 0;
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const int c = k == 0 ? 1 - first : first;
-            if (!ok[c]) continue;
+            if ((c == 0 ? live0 : live1) == 0u) continue;
             const uint32_t ref = __float_as_uint(c == 0 ? nd.l_lo.w : nd.r_lo.w);
             const uint32_t cnt = cnts[c];
             if (cnt == 0u) {
-                if (sp < S) stack[sp++] = ref;
+                stack.push(ref, lane);
                 continue;
             }
+            const bool mine = ok[c];
             for (uint32_t p = ref; p < ref + cnt; ++p) {
                 float t;
-                uint32_t id;
-                if (!hit(p, t, id)) continue;
+                uint32_t id, aux = p;
+                const float limit = count == W ? buf[W - 1].t : __int_as_float(0x7f800000);
+                if (!hit(p, mine, limit, t, id, aux)) continue;
                 if (cursor_valid && !win_less(cur_t, cur_idx, t, id)) continue;
                 if (count == W && !win_less(t, id, buf[W - 1].t, buf[W - 1].idx)) continue;
-                // insertion into the sorted window (static indexing keeps buf
-                // in registers)
-                WinKey nk{t, id, p};
+                WinKey nk{t, id, aux};
 #pragma unroll
                 for (int i = 0; i < W; ++i) {
                     if (i < count && win_less(nk.t, nk.idx, buf[i].t, buf[i].idx)) {

@@ -124,6 +124,17 @@ bv_status bv_radfoam_tracer_dispatch_batch(bv_tracer *tracer, float *out_rgba_de
 bv_status bv_radfoam_tracer_set_max_steps(bv_tracer *tracer, uint32_t max_steps);
 bv_status bv_radfoam_tracer_set_weight_threshold(bv_tracer *tracer, float weight_threshold);
 bv_status bv_radfoam_tracer_set_debug_cell_density(bv_tracer *tracer, uint32_t enabled);
+/* Exit-face choice of the render walk (dispatch / dispatch_batch).
+ * BV_TIE_BREAK_REFERENCE (default): the first face in CSR order with the
+ * smallest FP32 distance, find_exit_face (trace.rs:170-205) exactly.
+ * BV_TIE_BREAK_F64: when the runner-up's FP32 distance lies within 4 ulps of
+ * the winner's, both are re-evaluated in FP64 and the smaller wins (equal:
+ * the earlier face).  Cell sequences then differ from the reference's only at
+ * such near-ties, and follow the FP64 walk there.  No reference counterpart;
+ * recording and training keep the reference's rule. */
+#define BV_TIE_BREAK_REFERENCE 0u
+#define BV_TIE_BREAK_F64 1u
+bv_status bv_radfoam_tracer_set_tie_break(bv_tracer *tracer, uint32_t mode);
 uint32_t bv_radfoam_tracer_max_steps(const bv_tracer *tracer);
 float bv_radfoam_tracer_weight_threshold(const bv_tracer *tracer);
 uint32_t bv_radfoam_tracer_sh_degree(const bv_tracer *tracer);

@@ -213,13 +213,42 @@ static inline float read_radius(const bvo_model *m, uint32_t i) {
     return m->radii ? m->radii[i] : 0.0f;
 }
 
-/* find_exit_face (trace.rs:170-205). Returns face index or -1. */
+/* Exit distance through face k (neighbour j) of the cell at cp with power
+ * radius cr, evaluated in double from the FP32 inputs: the re-evaluation of
+ * the tie-break below. */
+static double face_t_f64(const bvo_model *m, const float cp[3], float cr, uint32_t j,
+                         const float o[3], const float d[3]) {
+    const float *np = m->points + 4 * (size_t)j;
+    const double off[3] = {(double)np[0] - cp[0], (double)np[1] - cp[1], (double)np[2] - cp[2]};
+    double shift = 0.5;
+    if (m->radii) {
+        const double rj = m->radii[j], ri = cr;
+        shift = 0.5 + 0.5 * (ri * ri - rj * rj) / fmax(dot3d(off, off), 1e-20);
+    }
+    const double rel[3] = {cp[0] + shift * off[0] - o[0], cp[1] + shift * off[1] - o[1],
+                           cp[2] + shift * off[2] - o[2]};
+    const double dd[3] = {d[0], d[1], d[2]};
+    return dot3d(rel, off) / dot3d(off, dd);
+}
+
+/* Spacing of FP32 values at |x| (x finite). */
+static inline float ulp_f(float x) {
+    union { float f; uint32_t u; } a = {fabsf(x)}, b;
+    b.u = a.u + 1u;
+    return b.f - a.f;
+}
+
+/* find_exit_face (trace.rs:170-205). Returns face index or -1.
+ * tie_break != 0: when the runner-up's FP32 distance is within
+ * BVO_TIE_ULPS ulps of the winner's, both are re-evaluated in FP64 and the
+ * smaller wins (equal: the earlier face in CSR order, the reference's rule). */
+#define BVO_TIE_ULPS 4.0f
 static int find_exit_face(const bvo_model *m, uint32_t cell, const float cp[3], float cr,
                           const float o[3], const float d[3], float t0, float depth,
-                          float *best_out) {
+                          float *best_out, int tie_break) {
     const uint32_t begin = m->offsets[cell], end = m->offsets[cell + 1];
-    float best = depth;
-    int face = -1;
+    float best = depth, second = INFINITY;
+    int face = -1, face2 = -1;
     const float ri2 = cr * cr;
     for (uint32_t k = begin; k < end; ++k) {
         const uint32_t j = m->neighbors[k];
@@ -239,9 +268,22 @@ static int find_exit_face(const bvo_model *m, uint32_t cell, const float cp[3], 
             const float rel[3] = {fo[0] - o[0], fo[1] - o[1], fo[2] - o[2]};
             const float t = dot3f(rel, off) / dp;
             if (isfinite(t) && t > t0 && t < best) {
+                second = best;
+                face2 = face;
                 best = t;
                 face = (int)(k - begin);
+            } else if (isfinite(t) && t > t0 && t < second && t < depth) {
+                second = t;
+                face2 = (int)(k - begin);
             }
+        }
+    }
+    if (tie_break && face >= 0 && face2 >= 0 && second - best <= BVO_TIE_ULPS * ulp_f(best)) {
+        const double tb = face_t_f64(m, cp, cr, m->neighbors[begin + (uint32_t)face], o, d);
+        const double t2 = face_t_f64(m, cp, cr, m->neighbors[begin + (uint32_t)face2], o, d);
+        if (t2 < tb || (t2 == tb && face2 < face)) {
+            face = face2;
+            best = second;
         }
     }
     *best_out = best;
@@ -426,7 +468,7 @@ static bvo_trace_result trace_one_ray_impl(const bvo_model *m, const float origi
         if (cells && visited < cap) cells[visited] = current;
         visited += 1;
         float best;
-        const int face = find_exit_face(m, current, cp, cr, o, d, t0, s->depth, &best);
+        const int face = find_exit_face(m, current, cp, cr, o, d, t0, s->depth, &best, s->tie_break);
         float ss, se;
         if (support_interval(bounded, o, d, cp, cr, t0, best, &ss, &se)) {
             const float dens = m->points[4 * (size_t)current + 3] * 1.0f;
@@ -485,10 +527,10 @@ bvo_trace_result bvo_trace_one_ray(const bvo_model *m, const float origin[3],
     return trace_one_ray_impl(m, origin, direction, s, NULL, 0, NULL);
 }
 
-void bvo_render_walk(const bvo_model *m, const bvo_camera *cam, uint32_t width, uint32_t height,
-                     uint32_t max_steps, float weight_threshold, uint32_t start_point,
-                     float *out_rgba, uint32_t *out_steps, uint32_t *cells, uint32_t cap,
-                     uint32_t *cell_count, int threads) {
+void bvo_render_walk_tb(const bvo_model *m, const bvo_camera *cam, uint32_t width,
+                        uint32_t height, uint32_t max_steps, float weight_threshold,
+                        uint32_t start_point, int tie_break, float *out_rgba, uint32_t *out_steps,
+                        uint32_t *cells, uint32_t cap, uint32_t *cell_count, int threads) {
     bvo_trace_settings s;
     memset(&s, 0, sizeof(s));
     s.weight_threshold = weight_threshold;
@@ -496,6 +538,7 @@ void bvo_render_walk(const bvo_model *m, const bvo_camera *cam, uint32_t width, 
     s.start_point = start_point;
     s.depth = cam->depth;
     s.eval_mode = BVO_EVAL_SH;
+    s.tie_break = tie_break;
     const long total = (long)width * (long)height;
 #ifdef _OPENMP
     if (threads <= 0) threads = omp_get_max_threads();
@@ -511,6 +554,14 @@ void bvo_render_walk(const bvo_model *m, const bvo_camera *cam, uint32_t width, 
         if (out_steps) out_steps[i] = r.steps;
     }
     (void)threads;
+}
+
+void bvo_render_walk(const bvo_model *m, const bvo_camera *cam, uint32_t width, uint32_t height,
+                     uint32_t max_steps, float weight_threshold, uint32_t start_point,
+                     float *out_rgba, uint32_t *out_steps, uint32_t *cells, uint32_t cap,
+                     uint32_t *cell_count, int threads) {
+    bvo_render_walk_tb(m, cam, width, height, max_steps, weight_threshold, start_point, 0,
+                       out_rgba, out_steps, cells, cap, cell_count, threads);
 }
 
 /* ------------------------------------------------------------------ */
@@ -537,7 +588,7 @@ static int record_walk(const bvo_model *m, const float origin[3], const float di
             break;
         }
         float best;
-        const int face = find_exit_face(m, current, cp, cr, origin, d, t0, s->depth, &best);
+        const int face = find_exit_face(m, current, cp, cr, origin, d, t0, s->depth, &best, 0);
         const uint32_t next =
             face >= 0 ? m->neighbors[m->offsets[current] + (uint32_t)face] : current;
         bvo_path_entry e;
@@ -866,7 +917,7 @@ static int record_training_walk(const bvo_model *m, const float o[3], const floa
         steps += 1;
         if (T <= thr || t0 > depth) break;
         float best;
-        const int face = find_exit_face(m, current, cp, cr, o, d, t0, depth, &best);
+        const int face = find_exit_face(m, current, cp, cr, o, d, t0, depth, &best, 0);
         const uint32_t next =
             face >= 0 ? m->neighbors[m->offsets[current] + (uint32_t)face] : current;
         float start_t = t0, end_t = best;
@@ -1645,6 +1696,144 @@ void bvo_gaussian_render(const bvo_gaussian_scene *s, const bvo_camera *cam, uin
         relight_camera_ray(cam, width, height, (uint32_t)(i % width), (uint32_t)(i / width), o, d);
         bvo_trace_gaussians(s, o, d, &st, background, out_rgba + 4 * (size_t)i,
                             out_hits ? out_hits + i : NULL);
+    }
+    (void)threads;
+}
+
+/* ------------------------------------------------------------------ */
+/* FP64 accuracy oracle of the walk                                    */
+/* ------------------------------------------------------------------ */
+
+/* trace_one_ray (trace.rs:1680-1820) with every quantity in double: the
+ * pixel ray (radfoam.wgsl:44-52 mapping), the exit-face search
+ * (find_exit_face :170-205), the support clip (:209-238), exp and SH.  The
+ * model's FP32 values are the exact inputs.  Used to state the FP32 path's
+ * image error, never as the thing measured. */
+static void camera_ray_d(const bvo_camera *cam, uint32_t width, uint32_t height, uint32_t x,
+                         uint32_t y, double o[3], double d[3]) {
+    const double tx = tan(0.5 * (double)cam->fov[0]), ty = tan(0.5 * (double)cam->fov[1]);
+    const double px = ((double)x + 0.5) / (double)width, py = ((double)y + 0.5) / (double)height;
+    const double v[3] = {(px * 2.0 - 1.0 - (double)cam->principal[0]) * tx,
+                         (py * 2.0 - 1.0 - (double)cam->principal[1]) * ty, 1.0};
+    const double q[4] = {cam->orientation[0], cam->orientation[1], cam->orientation[2],
+                         cam->orientation[3]};
+    const double t[3] = {2.0 * (q[1] * v[2] - q[2] * v[1]), 2.0 * (q[2] * v[0] - q[0] * v[2]),
+                         2.0 * (q[0] * v[1] - q[1] * v[0])};
+    const double r[3] = {v[0] + q[3] * t[0] + (q[1] * t[2] - q[2] * t[1]),
+                         v[1] + q[3] * t[1] + (q[2] * t[0] - q[0] * t[2]),
+                         v[2] + q[3] * t[2] + (q[0] * t[1] - q[1] * t[0])};
+    const double len = sqrt(dot3d(r, r));
+    for (int k = 0; k < 3; ++k) {
+        d[k] = r[k] / len;
+        o[k] = cam->position[k];
+    }
+}
+
+static int find_exit_face_d(const bvo_model *m, uint32_t cell, const double o[3],
+                            const double d[3], double t0, double depth, double *best_out) {
+    const float *cpf = m->points + 4 * (size_t)cell;
+    const double cp[3] = {cpf[0], cpf[1], cpf[2]};
+    const double cr = m->radii ? (double)m->radii[cell] : 0.0;
+    double best = depth;
+    int face = -1;
+    for (uint32_t k = m->offsets[cell]; k < m->offsets[cell + 1]; ++k) {
+        const uint32_t j = m->neighbors[k];
+        const float *np = m->points + 4 * (size_t)j;
+        const double off[3] = {np[0] - cp[0], np[1] - cp[1], np[2] - cp[2]};
+        double shift = 0.5;
+        if (m->radii) {
+            const double rj = m->radii[j];
+            shift = 0.5 + 0.5 * (cr * cr - rj * rj) / fmax(dot3d(off, off), 1e-20);
+        }
+        const double dp = dot3d(off, d);
+        if (dp > 0.0) {
+            const double rel[3] = {cp[0] + shift * off[0] - o[0], cp[1] + shift * off[1] - o[1],
+                                   cp[2] + shift * off[2] - o[2]};
+            const double t = dot3d(rel, off) / dp;
+            if (isfinite(t) && t > t0 && t < best) {
+                best = t;
+                face = (int)(k - m->offsets[cell]);
+            }
+        }
+    }
+    *best_out = best;
+    return face;
+}
+
+static void trace_one_ray_d(const bvo_model *m, const double o[3], const double d[3],
+                            uint32_t max_steps, double weight_threshold, double depth,
+                            uint32_t start, double rgba[4], uint32_t *cells, uint32_t cap,
+                            uint32_t *cell_count) {
+    double t0 = 0.0, T = 1.0, acc[3] = {0.0, 0.0, 0.0};
+    uint32_t cur = start, steps = 0, visited = 0;
+    const uint32_t deg = m->sh_degree > 3 ? 3 : m->sh_degree;
+    const uint32_t comps = sh_comps(deg);
+    double Y[16];
+    sh_basis_d(deg, d, Y);
+    while (steps < max_steps) {
+        steps += 1;
+        if (T <= weight_threshold || t0 > depth) break;
+        if (cells && visited < cap) cells[visited] = cur;
+        visited += 1;
+        double best;
+        const int face = find_exit_face_d(m, cur, o, d, t0, depth, &best);
+        double s = t0, e = best;
+        int nonempty = e > s;
+        if (m->radii) {
+            const float *cpf = m->points + 4 * (size_t)cur;
+            const double oc[3] = {o[0] - cpf[0], o[1] - cpf[1], o[2] - cpf[2]};
+            const double a = dot3d(d, d), b = dot3d(oc, d);
+            const double r = m->radii[cur];
+            const double disc = b * b - a * (dot3d(oc, oc) - r * r);
+            nonempty = 0;
+            if (disc > 0.0) {
+                const double root = sqrt(disc);
+                s = fmax(t0, (-b - root) / a);
+                e = fmin(best, (-b + root) / a);
+                nonempty = e > s;
+            }
+        }
+        const double dens = m->points[4 * (size_t)cur + 3];
+        if (nonempty && dens > 1e-6) {
+            const double alpha = 1.0 - exp(-dens * (e - s));
+            const double w = T * alpha;
+            const float *c = m->sh + (size_t)cur * 3u * comps;
+            for (int ch = 0; ch < 3; ++ch) {
+                double v = 0.0;
+                for (uint32_t k = 0; k < comps; ++k) v += Y[k] * (double)c[3 * k + ch];
+                acc[ch] += w * fmax(0.5 + v, 0.0);
+            }
+            T *= 1.0 - alpha;
+        }
+        if (face < 0) {
+            t0 = best;
+            break;
+        }
+        t0 = fmax(t0, best);
+        cur = m->neighbors[m->offsets[cur] + (uint32_t)face];
+    }
+    rgba[0] = acc[0];
+    rgba[1] = acc[1];
+    rgba[2] = acc[2];
+    rgba[3] = 1.0 - T;
+    if (cell_count) *cell_count = visited;
+}
+
+void bvo_render_walk_f64(const bvo_model *m, const bvo_camera *cam, uint32_t width,
+                         uint32_t height, uint32_t max_steps, double weight_threshold,
+                         uint32_t start_point, double *out_rgba, uint32_t *cells, uint32_t cap,
+                         uint32_t *cell_count, int threads) {
+    const long total = (long)width * (long)height;
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+#endif
+    for (long i = 0; i < total; ++i) {
+        double o[3], d[3];
+        camera_ray_d(cam, width, height, (uint32_t)(i % width), (uint32_t)(i / width), o, d);
+        trace_one_ray_d(m, o, d, max_steps, weight_threshold, (double)cam->depth, start_point,
+                        out_rgba + 4 * (size_t)i, cells ? cells + (size_t)i * cap : NULL, cap,
+                        cell_count ? cell_count + i : NULL);
     }
     (void)threads;
 }

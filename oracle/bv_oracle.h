@@ -57,6 +57,7 @@ typedef struct {
     float depth;
     int eval_mode;
     float constant_rgb[3];
+    int tie_break; /* 1: FP64 re-evaluation of near-tied exit faces (render walk) */
 } bvo_trace_settings;
 
 /* TraceResult (trace.rs:71-103). peak_point = -1 for None. */
@@ -108,6 +109,11 @@ void bvo_render_walk(const bvo_model *m, const bvo_camera *cam, uint32_t width, 
                      uint32_t max_steps, float weight_threshold, uint32_t start_point,
                      float *out_rgba, uint32_t *out_steps, uint32_t *cells, uint32_t cap,
                      uint32_t *cell_count, int threads);
+/* The same with the exit-face tie-break selected (0: the reference's rule). */
+void bvo_render_walk_tb(const bvo_model *m, const bvo_camera *cam, uint32_t width,
+                        uint32_t height, uint32_t max_steps, float weight_threshold,
+                        uint32_t start_point, int tie_break, float *out_rgba, uint32_t *out_steps,
+                        uint32_t *cells, uint32_t cap, uint32_t *cell_count, int threads);
 
 /* ---- path recorder (trace.rs:1548-1676) ---- */
 int bvo_record_path_jacobians(const bvo_model *m, const float origin[3],
@@ -271,6 +277,15 @@ void bvo_gaussian_render(const bvo_gaussian_scene *s, const bvo_camera *cam, uin
                          uint32_t height, float min_opacity, float min_transmittance,
                          const float background[3], float *out_rgba, uint32_t *out_hits,
                          int threads);
+
+/* ---- FP64 accuracy oracle of the walk ----
+ * trace_one_ray with every quantity in double (ray mapping, exit faces,
+ * support clip, exp, SH); the FP32 model values are its exact inputs.
+ * out_rgba [h*w*4] double; cells/cell_count as in bvo_render_walk. */
+void bvo_render_walk_f64(const bvo_model *m, const bvo_camera *cam, uint32_t width,
+                         uint32_t height, uint32_t max_steps, double weight_threshold,
+                         uint32_t start_point, double *out_rgba, uint32_t *cells, uint32_t cap,
+                         uint32_t *cell_count, int threads);
 
 #ifdef __cplusplus
 }

@@ -35,7 +35,7 @@ class Camera(C.Structure):
 class Settings(C.Structure):
     _fields_ = [("weight_threshold", C.c_float), ("max_steps", C.c_uint32),
                 ("start_point", C.c_uint32), ("depth", C.c_float), ("eval_mode", C.c_int),
-                ("constant_rgb", C.c_float * 3)]
+                ("constant_rgb", C.c_float * 3), ("tie_break", C.c_int)]
 
 
 class TraceResult(C.Structure):
@@ -148,6 +148,12 @@ def lib():
         L.bvo_relight_render.argtypes = [C.POINTER(RelightScene), C.POINTER(PointLight),
                                          C.c_uint32, C.POINTER(Camera), C.c_uint32, C.c_uint32,
                                          f32p, f32p, u32p, C.c_int]
+        L.bvo_render_walk_tb.argtypes = [C.POINTER(Model), C.POINTER(Camera), C.c_uint32,
+                                         C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.c_int,
+                                         f32p, u32p, u32p, C.c_uint32, u32p, C.c_int]
+        L.bvo_render_walk_f64.argtypes = [C.POINTER(Model), C.POINTER(Camera), C.c_uint32,
+                                          C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, f64p,
+                                          u32p, C.c_uint32, u32p, C.c_int]
         L.bvo_gaussian_response.restype = C.c_int
         L.bvo_gaussian_response.argtypes = [C.POINTER(GaussianScene), C.c_uint32, f32p, f32p,
                                             C.POINTER(GaussianSettings), f32p, f32p]
@@ -288,9 +294,10 @@ def containing_cell_f32(model: OracleModel, position) -> int:
 
 
 def render_walk(model: OracleModel, cam, width, height, max_steps=1024, weight_threshold=1e-3,
-                start_point=None, cell_capacity=0, threads=0):
+                start_point=None, cell_capacity=0, threads=0, tie_break=False):
     """Image of the walk forward; returns rgba [H, W, 4], steps [H, W] and
-    (if cell_capacity > 0) the visited cells [H, W, cap] and counts [H, W]."""
+    (if cell_capacity > 0) the visited cells [H, W, cap] and counts [H, W].
+    tie_break: FP64 re-evaluation of near-tied exit faces."""
     if start_point is None:
         start_point = containing_cell_f64(model, cam.position)
     rgba = np.zeros((height, width, 4), dtype=np.float32)
@@ -300,10 +307,35 @@ def render_walk(model: OracleModel, cam, width, height, max_steps=1024, weight_t
         cells = np.zeros((height, width, cell_capacity), dtype=np.uint32)
         counts = np.zeros((height, width), dtype=np.uint32)
     cs = camera_struct(cam)
-    lib().bvo_render_walk(C.byref(model.c), C.byref(cs), width, height, max_steps,
-                          weight_threshold, start_point, _ptr(rgba, f32p), _ptr(steps, u32p),
-                          _ptr(cells, u32p), cell_capacity, _ptr(counts, u32p), threads)
+    lib().bvo_render_walk_tb(C.byref(model.c), C.byref(cs), width, height, max_steps,
+                             weight_threshold, start_point, int(tie_break), _ptr(rgba, f32p),
+                             _ptr(steps, u32p), _ptr(cells, u32p), cell_capacity,
+                             _ptr(counts, u32p), threads)
     return rgba, steps, cells, counts
+
+
+def render_walk_f64(model: OracleModel, cam, width, height, max_steps=1024,
+                    weight_threshold=1e-3, start_point=None, cell_capacity=0, threads=0):
+    """FP64 accuracy oracle of the walk image: rgba [H, W, 4] float64 and (if
+    cell_capacity > 0) visited cells [H, W, cap] and counts [H, W]."""
+    if start_point is None:
+        start_point = containing_cell_f64(model, cam.position)
+    rgba = np.zeros((height, width, 4), dtype=np.float64)
+    cells = counts = None
+    if cell_capacity > 0:
+        cells = np.zeros((height, width, cell_capacity), dtype=np.uint32)
+        counts = np.zeros((height, width), dtype=np.uint32)
+    cs = camera_struct(cam)
+    lib().bvo_render_walk_f64(C.byref(model.c), C.byref(cs), width, height, max_steps,
+                              float(weight_threshold), start_point, _ptr(rgba, f64p),
+                              _ptr(cells, u32p), cell_capacity, _ptr(counts, u32p), threads)
+    return rgba, cells, counts
+
+
+def psnr(image, reference, peak=1.0) -> float:
+    """PSNR (dB) of image against reference over every channel given."""
+    mse = float(np.mean((np.asarray(image, np.float64) - np.asarray(reference, np.float64)) ** 2))
+    return float("inf") if mse == 0.0 else 10.0 * np.log10(peak * peak / mse)
 
 
 def record_image(model: OracleModel, cams: Sequence, width, height, max_steps, starts=None,
