@@ -5,8 +5,9 @@ gradient) on the 262,144-site, SH degree 3, 8 x 512^2 workload.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 One step = one bv_forward_backward call over the 8 views of a rank (start
-cells, walk, L2 loss, replay backward with gradient scatter), with inputs
-resident in HBM.  The gradient tables are zeroed inside the step.  L2 is
+cells, walk, L2 loss, replay backward with gradient scatter) followed by one
+bv_radfoam_tracer_adam_step on the device model (a complete training step),
+with inputs resident in HBM.  The gradient tables are zeroed inside the step.  L2 is
 flushed (a 256 MB write) between timed steps, outside the timed region.
 Under torchrun each rank renders its own 8 views (weak scaling) and the
 gradient tables are summed with one NCCL all-reduce per step.
@@ -43,6 +44,10 @@ VIEWS = 8
 WIDTH = HEIGHT = 512
 MAX_STEPS = 1024
 MAX_DT = 50.0
+# Adam rates of the reference's radfoam_v1 schedule at its start
+# (blade-volume-train/src/diff_render.rs:3215-3240, :3305-3310)
+ADAM = dict(lr_density=0.1, lr_sh_dc=5e-3, lr_sh_rest=5e-4, lr_position=2e-4, beta1=0.9,
+            beta2=0.999, eps=1e-15)
 
 
 def parse():
@@ -59,7 +64,8 @@ def parse():
                     help="side of the CPU-baseline sample image (view 0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="train",
-                    choices=["train", "relight", "render", "serving", "splat", "gaussian"],
+                    choices=["train", "powerfoam", "relight", "render", "serving", "splat",
+                             "gaussian"],
                     help="train: the headline fwd+bwd line; relight / render: secondary "
                          "lines for the Gaussian relight and forward-render paths; serving: "
                          "the request loop, batched against plain")
@@ -76,7 +82,7 @@ def parse():
     ap.add_argument("--batch-rays", type=int, default=0, help="serving: rays per batch (0: default)")
     ap.add_argument("--slots", type=int, default=0, help="serving: batches in flight (0: default)")
     args = ap.parse_args()
-    splat = args.workload == "splat"
+    splat = args.workload in ("splat", "powerfoam")
     if args.size is None:
         args.size = 1024 if splat else WIDTH
     if args.views is None:
@@ -96,7 +102,11 @@ def build_workload(args, rank):
 
     from blade_volume_b200 import dist as bvdist
 
-    model = scenes.radfoam_ball(args.sites, seed=0, sh_degree=3)
+    if args.workload == "powerfoam":
+        # the PowerFoam mixture (radii U[0, 0.02], BF16 SH degree 3), walk semantics
+        model = scenes.powerfoam_mixture(args.splat_sites, seed=0)
+    else:
+        model = scenes.radfoam_ball(args.sites, seed=0, sh_degree=3)
     return model, bvdist.rank_cameras(args.views, rank)
 
 
@@ -180,6 +190,18 @@ def cpu_baseline(model, cam, side, threads=None):
                       f"fwd+bwd with FP64 gradient accumulation, {dt:.2f} s"}
 
 
+def cpu_image_baseline(render, width, height, what):
+    """Times one oracle render (all host cores) of a width x height image of
+    the workload's own camera: a spread sample of its rays."""
+    t0 = time.perf_counter()
+    render(width, height)
+    dt = time.perf_counter() - t0
+    rays = width * height
+    return {"value": rays / dt / 1e6, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": f"{what}: {width}x{height} rays ({rays}) over the same field of view, "
+                      f"{dt:.2f} s"}
+
+
 def run_reference(args):
     """--impl reference: the CPU restatement of the reference's path
     (trace.rs walk + training gradient), timed on the host cores."""
@@ -259,6 +281,13 @@ def run_secondary(args):
         # counted as the reference's 96 B) + 16 B per ray out
         alg = hits * 96 + W * H * 16
         peak, kind = peaks()
+        cpu = None
+        if not args.no_cpu_baseline:
+            from oracle import oracle as O
+
+            osc = O.RelightOracleScene.from_scene(g)
+            cpu = cpu_image_baseline(lambda w, h: O.relight_render(osc, lights, cam, w, h), 32, 24,
+                                     "oracle relight (every particle tested per ray)")
         line = {"metric": "relight Mrays/s", "value": W * H / (ms * 1e-3) / 1e6, "unit": "Mrays/s",
                 "ms_per_step": ms, "steps": args.steps, "warmup": max(args.warmup, 3),
                 "dtype": "f32", "data": "synthetic",
@@ -270,6 +299,8 @@ def run_secondary(args):
                              "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
                              "traffic": None, "peak_source": kind},
                 "gpu_launches": args.steps, "clocks": clocks}
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
         return
     if args.workload == "gaussian":
@@ -292,6 +323,13 @@ def run_secondary(args):
         # per composited hit: particle 48 B + id 4 B + SH row 192 B; 16 B per ray out
         alg = hits * (48 + 4 + 192) + W * H * 16
         peak, kind = peaks()
+        cpu = None
+        if not args.no_cpu_baseline:
+            from oracle import oracle as O
+
+            osc = O.GaussianOracleScene.from_scene(g)
+            cpu = cpu_image_baseline(lambda w, h: O.gaussian_render(osc, cam, w, h), 32, 24,
+                                     "oracle trace_gaussians (every particle tested per ray)")
         line = {"metric": "gaussian Mrays/s", "value": W * H / (ms * 1e-3) / 1e6,
                 "unit": "Mrays/s", "ms_per_step": ms, "steps": args.steps,
                 "warmup": max(args.warmup, 3), "dtype": "f32", "data": "synthetic",
@@ -303,6 +341,8 @@ def run_secondary(args):
                              "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
                              "traffic": None, "peak_source": kind},
                 "gpu_launches": args.steps, "clocks": clocks}
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
         return
     if args.workload == "splat":
@@ -333,6 +373,15 @@ def run_secondary(args):
         # 16 B out per ray
         alg = hits * 16 + entries * 20 + st.steps * (2 * 3 * K + 4) + rays * 16
         peak, kind = peaks()
+        cpu = None
+        if not args.no_cpu_baseline:
+            from oracle import oracle as O
+
+            om = O.OracleModel.from_scene(w.model)
+            cpu = cpu_image_baseline(
+                lambda ww, hh: O.render_splats(om, w.cameras[0], ww, hh, w.max_steps,
+                                               w.weight_threshold), 16, 16,
+                "oracle trace_powerfoam_splats (every support tested per ray), view 0")
         line = {"metric": "splat Mrays/s", "value": rays / (ms * 1e-3) / 1e6, "unit": "Mrays/s",
                 "ms_per_step": ms, "steps": args.steps, "warmup": max(args.warmup, 3),
                 "dtype": "f32 (SH bf16)", "data": "synthetic",
@@ -347,6 +396,8 @@ def run_secondary(args):
                              "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
                              "traffic": None, "peak_source": kind},
                 "gpu_launches": args.steps, "clocks": clocks}
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
         return
     w = scenes.radfoam_tiny()
@@ -367,6 +418,14 @@ def run_secondary(args):
     b_step = 8 + deg * 20 + 4 * (3 * 1 + 1)
     alg = st.steps * b_step + w.width * w.height * 16
     peak, kind = peaks()
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        om = O.OracleModel.from_scene(w.model)
+        cpu = cpu_image_baseline(lambda ww, hh: O.render_walk(om, w.cameras[0], ww, hh,
+                                                              w.max_steps, w.weight_threshold),
+                                 w.width, w.height, "oracle trace_one_ray, the whole image")
     line = {"metric": "forward Mrays/s", "value": w.width * w.height / (ms * 1e-3) / 1e6,
             "unit": "Mrays/s", "ms_per_step": ms, "steps": args.steps,
             "warmup": max(args.warmup, 3), "dtype": "f32", "data": "synthetic",
@@ -377,6 +436,8 @@ def run_secondary(args):
                          "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
                          "traffic": None, "peak_source": kind},
             "clocks": clocks}
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
 
 
@@ -449,7 +510,7 @@ def main():
     if args.workload == "serving":
         run_serving(args)
         return
-    if args.workload != "train":
+    if args.workload not in ("train", "powerfoam"):
         run_secondary(args)
         return
     import torch
@@ -471,7 +532,6 @@ def main():
     from blade_volume_b200 import scenes
 
     W = H = args.size
-    tracer = bv.RadFoamGpuTracer(model, max_steps=MAX_STEPS, weight_threshold=1e-3)
     # targets: renders of the perturbed scene (densities x e^N(0,.1), SH + N(0,.05))
     tgt_tracer = bv.RadFoamGpuTracer(scenes.perturbed(model, seed=2), max_steps=MAX_STEPS,
                                      weight_threshold=1e-3)
@@ -479,29 +539,52 @@ def main():
     target = rgba[..., :3].contiguous()
     tgt_tracer.deinit()
     del rgba
-    grads = tracer.new_grads()
     loss = torch.zeros(1, dtype=torch.float32, device="cuda")
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     stream = torch.cuda.current_stream()
     rays = len(cams) * W * H
 
-    def step():
+    # The step trains the model, so the work per step drifts as it learns.
+    # The device-resident timing and the end-to-end timing each start from a
+    # tracer freshly built from the same host model and take the same warm-up
+    # steps, so both measure the same trajectory.
+    cur = {}
+
+    def fresh():
+        if "tracer" in cur:
+            cur["tracer"].deinit()
+        cur["tracer"] = bv.RadFoamGpuTracer(model, max_steps=MAX_STEPS, weight_threshold=1e-3)
+        cur["grads"] = cur["tracer"].new_grads()
+
+    def optimize():
+        cur["tracer"].adam_step(cur["grads"], density_activation=bv.DENSITY_SOFTPLUS,
+                                softplus_beta=10.0, **ADAM)
+
+    def step(tgt=None):
+        tracer, grads = cur["tracer"], cur["grads"]
         for g in grads.values():
             g.zero_()
-        tracer.forward_backward(cams, W, H, target, grads, max_steps=MAX_STEPS,
-                                weight_threshold=0.0, max_dt=MAX_DT, loss_out=loss)
+        tracer.forward_backward(cams, W, H, target if tgt is None else tgt, grads,
+                                max_steps=MAX_STEPS, weight_threshold=0.0, max_dt=MAX_DT,
+                                loss_out=loss)
         if dist is not None:
             bvdist.allreduce_grads(grads, dist)
+        optimize()
 
-    for _ in range(max(args.warmup, 3)):
+    def warm_up():
+        fresh()
+        for _ in range(max(args.warmup, 3)):
+            step()
+        torch.cuda.synchronize()
+        # per-launch stats of the walk kernels (device events on the launch stream)
+        cur["tracer"].enable_stats(True)
         step()
-    torch.cuda.synchronize()
+        st = cur["tracer"].last_stats()
+        cur["tracer"].enable_stats(False)
+        return st
 
-    # per-launch stats of the walk kernels (device events on the launch stream)
-    tracer.enable_stats(True)
-    step()
-    st = tracer.last_stats()
-    tracer.enable_stats(False)
+    st = warm_up()
+    tracer = cur["tracer"]
     steps_per_launch, faces_per_launch = st.steps, st.faces
 
     sampler = ClockSampler(local)
@@ -535,6 +618,18 @@ def main():
     ms_per_step = total_ms / args.steps
     value = rays * world / (ms_per_step * 1e-3) / 1e6
 
+    # the optimizer step alone (device events)
+    opt_times = []
+    for _ in range(3):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        optimize()
+        e1.record(stream)
+        e1.synchronize()
+        opt_times.append(e0.elapsed_time(e1))
+    opt_ms = statistics.median(opt_times)
+
     # forward-only throughput of the same views (render path)
     out = torch.empty((len(cams), H, W, 4), dtype=torch.float32, device="cuda")
     for _ in range(3):
@@ -551,29 +646,26 @@ def main():
         fwd_times.append(e0.elapsed_time(e1))
     fwd_ms = sum(fwd_times) / len(fwd_times)
 
-    # end to end through the public API: pinned host targets in, loss out
+    # end to end through the public API: pinned host targets in, loss out,
+    # on a fresh tracer taking the same warm-up as the device-resident timing
     host_target = torch.empty(target.shape, dtype=torch.float32, pin_memory=True)
     host_target.copy_(target.cpu())
     host_loss = torch.empty(1, dtype=torch.float32, pin_memory=True)
     dev_target = torch.empty_like(target)
+    warm_up()
+    tracer = cur["tracer"]
     e2e_times = []
-    for i in range(args.steps + 1):
+    for i in range(args.steps):
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         dev_target.copy_(host_target, non_blocking=True)
-        for g in grads.values():
-            g.zero_()
-        tracer.forward_backward(cams, W, H, dev_target, grads, max_steps=MAX_STEPS,
-                                weight_threshold=0.0, max_dt=MAX_DT, loss_out=loss)
-        if dist is not None:
-            bvdist.allreduce_grads(grads, dist)
+        step(dev_target)
         host_loss.copy_(loss, non_blocking=True)
         e1.record(stream)
         e1.synchronize()
-        if i > 0:
-            e2e_times.append(e0.elapsed_time(e1))
+        e2e_times.append(e0.elapsed_time(e1))
     e2e_ms = sum(e2e_times) / len(e2e_times)
     if dist is not None:
         e2e_ms, fwd_ms = bvdist.max_over_ranks([e2e_ms, fwd_ms], dist, "cuda")
@@ -586,7 +678,8 @@ def main():
     # deg = measured faces per executed step.
     K = 16
     deg = faces_per_launch / max(steps_per_launch, 1)
-    b_step = 8 + deg * 20 + 4 * (3 * K + 1)
+    sh_row = 2 * 3 * K + 4 if model.sh_bf16 else 4 * (3 * K + 1)
+    b_step = 8 + deg * 20 + sh_row
     b_atomic = 2 * (4 + 4 * 3 * K + 3 * 12)
     bwd_bytes = steps_per_launch * (b_step + b_atomic)
     fwd_bytes = steps_per_launch * b_step + rays * 12
@@ -596,10 +689,15 @@ def main():
     achieved = bwd_bytes / (kms_b * 1e-3) / 1e9
     traffic = None
     prof = os.path.join(ROOT, "profiles", "train_backward_radfoam_train.json")
-    if os.path.exists(prof):
+    if args.workload == "train" and os.path.exists(prof):
         with open(prof) as f:
             traffic = json.load(f).get("dram_bytes_per_launch")
 
+    # Adam bytes: per parameter p, g, m, v read and p, m, v written (28 B), the
+    # raw density parameter twice more, the BF16/FP32 SH row and the face
+    # table refresh (32 B per CSR entry written, 20 B gathered)
+    n_params = model.n * (1 + 3 * 16 + 3)
+    adam_bytes = n_params * 28 + model.n * 8 + len(model.neighbors) * 52
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(model, cams[0], args.cpu_sample)
@@ -608,10 +706,12 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "radfoam_train fwd+bwd", "sites": args.sites, "sh_degree": 3,
+        "config": {"workload": ("powerfoam_mixture fwd+bwd, BF16 SH" if model.radii is not None
+                                else "radfoam_train fwd+bwd"), "sites": model.n, "sh_degree": 3,
                    "views_per_gpu": len(cams), "width": W, "height": H, "loss": "L2",
                    "max_steps": MAX_STEPS, "max_dt": MAX_DT, "mean_degree": model.mean_degree(),
                    "parallelism": f"dp{world}" if world > 1 else "single",
+                   "optimizer": "adam on density (softplus beta 10), SH, positions",
                    "l2": "flushed between timed steps (256 MB write)"},
         "forward": {"value": rays * world / (fwd_ms * 1e-3) / 1e6, "unit": UNIT,
                     "ms_per_step": fwd_ms},
@@ -625,8 +725,9 @@ def main():
                      "faces_per_step": deg,
                      "note": "scene working set is largely L2-resident; see profiles/"},
         "kernels": {"train_forward_kernel": {"ms": kms_f, "alg_gbs": fwd_bytes / (kms_f * 1e-3) / 1e9},
-                    "train_backward_kernel": {"ms": kms_b, "alg_gbs": achieved}},
-        "gpu_launches": 4 * args.steps,
+                    "train_backward_kernel": {"ms": kms_b, "alg_gbs": achieved},
+                    "adam (4 kernels)": {"ms": opt_ms, "alg_gbs": adam_bytes / (opt_ms * 1e-3) / 1e9}},
+        "gpu_launches": 8 * args.steps,
         "clocks": clocks,
     }
     if cpu is not None:

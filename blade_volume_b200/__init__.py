@@ -69,7 +69,9 @@ EXPORTED_SYMBOLS = [
     "bv_gaussian_tracer_set_min_transmittance", "bv_gaussian_tracer_set_background",
     "bv_gaussian_tracer_num_points", "bv_gaussian_tracer_dispatch",
     "bv_gaussian_tracer_enable_stats", "bv_gaussian_tracer_last_stats",
+    "bv_radfoam_tracer_adam_step", "bv_radfoam_tracer_adam_steps", "bv_radfoam_tracer_read_model",
 ]
+DENSITY_IDENTITY, DENSITY_RELU, DENSITY_SOFTPLUS = 0, 1, 2
 SERVE_BATCHED, SERVE_PLAIN, SERVE_PLAIN_BATCH = 0, 1, 2
 REQUEST_RENDER, REQUEST_FORWARD_BACKWARD = 0, 1
 SCENE_GRADIENTS = 0x1
@@ -124,6 +126,13 @@ class LaunchStats(C.Structure):
                 ("forward_ms", C.c_float), ("backward_ms", C.c_float), ("rays", C.c_uint64),
                 ("steps", C.c_uint64), ("faces", C.c_uint64), ("launches", C.c_uint32),
                 ("reserved", C.c_uint32)]
+
+
+class AdamSettingsC(C.Structure):
+    _fields_ = [("lr_density", C.c_float), ("lr_sh_dc", C.c_float), ("lr_sh_rest", C.c_float),
+                ("lr_position", C.c_float), ("lr_radius", C.c_float), ("beta1", C.c_float),
+                ("beta2", C.c_float), ("eps", C.c_float), ("density_activation", C.c_uint32),
+                ("softplus_beta", C.c_float)]
 
 
 class MaterialC(C.Structure):
@@ -283,6 +292,11 @@ def load_library(path: str = LIB_PATH):
     L.bv_powerfoam_splat_tracer_set_weight_threshold.argtypes = [C.c_void_p, C.c_float]
     L.bv_powerfoam_splat_tracer_enable_stats.argtypes = [C.c_void_p, C.c_uint32]
     L.bv_powerfoam_splat_tracer_last_stats.argtypes = [C.c_void_p, C.POINTER(LaunchStats)]
+    L.bv_radfoam_tracer_adam_step.argtypes = [C.c_void_p, C.POINTER(Grads),
+                                              C.POINTER(AdamSettingsC), C.c_void_p]
+    L.bv_radfoam_tracer_adam_steps.argtypes = [C.c_void_p]
+    L.bv_radfoam_tracer_adam_steps.restype = C.c_uint32
+    L.bv_radfoam_tracer_read_model.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.bv_gaussian_tracer_new.argtypes = [C.POINTER(GaussianShDesc),
                                          C.POINTER(GaussianTraceSettingsC), C.POINTER(C.c_void_p)]
     L.bv_gaussian_tracer_destroy.argtypes = [C.c_void_p]
@@ -519,6 +533,35 @@ class RadFoamGpuTracer:
         if self.model.radii is not None:
             g["d_radius"] = torch.zeros(n, dtype=torch.float32, device="cuda")
         return g
+
+    def adam_step(self, grads: dict, lr_density=0.0, lr_sh_dc=0.0, lr_sh_rest=0.0,
+                  lr_position=0.0, lr_radius=0.0, beta1=0.9, beta2=0.999, eps=1e-15,
+                  density_activation=DENSITY_IDENTITY, softplus_beta=10.0, stream=None):
+        """One Adam step of the device model from gradient tables (a dict as
+        from new_grads); see bv_radfoam_tracer_adam_step."""
+        g = Grads()
+        g.d_density_dev = grads["d_density"].data_ptr() if grads.get("d_density") is not None else None
+        g.d_sh_dev = grads["d_sh"].data_ptr() if grads.get("d_sh") is not None else None
+        g.d_positions_dev = grads["d_pos"].data_ptr() if grads.get("d_pos") is not None else None
+        g.d_radii_dev = grads["d_radius"].data_ptr() if grads.get("d_radius") is not None else None
+        a = AdamSettingsC(lr_density, lr_sh_dc, lr_sh_rest, lr_position, lr_radius, beta1, beta2,
+                          eps, density_activation, softplus_beta)
+        _check(load_library().bv_radfoam_tracer_adam_step(self._h, C.byref(g), C.byref(a),
+                                                          _stream_handle(stream)))
+
+    @property
+    def adam_steps(self) -> int:
+        return load_library().bv_radfoam_tracer_adam_steps(self._h)
+
+    def read_model(self):
+        """(points [N, 4], sh [N, 3K], radii [N] or None) of the device model."""
+        n = self.model.n
+        pts = np.zeros((n, 4), np.float32)
+        sh = np.zeros((n, 3 * self.sh_components), np.float32)
+        rad = np.zeros(n, np.float32) if self.model.radii is not None else None
+        _check(load_library().bv_radfoam_tracer_read_model(
+            self._h, pts.ctypes.data, sh.ctypes.data, None if rad is None else rad.ctypes.data))
+        return pts, sh, rad
 
     # --- instrumentation
     def enable_stats(self, enabled: bool = True):

@@ -6,7 +6,9 @@ Every .cu file under csrc/ is compiled by nvcc for sm_100a and linked into
 blade_volume_b200/libbv_b200.so, in-tree next to this file.  The walk kernels
 are compiled with -fmad=false: each FP32/FP64 expression is then the exact
 sequence of rounded operations it is written as, which is what makes cell
-sequences, t values and colours bit-identical to the CPU restatement.
+sequences, t values and colours bit-identical to the CPU restatement.  Host
+code is built with -ffp-contract=off for the same reason: the PowerFoam splat
+tracer forms its Cech clip planes on the host in the kernel's FP32 order.
 """
 
 from __future__ import annotations
@@ -25,7 +27,8 @@ LIB = os.path.join(HERE, "libbv_b200.so")
 BUILD_DIR = os.path.join(ROOT, "_build", "bv_b200")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-fmad=false",
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
+              "-ffp-contract=off", "-fmad=false",
               "--expt-relaxed-constexpr", "-I" + INCLUDE, "-I" + CSRC]
 
 

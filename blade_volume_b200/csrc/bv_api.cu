@@ -73,6 +73,14 @@ struct bv_tracer {
     bool bounded = false;
     bv_trace_settings settings{};
     uint32_t tie_break = 0;            // render walk: FP64 exit-face tie-break
+    // optimizer state (allocated by the first bv_radfoam_tracer_adam_step)
+    uint32_t adam_t = 0;               // steps taken
+    uint32_t adam_activation = 0;
+    float adam_beta = 0.f;
+    float *adam_buf = nullptr;         // one allocation: the arrays below
+    float *density_param = nullptr, *m_density = nullptr, *v_density = nullptr;
+    float *sh_master = nullptr, *m_sh = nullptr, *v_sh = nullptr;
+    float *m_pos = nullptr, *v_pos = nullptr, *m_radius = nullptr, *v_radius = nullptr;
     // device model
     float4 *geom = nullptr;
     float *density = nullptr;
@@ -137,6 +145,7 @@ void free_tracer(bv_tracer *t) {
     cudaFree(t->partial_dist);
     cudaFree(t->partial_index);
     cudaFree(t->start_counters);
+    cudaFree(t->adam_buf);
     for (auto &e : t->ev)
         if (e) cudaEventDestroy(e);
     delete t;
@@ -696,6 +705,159 @@ bv_status bv_radfoam_tracer_last_stats(bv_tracer *t, bv_launch_stats *out) {
     out->rays = h[0];
     out->steps = h[1];
     out->faces = h[2];
+    return BV_OK;
+}
+
+bv_status bv_radfoam_tracer_adam_step(bv_tracer *t, const bv_grads *g, const bv_adam_settings *a,
+                                      bv_stream stream) {
+    if (!t || !g || !a) return fail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    const float rates[5] = {a->lr_density, a->lr_sh_dc, a->lr_sh_rest, a->lr_position,
+                            a->lr_radius};
+    for (float r : rates)
+        if (!std::isfinite(r) || r < 0.0f)
+            return fail(BV_ERR_INVALID_ARGUMENT, "learning rates must be finite and >= 0");
+    if (!(a->beta1 >= 0.0f && a->beta1 < 1.0f && a->beta2 >= 0.0f && a->beta2 < 1.0f))
+        return fail(BV_ERR_INVALID_ARGUMENT, "Adam betas must lie in [0, 1)");
+    if (!(std::isfinite(a->eps) && a->eps >= 0.0f))
+        return fail(BV_ERR_INVALID_ARGUMENT, "Adam eps must be finite and >= 0");
+    if (a->density_activation > BV_DENSITY_SOFTPLUS)
+        return fail(BV_ERR_INVALID_ARGUMENT, "unknown density activation %u", a->density_activation);
+    if (a->density_activation == BV_DENSITY_SOFTPLUS &&
+        !(std::isfinite(a->softplus_beta) && a->softplus_beta > 0.0f))
+        return fail(BV_ERR_INVALID_ARGUMENT, "softplus beta must be finite and positive");
+    if (g->d_radii_dev && !t->bounded)
+        return fail(BV_ERR_INVALID_ARGUMENT, "radius gradients need a PowerFoam model");
+    const uint32_t nsh = 3 * sh_components(t->sh_degree);
+    const float beta = a->density_activation == BV_DENSITY_SOFTPLUS ? a->softplus_beta : 0.0f;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!t->adam_buf) {
+        // raw density + 2 moments, (master) SH + 2 moments, positions and radii moments
+        const size_t n = t->n;
+        const size_t total = 3 * n + 3 * n * nsh + 6 * n + 2 * n;
+        BV_CUDA(cudaMalloc(&t->adam_buf, sizeof(float) * total), "cudaMalloc optimizer state");
+        float *q = t->adam_buf;
+        t->density_param = q; q += n;
+        t->m_density = q; q += n;
+        t->v_density = q; q += n;
+        t->sh_master = q; q += n * nsh;
+        t->m_sh = q; q += n * nsh;
+        t->v_sh = q; q += n * nsh;
+        t->m_pos = q; q += 3 * n;
+        t->v_pos = q; q += 3 * n;
+        t->m_radius = q; q += n;
+        t->v_radius = q;
+        BV_CUDA(cudaMemsetAsync(t->m_density, 0, sizeof(float) * 2 * n, s), "zero moments");
+        BV_CUDA(cudaMemsetAsync(t->m_sh, 0, sizeof(float) * 2 * n * nsh, s), "zero moments");
+        BV_CUDA(cudaMemsetAsync(t->m_pos, 0, sizeof(float) * 8 * n, s), "zero moments");
+        if (t->bf16) {
+            // the FP32 master copy starts at the stored BF16 values (exact widening)
+            std::vector<uint16_t> rows(n * t->sh_stride);
+            BV_CUDA(cudaMemcpy(rows.data(), t->sh, rows.size() * 2, cudaMemcpyDeviceToHost),
+                    "read SH");
+            std::vector<float> master(n * nsh);
+            for (size_t i = 0; i < n; ++i)
+                for (uint32_t k = 0; k < nsh; ++k) {
+                    const uint32_t u = (uint32_t)rows[i * t->sh_stride + k] << 16;
+                    std::memcpy(&master[i * nsh + k], &u, 4);
+                }
+            BV_CUDA(cudaMemcpyAsync(t->sh_master, master.data(), sizeof(float) * master.size(),
+                                    cudaMemcpyHostToDevice, s), "upload SH master");
+            BV_CUDA(cudaStreamSynchronize(s), "SH master upload");
+        }
+        BV_CUDA(launch_init_density_param(t->density, t->density_param, t->n,
+                                          a->density_activation, beta, s),
+                "density parameter init");
+        t->adam_activation = a->density_activation;
+        t->adam_beta = beta;
+        t->adam_t = 0;
+    } else if (a->density_activation != t->adam_activation || beta != t->adam_beta) {
+        return fail(BV_ERR_INVALID_ARGUMENT,
+                    "the density activation is fixed by the first optimizer step");
+    }
+    t->adam_t += 1;
+    AdamParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.n = t->n;
+    p.sh_row = nsh;
+    p.sh_stride = t->sh_stride;
+    p.s.beta1 = a->beta1;
+    p.s.beta2 = a->beta2;
+    p.s.one_minus_beta1 = 1.0f - a->beta1;
+    p.s.one_minus_beta2 = 1.0f - a->beta2;
+    p.s.c1 = (float)(1.0 - std::pow((double)a->beta1, (double)t->adam_t));
+    p.s.c2 = (float)(1.0 - std::pow((double)a->beta2, (double)t->adam_t));
+    p.s.eps = a->eps;
+    p.lr_density = a->lr_density;
+    p.lr_sh_dc = a->lr_sh_dc;
+    p.lr_sh_rest = a->lr_sh_rest;
+    p.lr_position = a->lr_position;
+    p.lr_radius = a->lr_radius;
+    p.activation = a->density_activation;
+    p.softplus_beta = beta;
+    p.density_param = t->density_param;
+    p.density = t->density;
+    p.g_density = g->d_density_dev;
+    p.m_density = t->m_density;
+    p.v_density = t->v_density;
+    p.sh = t->sh;
+    p.sh_master = t->sh_master;
+    p.g_sh = g->d_sh_dev;
+    p.m_sh = t->m_sh;
+    p.v_sh = t->v_sh;
+    p.geom = t->geom;
+    p.g_pos = g->d_positions_dev;
+    p.m_pos = t->m_pos;
+    p.v_pos = t->v_pos;
+    p.g_radius = t->bounded ? g->d_radii_dev : nullptr;
+    p.m_radius = t->m_radius;
+    p.v_radius = t->v_radius;
+    BV_CUDA(launch_adam_step(p, t->faces, t->m_edges, t->bf16, s), "optimizer launch");
+    return BV_OK;
+}
+
+uint32_t bv_radfoam_tracer_adam_steps(const bv_tracer *t) { return t ? t->adam_t : 0; }
+
+bv_status bv_radfoam_tracer_read_model(bv_tracer *t, float *points, float *sh, float *radii) {
+    if (!t) return fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
+    if (radii && !t->bounded) return fail(BV_ERR_INVALID_ARGUMENT, "the model has no radii");
+    BV_CUDA(cudaDeviceSynchronize(), "synchronize");
+    const size_t n = t->n;
+    if (points || radii) {
+        std::vector<float4> geom(n);
+        std::vector<float> dens(n);
+        BV_CUDA(cudaMemcpy(geom.data(), t->geom, sizeof(float4) * n, cudaMemcpyDeviceToHost),
+                "read sites");
+        BV_CUDA(cudaMemcpy(dens.data(), t->density, sizeof(float) * n, cudaMemcpyDeviceToHost),
+                "read densities");
+        for (size_t i = 0; i < n; ++i) {
+            if (points) {
+                points[4 * i + 0] = geom[i].x;
+                points[4 * i + 1] = geom[i].y;
+                points[4 * i + 2] = geom[i].z;
+                points[4 * i + 3] = dens[i];
+            }
+            if (radii) radii[i] = geom[i].w;
+        }
+    }
+    if (sh) {
+        const uint32_t nsh = 3 * sh_components(t->sh_degree);
+        if (t->bf16) {
+            std::vector<uint16_t> rows(n * t->sh_stride);
+            BV_CUDA(cudaMemcpy(rows.data(), t->sh, rows.size() * 2, cudaMemcpyDeviceToHost),
+                    "read SH");
+            for (size_t i = 0; i < n; ++i)
+                for (uint32_t k = 0; k < nsh; ++k) {
+                    const uint32_t u = (uint32_t)rows[i * t->sh_stride + k] << 16;
+                    std::memcpy(&sh[i * nsh + k], &u, 4);
+                }
+        } else {
+            std::vector<float> rows(n * t->sh_stride);
+            BV_CUDA(cudaMemcpy(rows.data(), t->sh, rows.size() * 4, cudaMemcpyDeviceToHost),
+                    "read SH");
+            for (size_t i = 0; i < n; ++i)
+                std::memcpy(&sh[i * nsh], &rows[i * t->sh_stride], sizeof(float) * nsh);
+        }
+    }
     return BV_OK;
 }
 

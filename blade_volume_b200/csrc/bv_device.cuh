@@ -50,6 +50,45 @@ __device__ __forceinline__ float bv_expf(float x) {
     return p * __int_as_float((ki + 127) << 23);
 }
 
+// log(x): x = m 2^e, m in [sqrt(1/2), sqrt(2)), log(1+f) = 2 atanh(f/(2+f))
+// arranged as f - (f^2/2 - s (f^2/2 + R)); same sequence as the oracle.
+__device__ __forceinline__ float bv_logf(float x) {
+    if (x != x || x < 0.0f) return __int_as_float(0x7fc00000);
+    if (x == 0.0f) return __int_as_float(0xff800000);
+    if (x == __int_as_float(0x7f800000)) return x;
+    uint32_t u = __float_as_uint(x);
+    int e = 0;
+    if (u < 0x00800000u) {
+        u = __float_as_uint(x * 16777216.0f);
+        e = -24;
+    }
+    e += (int)((u >> 23) & 0xffu) - 127;
+    float m = __uint_as_float((u & 0x007fffffu) | 0x3f800000u);
+    if (m > 1.41421353816986083984375f) {
+        m = m * 0.5f;
+        e += 1;
+    }
+    const float f = m - 1.0f;
+    const float s = f / (2.0f + f);
+    const float z = s * s;
+    float p = 0.1538461595773697f;
+    p = __fmaf_rn(p, z, 0.1818181872367859f);
+    p = __fmaf_rn(p, z, 0.2222222238779068f);
+    p = __fmaf_rn(p, z, 0.2857142984867096f);
+    p = __fmaf_rn(p, z, 0.4000000059604645f);
+    p = __fmaf_rn(p, z, 0.6666666865348816f);
+    const float R = z * p;
+    const float hfsq = 0.5f * f * f;
+    const float ef = (float)e;
+    return ef * 0.693115234375f -
+           ((hfsq - (s * (hfsq + R) + ef * 3.19461832987144589424133e-05f)) - f);
+}
+
+__device__ __forceinline__ float bv_powf(float x, float y) {
+    if (x == 0.0f) return y > 0.0f ? 0.0f : (y == 0.0f ? 1.0f : __int_as_float(0x7f800000));
+    return bv_expf(y * bv_logf(x));
+}
+
 __device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
     return ax * bx + ay * by + az * bz;
 }

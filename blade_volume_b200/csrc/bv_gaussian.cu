@@ -34,6 +34,10 @@ namespace bv {
 namespace {
 
 constexpr int kGaussBlock = 128;
+// resident blocks per SM requested from the register allocator
+#ifndef BV_MINB_GAUSS
+#define BV_MINB_GAUSS 4
+#endif
 constexpr int kWindow = 16;
 constexpr int kStack = 64;
 
@@ -76,13 +80,27 @@ __device__ __forceinline__ float3 gqrot(float4 q, float vx, float vy, float vz) 
                        (vz + q.w * t2) + (q.x * t1 - q.y * t0));
 }
 
+// Conservative pre-test: a hit lies inside the support ellipsoid, so within
+// sqrt(cut) * max(scale) of the mean; rays passing farther from the mean than
+// that (with a margin for the rounding of |oc|^2 - b^2) cannot hit.  d is unit.
+__device__ __forceinline__ bool support_sphere_hit(const float4 &co, const float4 &sc,
+                                                   const WinRay &r) {
+    const float ox = co.x - r.ox, oy = co.y - r.oy, oz = co.z - r.oz;
+    const float b = gdot(ox, oy, oz, r.dx, r.dy, r.dz);
+    const float oo = gdot(ox, oy, oz, ox, oy, oz);
+    const float smax = fmaxf(fmaxf(sc.x, sc.y), sc.z);
+    const float r2 = sc.w * (smax * smax);
+    return oo - b * b <= r2 * 1.001f + 1e-6f * oo + 1e-30f;
+}
+
 // Maximum-response depth and alpha (trace.rs:731-747); false when the
 // depth is outside (0, t_end) or alpha < min_opacity.
 __device__ __forceinline__ bool response(const GaussianParams &P, uint32_t pos, const WinRay &r,
                                          float &t_out, float &alpha_out) {
     const float4 co = __ldg(&P.prims[pos].center_opacity);
-    const float4 qi = __ldg(&P.prims[pos].qinv);
     const float4 sc = __ldg(&P.prims[pos].scale_cut);
+    if (!support_sphere_hit(co, sc, r)) return false;
+    const float4 qi = __ldg(&P.prims[pos].qinv);
     const float3 lo0 = gqrot(qi, r.ox - co.x, r.oy - co.y, r.oz - co.z);
     const float3 ld0 = gqrot(qi, r.dx, r.dy, r.dz);
     const float lox = lo0.x / sc.x, loy = lo0.y / sc.y, loz = lo0.z / sc.z;
@@ -100,7 +118,7 @@ __device__ __forceinline__ bool response(const GaussianParams &P, uint32_t pos, 
 }
 
 template <int DEG>
-__global__ void __launch_bounds__(kGaussBlock) gaussian_kernel(const __grid_constant__ GaussianParams P) {
+__global__ void __launch_bounds__(kGaussBlock, BV_MINB_GAUSS) gaussian_kernel(const __grid_constant__ GaussianParams P) {
     // whole warps past the last tile leave together; lanes of a partial edge
     // tile stay (inactive) because the traversal is warp-cooperative
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;

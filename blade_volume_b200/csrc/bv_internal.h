@@ -176,6 +176,40 @@ struct StartCellScratch {
     uint32_t *counters;
     int blocks_per_query;
 };
+// Adam over a tracer's tables (bv_optim.cu).  Scalars are formed on the host:
+// one_minus_beta_i = 1 - beta_i in FP32, c_i = 1 - beta_i^t in FP64 rounded.
+struct AdamScalars {
+    float beta1, beta2, one_minus_beta1, one_minus_beta2, c1, c2, eps;
+};
+
+struct AdamParams {
+    uint32_t n;
+    uint32_t sh_row;     // 3K coefficients per site (dense gradient / moment rows)
+    uint32_t sh_stride;  // elements per device SH row
+    AdamScalars s;
+    float lr_density, lr_sh_dc, lr_sh_rest, lr_position, lr_radius;
+    uint32_t activation;  // BV_DENSITY_*
+    float softplus_beta;
+    float *density_param;  // [N] raw parameter x, density = act(x)
+    float *density;        // [N] device model density
+    const float *g_density;
+    float *m_density, *v_density;
+    void *sh;              // device SH table (FP32 or BF16 rows)
+    float *sh_master;      // [N*3K] FP32 master copy when the table is BF16
+    const float *g_sh;
+    float *m_sh, *v_sh;
+    float4 *geom;          // [N] x, y, z, radius
+    const float *g_pos;    // [N*3]
+    float *m_pos, *v_pos;
+    const float *g_radius;  // [N] or null
+    float *m_radius, *v_radius;
+};
+
+cudaError_t launch_init_density_param(const float *density, float *param, uint32_t n,
+                                      uint32_t kind, float beta, cudaStream_t s);
+cudaError_t launch_adam_step(const AdamParams &p, FaceEntry *faces, uint32_t m_edges, bool bf16,
+                             cudaStream_t s);
+
 // Sets the calling thread's bv_last_error() message.
 void set_last_error(const char *message);
 

@@ -17,6 +17,7 @@
 // Compiled with -fmad=false: the arithmetic is the CPU oracle's, operation
 // for operation, so images are bit-identical.
 
+#include "bv_device.cuh"
 #include "bv_relight.h"
 #include "bv_window.cuh"
 
@@ -25,76 +26,6 @@ namespace {
 
 constexpr int kRelightBlock = 128;
 constexpr int kWindow = 16;
-
-__device__ __forceinline__ float r_expf(float x) {
-    if (x != x) return x;
-    if (x > 88.72283935546875f) return __int_as_float(0x7f800000);
-    if (x < -103.972084045410156f) return 0.0f;
-    const float k = rintf(x * 1.44269502162933349609375f);
-    float r = __fmaf_rn(k, -0.693115234375f, x);
-    r = __fmaf_rn(k, -3.19461832987144589424133e-05f, r);
-    float p = 1.98412701138295233249664e-04f;
-    p = __fmaf_rn(p, r, 1.38888892251998186111450e-03f);
-    p = __fmaf_rn(p, r, 8.33333376795053482055664e-03f);
-    p = __fmaf_rn(p, r, 4.16666679084300994873047e-02f);
-    p = __fmaf_rn(p, r, 1.66666671633720397949219e-01f);
-    p = __fmaf_rn(p, r, 0.5f);
-    p = __fmaf_rn(p, r, 1.0f);
-    p = __fmaf_rn(p, r, 1.0f);
-    int ki = (int)k;
-    if (ki > 127) {
-        p = p * 2.0f;
-        ki -= 1;
-    }
-    if (ki < -126) {
-        p = p * __int_as_float((ki + 64 + 127) << 23);
-        return p * 5.42101086242752217004e-20f;
-    }
-    return p * __int_as_float((ki + 127) << 23);
-}
-
-// log(x): x = m 2^e, m in [sqrt(1/2), sqrt(2)), log(1+f) = 2 atanh(f/(2+f))
-// arranged as f - (f^2/2 - s (f^2/2 + R)); same sequence as the oracle.
-__device__ __forceinline__ float r_logf(float x) {
-    if (x != x || x < 0.0f) return __int_as_float(0x7fc00000);
-    if (x == 0.0f) return __int_as_float(0xff800000);
-    if (x == __int_as_float(0x7f800000)) return x;
-    uint32_t u = __float_as_uint(x);
-    int e = 0;
-    if (u < 0x00800000u) {
-        u = __float_as_uint(x * 16777216.0f);
-        e = -24;
-    }
-    e += (int)((u >> 23) & 0xffu) - 127;
-    float m = __uint_as_float((u & 0x007fffffu) | 0x3f800000u);
-    if (m > 1.41421353816986083984375f) {
-        m = m * 0.5f;
-        e += 1;
-    }
-    const float f = m - 1.0f;
-    const float s = f / (2.0f + f);
-    const float z = s * s;
-    float p = 0.1538461595773697f;
-    p = __fmaf_rn(p, z, 0.1818181872367859f);
-    p = __fmaf_rn(p, z, 0.2222222238779068f);
-    p = __fmaf_rn(p, z, 0.2857142984867096f);
-    p = __fmaf_rn(p, z, 0.4000000059604645f);
-    p = __fmaf_rn(p, z, 0.6666666865348816f);
-    const float R = z * p;
-    const float hfsq = 0.5f * f * f;
-    const float ef = (float)e;
-    return ef * 0.693115234375f -
-           ((hfsq - (s * (hfsq + R) + ef * 3.19461832987144589424133e-05f)) - f);
-}
-
-__device__ __forceinline__ float r_powf(float x, float y) {
-    if (x == 0.0f) return y > 0.0f ? 0.0f : (y == 0.0f ? 1.0f : __int_as_float(0x7f800000));
-    return r_expf(y * r_logf(x));
-}
-
-__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
-    return ax * bx + ay * by + az * bz;
-}
 
 // qrot (common.wgsl:386-390)
 __device__ __forceinline__ float3 qrot(float4 q, float vx, float vy, float vz) {
@@ -111,8 +42,18 @@ __device__ __forceinline__ bool intersect(const GaussPrim *__restrict__ prims, u
                                           const WinRay &r, float t_end, float &t_out,
                                           float &alpha_out) {
     const float4 co = __ldg(&prims[pos].center_opacity);
-    const float4 qi = __ldg(&prims[pos].qinv);
     const float4 ss = __ldg(&prims[pos].scale_support);
+    {
+        // conservative pre-test: a hit lies inside the support ellipsoid, so
+        // within support * max(scale) of the mean (d is unit; the margin
+        // covers the rounding of |oc|^2 - b^2)
+        const float ox = co.x - r.ox, oy = co.y - r.oy, oz = co.z - r.oz;
+        const float b = dot3(ox, oy, oz, r.dx, r.dy, r.dz);
+        const float oo = dot3(ox, oy, oz, ox, oy, oz);
+        const float smax = fmaxf(fmaxf(ss.x, ss.y), ss.z);
+        if (oo - b * b > ss.w * (smax * smax) * 1.001f + 1e-6f * oo + 1e-30f) return false;
+    }
+    const float4 qi = __ldg(&prims[pos].qinv);
     const float3 lo0 = qrot(qi, r.ox - co.x, r.oy - co.y, r.oz - co.z);
     const float3 ld0 = qrot(qi, r.dx, r.dy, r.dz);
     const float lox = lo0.x / ss.x, loy = lo0.y / ss.y, loz = lo0.z / ss.z;
@@ -122,9 +63,9 @@ __device__ __forceinline__ bool intersect(const GaussPrim *__restrict__ prims, u
     const float px = lox + t * ldx, py = loy + t * ldy, pz = loz + t * ldz;
     const float sq = dot3(px, py, pz, px, py, pz);
     if (sq > ss.w) return false;
-    const float response = fminf(0.999f, co.w * r_expf(-0.5f * sq));
+    const float response = fminf(0.999f, co.w * bv_expf(-0.5f * sq));
     t_out = t;
-    alpha_out = 1.0f - r_powf(1.0f - response, 1.1f);
+    alpha_out = 1.0f - bv_powf(1.0f - response, 1.1f);
     return true;
 }
 
@@ -141,7 +82,7 @@ __device__ __forceinline__ void shade_light(const RelightLight &L, float px, flo
     const float awx = flx * inv, awy = fly * inv, awz = flz * inv;
     float angular = 1.0f;
     if (L.exponent != 0.0f)
-        angular = r_powf(fmaxf(dot3(L.direction[0], L.direction[1], L.direction[2], awx, awy, awz),
+        angular = bv_powf(fmaxf(dot3(L.direction[0], L.direction[1], L.direction[2], awx, awy, awz),
                                0.0f),
                          L.exponent);
     const float tx = -awx, ty = -awy, tz = -awz;

@@ -43,11 +43,20 @@ struct __align__(16) SplatPrim {
     uint4 link;   // cell (model index), Cech row begin, row end, 0
 };
 
+// One Cech entry of a support's row: the clip plane's point f = s_i + shift n
+// and normal n = s_j - s_i (shift = 0.5 + 0.5 (r_i^2 - r_j^2) / max(|n|^2,
+// 1e-20)), formed on the host in the kernel's FP32 operation order
+// (trace.rs:1351-1389), so each ray evaluates only (f - o).n and d.n.
+struct __align__(16) SplatFace {
+    float4 point;   // f, 0
+    float4 normal;  // n, 0
+};
+
 struct SplatParams {
     DeviceModel m;                 // density, SH rows (model order)
     const SplatPrim *prims;        // [N] leaf order
     const BvhNode *nodes;
-    const float4 *row_sites;       // [M] CSR order: the neighbour's x, y, z, radius
+    const SplatFace *row_faces;    // [M] CSR order: clip plane of each Cech entry
     uint32_t max_steps;
     float weight_threshold;
     uint32_t n_views;
@@ -86,33 +95,37 @@ __device__ __forceinline__ bool splat_sphere(const WinRay &ray, const float4 &s,
 
 // Cech-row clip of one support (trace.rs:1351-1389, path_interval_jacobian
 // :1199-1325 for the bounded clip), warp-cooperative: every lane calls it
-// for the same support; the row is read 32 entries at a time (one coalesced
-// load per chunk) and each entry is broadcast to the lanes that clip (need).
-// face_near / face_far are a max / min over the row and a parallel face
-// with num < 0 empties the interval, so the result does not depend on the
-// order the entries are taken in.  False for lanes whose interval is empty.
+// for the same support; the row's clip planes are read 32 at a time (one
+// coalesced load per chunk) and each is broadcast to the lanes that clip
+// (need).  face_near / face_far are a max / min over the row and a parallel
+// face with num < 0 empties the interval, so the result does not depend on
+// the order the entries are taken in; once a lane's interval is empty it
+// stays empty (face_near only grows, face_far only shrinks), and the warp
+// leaves the row when every lane's is.  False for lanes whose interval is
+// empty.
 __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinRay &ray,
-                                                const float4 &s, uint32_t begin, uint32_t end,
-                                                float depth, float sn, float sf, bool need,
-                                                float &start, float &dt) {
+                                                uint32_t begin, uint32_t end, float depth,
+                                                float sn, float sf, bool need, float &start,
+                                                float &dt) {
     const uint32_t lane = threadIdx.x & 31u;
     float face_near = 0.0f, face_far = depth;
     bool empty = !need;
     for (uint32_t base = begin; base < end; base += 32u) {
+        if (!__any_sync(0xffffffffu, !empty)) break;
         const uint32_t n = min(32u, end - base);
-        const float4 mine = base + lane < end ? __ldg(P.row_sites + base + lane)
-                                              : make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 fp = make_float4(0.f, 0.f, 0.f, 0.f), fn = fp;
+        if (base + lane < end) {
+            fp = __ldg(&P.row_faces[base + lane].point);
+            fn = __ldg(&P.row_faces[base + lane].normal);
+        }
         for (uint32_t j = 0; j < n; ++j) {
-            float4 a;
-            a.x = __shfl_sync(0xffffffffu, mine.x, j);
-            a.y = __shfl_sync(0xffffffffu, mine.y, j);
-            a.z = __shfl_sync(0xffffffffu, mine.z, j);
-            a.w = __shfl_sync(0xffffffffu, mine.w, j);
+            const float fx = __shfl_sync(0xffffffffu, fp.x, j);
+            const float fy = __shfl_sync(0xffffffffu, fp.y, j);
+            const float fz = __shfl_sync(0xffffffffu, fp.z, j);
+            const float nx = __shfl_sync(0xffffffffu, fn.x, j);
+            const float ny = __shfl_sync(0xffffffffu, fn.y, j);
+            const float nz = __shfl_sync(0xffffffffu, fn.z, j);
             if (empty) continue;
-            const float nx = a.x - s.x, ny = a.y - s.y, nz = a.z - s.z;
-            const float dsq = fmaxf(dot3(nx, ny, nz, nx, ny, nz), 1.0e-20f);
-            const float shift = 0.5f + 0.5f * (s.w * s.w - a.w * a.w) / dsq;
-            const float fx = s.x + shift * nx, fy = s.y + shift * ny, fz = s.z + shift * nz;
             const float rx = fx - ray.ox, ry = fy - ray.oy, rz = fz - ray.oz;
             const float num = dot3(rx, ry, rz, nx, ny, nz);
             const float den = dot3(ray.dx, ray.dy, ray.dz, nx, ny, nz);
@@ -125,6 +138,9 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
             } else if (num < 0.0f) {
                 empty = true;
             }
+            const float st = sn > face_near ? sn : face_near;
+            const float en = sf < face_far ? sf : face_far;
+            if (en <= st) empty = true;
         }
     }
     if (empty) return false;
@@ -224,7 +240,7 @@ splat_kernel(const __grid_constant__ SplatParams P) {
         const uint4 link = __ldg(&P.prims[p].link);
         if (need) clipped += link.z - link.y;
         float st, dt;
-        if (!splat_clip_warp(P, ray, s, link.y, link.z, depth, sn, sf, need, st, dt)) return false;
+        if (!splat_clip_warp(P, ray, link.y, link.z, depth, sn, sf, need, st, dt)) return false;
         t = st;
         cell = link.x;
         aux = __float_as_uint(dt);
@@ -332,7 +348,7 @@ struct bv_splat_tracer {
     // device
     SplatPrim *prims = nullptr;
     BvhNode *nodes = nullptr;
-    float4 *row_sites = nullptr;
+    SplatFace *row_faces = nullptr;
     float *density = nullptr;
     void *sh = nullptr;
     unsigned long long *stats = nullptr;
@@ -366,7 +382,7 @@ void free_splat(bv_splat_tracer *t) {
     if (!t) return;
     cudaFree(t->prims);
     cudaFree(t->nodes);
-    cudaFree(t->row_sites);
+    cudaFree(t->row_faces);
     cudaFree(t->density);
     cudaFree(t->sh);
     cudaFree(t->stats);
@@ -394,7 +410,7 @@ bv_status enqueue_splats(bv_splat_tracer *t, float4 *out, const bv_camera *cams,
         p.m = t->model();
         p.prims = t->prims;
         p.nodes = t->nodes;
-        p.row_sites = t->row_sites;
+        p.row_faces = t->row_faces;
         p.max_steps = t->settings.max_steps;
         p.weight_threshold = t->settings.weight_threshold;
         p.n_views = nc;
@@ -470,11 +486,22 @@ bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *md, const bv_trace_
         prims[i].site = make_float4(p[0], p[1], p[2], md->radii[c]);
         prims[i].link = make_uint4(c, md->adjacency_offsets[c], md->adjacency_offsets[c + 1], 0u);
     }
-    std::vector<float4> rows(std::max<uint32_t>(m_edges, 1));
-    for (uint32_t k = 0; k < m_edges; ++k) {
-        const uint32_t j = md->adjacency_neighbors[k];
-        const float *p = md->points + 4 * (size_t)j;
-        rows[k] = make_float4(p[0], p[1], p[2], md->radii[j]);
+    // clip planes of every Cech entry, FP32 in the per-ray order of
+    // powerfoam_splat_interval (this file is built with FP contraction off)
+    std::vector<SplatFace> rows(std::max<uint32_t>(m_edges, 1));
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *si = md->points + 4 * (size_t)i;
+        const float ri = md->radii[i];
+        for (uint32_t k = md->adjacency_offsets[i]; k < md->adjacency_offsets[i + 1]; ++k) {
+            const uint32_t j = md->adjacency_neighbors[k];
+            const float *a = md->points + 4 * (size_t)j;
+            const float rj = md->radii[j];
+            const float nx = a[0] - si[0], ny = a[1] - si[1], nz = a[2] - si[2];
+            const float dsq = std::max((nx * nx + ny * ny) + nz * nz, 1.0e-20f);
+            const float shift = 0.5f + 0.5f * (ri * ri - rj * rj) / dsq;
+            rows[k].point = make_float4(si[0] + shift * nx, si[1] + shift * ny, si[2] + shift * nz, 0.f);
+            rows[k].normal = make_float4(nx, ny, nz, 0.f);
+        }
     }
     std::vector<float> dens(n);
     for (uint32_t i = 0; i < n; ++i) dens[i] = md->points[4 * (size_t)i + 3];
@@ -500,7 +527,7 @@ bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *md, const bv_trace_
     } while (0)
     SP_TRY(cudaMalloc(&t->prims, sizeof(SplatPrim) * n), "cudaMalloc supports");
     SP_TRY(cudaMalloc(&t->nodes, sizeof(BvhNode) * t->n_nodes), "cudaMalloc nodes");
-    SP_TRY(cudaMalloc(&t->row_sites, sizeof(float4) * rows.size()), "cudaMalloc rows");
+    SP_TRY(cudaMalloc(&t->row_faces, sizeof(SplatFace) * rows.size()), "cudaMalloc rows");
     SP_TRY(cudaMalloc(&t->density, sizeof(float) * n), "cudaMalloc density");
     SP_TRY(cudaMalloc(&t->stats, sizeof(unsigned long long) * 4), "cudaMalloc stats");
     SP_TRY(cudaMalloc(&t->max_candidates, sizeof(uint32_t)), "cudaMalloc counter");
@@ -508,7 +535,7 @@ bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *md, const bv_trace_
     SP_TRY(cudaMemcpy(t->prims, prims.data(), sizeof(SplatPrim) * n, cudaMemcpyHostToDevice), "upload supports");
     SP_TRY(cudaMemcpy(t->nodes, bvh.nodes.data(), sizeof(BvhNode) * t->n_nodes, cudaMemcpyHostToDevice),
            "upload nodes");
-    SP_TRY(cudaMemcpy(t->row_sites, rows.data(), sizeof(float4) * rows.size(), cudaMemcpyHostToDevice),
+    SP_TRY(cudaMemcpy(t->row_faces, rows.data(), sizeof(SplatFace) * rows.size(), cudaMemcpyHostToDevice),
            "upload rows");
     SP_TRY(cudaMemcpy(t->density, dens.data(), sizeof(float) * n, cudaMemcpyHostToDevice), "upload density");
     if (bf16) {

@@ -42,6 +42,7 @@ constexpr int kWalkBlock = 256;
 #endif
 constexpr int kFaceUnroll = BV_FACE_UNROLL;
 
+
 // Tile-ordered work index -> (view, pixel).  Returns false for the padding
 // lanes of partial edge tiles.
 template <typename Params>

@@ -240,6 +240,20 @@ def cech_csr(xyz: np.ndarray, radii: np.ndarray):
     return _csr_from_pairs(len(xyz), a[keep], b[keep])
 
 
+def rebuild_adjacency(model: "PointCloudModel") -> "PointCloudModel":
+    """A copy of the model with its CSR rebuilt from the current sites:
+    Delaunay edges for RadFoam, the Cech overlap graph for PowerFoam
+    (try_compute_adjacency / compute_cech, adjacency.rs:142-200, :418).  Use
+    it after optimizer steps have moved sites, then build a new tracer."""
+    out = model.copy()
+    xyz = np.ascontiguousarray(out.points[:, :3], np.float32)
+    if out.radii is None:
+        out.offsets, out.neighbors = delaunay_csr(xyz)
+    else:
+        out.offsets, out.neighbors = cech_csr(xyz, out.radii)
+    return out
+
+
 # --------------------------------------------------------------------------
 # generators
 # --------------------------------------------------------------------------

@@ -212,6 +212,52 @@ bv_status bv_forward_backward(bv_tracer *tracer, const bv_camera *cameras, uint3
                               const bv_train_settings *settings, const bv_grads *grads,
                               float *loss_dev, float *rgb_out_dev, bv_stream stream);
 
+/* ---- optimizer step ---------------------------------------------------------
+ * The trainer's Adam (meganeura, configured per parameter group by
+ * configure_optimizer / radfoam_v1_lrs, blade-volume-train/src/diff_render.rs:
+ * 3215-3330) over the gradient tables of bv_forward_backward, applied to the
+ * tracer's own device model, so that a training loop needs no other library:
+ * forward_backward -> adam_step -> forward_backward ...  Kingma & Ba's Adam
+ * with bias correction in FP32.  The density table is the activation of a
+ * raw parameter x (density_activation, diff_render.rs:4649-4656): identity,
+ * ReLU, or softplus(beta x) / beta; x starts at the inverse activation of the
+ * model's density (:4658-4672).  A table whose rate is 0 is frozen; a NULL
+ * gradient pointer skips its table.  BF16 SH models keep an FP32 master copy
+ * (starting at the BF16 values) and store each update rounded to BF16.  The
+ * optimizer state (moments, raw density, master SH; 4 to 8 floats per
+ * parameter) is allocated by the first call; its activation and beta must
+ * stay the same across calls.  Position updates move sites within the
+ * model's fixed adjacency (the reference rebuilds adjacency in its densify
+ * schedule, outside this path). */
+#define BV_DENSITY_IDENTITY 0u
+#define BV_DENSITY_RELU 1u
+#define BV_DENSITY_SOFTPLUS 2u
+
+typedef struct bv_adam_settings {
+    float lr_density;           /* rate of the raw density parameter */
+    float lr_sh_dc;             /* SH component 0 (three DC coefficients per site) */
+    float lr_sh_rest;           /* SH components 1..K-1 */
+    float lr_position;          /* site positions */
+    float lr_radius;            /* PowerFoam radii */
+    float beta1;                /* 0.9 */
+    float beta2;                /* 0.999 */
+    float eps;                  /* 1e-15 in radfoam_v1 (diff_render.rs:3307) */
+    uint32_t density_activation; /* BV_DENSITY_* */
+    float softplus_beta;        /* beta > 0 for BV_DENSITY_SOFTPLUS */
+} bv_adam_settings;
+
+bv_status bv_radfoam_tracer_adam_step(bv_tracer *tracer, const bv_grads *grads,
+                                      const bv_adam_settings *settings, bv_stream stream);
+/* Optimizer steps taken so far. */
+uint32_t bv_radfoam_tracer_adam_steps(const bv_tracer *tracer);
+
+/* Reads the tracer's current device model back into host arrays in the
+ * model's layout (the trainer's parameter readback, diff_render.rs:4812-4851):
+ * points [N*4] (x, y, z, density), sh [N*3K], radii [N] (PowerFoam; may be
+ * NULL).  Any pointer may be NULL to skip it.  Synchronises the device. */
+bv_status bv_radfoam_tracer_read_model(bv_tracer *tracer, float *points, float *sh,
+                                       float *radii);
+
 /* ---- instrumentation -----------------------------------------------------
  * Device time (ms, CUDA events on the launch stream) and work counters of
  * the last dispatch / record / forward_backward call on this tracer.

@@ -1837,3 +1837,72 @@ void bvo_render_walk_f64(const bvo_model *m, const bvo_camera *cam, uint32_t wid
     }
     (void)threads;
 }
+
+/* ------------------------------------------------------------------ */
+/* optimizer step (Adam), FP32                                         */
+/* ------------------------------------------------------------------ */
+float bvo_density_activation(float x, int kind, float beta) {
+    if (kind == 1) return fmaxf(x, 0.0f);
+    if (kind == 2) {
+        const float bx = beta * x;
+        const float sp = bx > 20.0f ? bx : bvo_logf(1.0f + bvo_expf(bx));
+        return sp / beta;
+    }
+    return x;
+}
+
+static float density_activation_grad(float x, int kind, float beta) {
+    if (kind == 1) return x > 0.0f ? 1.0f : 0.0f;
+    if (kind == 2) return 1.0f / (1.0f + bvo_expf(-(beta * x)));
+    return 1.0f;
+}
+
+float bvo_density_activation_inverse(float y, int kind, float beta) {
+    if (kind != 2) return y;
+    const float by = beta * y;
+    const float x = by > 20.0f ? by : bvo_logf(fmaxf(bvo_expf(by) - 1.0f, 1e-20f));
+    return x / beta;
+}
+
+typedef struct {
+    float beta1, beta2, omb1, omb2, c1, c2, eps;
+} adam_scalars;
+
+static inline float adam_update(float p, float g, float *m, float *v, const adam_scalars *a,
+                                float lr) {
+    *m = a->beta1 * *m + a->omb1 * g;
+    *v = a->beta2 * *v + a->omb2 * (g * g);
+    const float mhat = *m / a->c1;
+    const float vhat = *v / a->c2;
+    return p - (lr * mhat) / (sqrtf(vhat) + a->eps);
+}
+
+void bvo_adam_step(bvo_adam_state *s, const bvo_adam_settings *a, uint32_t t, const float *gd,
+                   const float *gsh, const float *gpos, const float *gr) {
+    const adam_scalars k = {a->beta1, a->beta2, 1.0f - a->beta1, 1.0f - a->beta2,
+                            (float)(1.0 - pow((double)a->beta1, (double)t)),
+                            (float)(1.0 - pow((double)a->beta2, (double)t)), a->eps};
+    const float beta = a->activation == 2 ? a->softplus_beta : 0.0f;
+    for (uint32_t i = 0; i < s->n; ++i) {
+        if (gd && a->lr_density != 0.0f) {
+            const float g = gd[i] * density_activation_grad(s->x[i], a->activation, beta);
+            s->x[i] = adam_update(s->x[i], g, &s->m_d[i], &s->v_d[i], &k, a->lr_density);
+            s->density[i] = bvo_density_activation(s->x[i], a->activation, beta);
+        }
+        if (gsh)
+            for (uint32_t c = 0; c < s->nsh; ++c) {
+                const float lr = c < 3 ? a->lr_sh_dc : a->lr_sh_rest;
+                if (lr == 0.0f) continue;
+                const size_t j = (size_t)i * s->nsh + c;
+                s->sh[j] = adam_update(s->sh[j], gsh[j], &s->m_sh[j], &s->v_sh[j], &k, lr);
+            }
+        if (gpos && a->lr_position != 0.0f)
+            for (int c = 0; c < 3; ++c) {
+                const size_t j = (size_t)i * 3 + c;
+                s->pos[j] = adam_update(s->pos[j], gpos[j], &s->m_pos[j], &s->v_pos[j], &k,
+                                        a->lr_position);
+            }
+        if (gr && s->radii && a->lr_radius != 0.0f)
+            s->radii[i] = adam_update(s->radii[i], gr[i], &s->m_r[i], &s->v_r[i], &k, a->lr_radius);
+    }
+}

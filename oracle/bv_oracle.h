@@ -287,6 +287,34 @@ void bvo_render_walk_f64(const bvo_model *m, const bvo_camera *cam, uint32_t wid
                          uint32_t start_point, double *out_rgba, uint32_t *cells, uint32_t cap,
                          uint32_t *cell_count, int threads);
 
+/* ---- optimizer step (Adam) ----
+ * Kingma & Ba's Adam with bias correction in FP32, the restatement the
+ * device optimizer follows operation for operation; the density table is
+ * the activation of a raw parameter (density_activation,
+ * blade-volume-train/src/diff_render.rs:4649-4672): 0 identity, 1 ReLU,
+ * 2 softplus(beta x)/beta.  c_i = 1 - beta_i^t in FP64, rounded once. */
+typedef struct {
+    float lr_density, lr_sh_dc, lr_sh_rest, lr_position, lr_radius;
+    float beta1, beta2, eps;
+    int activation;
+    float softplus_beta;
+} bvo_adam_settings;
+
+typedef struct {
+    uint32_t n, nsh;
+    float *x, *m_d, *v_d;      /* [n] raw density parameter and moments */
+    float *density;            /* [n] out: activation of x */
+    float *sh, *m_sh, *v_sh;   /* [n*nsh] */
+    float *pos, *m_pos, *v_pos; /* [n*3] */
+    float *radii, *m_r, *v_r;  /* [n] or NULL */
+} bvo_adam_state;
+
+float bvo_density_activation(float x, int kind, float beta);
+float bvo_density_activation_inverse(float y, int kind, float beta);
+/* One step t (1-based); a NULL gradient skips its table, a zero rate freezes it. */
+void bvo_adam_step(bvo_adam_state *s, const bvo_adam_settings *a, uint32_t t, const float *g_density,
+                   const float *g_sh, const float *g_pos, const float *g_radii);
+
 #ifdef __cplusplus
 }
 #endif

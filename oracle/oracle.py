@@ -78,6 +78,20 @@ class GaussianSettings(C.Structure):
                 ("t_start", C.c_float), ("t_end", C.c_float)]
 
 
+class AdamSettings(C.Structure):
+    _fields_ = [("lr_density", C.c_float), ("lr_sh_dc", C.c_float), ("lr_sh_rest", C.c_float),
+                ("lr_position", C.c_float), ("lr_radius", C.c_float), ("beta1", C.c_float),
+                ("beta2", C.c_float), ("eps", C.c_float), ("activation", C.c_int),
+                ("softplus_beta", C.c_float)]
+
+
+class AdamState(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("nsh", C.c_uint32), ("x", f32p), ("m_d", f32p),
+                ("v_d", f32p), ("density", f32p), ("sh", f32p), ("m_sh", f32p), ("v_sh", f32p),
+                ("pos", f32p), ("m_pos", f32p), ("v_pos", f32p), ("radii", f32p), ("m_r", f32p),
+                ("v_r", f32p)]
+
+
 class ParamsF64(C.Structure):
     _fields_ = [("points", f64p), ("sh", f64p), ("radii", f64p)]
 
@@ -154,6 +168,12 @@ def lib():
         L.bvo_render_walk_f64.argtypes = [C.POINTER(Model), C.POINTER(Camera), C.c_uint32,
                                           C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, f64p,
                                           u32p, C.c_uint32, u32p, C.c_int]
+        L.bvo_density_activation.restype = C.c_float
+        L.bvo_density_activation.argtypes = [C.c_float, C.c_int, C.c_float]
+        L.bvo_density_activation_inverse.restype = C.c_float
+        L.bvo_density_activation_inverse.argtypes = [C.c_float, C.c_int, C.c_float]
+        L.bvo_adam_step.argtypes = [C.POINTER(AdamState), C.POINTER(AdamSettings), C.c_uint32,
+                                    f32p, f32p, f32p, f32p]
         L.bvo_gaussian_response.restype = C.c_int
         L.bvo_gaussian_response.argtypes = [C.POINTER(GaussianScene), C.c_uint32, f32p, f32p,
                                             C.POINTER(GaussianSettings), f32p, f32p]
@@ -576,3 +596,50 @@ def gaussian_render(scene: GaussianOracleScene, cam, width, height, min_transmit
                               float(min_transmittance), _ptr(bg, f32p), _ptr(out, f32p),
                               _ptr(hits, u32p), threads)
     return out, hits
+
+
+# --------------------------------------------------------------------------
+# optimizer step (Adam, FP32)
+# --------------------------------------------------------------------------
+class AdamOracle:
+    """FP32 Adam over a model's tables (bvo_adam_step); starts from the
+    model's values, the raw density parameter at the inverse activation."""
+
+    def __init__(self, points, sh, radii, activation=0, softplus_beta=10.0):
+        points = np.asarray(points, np.float32).reshape(-1, 4)
+        n = len(points)
+        self.activation = int(activation)
+        self.beta = float(softplus_beta) if activation == 2 else 0.0
+        self.density = np.ascontiguousarray(points[:, 3])
+        self.x = np.array([lib().bvo_density_activation_inverse(float(y), self.activation,
+                                                                  self.beta)
+                           for y in self.density], np.float32)
+        self.pos = np.ascontiguousarray(points[:, :3]).copy()
+        self.sh = np.ascontiguousarray(sh, np.float32).reshape(n, -1).copy()
+        self.radii = None if radii is None else np.ascontiguousarray(radii, np.float32).copy()
+        z = lambda a: np.zeros_like(a)  # noqa: E731
+        self.m_d, self.v_d = z(self.x), z(self.x)
+        self.m_sh, self.v_sh = z(self.sh), z(self.sh)
+        self.m_pos, self.v_pos = z(self.pos), z(self.pos)
+        r = self.radii if self.radii is not None else np.zeros(n, np.float32)
+        self.m_r, self.v_r = z(r), z(r)
+        self.t = 0
+        self.c = AdamState(n, self.sh.shape[1], _ptr(self.x, f32p), _ptr(self.m_d, f32p),
+                           _ptr(self.v_d, f32p), _ptr(self.density, f32p), _ptr(self.sh, f32p),
+                           _ptr(self.m_sh, f32p), _ptr(self.v_sh, f32p), _ptr(self.pos, f32p),
+                           _ptr(self.m_pos, f32p), _ptr(self.v_pos, f32p),
+                           _ptr(self.radii, f32p), _ptr(self.m_r, f32p), _ptr(self.v_r, f32p))
+
+    def step(self, settings: dict, g_density=None, g_sh=None, g_pos=None, g_radii=None):
+        a = AdamSettings(settings.get("lr_density", 0.0), settings.get("lr_sh_dc", 0.0),
+                         settings.get("lr_sh_rest", 0.0), settings.get("lr_position", 0.0),
+                         settings.get("lr_radius", 0.0), settings.get("beta1", 0.9),
+                         settings.get("beta2", 0.999), settings.get("eps", 1e-15),
+                         self.activation, self.beta)
+        self.t += 1
+        conv = lambda g: None if g is None else np.ascontiguousarray(g, np.float32).reshape(-1)  # noqa: E731
+        gs = [conv(g) for g in (g_density, g_sh, g_pos, g_radii)]
+        lib().bvo_adam_step(C.byref(self.c), C.byref(a), self.t, *[_ptr(g, f32p) for g in gs])
+
+    def points(self):
+        return np.concatenate([self.pos, self.density[:, None]], axis=1).astype(np.float32)
