@@ -102,11 +102,7 @@ def build_workload(args, rank):
 
     from blade_volume_b200 import dist as bvdist
 
-    if args.workload == "powerfoam":
-        # the PowerFoam mixture (radii U[0, 0.02], BF16 SH degree 3), walk semantics
-        model = scenes.powerfoam_mixture(args.splat_sites, seed=0)
-    else:
-        model = scenes.radfoam_ball(args.sites, seed=0, sh_degree=3)
+    model = scenes.radfoam_ball(args.sites, seed=0, sh_degree=3)
     return model, bvdist.rank_cameras(args.views, rank)
 
 
@@ -441,6 +437,110 @@ def run_secondary(args):
     print(json.dumps(line), flush=True)
 
 
+def run_powerfoam_train(args):
+    """PowerFoam forward+backward (1,048,576-site mixture, radii U[0, 0.02],
+    BF16 SH degree 3, 4 x 1024^2, L2) with splat semantics, the training
+    recorder's PowerFoam path: the Cech graph of these radii is disconnected,
+    so a walk from the camera cell would miss most of the scene."""
+    import torch
+
+    import blade_volume_b200 as bv
+    from blade_volume_b200 import dist as bvdist
+    from blade_volume_b200 import scenes
+
+    torch.cuda.set_device(0)
+    t_build = time.time()
+    model = scenes.powerfoam_mixture(args.splat_sites, seed=0)
+    t_build = time.time() - t_build
+    cams = bvdist.rank_cameras(args.views, 0)
+    W = H = args.size
+    tgt_tracer = bv.PowerFoamSplatTracer(scenes.perturbed(model, seed=2), max_steps=MAX_STEPS,
+                                         weight_threshold=1e-3)
+    target = tgt_tracer.render(cams, W, H)[..., :3].contiguous()
+    tgt_tracer.deinit()
+    tracer = bv.PowerFoamSplatTracer(model, max_steps=MAX_STEPS, weight_threshold=0.0)
+    grads = tracer.new_grads()
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    rays = len(cams) * W * H
+
+    def step(tgt):
+        for g in grads.values():
+            g.zero_()
+        tracer.forward_backward(cams, W, H, tgt, grads, max_steps=MAX_STEPS, weight_threshold=0.0,
+                                max_dt=MAX_DT, loss_out=loss)
+
+    for _ in range(max(args.warmup, 3)):
+        step(target)
+    tracer.enable_stats(True)
+    step(target)
+    st = tracer.last_stats()
+    tracer.enable_stats(False)
+    sampler = ClockSampler(0)
+    torch.cuda.synchronize()
+    sampler.start()
+    ts = timed_events(lambda: step(target), args.steps, flush, stream)
+    clocks = sampler.stop()
+    ms = sum(ts) / len(ts)
+    # end to end: pinned host targets in, loss out
+    host_target = torch.empty(target.shape, dtype=torch.float32, pin_memory=True)
+    host_target.copy_(target.cpu())
+    host_loss = torch.empty(1, dtype=torch.float32, pin_memory=True)
+    dev_target = torch.empty_like(target)
+
+    def e2e_step():
+        dev_target.copy_(host_target, non_blocking=True)
+        step(dev_target)
+        host_loss.copy_(loss, non_blocking=True)
+
+    e2e = timed_events(e2e_step, args.steps, flush, stream)
+    e2e_ms = sum(e2e) / len(e2e)
+    # bytes (reference layout): per Cech entry clipped 20 B, per composited
+    # interval the BF16 SH row (2*3K + 4 B) twice (forward, replay) plus the
+    # gradient atomics 2 * (4 + 4 * 3K + 3 * 16) B, 16 B per ray out
+    K = 16
+    alg = (2 * st.faces * 20 + st.steps * (2 * (2 * 3 * K + 4) + 2 * (4 + 4 * 3 * K + 48))
+           + rays * 16)
+    peak, kind = peaks()
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        om = O.OracleModel.from_scene(model)
+        side = 16
+        tg = np.zeros((1, side, side, 3), np.float32)
+        t0 = time.perf_counter()
+        O.forward_backward(om, cams[:1], side, side, MAX_STEPS, 0.0, MAX_DT, tg, 0,
+                           splats=True)
+        dt = time.perf_counter() - t0
+        cpu = {"value": side * side / dt / 1e6, "unit": UNIT, "cores": os.cpu_count() or 1,
+               "kind": "port",
+               "sample": f"oracle splat fwd+bwd (every support tested per ray), view 0 at "
+                         f"{side}x{side}, {dt:.2f} s"}
+    line = {"metric": METRIC, "value": rays / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (SH bf16)", "data": "synthetic",
+            "config": {"workload": "powerfoam_mixture fwd+bwd, splat semantics, BF16 SH",
+                       "sites": model.n, "cech_mean_degree": model.mean_degree(), "sh_degree": 3,
+                       "views": len(cams), "width": W, "height": H, "loss": "L2",
+                       "max_steps": MAX_STEPS, "max_dt": MAX_DT, "scene_build_s": t_build,
+                       "l2": "flushed between timed steps (256 MB write)"},
+            "e2e": {"value": rays / (e2e_ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": int(target.numel() * 4), "d2h_bytes_per_step": 4},
+            "intervals_per_ray": st.steps / max(st.rays, 1),
+            "cech_entries_clipped_per_ray": st.faces / max(st.rays, 1),
+            "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
+                         "traffic": None, "peak_source": kind},
+            "gpu_launches": 3 * args.steps, "clocks": clocks}
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    tracer.deinit()
+
+
 def run_serving(args):
     """Serving loop: resident RadFoam scenes, Poisson request streams (mixed
     resolution, 1-16 views, 10% forward+backward with L2 loss), batched
@@ -510,7 +610,10 @@ def main():
     if args.workload == "serving":
         run_serving(args)
         return
-    if args.workload not in ("train", "powerfoam"):
+    if args.workload == "powerfoam":
+        run_powerfoam_train(args)
+        return
+    if args.workload != "train":
         run_secondary(args)
         return
     import torch

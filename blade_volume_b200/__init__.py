@@ -70,6 +70,7 @@ EXPORTED_SYMBOLS = [
     "bv_gaussian_tracer_num_points", "bv_gaussian_tracer_dispatch",
     "bv_gaussian_tracer_enable_stats", "bv_gaussian_tracer_last_stats",
     "bv_radfoam_tracer_adam_step", "bv_radfoam_tracer_adam_steps", "bv_radfoam_tracer_read_model",
+    "bv_powerfoam_splat_tracer_forward_backward",
 ]
 DENSITY_IDENTITY, DENSITY_RELU, DENSITY_SOFTPLUS = 0, 1, 2
 SERVE_BATCHED, SERVE_PLAIN, SERVE_PLAIN_BATCH = 0, 1, 2
@@ -292,6 +293,9 @@ def load_library(path: str = LIB_PATH):
     L.bv_powerfoam_splat_tracer_set_weight_threshold.argtypes = [C.c_void_p, C.c_float]
     L.bv_powerfoam_splat_tracer_enable_stats.argtypes = [C.c_void_p, C.c_uint32]
     L.bv_powerfoam_splat_tracer_last_stats.argtypes = [C.c_void_p, C.POINTER(LaunchStats)]
+    L.bv_powerfoam_splat_tracer_forward_backward.argtypes = [
+        C.c_void_p, C.POINTER(CameraC), C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+        C.POINTER(TrainSettings), C.POINTER(Grads), C.c_void_p, C.c_void_p, C.c_void_p]
     L.bv_radfoam_tracer_adam_step.argtypes = [C.c_void_p, C.POINTER(Grads),
                                               C.POINTER(AdamSettingsC), C.c_void_p]
     L.bv_radfoam_tracer_adam_steps.argtypes = [C.c_void_p]
@@ -719,12 +723,13 @@ class GaussianTracer:
 class PowerFoamSplatTracer:
     """PowerFoamGpuSplatTracer (gpu/powerfoam_splat.rs:38-370) over the C ABI:
     the order-exact splat render of a PowerFoam model (radii required; the
-    CSR is the Cech overlap graph)."""
+    CSR is the Cech overlap graph), and training with splat semantics."""
 
     def __init__(self, model: PointCloudModel, max_steps: int = 1024,
                  weight_threshold: float = 0.001, candidate_capacity: int = 0):
         L = load_library()
         self.model = model
+        self.sh_components = model.sh_components
         d = _DescHolder(model)
         s = TraceSettings(max_steps, candidate_capacity, weight_threshold, 0)
         h = C.c_void_p()
@@ -784,6 +789,39 @@ class PowerFoamSplatTracer:
         _check(load_library().bv_powerfoam_splat_tracer_validate_candidate_counts(self._h,
                                                                                  C.byref(v)))
         return v.value
+
+    def forward_backward(self, cameras: Sequence[Camera], width: int, height: int, target,
+                         grads: dict, max_steps: int = 1024, weight_threshold: float = 0.0,
+                         max_dt: float = 50.0, loss: int = LOSS_L2, loss_out=None, rgb_out=None,
+                         stream=None):
+        """bv_powerfoam_splat_tracer_forward_backward: the training step's
+        gradients with splat semantics (same arguments as
+        RadFoamGpuTracer.forward_backward)."""
+        import torch
+
+        if loss_out is None:
+            loss_out = torch.zeros(1, dtype=torch.float32, device="cuda")
+        ts = TrainSettings(max_steps, weight_threshold, max_dt, loss)
+        g = Grads(grads["d_density"].data_ptr(), grads["d_sh"].data_ptr(),
+                  grads["d_pos"].data_ptr() if grads.get("d_pos") is not None else None,
+                  grads["d_radius"].data_ptr() if grads.get("d_radius") is not None else None)
+        arr = (CameraC * len(cameras))(*[camera_c(c) for c in cameras])
+        _check(load_library().bv_powerfoam_splat_tracer_forward_backward(
+            self._h, arr, len(cameras), width, height, C.c_void_p(target.data_ptr()),
+            C.byref(ts), C.byref(g), C.c_void_p(loss_out.data_ptr()),
+            C.c_void_p(rgb_out.data_ptr()) if rgb_out is not None else None,
+            _stream_handle(stream)))
+        return loss_out
+
+    def new_grads(self):
+        import torch
+
+        n = self.model.n
+        return dict(d_density=torch.zeros(n, dtype=torch.float32, device="cuda"),
+                    d_sh=torch.zeros(n * 3 * self.sh_components, dtype=torch.float32,
+                                     device="cuda"),
+                    d_pos=torch.zeros(n * 3, dtype=torch.float32, device="cuda"),
+                    d_radius=torch.zeros(n, dtype=torch.float32, device="cuda"))
 
     def candidate_stats(self):
         """(max support hits of one ray, total hits, Cech row entries of the

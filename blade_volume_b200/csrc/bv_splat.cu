@@ -28,6 +28,7 @@
 #include "bv_bvh.h"
 #include "bv_device.cuh"
 #include "bv_internal.h"
+#include "bv_segment.cuh"
 #include "bv_window.cuh"
 
 namespace bv {
@@ -153,6 +154,67 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
     return true;
 }
 
+// Window candidate test of support p for win_gather_warp (every lane calls
+// it): the sphere test per lane, then the warp clips the support's Cech row
+// for the lanes whose sphere interval can still enter their window; the key
+// is (clipped entry depth, cell) and aux carries the interval length.
+__device__ __forceinline__ bool splat_hit(const SplatParams &P, const WinRay &ray, float depth,
+                                          bool cursor_valid, float cur_t, uint32_t p, bool mine,
+                                          float limit, float &t, uint32_t &cell, uint32_t &aux,
+                                          uint32_t &clipped) {
+    const float4 s = __ldg(&P.prims[p].site);
+    float sn = 0.f, sf = 0.f;
+    bool need = mine && splat_sphere(ray, s, depth, sn, sf);
+    // the clipped start lies in [sn, sf): skip supports whose every key is at
+    // or below the cursor or past the window end
+    if (need && cursor_valid && sf <= cur_t) need = false;
+    if (need && sn > limit) need = false;
+    if (!__any_sync(0xffffffffu, need)) return false;
+    const uint4 link = __ldg(&P.prims[p].link);
+    if (need) clipped += link.z - link.y;
+    float st, dt;
+    if (!splat_clip_warp(P, ray, link.y, link.z, depth, sn, sf, need, st, dt)) return false;
+    t = st;
+    cell = link.x;
+    aux = __float_as_uint(dt);
+    return true;
+}
+
+// The tile / view of work item w and its camera ray (radfoam.wgsl:44-52).
+// active: the lane has a pixel and a valid direction.
+struct SplatLane {
+    WinRay ray;
+    Ray r0;
+    const ViewDesc *vd;
+    uint32_t x, y;
+    bool inside, active;
+};
+
+template <typename Params>
+__device__ __forceinline__ SplatLane splat_lane(const Params &P, uint32_t w) {
+    SplatLane L;
+    uint32_t view = 0;
+    while (view + 1 < P.n_views && w >= P.views[view + 1].ray_begin) ++view;
+    L.vd = &P.views[view];
+    const uint32_t local = w - L.vd->ray_begin;
+    const uint32_t tile = local / kTileRays, in = local % kTileRays;
+    L.x = (tile % L.vd->tiles_x) * kTileW + in % kTileW;
+    L.y = (tile / L.vd->tiles_x) * kTileH + in / kTileW;
+    L.inside = L.x < L.vd->width && L.y < L.vd->height;
+    L.r0 = Ray{0.f, 0.f, 0.f, 1.f, 0.f, 0.f};
+    L.active = L.inside && make_ray(*L.vd, L.x, L.y, L.r0);
+    L.ray.ox = L.r0.ox;
+    L.ray.oy = L.r0.oy;
+    L.ray.oz = L.r0.oz;
+    L.ray.dx = L.active ? L.r0.dx : 1.0f;
+    L.ray.dy = L.active ? L.r0.dy : 0.0f;
+    L.ray.dz = L.active ? L.r0.dz : 0.0f;
+    L.ray.ix = win_inverse(L.ray.dx);
+    L.ray.iy = win_inverse(L.ray.dy);
+    L.ray.iz = win_inverse(L.ray.dz);
+    return L;
+}
+
 template <int DEG, bool BF16>
 __global__ void __launch_bounds__(kSplatBlock)
 splat_kernel(const __grid_constant__ SplatParams P) {
@@ -161,29 +223,12 @@ splat_kernel(const __grid_constant__ SplatParams P) {
     // stay (inactive) because the main pass is warp-cooperative.
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
     if ((w & ~31u) >= P.total_work) return;
-    uint32_t view = 0;
-    while (view + 1 < P.n_views && w >= P.views[view + 1].ray_begin) ++view;
-    const ViewDesc &vd = P.views[view];
-    const uint32_t local = w - vd.ray_begin;
-    const uint32_t tile = local / kTileRays, in = local % kTileRays;
-    const uint32_t x = (tile % vd.tiles_x) * kTileW + in % kTileW;
-    const uint32_t y = (tile / vd.tiles_x) * kTileH + in / kTileW;
-    const bool inside = x < vd.width && y < vd.height;
-    float4 *out = P.out + (size_t)vd.pixel_begin + (size_t)y * vd.width + x;
-    Ray r0{0.f, 0.f, 0.f, 1.f, 0.f, 0.f};
-    const bool active = inside && make_ray(vd, x, y, r0);
-    if (inside && !active && !P.count_only) *out = make_float4(0.f, 0.f, 0.f, 0.f);
-    WinRay ray;
-    ray.ox = r0.ox;
-    ray.oy = r0.oy;
-    ray.oz = r0.oz;
-    ray.dx = active ? r0.dx : 1.0f;
-    ray.dy = active ? r0.dy : 0.0f;
-    ray.dz = active ? r0.dz : 0.0f;
-    ray.ix = win_inverse(ray.dx);
-    ray.iy = win_inverse(ray.dy);
-    ray.iz = win_inverse(ray.dz);
-    const float depth = vd.depth;
+    const SplatLane L = splat_lane(P, w);
+    const WinRay &ray = L.ray;
+    const bool active = L.active;
+    float4 *out = P.out + (size_t)L.vd->pixel_begin + (size_t)L.y * L.vd->width + L.x;
+    if (L.inside && !active && !P.count_only) *out = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float depth = L.vd->depth;
 
     if (P.count_only) {
         // every support hit, no window pruning, one ray per thread
@@ -225,26 +270,10 @@ splat_kernel(const __grid_constant__ SplatParams P) {
     bool cursor_valid = false, finished = !active;
     float cur_t = 0.f;
     uint32_t cur_cell = 0;
-    // support p: sphere test per lane, then the warp clips its Cech row for
-    // the lanes whose sphere interval can still enter their window
     auto hit = [&](uint32_t p, bool mine, float limit, float &t, uint32_t &cell,
                    uint32_t &aux) -> bool {
-        const float4 s = __ldg(&P.prims[p].site);
-        float sn = 0.f, sf = 0.f;
-        bool need = mine && splat_sphere(ray, s, depth, sn, sf);
-        // the clipped start lies in [sn, sf): skip supports whose every key is
-        // at or below the cursor or past the window end
-        if (need && cursor_valid && sf <= cur_t) need = false;
-        if (need && sn > limit) need = false;
-        if (!__any_sync(0xffffffffu, need)) return false;
-        const uint4 link = __ldg(&P.prims[p].link);
-        if (need) clipped += link.z - link.y;
-        float st, dt;
-        if (!splat_clip_warp(P, ray, link.y, link.z, depth, sn, sf, need, st, dt)) return false;
-        t = st;
-        cell = link.x;
-        aux = __float_as_uint(dt);
-        return true;
+        return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, t, cell, aux,
+                         clipped);
     };
     for (;;) {
         const bool want = !finished;
@@ -291,6 +320,316 @@ splat_kernel(const __grid_constant__ SplatParams P) {
         atomicAdd(P.stats + 1, (unsigned long long)steps);
         atomicAdd(P.stats + 2, (unsigned long long)clipped);
     }
+}
+
+// ---------------------------------------------------------------------------
+// training with splat semantics: record_powerfoam_splats_jacobians
+// (trace.rs:1421-1452) integrated like the walk's training contract
+// ---------------------------------------------------------------------------
+struct SplatTrainParams {
+    SplatParams base;           // traversal, density / SH tables, views
+    const float4 *geom;         // [N] model order: site, radius
+    const uint32_t *offsets;    // [N+1] CSR
+    const uint32_t *neighbors;  // [M] CSR neighbour ids
+    float max_dt;
+    uint32_t loss_kind;
+    float inv_count;            // 1 / (3 * rays of the whole call)
+    const float *target;        // [pixels][3] of this launch's views
+    float *rgb_out;             // [pixels][3] or null
+    float *loss;
+    RayState *ray_state;        // [pixels]
+    float *d_density, *d_sh;
+    float4 *d_site;             // [N] or null
+};
+
+// The Cech-row planes of one support for one lane (the per-ray order of
+// splat_clip_warp, from the same precomputed planes): entry / exit depths
+// before the sphere clip and the neighbours that set them (the cell itself
+// when no plane bounds that side).
+__device__ __forceinline__ void splat_planes_lane(const SplatTrainParams &TP, const WinRay &ray,
+                                                  uint32_t cell, float depth, float &face_near,
+                                                  float &face_far, uint32_t &prev,
+                                                  uint32_t &next) {
+    face_near = 0.0f;
+    face_far = depth;
+    prev = next = cell;
+    const uint32_t b = __ldg(TP.offsets + cell), e = __ldg(TP.offsets + cell + 1);
+    for (uint32_t k = b; k < e; ++k) {
+        const float4 fp = __ldg(&TP.base.row_faces[k].point);
+        const float4 fn = __ldg(&TP.base.row_faces[k].normal);
+        const float rx = fp.x - ray.ox, ry = fp.y - ray.oy, rz = fp.z - ray.oz;
+        const float num = dot3(rx, ry, rz, fn.x, fn.y, fn.z);
+        const float den = dot3(ray.dx, ray.dy, ray.dz, fn.x, fn.y, fn.z);
+        if (den > 1.0e-20f) {
+            const float t = num / den;
+            if (t < face_far) {
+                face_far = t;
+                next = __ldg(TP.neighbors + k);
+            }
+        } else if (den < -1.0e-20f) {
+            const float t = num / den;
+            if (t > face_near) {
+                face_near = t;
+                prev = __ldg(TP.neighbors + k);
+            }
+        }
+    }
+}
+
+template <int DEG, bool BF16>
+__global__ void __launch_bounds__(kSplatBlock)
+splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
+    const SplatParams &P = TP.base;
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((w & ~31u) >= P.total_work) return;
+    const SplatLane L = splat_lane(P, w);
+    const WinRay &ray = L.ray;
+    const float depth = L.vd->depth;
+    const size_t pix = (size_t)L.vd->pixel_begin + (size_t)L.y * L.vd->width + L.x;
+    float Ch[3] = {0.f, 0.f, 0.f}, Cl[3] = {0.f, 0.f, 0.f};
+    float T = 1.0f;
+    uint32_t steps = 0, clipped = 0, nodes_visited = 0, composited = 0;
+    bool cursor_valid = false, finished = !L.active;
+    float cur_t = 0.f;
+    uint32_t cur_cell = 0;
+    auto hit = [&](uint32_t p, bool mine, float limit, float &t, uint32_t &cell,
+                   uint32_t &aux) -> bool {
+        return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, t, cell, aux,
+                         clipped);
+    };
+    for (;;) {
+        const bool want = !finished;
+        if (!__any_sync(0xffffffffu, want)) break;
+        WinKey buf[kSplatWindow];
+        const int count = win_gather_warp<kSplatWindow, kSplatStack>(
+            P.nodes, ray, depth, want, cursor_valid, cur_t, cur_cell, buf, nodes_visited, hit);
+        if (!want) continue;
+#pragma unroll 1
+        for (int i = 0; i < count; ++i) {
+            const WinKey e = win_at(buf, i);
+            if (T <= P.weight_threshold || steps >= P.max_steps) {
+                finished = true;
+                break;
+            }
+            steps += 1;
+            const float dens = __ldg(P.m.density + e.idx) * 1.0f;
+            if (dens <= 1.0e-6f) continue;
+            const float dt = fminf(__uint_as_float(e.pos), TP.max_dt);
+            const float alpha = 1.0f - bv_expf(-dens * dt);
+            const float wgt = T * alpha;
+            float coef[ShDims<DEG>::N];
+            load_sh_row<DEG, BF16>(P.m, e.idx, coef);
+            float cu[3];
+            eval_sh<DEG>(coef, ray.dx, ray.dy, ray.dz, cu[0], cu[1], cu[2]);
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) acc_add(Ch[ch], Cl[ch], wgt * fmaxf(cu[ch], 0.f));
+            T = T * (1.0f - alpha);
+            composited += 1;
+        }
+        if (finished) continue;
+        if (count < kSplatWindow) {
+            finished = true;
+        } else {
+            cursor_valid = true;
+            cur_t = buf[kSplatWindow - 1].t;
+            cur_cell = buf[kSplatWindow - 1].idx;
+        }
+    }
+    // loss and dL/dC of the pixel (the walk's training epilogue)
+    float l = 0.f;
+    if (L.inside) {
+        const float *tg = TP.target + 3 * pix;
+        float gC[3];
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+            const float col = Ch[ch] + Cl[ch];
+            const float diff = col - __ldg(tg + ch);
+            if (TP.loss_kind == BV_LOSS_L2) {
+                l += diff * diff;
+                gC[ch] = 2.0f * diff * TP.inv_count;
+            } else {
+                l += fabsf(diff);
+                gC[ch] = (diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f)) * TP.inv_count;
+            }
+            if (TP.rgb_out) TP.rgb_out[3 * pix + ch] = col;
+        }
+        RayState st;
+        st.c_hi = make_float4(Ch[0], Ch[1], Ch[2], gC[0]);
+        st.c_lo = make_float4(Cl[0], Cl[1], Cl[2], gC[1]);
+        st.g = make_float4(gC[2], 0.f, 0.f, 0.f);
+        TP.ray_state[pix] = st;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31u) == 0 && l != 0.f) atomicAdd(TP.loss, l * TP.inv_count);
+    if (P.stats && L.active) {
+        atomicAdd(P.stats + 0, 1ull);
+        atomicAdd(P.stats + 1, (unsigned long long)composited);
+        atomicAdd(P.stats + 2, (unsigned long long)clipped);
+    }
+}
+
+// Replay: the same windows in the same order, recomputing T, w and colour,
+// the suffix S_{k+1} = C - P_k from the compensated prefix, and scattering
+//   dL/dsigma_k = dt_k sum_c g_c (T_{k+1} c_kc - S_{k+1,c})
+//   dL/dSH_kmc  = g_c w_k Y_m(d) [c_kc unclamped > 0]
+//   dL/ddt_k    = sigma_k sum_c g_c (T_{k+1} c_kc - S_{k+1,c})  -> sites, radii
+// through the interval's exact Jacobians (path_interval_jacobian of the
+// entry / exit neighbours, trace.rs:1199-1325).
+template <int DEG, bool BF16>
+__global__ void __launch_bounds__(kSplatBlock)
+splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
+    const SplatParams &P = TP.base;
+    constexpr int K = ShDims<DEG>::K;
+    constexpr int N = 3 * K;
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((w & ~31u) >= P.total_work) return;
+    const SplatLane L = splat_lane(P, w);
+    const WinRay &ray = L.ray;
+    const float depth = L.vd->depth;
+    const Ray r{ray.ox, ray.oy, ray.oz, ray.dx, ray.dy, ray.dz};
+    float Ch[3] = {0.f, 0.f, 0.f}, Cl[3] = {0.f, 0.f, 0.f}, gC[3] = {0.f, 0.f, 0.f};
+    if (L.active) {
+        const RayState st =
+            TP.ray_state[(size_t)L.vd->pixel_begin + (size_t)L.y * L.vd->width + L.x];
+        Ch[0] = st.c_hi.x;
+        Ch[1] = st.c_hi.y;
+        Ch[2] = st.c_hi.z;
+        Cl[0] = st.c_lo.x;
+        Cl[1] = st.c_lo.y;
+        Cl[2] = st.c_lo.z;
+        gC[0] = st.c_hi.w;
+        gC[1] = st.c_lo.w;
+        gC[2] = st.g.x;
+    }
+    float Ph[3] = {0.f, 0.f, 0.f}, Pl[3] = {0.f, 0.f, 0.f};
+    float Y[K];
+    sh_basis<DEG>(ray.dx, ray.dy, ray.dz, Y);
+    float T = 1.0f;
+    uint32_t steps = 0, clipped = 0, nodes_visited = 0;
+    bool cursor_valid = false;
+    bool finished = !L.active || (gC[0] == 0.f && gC[1] == 0.f && gC[2] == 0.f);
+    float cur_t = 0.f;
+    uint32_t cur_cell = 0;
+    auto hit = [&](uint32_t p, bool mine, float limit, float &t, uint32_t &cell,
+                   uint32_t &aux) -> bool {
+        return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, t, cell, aux,
+                         clipped);
+    };
+    for (;;) {
+        const bool want = !finished;
+        if (!__any_sync(0xffffffffu, want)) break;
+        WinKey buf[kSplatWindow];
+        const int count = win_gather_warp<kSplatWindow, kSplatStack>(
+            P.nodes, ray, depth, want, cursor_valid, cur_t, cur_cell, buf, nodes_visited, hit);
+        if (!want) continue;
+#pragma unroll 1
+        for (int i = 0; i < count; ++i) {
+            const WinKey e = win_at(buf, i);
+            if (T <= P.weight_threshold || steps >= P.max_steps) {
+                finished = true;
+                break;
+            }
+            steps += 1;
+            const uint32_t cell = e.idx;
+            const float dens = __ldg(P.m.density + cell) * 1.0f;
+            if (dens <= 1.0e-6f) continue;
+            const float dt_raw = __uint_as_float(e.pos);
+            const float dt = fminf(dt_raw, TP.max_dt);
+            const float alpha = 1.0f - bv_expf(-dens * dt);
+            const float wgt = T * alpha;
+            const float Tn = T * (1.0f - alpha);
+            float coef[ShDims<DEG>::N];
+            load_sh_row<DEG, BF16>(P.m, cell, coef);
+            float cu[3];
+            eval_sh<DEG>(coef, ray.dx, ray.dy, ray.dz, cu[0], cu[1], cu[2]);
+            float gs = 0.f, gw[3];
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) {
+                const float cc = fmaxf(cu[ch], 0.f);
+                acc_add(Ph[ch], Pl[ch], wgt * cc);
+                const float suffix = (Ch[ch] - Ph[ch]) + (Cl[ch] - Pl[ch]);
+                gs += gC[ch] * (Tn * cc - suffix);
+                gw[ch] = cu[ch] > 0.f ? gC[ch] * wgt : 0.f;
+            }
+            atomicAdd(TP.d_density + cell, dt * gs);
+            if (N % 4 == 0) {
+                float4 *row4 = reinterpret_cast<float4 *>(TP.d_sh + (size_t)cell * N);
+#pragma unroll
+                for (int q = 0; q < N / 4; ++q) {
+                    float v[4];
+#pragma unroll
+                    for (int h = 0; h < 4; ++h) v[h] = gw[(q * 4 + h) % 3] * Y[(q * 4 + h) / 3];
+                    atomicAdd(row4 + q, make_float4(v[0], v[1], v[2], v[3]));
+                }
+            } else {
+                float *row = TP.d_sh + (size_t)cell * N;
+#pragma unroll
+                for (int m = 0; m < N; ++m) {
+                    const float v = gw[m % 3] * Y[m / 3];
+                    if (v != 0.0f) atomicAdd(row + m, v);
+                }
+            }
+            if (TP.d_site && dt_raw < TP.max_dt) {
+                float face_near, face_far;
+                uint32_t prev, next;
+                splat_planes_lane(TP, ray, cell, depth, face_near, face_far, prev, next);
+                const float4 g = __ldg(TP.geom + cell);
+                Cell c;
+                c.id = cell;
+                c.x = g.x;
+                c.y = g.y;
+                c.z = g.z;
+                c.r = g.w;
+                c.density = dens;
+                Interval iv;
+                record_interval<true>(r, c, face_near, face_far, iv);
+                const float4 pp = __ldg(TP.geom + prev), np = __ldg(TP.geom + next);
+                const Jacobians J =
+                    interval_jacobians(r, iv, prev, pp, c, next != cell, np, face_near, face_far);
+                const float gdt = dens * gs;
+                scatter_site(TP.d_site, cell, gdt, J.jc);
+                if (prev != cell && !iv.start_sphere) scatter_site(TP.d_site, prev, gdt, J.jp);
+                if (next != cell && !iv.end_sphere) scatter_site(TP.d_site, next, gdt, J.jn);
+            }
+            T = Tn;
+        }
+        if (finished) continue;
+        if (count < kSplatWindow) {
+            finished = true;
+        } else {
+            cursor_valid = true;
+            cur_t = buf[kSplatWindow - 1].t;
+            cur_cell = buf[kSplatWindow - 1].idx;
+        }
+    }
+}
+
+#define BV_SPLAT_SELECT(KERNEL, PARAMS, DEGREE, BF, BLOCKS, STREAM)                       \
+    do {                                                                                  \
+        switch ((int)(DEGREE) * 2 + ((BF) ? 1 : 0)) {                                     \
+            case 0: KERNEL<0, false><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;  \
+            case 1: KERNEL<0, true><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;   \
+            case 2: KERNEL<1, false><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;  \
+            case 3: KERNEL<1, true><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;   \
+            case 4: KERNEL<2, false><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;  \
+            case 5: KERNEL<2, true><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;   \
+            case 6: KERNEL<3, false><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;  \
+            case 7: KERNEL<3, true><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;   \
+            default: return cudaErrorInvalidValue;                                        \
+        }                                                                                 \
+    } while (0)
+
+cudaError_t launch_splat_train(const SplatTrainParams &p, bool backward, cudaStream_t s) {
+    const int blocks = (int)((p.base.total_work + kSplatBlock - 1) / kSplatBlock);
+    if (blocks == 0) return cudaSuccess;
+    if (backward)
+        BV_SPLAT_SELECT(splat_train_backward_kernel, p, p.base.m.sh_degree, p.base.m.sh_bf16,
+                        blocks, s);
+    else
+        BV_SPLAT_SELECT(splat_train_forward_kernel, p, p.base.m.sh_degree, p.base.m.sh_bf16,
+                        blocks, s);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_splat(const SplatParams &p, cudaStream_t s) {
@@ -349,7 +688,14 @@ struct bv_splat_tracer {
     SplatPrim *prims = nullptr;
     BvhNode *nodes = nullptr;
     SplatFace *row_faces = nullptr;
+    float4 *geom = nullptr;          // [N] model order (training Jacobians)
+    uint32_t *offsets = nullptr;     // [N+1] CSR
+    uint32_t *neighbors = nullptr;   // [M] CSR
     float *density = nullptr;
+    // training scratch
+    RayState *ray_state = nullptr;
+    size_t ray_state_capacity = 0;
+    float4 *site_grads = nullptr;    // [N], kept zero between calls
     void *sh = nullptr;
     unsigned long long *stats = nullptr;
     uint32_t *max_candidates = nullptr;
@@ -383,6 +729,11 @@ void free_splat(bv_splat_tracer *t) {
     cudaFree(t->prims);
     cudaFree(t->nodes);
     cudaFree(t->row_faces);
+    cudaFree(t->geom);
+    cudaFree(t->offsets);
+    cudaFree(t->neighbors);
+    cudaFree(t->ray_state);
+    cudaFree(t->site_grads);
     cudaFree(t->density);
     cudaFree(t->sh);
     cudaFree(t->stats);
@@ -504,7 +855,12 @@ bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *md, const bv_trace_
         }
     }
     std::vector<float> dens(n);
-    for (uint32_t i = 0; i < n; ++i) dens[i] = md->points[4 * (size_t)i + 3];
+    std::vector<float4> geom(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *p = md->points + 4 * (size_t)i;
+        dens[i] = p[3];
+        geom[i] = make_float4(p[0], p[1], p[2], md->radii[i]);
+    }
 
     bv_splat_tracer *t = new bv_splat_tracer();
     t->n = n;
@@ -538,6 +894,19 @@ bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *md, const bv_trace_
     SP_TRY(cudaMemcpy(t->row_faces, rows.data(), sizeof(SplatFace) * rows.size(), cudaMemcpyHostToDevice),
            "upload rows");
     SP_TRY(cudaMemcpy(t->density, dens.data(), sizeof(float) * n, cudaMemcpyHostToDevice), "upload density");
+    SP_TRY(cudaMalloc(&t->geom, sizeof(float4) * n), "cudaMalloc sites");
+    SP_TRY(cudaMalloc(&t->offsets, sizeof(uint32_t) * (n + 1)), "cudaMalloc offsets");
+    SP_TRY(cudaMalloc(&t->neighbors, sizeof(uint32_t) * std::max<uint32_t>(m_edges, 1)),
+           "cudaMalloc neighbours");
+    SP_TRY(cudaMalloc(&t->site_grads, sizeof(float4) * n), "cudaMalloc site grads");
+    SP_TRY(cudaMemset(t->site_grads, 0, sizeof(float4) * n), "memset site grads");
+    SP_TRY(cudaMemcpy(t->geom, geom.data(), sizeof(float4) * n, cudaMemcpyHostToDevice),
+           "upload sites");
+    SP_TRY(cudaMemcpy(t->offsets, md->adjacency_offsets, sizeof(uint32_t) * (n + 1),
+                      cudaMemcpyHostToDevice), "upload offsets");
+    if (m_edges)
+        SP_TRY(cudaMemcpy(t->neighbors, md->adjacency_neighbors, sizeof(uint32_t) * m_edges,
+                          cudaMemcpyHostToDevice), "upload neighbours");
     if (bf16) {
         std::vector<uint16_t> row((size_t)n * stride, 0);
         for (uint32_t i = 0; i < n; ++i)
@@ -672,6 +1041,92 @@ bv_status bv_powerfoam_splat_tracer_last_stats(bv_splat_tracer *t, bv_launch_sta
     out->rays = h[0];
     out->steps = h[1];
     out->faces = h[2];
+    return BV_OK;
+}
+
+bv_status bv_powerfoam_splat_tracer_forward_backward(
+    bv_splat_tracer *t, const bv_camera *cams, uint32_t n_cams, uint32_t width, uint32_t height,
+    const float *target, const bv_train_settings *ts, const bv_grads *grads, float *loss,
+    float *rgb_out, bv_stream stream) {
+    if (!t || !cams || !target || !ts || !grads || !loss)
+        return sp_fail(BV_ERR_INVALID_ARGUMENT, "null argument");
+    if (!grads->d_density_dev || !grads->d_sh_dev)
+        return sp_fail(BV_ERR_INVALID_ARGUMENT, "density and SH gradient tables are required");
+    if (width == 0 || height == 0 || n_cams == 0)
+        return sp_fail(BV_ERR_INVALID_ARGUMENT, "render size must be non-zero");
+    if (ts->loss != BV_LOSS_L2 && ts->loss != BV_LOSS_L1)
+        return sp_fail(BV_ERR_INVALID_ARGUMENT, "unknown loss %u", ts->loss);
+    if (!(ts->max_dt > 0.0f)) return sp_fail(BV_ERR_INVALID_ARGUMENT, "max_dt must be positive");
+    if (ts->max_steps == 0) return sp_fail(BV_ERR_INVALID_ARGUMENT, "max_steps must be non-zero");
+    const uint32_t nsh = 3 * (t->sh_degree + 1) * (t->sh_degree + 1);
+    if ((nsh % 4) == 0 && (reinterpret_cast<uintptr_t>(grads->d_sh_dev) & 15u) != 0)
+        return sp_fail(BV_ERR_INVALID_ARGUMENT, "d_sh table must be 16-byte aligned");
+    const uint64_t chunk_rays = (uint64_t)std::min<uint32_t>(n_cams, kMaxViewsPerLaunch) * width * height;
+    if (chunk_rays >= (1ull << 31)) return sp_fail(BV_ERR_INVALID_ARGUMENT, "batch too large");
+    for (uint32_t i = 0; i < n_cams; ++i) {
+        bv_status st = validate_camera(cams[i]);
+        if (st != BV_OK) return st;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (chunk_rays > t->ray_state_capacity) {
+        cudaFree(t->ray_state);
+        t->ray_state = nullptr;
+        t->ray_state_capacity = 0;
+        SP_CUDA(cudaMalloc(&t->ray_state, sizeof(RayState) * chunk_rays), "cudaMalloc ray state");
+        t->ray_state_capacity = chunk_rays;
+    }
+    t->last_launches = 0;
+    t->last_has_stats = t->stats_enabled;
+    if (t->stats_enabled) {
+        SP_CUDA(cudaMemsetAsync(t->stats, 0, sizeof(unsigned long long) * 4, s), "stats reset");
+        SP_CUDA(cudaEventRecord(t->ev[0], s), "event");
+    }
+    SP_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), s), "loss reset");
+    const bool want_site = grads->d_positions_dev || grads->d_radii_dev;
+    const double total_rays = (double)n_cams * width * height;
+    for (uint32_t c0 = 0; c0 < n_cams; c0 += kMaxViewsPerLaunch) {
+        const uint32_t nc = std::min<uint32_t>(kMaxViewsPerLaunch, n_cams - c0);
+        SplatTrainParams p;
+        std::memset(&p, 0, sizeof(p));
+        p.base.m = t->model();
+        p.base.prims = t->prims;
+        p.base.nodes = t->nodes;
+        p.base.row_faces = t->row_faces;
+        p.base.max_steps = ts->max_steps;
+        p.base.weight_threshold = ts->weight_threshold;
+        p.base.n_views = nc;
+        uint32_t work = 0;
+        for (uint32_t v = 0; v < nc; ++v) {
+            p.base.views[v] = view_desc(cams[c0 + v], width, height, work, (uint64_t)v * width * height);
+            work += tile_padded_rays(width, height);
+        }
+        p.base.total_work = work;
+        p.base.stats = t->stats_enabled ? t->stats : nullptr;
+        const size_t off = (size_t)c0 * width * height;
+        p.geom = t->geom;
+        p.offsets = t->offsets;
+        p.neighbors = t->neighbors;
+        p.max_dt = ts->max_dt;
+        p.loss_kind = ts->loss;
+        p.inv_count = (float)(1.0 / (3.0 * total_rays));
+        p.target = target + 3 * off;
+        p.rgb_out = rgb_out ? rgb_out + 3 * off : nullptr;
+        p.loss = loss;
+        p.ray_state = t->ray_state;
+        p.d_density = grads->d_density_dev;
+        p.d_sh = grads->d_sh_dev;
+        p.d_site = want_site ? t->site_grads : nullptr;
+        SP_CUDA(launch_splat_train(p, false, s), "splat training forward launch");
+        p.base.stats = nullptr;
+        SP_CUDA(launch_splat_train(p, true, s), "splat training backward launch");
+        t->last_launches += 2;
+    }
+    if (want_site) {
+        SP_CUDA(launch_fold_site_grads(t->site_grads, t->n, grads->d_positions_dev,
+                                       grads->d_radii_dev, s), "site gradient fold");
+        t->last_launches += 1;
+    }
+    if (t->stats_enabled) SP_CUDA(cudaEventRecord(t->ev[1], s), "event");
     return BV_OK;
 }
 

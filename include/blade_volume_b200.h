@@ -381,6 +381,20 @@ bv_status bv_powerfoam_splat_tracer_set_weight_threshold(bv_splat_tracer *tracer
  * counting re-clips in later windows) of the last dispatch */
 bv_status bv_powerfoam_splat_tracer_enable_stats(bv_splat_tracer *tracer, uint32_t enabled);
 bv_status bv_powerfoam_splat_tracer_last_stats(bv_splat_tracer *tracer, bv_launch_stats *out);
+/* Forward + loss + backward with splat semantics: the training recorder's
+ * PowerFoam splats (record_powerfoam_splats_jacobians, trace.rs:1421-1452;
+ * path_record.rs:1107-1218 on the GPU) integrated and differentiated under
+ * the same contract as bv_forward_backward: the sorted support intervals of
+ * every ray, truncated to settings->max_steps and cut at
+ * settings->weight_threshold, dt clamped to max_dt, L2/L1 loss; density,
+ * SH, site-position and radius gradients (through each interval's exact
+ * Jacobians w.r.t. the entry / exit neighbours and the support sphere)
+ * accumulate into the caller's tables.  Same arguments as
+ * bv_forward_backward. */
+bv_status bv_powerfoam_splat_tracer_forward_backward(
+    bv_splat_tracer *tracer, const bv_camera *cameras, uint32_t n_cameras, uint32_t width,
+    uint32_t height, const float *target_rgb_dev, const bv_train_settings *settings,
+    const bv_grads *grads, float *loss_dev, float *rgb_out_dev, bv_stream stream);
 
 /* ---- Gaussian ray tracing with SH colour ---------------------------------
  * GaussianGpuCloud (blade-volume/src/gpu/gaussian.rs:94-280) and its draw

@@ -674,8 +674,14 @@ void bvo_record_image(const bvo_model *m, const bvo_camera *cams, uint32_t n_cam
 /* ------------------------------------------------------------------ */
 /* PowerFoam splats (trace.rs:1327-1546)                               */
 /* ------------------------------------------------------------------ */
-static int powerfoam_splat_interval(const bvo_model *m, const float o[3], const float d[3],
-                                    float depth, uint32_t cell, bvo_path_entry *e) {
+/* The Cech-row clip of one support (trace.rs:1331-1385) before the sphere
+ * clip: the entry / exit plane depths and the neighbours that set them
+ * (the cell itself when no plane bounds that side).  0 when the support is
+ * excluded (camera within 4 r), missed, outside (0, depth) or emptied by a
+ * parallel face. */
+static int splat_planes(const bvo_model *m, const float o[3], const float d[3], float depth,
+                        uint32_t cell, float *near_out, float *far_out, uint32_t *prev_out,
+                        uint32_t *next_out) {
     const float *cpp = m->points + 4 * (size_t)cell;
     const float cur[3] = {cpp[0], cpp[1], cpp[2]};
     const float cr = read_radius(m, cell);
@@ -714,6 +720,19 @@ static int powerfoam_splat_interval(const bvo_model *m, const float o[3], const 
             return 0;
         }
     }
+    *near_out = face_near;
+    *far_out = face_far;
+    *prev_out = previous;
+    *next_out = next;
+    return 1;
+}
+
+/* powerfoam_splat_interval (trace.rs:1331-1389). */
+static int powerfoam_splat_interval(const bvo_model *m, const float o[3], const float d[3],
+                                    float depth, uint32_t cell, bvo_path_entry *e) {
+    float face_near, face_far;
+    uint32_t previous, next;
+    if (!splat_planes(m, o, d, depth, cell, &face_near, &face_far, &previous, &next)) return 0;
     return path_interval_jacobian(m, o, d, 1, previous, cell, next, face_near, face_far, e);
 }
 
@@ -979,6 +998,68 @@ static int record_training_walk(const bvo_model *m, const float o[3], const floa
     return count;
 }
 
+/* Recorded PowerFoam splats of the training contract: the sorted intervals
+ * of record_powerfoam_splats_jacobians (trace.rs:1421-1452), truncated to
+ * max_steps, integrated like the walk (dt clamped to max_dt, the FP32
+ * transmittance cut).  Each segment carries the entry / exit neighbours and
+ * roles that path_interval_jacobian differentiates.  Identical, operation
+ * for operation, to the device splat fwd+bwd. */
+static int record_training_splats(const bvo_model *m, const float o[3], const float d[3],
+                                  uint32_t max_steps, float depth, float thr, float max_dt,
+                                  seg_t *segs, float rgb32[3]) {
+    float ch[3] = {0.0f, 0.0f, 0.0f}, cl[3] = {0.0f, 0.0f, 0.0f};
+    float T = 1.0f;
+    bvo_path_entry *ents = NULL;
+    const int n = sorted_splats(m, o, d, depth, max_steps, &ents);
+    int count = 0;
+    for (int k = 0; k < n; ++k) {
+        if (T <= thr) break;
+        const uint32_t cell = ents[k].cell;
+        float face_near, face_far;
+        uint32_t previous, next;
+        splat_planes(m, o, d, depth, cell, &face_near, &face_far, &previous, &next);
+        const float *cpp = m->points + 4 * (size_t)cell;
+        const float cp[3] = {cpp[0], cpp[1], cpp[2]};
+        float sn, sf;
+        sphere_jac(o, d, cp, read_radius(m, cell), &sn, &sf, NULL, NULL);
+        float start_t = face_near, end_t = face_far;
+        uint8_t srole = previous != cell ? ROLE_FACE : ROLE_FIXED;
+        uint8_t erole = next != cell ? ROLE_FACE : ROLE_FIXED;
+        if (sn > start_t) {
+            start_t = sn;
+            srole = ROLE_SPHERE;
+        }
+        if (sf < end_t) {
+            end_t = sf;
+            erole = ROLE_SPHERE;
+        }
+        seg_t sg = {previous, cell, next, srole, erole, start_t, end_t,
+                    {0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+        memcpy(sg.jp32, ents[k].dt_d_previous, 16);
+        memcpy(sg.jc32, ents[k].dt_d_current, 16);
+        memcpy(sg.jn32, ents[k].dt_d_next, 16);
+        segs[count++] = sg;
+        const float dens = m->points[4 * (size_t)cell + 3];
+        if (dens > 1e-6f) {
+            const float dt = fminf(end_t - start_t, max_dt);
+            const float alpha = 1.0f - bvo_expf(-dens * dt);
+            const float w = T * alpha;
+            float c[3];
+            bvo_eval_rgb_sh(m, cell, d, c, NULL);
+            for (int ch_i = 0; ch_i < 3; ++ch_i) {
+                float sum, err;
+                two_sum_f(ch[ch_i], w * c[ch_i], &sum, &err);
+                ch[ch_i] = sum;
+                cl[ch_i] = cl[ch_i] + err;
+            }
+            T = T * (1.0f - alpha);
+        }
+    }
+    free(ents);
+    for (int i = 0; i < 3; ++i) rgb32[i] = ch[i] + cl[i];
+    return count;
+}
+
 typedef struct {
     const double *pts; /* [n*4] */
     const double *sh;  /* [n*3K] */
@@ -1098,6 +1179,18 @@ double bvo_forward_backward(const bvo_model *m, const bvo_camera *cams, uint32_t
                             int loss_kind, const bvo_params_f64 *override_params,
                             double *out_rgb, float *out_rgb32, double *d_density, double *d_sh,
                             double *d_pos, double *d_radius, int threads) {
+    return bvo_forward_backward_ex(m, cams, n_cams, width, height, max_steps, weight_threshold,
+                                   max_dt, target, loss_kind, override_params, out_rgb,
+                                   out_rgb32, d_density, d_sh, d_pos, d_radius, threads, 0);
+}
+
+double bvo_forward_backward_ex(const bvo_model *m, const bvo_camera *cams, uint32_t n_cams,
+                               uint32_t width, uint32_t height, uint32_t max_steps,
+                               float weight_threshold, float max_dt, const float *target,
+                               int loss_kind, const bvo_params_f64 *override_params,
+                               double *out_rgb, float *out_rgb32, double *d_density,
+                               double *d_sh, double *d_pos, double *d_radius, int threads,
+                               int splats) {
     const uint32_t deg = m->sh_degree > 3 ? 3 : m->sh_degree;
     const uint32_t K = sh_comps(deg);
     /* FP64 parameter view */
@@ -1151,8 +1244,11 @@ double bvo_forward_backward(const bvo_model *m, const bvo_camera *cams, uint32_t
                 d[0] = dn[0];
                 d[1] = dn[1];
                 d[2] = dn[2];
-                nseg = record_training_walk(m, of, dn, starts[v], max_steps, cams[v].depth,
-                                            weight_threshold, max_dt, segs, rgb32);
+                nseg = splats ? record_training_splats(m, of, dn, max_steps, cams[v].depth,
+                                                       weight_threshold, max_dt, segs, rgb32)
+                              : record_training_walk(m, of, dn, starts[v], max_steps,
+                                                     cams[v].depth, weight_threshold, max_dt,
+                                                     segs, rgb32);
             }
             if (out_rgb32)
                 for (int ch = 0; ch < 3; ++ch) out_rgb32[3 * (size_t)i + ch] = rgb32[ch];

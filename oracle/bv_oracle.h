@@ -175,6 +175,17 @@ double bvo_forward_backward(const bvo_model *m, const bvo_camera *cams, uint32_t
                             int loss_kind, const bvo_params_f64 *override_params,
                             double *out_rgb, float *out_rgb32, double *d_density, double *d_sh,
                             double *d_pos, double *d_radius, int threads);
+/* splats != 0: PowerFoam splat semantics (record_powerfoam_splats_jacobians,
+ * trace.rs:1421-1452) instead of the walk: the sorted support intervals of
+ * every ray, truncated to max_steps, with the same integration and
+ * gradients (the model must carry radii). */
+double bvo_forward_backward_ex(const bvo_model *m, const bvo_camera *cams, uint32_t n_cams,
+                               uint32_t width, uint32_t height, uint32_t max_steps,
+                               float weight_threshold, float max_dt, const float *target,
+                               int loss_kind, const bvo_params_f64 *override_params,
+                               double *out_rgb, float *out_rgb32, double *d_density,
+                               double *d_sh, double *d_pos, double *d_radius, int threads,
+                               int splats);
 
 /* ---- relightable Gaussians with finite point lights ----
  * blade-volume/shaders/relight.wgsl (kernel 2 = learned volumetric

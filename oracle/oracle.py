@@ -143,6 +143,8 @@ def lib():
                                            C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
                                            C.c_float, f32p, C.c_int, C.POINTER(ParamsF64), f64p,
                                            f32p, f64p, f64p, f64p, f64p, C.c_int]
+        L.bvo_forward_backward_ex.restype = C.c_double
+        L.bvo_forward_backward_ex.argtypes = L.bvo_forward_backward.argtypes + [C.c_int]
         L.bvo_logf.restype = C.c_float
         L.bvo_logf.argtypes = [C.c_float]
         L.bvo_powf.restype = C.c_float
@@ -397,9 +399,10 @@ def render_splats(model: OracleModel, cam, width, height, max_steps=1024, weight
 
 def forward_backward(model: OracleModel, cams: Sequence, width, height, max_steps=1024,
                      weight_threshold=0.0, max_dt=50.0, target=None, loss_kind=0,
-                     override=None, want_grads=True, threads=0):
+                     override=None, want_grads=True, threads=0, splats=False):
     """FP64 training-contract oracle.  Returns dict(loss, rgb, d_density,
-    d_sh, d_pos, d_radius)."""
+    d_sh, d_pos, d_radius).  splats: PowerFoam splat semantics instead of the
+    walk."""
     n = model.n
     K3 = model.sh.size // max(n, 1)
     cam_arr = (Camera * len(cams))(*[camera_struct(c) for c in cams])
@@ -421,11 +424,11 @@ def forward_backward(model: OracleModel, cams: Sequence, width, height, max_step
         rad = None if rad is None else np.ascontiguousarray(rad, dtype=np.float64)
         keep = [pts, sh, rad]
         ov = ParamsF64(_ptr(pts, f64p), _ptr(sh, f64p), _ptr(rad, f64p))
-    loss = lib().bvo_forward_backward(
+    loss = lib().bvo_forward_backward_ex(
         C.byref(model.c), cam_arr, len(cams), width, height, max_steps, weight_threshold,
         max_dt, _ptr(tgt, f32p), loss_kind, C.byref(ov) if ov is not None else None,
         _ptr(rgb, f64p), _ptr(rgb32, f32p), _ptr(dd, f64p), _ptr(dsh, f64p), _ptr(dpos, f64p),
-        _ptr(drad, f64p), threads)
+        _ptr(drad, f64p), threads, int(splats))
     del keep
     return dict(loss=loss, rgb=rgb, rgb32=rgb32, d_density=dd, d_sh=dsh,
                 d_pos=None if dpos is None else dpos.reshape(n, 3), d_radius=drad)

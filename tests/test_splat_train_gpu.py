@@ -1,0 +1,81 @@
+"""PowerFoam training with splat semantics
+(bv_powerfoam_splat_tracer_forward_backward) against the FP64 oracle.
+
+The oracle records each ray's sorted support intervals as
+record_powerfoam_splats_jacobians does (trace.rs:1421-1452) and evaluates the
+training contract on them in FP64 (its gradients are pinned by central
+differences in tests/test_train_oracle.py).  Bar, as for the walk: forward
+colours bit-exact against the oracle's FP32 restatement, the loss within
+1e-5 relative, every gradient table within 1e-4 of the oracle relative to the
+table's largest entry.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import blade_volume_b200 as bv  # noqa: E402
+from blade_volume_b200 import scenes  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+from tests.test_train_gpu import assert_table  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+W = H = 40
+
+
+def case(seed=3, n=4096, bf16=False, radius_max=0.1):
+    m = scenes.powerfoam_mixture(n, seed=seed, radius_max=radius_max, bf16=bf16)
+    cams = scenes.sphere_cameras(3, 3.0, seed + 1, math.radians(55.0), 1.0, 100.0)
+    target = np.random.default_rng(seed).random((3, H, W, 3)).astype(np.float32)
+    return m, cams, target
+
+
+def run_gpu(m, cams, target, repeat=1, **kw):
+    t = bv.PowerFoamSplatTracer(m)
+    grads = t.new_grads()
+    tg = torch.from_numpy(target).cuda()
+    rgb = torch.zeros((len(cams), H, W, 3), dtype=torch.float32, device="cuda")
+    loss_out = None
+    for _ in range(repeat):
+        loss_out = t.forward_backward(cams, W, H, tg, grads, rgb_out=rgb, **kw)
+    torch.cuda.synchronize()
+    out = {k: v.cpu().numpy().astype(np.float64) for k, v in grads.items()}
+    out["loss"] = float(loss_out.item())
+    out["rgb"] = rgb.cpu().numpy()
+    t.deinit()
+    return out
+
+
+@pytest.mark.parametrize("bf16,radius_max", [(False, 0.1), (True, 0.1), (False, 0.03)])
+def test_splat_gradients_match_fp64_oracle(bf16, radius_max):
+    m, cams, target = case(bf16=bf16, radius_max=radius_max)
+    g = run_gpu(m, cams, target)
+    om = O.OracleModel.from_scene(m)
+    ref = O.forward_backward(om, cams, W, H, target=target, splats=True)
+    assert abs(g["loss"] - ref["loss"]) <= 1e-5 * ref["loss"]
+    assert np.array_equal(g["rgb"].view(np.uint32), ref["rgb32"].view(np.uint32))
+    for k, name in (("d_density", "density"), ("d_sh", "sh"), ("d_radius", "radius")):
+        assert_table(name, g[k], ref[k])
+    assert_table("pos", g["d_pos"].reshape(-1, 3), ref["d_pos"])
+
+
+def test_splat_training_settings_and_accumulation():
+    m, cams, target = case(seed=6, n=2048)
+    om = O.OracleModel.from_scene(m)
+    for loss, max_dt, thr, steps in [(bv.LOSS_L1, 50.0, 0.0, 1024), (bv.LOSS_L2, 0.01, 0.0, 1024),
+                                     (bv.LOSS_L2, 50.0, 1e-2, 1024), (bv.LOSS_L2, 50.0, 0.0, 3)]:
+        g = run_gpu(m, cams, target, loss=loss, max_dt=max_dt, weight_threshold=thr,
+                    max_steps=steps)
+        ref = O.forward_backward(om, cams, W, H, target=target, loss_kind=loss, max_dt=max_dt,
+                                 weight_threshold=thr, max_steps=steps, splats=True)
+        assert abs(g["loss"] - ref["loss"]) <= 1e-5 * ref["loss"], (loss, max_dt, thr, steps)
+        assert_table("density", g["d_density"], ref["d_density"])
+        assert_table("sh", g["d_sh"], ref["d_sh"])
+    once = run_gpu(m, cams, target)
+    twice = run_gpu(m, cams, target, repeat=2)
+    for k in ("d_density", "d_sh", "d_pos", "d_radius"):
+        assert_table(k, twice[k], 2.0 * once[k], tol=1e-5)

@@ -24,15 +24,18 @@ def small_case(seed=3, n=1024, radii=False):
     return m, cams, target
 
 
-def loss_at(om, cams, target, pts, sh, rad, max_dt, loss_kind):
+def loss_at(om, cams, target, pts, sh, rad, max_dt, loss_kind, splats=False):
     r = O.forward_backward(om, cams, 20, 20, max_dt=max_dt, target=target, loss_kind=loss_kind,
-                           override=(pts, sh, rad), want_grads=False, threads=4)
+                           override=(pts, sh, rad), want_grads=False, threads=4, splats=splats)
     return r["loss"]
 
 
-@pytest.mark.parametrize("radii,loss_kind,max_dt", [(False, 0, 50.0), (True, 0, 50.0),
-                                                    (False, 1, 50.0), (False, 0, 0.05)])
-def test_oracle_gradient_matches_central_differences(radii, loss_kind, max_dt):
+@pytest.mark.parametrize("radii,loss_kind,max_dt,splats", [
+    (False, 0, 50.0, False), (True, 0, 50.0, False), (False, 1, 50.0, False),
+    (False, 0, 0.05, False),
+    # PowerFoam splat semantics (record_powerfoam_splats_jacobians, trace.rs:1421)
+    (True, 0, 50.0, True)])
+def test_oracle_gradient_matches_central_differences(radii, loss_kind, max_dt, splats):
     m, cams, target = small_case(radii=radii)
     om = O.OracleModel.from_scene(m)
     pts = m.points.astype(np.float64)
@@ -41,7 +44,7 @@ def test_oracle_gradient_matches_central_differences(radii, loss_kind, max_dt):
     # FP64 parameters given explicitly: every segment length and Jacobian is
     # then derived in FP64, the same function the differences perturb
     g = O.forward_backward(om, cams, 20, 20, max_dt=max_dt, target=target, loss_kind=loss_kind,
-                           override=(pts, sh, rad), threads=4)
+                           override=(pts, sh, rad), threads=4, splats=splats)
     rng = np.random.default_rng(0)
     checks = []
     tables = [("density", g["d_density"]), ("sh", g["d_sh"]), ("pos", g["d_pos"].reshape(-1))]
@@ -53,6 +56,7 @@ def test_oracle_gradient_matches_central_differences(radii, loss_kind, max_dt):
             continue  # L1's kink makes position FD noisy; density/SH are checked
         for idx in rng.choice(nz, size=min(6, len(nz)), replace=False):
             checks.append((name, int(idx), float(tab[idx])))
+    assert len(checks) >= 12
     eps = 1e-7
     for name, idx, analytic in checks:
         def perturbed(delta):
@@ -65,7 +69,7 @@ def test_oracle_gradient_matches_central_differences(radii, loss_kind, max_dt):
                 p[idx // 3, idx % 3] += delta
             else:
                 r[idx] += delta
-            return loss_at(om, cams, target, p, s, r, max_dt, loss_kind)
+            return loss_at(om, cams, target, p, s, r, max_dt, loss_kind, splats)
         lp, lm = perturbed(eps), perturbed(-eps)
         fd = (lp - lm) / (2 * eps)
         scale = max(abs(fd), abs(analytic))
