@@ -154,7 +154,9 @@ __global__ void __launch_bounds__(kGaussBlock, BV_MINB_GAUSS) gaussian_kernel(co
     bool cursor_valid = false, finished = !active;
     float cur_t = 0.f;
     uint32_t cur_idx = 0, hits_used = 0, nodes_visited = 0;
-    auto hit = [&](uint32_t p, bool mine, float, float &t, uint32_t &id, uint32_t &) -> bool {
+    auto hit = [&](uint32_t p, bool mine, float, WinKey &k) -> bool {
+        float &t = k.t;
+        uint32_t &id = k.idx;
         float a;
         if (!mine || !response(P, p, ray, t, a)) return false;
         id = __ldg(&P.ids[p]);

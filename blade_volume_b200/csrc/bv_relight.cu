@@ -163,7 +163,9 @@ relight_kernel(const __grid_constant__ RelightParams P) {
     float cur_t = 0.f;
     uint32_t cur_idx = 0;
     uint32_t hits_used = 0, nodes_visited = 0;
-    auto hit = [&](uint32_t p, bool mine, float, float &t, uint32_t &id, uint32_t &) -> bool {
+    auto hit = [&](uint32_t p, bool mine, float, WinKey &k) -> bool {
+        float &t = k.t;
+        uint32_t &id = k.idx;
         float a;
         if (!mine || !intersect(P.prims, p, ray, t_end, t, a) || !(a > 0.0f)) return false;
         id = __ldg(&P.prims[p].ids.x);

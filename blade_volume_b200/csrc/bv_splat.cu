@@ -37,6 +37,9 @@ namespace {
 constexpr int kSplatBlock = 128;
 constexpr int kSplatWindow = 16;
 constexpr int kSplatStack = 80;  // > BVH depth, checked at tracer creation
+// Entry / exit plane of an interval as an offset in its Cech row (16 bits
+// each in the key; rows are at most 65,534 entries, checked at creation).
+constexpr uint32_t kNoPlane = 0xffffu;
 
 // One support sphere in BVH leaf order, 32 B.
 struct __align__(16) SplatPrim {
@@ -107,9 +110,10 @@ __device__ __forceinline__ bool splat_sphere(const WinRay &ray, const float4 &s,
 __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinRay &ray,
                                                 uint32_t begin, uint32_t end, float depth,
                                                 float sn, float sf, bool need, float &start,
-                                                float &dt) {
+                                                float &dt, uint32_t &links) {
     const uint32_t lane = threadIdx.x & 31u;
     float face_near = 0.0f, face_far = depth;
+    uint32_t near_k = kNoPlane, far_k = kNoPlane;
     bool empty = !need;
     for (uint32_t base = begin; base < end; base += 32u) {
         if (!__any_sync(0xffffffffu, !empty)) break;
@@ -132,10 +136,16 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
             const float den = dot3(ray.dx, ray.dy, ray.dz, nx, ny, nz);
             if (den > 1.0e-20f) {
                 const float t = num / den;
-                if (t < face_far) face_far = t;
+                if (t < face_far) {
+                    face_far = t;
+                    far_k = base + j - begin;
+                }
             } else if (den < -1.0e-20f) {
                 const float t = num / den;
-                if (t > face_near) face_near = t;
+                if (t > face_near) {
+                    face_near = t;
+                    near_k = base + j - begin;
+                }
             } else if (num < 0.0f) {
                 empty = true;
             }
@@ -151,17 +161,22 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
     if (en <= st || !isfinite(st) || !isfinite(en)) return false;
     start = st;
     dt = en - st;
+    links = near_k | (far_k << 16);
     return true;
 }
 
 // Window candidate test of support p for win_gather_warp (every lane calls
 // it): the sphere test per lane, then the warp clips the support's Cech row
 // for the lanes whose sphere interval can still enter their window; the key
-// is (clipped entry depth, cell) and aux carries the interval length.
+// is (clipped entry depth, cell), pos carries the interval length and a
+// WinKey2's aux the row offsets of its entry / exit planes.
+__device__ __forceinline__ void set_links(WinKey &, uint32_t) {}
+__device__ __forceinline__ void set_links(WinKey2 &k, uint32_t links) { k.aux = links; }
+
+template <class Key>
 __device__ __forceinline__ bool splat_hit(const SplatParams &P, const WinRay &ray, float depth,
                                           bool cursor_valid, float cur_t, uint32_t p, bool mine,
-                                          float limit, float &t, uint32_t &cell, uint32_t &aux,
-                                          uint32_t &clipped) {
+                                          float limit, Key &k, uint32_t &clipped) {
     const float4 s = __ldg(&P.prims[p].site);
     float sn = 0.f, sf = 0.f;
     bool need = mine && splat_sphere(ray, s, depth, sn, sf);
@@ -173,10 +188,12 @@ __device__ __forceinline__ bool splat_hit(const SplatParams &P, const WinRay &ra
     const uint4 link = __ldg(&P.prims[p].link);
     if (need) clipped += link.z - link.y;
     float st, dt;
-    if (!splat_clip_warp(P, ray, link.y, link.z, depth, sn, sf, need, st, dt)) return false;
-    t = st;
-    cell = link.x;
-    aux = __float_as_uint(dt);
+    uint32_t links;
+    if (!splat_clip_warp(P, ray, link.y, link.z, depth, sn, sf, need, st, dt, links)) return false;
+    k.t = st;
+    k.idx = link.x;
+    k.pos = __float_as_uint(dt);
+    set_links(k, links);
     return true;
 }
 
@@ -270,10 +287,8 @@ splat_kernel(const __grid_constant__ SplatParams P) {
     bool cursor_valid = false, finished = !active;
     float cur_t = 0.f;
     uint32_t cur_cell = 0;
-    auto hit = [&](uint32_t p, bool mine, float limit, float &t, uint32_t &cell,
-                   uint32_t &aux) -> bool {
-        return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, t, cell, aux,
-                         clipped);
+    auto hit = [&](uint32_t p, bool mine, float limit, auto &k) -> bool {
+        return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, k, clipped);
     };
     for (;;) {
         const bool want = !finished;
@@ -342,37 +357,36 @@ struct SplatTrainParams {
     float4 *d_site;             // [N] or null
 };
 
-// The Cech-row planes of one support for one lane (the per-ray order of
-// splat_clip_warp, from the same precomputed planes): entry / exit depths
-// before the sphere clip and the neighbours that set them (the cell itself
-// when no plane bounds that side).
-__device__ __forceinline__ void splat_planes_lane(const SplatTrainParams &TP, const WinRay &ray,
-                                                  uint32_t cell, float depth, float &face_near,
-                                                  float &face_far, uint32_t &prev,
-                                                  uint32_t &next) {
+// The entry / exit planes of a windowed interval from the row offsets its
+// key carries (kNoPlane: no plane bounds that side): their depths before
+// the sphere clip, evaluated as splat_clip_warp evaluates them, and the
+// neighbours across them (the cell itself when none).
+__device__ __forceinline__ float splat_plane_t(const SplatTrainParams &TP, const WinRay &ray,
+                                               uint32_t k) {
+    const float4 fp = __ldg(&TP.base.row_faces[k].point);
+    const float4 fn = __ldg(&TP.base.row_faces[k].normal);
+    const float rx = fp.x - ray.ox, ry = fp.y - ray.oy, rz = fp.z - ray.oz;
+    const float num = dot3(rx, ry, rz, fn.x, fn.y, fn.z);
+    const float den = dot3(ray.dx, ray.dy, ray.dz, fn.x, fn.y, fn.z);
+    return num / den;
+}
+
+__device__ __forceinline__ void splat_planes_of(const SplatTrainParams &TP, const WinRay &ray,
+                                                uint32_t cell, float depth, uint32_t links,
+                                                float &face_near, float &face_far,
+                                                uint32_t &prev, uint32_t &next) {
+    const uint32_t b = __ldg(TP.offsets + cell);
+    const uint32_t nk = links & 0xffffu, fk = links >> 16;
     face_near = 0.0f;
     face_far = depth;
     prev = next = cell;
-    const uint32_t b = __ldg(TP.offsets + cell), e = __ldg(TP.offsets + cell + 1);
-    for (uint32_t k = b; k < e; ++k) {
-        const float4 fp = __ldg(&TP.base.row_faces[k].point);
-        const float4 fn = __ldg(&TP.base.row_faces[k].normal);
-        const float rx = fp.x - ray.ox, ry = fp.y - ray.oy, rz = fp.z - ray.oz;
-        const float num = dot3(rx, ry, rz, fn.x, fn.y, fn.z);
-        const float den = dot3(ray.dx, ray.dy, ray.dz, fn.x, fn.y, fn.z);
-        if (den > 1.0e-20f) {
-            const float t = num / den;
-            if (t < face_far) {
-                face_far = t;
-                next = __ldg(TP.neighbors + k);
-            }
-        } else if (den < -1.0e-20f) {
-            const float t = num / den;
-            if (t > face_near) {
-                face_near = t;
-                prev = __ldg(TP.neighbors + k);
-            }
-        }
+    if (nk != kNoPlane) {
+        face_near = splat_plane_t(TP, ray, b + nk);
+        prev = __ldg(TP.neighbors + b + nk);
+    }
+    if (fk != kNoPlane) {
+        face_far = splat_plane_t(TP, ray, b + fk);
+        next = __ldg(TP.neighbors + b + fk);
     }
 }
 
@@ -392,10 +406,8 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
     bool cursor_valid = false, finished = !L.active;
     float cur_t = 0.f;
     uint32_t cur_cell = 0;
-    auto hit = [&](uint32_t p, bool mine, float limit, float &t, uint32_t &cell,
-                   uint32_t &aux) -> bool {
-        return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, t, cell, aux,
-                         clipped);
+    auto hit = [&](uint32_t p, bool mine, float limit, auto &k) -> bool {
+        return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, k, clipped);
     };
     for (;;) {
         const bool want = !finished;
@@ -511,21 +523,19 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
     bool finished = !L.active || (gC[0] == 0.f && gC[1] == 0.f && gC[2] == 0.f);
     float cur_t = 0.f;
     uint32_t cur_cell = 0;
-    auto hit = [&](uint32_t p, bool mine, float limit, float &t, uint32_t &cell,
-                   uint32_t &aux) -> bool {
-        return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, t, cell, aux,
-                         clipped);
+    auto hit = [&](uint32_t p, bool mine, float limit, auto &k) -> bool {
+        return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, k, clipped);
     };
     for (;;) {
         const bool want = !finished;
         if (!__any_sync(0xffffffffu, want)) break;
-        WinKey buf[kSplatWindow];
+        WinKey2 buf[kSplatWindow];
         const int count = win_gather_warp<kSplatWindow, kSplatStack>(
             P.nodes, ray, depth, want, cursor_valid, cur_t, cur_cell, buf, nodes_visited, hit);
         if (!want) continue;
 #pragma unroll 1
         for (int i = 0; i < count; ++i) {
-            const WinKey e = win_at(buf, i);
+            const WinKey2 e = win_at(buf, i);
             if (T <= P.weight_threshold || steps >= P.max_steps) {
                 finished = true;
                 break;
@@ -573,7 +583,7 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
             if (TP.d_site && dt_raw < TP.max_dt) {
                 float face_near, face_far;
                 uint32_t prev, next;
-                splat_planes_lane(TP, ray, cell, depth, face_near, face_far, prev, next);
+                splat_planes_of(TP, ray, cell, depth, e.aux, face_near, face_far, prev, next);
                 const float4 g = __ldg(TP.geom + cell);
                 Cell c;
                 c.id = cell;
@@ -827,6 +837,9 @@ bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *md, const bv_trace_
             centers[3 * (size_t)i + k] = p[k];
         }
     }
+    for (uint32_t i = 0; i < n; ++i)
+        if (md->adjacency_offsets[i + 1] - md->adjacency_offsets[i] >= kNoPlane)
+            return sp_fail(BV_ERR_NOT_SUPPORTED, "a Cech row longer than 65,534 entries");
     BvhBuild bvh = build_bvh(boxes, centers);
     if (bvh_depth(bvh.nodes) >= (uint32_t)kSplatStack)
         return sp_fail(BV_ERR_NOT_SUPPORTED, "BVH deeper than the traversal stack");

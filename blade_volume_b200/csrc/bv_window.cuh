@@ -30,6 +30,14 @@ struct WinKey {
     uint32_t pos;  // position in the BVH-ordered particle table
 };
 
+// A key with one more payload word (the splat's entry / exit plane indices).
+struct WinKey2 {
+    float t;
+    uint32_t idx;
+    uint32_t pos;
+    uint32_t aux;
+};
+
 __device__ __forceinline__ bool win_less(float ta, uint32_t ia, float tb, uint32_t ib) {
     return ta < tb || (ta == tb && ia < ib);
 }
@@ -98,16 +106,17 @@ struct WarpStack {
 // The window a lane ends with is the W smallest keys above its cursor,
 // whatever the traversal order, because pruning only drops boxes that cannot
 // hold such a key.
-// `hit(pos, mine, limit, t, idx, aux)` is called by every lane for every
-// primitive of an entered leaf and must return false where mine is false (it
-// may use warp collectives).  limit is the lane's current window end (+inf
-// while the window has room): a key at or past it cannot enter.  aux is
-// stored in the key's pos field.
-template <int W, int S, class Hit>
+// `hit(pos, mine, limit, key)` is called by every lane for every primitive
+// of an entered leaf and must return false where mine is false (it may use
+// warp collectives); on a hit it fills key.t and key.idx and may overwrite
+// the payload (key.pos starts as the table position).  limit is the lane's
+// current window end (+inf while the window has room): a key at or past it
+// cannot enter.
+template <int W, int S, class Key, class Hit>
 __device__ __forceinline__ int win_gather_warp(const BvhNode *__restrict__ nodes,
                                                const WinRay &ray, float t_end, bool want,
                                                bool cursor_valid, float cur_t, uint32_t cur_idx,
-                                               WinKey (&buf)[W], uint32_t &nodes_visited,
+                                               Key (&buf)[W], uint32_t &nodes_visited,
                                                Hit hit) {
     const uint32_t lane = threadIdx.x & 31u;
     int count = 0;
@@ -147,17 +156,16 @@ __device__ __forceinline__ int win_gather_warp(const BvhNode *__restrict__ nodes
             }
             const bool mine = ok[c];
             for (uint32_t p = ref; p < ref + cnt; ++p) {
-                float t;
-                uint32_t id, aux = p;
+                Key nk;
+                nk.pos = p;
                 const float limit = count == W ? buf[W - 1].t : __int_as_float(0x7f800000);
-                if (!hit(p, mine, limit, t, id, aux)) continue;
-                if (cursor_valid && !win_less(cur_t, cur_idx, t, id)) continue;
-                if (count == W && !win_less(t, id, buf[W - 1].t, buf[W - 1].idx)) continue;
-                WinKey nk{t, id, aux};
+                if (!hit(p, mine, limit, nk)) continue;
+                if (cursor_valid && !win_less(cur_t, cur_idx, nk.t, nk.idx)) continue;
+                if (count == W && !win_less(nk.t, nk.idx, buf[W - 1].t, buf[W - 1].idx)) continue;
 #pragma unroll
                 for (int i = 0; i < W; ++i) {
                     if (i < count && win_less(nk.t, nk.idx, buf[i].t, buf[i].idx)) {
-                        const WinKey tmp = buf[i];
+                        const Key tmp = buf[i];
                         buf[i] = nk;
                         nk = tmp;
                     }
@@ -173,9 +181,9 @@ __device__ __forceinline__ int win_gather_warp(const BvhNode *__restrict__ nodes
 }
 
 // buf[i] with a runtime i, by a static scan (keeps buf in registers).
-template <int W>
-__device__ __forceinline__ WinKey win_at(const WinKey (&buf)[W], int i) {
-    WinKey h = buf[0];
+template <int W, class Key>
+__device__ __forceinline__ Key win_at(const Key (&buf)[W], int i) {
+    Key h = buf[0];
 #pragma unroll
     for (int j = 0; j < W; ++j)
         if (j == i) h = buf[j];
