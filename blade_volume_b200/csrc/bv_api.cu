@@ -728,6 +728,8 @@ bv_status bv_radfoam_tracer_adam_step(bv_tracer *t, const bv_grads *g, const bv_
     if (g->d_radii_dev && !t->bounded)
         return fail(BV_ERR_INVALID_ARGUMENT, "radius gradients need a PowerFoam model");
     const uint32_t nsh = 3 * sh_components(t->sh_degree);
+    if ((uint64_t)t->n * nsh >= (1ull << 31))
+        return fail(BV_ERR_NOT_SUPPORTED, "more than 2^31 SH coefficients for the optimizer");
     const float beta = a->density_activation == BV_DENSITY_SOFTPLUS ? a->softplus_beta : 0.0f;
     cudaStream_t s = (cudaStream_t)stream;
     if (!t->adam_buf) {

@@ -373,7 +373,7 @@ bv_status bv_gaussian_tracer_new(const bv_gaussian_sh_desc *g,
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
         return gfail(BV_ERR_NO_DEVICE, "no CUDA device");
 
-    BvhBuild bvh = build_bvh(boxes, centers);
+    BvhBuild bvh = build_bvh(boxes, centers, BvhMethod::kSah);
     if (bvh_depth(bvh.nodes) >= (uint32_t)kStack)
         return gfail(BV_ERR_NOT_SUPPORTED, "BVH deeper than the traversal stack");
     std::vector<GaussShPrim> sorted(kept);

@@ -85,9 +85,10 @@ __global__ void __launch_bounds__(kOptBlock) adam_density_kernel(AdamParams P) {
 // SH coefficient c of site i (c < 3K): DC (c < 3) and higher-order rates.
 template <bool BF16>
 __global__ void __launch_bounds__(kOptBlock) adam_sh_kernel(AdamParams P) {
-    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= (uint64_t)P.n * P.sh_row) return;
-    const uint32_t i = (uint32_t)(k / P.sh_row), c = (uint32_t)(k % P.sh_row);
+    // 32-bit index arithmetic: n * 3K < 2^31 is checked on the host
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.n * P.sh_row) return;
+    const uint32_t i = k / P.sh_row, c = k - i * P.sh_row;
     const float lr = c < 3u ? P.lr_sh_dc : P.lr_sh_rest;
     if (lr == 0.0f) return;
     const size_t dev = (size_t)i * P.sh_stride + c;

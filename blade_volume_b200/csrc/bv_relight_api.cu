@@ -155,7 +155,7 @@ bv_status bv_relight_tracer_new_gaussian(const bv_gaussian_desc *g,
         return rfail(BV_ERR_INVALID_MODEL, "PBR Gaussian geometry has no particles above alpha 0.03");
 
     // BVH over the support boxes, particles stored in leaf order
-    BvhBuild bvh = build_bvh(boxes, centers);
+    BvhBuild bvh = build_bvh(boxes, centers, BvhMethod::kMorton);
     if (bvh_depth(bvh.nodes) >= (uint32_t)kRelightStack)
         return rfail(BV_ERR_NOT_SUPPORTED, "BVH deeper than the traversal stack");
     std::vector<GaussPrim> sorted_prims(kept);

@@ -840,7 +840,7 @@ bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *md, const bv_trace_
     for (uint32_t i = 0; i < n; ++i)
         if (md->adjacency_offsets[i + 1] - md->adjacency_offsets[i] >= kNoPlane)
             return sp_fail(BV_ERR_NOT_SUPPORTED, "a Cech row longer than 65,534 entries");
-    BvhBuild bvh = build_bvh(boxes, centers);
+    BvhBuild bvh = build_bvh(boxes, centers, BvhMethod::kMorton);
     if (bvh_depth(bvh.nodes) >= (uint32_t)kSplatStack)
         return sp_fail(BV_ERR_NOT_SUPPORTED, "BVH deeper than the traversal stack");
     std::vector<SplatPrim> prims(n);
