@@ -45,6 +45,7 @@ EXPORTED_SYMBOLS = [
     "bv_radfoam_tracer_destroy", "bv_radfoam_tracer_dispatch", "bv_radfoam_tracer_dispatch_batch",
     "bv_radfoam_tracer_set_max_steps", "bv_radfoam_tracer_set_weight_threshold",
     "bv_radfoam_tracer_set_debug_cell_density", "bv_radfoam_tracer_set_tie_break",
+    "bv_radfoam_tracer_set_exit_record",
     "bv_radfoam_tracer_max_steps",
     "bv_radfoam_tracer_weight_threshold", "bv_radfoam_tracer_sh_degree",
     "bv_radfoam_tracer_start_point", "bv_radfoam_tracer_num_points", "bv_containing_point",
@@ -226,6 +227,7 @@ def load_library(path: str = LIB_PATH):
     L.bv_radfoam_tracer_set_weight_threshold.argtypes = [C.c_void_p, C.c_float]
     L.bv_radfoam_tracer_set_debug_cell_density.argtypes = [C.c_void_p, C.c_uint32]
     L.bv_radfoam_tracer_set_tie_break.argtypes = [C.c_void_p, C.c_uint32]
+    L.bv_radfoam_tracer_set_exit_record.argtypes = [C.c_void_p, C.c_uint32]
     L.bv_radfoam_tracer_max_steps.argtypes = [C.c_void_p]
     L.bv_radfoam_tracer_max_steps.restype = C.c_uint32
     L.bv_radfoam_tracer_weight_threshold.argtypes = [C.c_void_p]
@@ -433,6 +435,11 @@ class RadFoamGpuTracer:
         """Render walk: FP64 re-evaluation of exit faces tied within 4 FP32 ulps
         (False: the reference's first-minimum rule)."""
         _check(load_library().bv_radfoam_tracer_set_tie_break(self._h, int(enabled)))
+
+    def set_exit_record(self, steps: int):
+        """Training: exit faces recorded per ray by the forward for the replay
+        (default 256 steps; 0: the replay searches every step's faces)."""
+        _check(load_library().bv_radfoam_tracer_set_exit_record(self._h, int(steps)))
 
     @property
     def max_steps(self) -> int:

@@ -22,6 +22,16 @@ namespace {
 
 thread_local std::string g_error;
 
+// Exit-face record of the training forward (4 bytes per ray and step): by
+// default this many steps per ray, and at most this many bytes per launch.
+// The replay reads one face entry per recorded step instead of searching the
+// cell's row.  0 steps disables the record.
+#ifndef BV_EXIT_REC_STEPS
+#define BV_EXIT_REC_STEPS 256
+#endif
+constexpr uint32_t kExitRecSteps = BV_EXIT_REC_STEPS;
+constexpr size_t kExitRecBytes = size_t(4) << 30;
+
 bv_status fail(bv_status code, const char *fmt, ...) {
     char buf[512];
     va_list ap;
@@ -99,6 +109,9 @@ struct bv_tracer {
     size_t ray_state_capacity = 0;
     bool ray_state_owned = true;       // false: lent by a serving engine
     float4 *site_grads = nullptr;      // [N] site gradient accumulator (kept zero)
+    uint32_t *exit_rec = nullptr;      // training forward's exit faces, read by the replay
+    size_t exit_rec_capacity = 0;      // entries
+    uint32_t exit_rec_steps = kExitRecSteps;  // recorded steps per ray
     int grid_forward = 0;
     int grid_train_fwd = 0;
     int grid_train_bwd = 0;
@@ -139,6 +152,7 @@ void free_tracer(bv_tracer *t) {
     cudaFree(t->faces);
     if (t->ray_state_owned) cudaFree(t->ray_state);
     cudaFree(t->site_grads);
+    cudaFree(t->exit_rec);
     cudaFree(t->start_cells);
     cudaFree(t->work_counter);
     cudaFree(t->stats);
@@ -509,6 +523,17 @@ bv_status bv_radfoam_tracer_set_tie_break(bv_tracer *t, uint32_t mode) {
     return BV_OK;
 }
 
+bv_status bv_radfoam_tracer_set_exit_record(bv_tracer *t, uint32_t steps) {
+    if (!t) return fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
+    t->exit_rec_steps = steps;
+    if (steps == 0) {
+        cudaFree(t->exit_rec);
+        t->exit_rec = nullptr;
+        t->exit_rec_capacity = 0;
+    }
+    return BV_OK;
+}
+
 uint32_t bv_radfoam_tracer_max_steps(const bv_tracer *t) { return t ? t->settings.max_steps : 0; }
 float bv_radfoam_tracer_weight_threshold(const bv_tracer *t) {
     return t ? t->settings.weight_threshold : 0.0f;
@@ -622,6 +647,30 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         BV_CUDA(cudaMalloc(&t->ray_state, sizeof(RayState) * chunk_rays), "cudaMalloc ray state");
         t->ray_state_capacity = chunk_rays;
     }
+    // exit-face record: the first rec_steps steps of every ray, within
+    // kExitRecBytes; a tracer whose scratch is lent by a serving engine
+    // (which budgets its device memory itself) and any steps past the record
+    // replay the exit-face search instead
+    uint32_t rec_steps = 0;
+    if (t->ray_state_owned) {
+        const size_t chunk_work =
+            (size_t)std::min<uint32_t>(n_cams, kMaxViewsPerLaunch) * padded_rays(width, height);
+        const size_t fit = kExitRecBytes / (chunk_work * sizeof(uint32_t));
+        rec_steps = (uint32_t)std::min<size_t>({(size_t)t->exit_rec_steps, (size_t)ts->max_steps, fit});
+        const size_t need = chunk_work * rec_steps;
+        if (rec_steps > 0 && need > t->exit_rec_capacity) {
+            cudaFree(t->exit_rec);
+            t->exit_rec = nullptr;
+            t->exit_rec_capacity = 0;
+            if (cudaMalloc(&t->exit_rec, need * sizeof(uint32_t)) == cudaSuccess) {
+                t->exit_rec_capacity = need;
+            } else {
+                (void)cudaGetLastError();  // out of memory: replay searches
+                t->exit_rec = nullptr;
+                rec_steps = 0;
+            }
+        }
+    }
     bv_status st = begin_timing(t, s);
     if (st != BV_OK) return st;
     BV_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), s), "loss reset");
@@ -657,6 +706,8 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         p.d_site = (grads->d_positions_dev || grads->d_radii_dev) ? t->site_grads : nullptr;
         p.loss = loss;
         p.stats = t->stats_enabled ? t->stats : nullptr;
+        p.exit_rec = rec_steps ? t->exit_rec : nullptr;
+        p.rec_steps = rec_steps;
         BV_CUDA(cudaMemsetAsync(t->work_counter, 0, 2 * sizeof(uint32_t), s), "counter reset");
         const int blocks_needed = std::max((int)((work + 255) / 256), 1);
         BV_CUDA(launch_train_forward(p, std::min(t->grid_train_fwd, blocks_needed), s),

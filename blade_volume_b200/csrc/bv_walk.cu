@@ -89,6 +89,34 @@ __device__ __noinline__ double face_t_f64(const Cell &c, const float4 &s, const 
 constexpr float kTieUlps = 4.0f;
 
 // ---------------------------------------------------------------------------
+// Exit distance through the face of cell c towards neighbour site s
+// (find_exit_face's per-face arithmetic, trace.rs:170-205): the radical
+// plane's point c + shift (s - c), shift = 0.5 + 0.5 (r_c^2 - r_s^2) / |s - c|^2
+// (0.5 for RadFoam), and t = <point - o, s - c> / <s - c, d>.  False when the
+// ray does not move towards the face (<s - c, d> <= 0).  The search and the
+// replay of a recorded exit both evaluate a face through this function, so a
+// recorded face reproduces the searched t bit for bit.
+template <bool BOUNDED>
+__device__ __forceinline__ bool face_exit_t(const Cell &c, float ri2, const float4 &site,
+                                            const Ray &ray, float &t) {
+    const float offx = site.x - c.x, offy = site.y - c.y, offz = site.z - c.z;
+    float shift;
+    if (BOUNDED) {
+        const float rj = site.w;
+        const float dsq = fmaxf(dot3(offx, offy, offz, offx, offy, offz), 1e-20f);
+        shift = 0.5f + 0.5f * (ri2 - rj * rj) / dsq;
+    } else {
+        shift = 0.5f;
+    }
+    const float fox = c.x + shift * offx;
+    const float foy = c.y + shift * offy;
+    const float foz = c.z + shift * offz;
+    const float dp = dot3(offx, offy, offz, ray.dx, ray.dy, ray.dz);
+    if (!(dp > 0.0f)) return false;
+    t = dot3(fox - ray.ox, foy - ray.oy, foz - ray.oz, offx, offy, offz) / dp;
+    return true;
+}
+
 // find_exit_face (trace.rs:170-205): the first face in CSR order with the
 // smallest t in (t0, best).  The face entries of the current cell are read
 // four at a time so that four independent loads are in flight; the winner's
@@ -99,7 +127,8 @@ constexpr float kTieUlps = 4.0f;
 // ---------------------------------------------------------------------------
 template <bool BOUNDED, bool TIE = false>
 __device__ __forceinline__ bool find_exit(const DeviceModel &m, const Cell &c, const Ray &ray,
-                                          float t0, float depth, float &best, FaceEntry &win) {
+                                          float t0, float depth, float &best, FaceEntry &win,
+                                          uint32_t &face) {
     best = depth;
     uint32_t best_k = 0xffffffffu;
     float4 best_site = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -114,22 +143,8 @@ __device__ __forceinline__ bool find_exit(const DeviceModel &m, const Cell &c, c
 #pragma unroll
         for (int u = 0; u < kFaceUnroll; ++u) {
             if (k + u < c.end) {
-                const float offx = site[u].x - c.x, offy = site[u].y - c.y, offz = site[u].z - c.z;
-                float shift;
-                if (BOUNDED) {
-                    const float rj = site[u].w;
-                    const float dsq = fmaxf(dot3(offx, offy, offz, offx, offy, offz), 1e-20f);
-                    shift = 0.5f + 0.5f * (ri2 - rj * rj) / dsq;
-                } else {
-                    shift = 0.5f;
-                }
-                const float fox = c.x + shift * offx;
-                const float foy = c.y + shift * offy;
-                const float foz = c.z + shift * offz;
-                const float dp = dot3(offx, offy, offz, ray.dx, ray.dy, ray.dz);
-                if (dp > 0.0f) {
-                    const float t =
-                        dot3(fox - ray.ox, foy - ray.oy, foz - ray.oz, offx, offy, offz) / dp;
+                float t;
+                if (face_exit_t<BOUNDED>(c, ri2, site[u], ray, t)) {
                     if (isfinite(t) && t > t0 && t < best) {
                         if (TIE) {
                             second = best;
@@ -165,6 +180,7 @@ __device__ __forceinline__ bool find_exit(const DeviceModel &m, const Cell &c, c
     // The winner's link shares the 32-byte sector of the site just read.
     win.site = best_site;
     win.link = __ldg(&m.faces[best_k].link);
+    face = best_k;
     return true;
 }
 
@@ -253,7 +269,9 @@ __device__ __forceinline__ void walk_forward_body(const WalkParams &P) {
             } else {
                 float best;
                 FaceEntry win;
-                const bool has_exit = find_exit<BOUNDED, TIE>(m, c, ray, t0, depth, best, win);
+                uint32_t face;
+                const bool has_exit =
+                    find_exit<BOUNDED, TIE>(m, c, ray, t0, depth, best, win, face);
                 n_steps += 1;
                 n_faces += c.end - c.begin;
                 float ss, se;
@@ -354,7 +372,8 @@ record_paths_kernel(const __grid_constant__ RecordParams P) {
             }
             float best;
             FaceEntry win;
-            const bool has_exit = find_exit<BOUNDED>(m, c, ray, t0, vd.depth, best, win);
+            uint32_t face;
+            const bool has_exit = find_exit<BOUNDED>(m, c, ray, t0, vd.depth, best, win, face);
             const uint32_t next = has_exit ? win.link.x : c.id;
             Interval iv;
             if (record_interval<BOUNDED>(ray, c, t0, best, iv)) {
@@ -406,7 +425,17 @@ struct TrainWalk {
     float4 pp;
     float t0, T, depth;
     uint32_t steps;
+    uint32_t work;  // dispenser index of the ray
 };
+
+// Exit-face record of the training forward, read back by the replay: entry
+// (ray w, step s) for s < rec_steps at ((w / 32) rec_steps + s) 32 + w % 32,
+// so the 32 rays of a tile, which step together, write and read one 128-byte
+// line per step.  kNoExitFace marks a step whose cell has no exit face.
+constexpr uint32_t kNoExitFace = 0xffffffffu;
+__device__ __forceinline__ size_t exit_rec_index(const TrainParams &P, uint32_t w, uint32_t s) {
+    return ((size_t)(w >> 5) * P.rec_steps + s) * 32u + (w & 31u);
+}
 
 template <int DEG, bool BOUNDED, bool BF16>
 __global__ void __launch_bounds__(kWalkBlock, BV_MINB_TRAIN_FWD)
@@ -432,6 +461,7 @@ train_forward_kernel(const __grid_constant__ TrainParams P) {
                 W.T = 1.f;
                 W.depth = ok ? vd.depth : -1.0f;  // a failed direction records nothing
                 W.steps = 0;
+                W.work = w;
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch) Ch[ch] = Cl[ch] = 0.f;
                 active = true;
@@ -453,7 +483,12 @@ train_forward_kernel(const __grid_constant__ TrainParams P) {
             } else {
                 float best;
                 FaceEntry win;
-                const bool has_exit = find_exit<BOUNDED>(m, W.c, W.ray, W.t0, W.depth, best, win);
+                uint32_t face = kNoExitFace;
+                const bool has_exit =
+                    find_exit<BOUNDED>(m, W.c, W.ray, W.t0, W.depth, best, win, face);
+                if (W.steps <= P.rec_steps)
+                    __stcs(P.exit_rec + exit_rec_index(P, W.work, W.steps - 1),
+                           has_exit ? face : kNoExitFace);
                 n_steps += 1;
                 n_faces += W.c.end - W.c.begin;
                 Interval iv;
@@ -603,6 +638,7 @@ train_backward_kernel(const __grid_constant__ TrainParams P) {
                 W.T = 1.f;
                 W.depth = ok ? vd.depth : -1.0f;
                 W.steps = 0;
+                W.work = w;
                 const RayState st = P.ray_state[pix];
                 Ch[0] = st.c_hi.x;
                 Ch[1] = st.c_hi.y;
@@ -638,8 +674,23 @@ train_backward_kernel(const __grid_constant__ TrainParams P) {
                 } else {
                     float best;
                     FaceEntry win;
-                    const bool has_exit =
-                        find_exit<BOUNDED>(m, W.c, W.ray, W.t0, W.depth, best, win);
+                    bool has_exit;
+                    if (W.steps <= P.rec_steps) {
+                        // the forward's exit face of this step: one entry
+                        // instead of the cell's row
+                        const uint32_t face =
+                            __ldcs(P.exit_rec + exit_rec_index(P, W.work, W.steps - 1));
+                        has_exit = face != kNoExitFace;
+                        best = W.depth;
+                        if (has_exit) {
+                            win.site = __ldg(&m.faces[face].site);
+                            win.link = __ldg(&m.faces[face].link);
+                            face_exit_t<BOUNDED>(W.c, W.c.r * W.c.r, win.site, W.ray, best);
+                        }
+                    } else {
+                        uint32_t face;
+                        has_exit = find_exit<BOUNDED>(m, W.c, W.ray, W.t0, W.depth, best, win, face);
+                    }
                     Interval iv;
                     if (record_interval<BOUNDED>(W.ray, W.c, W.t0, best, iv)) {
                         const float dens = W.c.density;
@@ -797,7 +848,8 @@ serve_walk_kernel(const __grid_constant__ ServeParams P) {
             } else {
                 float best;
                 FaceEntry win;
-                const bool has_exit = find_exit<BOUNDED>(m, c, ray, t0, depth, best, win);
+                uint32_t face;
+                const bool has_exit = find_exit<BOUNDED>(m, c, ray, t0, depth, best, win, face);
                 float ss, se;
                 if (support<BOUNDED>(ray, c.x, c.y, c.z, c.r, t0, best, ss, se)) {
                     const float dens = c.density * 1.0f;

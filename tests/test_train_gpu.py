@@ -36,8 +36,11 @@ def case(kind="plain", seed=3, n=4096):
     return m, cams, target
 
 
-def run_gpu(m, cams, target, max_dt=50.0, loss=bv.LOSS_L2, weight_threshold=0.0, repeat=1):
+def run_gpu(m, cams, target, max_dt=50.0, loss=bv.LOSS_L2, weight_threshold=0.0, repeat=1,
+            exit_record=None):
     t = bv.RadFoamGpuTracer(m)
+    if exit_record is not None:
+        t.set_exit_record(exit_record)
     grads = t.new_grads()
     tg = torch.from_numpy(target).cuda()
     rgb = torch.zeros((len(cams), H, W, 3), dtype=torch.float32, device="cuda")
@@ -73,6 +76,24 @@ def test_gradients_match_fp64_oracle(kind):
     assert_table("pos", g["d_pos"].reshape(-1, 3), ref["d_pos"])
     if m.radii is not None:
         assert_table("radius", g["d_radius"], ref["d_radius"])
+
+
+# The replay reads the forward's recorded exit faces for the first `rec`
+# steps of each ray and searches the rest: no record, a record that ends a few
+# steps into every ray, and the default all give the oracle's results.
+@pytest.mark.parametrize("kind,rec", [("plain", 0), ("plain", 3), ("power", 0), ("power", 5)])
+def test_exit_record_lengths_match_oracle(kind, rec):
+    m, cams, target = case(kind, seed=7, n=3000)
+    g = run_gpu(m, cams, target, exit_record=rec, repeat=2)
+    om = O.OracleModel.from_scene(m)
+    ref = O.forward_backward(om, cams, W, H, target=target)
+    assert np.array_equal(g["rgb"].view(np.uint32), ref["rgb32"].view(np.uint32))
+    # repeat=2 accumulates two identical passes
+    assert_table("density", g["d_density"], 2 * ref["d_density"])
+    assert_table("sh", g["d_sh"], 2 * ref["d_sh"])
+    assert_table("pos", g["d_pos"].reshape(-1, 3), 2 * ref["d_pos"])
+    if m.radii is not None:
+        assert_table("radius", g["d_radius"], 2 * ref["d_radius"])
 
 
 def test_l1_loss_clamped_dt_and_threshold():
