@@ -561,9 +561,13 @@ train_forward_kernel(const __grid_constant__ TrainParams P) {
 
 // Lanes of a warp that scatter into the same cell at the same replay step
 // (coherent rays walk the same cells) are reduced first: __match_any_sync
-// groups them, a binary tree over their ranks sums the values (the partner at
-// rank r + 2^l is found with __fns), and the rank-0 lane issues one vector
-// atomic per float4.  All 32 lanes must call these together.
+// groups them, a binary tree over their ranks sums the values, and the
+// rank-0 lane issues one vector atomic per float4.  At level l the lane of
+// rank r (r a multiple of 2^(l+1)) adds the value of rank r + 2^l; that
+// partner is found by pointer doubling: each lane knows the next member of
+// its group, and the member 2^l ranks above is the 2^(l-1)-above member's
+// own 2^(l-1)-above member (one shuffle per level).  All 32 lanes must call
+// these together.
 struct PeerTree {
     int levels;          // warp-uniform tree depth
     bool leader;         // rank 0 of its group
@@ -580,12 +584,17 @@ __device__ __forceinline__ PeerTree peer_tree(bool valid, uint32_t key) {
     const unsigned maxn = __reduce_max_sync(kFull, valid ? (unsigned)n : 1u);
     t.levels = maxn <= 1 ? 0 : 32 - __clz(maxn - 1);
     t.leader = rank == 0;
+    const unsigned above = peers & ~((2u << lane) - 1u);  // members after this lane
+    int up = above ? __ffs(above) - 1 : 32;                 // 2^l ranks above; 32: none
 #pragma unroll
     for (int l = 0; l < 5; ++l) {
-        const int off = 1 << l;
-        const bool r = (rank & ((off << 1) - 1)) == 0 && rank + off < n;
+        if (l > 0 && l < t.levels) {
+            const int far = __shfl_sync(kFull, up, up < 32 ? up : (int)lane);
+            up = up < 32 ? far : 32;
+        }
+        const bool r = (rank & ((2 << l) - 1)) == 0 && up < 32;
         t.recv[l] = r;
-        t.src[l] = r ? (int)__fns(peers, 0, rank + off + 1) : (int)lane;
+        t.src[l] = r ? up : (int)lane;
     }
     return t;
 }
