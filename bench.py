@@ -53,7 +53,8 @@ ADAM = dict(lr_density=0.1, lr_sh_dc=5e-3, lr_sh_rest=5e-4, lr_position=2e-4, be
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default per workload: enough for a few clock samples)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--sites", type=int, default=N_SITES)
@@ -87,6 +88,11 @@ def parse():
         args.size = 1024 if splat else WIDTH
     if args.views is None:
         args.views = 4 if splat else VIEWS
+    if args.steps is None:
+        # render (config 0) is a 0.3 ms launch: 500 of them span 0.2 s of
+        # clock samples; the BVH tracers take 10-20 ms per step
+        args.steps = {"render": 500, "gaussian": 20, "relight": 20, "splat": 5,
+                      "powerfoam": 5}.get(args.workload, 10)
     return args
 
 
@@ -127,15 +133,30 @@ class ClockSampler:
         self.proc = None
         self.file = None
 
+    def _rows(self):
+        with open(self.file.name) as f:
+            return [r.strip().split(",") for r in f.read().strip().splitlines() if r.strip()]
+
     def start(self):
+        """Starts nvidia-smi and returns once it has written its first row, so
+        that the rows after this call are samples of the timed region."""
+        self.skip = 0
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.file, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        t_end = time.time() + 10.0
+        while time.time() < t_end and self.proc.poll() is None:
+            rows = self._rows()
+            if rows:
+                self.skip = len(rows)
+                return
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
@@ -146,8 +167,7 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self.file.flush()
-        self.file.seek(0)
-        rows = [r.strip().split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        rows = self._rows()[self.skip:]
         os.unlink(self.file.name)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]

@@ -599,19 +599,21 @@ __device__ __forceinline__ PeerTree peer_tree(bool valid, uint32_t key) {
     return t;
 }
 
-__device__ __forceinline__ float group_sum(const PeerTree &t, float v) {
+// Sums M values over each lane group: per tree level the M shuffles are
+// issued together and the level test is taken once for all of them.
+template <int M>
+__device__ __forceinline__ void group_sum(const PeerTree &t, float (&v)[M]) {
 #pragma unroll
     for (int l = 0; l < 5; ++l) {
-        if (l < t.levels) {
-            const float o = __shfl_sync(kFull, v, t.src[l]);
-            if (t.recv[l]) v += o;
+        if (l >= t.levels) break;
+        float o[M];
+#pragma unroll
+        for (int i = 0; i < M; ++i) o[i] = __shfl_sync(kFull, v[i], t.src[l]);
+        if (t.recv[l]) {
+#pragma unroll
+            for (int i = 0; i < M; ++i) v[i] += o[i];
         }
     }
-    return v;
-}
-
-__device__ __forceinline__ float4 group_sum4(const PeerTree &t, float4 v) {
-    return make_float4(group_sum(t, v.x), group_sum(t, v.y), group_sum(t, v.z), group_sum(t, v.w));
 }
 
 // Replay: walk each ray again front to back, recompute T, w and the colour
@@ -754,29 +756,44 @@ train_backward_kernel(const __grid_constant__ TrainParams P) {
         const PeerTree tree = peer_tree(contrib, cell);
         float Y[K];
         sh_basis<DEG>(W.ray.dx, W.ray.dy, W.ray.dz, Y);
-        const float gd = group_sum(tree, g_density);
-        if (contrib && tree.leader) atomicAdd(P.d_density + cell, gd);
+        if (P.d_site) {
+            float v[5] = {g_density, g_site.x, g_site.y, g_site.z, g_site.w};
+            group_sum(tree, v);
+            if (contrib && tree.leader) {
+                atomicAdd(P.d_density + cell, v[0]);
+                atomicAdd(P.d_site + cell, make_float4(v[1], v[2], v[3], v[4]));
+            }
+        } else {
+            float v[1] = {g_density};
+            group_sum(tree, v);
+            if (contrib && tree.leader) atomicAdd(P.d_density + cell, v[0]);
+        }
         if (N % 4 == 0) {
+            // eight coefficients per tree pass (four for N = 12)
+            constexpr int Q = N % 8 == 0 ? 8 : 4;
             float4 *row4 = reinterpret_cast<float4 *>(P.d_sh + (size_t)cell * N);
 #pragma unroll
-            for (int q = 0; q < N / 4; ++q) {
-                float v[4];
+            for (int q = 0; q < N / Q; ++q) {
+                float v[Q];
 #pragma unroll
-                for (int h = 0; h < 4; ++h) v[h] = gw[(q * 4 + h) % 3] * Y[(q * 4 + h) / 3];
-                const float4 s4 = group_sum4(tree, make_float4(v[0], v[1], v[2], v[3]));
-                if (contrib && tree.leader) atomicAdd(row4 + q, s4);
+                for (int h = 0; h < Q; ++h) v[h] = gw[(q * Q + h) % 3] * Y[(q * Q + h) / 3];
+                group_sum(tree, v);
+                if (contrib && tree.leader) {
+#pragma unroll
+                    for (int h = 0; h < Q; h += 4)
+                        atomicAdd(row4 + (q * Q + h) / 4, make_float4(v[h], v[h + 1], v[h + 2], v[h + 3]));
+                }
             }
         } else {
             float *row = P.d_sh + (size_t)cell * N;
 #pragma unroll
-            for (int i = 0; i < N; ++i) {
-                const float sv = group_sum(tree, gw[i % 3] * Y[i / 3]);
-                if (contrib && tree.leader && sv != 0.0f) atomicAdd(row + i, sv);
+            for (int i = 0; i < N; i += 3) {
+                float v[3] = {gw[0] * Y[i / 3], gw[1] * Y[i / 3], gw[2] * Y[i / 3]};
+                group_sum(tree, v);
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    if (contrib && tree.leader && v[c] != 0.0f) atomicAdd(row + i + c, v[c]);
             }
-        }
-        if (P.d_site) {
-            const float4 s4 = group_sum4(tree, g_site);
-            if (contrib && tree.leader) atomicAdd(P.d_site + cell, s4);
         }
         if (done) active = false;
     }
