@@ -22,15 +22,17 @@ namespace {
 
 thread_local std::string g_error;
 
-// Exit-face record of the training forward (4 bytes per ray and step): by
-// default this many steps per ray, and at most this many bytes per launch.
-// The replay reads one face entry per recorded step instead of searching the
-// cell's row.  0 steps disables the record.
+// Step record of the training forward (exit face and unclamped SH colour,
+// 16 bytes per ray and step): by default this many steps per ray, and at
+// most this many bytes per launch.  The replay reads one face entry and the
+// colour per recorded step instead of searching the cell's row and
+// evaluating its SH row.  0 steps disables the record.
 #ifndef BV_EXIT_REC_STEPS
 #define BV_EXIT_REC_STEPS 256
 #endif
 constexpr uint32_t kExitRecSteps = BV_EXIT_REC_STEPS;
-constexpr size_t kExitRecBytes = size_t(4) << 30;
+constexpr size_t kExitRecBytes = size_t(8) << 30;
+constexpr size_t kStepRecWords = 4;  // face, r, g, b
 
 bv_status fail(bv_status code, const char *fmt, ...) {
     char buf[512];
@@ -109,8 +111,8 @@ struct bv_tracer {
     size_t ray_state_capacity = 0;
     bool ray_state_owned = true;       // false: lent by a serving engine
     float4 *site_grads = nullptr;      // [N] site gradient accumulator (kept zero)
-    uint32_t *exit_rec = nullptr;      // training forward's exit faces, read by the replay
-    size_t exit_rec_capacity = 0;      // entries
+    uint32_t *exit_rec = nullptr;      // training forward's step record, read by the replay
+    size_t exit_rec_capacity = 0;      // words
     uint32_t exit_rec_steps = kExitRecSteps;  // recorded steps per ray
     int grid_forward = 0;
     int grid_train_fwd = 0;
@@ -647,17 +649,17 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         BV_CUDA(cudaMalloc(&t->ray_state, sizeof(RayState) * chunk_rays), "cudaMalloc ray state");
         t->ray_state_capacity = chunk_rays;
     }
-    // exit-face record: the first rec_steps steps of every ray, within
+    // step record: the first rec_steps steps of every ray, within
     // kExitRecBytes; a tracer whose scratch is lent by a serving engine
     // (which budgets its device memory itself) and any steps past the record
-    // replay the exit-face search instead
+    // replay the exit-face search and the SH evaluation instead
     uint32_t rec_steps = 0;
     if (t->ray_state_owned) {
         const size_t chunk_work =
             (size_t)std::min<uint32_t>(n_cams, kMaxViewsPerLaunch) * padded_rays(width, height);
-        const size_t fit = kExitRecBytes / (chunk_work * sizeof(uint32_t));
+        const size_t fit = kExitRecBytes / (chunk_work * kStepRecWords * sizeof(uint32_t));
         rec_steps = (uint32_t)std::min<size_t>({(size_t)t->exit_rec_steps, (size_t)ts->max_steps, fit});
-        const size_t need = chunk_work * rec_steps;
+        const size_t need = chunk_work * rec_steps * kStepRecWords;
         if (rec_steps > 0 && need > t->exit_rec_capacity) {
             cudaFree(t->exit_rec);
             t->exit_rec = nullptr;
@@ -706,7 +708,7 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         p.d_site = (grads->d_positions_dev || grads->d_radii_dev) ? t->site_grads : nullptr;
         p.loss = loss;
         p.stats = t->stats_enabled ? t->stats : nullptr;
-        p.exit_rec = rec_steps ? t->exit_rec : nullptr;
+        p.step_rec = rec_steps ? t->exit_rec : nullptr;
         p.rec_steps = rec_steps;
         BV_CUDA(cudaMemsetAsync(t->work_counter, 0, 2 * sizeof(uint32_t), s), "counter reset");
         const int blocks_needed = std::max((int)((work + 255) / 256), 1);

@@ -108,8 +108,8 @@ struct TrainParams {
     float4 *d_site;               // [N] x, y, z, radius gradients (scratch) or null
     float *loss;                  // device scalar accumulator
     unsigned long long *stats;
-    uint32_t *exit_rec;           // exit face per (ray, step < rec_steps), or null
-    uint32_t rec_steps;           // 0: the replay searches every exit face
+    uint32_t *step_rec;           // exit face + SH colour per (ray, step < rec_steps), or null
+    uint32_t rec_steps;           // 0: the replay searches and evaluates every step
     ViewDesc views[kMaxViewsPerLaunch];
 };
 

@@ -428,13 +428,17 @@ struct TrainWalk {
     uint32_t work;  // dispenser index of the ray
 };
 
-// Exit-face record of the training forward, read back by the replay: entry
-// (ray w, step s) for s < rec_steps at ((w / 32) rec_steps + s) 32 + w % 32,
-// so the 32 rays of a tile, which step together, write and read one 128-byte
-// line per step.  kNoExitFace marks a step whose cell has no exit face.
+// Step record of the training forward, read back by the replay: for ray w
+// and step s < rec_steps a block of 4 x 32 words at ((w / 32) rec_steps + s)
+// 128 holds, at lane w % 32 of each row, the exit face (kNoExitFace: the cell
+// has none) and the unclamped SH colour r, g, b of the step (written when
+// the step composites), so the 32 rays of a tile, which step together, write
+// and read whole 128-byte lines.
+// The host bounds the record to 2^31 words, so its index is 32-bit.
 constexpr uint32_t kNoExitFace = 0xffffffffu;
-__device__ __forceinline__ size_t exit_rec_index(const TrainParams &P, uint32_t w, uint32_t s) {
-    return ((size_t)(w >> 5) * P.rec_steps + s) * 32u + (w & 31u);
+constexpr uint32_t kNotRecorded = 0xffffffffu;
+__device__ __forceinline__ uint32_t step_rec_index(const TrainParams &P, uint32_t w, uint32_t s) {
+    return s < P.rec_steps ? ((w >> 5) * P.rec_steps + s) * 128u + (w & 31u) : kNotRecorded;
 }
 
 template <int DEG, bool BOUNDED, bool BF16>
@@ -487,7 +491,7 @@ train_forward_kernel(const __grid_constant__ TrainParams P) {
                 const bool has_exit =
                     find_exit<BOUNDED>(m, W.c, W.ray, W.t0, W.depth, best, win, face);
                 if (W.steps <= P.rec_steps)
-                    __stcs(P.exit_rec + exit_rec_index(P, W.work, W.steps - 1),
+                    __stcs(P.step_rec + step_rec_index(P, W.work, W.steps - 1),
                            has_exit ? face : kNoExitFace);
                 n_steps += 1;
                 n_faces += W.c.end - W.c.begin;
@@ -502,6 +506,12 @@ train_forward_kernel(const __grid_constant__ TrainParams P) {
                         load_sh_row<DEG, BF16>(m, W.c.id, coef);
                         float cu[3];
                         eval_sh<DEG>(coef, W.ray.dx, W.ray.dy, W.ray.dz, cu[0], cu[1], cu[2]);
+                        if (W.steps <= P.rec_steps) {
+                            uint32_t *col = P.step_rec + step_rec_index(P, W.work, W.steps - 1);
+#pragma unroll
+                            for (int ch = 0; ch < 3; ++ch)
+                                __stcs(col + 32u * (ch + 1), __float_as_uint(cu[ch]));
+                        }
 #pragma unroll
                         for (int ch = 0; ch < 3; ++ch)
                             acc_add(Ch[ch], Cl[ch], wgt * fmaxf(cu[ch], 0.f));
@@ -686,11 +696,11 @@ train_backward_kernel(const __grid_constant__ TrainParams P) {
                     float best;
                     FaceEntry win;
                     bool has_exit;
-                    if (W.steps <= P.rec_steps) {
+                    const uint32_t rec = step_rec_index(P, W.work, W.steps - 1);
+                    if (rec != kNotRecorded) {
                         // the forward's exit face of this step: one entry
                         // instead of the cell's row
-                        const uint32_t face =
-                            __ldcs(P.exit_rec + exit_rec_index(P, W.work, W.steps - 1));
+                        const uint32_t face = __ldcs(P.step_rec + rec);
                         has_exit = face != kNoExitFace;
                         best = W.depth;
                         if (has_exit) {
@@ -711,10 +721,17 @@ train_backward_kernel(const __grid_constant__ TrainParams P) {
                             const float alpha = 1.0f - bv_expf(-dens * dt);
                             const float wgt = W.T * alpha;
                             const float Tn = W.T * (1.0f - alpha);
-                            float coef[ShDims<DEG>::N];
-                            load_sh_row<DEG, BF16>(m, W.c.id, coef);
                             float cu[3];
-                            eval_sh<DEG>(coef, W.ray.dx, W.ray.dy, W.ray.dz, cu[0], cu[1], cu[2]);
+                            if (rec != kNotRecorded) {
+                                // the forward's colour of this step
+#pragma unroll
+                                for (int ch = 0; ch < 3; ++ch)
+                                    cu[ch] = __uint_as_float(__ldcs(P.step_rec + rec + 32u * (ch + 1)));
+                            } else {
+                                float coef[ShDims<DEG>::N];
+                                load_sh_row<DEG, BF16>(m, W.c.id, coef);
+                                eval_sh<DEG>(coef, W.ray.dx, W.ray.dy, W.ray.dz, cu[0], cu[1], cu[2]);
+                            }
                             float gs = 0.f;
 #pragma unroll
                             for (int ch = 0; ch < 3; ++ch) {

@@ -135,12 +135,13 @@ bv_status bv_radfoam_tracer_set_debug_cell_density(bv_tracer *tracer, uint32_t e
 #define BV_TIE_BREAK_REFERENCE 0u
 #define BV_TIE_BREAK_F64 1u
 bv_status bv_radfoam_tracer_set_tie_break(bv_tracer *tracer, uint32_t mode);
-/* Training (bv_forward_backward): the forward records the exit face of each
- * ray's first `steps` walk steps (4 bytes per ray and step, at most 4 GiB per
- * launch of 32 views) and the replay reads those instead of searching the
- * cell's faces again; later steps are searched.  Default 256; 0 disables the
- * record.  Results are identical for every setting.  No reference
- * counterpart (the reference records whole paths, path_record.rs:519). */
+/* Training (bv_forward_backward): the forward records the exit face and the
+ * unclamped SH colour of each ray's first `steps` walk steps (16 bytes per
+ * ray and step, at most 8 GiB per launch of 32 views) and the replay reads
+ * those instead of searching the cell's faces and evaluating its SH row
+ * again; later steps are recomputed.  Default 256; 0 disables the record.
+ * Results are identical for every setting.  No reference counterpart (the
+ * reference records whole paths, path_record.rs:519). */
 bv_status bv_radfoam_tracer_set_exit_record(bv_tracer *tracer, uint32_t steps);
 uint32_t bv_radfoam_tracer_max_steps(const bv_tracer *tracer);
 float bv_radfoam_tracer_weight_threshold(const bv_tracer *tracer);
