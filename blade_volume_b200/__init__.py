@@ -65,6 +65,7 @@ EXPORTED_SYMBOLS = [
     "bv_powerfoam_splat_tracer_candidate_capacity", "bv_powerfoam_splat_tracer_max_steps",
     "bv_powerfoam_splat_tracer_weight_threshold",
     "bv_powerfoam_splat_tracer_set_weight_threshold", "bv_powerfoam_splat_tracer_enable_stats",
+    "bv_powerfoam_splat_tracer_set_interval_record",
     "bv_powerfoam_splat_tracer_last_stats",
     "bv_gaussian_tracer_new", "bv_gaussian_tracer_destroy",
     "bv_gaussian_tracer_set_min_transmittance", "bv_gaussian_tracer_set_background",
@@ -294,6 +295,7 @@ def load_library(path: str = LIB_PATH):
     L.bv_powerfoam_splat_tracer_weight_threshold.restype = C.c_float
     L.bv_powerfoam_splat_tracer_set_weight_threshold.argtypes = [C.c_void_p, C.c_float]
     L.bv_powerfoam_splat_tracer_enable_stats.argtypes = [C.c_void_p, C.c_uint32]
+    L.bv_powerfoam_splat_tracer_set_interval_record.argtypes = [C.c_void_p, C.c_uint32]
     L.bv_powerfoam_splat_tracer_last_stats.argtypes = [C.c_void_p, C.POINTER(LaunchStats)]
     L.bv_powerfoam_splat_tracer_forward_backward.argtypes = [
         C.c_void_p, C.POINTER(CameraC), C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
@@ -840,6 +842,11 @@ class PowerFoamSplatTracer:
 
     def enable_stats(self, enabled: bool = True):
         _check(load_library().bv_powerfoam_splat_tracer_enable_stats(self._h, 1 if enabled else 0))
+
+    def set_interval_record(self, entries: int):
+        """Training: composited intervals recorded per ray by the forward for
+        the replay (default 128; 0: the replay traverses every ray again)."""
+        _check(load_library().bv_powerfoam_splat_tracer_set_interval_record(self._h, int(entries)))
 
     def last_stats(self) -> LaunchStats:
         st = LaunchStats()

@@ -355,7 +355,26 @@ struct SplatTrainParams {
     RayState *ray_state;        // [pixels]
     float *d_density, *d_sh;
     float4 *d_site;             // [N] or null
+    uint32_t *interval_rec;     // composited intervals per ray (< rec_entries), or null
+    uint32_t rec_entries;       // 0: the replay traverses every ray again
 };
+
+// Interval record of the training forward, read back by the replay: entry i
+// (< rec_entries) of ray w is a block of 6 x 32 words at ((w / 32)
+// rec_entries + i) 192 holding, at lane w % 32 of each row, the cell, the
+// raw interval length (float bits), the entry / exit plane offsets (the
+// WinKey2 aux) and the unclamped SH colour r, g, b of the w-th ray's i-th
+// composited interval.  The host bounds the record to 2^32 words.  The
+// forward keeps the count (or kRecOverflow when the ray composited more
+// intervals than the record holds) in its RayState.
+constexpr uint32_t kRecWords = 6;
+constexpr uint32_t kSplatRecEntries = 128;
+constexpr size_t kSplatRecBytes = size_t(12) << 30;  // < 2^32 words: 32-bit indices
+constexpr uint32_t kRecOverflow = 0xffffffffu;
+__device__ __forceinline__ uint32_t interval_rec_index(const SplatTrainParams &TP, uint32_t w,
+                                                       uint32_t i) {
+    return ((w >> 5) * TP.rec_entries + i) * (kRecWords * 32u) + (w & 31u);
+}
 
 // The entry / exit planes of a windowed interval from the row offsets its
 // key carries (kNoPlane: no plane bounds that side): their depths before
@@ -412,13 +431,13 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
     for (;;) {
         const bool want = !finished;
         if (!__any_sync(0xffffffffu, want)) break;
-        WinKey buf[kSplatWindow];
+        WinKey2 buf[kSplatWindow];
         const int count = win_gather_warp<kSplatWindow, kSplatStack>(
             P.nodes, ray, depth, want, cursor_valid, cur_t, cur_cell, buf, nodes_visited, hit);
         if (!want) continue;
 #pragma unroll 1
         for (int i = 0; i < count; ++i) {
-            const WinKey e = win_at(buf, i);
+            const WinKey2 e = win_at(buf, i);
             if (T <= P.weight_threshold || steps >= P.max_steps) {
                 finished = true;
                 break;
@@ -433,6 +452,14 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
             load_sh_row<DEG, BF16>(P.m, e.idx, coef);
             float cu[3];
             eval_sh<DEG>(coef, ray.dx, ray.dy, ray.dz, cu[0], cu[1], cu[2]);
+            if (composited < TP.rec_entries) {
+                uint32_t *rec = TP.interval_rec + interval_rec_index(TP, w, composited);
+                __stcs(rec, e.idx);
+                __stcs(rec + 32, e.pos);
+                __stcs(rec + 64, e.aux);
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) __stcs(rec + 96 + 32 * ch, __float_as_uint(cu[ch]));
+            }
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch) acc_add(Ch[ch], Cl[ch], wgt * fmaxf(cu[ch], 0.f));
             T = T * (1.0f - alpha);
@@ -468,7 +495,8 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
         RayState st;
         st.c_hi = make_float4(Ch[0], Ch[1], Ch[2], gC[0]);
         st.c_lo = make_float4(Cl[0], Cl[1], Cl[2], gC[1]);
-        st.g = make_float4(gC[2], 0.f, 0.f, 0.f);
+        const uint32_t recorded = composited <= TP.rec_entries ? composited : kRecOverflow;
+        st.g = make_float4(gC[2], __uint_as_float(recorded), 0.f, 0.f);
         TP.ray_state[pix] = st;
     }
 #pragma unroll
@@ -481,19 +509,89 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
     }
 }
 
-// Replay: the same windows in the same order, recomputing T, w and colour,
-// the suffix S_{k+1} = C - P_k from the compensated prefix, and scattering
+// Gradient of one composited interval of the replay (cell, raw length,
+// entry / exit plane offsets, unclamped colour cu), advancing T and the
+// compensated prefix P:
 //   dL/dsigma_k = dt_k sum_c g_c (T_{k+1} c_kc - S_{k+1,c})
 //   dL/dSH_kmc  = g_c w_k Y_m(d) [c_kc unclamped > 0]
 //   dL/ddt_k    = sigma_k sum_c g_c (T_{k+1} c_kc - S_{k+1,c})  -> sites, radii
-// through the interval's exact Jacobians (path_interval_jacobian of the
-// entry / exit neighbours, trace.rs:1199-1325).
+// with S_{k+1} = C - P_k, through the interval's exact Jacobians
+// (path_interval_jacobian of the entry / exit neighbours, trace.rs:1199-1325).
+template <int DEG>
+__device__ __forceinline__ void splat_interval_grad(const SplatTrainParams &TP, const WinRay &ray,
+                                                    const Ray &r, float depth,
+                                                    const float (&Y)[ShDims<DEG>::K],
+                                                    uint32_t cell, float dens, float dt_raw,
+                                                    uint32_t links, const float (&cu)[3],
+                                                    const float (&Ch)[3], const float (&Cl)[3],
+                                                    const float (&gC)[3], float &T, float (&Ph)[3],
+                                                    float (&Pl)[3]) {
+    constexpr int N = 3 * ShDims<DEG>::K;
+    const float dt = fminf(dt_raw, TP.max_dt);
+    const float alpha = 1.0f - bv_expf(-dens * dt);
+    const float wgt = T * alpha;
+    const float Tn = T * (1.0f - alpha);
+    float gs = 0.f, gw[3];
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+        const float cc = fmaxf(cu[ch], 0.f);
+        acc_add(Ph[ch], Pl[ch], wgt * cc);
+        const float suffix = (Ch[ch] - Ph[ch]) + (Cl[ch] - Pl[ch]);
+        gs += gC[ch] * (Tn * cc - suffix);
+        gw[ch] = cu[ch] > 0.f ? gC[ch] * wgt : 0.f;
+    }
+    atomicAdd(TP.d_density + cell, dt * gs);
+    if (N % 4 == 0) {
+        float4 *row4 = reinterpret_cast<float4 *>(TP.d_sh + (size_t)cell * N);
+#pragma unroll
+        for (int q = 0; q < N / 4; ++q) {
+            float v[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) v[h] = gw[(q * 4 + h) % 3] * Y[(q * 4 + h) / 3];
+            atomicAdd(row4 + q, make_float4(v[0], v[1], v[2], v[3]));
+        }
+    } else {
+        float *row = TP.d_sh + (size_t)cell * N;
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+            const float v = gw[m % 3] * Y[m / 3];
+            if (v != 0.0f) atomicAdd(row + m, v);
+        }
+    }
+    if (TP.d_site && dt_raw < TP.max_dt) {
+        float face_near, face_far;
+        uint32_t prev, next;
+        splat_planes_of(TP, ray, cell, depth, links, face_near, face_far, prev, next);
+        const float4 g = __ldg(TP.geom + cell);
+        Cell c;
+        c.id = cell;
+        c.x = g.x;
+        c.y = g.y;
+        c.z = g.z;
+        c.r = g.w;
+        c.density = dens;
+        Interval iv;
+        record_interval<true>(r, c, face_near, face_far, iv);
+        const float4 pp = __ldg(TP.geom + prev), np = __ldg(TP.geom + next);
+        const Jacobians J =
+            interval_jacobians(r, iv, prev, pp, c, next != cell, np, face_near, face_far);
+        const float gdt = dens * gs;
+        scatter_site(TP.d_site, cell, gdt, J.jc);
+        if (prev != cell && !iv.start_sphere) scatter_site(TP.d_site, prev, gdt, J.jp);
+        if (next != cell && !iv.end_sphere) scatter_site(TP.d_site, next, gdt, J.jn);
+    }
+    T = Tn;
+}
+
+// Replay.  A ray whose composited intervals all fit the forward's record
+// walks that list: no traversal, no clip, no SH row.  The others (record
+// overflow, or no record) gather the same windows in the same order again
+// and recompute each interval's colour.  Both feed splat_interval_grad.
 template <int DEG, bool BF16>
 __global__ void __launch_bounds__(kSplatBlock)
 splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
     const SplatParams &P = TP.base;
     constexpr int K = ShDims<DEG>::K;
-    constexpr int N = 3 * K;
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
     if ((w & ~31u) >= P.total_work) return;
     const SplatLane L = splat_lane(P, w);
@@ -501,6 +599,7 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
     const float depth = L.vd->depth;
     const Ray r{ray.ox, ray.oy, ray.oz, ray.dx, ray.dy, ray.dz};
     float Ch[3] = {0.f, 0.f, 0.f}, Cl[3] = {0.f, 0.f, 0.f}, gC[3] = {0.f, 0.f, 0.f};
+    uint32_t recorded = kRecOverflow;
     if (L.active) {
         const RayState st =
             TP.ray_state[(size_t)L.vd->pixel_begin + (size_t)L.y * L.vd->width + L.x];
@@ -513,14 +612,31 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
         gC[0] = st.c_hi.w;
         gC[1] = st.c_lo.w;
         gC[2] = st.g.x;
+        recorded = __float_as_uint(st.g.y);
     }
     float Ph[3] = {0.f, 0.f, 0.f}, Pl[3] = {0.f, 0.f, 0.f};
     float Y[K];
     sh_basis<DEG>(ray.dx, ray.dy, ray.dz, Y);
     float T = 1.0f;
+    bool finished = !L.active || (gC[0] == 0.f && gC[1] == 0.f && gC[2] == 0.f);
+    if (!finished && recorded != kRecOverflow) {
+#pragma unroll 1
+        for (uint32_t i = 0; i < recorded; ++i) {
+            const uint32_t *rec = TP.interval_rec + interval_rec_index(TP, w, i);
+            const uint32_t cell = __ldcs(rec);
+            const float dt_raw = __uint_as_float(__ldcs(rec + 32));
+            const uint32_t links = __ldcs(rec + 64);
+            float cu[3];
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) cu[ch] = __uint_as_float(__ldcs(rec + 96 + 32 * ch));
+            const float dens = __ldg(P.m.density + cell) * 1.0f;
+            splat_interval_grad<DEG>(TP, ray, r, depth, Y, cell, dens, dt_raw, links, cu, Ch, Cl,
+                                     gC, T, Ph, Pl);
+        }
+        finished = true;
+    }
     uint32_t steps = 0, clipped = 0, nodes_visited = 0;
     bool cursor_valid = false;
-    bool finished = !L.active || (gC[0] == 0.f && gC[1] == 0.f && gC[2] == 0.f);
     float cur_t = 0.f;
     uint32_t cur_cell = 0;
     auto hit = [&](uint32_t p, bool mine, float limit, auto &k) -> bool {
@@ -544,65 +660,12 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
             const uint32_t cell = e.idx;
             const float dens = __ldg(P.m.density + cell) * 1.0f;
             if (dens <= 1.0e-6f) continue;
-            const float dt_raw = __uint_as_float(e.pos);
-            const float dt = fminf(dt_raw, TP.max_dt);
-            const float alpha = 1.0f - bv_expf(-dens * dt);
-            const float wgt = T * alpha;
-            const float Tn = T * (1.0f - alpha);
             float coef[ShDims<DEG>::N];
             load_sh_row<DEG, BF16>(P.m, cell, coef);
             float cu[3];
             eval_sh<DEG>(coef, ray.dx, ray.dy, ray.dz, cu[0], cu[1], cu[2]);
-            float gs = 0.f, gw[3];
-#pragma unroll
-            for (int ch = 0; ch < 3; ++ch) {
-                const float cc = fmaxf(cu[ch], 0.f);
-                acc_add(Ph[ch], Pl[ch], wgt * cc);
-                const float suffix = (Ch[ch] - Ph[ch]) + (Cl[ch] - Pl[ch]);
-                gs += gC[ch] * (Tn * cc - suffix);
-                gw[ch] = cu[ch] > 0.f ? gC[ch] * wgt : 0.f;
-            }
-            atomicAdd(TP.d_density + cell, dt * gs);
-            if (N % 4 == 0) {
-                float4 *row4 = reinterpret_cast<float4 *>(TP.d_sh + (size_t)cell * N);
-#pragma unroll
-                for (int q = 0; q < N / 4; ++q) {
-                    float v[4];
-#pragma unroll
-                    for (int h = 0; h < 4; ++h) v[h] = gw[(q * 4 + h) % 3] * Y[(q * 4 + h) / 3];
-                    atomicAdd(row4 + q, make_float4(v[0], v[1], v[2], v[3]));
-                }
-            } else {
-                float *row = TP.d_sh + (size_t)cell * N;
-#pragma unroll
-                for (int m = 0; m < N; ++m) {
-                    const float v = gw[m % 3] * Y[m / 3];
-                    if (v != 0.0f) atomicAdd(row + m, v);
-                }
-            }
-            if (TP.d_site && dt_raw < TP.max_dt) {
-                float face_near, face_far;
-                uint32_t prev, next;
-                splat_planes_of(TP, ray, cell, depth, e.aux, face_near, face_far, prev, next);
-                const float4 g = __ldg(TP.geom + cell);
-                Cell c;
-                c.id = cell;
-                c.x = g.x;
-                c.y = g.y;
-                c.z = g.z;
-                c.r = g.w;
-                c.density = dens;
-                Interval iv;
-                record_interval<true>(r, c, face_near, face_far, iv);
-                const float4 pp = __ldg(TP.geom + prev), np = __ldg(TP.geom + next);
-                const Jacobians J =
-                    interval_jacobians(r, iv, prev, pp, c, next != cell, np, face_near, face_far);
-                const float gdt = dens * gs;
-                scatter_site(TP.d_site, cell, gdt, J.jc);
-                if (prev != cell && !iv.start_sphere) scatter_site(TP.d_site, prev, gdt, J.jp);
-                if (next != cell && !iv.end_sphere) scatter_site(TP.d_site, next, gdt, J.jn);
-            }
-            T = Tn;
+            splat_interval_grad<DEG>(TP, ray, r, depth, Y, cell, dens, __uint_as_float(e.pos),
+                                     e.aux, cu, Ch, Cl, gC, T, Ph, Pl);
         }
         if (finished) continue;
         if (count < kSplatWindow) {
@@ -705,6 +768,9 @@ struct bv_splat_tracer {
     // training scratch
     RayState *ray_state = nullptr;
     size_t ray_state_capacity = 0;
+    uint32_t *interval_rec = nullptr;  // training forward's composited intervals
+    size_t interval_rec_capacity = 0;  // words
+    uint32_t rec_entries = kSplatRecEntries;
     float4 *site_grads = nullptr;    // [N], kept zero between calls
     void *sh = nullptr;
     unsigned long long *stats = nullptr;
@@ -743,6 +809,7 @@ void free_splat(bv_splat_tracer *t) {
     cudaFree(t->offsets);
     cudaFree(t->neighbors);
     cudaFree(t->ray_state);
+    cudaFree(t->interval_rec);
     cudaFree(t->site_grads);
     cudaFree(t->density);
     cudaFree(t->sh);
@@ -1034,6 +1101,17 @@ bv_status bv_powerfoam_splat_tracer_set_weight_threshold(bv_splat_tracer *t, flo
     return BV_OK;
 }
 
+bv_status bv_powerfoam_splat_tracer_set_interval_record(bv_splat_tracer *t, uint32_t entries) {
+    if (!t) return sp_fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
+    t->rec_entries = entries;
+    if (entries == 0) {
+        cudaFree(t->interval_rec);
+        t->interval_rec = nullptr;
+        t->interval_rec_capacity = 0;
+    }
+    return BV_OK;
+}
+
 bv_status bv_powerfoam_splat_tracer_enable_stats(bv_splat_tracer *t, uint32_t enabled) {
     if (!t) return sp_fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
     t->stats_enabled = enabled != 0;
@@ -1088,6 +1166,28 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         SP_CUDA(cudaMalloc(&t->ray_state, sizeof(RayState) * chunk_rays), "cudaMalloc ray state");
         t->ray_state_capacity = chunk_rays;
     }
+    // interval record: up to rec_entries composited intervals of every ray,
+    // within kSplatRecBytes (rays with more are traversed again)
+    uint32_t rec_entries = 0;
+    {
+        const size_t chunk_work =
+            (size_t)std::min<uint32_t>(n_cams, kMaxViewsPerLaunch) * tile_padded_rays(width, height);
+        const size_t fit = kSplatRecBytes / (chunk_work * kRecWords * sizeof(uint32_t));
+        rec_entries = (uint32_t)std::min<size_t>({(size_t)t->rec_entries, (size_t)ts->max_steps, fit});
+        const size_t need = chunk_work * rec_entries * kRecWords;
+        if (rec_entries > 0 && need > t->interval_rec_capacity) {
+            cudaFree(t->interval_rec);
+            t->interval_rec = nullptr;
+            t->interval_rec_capacity = 0;
+            if (cudaMalloc(&t->interval_rec, need * sizeof(uint32_t)) == cudaSuccess) {
+                t->interval_rec_capacity = need;
+            } else {
+                (void)cudaGetLastError();  // out of memory: the replay traverses
+                t->interval_rec = nullptr;
+                rec_entries = 0;
+            }
+        }
+    }
     t->last_launches = 0;
     t->last_has_stats = t->stats_enabled;
     if (t->stats_enabled) {
@@ -1129,6 +1229,8 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         p.d_density = grads->d_density_dev;
         p.d_sh = grads->d_sh_dev;
         p.d_site = want_site ? t->site_grads : nullptr;
+        p.interval_rec = rec_entries ? t->interval_rec : nullptr;
+        p.rec_entries = rec_entries;
         SP_CUDA(launch_splat_train(p, false, s), "splat training forward launch");
         p.base.stats = nullptr;
         SP_CUDA(launch_splat_train(p, true, s), "splat training backward launch");

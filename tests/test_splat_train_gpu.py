@@ -34,8 +34,10 @@ def case(seed=3, n=4096, bf16=False, radius_max=0.1):
     return m, cams, target
 
 
-def run_gpu(m, cams, target, repeat=1, **kw):
+def run_gpu(m, cams, target, repeat=1, interval_record=None, **kw):
     t = bv.PowerFoamSplatTracer(m)
+    if interval_record is not None:
+        t.set_interval_record(interval_record)
     grads = t.new_grads()
     tg = torch.from_numpy(target).cuda()
     rgb = torch.zeros((len(cams), H, W, 3), dtype=torch.float32, device="cuda")
@@ -54,6 +56,23 @@ def run_gpu(m, cams, target, repeat=1, **kw):
 def test_splat_gradients_match_fp64_oracle(bf16, radius_max):
     m, cams, target = case(bf16=bf16, radius_max=radius_max)
     g = run_gpu(m, cams, target)
+    om = O.OracleModel.from_scene(m)
+    ref = O.forward_backward(om, cams, W, H, target=target, splats=True)
+    assert abs(g["loss"] - ref["loss"]) <= 1e-5 * ref["loss"]
+    assert np.array_equal(g["rgb"].view(np.uint32), ref["rgb32"].view(np.uint32))
+    for k, name in (("d_density", "density"), ("d_sh", "sh"), ("d_radius", "radius")):
+        assert_table(name, g[k], ref[k])
+    assert_table("pos", g["d_pos"].reshape(-1, 3), ref["d_pos"])
+
+
+# The replay walks the forward's recorded intervals of a ray when they all
+# fit and traverses the BVH again otherwise: no record, a record of two
+# intervals (rays split between both paths within a warp) and the default
+# all give the oracle's results.
+@pytest.mark.parametrize("entries", [0, 2])
+def test_interval_record_lengths_match_oracle(entries):
+    m, cams, target = case(seed=8, n=3000)
+    g = run_gpu(m, cams, target, interval_record=entries)
     om = O.OracleModel.from_scene(m)
     ref = O.forward_backward(om, cams, W, H, target=target, splats=True)
     assert abs(g["loss"] - ref["loss"]) <= 1e-5 * ref["loss"]
