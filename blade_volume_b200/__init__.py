@@ -845,7 +845,7 @@ class PowerFoamSplatTracer:
 
     def set_interval_record(self, entries: int):
         """Training: composited intervals recorded per ray by the forward for
-        the replay (default 128; 0: the replay traverses every ray again)."""
+        the replay (default 1024; 0: the replay traverses every ray again)."""
         _check(load_library().bv_powerfoam_splat_tracer_set_interval_record(self._h, int(entries)))
 
     def last_stats(self) -> LaunchStats:

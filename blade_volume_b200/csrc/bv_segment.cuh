@@ -178,5 +178,63 @@ __device__ __forceinline__ void scatter_site(float4 *d_site, uint32_t cell, floa
     atomicAdd(d_site + cell, make_float4(gdt * j.x, gdt * j.y, gdt * j.z, gdt * j.w));
 }
 
+// Lanes of a warp that scatter into the same cell at the same replay step
+// (coherent rays walk the same cells, and composite the same supports) are
+// reduced first: __match_any_sync
+// groups them, a binary tree over their ranks sums the values, and the
+// rank-0 lane issues one vector atomic per float4.  At level l the lane of
+// rank r (r a multiple of 2^(l+1)) adds the value of rank r + 2^l; that
+// partner is found by pointer doubling: each lane knows the next member of
+// its group, and the member 2^l ranks above is the 2^(l-1)-above member's
+// own 2^(l-1)-above member (one shuffle per level).  All 32 lanes must call
+// these together.
+struct PeerTree {
+    int levels;          // warp-uniform tree depth
+    bool leader;         // rank 0 of its group
+    int src[5];          // partner lane per level
+    bool recv[5];        // adds the partner's value at that level
+};
+
+__device__ __forceinline__ PeerTree peer_tree(bool valid, uint32_t key) {
+    PeerTree t;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned peers = __match_any_sync(kFull, valid ? key : 0xffffffffu);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    const int n = __popc(peers);
+    const unsigned maxn = __reduce_max_sync(kFull, valid ? (unsigned)n : 1u);
+    t.levels = maxn <= 1 ? 0 : 32 - __clz(maxn - 1);
+    t.leader = rank == 0;
+    const unsigned above = peers & ~((2u << lane) - 1u);  // members after this lane
+    int up = above ? __ffs(above) - 1 : 32;                 // 2^l ranks above; 32: none
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+        if (l > 0 && l < t.levels) {
+            const int far = __shfl_sync(kFull, up, up < 32 ? up : (int)lane);
+            up = up < 32 ? far : 32;
+        }
+        const bool r = (rank & ((2 << l) - 1)) == 0 && up < 32;
+        t.recv[l] = r;
+        t.src[l] = r ? up : (int)lane;
+    }
+    return t;
+}
+
+// Sums M values over each lane group: per tree level the M shuffles are
+// issued together and the level test is taken once for all of them.
+template <int M>
+__device__ __forceinline__ void group_sum(const PeerTree &t, float (&v)[M]) {
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+        if (l >= t.levels) break;
+        float o[M];
+#pragma unroll
+        for (int i = 0; i < M; ++i) o[i] = __shfl_sync(kFull, v[i], t.src[l]);
+        if (t.recv[l]) {
+#pragma unroll
+            for (int i = 0; i < M; ++i) v[i] += o[i];
+        }
+    }
+}
+
 }  // namespace
 }  // namespace bv

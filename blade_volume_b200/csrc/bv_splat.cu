@@ -355,25 +355,73 @@ struct SplatTrainParams {
     RayState *ray_state;        // [pixels]
     float *d_density, *d_sh;
     float4 *d_site;             // [N] or null
-    uint32_t *interval_rec;     // composited intervals per ray (< rec_entries), or null
-    uint32_t rec_entries;       // 0: the replay traverses every ray again
+    uint32_t *rec_pool;         // interval-record chunks, or null
+    uint32_t *rec_table;        // [tiles][rec_chunks] chunk of each (tile, chunk rank)
+    uint32_t *rec_next;         // next free chunk of the pool
+    uint32_t rec_chunks;        // chunk ranks per tile; 0: the replay traverses every ray
+    uint32_t rec_limit;         // intervals recorded per ray at most
+    uint32_t pool_chunks;       // chunks in the pool
 };
 
-// Interval record of the training forward, read back by the replay: entry i
-// (< rec_entries) of ray w is a block of 6 x 32 words at ((w / 32)
-// rec_entries + i) 192 holding, at lane w % 32 of each row, the cell, the
-// raw interval length (float bits), the entry / exit plane offsets (the
-// WinKey2 aux) and the unclamped SH colour r, g, b of the w-th ray's i-th
-// composited interval.  The host bounds the record to 2^32 words.  The
-// forward keeps the count (or kRecOverflow when the ray composited more
-// intervals than the record holds) in its RayState.
+// Interval record of the training forward, read back by the replay.  The
+// i-th composited interval of ray w (the cell, the raw interval length as
+// float bits, the entry / exit plane offsets of its WinKey2 and the
+// unclamped SH colour r, g, b) sits in the chunk that the tile of w (the 32
+// rays w / 32) holds for ranks 16 (i / 16) .. +15: a chunk is 16 ranks x 6
+// rows x 32 lanes of words, so the rays of a tile, which composite together,
+// write and read whole 128-byte rows.  Chunks are taken from a pool when a
+// ray of the tile first needs that rank (an atomic counter; a CAS publishes
+// the chunk in the tile's table, and a lane that loses the race uses the
+// winner's), so the record grows with the intervals actually composited.  A
+// ray that finds the pool empty, or composites more than rec_limit
+// intervals, stops recording and is marked kRecOverflow in its RayState; the
+// replay traverses it again.
+#ifndef BV_SPLAT_REC_ENTRIES
+#define BV_SPLAT_REC_ENTRIES 1024
+#endif
+#ifndef BV_SPLAT_REC_GIB
+#define BV_SPLAT_REC_GIB 12
+#endif
 constexpr uint32_t kRecWords = 6;
-constexpr uint32_t kSplatRecEntries = 128;
-constexpr size_t kSplatRecBytes = size_t(12) << 30;  // < 2^32 words: 32-bit indices
+constexpr uint32_t kChunkEntries = 16;
+constexpr uint32_t kChunkWords = kChunkEntries * kRecWords * 32u;  // 12 KiB
+constexpr uint32_t kSplatRecEntries = BV_SPLAT_REC_ENTRIES;
+constexpr size_t kSplatRecBytes = size_t(BV_SPLAT_REC_GIB) << 30;
+constexpr uint32_t kNoChunk = 0xffffffffu;
 constexpr uint32_t kRecOverflow = 0xffffffffu;
-__device__ __forceinline__ uint32_t interval_rec_index(const SplatTrainParams &TP, uint32_t w,
-                                                       uint32_t i) {
-    return ((w >> 5) * TP.rec_entries + i) * (kRecWords * 32u) + (w & 31u);
+
+__device__ __forceinline__ uint32_t *rec_entry(const SplatTrainParams &TP, uint32_t chunk,
+                                               uint32_t w, uint32_t i) {
+    return TP.rec_pool + (size_t)chunk * kChunkWords + (i % kChunkEntries) * (kRecWords * 32u) +
+           (w & 31u);
+}
+
+// The chunk for rank i of ray w's tile (i a multiple of 16), taken from the
+// pool if no ray of the tile holds it yet; kNoChunk when none can be had.
+// The lanes of the tile that reach rank i together (the calling lanes that
+// ask for the same chunk) elect one of them to take it, so a tile takes one
+// chunk per rank; a lane that asks later finds it in the table.
+__device__ __forceinline__ uint32_t rec_chunk_for_write(const SplatTrainParams &TP, uint32_t w,
+                                                        uint32_t i) {
+    const uint32_t c = i / kChunkEntries;
+    const unsigned active = __activemask();
+    const unsigned group = __match_any_sync(active, c);
+    const int leader = __ffs(group) - 1;
+    uint32_t id = kNoChunk;
+    if ((int)(threadIdx.x & 31u) == leader && c < TP.rec_chunks) {
+        uint32_t *slot = TP.rec_table + (size_t)(w >> 5) * TP.rec_chunks + c;
+        id = *reinterpret_cast<volatile uint32_t *>(slot);
+        if (id == kNoChunk) {
+            const uint32_t mine = atomicAdd(TP.rec_next, 1u);
+            if (mine < TP.pool_chunks) {
+                const uint32_t prev = atomicCAS(slot, kNoChunk, mine);
+                id = prev == kNoChunk ? mine : prev;
+            } else {
+                id = *reinterpret_cast<volatile uint32_t *>(slot);
+            }
+        }
+    }
+    return __shfl_sync(group, id, leader);
 }
 
 // The entry / exit planes of a windowed interval from the row offsets its
@@ -422,6 +470,8 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
     float Ch[3] = {0.f, 0.f, 0.f}, Cl[3] = {0.f, 0.f, 0.f};
     float T = 1.0f;
     uint32_t steps = 0, clipped = 0, nodes_visited = 0, composited = 0;
+    bool rec_ok = TP.rec_chunks != 0;
+    uint32_t rec_chunk = kNoChunk;
     bool cursor_valid = false, finished = !L.active;
     float cur_t = 0.f;
     uint32_t cur_cell = 0;
@@ -452,8 +502,13 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
             load_sh_row<DEG, BF16>(P.m, e.idx, coef);
             float cu[3];
             eval_sh<DEG>(coef, ray.dx, ray.dy, ray.dz, cu[0], cu[1], cu[2]);
-            if (composited < TP.rec_entries) {
-                uint32_t *rec = TP.interval_rec + interval_rec_index(TP, w, composited);
+            if (composited >= TP.rec_limit) rec_ok = false;
+            if (rec_ok && composited % kChunkEntries == 0) {
+                rec_chunk = rec_chunk_for_write(TP, w, composited);
+                rec_ok = rec_chunk != kNoChunk;
+            }
+            if (rec_ok) {
+                uint32_t *rec = rec_entry(TP, rec_chunk, w, composited);
                 __stcs(rec, e.idx);
                 __stcs(rec + 32, e.pos);
                 __stcs(rec + 64, e.aux);
@@ -495,7 +550,7 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
         RayState st;
         st.c_hi = make_float4(Ch[0], Ch[1], Ch[2], gC[0]);
         st.c_lo = make_float4(Cl[0], Cl[1], Cl[2], gC[1]);
-        const uint32_t recorded = composited <= TP.rec_entries ? composited : kRecOverflow;
+        const uint32_t recorded = rec_ok ? composited : kRecOverflow;
         st.g = make_float4(gC[2], __uint_as_float(recorded), 0.f, 0.f);
         TP.ray_state[pix] = st;
     }
@@ -517,47 +572,35 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
 //   dL/ddt_k    = sigma_k sum_c g_c (T_{k+1} c_kc - S_{k+1,c})  -> sites, radii
 // with S_{k+1} = C - P_k, through the interval's exact Jacobians
 // (path_interval_jacobian of the entry / exit neighbours, trace.rs:1199-1325).
+// The entry / exit neighbours' site gradients are scattered here; the
+// cell's own terms are returned for the caller's scatter.
+struct IntervalGrad {
+    float g_density;
+    float gw[3];     // dL/dSH_kmc = gw[c] Y_m
+    float4 g_site;   // the cell's site / radius gradient (zero without one)
+};
+
 template <int DEG>
-__device__ __forceinline__ void splat_interval_grad(const SplatTrainParams &TP, const WinRay &ray,
-                                                    const Ray &r, float depth,
-                                                    const float (&Y)[ShDims<DEG>::K],
-                                                    uint32_t cell, float dens, float dt_raw,
-                                                    uint32_t links, const float (&cu)[3],
-                                                    const float (&Ch)[3], const float (&Cl)[3],
-                                                    const float (&gC)[3], float &T, float (&Ph)[3],
-                                                    float (&Pl)[3]) {
-    constexpr int N = 3 * ShDims<DEG>::K;
+__device__ __forceinline__ IntervalGrad splat_interval_terms(
+    const SplatTrainParams &TP, const WinRay &ray, const Ray &r, float depth, uint32_t cell,
+    float dens, float dt_raw, uint32_t links, const float (&cu)[3], const float (&Ch)[3],
+    const float (&Cl)[3], const float (&gC)[3], float &T, float (&Ph)[3], float (&Pl)[3]) {
+    IntervalGrad G;
     const float dt = fminf(dt_raw, TP.max_dt);
     const float alpha = 1.0f - bv_expf(-dens * dt);
     const float wgt = T * alpha;
     const float Tn = T * (1.0f - alpha);
-    float gs = 0.f, gw[3];
+    float gs = 0.f;
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
         const float cc = fmaxf(cu[ch], 0.f);
         acc_add(Ph[ch], Pl[ch], wgt * cc);
         const float suffix = (Ch[ch] - Ph[ch]) + (Cl[ch] - Pl[ch]);
         gs += gC[ch] * (Tn * cc - suffix);
-        gw[ch] = cu[ch] > 0.f ? gC[ch] * wgt : 0.f;
+        G.gw[ch] = cu[ch] > 0.f ? gC[ch] * wgt : 0.f;
     }
-    atomicAdd(TP.d_density + cell, dt * gs);
-    if (N % 4 == 0) {
-        float4 *row4 = reinterpret_cast<float4 *>(TP.d_sh + (size_t)cell * N);
-#pragma unroll
-        for (int q = 0; q < N / 4; ++q) {
-            float v[4];
-#pragma unroll
-            for (int h = 0; h < 4; ++h) v[h] = gw[(q * 4 + h) % 3] * Y[(q * 4 + h) / 3];
-            atomicAdd(row4 + q, make_float4(v[0], v[1], v[2], v[3]));
-        }
-    } else {
-        float *row = TP.d_sh + (size_t)cell * N;
-#pragma unroll
-        for (int m = 0; m < N; ++m) {
-            const float v = gw[m % 3] * Y[m / 3];
-            if (v != 0.0f) atomicAdd(row + m, v);
-        }
-    }
+    G.g_density = dt * gs;
+    G.g_site = make_float4(0.f, 0.f, 0.f, 0.f);
     if (TP.d_site && dt_raw < TP.max_dt) {
         float face_near, face_far;
         uint32_t prev, next;
@@ -576,11 +619,90 @@ __device__ __forceinline__ void splat_interval_grad(const SplatTrainParams &TP, 
         const Jacobians J =
             interval_jacobians(r, iv, prev, pp, c, next != cell, np, face_near, face_far);
         const float gdt = dens * gs;
-        scatter_site(TP.d_site, cell, gdt, J.jc);
+        G.g_site = make_float4(gdt * J.jc.x, gdt * J.jc.y, gdt * J.jc.z, gdt * J.jc.w);
         if (prev != cell && !iv.start_sphere) scatter_site(TP.d_site, prev, gdt, J.jp);
         if (next != cell && !iv.end_sphere) scatter_site(TP.d_site, next, gdt, J.jn);
     }
     T = Tn;
+    return G;
+}
+
+// The cell's terms of one interval, one lane's own atomics.
+template <int DEG>
+__device__ __forceinline__ void scatter_interval(const SplatTrainParams &TP,
+                                                 const float (&Y)[ShDims<DEG>::K], uint32_t cell,
+                                                 const IntervalGrad &G) {
+    constexpr int N = 3 * ShDims<DEG>::K;
+    atomicAdd(TP.d_density + cell, G.g_density);
+    if (N % 4 == 0) {
+        float4 *row4 = reinterpret_cast<float4 *>(TP.d_sh + (size_t)cell * N);
+#pragma unroll
+        for (int q = 0; q < N / 4; ++q) {
+            float v[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) v[h] = G.gw[(q * 4 + h) % 3] * Y[(q * 4 + h) / 3];
+            atomicAdd(row4 + q, make_float4(v[0], v[1], v[2], v[3]));
+        }
+    } else {
+        float *row = TP.d_sh + (size_t)cell * N;
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+            const float v = G.gw[m % 3] * Y[m / 3];
+            if (v != 0.0f) atomicAdd(row + m, v);
+        }
+    }
+    if (TP.d_site) atomicAdd(TP.d_site + cell, G.g_site);
+}
+
+// The same, reduced over the lanes of the warp that scatter into the same
+// cell at this point first (all 32 lanes call it; `valid` marks the lanes
+// with an interval).
+template <int DEG>
+__device__ __forceinline__ void scatter_interval_warp(const SplatTrainParams &TP,
+                                                      const float (&Y)[ShDims<DEG>::K],
+                                                      bool valid, uint32_t cell,
+                                                      const IntervalGrad &G) {
+    constexpr int N = 3 * ShDims<DEG>::K;
+    const PeerTree tree = peer_tree(valid, cell);
+    const bool lead = valid && tree.leader;
+    if (TP.d_site) {
+        float v[5] = {G.g_density, G.g_site.x, G.g_site.y, G.g_site.z, G.g_site.w};
+        group_sum(tree, v);
+        if (lead) {
+            atomicAdd(TP.d_density + cell, v[0]);
+            atomicAdd(TP.d_site + cell, make_float4(v[1], v[2], v[3], v[4]));
+        }
+    } else {
+        float v[1] = {G.g_density};
+        group_sum(tree, v);
+        if (lead) atomicAdd(TP.d_density + cell, v[0]);
+    }
+    if (N % 4 == 0) {
+        constexpr int Q = N % 8 == 0 ? 8 : 4;
+        float4 *row4 = reinterpret_cast<float4 *>(TP.d_sh + (size_t)cell * N);
+#pragma unroll
+        for (int q = 0; q < N / Q; ++q) {
+            float v[Q];
+#pragma unroll
+            for (int h = 0; h < Q; ++h) v[h] = G.gw[(q * Q + h) % 3] * Y[(q * Q + h) / 3];
+            group_sum(tree, v);
+            if (lead) {
+#pragma unroll
+                for (int h = 0; h < Q; h += 4)
+                    atomicAdd(row4 + (q * Q + h) / 4, make_float4(v[h], v[h + 1], v[h + 2], v[h + 3]));
+            }
+        }
+    } else {
+        float *row = TP.d_sh + (size_t)cell * N;
+#pragma unroll
+        for (int i = 0; i < N; i += 3) {
+            float v[3] = {G.gw[0] * Y[i / 3], G.gw[1] * Y[i / 3], G.gw[2] * Y[i / 3]};
+            group_sum(tree, v);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                if (lead && v[c] != 0.0f) atomicAdd(row + i + c, v[c]);
+        }
+    }
 }
 
 // Replay.  A ray whose composited intervals all fit the forward's record
@@ -619,22 +741,32 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
     sh_basis<DEG>(ray.dx, ray.dy, ray.dz, Y);
     float T = 1.0f;
     bool finished = !L.active || (gC[0] == 0.f && gC[1] == 0.f && gC[2] == 0.f);
-    if (!finished && recorded != kRecOverflow) {
+    // recorded rays: entry i of every lane at once, so that lanes compositing
+    // the same support at the same rank share one atomic per value
+    const bool replay = !finished && recorded != kRecOverflow;
+    const uint32_t rounds = __reduce_max_sync(0xffffffffu, replay ? recorded : 0u);
 #pragma unroll 1
-        for (uint32_t i = 0; i < recorded; ++i) {
-            const uint32_t *rec = TP.interval_rec + interval_rec_index(TP, w, i);
-            const uint32_t cell = __ldcs(rec);
+    for (uint32_t i = 0; i < rounds; ++i) {
+        const bool valid = replay && i < recorded;
+        uint32_t cell = 0;
+        IntervalGrad G{};
+        if (valid) {
+            const uint32_t chunk =
+                __ldg(TP.rec_table + (size_t)(w >> 5) * TP.rec_chunks + i / kChunkEntries);
+            const uint32_t *rec = rec_entry(TP, chunk, w, i);
+            cell = __ldcs(rec);
             const float dt_raw = __uint_as_float(__ldcs(rec + 32));
             const uint32_t links = __ldcs(rec + 64);
             float cu[3];
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch) cu[ch] = __uint_as_float(__ldcs(rec + 96 + 32 * ch));
             const float dens = __ldg(P.m.density + cell) * 1.0f;
-            splat_interval_grad<DEG>(TP, ray, r, depth, Y, cell, dens, dt_raw, links, cu, Ch, Cl,
-                                     gC, T, Ph, Pl);
+            G = splat_interval_terms<DEG>(TP, ray, r, depth, cell, dens, dt_raw, links, cu, Ch,
+                                          Cl, gC, T, Ph, Pl);
         }
-        finished = true;
+        scatter_interval_warp<DEG>(TP, Y, valid, cell, G);
     }
+    if (replay) finished = true;
     uint32_t steps = 0, clipped = 0, nodes_visited = 0;
     bool cursor_valid = false;
     float cur_t = 0.f;
@@ -664,8 +796,10 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
             load_sh_row<DEG, BF16>(P.m, cell, coef);
             float cu[3];
             eval_sh<DEG>(coef, ray.dx, ray.dy, ray.dz, cu[0], cu[1], cu[2]);
-            splat_interval_grad<DEG>(TP, ray, r, depth, Y, cell, dens, __uint_as_float(e.pos),
-                                     e.aux, cu, Ch, Cl, gC, T, Ph, Pl);
+            const IntervalGrad G =
+                splat_interval_terms<DEG>(TP, ray, r, depth, cell, dens, __uint_as_float(e.pos),
+                                          e.aux, cu, Ch, Cl, gC, T, Ph, Pl);
+            scatter_interval<DEG>(TP, Y, cell, G);
         }
         if (finished) continue;
         if (count < kSplatWindow) {
@@ -768,8 +902,10 @@ struct bv_splat_tracer {
     // training scratch
     RayState *ray_state = nullptr;
     size_t ray_state_capacity = 0;
-    uint32_t *interval_rec = nullptr;  // training forward's composited intervals
-    size_t interval_rec_capacity = 0;  // words
+    uint32_t *rec_pool = nullptr;      // training forward's interval-record chunks
+    size_t rec_pool_chunks = 0;
+    uint32_t *rec_table = nullptr;     // chunk of each (tile, chunk rank), then the pool counter
+    size_t rec_table_words = 0;
     uint32_t rec_entries = kSplatRecEntries;
     float4 *site_grads = nullptr;    // [N], kept zero between calls
     void *sh = nullptr;
@@ -809,7 +945,8 @@ void free_splat(bv_splat_tracer *t) {
     cudaFree(t->offsets);
     cudaFree(t->neighbors);
     cudaFree(t->ray_state);
-    cudaFree(t->interval_rec);
+    cudaFree(t->rec_pool);
+    cudaFree(t->rec_table);
     cudaFree(t->site_grads);
     cudaFree(t->density);
     cudaFree(t->sh);
@@ -1105,9 +1242,10 @@ bv_status bv_powerfoam_splat_tracer_set_interval_record(bv_splat_tracer *t, uint
     if (!t) return sp_fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
     t->rec_entries = entries;
     if (entries == 0) {
-        cudaFree(t->interval_rec);
-        t->interval_rec = nullptr;
-        t->interval_rec_capacity = 0;
+        cudaFree(t->rec_pool);
+        cudaFree(t->rec_table);
+        t->rec_pool = t->rec_table = nullptr;
+        t->rec_pool_chunks = t->rec_table_words = 0;
     }
     return BV_OK;
 }
@@ -1167,26 +1305,38 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         t->ray_state_capacity = chunk_rays;
     }
     // interval record: up to rec_entries composited intervals of every ray,
-    // within kSplatRecBytes (rays with more are traversed again)
-    uint32_t rec_entries = 0;
+    // in chunks from a pool of at most kSplatRecBytes (rays beyond either
+    // limit are traversed again by the replay)
+    uint32_t rec_chunks = 0;
+    size_t tiles = 0;
     {
         const size_t chunk_work =
             (size_t)std::min<uint32_t>(n_cams, kMaxViewsPerLaunch) * tile_padded_rays(width, height);
-        const size_t fit = kSplatRecBytes / (chunk_work * kRecWords * sizeof(uint32_t));
-        rec_entries = (uint32_t)std::min<size_t>({(size_t)t->rec_entries, (size_t)ts->max_steps, fit});
-        const size_t need = chunk_work * rec_entries * kRecWords;
-        if (rec_entries > 0 && need > t->interval_rec_capacity) {
-            cudaFree(t->interval_rec);
-            t->interval_rec = nullptr;
-            t->interval_rec_capacity = 0;
-            if (cudaMalloc(&t->interval_rec, need * sizeof(uint32_t)) == cudaSuccess) {
-                t->interval_rec_capacity = need;
+        tiles = chunk_work / 32;
+        const uint32_t entries = std::min<uint32_t>(t->rec_entries, ts->max_steps);
+        rec_chunks = (entries + kChunkEntries - 1) / kChunkEntries;
+        const size_t pool = std::min<size_t>(kSplatRecBytes / (kChunkWords * sizeof(uint32_t)),
+                                             tiles * rec_chunks);
+        const size_t table = tiles * rec_chunks + 1;
+        bool ok = rec_chunks > 0;
+        if (ok && (pool > t->rec_pool_chunks || table > t->rec_table_words)) {
+            cudaFree(t->rec_pool);
+            cudaFree(t->rec_table);
+            t->rec_pool = t->rec_table = nullptr;
+            t->rec_pool_chunks = t->rec_table_words = 0;
+            if (cudaMalloc(&t->rec_pool, pool * kChunkWords * sizeof(uint32_t)) == cudaSuccess &&
+                cudaMalloc(&t->rec_table, table * sizeof(uint32_t)) == cudaSuccess) {
+                t->rec_pool_chunks = pool;
+                t->rec_table_words = table;
             } else {
                 (void)cudaGetLastError();  // out of memory: the replay traverses
-                t->interval_rec = nullptr;
-                rec_entries = 0;
+                cudaFree(t->rec_pool);
+                cudaFree(t->rec_table);
+                t->rec_pool = t->rec_table = nullptr;
+                ok = false;
             }
         }
+        if (!ok) rec_chunks = 0;
     }
     t->last_launches = 0;
     t->last_has_stats = t->stats_enabled;
@@ -1229,8 +1379,17 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         p.d_density = grads->d_density_dev;
         p.d_sh = grads->d_sh_dev;
         p.d_site = want_site ? t->site_grads : nullptr;
-        p.interval_rec = rec_entries ? t->interval_rec : nullptr;
-        p.rec_entries = rec_entries;
+        if (rec_chunks) {
+            const size_t words = tiles * rec_chunks;
+            SP_CUDA(cudaMemsetAsync(t->rec_table, 0xff, words * sizeof(uint32_t), s), "record reset");
+            SP_CUDA(cudaMemsetAsync(t->rec_table + words, 0, sizeof(uint32_t), s), "record reset");
+            p.rec_pool = t->rec_pool;
+            p.rec_table = t->rec_table;
+            p.rec_next = t->rec_table + words;
+            p.rec_chunks = rec_chunks;
+            p.rec_limit = std::min<uint32_t>(t->rec_entries, ts->max_steps);
+            p.pool_chunks = (uint32_t)std::min<size_t>(t->rec_pool_chunks, 0xfffffff0u);
+        }
         SP_CUDA(launch_splat_train(p, false, s), "splat training forward launch");
         p.base.stats = nullptr;
         SP_CUDA(launch_splat_train(p, true, s), "splat training backward launch");

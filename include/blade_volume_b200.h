@@ -391,11 +391,12 @@ bv_status bv_powerfoam_splat_tracer_enable_stats(bv_splat_tracer *tracer, uint32
 bv_status bv_powerfoam_splat_tracer_last_stats(bv_splat_tracer *tracer, bv_launch_stats *out);
 /* Training (bv_powerfoam_splat_tracer_forward_backward): the forward records
  * up to `entries` composited intervals per ray (cell, length, entry / exit
- * planes, unclamped colour: 24 bytes each, at most 12 GiB per launch of 32
- * views) and the replay walks that list instead of traversing the BVH and
- * clipping Cech rows again; rays with more intervals are traversed again.
- * Default 128; 0 disables the record.  Results are identical for every
- * setting.  No reference counterpart. */
+ * planes, unclamped colour: 24 bytes each, in 12 KiB chunks per 8x4 pixel
+ * tile taken as the tile's rays need them, from a pool of at most 12 GiB)
+ * and the replay walks that list instead of traversing the BVH and clipping
+ * Cech rows again; rays past either limit are traversed again.  Default
+ * 1024; 0 disables the record.  Results are identical for every setting.
+ * No reference counterpart. */
 bv_status bv_powerfoam_splat_tracer_set_interval_record(bv_splat_tracer *tracer, uint32_t entries);
 /* Forward + loss + backward with splat semantics: the training recorder's
  * PowerFoam splats (record_powerfoam_splats_jacobians, trace.rs:1421-1452;

@@ -67,9 +67,10 @@ def test_splat_gradients_match_fp64_oracle(bf16, radius_max):
 
 # The replay walks the forward's recorded intervals of a ray when they all
 # fit and traverses the BVH again otherwise: no record, a record of two
-# intervals (rays split between both paths within a warp) and the default
-# all give the oracle's results.
-@pytest.mark.parametrize("entries", [0, 2])
+# intervals (rays split between both paths within a warp), one of twenty
+# (records spanning two 16-interval chunks) and the default all give the
+# oracle's results.
+@pytest.mark.parametrize("entries", [0, 2, 20])
 def test_interval_record_lengths_match_oracle(entries):
     m, cams, target = case(seed=8, n=3000)
     g = run_gpu(m, cams, target, interval_record=entries)
