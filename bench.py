@@ -805,9 +805,10 @@ def main():
     b_step = 8 + deg * 20 + sh_row
     b_atomic = 2 * (4 + 4 * 3 * K + 3 * 12)
     bwd_bytes = steps_per_launch * (b_step + b_atomic)
-    # this design's replay reads the forward's recorded exit face (4 B) and
-    # that one 32-byte face entry instead of the cell's CSR row
-    bwd_design_bytes = steps_per_launch * (4 + 32 + sh_row + b_atomic)
+    # this design's replay reads the forward's step record (exit face and
+    # unclamped colour, 16 B) and that one 32-byte face entry instead of the
+    # cell's CSR row and SH row
+    bwd_design_bytes = steps_per_launch * (16 + 32 + b_atomic)
     fwd_bytes = steps_per_launch * b_step + rays * 12
     kms_b = statistics.median(bwd_k_ms)
     kms_f = statistics.median(fwd_k_ms)
@@ -852,9 +853,11 @@ def main():
                      "design_bytes_per_launch": bwd_design_bytes,
                      "design_frac": bwd_design_bytes / (kms_b * 1e-3) / 1e9 / peak,
                      "note": ("achieved uses the reference's per-step byte model, whose "
-                              "replay re-reads the cell's CSR row; this replay reads the "
-                              "forward's recorded exit face instead (design_bytes), and the "
-                              "scene working set is largely L2-resident; see profiles/")},
+                              "replay re-reads the cell's CSR row and SH row; this replay "
+                              "reads the forward's 16-byte step record instead "
+                              "(design_bytes), and the scene working set and the gradient "
+                              "atomics are largely L2-resident (traffic = DRAM bytes); "
+                              "see profiles/")},
         "kernels": {"train_forward_kernel": {"ms": kms_f, "alg_gbs": fwd_bytes / (kms_f * 1e-3) / 1e9},
                     "train_backward_kernel": {"ms": kms_b, "alg_gbs": achieved},
                     "adam (4 kernels)": {"ms": opt_ms, "alg_gbs": adam_bytes / (opt_ms * 1e-3) / 1e9}},
