@@ -34,8 +34,20 @@
 namespace bv {
 namespace {
 
+// Tuning knobs (measured on B200, 1M-site mixture at 4 x 1024^2): keys per
+// lane per window pass (8 and 12 were slower than 16: more passes over the
+// BVH) and the resident blocks per SM requested for the render kernel (4:
+// 128 registers, 19.4 Mrays/s; without the bound 162 registers, 16.3).  The
+// training kernels keep the allocator's choice (capping them at 128
+// registers spills and is no faster).
+#ifndef BV_SPLAT_WINDOW
+#define BV_SPLAT_WINDOW 16
+#endif
+#ifndef BV_MINB_SPLAT
+#define BV_MINB_SPLAT 4
+#endif
 constexpr int kSplatBlock = 128;
-constexpr int kSplatWindow = 16;
+constexpr int kSplatWindow = BV_SPLAT_WINDOW;
 constexpr int kSplatStack = 80;  // > BVH depth, checked at tracer creation
 // Entry / exit plane of an interval as an offset in its Cech row (16 bits
 // each in the key; rows are at most 65,534 entries, checked at creation).
@@ -233,7 +245,7 @@ __device__ __forceinline__ SplatLane splat_lane(const Params &P, uint32_t w) {
 }
 
 template <int DEG, bool BF16>
-__global__ void __launch_bounds__(kSplatBlock)
+__global__ void __launch_bounds__(kSplatBlock, BV_MINB_SPLAT)
 splat_kernel(const __grid_constant__ SplatParams P) {
     // A view's work is whole 8x4 tiles, so a warp is one tile of one view;
     // whole warps past the end leave together, lanes of a partial edge tile
