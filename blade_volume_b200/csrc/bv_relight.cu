@@ -25,6 +25,13 @@ namespace bv {
 namespace {
 
 constexpr int kRelightBlock = 128;
+// resident blocks per SM requested from the register allocator (unset: the
+// allocator's choice, 128 registers)
+#ifdef BV_MINB_RELIGHT
+#define BV_RELIGHT_BOUNDS __launch_bounds__(kRelightBlock, BV_MINB_RELIGHT)
+#else
+#define BV_RELIGHT_BOUNDS __launch_bounds__(kRelightBlock)
+#endif
 constexpr int kWindow = 16;
 
 // qrot (common.wgsl:386-390)
@@ -122,7 +129,7 @@ __device__ __forceinline__ void shade_light(const RelightLight &L, float px, flo
     ab += outb;
 }
 
-__global__ void __launch_bounds__(kRelightBlock)
+__global__ void BV_RELIGHT_BOUNDS
 relight_kernel(const __grid_constant__ RelightParams P) {
     // whole warps past the last tile leave together; lanes of a partial edge
     // tile stay (inactive) because the traversal is warp-cooperative
