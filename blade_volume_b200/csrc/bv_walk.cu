@@ -41,6 +41,9 @@ constexpr int kWalkBlock = 256;
 #ifndef BV_MINB_TRAIN_BWD
 #define BV_MINB_TRAIN_BWD 3
 #endif
+#ifndef BV_REC_PREFETCH
+#define BV_REC_PREFETCH 1
+#endif
 constexpr int kFaceUnroll = BV_FACE_UNROLL;
 
 
@@ -641,6 +644,17 @@ train_backward_kernel(const __grid_constant__ TrainParams P) {
                     bool has_exit;
                     const uint32_t rec = step_rec_index(P, W.work, W.steps - 1);
                     if (rec != kNotRecorded) {
+#if BV_REC_PREFETCH
+                        // the record streams from DRAM: start the next
+                        // step's four lines on their way to L2 now
+                        if (W.steps < P.rec_steps) {
+                            const uint32_t *nx =
+                                P.step_rec + step_rec_index(P, W.work, W.steps);
+#pragma unroll
+                            for (int f = 0; f < 4; ++f)
+                                asm volatile("prefetch.global.L2 [%0];" ::"l"(nx + 32 * f));
+                        }
+#endif
                         // the forward's exit face of this step: one entry
                         // instead of the cell's row
                         const uint32_t face = __ldcs(P.step_rec + rec);
