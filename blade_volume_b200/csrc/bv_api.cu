@@ -111,9 +111,9 @@ struct bv_tracer {
     size_t ray_state_capacity = 0;
     bool ray_state_owned = true;       // false: lent by a serving engine
     float4 *site_grads = nullptr;      // [N] site gradient accumulator (kept zero)
-    uint32_t *exit_rec = nullptr;      // training forward's step record, read by the replay
-    size_t exit_rec_capacity = 0;      // words
-    uint32_t exit_rec_steps = kExitRecSteps;  // recorded steps per ray
+    uint32_t *step_rec = nullptr;      // training forward's step record, read by the replay
+    size_t step_rec_capacity = 0;      // words
+    uint32_t step_rec_steps = kExitRecSteps;  // recorded steps per ray
     int grid_forward = 0;
     int grid_train_fwd = 0;
     int grid_train_bwd = 0;
@@ -154,7 +154,7 @@ void free_tracer(bv_tracer *t) {
     cudaFree(t->faces);
     if (t->ray_state_owned) cudaFree(t->ray_state);
     cudaFree(t->site_grads);
-    cudaFree(t->exit_rec);
+    cudaFree(t->step_rec);
     cudaFree(t->start_cells);
     cudaFree(t->work_counter);
     cudaFree(t->stats);
@@ -527,11 +527,11 @@ bv_status bv_radfoam_tracer_set_tie_break(bv_tracer *t, uint32_t mode) {
 
 bv_status bv_radfoam_tracer_set_exit_record(bv_tracer *t, uint32_t steps) {
     if (!t) return fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
-    t->exit_rec_steps = steps;
+    t->step_rec_steps = steps;
     if (steps == 0) {
-        cudaFree(t->exit_rec);
-        t->exit_rec = nullptr;
-        t->exit_rec_capacity = 0;
+        cudaFree(t->step_rec);
+        t->step_rec = nullptr;
+        t->step_rec_capacity = 0;
     }
     return BV_OK;
 }
@@ -658,17 +658,17 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         const size_t chunk_work =
             (size_t)std::min<uint32_t>(n_cams, kMaxViewsPerLaunch) * padded_rays(width, height);
         const size_t fit = kExitRecBytes / (chunk_work * kStepRecWords * sizeof(uint32_t));
-        rec_steps = (uint32_t)std::min<size_t>({(size_t)t->exit_rec_steps, (size_t)ts->max_steps, fit});
+        rec_steps = (uint32_t)std::min<size_t>({(size_t)t->step_rec_steps, (size_t)ts->max_steps, fit});
         const size_t need = chunk_work * rec_steps * kStepRecWords;
-        if (rec_steps > 0 && need > t->exit_rec_capacity) {
-            cudaFree(t->exit_rec);
-            t->exit_rec = nullptr;
-            t->exit_rec_capacity = 0;
-            if (cudaMalloc(&t->exit_rec, need * sizeof(uint32_t)) == cudaSuccess) {
-                t->exit_rec_capacity = need;
+        if (rec_steps > 0 && need > t->step_rec_capacity) {
+            cudaFree(t->step_rec);
+            t->step_rec = nullptr;
+            t->step_rec_capacity = 0;
+            if (cudaMalloc(&t->step_rec, need * sizeof(uint32_t)) == cudaSuccess) {
+                t->step_rec_capacity = need;
             } else {
                 (void)cudaGetLastError();  // out of memory: replay searches
-                t->exit_rec = nullptr;
+                t->step_rec = nullptr;
                 rec_steps = 0;
             }
         }
@@ -708,7 +708,7 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         p.d_site = (grads->d_positions_dev || grads->d_radii_dev) ? t->site_grads : nullptr;
         p.loss = loss;
         p.stats = t->stats_enabled ? t->stats : nullptr;
-        p.step_rec = rec_steps ? t->exit_rec : nullptr;
+        p.step_rec = rec_steps ? t->step_rec : nullptr;
         p.rec_steps = rec_steps;
         BV_CUDA(cudaMemsetAsync(t->work_counter, 0, 2 * sizeof(uint32_t), s), "counter reset");
         const int blocks_needed = std::max((int)((work + 255) / 256), 1);
