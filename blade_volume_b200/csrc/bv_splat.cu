@@ -918,6 +918,8 @@ struct bv_splat_tracer {
     size_t rec_pool_chunks = 0;
     uint32_t *rec_table = nullptr;     // chunk of each (tile, chunk rank), then the pool counter
     size_t rec_table_words = 0;
+    uint32_t *rec_demand = nullptr;    // pinned: the pool counter after the last forward
+    cudaEvent_t rec_event = nullptr;   // that copy has landed
     uint32_t rec_entries = kSplatRecEntries;
     float4 *site_grads = nullptr;    // [N], kept zero between calls
     void *sh = nullptr;
@@ -959,6 +961,8 @@ void free_splat(bv_splat_tracer *t) {
     cudaFree(t->ray_state);
     cudaFree(t->rec_pool);
     cudaFree(t->rec_table);
+    cudaFreeHost(t->rec_demand);
+    if (t->rec_event) cudaEventDestroy(t->rec_event);
     cudaFree(t->site_grads);
     cudaFree(t->density);
     cudaFree(t->sh);
@@ -1317,8 +1321,11 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         t->ray_state_capacity = chunk_rays;
     }
     // interval record: up to rec_entries composited intervals of every ray,
-    // in chunks from a pool of at most kSplatRecBytes (rays beyond either
-    // limit are traversed again by the replay)
+    // in chunks from a pool (rays beyond the limit, or finding the pool
+    // empty, are traversed again by the replay).  The pool starts at two
+    // chunks per tile and grows to twice the demand the previous call
+    // reported (the allocation counter, copied back after each forward),
+    // up to kSplatRecBytes.
     uint32_t rec_chunks = 0;
     size_t tiles = 0;
     {
@@ -1327,10 +1334,27 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         tiles = chunk_work / 32;
         const uint32_t entries = std::min<uint32_t>(t->rec_entries, ts->max_steps);
         rec_chunks = (entries + kChunkEntries - 1) / kChunkEntries;
-        const size_t pool = std::min<size_t>(kSplatRecBytes / (kChunkWords * sizeof(uint32_t)),
-                                             tiles * rec_chunks);
+        const size_t cap = std::min<size_t>(kSplatRecBytes / (kChunkWords * sizeof(uint32_t)),
+                                            tiles * rec_chunks);
+        size_t pool = std::min<size_t>(cap, tiles * 2);
+        if (t->rec_event) {
+            const cudaError_t q = cudaEventQuery(t->rec_event);
+            if (q == cudaSuccess && *t->rec_demand > t->rec_pool_chunks)
+                pool = std::min<size_t>(cap, std::max<size_t>(pool, 2 * (size_t)*t->rec_demand));
+            else if (q == cudaErrorNotReady)
+                (void)cudaGetLastError();  // still in flight: keep the current pool
+        }
         const size_t table = tiles * rec_chunks + 1;
         bool ok = rec_chunks > 0;
+        if (ok && !t->rec_demand) {
+            if (cudaMallocHost(&t->rec_demand, sizeof(uint32_t)) != cudaSuccess ||
+                cudaEventCreateWithFlags(&t->rec_event, cudaEventDisableTiming) != cudaSuccess) {
+                (void)cudaGetLastError();
+                ok = false;
+            } else {
+                *t->rec_demand = 0;
+            }
+        }
         if (ok && (pool > t->rec_pool_chunks || table > t->rec_table_words)) {
             cudaFree(t->rec_pool);
             cudaFree(t->rec_table);
@@ -1403,6 +1427,11 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
             p.pool_chunks = (uint32_t)std::min<size_t>(t->rec_pool_chunks, 0xfffffff0u);
         }
         SP_CUDA(launch_splat_train(p, false, s), "splat training forward launch");
+        if (rec_chunks) {
+            SP_CUDA(cudaMemcpyAsync(t->rec_demand, p.rec_next, sizeof(uint32_t),
+                                    cudaMemcpyDeviceToHost, s), "record demand");
+            SP_CUDA(cudaEventRecord(t->rec_event, s), "event");
+        }
         p.base.stats = nullptr;
         SP_CUDA(launch_splat_train(p, true, s), "splat training backward launch");
         t->last_launches += 2;

@@ -392,7 +392,8 @@ bv_status bv_powerfoam_splat_tracer_last_stats(bv_splat_tracer *tracer, bv_launc
 /* Training (bv_powerfoam_splat_tracer_forward_backward): the forward records
  * up to `entries` composited intervals per ray (cell, length, entry / exit
  * planes, unclamped colour: 24 bytes each, in 12 KiB chunks per 8x4 pixel
- * tile taken as the tile's rays need them, from a pool of at most 12 GiB)
+ * tile taken as the tile's rays need them, from a pool that starts at two
+ * chunks per tile and grows after a call that ran it dry, up to 12 GiB)
  * and the replay walks that list instead of traversing the BVH and clipping
  * Cech rows again; rays past either limit are traversed again.  Default
  * 1024; 0 disables the record.  Results are identical for every setting.
