@@ -46,6 +46,9 @@ namespace {
 #ifndef BV_MINB_SPLAT
 #define BV_MINB_SPLAT 4
 #endif
+#ifndef BV_SPLAT_SHARED_NUM
+#define BV_SPLAT_SHARED_NUM 1
+#endif
 constexpr int kSplatBlock = 128;
 constexpr int kSplatWindow = BV_SPLAT_WINDOW;
 constexpr int kSplatStack = 80;  // > BVH depth, checked at tracer creation
@@ -135,16 +138,29 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
             fp = __ldg(&P.row_faces[base + lane].point);
             fn = __ldg(&P.row_faces[base + lane].normal);
         }
+#if BV_SPLAT_SHARED_NUM
+        // The warp's rays share one camera origin, so <p - o, n> of an entry
+        // is the same in every lane: the lane that loaded it evaluates it
+        // (the same operations each lane would apply) and broadcasts it
+        // with the normal.
+        const float num_own = dot3(fp.x - ray.ox, fp.y - ray.oy, fp.z - ray.oz, fn.x, fn.y, fn.z);
+#endif
         for (uint32_t j = 0; j < n; ++j) {
+#if BV_SPLAT_SHARED_NUM
+            const float num = __shfl_sync(0xffffffffu, num_own, j);
+#else
             const float fx = __shfl_sync(0xffffffffu, fp.x, j);
             const float fy = __shfl_sync(0xffffffffu, fp.y, j);
             const float fz = __shfl_sync(0xffffffffu, fp.z, j);
+#endif
             const float nx = __shfl_sync(0xffffffffu, fn.x, j);
             const float ny = __shfl_sync(0xffffffffu, fn.y, j);
             const float nz = __shfl_sync(0xffffffffu, fn.z, j);
             if (empty) continue;
+#if !BV_SPLAT_SHARED_NUM
             const float rx = fx - ray.ox, ry = fy - ray.oy, rz = fz - ray.oz;
             const float num = dot3(rx, ry, rz, nx, ny, nz);
+#endif
             const float den = dot3(ray.dx, ray.dy, ray.dz, nx, ny, nz);
             if (den > 1.0e-20f) {
                 const float t = num / den;
@@ -232,9 +248,11 @@ __device__ __forceinline__ SplatLane splat_lane(const Params &P, uint32_t w) {
     L.inside = L.x < L.vd->width && L.y < L.vd->height;
     L.r0 = Ray{0.f, 0.f, 0.f, 1.f, 0.f, 0.f};
     L.active = L.inside && make_ray(*L.vd, L.x, L.y, L.r0);
-    L.ray.ox = L.r0.ox;
-    L.ray.oy = L.r0.oy;
-    L.ray.oz = L.r0.oz;
+    // every lane, inside the image or not, carries its view's camera origin
+    // (make_ray's own value for the active ones), which the clip relies on
+    L.ray.ox = L.vd->origin[0];
+    L.ray.oy = L.vd->origin[1];
+    L.ray.oz = L.vd->origin[2];
     L.ray.dx = L.active ? L.r0.dx : 1.0f;
     L.ray.dy = L.active ? L.r0.dy : 0.0f;
     L.ray.dz = L.active ? L.r0.dz : 0.0f;
