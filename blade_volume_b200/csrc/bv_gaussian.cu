@@ -38,6 +38,12 @@ constexpr int kGaussBlock = 128;
 #ifndef BV_MINB_GAUSS
 #define BV_MINB_GAUSS 4
 #endif
+// Per-view table of each particle's camera-origin terms (local origin and
+// squared distance), formed once per dispatch instead of in every lane for
+// every candidate test.
+#ifndef BV_GAUSS_LOCAL
+#define BV_GAUSS_LOCAL 1
+#endif
 constexpr int kWindow = 16;
 constexpr int kStack = 64;
 
@@ -50,6 +56,7 @@ struct __align__(16) GaussShPrim {
 
 struct GaussianParams {
     const GaussShPrim *prims;
+    const float4 *local;  // per table position, for this view's camera: R^-1 (o - mu) / s, |mu - o|^2
     const uint32_t *ids;  // filtered model index per table position
     const BvhNode *nodes;
     const float *sh;      // [n][sh_stride] in table order
@@ -84,10 +91,15 @@ __device__ __forceinline__ float3 gqrot(float4 q, float vx, float vy, float vz) 
 // sqrt(cut) * max(scale) of the mean; rays passing farther from the mean than
 // that (with a margin for the rounding of |oc|^2 - b^2) cannot hit.  d is unit.
 __device__ __forceinline__ bool support_sphere_hit(const float4 &co, const float4 &sc,
-                                                   const WinRay &r) {
+                                                   const float4 &local, const WinRay &r) {
     const float ox = co.x - r.ox, oy = co.y - r.oy, oz = co.z - r.oz;
     const float b = gdot(ox, oy, oz, r.dx, r.dy, r.dz);
+#if BV_GAUSS_LOCAL
+    const float oo = local.w;
+#else
+    (void)local;
     const float oo = gdot(ox, oy, oz, ox, oy, oz);
+#endif
     const float smax = fmaxf(fmaxf(sc.x, sc.y), sc.z);
     const float r2 = sc.w * (smax * smax);
     return oo - b * b <= r2 * 1.001f + 1e-6f * oo + 1e-30f;
@@ -99,11 +111,20 @@ __device__ __forceinline__ bool response(const GaussianParams &P, uint32_t pos, 
                                          float &t_out, float &alpha_out) {
     const float4 co = __ldg(&P.prims[pos].center_opacity);
     const float4 sc = __ldg(&P.prims[pos].scale_cut);
-    if (!support_sphere_hit(co, sc, r)) return false;
+#if BV_GAUSS_LOCAL
+    const float4 local = __ldg(&P.local[pos]);
+#else
+    const float4 local = make_float4(0.f, 0.f, 0.f, 0.f);
+#endif
+    if (!support_sphere_hit(co, sc, local, r)) return false;
     const float4 qi = __ldg(&P.prims[pos].qinv);
-    const float3 lo0 = gqrot(qi, r.ox - co.x, r.oy - co.y, r.oz - co.z);
     const float3 ld0 = gqrot(qi, r.dx, r.dy, r.dz);
+#if BV_GAUSS_LOCAL
+    const float lox = local.x, loy = local.y, loz = local.z;
+#else
+    const float3 lo0 = gqrot(qi, r.ox - co.x, r.oy - co.y, r.oz - co.z);
     const float lox = lo0.x / sc.x, loy = lo0.y / sc.y, loz = lo0.z / sc.z;
+#endif
     const float ldx = ld0.x / sc.x, ldy = ld0.y / sc.y, ldz = ld0.z / sc.z;
     const float t = -gdot(lox, loy, loz, ldx, ldy, ldz) / gdot(ldx, ldy, ldz, ldx, ldy, ldz);
     if (!(t > 0.0f && t < P.depth)) return false;
@@ -217,7 +238,32 @@ __global__ void __launch_bounds__(kGaussBlock, BV_MINB_GAUSS) gaussian_kernel(co
     }
 }
 
-cudaError_t launch_gaussian(const GaussianParams &p, uint32_t deg, cudaStream_t s) {
+// The camera-origin terms of every particle for one view, with the
+// operations response() and support_sphere_hit() would apply per lane.
+__global__ void __launch_bounds__(256) gauss_local_kernel(const GaussShPrim *prims, uint32_t n,
+                                                          float ox, float oy, float oz,
+                                                          float4 *local) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 co = __ldg(&prims[i].center_opacity);
+    const float4 sc = __ldg(&prims[i].scale_cut);
+    const float4 qi = __ldg(&prims[i].qinv);
+    const float3 lo0 = gqrot(qi, ox - co.x, oy - co.y, oz - co.z);
+    const float cx = co.x - ox, cy = co.y - oy, cz = co.z - oz;
+    local[i] = make_float4(lo0.x / sc.x, lo0.y / sc.y, lo0.z / sc.z, gdot(cx, cy, cz, cx, cy, cz));
+}
+
+cudaError_t launch_gaussian(const GaussianParams &p, uint32_t n, uint32_t deg, cudaStream_t s) {
+#if BV_GAUSS_LOCAL
+    if (n) {
+        gauss_local_kernel<<<(n + 255) / 256, 256, 0, s>>>(p.prims, n, p.origin[0], p.origin[1],
+                                                           p.origin[2], const_cast<float4 *>(p.local));
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+#else
+    (void)n;
+#endif
     const int blocks = (int)((p.total_work + kGaussBlock - 1) / kGaussBlock);
     if (blocks == 0) return cudaSuccess;
     switch (deg) {
@@ -239,6 +285,7 @@ struct bv_gaussian_tracer {
     float min_opacity = 0.01f, min_transmittance = 0.01f;
     float background[3] = {0.f, 0.f, 0.f};
     GaussShPrim *prims = nullptr;
+    float4 *local = nullptr;  // per-view camera-origin terms, refilled by each dispatch
     uint32_t *ids = nullptr;
     BvhNode *nodes = nullptr;
     float *sh = nullptr;
@@ -257,6 +304,7 @@ bv_status gfail(bv_status code, const char *msg) {
 void free_gaussian(bv_gaussian_tracer *t) {
     if (!t) return;
     cudaFree(t->prims);
+    cudaFree(t->local);
     cudaFree(t->ids);
     cudaFree(t->nodes);
     cudaFree(t->sh);
@@ -407,6 +455,7 @@ bv_status bv_gaussian_tracer_new(const bv_gaussian_sh_desc *g,
         if (e_ != cudaSuccess) return cleanup(e_, what); \
     } while (0)
     BV_GTRY(cudaMalloc(&t->prims, sizeof(GaussShPrim) * kept), "cudaMalloc particles");
+    BV_GTRY(cudaMalloc(&t->local, sizeof(float4) * kept), "cudaMalloc particle origin terms");
     BV_GTRY(cudaMalloc(&t->ids, sizeof(uint32_t) * kept), "cudaMalloc ids");
     BV_GTRY(cudaMalloc(&t->nodes, sizeof(BvhNode) * t->n_nodes), "cudaMalloc nodes");
     BV_GTRY(cudaMalloc(&t->sh, sizeof(float) * sh.size()), "cudaMalloc SH");
@@ -459,6 +508,7 @@ bv_status bv_gaussian_tracer_dispatch(bv_gaussian_tracer *t, float *out_rgba_dev
     GaussianParams p;
     std::memset(&p, 0, sizeof(p));
     p.prims = t->prims;
+    p.local = t->local;
     p.ids = t->ids;
     p.nodes = t->nodes;
     p.sh = t->sh;
@@ -488,7 +538,7 @@ bv_status bv_gaussian_tracer_dispatch(bv_gaussian_tracer *t, float *out_rgba_dev
             cudaEventRecord(t->ev[0], s) != cudaSuccess)
             return gfail(BV_ERR_CUDA, "stats setup failed");
     }
-    cudaError_t e = launch_gaussian(p, t->sh_degree, s);
+    cudaError_t e = launch_gaussian(p, t->n_kept, t->sh_degree, s);
     if (e != cudaSuccess) {
         set_last_error(cudaGetErrorString(e));
         return BV_ERR_CUDA;
@@ -507,7 +557,7 @@ bv_status bv_gaussian_tracer_enable_stats(bv_gaussian_tracer *t, uint32_t enable
 bv_status bv_gaussian_tracer_last_stats(bv_gaussian_tracer *t, bv_launch_stats *out) {
     if (!t || !out) return gfail(BV_ERR_INVALID_ARGUMENT, "null argument");
     std::memset(out, 0, sizeof(*out));
-    out->launches = 1;
+    out->launches = BV_GAUSS_LOCAL ? 2 : 1;
     if (!t->last_has_stats) return BV_OK;
     if (cudaEventSynchronize(t->ev[1]) != cudaSuccess)
         return gfail(BV_ERR_CUDA, "event sync failed");
