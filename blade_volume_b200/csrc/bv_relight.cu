@@ -45,25 +45,39 @@ __device__ __forceinline__ float3 qrot(float4 q, float vx, float vy, float vz) {
 }
 
 // intersect_surfel, kernel 2 (relight.wgsl:419-441).
-__device__ __forceinline__ bool intersect(const GaussPrim *__restrict__ prims, uint32_t pos,
+__device__ __forceinline__ bool intersect(const GaussPrim *__restrict__ prims,
+                                          const float4 *__restrict__ local_terms, uint32_t pos,
                                           const WinRay &r, float t_end, float &t_out,
                                           float &alpha_out) {
     const float4 co = __ldg(&prims[pos].center_opacity);
     const float4 ss = __ldg(&prims[pos].scale_support);
+#if BV_RELIGHT_LOCAL
+    const float4 local = __ldg(&local_terms[pos]);
+#else
+    (void)local_terms;
+#endif
     {
         // conservative pre-test: a hit lies inside the support ellipsoid, so
         // within support * max(scale) of the mean (d is unit; the margin
         // covers the rounding of |oc|^2 - b^2)
         const float ox = co.x - r.ox, oy = co.y - r.oy, oz = co.z - r.oz;
         const float b = dot3(ox, oy, oz, r.dx, r.dy, r.dz);
+#if BV_RELIGHT_LOCAL
+        const float oo = local.w;
+#else
         const float oo = dot3(ox, oy, oz, ox, oy, oz);
+#endif
         const float smax = fmaxf(fmaxf(ss.x, ss.y), ss.z);
         if (oo - b * b > ss.w * (smax * smax) * 1.001f + 1e-6f * oo + 1e-30f) return false;
     }
     const float4 qi = __ldg(&prims[pos].qinv);
-    const float3 lo0 = qrot(qi, r.ox - co.x, r.oy - co.y, r.oz - co.z);
     const float3 ld0 = qrot(qi, r.dx, r.dy, r.dz);
+#if BV_RELIGHT_LOCAL
+    const float lox = local.x, loy = local.y, loz = local.z;
+#else
+    const float3 lo0 = qrot(qi, r.ox - co.x, r.oy - co.y, r.oz - co.z);
     const float lox = lo0.x / ss.x, loy = lo0.y / ss.y, loz = lo0.z / ss.z;
+#endif
     const float ldx = ld0.x / ss.x, ldy = ld0.y / ss.y, ldz = ld0.z / ss.z;
     const float t = -dot3(lox, loy, loz, ldx, ldy, ldz) / dot3(ldx, ldy, ldz, ldx, ldy, ldz);
     if (t <= 0.0f || t >= t_end) return false;
@@ -174,7 +188,7 @@ relight_kernel(const __grid_constant__ RelightParams P) {
         float &t = k.t;
         uint32_t &id = k.idx;
         float a;
-        if (!mine || !intersect(P.prims, p, ray, t_end, t, a) || !(a > 0.0f)) return false;
+        if (!mine || !intersect(P.prims, P.local, p, ray, t_end, t, a) || !(a > 0.0f)) return false;
         id = __ldg(&P.prims[p].ids.x);
         return true;
     };
@@ -219,7 +233,7 @@ relight_kernel(const __grid_constant__ RelightParams P) {
                 group_T = 1.f;
             }
             float tt, a;
-            intersect(P.prims, h.pos, ray, t_end, tt, a);
+            intersect(P.prims, P.local, h.pos, ray, t_end, tt, a);
             hits_used += 1;
             const float ptx = ray.ox + h.t * ray.dx, pty = ray.oy + h.t * ray.dy,
                         ptz = ray.oz + h.t * ray.dz;
@@ -287,11 +301,34 @@ relight_kernel(const __grid_constant__ RelightParams P) {
     }
 }
 
+// The camera-origin terms of every particle for one view, with the
+// operations intersect() would apply per lane.
+__global__ void __launch_bounds__(256) relight_local_kernel(const GaussPrim *prims, uint32_t n,
+                                                            float ox, float oy, float oz,
+                                                            float4 *local) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 co = __ldg(&prims[i].center_opacity);
+    const float4 ss = __ldg(&prims[i].scale_support);
+    const float4 qi = __ldg(&prims[i].qinv);
+    const float3 lo0 = qrot(qi, ox - co.x, oy - co.y, oz - co.z);
+    const float cx = co.x - ox, cy = co.y - oy, cz = co.z - oz;
+    local[i] = make_float4(lo0.x / ss.x, lo0.y / ss.y, lo0.z / ss.z, dot3(cx, cy, cz, cx, cy, cz));
+}
+
 }  // namespace
 
 cudaError_t launch_relight(const RelightParams &p, cudaStream_t s) {
     const int blocks = (int)((p.total_work + kRelightBlock - 1) / kRelightBlock);
     if (blocks == 0) return cudaSuccess;
+#if BV_RELIGHT_LOCAL
+    if (p.n_prims) {
+        relight_local_kernel<<<(p.n_prims + 255) / 256, 256, 0, s>>>(p.prims, p.n_prims, p.origin[0],
+                                                                     p.origin[1], p.origin[2], p.local);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+#endif
     relight_kernel<<<blocks, kRelightBlock, 0, s>>>(p);
     return cudaGetLastError();
 }

@@ -35,8 +35,17 @@ constexpr int kMaxRelightLights = 64;
 // Traversal stack entries per ray; the BVH depth must stay below it.
 constexpr int kRelightStack = 64;
 
+// Per-view table of each particle's camera-origin terms (local origin and
+// squared distance), formed once per dispatch instead of in every lane for
+// every candidate test.
+#ifndef BV_RELIGHT_LOCAL
+#define BV_RELIGHT_LOCAL 1
+#endif
+
 struct RelightParams {
     const GaussPrim *prims;
+    float4 *local;      // per table position, for this view's camera: R^-1 (o - mu) / s, |mu - o|^2
+    uint32_t n_prims;
     const BvhNode *nodes;
     const RelightMaterial *materials;
     float4 *out;

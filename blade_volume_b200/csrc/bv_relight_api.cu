@@ -21,6 +21,7 @@ struct bv_relight_tracer {
     uint32_t n_nodes = 0;
     uint32_t n_materials = 0;
     GaussPrim *prims = nullptr;
+    float4 *local = nullptr;  // per-view camera-origin terms, refilled by each dispatch
     BvhNode *nodes = nullptr;
     RelightMaterial *materials = nullptr;
     unsigned long long *stats = nullptr;
@@ -41,6 +42,7 @@ bv_status rfail(bv_status code, const char *msg) {
 void free_relight(bv_relight_tracer *t) {
     if (!t) return;
     cudaFree(t->prims);
+    cudaFree(t->local);
     cudaFree(t->nodes);
     cudaFree(t->materials);
     cudaFree(t->stats);
@@ -183,6 +185,7 @@ bv_status bv_relight_tracer_new_gaussian(const bv_gaussian_desc *g,
         if (e_ != cudaSuccess) return cleanup(e_, what); \
     } while (0)
     BV_RTRY(cudaMalloc(&t->prims, sizeof(GaussPrim) * kept), "cudaMalloc particles");
+    BV_RTRY(cudaMalloc(&t->local, sizeof(float4) * kept), "cudaMalloc particle origin terms");
     BV_RTRY(cudaMalloc(&t->nodes, sizeof(BvhNode) * t->n_nodes), "cudaMalloc nodes");
     BV_RTRY(cudaMalloc(&t->materials, sizeof(RelightMaterial) * mats.size()), "cudaMalloc materials");
     BV_RTRY(cudaMalloc(&t->stats, sizeof(unsigned long long) * 4), "cudaMalloc stats");
@@ -255,6 +258,8 @@ bv_status bv_relight_tracer_dispatch(bv_relight_tracer *t, float *out_rgba_dev,
     RelightParams p;
     std::memset(&p, 0, sizeof(p));
     p.prims = t->prims;
+    p.local = t->local;
+    p.n_prims = t->n_kept;
     p.nodes = t->nodes;
     p.materials = t->materials;
     p.out = reinterpret_cast<float4 *>(out_rgba_dev);
@@ -303,7 +308,7 @@ bv_status bv_relight_tracer_enable_stats(bv_relight_tracer *t, uint32_t enabled)
 bv_status bv_relight_tracer_last_stats(bv_relight_tracer *t, bv_launch_stats *out) {
     if (!t || !out) return rfail(BV_ERR_INVALID_ARGUMENT, "null argument");
     std::memset(out, 0, sizeof(*out));
-    out->launches = 1;
+    out->launches = BV_RELIGHT_LOCAL ? 2 : 1;  // origin terms, trace
     if (!t->last_has_stats) return BV_OK;
     if (cudaEventSynchronize(t->ev[1]) != cudaSuccess)
         return rfail(BV_ERR_CUDA, "event sync failed");
