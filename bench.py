@@ -451,7 +451,7 @@ def run_secondary(args):
             "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak,
                          "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
                          "traffic": None, "peak_source": kind},
-            "clocks": clocks}
+            "gpu_launches": max(int(st.launches), 1) * args.steps, "clocks": clocks}
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
