@@ -338,7 +338,10 @@ bv_status bv_relight_tracer_set_point_lights(bv_relight_tracer *tracer,
                                              const bv_point_light *lights, uint32_t n_lights);
 bv_status bv_relight_tracer_set_background(bv_relight_tracer *tracer, const float rgb[3]);
 /* Renders width x height into out_rgba_dev ([h][w][4] float32): radiance +
- * transmittance * background, alpha = 1 - transmittance (relight.wgsl:747-780). */
+ * transmittance * background, alpha = 1 - transmittance (relight.wgsl:747-780).
+ * Two launches: each particle's camera-origin terms into the tracer's
+ * per-view table, then the trace; two dispatches of one tracer must
+ * therefore not overlap on the GPU (one stream per tracer). */
 bv_status bv_relight_tracer_dispatch(bv_relight_tracer *tracer, float *out_rgba_dev,
                                      const bv_camera *camera, uint32_t width, uint32_t height,
                                      bv_stream stream);
@@ -452,7 +455,10 @@ bv_status bv_gaussian_tracer_set_background(bv_gaussian_tracer *tracer, const fl
 /* particles kept (GaussianGpuCloud::num_points) */
 uint32_t bv_gaussian_tracer_num_points(const bv_gaussian_tracer *tracer);
 /* Renders width x height into out_rgba_dev ([h][w][4] float32):
- * (radiance + T * background, 1 - T). */
+ * (radiance + T * background, 1 - T).  Two launches: each particle's
+ * camera-origin terms into the tracer's per-view table, then the trace; two
+ * dispatches of one tracer must therefore not overlap on the GPU (one
+ * stream per tracer). */
 bv_status bv_gaussian_tracer_dispatch(bv_gaussian_tracer *tracer, float *out_rgba_dev,
                                       const bv_camera *camera, uint32_t width, uint32_t height,
                                       bv_stream stream);
