@@ -381,10 +381,47 @@ def containing_points_noalloc(sites, positions, out, stream=None):
     positions without any device allocation.  ``sites`` is a CUDA float32
     tensor [N, 4] (x, y, z, power radius), ``out`` a CUDA int32 tensor with
     room for the indices; ``positions`` host floats [Q, 3]."""
+    import torch
+
     p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+    if sites.dtype != torch.float32 or sites.dim() != 2 or sites.shape[1] != 4:
+        raise ValueError("sites must be a float32 tensor of shape [N, 4]")
+    if not sites.is_contiguous():
+        raise ValueError("sites must be contiguous")
+    if out.dtype != torch.int32 or out.numel() < p.shape[0]:
+        raise ValueError(f"out must be an int32 tensor with at least {p.shape[0]} elements")
+    if not out.is_contiguous():
+        raise ValueError("out must be contiguous")
+    if not sites.is_cuda or not out.is_cuda:
+        raise ValueError("sites and out must be CUDA tensors")
     _check(load_library().bv_containing_points_noalloc(
         C.c_void_p(sites.data_ptr()), sites.shape[0], _fptr(p), p.shape[0],
         C.c_void_p(out.data_ptr()), _stream_handle(stream)))
+
+
+class GradTables(dict):
+    """The gradient tables of a tracer (d_density [N], d_sh [N*3K], d_pos
+    [N*3], d_radius [N]) as views into ONE flat device buffer, ``flat``, so
+    that the data-parallel step sums them with one collective and no copies.
+    d_sh comes first, at the buffer's start, which keeps it 16-byte aligned."""
+
+    flat = None
+
+
+def _grad_tables(n: int, k3: int, radii: bool, device="cuda") -> GradTables:
+    import torch
+
+    sizes = [("d_sh", n * k3), ("d_density", n), ("d_pos", n * 3)]
+    if radii:
+        sizes.append(("d_radius", n))
+    flat = torch.zeros(sum(s for _, s in sizes), dtype=torch.float32, device=device)
+    g = GradTables()
+    off = 0
+    for name, size in sizes:
+        g[name] = flat[off:off + size]
+        off += size
+    g.flat = flat
+    return g
 
 
 def _stream_handle(stream) -> C.c_void_p:
@@ -538,14 +575,7 @@ class RadFoamGpuTracer:
     def new_grads(self):
         import torch
 
-        n = self.model.n
-        K3 = 3 * self.sh_components
-        g = dict(d_density=torch.zeros(n, dtype=torch.float32, device="cuda"),
-                 d_sh=torch.zeros(n * K3, dtype=torch.float32, device="cuda"),
-                 d_pos=torch.zeros(n * 3, dtype=torch.float32, device="cuda"))
-        if self.model.radii is not None:
-            g["d_radius"] = torch.zeros(n, dtype=torch.float32, device="cuda")
-        return g
+        return _grad_tables(self.model.n, 3 * self.sh_components, self.model.radii is not None)
 
     def adam_step(self, grads: dict, lr_density=0.0, lr_sh_dc=0.0, lr_sh_rest=0.0,
                   lr_position=0.0, lr_radius=0.0, beta1=0.9, beta2=0.999, eps=1e-15,
@@ -825,12 +855,7 @@ class PowerFoamSplatTracer:
     def new_grads(self):
         import torch
 
-        n = self.model.n
-        return dict(d_density=torch.zeros(n, dtype=torch.float32, device="cuda"),
-                    d_sh=torch.zeros(n * 3 * self.sh_components, dtype=torch.float32,
-                                     device="cuda"),
-                    d_pos=torch.zeros(n * 3, dtype=torch.float32, device="cuda"),
-                    d_radius=torch.zeros(n, dtype=torch.float32, device="cuda"))
+        return _grad_tables(self.model.n, 3 * self.sh_components, True)
 
     def candidate_stats(self):
         """(max support hits of one ray, total hits, Cech row entries of the

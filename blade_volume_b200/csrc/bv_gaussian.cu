@@ -253,19 +253,23 @@ __global__ void __launch_bounds__(256) gauss_local_kernel(const GaussShPrim *pri
     local[i] = make_float4(lo0.x / sc.x, lo0.y / sc.y, lo0.z / sc.z, gdot(cx, cy, cz, cx, cy, cz));
 }
 
-cudaError_t launch_gaussian(const GaussianParams &p, uint32_t n, uint32_t deg, cudaStream_t s) {
+cudaError_t launch_gaussian(const GaussianParams &p, uint32_t n, uint32_t deg, cudaStream_t s,
+                            uint32_t &launches) {
+    launches = 0;
 #if BV_GAUSS_LOCAL
     if (n) {
         gauss_local_kernel<<<(n + 255) / 256, 256, 0, s>>>(p.prims, n, p.origin[0], p.origin[1],
                                                            p.origin[2], const_cast<float4 *>(p.local));
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
+        launches += 1;
     }
 #else
     (void)n;
 #endif
     const int blocks = (int)((p.total_work + kGaussBlock - 1) / kGaussBlock);
     if (blocks == 0) return cudaSuccess;
+    launches += 1;
     switch (deg) {
         case 0: gaussian_kernel<0><<<blocks, kGaussBlock, 0, s>>>(p); break;
         case 1: gaussian_kernel<1><<<blocks, kGaussBlock, 0, s>>>(p); break;
@@ -292,6 +296,12 @@ struct bv_gaussian_tracer {
     unsigned long long *stats = nullptr;
     bool stats_enabled = false, last_has_stats = false;
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    // The per-view origin table is rewritten by every dispatch: a dispatch on
+    // another stream than the previous one first waits for the previous one.
+    cudaEvent_t done = nullptr;
+    cudaStream_t last_stream = nullptr;
+    bool dispatched = false;
+    uint32_t last_launches = 0;
 };
 
 namespace {
@@ -311,6 +321,7 @@ void free_gaussian(bv_gaussian_tracer *t) {
     cudaFree(t->stats);
     for (auto &e : t->ev)
         if (e) cudaEventDestroy(e);
+    if (t->done) cudaEventDestroy(t->done);
     delete t;
 }
 
@@ -469,6 +480,7 @@ bv_status bv_gaussian_tracer_new(const bv_gaussian_sh_desc *g,
     BV_GTRY(cudaMemcpy(t->sh, sh.data(), sizeof(float) * sh.size(), cudaMemcpyHostToDevice),
             "upload SH");
     for (auto &e : t->ev) BV_GTRY(cudaEventCreate(&e), "cudaEventCreate");
+    BV_GTRY(cudaEventCreateWithFlags(&t->done, cudaEventDisableTiming), "cudaEventCreate");
 #undef BV_GTRY
     *out = t;
     return BV_OK;
@@ -538,11 +550,19 @@ bv_status bv_gaussian_tracer_dispatch(bv_gaussian_tracer *t, float *out_rgba_dev
             cudaEventRecord(t->ev[0], s) != cudaSuccess)
             return gfail(BV_ERR_CUDA, "stats setup failed");
     }
-    cudaError_t e = launch_gaussian(p, t->n_kept, t->sh_degree, s);
+    if (t->dispatched && t->last_stream != s && cudaStreamWaitEvent(s, t->done, 0) != cudaSuccess)
+        return gfail(BV_ERR_CUDA, "stream wait on the previous dispatch failed");
+    uint32_t launches = 0;
+    cudaError_t e = launch_gaussian(p, t->n_kept, t->sh_degree, s, launches);
     if (e != cudaSuccess) {
         set_last_error(cudaGetErrorString(e));
         return BV_ERR_CUDA;
     }
+    t->last_launches = launches;
+    if (cudaEventRecord(t->done, s) != cudaSuccess)
+        return gfail(BV_ERR_CUDA, "event record failed");
+    t->last_stream = s;
+    t->dispatched = true;
     if (t->stats_enabled && cudaEventRecord(t->ev[1], s) != cudaSuccess)
         return gfail(BV_ERR_CUDA, "event record failed");
     return BV_OK;
@@ -557,7 +577,7 @@ bv_status bv_gaussian_tracer_enable_stats(bv_gaussian_tracer *t, uint32_t enable
 bv_status bv_gaussian_tracer_last_stats(bv_gaussian_tracer *t, bv_launch_stats *out) {
     if (!t || !out) return gfail(BV_ERR_INVALID_ARGUMENT, "null argument");
     std::memset(out, 0, sizeof(*out));
-    out->launches = BV_GAUSS_LOCAL ? 2 : 1;
+    out->launches = t->last_launches;
     if (!t->last_has_stats) return BV_OK;
     if (cudaEventSynchronize(t->ev[1]) != cudaSuccess)
         return gfail(BV_ERR_CUDA, "event sync failed");

@@ -12,6 +12,7 @@
 // fixed-size device array below, which every GPU that loads this library
 // holds until the process exits.
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -40,15 +41,25 @@ static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
-NoAllocScratch *g_noalloc_ptr[kMaxDevices] = {};
+// Per device: the context the address was looked up in, and the address.  A
+// cudaDeviceReset (or a primary context torn down and made again) loads the
+// module anew, and the array may then sit elsewhere, so the address is only
+// reused while the current context is the one it was looked up in.
+struct NoAllocSlot {
+    CUcontext ctx;
+    NoAllocScratch *ptr;
+};
+NoAllocSlot g_noalloc_slot[kMaxDevices] = {};
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
 
 bv_status noalloc_fail(bv_status code, const std::string &msg) {
     set_last_error(msg.c_str());  // read back through bv_last_error()
     return code;
 }
 
-// Once per device, with that device current: look up the device address of
-// the scratch array.
+// Once per device and context, with that device current: look up the device
+// address of the scratch array.
 bv_status noalloc_scratch_for_current_device(NoAllocScratch **out) {
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
@@ -57,15 +68,38 @@ bv_status noalloc_scratch_for_current_device(NoAllocScratch **out) {
     if (device < 0 || device >= kMaxDevices)
         return noalloc_fail(BV_ERR_NOT_SUPPORTED, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[device]) {
+    if (!g_ctx_get_current) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+            return noalloc_fail(BV_ERR_CUDA, "cuCtxGetCurrent is not available from the driver");
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+    }
+    // The context the launch will use: the thread's current one, or, when
+    // the runtime has not made one current yet, the device's primary
+    // context (cudaSetDevice initialises it and makes it current).
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS)
+        return noalloc_fail(BV_ERR_CUDA, "cuCtxGetCurrent failed");
+    if (!ctx) {
+        e = cudaSetDevice(device);
+        if (e != cudaSuccess)
+            return noalloc_fail(BV_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+        if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx)
+            return noalloc_fail(BV_ERR_CUDA, "no current CUDA context");
+    }
+    NoAllocSlot &slot = g_noalloc_slot[device];
+    if (!slot.ptr || slot.ctx != ctx) {
         void *ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
         if (e != cudaSuccess || ptr == nullptr)
             return noalloc_fail(BV_ERR_CUDA,
                                 std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_noalloc_ptr[device] = static_cast<NoAllocScratch *>(ptr);
+        slot.ctx = ctx;
+        slot.ptr = static_cast<NoAllocScratch *>(ptr);
     }
-    *out = g_noalloc_ptr[device];
+    *out = slot.ptr;
     return BV_OK;
 }
 

@@ -318,7 +318,8 @@ __global__ void __launch_bounds__(256) relight_local_kernel(const GaussPrim *pri
 
 }  // namespace
 
-cudaError_t launch_relight(const RelightParams &p, cudaStream_t s) {
+cudaError_t launch_relight(const RelightParams &p, cudaStream_t s, uint32_t &launches) {
+    launches = 0;
     const int blocks = (int)((p.total_work + kRelightBlock - 1) / kRelightBlock);
     if (blocks == 0) return cudaSuccess;
 #if BV_RELIGHT_LOCAL
@@ -327,9 +328,11 @@ cudaError_t launch_relight(const RelightParams &p, cudaStream_t s) {
                                                                      p.origin[1], p.origin[2], p.local);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
+        launches += 1;
     }
 #endif
     relight_kernel<<<blocks, kRelightBlock, 0, s>>>(p);
+    launches += 1;
     return cudaGetLastError();
 }
 

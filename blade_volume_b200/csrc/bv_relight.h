@@ -61,6 +61,8 @@ struct RelightParams {
     RelightLight lights[kMaxRelightLights];
 };
 
-cudaError_t launch_relight(const RelightParams &p, cudaStream_t s);
+// launches: kernels enqueued (the origin-term kernel is skipped for an empty
+// scene, both for an empty image).
+cudaError_t launch_relight(const RelightParams &p, cudaStream_t s, uint32_t &launches);
 
 }  // namespace bv

@@ -30,6 +30,12 @@ struct bv_relight_tracer {
     bool stats_enabled = false;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     bool last_has_stats = false;
+    // The per-view origin table is rewritten by every dispatch: a dispatch on
+    // another stream than the previous one first waits for the previous one.
+    cudaEvent_t done = nullptr;
+    cudaStream_t last_stream = nullptr;
+    bool dispatched = false;
+    uint32_t last_launches = 0;
 };
 
 namespace {
@@ -48,6 +54,7 @@ void free_relight(bv_relight_tracer *t) {
     cudaFree(t->stats);
     for (auto &e : t->ev)
         if (e) cudaEventDestroy(e);
+    if (t->done) cudaEventDestroy(t->done);
     delete t;
 }
 
@@ -196,6 +203,7 @@ bv_status bv_relight_tracer_new_gaussian(const bv_gaussian_desc *g,
     BV_RTRY(cudaMemcpy(t->materials, mats.data(), sizeof(RelightMaterial) * mats.size(),
                        cudaMemcpyHostToDevice), "upload materials");
     for (auto &e : t->ev) BV_RTRY(cudaEventCreate(&e), "cudaEventCreate");
+    BV_RTRY(cudaEventCreateWithFlags(&t->done, cudaEventDisableTiming), "cudaEventCreate");
 #undef BV_RTRY
     if (settings) std::memcpy(t->background, settings->background, sizeof(t->background));
     *out = t;
@@ -287,11 +295,18 @@ bv_status bv_relight_tracer_dispatch(bv_relight_tracer *t, float *out_rgba_dev,
             cudaEventRecord(t->ev[0], s) != cudaSuccess)
             return rfail(BV_ERR_CUDA, "stats setup failed");
     }
-    cudaError_t e = launch_relight(p, s);
+    if (t->dispatched && t->last_stream != s && cudaStreamWaitEvent(s, t->done, 0) != cudaSuccess)
+        return rfail(BV_ERR_CUDA, "stream wait on the previous dispatch failed");
+    uint32_t launches = 0;
+    cudaError_t e = launch_relight(p, s, launches);
     if (e != cudaSuccess) {
         set_last_error(cudaGetErrorString(e));
         return BV_ERR_CUDA;
     }
+    t->last_launches = launches;
+    if (cudaEventRecord(t->done, s) != cudaSuccess) return rfail(BV_ERR_CUDA, "event record failed");
+    t->last_stream = s;
+    t->dispatched = true;
     if (t->stats_enabled && cudaEventRecord(t->ev[1], s) != cudaSuccess)
         return rfail(BV_ERR_CUDA, "event record failed");
     return BV_OK;
@@ -308,7 +323,7 @@ bv_status bv_relight_tracer_enable_stats(bv_relight_tracer *t, uint32_t enabled)
 bv_status bv_relight_tracer_last_stats(bv_relight_tracer *t, bv_launch_stats *out) {
     if (!t || !out) return rfail(BV_ERR_INVALID_ARGUMENT, "null argument");
     std::memset(out, 0, sizeof(*out));
-    out->launches = BV_RELIGHT_LOCAL ? 2 : 1;  // origin terms, trace
+    out->launches = t->last_launches;  // origin terms, trace
     if (!t->last_has_stats) return BV_OK;
     if (cudaEventSynchronize(t->ev[1]) != cudaSuccess)
         return rfail(BV_ERR_CUDA, "event sync failed");

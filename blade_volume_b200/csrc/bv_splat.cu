@@ -112,6 +112,24 @@ __device__ __forceinline__ bool splat_sphere(const WinRay &ray, const float4 &s,
     return !(sf <= 0.0f || sn >= depth);
 }
 
+// Division savers of the clip, exact: true only when the plane's rounded
+// quotient num / den cannot move the bound.  For a far plane (den > 0) that
+// is num / den >= face_far; for a near plane (den < 0) num / den <=
+// face_near, i.e. num >= face_near den.  p = fl(bound den) is within one
+// rounding of the exact product, so fl(p (1 +- 2^-21)) (the factor that moves
+// p away from zero's side the product could lie on) bounds it whenever p is
+// normal; otherwise the caller divides.
+__device__ __forceinline__ bool clip_far_cannot_tighten(float num, float den, float face_far) {
+    const float p = face_far * den;
+    return p > 1.0e-30f && num >= p * 1.000000476837158203125f;
+}
+
+__device__ __forceinline__ bool clip_near_cannot_tighten(float num, float den, float face_near) {
+    if (face_near == 0.0f) return num >= 0.0f;  // num / den <= 0 exactly
+    const float p = face_near * den;            // face_near > 0, den < 0
+    return p < -1.0e-30f && num >= p * 0.999999523162841796875f;
+}
+
 // Cech-row clip of one support (trace.rs:1351-1389, path_interval_jacobian
 // :1199-1325 for the bounded clip), warp-cooperative: every lane calls it
 // for the same support; the row's clip planes are read 32 at a time (one
@@ -162,24 +180,37 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
             const float num = dot3(rx, ry, rz, nx, ny, nz);
 #endif
             const float den = dot3(ray.dx, ray.dy, ray.dz, nx, ny, nz);
+            // A plane whose quotient provably cannot tighten the interval is
+            // passed without dividing (clip_cannot_tighten); the planes
+            // that can are divided and compared as before, so the interval
+            // and the planes that bound it are the same bit for bit.
+            bool moved = false;
             if (den > 1.0e-20f) {
-                const float t = num / den;
-                if (t < face_far) {
-                    face_far = t;
-                    far_k = base + j - begin;
+                if (!clip_far_cannot_tighten(num, den, face_far)) {
+                    const float t = num / den;
+                    if (t < face_far) {
+                        face_far = t;
+                        far_k = base + j - begin;
+                        moved = true;
+                    }
                 }
             } else if (den < -1.0e-20f) {
-                const float t = num / den;
-                if (t > face_near) {
-                    face_near = t;
-                    near_k = base + j - begin;
+                if (!clip_near_cannot_tighten(num, den, face_near)) {
+                    const float t = num / den;
+                    if (t > face_near) {
+                        face_near = t;
+                        near_k = base + j - begin;
+                        moved = true;
+                    }
                 }
             } else if (num < 0.0f) {
                 empty = true;
             }
-            const float st = sn > face_near ? sn : face_near;
-            const float en = sf < face_far ? sf : face_far;
-            if (en <= st) empty = true;
+            if (moved) {
+                const float st = sn > face_near ? sn : face_near;
+                const float en = sf < face_far ? sf : face_far;
+                if (en <= st) empty = true;
+            }
         }
     }
     if (empty) return false;

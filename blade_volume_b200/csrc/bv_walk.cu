@@ -9,11 +9,11 @@
 // the FP32 CPU restatement bit for bit (cells, t values, colours, alpha).
 // The only fused operations are the explicit __fmaf_rn calls in bv_expf.
 //
-// Scheduling: one ray per lane, persistent warps.  A warp refills idle lanes
-// from a global ray dispenser (one atomic per refill, ballot + popc to rank
-// the idle lanes), so rays that finish early do not leave lanes idle while
-// their neighbours walk long paths.  Work items are tile-ordered (8x4
-// pixels) so that lanes refilled together start on neighbouring pixels.
+// Scheduling: one ray per lane, persistent warps.  A warp takes a whole 8x4
+// pixel tile (32 tile-ordered work items) from a global ray dispenser and
+// keeps it until every lane is done (BV_REFILL_MIN = 32: refilling single
+// lanes was measured slower, because lockstep rays of one tile share cells,
+// which the L1 and the gradient aggregation exploit).
 
 #include <cuda_bf16.h>
 
@@ -100,8 +100,8 @@ constexpr float kTieUlps = 4.0f;
 // replay of a recorded exit both evaluate a face through this function, so a
 // recorded face reproduces the searched t bit for bit.
 template <bool BOUNDED>
-__device__ __forceinline__ bool face_exit_t(const Cell &c, float ri2, const float4 &site,
-                                            const Ray &ray, float &t) {
+__device__ __forceinline__ bool face_exit_nd(const Cell &c, float ri2, const float4 &site,
+                                             const Ray &ray, float &num, float &dp) {
     const float offx = site.x - c.x, offy = site.y - c.y, offz = site.z - c.z;
     float shift;
     if (BOUNDED) {
@@ -114,10 +114,29 @@ __device__ __forceinline__ bool face_exit_t(const Cell &c, float ri2, const floa
     const float fox = c.x + shift * offx;
     const float foy = c.y + shift * offy;
     const float foz = c.z + shift * offz;
-    const float dp = dot3(offx, offy, offz, ray.dx, ray.dy, ray.dz);
+    dp = dot3(offx, offy, offz, ray.dx, ray.dy, ray.dz);
     if (!(dp > 0.0f)) return false;
-    t = dot3(fox - ray.ox, foy - ray.oy, foz - ray.oz, offx, offy, offz) / dp;
+    num = dot3(fox - ray.ox, foy - ray.oy, foz - ray.oz, offx, offy, offz);
     return true;
+}
+
+template <bool BOUNDED>
+__device__ __forceinline__ bool face_exit_t(const Cell &c, float ri2, const float4 &site,
+                                            const Ray &ray, float &t) {
+    float num, dp;
+    if (!face_exit_nd<BOUNDED>(c, ri2, site, ray, num, dp)) return false;
+    t = num / dp;
+    return true;
+}
+
+// True when num / dp >= best holds exactly (dp > 0, best > 0), so that the
+// rounded quotient cannot be below best and the face cannot win: a division
+// saved.  p = fl(best dp) is within one rounding of best dp, so
+// fl(p (1 + 2^-21)) >= best dp whenever p is a normal number.  Otherwise (and
+// for NaN) the caller divides, which keeps the search's result bit for bit.
+__device__ __forceinline__ bool quotient_not_below(float num, float dp, float best) {
+    const float p = best * dp;
+    return p > 1.0e-30f && num >= p * 1.000000476837158203125f;
 }
 
 // find_exit_face (trace.rs:170-205): the first face in CSR order with the
@@ -146,8 +165,10 @@ __device__ __forceinline__ bool find_exit(const DeviceModel &m, const Cell &c, c
 #pragma unroll
         for (int u = 0; u < kFaceUnroll; ++u) {
             if (k + u < c.end) {
-                float t;
-                if (face_exit_t<BOUNDED>(c, ri2, site[u], ray, t)) {
+                float num, dp;
+                if (face_exit_nd<BOUNDED>(c, ri2, site[u], ray, num, dp) &&
+                    (TIE || !quotient_not_below(num, dp, best))) {
+                    const float t = num / dp;
                     if (isfinite(t) && t > t0 && t < best) {
                         if (TIE) {
                             second = best;

@@ -26,12 +26,37 @@ def rank_cameras(views: int, rank: int, radius: float = 3.0, fov_deg: float = 60
     return scenes.sphere_cameras(views, radius, 1 + rank, math.radians(fov_deg), aspect, depth)
 
 
-def allreduce_grads(grads: Dict[str, object], dist) -> None:
-    """Sum every gradient table over the ranks, in place, in a fixed order
-    (every rank issues the same collectives in the same order)."""
-    for name in GRAD_TABLES:
-        if name in grads and grads[name] is not None:
-            dist.all_reduce(grads[name])
+def allreduce_grads(grads: Dict[str, object], dist, bucket=None):
+    """Sum every gradient table over the ranks, in place, with ONE all-reduce.
+    Tables from a tracer's new_grads() are views of one flat buffer
+    (``grads.flat``), which is reduced directly.  Otherwise the tables are
+    packed into one flat bucket in a fixed order (every rank packs the same
+    tables the same way), reduced, and unpacked; ``bucket`` may be a
+    preallocated flat tensor of at least the tables' total size (it is
+    returned, so a caller can keep it across steps)."""
+    import torch
+
+    flat = getattr(grads, "flat", None)
+    if flat is not None:
+        dist.all_reduce(flat)
+        return bucket
+    tabs = [grads[n] for n in GRAD_TABLES if grads.get(n) is not None]
+    if not tabs:
+        return bucket
+    total = sum(t.numel() for t in tabs)
+    if bucket is None or bucket.numel() < total:
+        bucket = torch.empty(total, dtype=tabs[0].dtype, device=tabs[0].device)
+    flat = bucket[:total]
+    off = 0
+    for t in tabs:
+        flat[off:off + t.numel()].copy_(t.reshape(-1))
+        off += t.numel()
+    dist.all_reduce(flat)
+    off = 0
+    for t in tabs:
+        t.copy_(flat[off:off + t.numel()].view_as(t))
+        off += t.numel()
+    return bucket
 
 
 def max_over_ranks(values: List[float], dist, device) -> List[float]:

@@ -198,21 +198,55 @@ def sphere_cameras(count: int, radius: float, seed: int, fov_y: float, aspect: f
 # adjacency
 # --------------------------------------------------------------------------
 def _csr_from_pairs(n: int, a: np.ndarray, b: np.ndarray):
+    """Sorted symmetric CSR of the undirected pairs (a, b), duplicates and
+    self-pairs dropped.  scipy's COO -> CSR conversion is a counting sort by
+    row, so this stays linear in the number of pairs."""
+    import scipy.sparse as sp
+
     a = np.asarray(a, dtype=np.int64)
     b = np.asarray(b, dtype=np.int64)
     keep = a != b
     a, b = a[keep], b[keep]
-    key = np.concatenate([a * n + b, b * n + a])
-    key = np.unique(key)
-    rows = key // n
-    cols = (key % n).astype(np.uint32)
-    offsets = np.zeros(n + 1, dtype=np.uint32)
-    np.cumsum(np.bincount(rows, minlength=n), out=offsets[1:])
-    return offsets, cols
+    rows = np.concatenate([a, b])
+    cols = np.concatenate([b, a])
+    m = sp.csr_matrix((np.ones(len(rows), dtype=np.int32), (rows, cols)), shape=(n, n))
+    m.sum_duplicates()
+    m.sort_indices()
+    return m.indptr.astype(np.uint32), m.indices.astype(np.uint32)
+
+
+def _cached_csr(kind: str, build, *arrays):
+    """build() memoised on disk when BV_SCENE_CACHE names a directory, keyed
+    by the bytes of the input arrays (the adjacency of the large scenes
+    takes most of a minute to build, and several processes of one run build
+    the same scenes)."""
+    import hashlib
+    import os
+
+    root = os.environ.get("BV_SCENE_CACHE")
+    if not root:
+        return build()
+    h = hashlib.sha1(kind.encode())
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    path = os.path.join(root, f"{kind}_{h.hexdigest()}.npz")
+    if os.path.exists(path):
+        with np.load(path) as z:
+            return z["offsets"], z["neighbors"]
+    offsets, neighbors = build()
+    os.makedirs(root, exist_ok=True)
+    tmp = path + f".{os.getpid()}.tmp.npz"
+    np.savez(tmp, offsets=offsets, neighbors=neighbors)
+    os.replace(tmp, path)
+    return offsets, neighbors
 
 
 def delaunay_csr(xyz: np.ndarray):
     """Delaunay edges -> sorted symmetric CSR (adjacency.rs:55-136, :142)."""
+    return _cached_csr("delaunay", lambda: _delaunay_csr(xyz), np.asarray(xyz, np.float32))
+
+
+def _delaunay_csr(xyz: np.ndarray):
     from scipy.spatial import Delaunay
 
     tri = Delaunay(np.asarray(xyz, dtype=np.float64))
@@ -224,6 +258,11 @@ def delaunay_csr(xyz: np.ndarray):
 
 def cech_csr(xyz: np.ndarray, radii: np.ndarray):
     """Cech overlap graph |p_i - p_j| <= r_i + r_j (adjacency.rs:405-420)."""
+    return _cached_csr("cech", lambda: _cech_csr(xyz, radii), np.asarray(xyz, np.float32),
+                       np.asarray(radii, np.float32))
+
+
+def _cech_csr(xyz: np.ndarray, radii: np.ndarray):
     from scipy.spatial import cKDTree
 
     xyz32 = np.asarray(xyz, dtype=np.float32)
@@ -233,11 +272,15 @@ def cech_csr(xyz: np.ndarray, radii: np.ndarray):
     pairs = tree.query_pairs(2.0 * rmax, output_type="ndarray")
     if len(pairs) == 0:
         return _csr_from_pairs(len(xyz), np.zeros(0), np.zeros(0))
-    a, b = pairs[:, 0], pairs[:, 1]
-    d = xyz32[a] - xyz32[b]
-    dist = np.sqrt((d.astype(np.float32) ** 2).sum(axis=1, dtype=np.float32))
-    keep = dist <= (r[a] + r[b])
-    return _csr_from_pairs(len(xyz), a[keep], b[keep])
+    keep_a, keep_b = [], []
+    for c0 in range(0, len(pairs), 1 << 22):  # chunks stay cache-sized
+        a, b = pairs[c0:c0 + (1 << 22), 0], pairs[c0:c0 + (1 << 22), 1]
+        d = xyz32[a] - xyz32[b]
+        dist = np.sqrt((d.astype(np.float32) ** 2).sum(axis=1, dtype=np.float32))
+        keep = dist <= (r[a] + r[b])
+        keep_a.append(a[keep])
+        keep_b.append(b[keep])
+    return _csr_from_pairs(len(xyz), np.concatenate(keep_a), np.concatenate(keep_b))
 
 
 def rebuild_adjacency(model: "PointCloudModel") -> "PointCloudModel":

@@ -340,8 +340,9 @@ bv_status bv_relight_tracer_set_background(bv_relight_tracer *tracer, const floa
 /* Renders width x height into out_rgba_dev ([h][w][4] float32): radiance +
  * transmittance * background, alpha = 1 - transmittance (relight.wgsl:747-780).
  * Two launches: each particle's camera-origin terms into the tracer's
- * per-view table, then the trace; two dispatches of one tracer must
- * therefore not overlap on the GPU (one stream per tracer). */
+ * per-view table, then the trace.  Because that table is rewritten by each
+ * dispatch, a dispatch on a different stream than the tracer's previous one
+ * is ordered after it (an event wait), so dispatches never overlap. */
 bv_status bv_relight_tracer_dispatch(bv_relight_tracer *tracer, float *out_rgba_dev,
                                      const bv_camera *camera, uint32_t width, uint32_t height,
                                      bv_stream stream);
@@ -456,9 +457,10 @@ bv_status bv_gaussian_tracer_set_background(bv_gaussian_tracer *tracer, const fl
 uint32_t bv_gaussian_tracer_num_points(const bv_gaussian_tracer *tracer);
 /* Renders width x height into out_rgba_dev ([h][w][4] float32):
  * (radiance + T * background, 1 - T).  Two launches: each particle's
- * camera-origin terms into the tracer's per-view table, then the trace; two
- * dispatches of one tracer must therefore not overlap on the GPU (one
- * stream per tracer). */
+ * camera-origin terms into the tracer's per-view table, then the trace.
+ * Because that table is rewritten by each dispatch, a dispatch on a
+ * different stream than the tracer's previous one is ordered after it (an
+ * event wait), so dispatches never overlap. */
 bv_status bv_gaussian_tracer_dispatch(bv_gaussian_tracer *tracer, float *out_rgba_dev,
                                       const bv_camera *camera, uint32_t width, uint32_t height,
                                       bv_stream stream);
@@ -481,7 +483,9 @@ bv_status bv_gaussian_tracer_last_stats(bv_gaussian_tracer *tracer, bv_launch_st
  * device array that every GPU loading the library holds until exit; every
  * call shares it, so calls that overlap on the GPU (other streams, other
  * threads) race.  More than 32 queries is rejected with
- * BV_ERR_INVALID_ARGUMENT.  The first call on each device looks up the
+ * BV_ERR_INVALID_ARGUMENT (any site count is searched by at most 296 blocks,
+ * which the array holds).  The first call on each device, and again after
+ * the device's context has been replaced (cudaDeviceReset), looks up the
  * array's device address (cudaGetSymbolAddress); make that first call
  * before any stream capture. */
 bv_status bv_containing_points_noalloc(const float *sites_dev, uint32_t num_sites,

@@ -859,6 +859,33 @@ void bvo_render_splats(const bvo_model *m, const bvo_camera *cam, uint32_t width
     (void)threads;
 }
 
+/* bvo_render_splats over a list of pixel indices (y * width + x) only:
+ * out_rgba [n_px * 4], out_steps [n_px]. */
+void bvo_render_splats_px(const bvo_model *m, const bvo_camera *cam, uint32_t width,
+                          uint32_t height, uint32_t max_steps, float weight_threshold,
+                          uint32_t n_px, const uint32_t *px, float *out_rgba,
+                          uint32_t *out_steps, int threads) {
+    bvo_trace_settings s;
+    memset(&s, 0, sizeof(s));
+    s.weight_threshold = weight_threshold;
+    s.max_steps = max_steps;
+    s.depth = cam->depth;
+    s.eval_mode = BVO_EVAL_SH;
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+#endif
+    for (long k = 0; k < (long)n_px; ++k) {
+        const uint32_t x = px[k] % width, y = px[k] / width;
+        float o[3], d[3];
+        bvo_camera_ray(cam, width, height, x, y, o, d);
+        bvo_trace_result r = bvo_trace_powerfoam_splats(m, o, d, &s);
+        memcpy(out_rgba + 4 * (size_t)k, r.rgba, 16);
+        if (out_steps) out_steps[k] = r.steps;
+    }
+    (void)threads;
+}
+
 /* ------------------------------------------------------------------ */
 /* start cell                                                          */
 /* ------------------------------------------------------------------ */
@@ -1114,6 +1141,8 @@ static int sphere_t_d(const dparams *P, const double o[3], const double d[3], ui
 typedef struct {
     double dt_raw, dt, sigma, alpha, T, w;
     double c[3], cu[3];
+    double csum[3]; /* 0.5 + sum_m |Y_m coef_m|: the magnitude the FP32 SH sum rounds */
+    double Et;      /* error budget of T at this segment (units of 2^-24) */
     double j_prev[4], j_cur[4], j_next[4];
 } seg_eval_t;
 
@@ -1165,12 +1194,70 @@ static void eval_segment(const dparams *P, uint32_t K, const double o[3], const 
     }
     const double *c = P->sh + (size_t)sg->cell * 3u * K;
     for (int ch = 0; ch < 3; ++ch) {
-        double acc = 0.0;
-        for (uint32_t k = 0; k < K; ++k) acc += Y[k] * c[3 * k + ch];
+        double acc = 0.0, mag = 0.5;
+        for (uint32_t k = 0; k < K; ++k) {
+            acc += Y[k] * c[3 * k + ch];
+            mag += fabs(Y[k] * c[3 * k + ch]);
+        }
         ev->cu[ch] = 0.5 + acc;
         ev->c[ch] = ev->cu[ch] > 0.0 ? ev->cu[ch] : 0.0;
+        ev->csum[ch] = mag;
     }
     ev->sigma = P->pts[4 * (size_t)sg->cell + 3];
+}
+
+static inline void atomic_add_d(double *p, double v) {
+#ifdef _OPENMP
+#pragma omp atomic update
+#endif
+    *p += v;
+}
+
+/* Per-entry FP32 error budget of one segment's gradient contributions (the
+ * magnitudes that the device's FP32 evaluation and FP32 scatter round), in
+ * units of 2^-24, added to the mass tables; also advances the suffix budget
+ * Se past this segment.  First-order bounds: each product and sum carries one
+ * relative rounding of its operands' magnitudes, 1 - alpha carries one
+ * rounding of 1, and an error budget propagates through every factor. */
+static void add_mass(const bvo_grad_mass *mass, const seg_eval_t *ev, const seg_t *sg,
+                     uint32_t cell, uint32_t K, const double Y[16], const double g[3],
+                     const double ge[3], const double S[3], double Se[3], double gs, double Tn,
+                     float max_dt, int want_pos, int want_radius, double u32) {
+    const double Etn = ev->Et * (1.0 - ev->alpha) + ev->T + Tn; /* budget of T_{k+1} */
+    double egs = 0.0;
+    for (int ch = 0; ch < 3; ++ch) {
+        const double D = Tn * ev->c[ch] - S[ch];
+        const double eD = (Etn + Tn) * ev->c[ch] + Tn * ev->csum[ch] + Se[ch] + fabs(S[ch]);
+        egs += ge[ch] * fabs(D) + fabs(g[ch]) * eD;
+    }
+    if (mass->density) atomic_add_d(&mass->density[cell], ev->dt * egs + fabs(ev->dt * gs));
+    const double ew = ev->Et * ev->alpha + ev->T + ev->w; /* budget of w = T alpha */
+    if (mass->sh) {
+        for (int ch = 0; ch < 3; ++ch) {
+            /* a colour within its rounding of 0 may clamp either way */
+            if (!(ev->cu[ch] > 0.0 || fabs(ev->cu[ch]) <= 64.0 * u32 * ev->csum[ch])) continue;
+            for (uint32_t mm = 0; mm < K; ++mm) {
+                const double v = (ge[ch] * ev->w + fabs(g[ch]) * ew) * fabs(Y[mm]) +
+                                 fabs(g[ch] * ev->w * Y[mm]);
+                atomic_add_d(&mass->sh[(size_t)cell * 3 * K + 3 * mm + ch], v);
+            }
+        }
+    }
+    const int dt_active = ev->dt_raw > 0.0 && ev->dt_raw < (double)max_dt;
+    if (dt_active && (want_pos || want_radius)) {
+        const uint32_t who[3] = {sg->prev, cell, sg->next};
+        const double *js[3] = {ev->j_prev, ev->j_cur, ev->j_next};
+        const double gdt = ev->sigma * gs, egdt = ev->sigma * egs + fabs(gdt);
+        for (int r = 0; r < 3; ++r) {
+            if (want_pos && mass->pos)
+                for (int a = 0; a < 3; ++a)
+                    if (js[r][a] != 0.0)
+                        atomic_add_d(&mass->pos[3 * (size_t)who[r] + a], egdt * fabs(js[r][a]));
+            if (want_radius && mass->radius && js[r][3] != 0.0)
+                atomic_add_d(&mass->radius[who[r]], egdt * fabs(js[r][3]));
+        }
+    }
+    for (int ch = 0; ch < 3; ++ch) Se[ch] += ew * ev->c[ch] + ev->w * ev->csum[ch];
 }
 
 double bvo_forward_backward(const bvo_model *m, const bvo_camera *cams, uint32_t n_cams,
@@ -1191,6 +1278,20 @@ double bvo_forward_backward_ex(const bvo_model *m, const bvo_camera *cams, uint3
                                double *out_rgb, float *out_rgb32, double *d_density,
                                double *d_sh, double *d_pos, double *d_radius, int threads,
                                int splats) {
+    return bvo_forward_backward_mx(m, cams, n_cams, width, height, max_steps, weight_threshold,
+                                   max_dt, target, loss_kind, override_params, out_rgb,
+                                   out_rgb32, d_density, d_sh, d_pos, d_radius, threads, splats,
+                                   NULL, NULL);
+}
+
+double bvo_forward_backward_mx(const bvo_model *m, const bvo_camera *cams, uint32_t n_cams,
+                               uint32_t width, uint32_t height, uint32_t max_steps,
+                               float weight_threshold, float max_dt, const float *target,
+                               int loss_kind, const bvo_params_f64 *override_params,
+                               double *out_rgb, float *out_rgb32, double *d_density,
+                               double *d_sh, double *d_pos, double *d_radius, int threads,
+                               int splats, const uint8_t *ray_mask, const bvo_grad_mass *mass) {
+    const double u32 = 5.9604644775390625e-08; /* 2^-24 */
     const uint32_t deg = m->sh_degree > 3 ? 3 : m->sh_degree;
     const uint32_t K = sh_comps(deg);
     /* FP64 parameter view */
@@ -1231,6 +1332,7 @@ double bvo_forward_backward_ex(const bvo_model *m, const bvo_camera *cams, uint3
 #pragma omp for schedule(dynamic, 32)
 #endif
         for (long i = 0; i < total; ++i) {
+            if (ray_mask && !ray_mask[i]) continue;
             const uint32_t v = (uint32_t)(i / per_view);
             const long pix = i % per_view;
             const uint32_t x = (uint32_t)(pix % width), y = (uint32_t)(pix / width);
@@ -1254,6 +1356,11 @@ double bvo_forward_backward_ex(const bvo_model *m, const bvo_camera *cams, uint3
                 for (int ch = 0; ch < 3; ++ch) out_rgb32[3 * (size_t)i + ch] = rgb32[ch];
             sh_basis_d(deg, d, Y);
             double T = 1.0;
+            /* FP32 error budget of the device's forward, in units of 2^-24:
+             * Et bounds |T32 - T| before segment k (each 1 - alpha carries
+             * one rounding of 1, each product one relative rounding), Cerr
+             * bounds the colour's error. */
+            double Et = 0.0, Cerr[3] = {0.0, 0.0, 0.0};
             for (int k = 0; k < nseg; ++k) {
                 seg_eval_t *ev = &evs[k];
                 eval_segment(&P, K, o, d, Y, &segs[k], (double)cams[v].depth,
@@ -1267,6 +1374,12 @@ double bvo_forward_backward_ex(const bvo_model *m, const bvo_camera *cams, uint3
                     ev->alpha = 1.0 - exp(-ev->sigma * dt);
                     ev->w = T * ev->alpha;
                     for (int ch = 0; ch < 3; ++ch) C[ch] += ev->w * ev->c[ch];
+                    if (mass) {
+                        ev->Et = Et;
+                        const double ew = Et * ev->alpha + T + ev->w;
+                        for (int ch = 0; ch < 3; ++ch) Cerr[ch] += ew * ev->c[ch] + ev->w * ev->csum[ch];
+                        Et = Et * (1.0 - ev->alpha) + T + T * (1.0 - ev->alpha);
+                    }
                     T *= 1.0 - ev->alpha;
                 } else {
                     ev->alpha = 0.0;
@@ -1288,6 +1401,18 @@ double bvo_forward_backward_ex(const bvo_model *m, const bvo_camera *cams, uint3
             }
             if (!d_density) continue;
             double S[3] = {0, 0, 0};
+            /* error budgets (units of 2^-24) of dL/dC and of the suffix S */
+            double ge[3], Se[3] = {0.0, 0.0, 0.0};
+            for (int ch = 0; ch < 3; ++ch) {
+                if (loss_kind == 0) {
+                    ge[ch] = fabs(g[ch]) + 2.0 * Cerr[ch] / M;
+                } else {
+                    /* L1: a residual within the colour's rounding may take either sign */
+                    const double diff = C[ch] - (tg ? (double)tg[ch] : 0.0);
+                    ge[ch] = fabs(g[ch]) + (fabs(diff) <= 64.0 * u32 * (Cerr[ch] + fabs(C[ch]))
+                                                ? 2.0 / (M * u32) : 0.0);
+                }
+            }
             for (int k = nseg - 1; k >= 0; --k) {
                 const seg_eval_t *ev = &evs[k];
                 if (ev->sigma <= 1e-6) continue;
@@ -1295,6 +1420,10 @@ double bvo_forward_backward_ex(const bvo_model *m, const bvo_camera *cams, uint3
                 double gs = 0.0;
                 for (int ch = 0; ch < 3; ++ch) gs += g[ch] * (Tn * ev->c[ch] - S[ch]);
                 const uint32_t cell = segs[k].cell;
+                if (mass) {
+                    add_mass(mass, ev, segs + k, cell, K, Y, g, ge, S, Se, gs, Tn, max_dt,
+                             d_pos != NULL, d_radius != NULL, u32);
+                }
 #ifdef _OPENMP
 #pragma omp atomic update
 #endif
@@ -1708,6 +1837,25 @@ void bvo_relight_render(const bvo_relight_scene *s, const bvo_point_light *light
     (void)threads;
 }
 
+/* bvo_relight_render over a list of pixel indices (y * width + x) only. */
+void bvo_relight_render_px(const bvo_relight_scene *s, const bvo_point_light *lights,
+                           uint32_t n_lights, const bvo_camera *cam, uint32_t width,
+                           uint32_t height, const float background[3], uint32_t n_px,
+                           const uint32_t *px, float *out_rgba, uint32_t *out_hits, int threads) {
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+#endif
+    for (long k = 0; k < (long)n_px; ++k) {
+        float o[3], d[3];
+        relight_camera_ray(cam, width, height, px[k] % width, px[k] / width, o, d);
+        bvo_relight_ray(s, lights, n_lights, o, d, cam->depth, background,
+                        out_rgba + 4 * (size_t)k, out_hits ? out_hits + k : NULL);
+    }
+    (void)height;
+    (void)threads;
+}
+
 /* ------------------------------------------------------------------ */
 /* Gaussian ray tracing with SH colour (trace.rs:695-773)              */
 /* ------------------------------------------------------------------ */
@@ -1793,6 +1941,26 @@ void bvo_gaussian_render(const bvo_gaussian_scene *s, const bvo_camera *cam, uin
         bvo_trace_gaussians(s, o, d, &st, background, out_rgba + 4 * (size_t)i,
                             out_hits ? out_hits + i : NULL);
     }
+    (void)threads;
+}
+
+/* bvo_gaussian_render over a list of pixel indices (y * width + x) only. */
+void bvo_gaussian_render_px(const bvo_gaussian_scene *s, const bvo_camera *cam, uint32_t width,
+                            uint32_t height, float min_opacity, float min_transmittance,
+                            const float background[3], uint32_t n_px, const uint32_t *px,
+                            float *out_rgba, uint32_t *out_hits, int threads) {
+    const bvo_gaussian_settings st = {min_opacity, min_transmittance, 0.0f, cam->depth};
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+#endif
+    for (long k = 0; k < (long)n_px; ++k) {
+        float o[3], d[3];
+        relight_camera_ray(cam, width, height, px[k] % width, px[k] / width, o, d);
+        bvo_trace_gaussians(s, o, d, &st, background, out_rgba + 4 * (size_t)k,
+                            out_hits ? out_hits + k : NULL);
+    }
+    (void)height;
     (void)threads;
 }
 
@@ -2001,4 +2169,294 @@ void bvo_adam_step(bvo_adam_state *s, const bvo_adam_settings *a, uint32_t t, co
         if (gr && s->radii && a->lr_radius != 0.0f)
             s->radii[i] = adam_update(s->radii[i], gr[i], &s->m_r[i], &s->v_r[i], &k, a->lr_radius);
     }
+}
+
+/* ------------------------------------------------------------------ */
+/* FP64 accuracy oracles of the PowerFoam splat and the relight        */
+/* ------------------------------------------------------------------ */
+/* The same functions as bvo_trace_powerfoam_splats (trace.rs:1331-1546) and
+ * bvo_relight_ray (relight.wgsl:419-441, :606-744, :190-261) with every
+ * quantity in double and libm's exp / log / pow / cbrt: the model's FP32
+ * values are the exact inputs.  Used only to state the FP32 paths' image
+ * error, never as the thing measured. */
+
+typedef struct {
+    double t_start, dt;
+    uint32_t cell;
+} splat_d;
+
+static int cmp_splat_d(const void *a, const void *b) {
+    const splat_d *x = (const splat_d *)a, *y = (const splat_d *)b;
+    if (x->t_start < y->t_start) return -1;
+    if (x->t_start > y->t_start) return 1;
+    return (x->cell > y->cell) - (x->cell < y->cell);
+}
+
+static void trace_splats_d(const bvo_model *m, const double o[3], const double d[3],
+                           uint32_t max_steps, double thr, double depth, double rgba[4]) {
+    size_t cap = 64, count = 0;
+    splat_d *buf = (splat_d *)malloc(sizeof(splat_d) * cap);
+    for (uint32_t cell = 0; cell < m->n; ++cell) {
+        const float *cpf = m->points + 4 * (size_t)cell;
+        const double cur[3] = {cpf[0], cpf[1], cpf[2]};
+        const double cr = m->radii ? (double)m->radii[cell] : 0.0;
+        const double cam[3] = {cur[0] - o[0], cur[1] - o[1], cur[2] - o[2]};
+        if (dot3d(cam, cam) < (4.0 * cr) * (4.0 * cr)) continue;
+        const double oc[3] = {o[0] - cur[0], o[1] - cur[1], o[2] - cur[2]};
+        const double b = dot3d(oc, d);
+        const double disc = b * b - (dot3d(oc, oc) - cr * cr);
+        if (!(disc > 0.0)) continue;
+        const double root = sqrt(disc);
+        const double sn = -b - root, sf = -b + root;
+        if (sf <= 0.0 || sn >= depth) continue;
+        double face_near = 0.0, face_far = depth;
+        int empty = 0;
+        for (uint32_t k = m->offsets[cell]; k < m->offsets[cell + 1]; ++k) {
+            const uint32_t a = m->neighbors[k];
+            const float *apf = m->points + 4 * (size_t)a;
+            const double ar = m->radii ? (double)m->radii[a] : 0.0;
+            const double n[3] = {apf[0] - cur[0], apf[1] - cur[1], apf[2] - cur[2]};
+            const double dsq = fmax(dot3d(n, n), 1e-20);
+            const double shift = 0.5 + 0.5 * (cr * cr - ar * ar) / dsq;
+            const double rel[3] = {cur[0] + shift * n[0] - o[0], cur[1] + shift * n[1] - o[1],
+                                   cur[2] + shift * n[2] - o[2]};
+            const double num = dot3d(rel, n), den = dot3d(d, n);
+            if (den > 1e-20) {
+                face_far = fmin(face_far, num / den);
+            } else if (den < -1e-20) {
+                face_near = fmax(face_near, num / den);
+            } else if (num < 0.0) {
+                empty = 1;
+                break;
+            }
+        }
+        if (empty) continue;
+        const double start = fmax(face_near, sn), end = fmin(face_far, sf);
+        if (!(end > start)) continue;
+        if (count == cap) {
+            cap *= 2;
+            buf = (splat_d *)realloc(buf, sizeof(splat_d) * cap);
+        }
+        buf[count].t_start = start;
+        buf[count].dt = end - start;
+        buf[count].cell = cell;
+        count += 1;
+    }
+    qsort(buf, count, sizeof(splat_d), cmp_splat_d);
+    if (count > max_steps) count = max_steps;
+    const uint32_t deg = m->sh_degree > 3 ? 3 : m->sh_degree;
+    const uint32_t comps = sh_comps(deg);
+    double Y[16];
+    sh_basis_d(deg, d, Y);
+    double T = 1.0, acc[3] = {0.0, 0.0, 0.0};
+    for (size_t i = 0; i < count; ++i) {
+        if (T <= thr) break;
+        const double dens = m->points[4 * (size_t)buf[i].cell + 3];
+        if (dens <= 1e-6) continue;
+        const double alpha = 1.0 - exp(-dens * buf[i].dt);
+        const double w = T * alpha;
+        const float *c = m->sh + (size_t)buf[i].cell * 3u * comps;
+        for (int ch = 0; ch < 3; ++ch) {
+            double v = 0.0;
+            for (uint32_t k = 0; k < comps; ++k) v += Y[k] * (double)c[3 * k + ch];
+            acc[ch] += w * fmax(0.5 + v, 0.0);
+        }
+        T *= 1.0 - alpha;
+    }
+    free(buf);
+    rgba[0] = acc[0];
+    rgba[1] = acc[1];
+    rgba[2] = acc[2];
+    rgba[3] = 1.0 - T;
+}
+
+void bvo_render_splats_f64_px(const bvo_model *m, const bvo_camera *cam, uint32_t width,
+                              uint32_t height, uint32_t max_steps, double weight_threshold,
+                              uint32_t n_px, const uint32_t *px, double *out_rgba, int threads) {
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+#endif
+    for (long k = 0; k < (long)n_px; ++k) {
+        double o[3], d[3];
+        camera_ray_d(cam, width, height, px[k] % width, px[k] / width, o, d);
+        trace_splats_d(m, o, d, max_steps, weight_threshold, (double)cam->depth,
+                       out_rgba + 4 * (size_t)k);
+    }
+    (void)threads;
+}
+
+static void qrot_d(const double q[4], const double v[3], double out[3]) {
+    const double t0 = 2.0 * (q[1] * v[2] - q[2] * v[1]);
+    const double t1 = 2.0 * (q[2] * v[0] - q[0] * v[2]);
+    const double t2 = 2.0 * (q[0] * v[1] - q[1] * v[0]);
+    out[0] = (v[0] + q[3] * t0) + (q[1] * t2 - q[2] * t1);
+    out[1] = (v[1] + q[3] * t1) + (q[2] * t0 - q[0] * t2);
+    out[2] = (v[2] + q[3] * t2) + (q[0] * t1 - q[1] * t0);
+}
+
+static void point_light_shade_d(const bvo_point_light *L, const double p[3], const double n[3],
+                                const double view[3], const bvo_material *mt, double out[3]) {
+    out[0] = out[1] = out[2] = 0.0;
+    const double fl[3] = {p[0] - L->position[0], p[1] - L->position[1], p[2] - L->position[2]};
+    const double d2 = dot3d(fl, fl);
+    if (d2 <= 1.1920929e-7) return;
+    const double inv = 1.0 / sqrt(d2);
+    const double away[3] = {fl[0] * inv, fl[1] * inv, fl[2] * inv};
+    double angular = 1.0;
+    if (L->exponent != 0.0f) {
+        const double ld[3] = {L->direction[0], L->direction[1], L->direction[2]};
+        angular = pow(fmax(dot3d(ld, away), 0.0), (double)L->exponent);
+    }
+    const double towards[3] = {-away[0], -away[1], -away[2]};
+    const double ndl = fmax(dot3d(n, towards), 0.0);
+    if (ndl == 0.0) return;
+    double rad[3];
+    for (int c = 0; c < 3; ++c) {
+        rad[c] = (double)L->intensity[c] * angular / d2;
+        out[c] = (double)mt->albedo[c] * rad[c] * ndl;
+    }
+    if (mt->specular_f0[0] == 0.0f && mt->specular_f0[1] == 0.0f && mt->specular_f0[2] == 0.0f)
+        return;
+    const double ndv = fmax(dot3d(n, view), 0.0);
+    const double hs[3] = {towards[0] + view[0], towards[1] + view[1], towards[2] + view[2]};
+    const double hs2 = dot3d(hs, hs);
+    if (ndv == 0.0 || hs2 <= 1.1920929e-7) return;
+    const double hinv = 1.0 / sqrt(hs2);
+    const double h[3] = {hs[0] * hinv, hs[1] * hinv, hs[2] * hinv};
+    const double ndh = fmax(dot3d(n, h), 0.0);
+    const double vdh = fmin(fmax(dot3d(view, h), 0.0), 1.0);
+    const double rc = fmin(fmax((double)mt->roughness, 0.045), 1.0);
+    const double alpha = rc * rc, a2 = alpha * alpha;
+    const double den = ndh * ndh * (a2 - 1.0) + 1.0;
+    const double pi = 3.14159265358979323846;
+    const double dist = a2 / fmax(pi * den * den, 1.1754944e-38);
+    const double sl = 2.0 * ndl / (ndl + sqrt(a2 + (1.0 - a2) * ndl * ndl));
+    const double sv = 2.0 * ndv / (ndv + sqrt(a2 + (1.0 - a2) * ndv * ndv));
+    const double g1 = 1.0 - vdh;
+    const double grazing = (g1 * g1) * (g1 * g1) * g1;
+    const double scale = pi * dist * sl * sv / (4.0 * ndv);
+    for (int c = 0; c < 3; ++c) {
+        const double f0 = mt->specular_f0[c];
+        out[c] += rad[c] * scale * (f0 + (1.0 - f0) * grazing);
+    }
+}
+
+typedef struct {
+    double t, alpha;
+    uint32_t index;
+} relight_hit_d;
+
+static int cmp_hit_d(const void *a, const void *b) {
+    const relight_hit_d *x = (const relight_hit_d *)a, *y = (const relight_hit_d *)b;
+    if (x->t < y->t) return -1;
+    if (x->t > y->t) return 1;
+    return (x->index > y->index) - (x->index < y->index);
+}
+
+static void relight_ray_d(const bvo_relight_scene *s, const bvo_point_light *lights,
+                          uint32_t n_lights, const double o[3], const double d[3], double depth,
+                          const float background[3], double rgba[4]) {
+    relight_hit_d *hits = NULL;
+    size_t nh = 0, cap = 0;
+    for (uint32_t i = 0; i < s->n; ++i) {
+        const float *q = s->rotation + 4 * (size_t)i;
+        const double qi[4] = {-(double)q[0], -(double)q[1], -(double)q[2], q[3]};
+        const float *c = s->center + 3 * (size_t)i;
+        const float *sc = s->scale + 3 * (size_t)i;
+        const double oc[3] = {o[0] - c[0], o[1] - c[1], o[2] - c[2]};
+        double lo[3], ld[3];
+        qrot_d(qi, oc, lo);
+        qrot_d(qi, d, ld);
+        for (int k = 0; k < 3; ++k) {
+            lo[k] /= (double)sc[k];
+            ld[k] /= (double)sc[k];
+        }
+        const double t = -dot3d(lo, ld) / dot3d(ld, ld);
+        if (t <= 0.0 || t >= depth) continue;
+        const double lp[3] = {lo[0] + t * ld[0], lo[1] + t * ld[1], lo[2] + t * ld[2]};
+        const double sq = dot3d(lp, lp);
+        const double op = s->opacity[i];
+        if (sq > 2.0 * log(op / 0.03)) continue;
+        const double response = fmin(0.999, op * exp(-0.5 * sq));
+        const double a = 1.0 - pow(1.0 - response, 1.1);
+        if (!(a > 0.0)) continue;
+        if (nh == cap) {
+            cap = cap ? cap * 2 : 64;
+            hits = (relight_hit_d *)realloc(hits, cap * sizeof(relight_hit_d));
+        }
+        hits[nh].t = t;
+        hits[nh].alpha = a;
+        hits[nh].index = i;
+        nh += 1;
+    }
+    qsort(hits, nh, sizeof(relight_hit_d), cmp_hit_d);
+    double radiance[3] = {0, 0, 0}, T = 1.0, limit = 0.0, sum_c[3] = {0, 0, 0}, sum_w = 0.0,
+           group_T = 1.0;
+    int active = 0, stopped = 0;
+    for (size_t k = 0; k < nh; ++k) {
+        const relight_hit_d *h = &hits[k];
+        if (!active || h->t > limit) {
+            if (active) {
+                const double alpha = (1.0 - group_T) * 0.25 + fmin(1.0, sum_w) * 0.75;
+                for (int c = 0; c < 3; ++c) radiance[c] += T * (alpha * sum_c[c] / fmax(sum_w, 1e-6));
+                T *= 1.0 - alpha;
+                active = 0;
+                if (T <= 0.003) {
+                    stopped = 1;
+                    break;
+                }
+            }
+            active = 1;
+            const float *sc = s->scale + 3 * (size_t)h->index;
+            limit = h->t + 0.5 * 3.0 * cbrt((double)sc[0] * (double)sc[1] * (double)sc[2]);
+            sum_c[0] = sum_c[1] = sum_c[2] = 0.0;
+            sum_w = 0.0;
+            group_T = 1.0;
+        }
+        const double point[3] = {o[0] + h->t * d[0], o[1] + h->t * d[1], o[2] + h->t * d[2]};
+        const float *nrm = s->normal + 3 * (size_t)h->index;
+        double n[3] = {nrm[0], nrm[1], nrm[2]};
+        if (dot3d(n, d) > 0.0) {
+            n[0] = -n[0];
+            n[1] = -n[1];
+            n[2] = -n[2];
+        }
+        const double view[3] = {-d[0], -d[1], -d[2]};
+        const bvo_material *mat = &s->materials[s->material[h->index]];
+        double shade[3] = {0, 0, 0};
+        for (uint32_t l = 0; l < n_lights; ++l) {
+            double one[3];
+            point_light_shade_d(&lights[l], point, n, view, mat, one);
+            for (int c = 0; c < 3; ++c) shade[c] += one[c];
+        }
+        for (int c = 0; c < 3; ++c) sum_c[c] += h->alpha * shade[c];
+        sum_w += h->alpha;
+        group_T *= 1.0 - h->alpha;
+    }
+    if (active && !stopped) {
+        const double alpha = (1.0 - group_T) * 0.25 + fmin(1.0, sum_w) * 0.75;
+        for (int c = 0; c < 3; ++c) radiance[c] += T * (alpha * sum_c[c] / fmax(sum_w, 1e-6));
+        T *= 1.0 - alpha;
+    }
+    free(hits);
+    for (int c = 0; c < 3; ++c) rgba[c] = radiance[c] + T * (double)background[c];
+    rgba[3] = 1.0 - T;
+}
+
+void bvo_relight_render_f64_px(const bvo_relight_scene *s, const bvo_point_light *lights,
+                               uint32_t n_lights, const bvo_camera *cam, uint32_t width,
+                               uint32_t height, const float background[3], uint32_t n_px,
+                               const uint32_t *px, double *out_rgba, int threads) {
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+#endif
+    for (long k = 0; k < (long)n_px; ++k) {
+        double o[3], d[3];
+        camera_ray_d(cam, width, height, px[k] % width, px[k] / width, o, d);
+        relight_ray_d(s, lights, n_lights, o, d, (double)cam->depth, background,
+                      out_rgba + 4 * (size_t)k);
+    }
+    (void)threads;
 }

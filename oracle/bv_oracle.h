@@ -141,6 +141,12 @@ void bvo_render_splats(const bvo_model *m, const bvo_camera *cam, uint32_t width
                        float *out_rgba, uint32_t *out_steps, int threads);
 
 /* ---- start cell (lib.rs:526-541; gpu/radfoam.rs:77-112) ---- */
+/* bvo_render_splats restricted to a list of pixel indices (y * width + x):
+ * out_rgba [n_px * 4], out_steps [n_px] (may be NULL). */
+void bvo_render_splats_px(const bvo_model *m, const bvo_camera *cam, uint32_t width,
+                          uint32_t height, uint32_t max_steps, float weight_threshold,
+                          uint32_t n_px, const uint32_t *px, float *out_rgba,
+                          uint32_t *out_steps, int threads);
 uint32_t bvo_containing_cell_f64(const bvo_model *m, const float position[3]);
 uint32_t bvo_containing_cell_f32(const bvo_model *m, const float position[3]);
 
@@ -186,6 +192,31 @@ double bvo_forward_backward_ex(const bvo_model *m, const bvo_camera *cams, uint3
                                double *out_rgb, float *out_rgb32, double *d_density,
                                double *d_sh, double *d_pos, double *d_radius, int threads,
                                int splats);
+
+/* Per-entry FP32 error budget of the gradient tables (test infrastructure):
+ * for every gradient entry the sum, over the contributions that form it, of
+ * the magnitudes that an FP32 evaluation of the same contract rounds (the
+ * transmittance product, 1 - alpha, the SH sum, dL/dC through the colour,
+ * the suffix, the scatter), in units of 2^-24.  An FP32 implementation of
+ * the contract then differs from the FP64 gradient by at most a small
+ * multiple of 2^-24 times this mass.  Any table may be NULL. */
+typedef struct {
+    double *density; /* [n] */
+    double *sh;      /* [n*3K] */
+    double *pos;     /* [n*3] */
+    double *radius;  /* [n] */
+} bvo_grad_mass;
+
+/* bvo_forward_backward_ex restricted to the rays whose ray_mask byte is
+ * non-zero (NULL: every ray; the loss normalisation still counts every ray
+ * of the batch), optionally accumulating the error-budget tables. */
+double bvo_forward_backward_mx(const bvo_model *m, const bvo_camera *cams, uint32_t n_cams,
+                               uint32_t width, uint32_t height, uint32_t max_steps,
+                               float weight_threshold, float max_dt, const float *target,
+                               int loss_kind, const bvo_params_f64 *override_params,
+                               double *out_rgb, float *out_rgb32, double *d_density,
+                               double *d_sh, double *d_pos, double *d_radius, int threads,
+                               int splats, const uint8_t *ray_mask, const bvo_grad_mass *mass);
 
 /* ---- relightable Gaussians with finite point lights ----
  * blade-volume/shaders/relight.wgsl (kernel 2 = learned volumetric
@@ -249,6 +280,11 @@ void bvo_relight_render(const bvo_relight_scene *s, const bvo_point_light *light
                         uint32_t n_lights, const bvo_camera *cam, uint32_t width,
                         uint32_t height, const float background[3], float *out_rgba,
                         uint32_t *out_hits, int threads);
+/* bvo_relight_render restricted to a list of pixel indices (y * width + x). */
+void bvo_relight_render_px(const bvo_relight_scene *s, const bvo_point_light *lights,
+                           uint32_t n_lights, const bvo_camera *cam, uint32_t width,
+                           uint32_t height, const float background[3], uint32_t n_px,
+                           const uint32_t *px, float *out_rgba, uint32_t *out_hits, int threads);
 
 /* ---- Gaussian ray tracing with SH colour (trace.rs:695-773) ----
  * Particles with opacity > min_opacity only (GaussianGpuCloud::new,
@@ -288,6 +324,11 @@ void bvo_gaussian_render(const bvo_gaussian_scene *s, const bvo_camera *cam, uin
                          uint32_t height, float min_opacity, float min_transmittance,
                          const float background[3], float *out_rgba, uint32_t *out_hits,
                          int threads);
+/* bvo_gaussian_render restricted to a list of pixel indices (y * width + x). */
+void bvo_gaussian_render_px(const bvo_gaussian_scene *s, const bvo_camera *cam, uint32_t width,
+                            uint32_t height, float min_opacity, float min_transmittance,
+                            const float background[3], uint32_t n_px, const uint32_t *px,
+                            float *out_rgba, uint32_t *out_hits, int threads);
 
 /* ---- FP64 accuracy oracle of the walk ----
  * trace_one_ray with every quantity in double (ray mapping, exit faces,
@@ -325,6 +366,18 @@ float bvo_density_activation_inverse(float y, int kind, float beta);
 /* One step t (1-based); a NULL gradient skips its table, a zero rate freezes it. */
 void bvo_adam_step(bvo_adam_state *s, const bvo_adam_settings *a, uint32_t t, const float *g_density,
                    const float *g_sh, const float *g_pos, const float *g_radii);
+
+/* ---- FP64 accuracy oracles of the splat and the relight ----
+ * bvo_render_splats_px / bvo_relight_render_px with every quantity in
+ * double (libm exp, log, pow, cbrt); the FP32 model values are the exact
+ * inputs.  out_rgba [n_px * 4] double. */
+void bvo_render_splats_f64_px(const bvo_model *m, const bvo_camera *cam, uint32_t width,
+                              uint32_t height, uint32_t max_steps, double weight_threshold,
+                              uint32_t n_px, const uint32_t *px, double *out_rgba, int threads);
+void bvo_relight_render_f64_px(const bvo_relight_scene *s, const bvo_point_light *lights,
+                               uint32_t n_lights, const bvo_camera *cam, uint32_t width,
+                               uint32_t height, const float background[3], uint32_t n_px,
+                               const uint32_t *px, double *out_rgba, int threads);
 
 #ifdef __cplusplus
 }

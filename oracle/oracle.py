@@ -99,6 +99,10 @@ class ParamsF64(C.Structure):
 EVAL_OPACITY, EVAL_CONSTANT, EVAL_SH = 0, 1, 2
 
 
+class GradMass(C.Structure):
+    _fields_ = [("density", f64p), ("sh", f64p), ("pos", f64p), ("radius", f64p)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -145,6 +149,26 @@ def lib():
                                            f32p, f64p, f64p, f64p, f64p, C.c_int]
         L.bvo_forward_backward_ex.restype = C.c_double
         L.bvo_forward_backward_ex.argtypes = L.bvo_forward_backward.argtypes + [C.c_int]
+        L.bvo_forward_backward_mx.restype = C.c_double
+        L.bvo_forward_backward_mx.argtypes = L.bvo_forward_backward_ex.argtypes + [
+            C.POINTER(C.c_uint8), C.POINTER(GradMass)]
+        L.bvo_render_splats_px.argtypes = [C.POINTER(Model), C.POINTER(Camera), C.c_uint32,
+                                           C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, u32p,
+                                           f32p, u32p, C.c_int]
+        L.bvo_relight_render_px.argtypes = [C.POINTER(RelightScene), C.POINTER(PointLight),
+                                            C.c_uint32, C.POINTER(Camera), C.c_uint32,
+                                            C.c_uint32, f32p, C.c_uint32, u32p, f32p, u32p,
+                                            C.c_int]
+        L.bvo_gaussian_render_px.argtypes = [C.POINTER(GaussianScene), C.POINTER(Camera),
+                                             C.c_uint32, C.c_uint32, C.c_float, C.c_float, f32p,
+                                             C.c_uint32, u32p, f32p, u32p, C.c_int]
+        L.bvo_render_splats_f64_px.argtypes = [C.POINTER(Model), C.POINTER(Camera), C.c_uint32,
+                                               C.c_uint32, C.c_uint32, C.c_double, C.c_uint32,
+                                               u32p, f64p, C.c_int]
+        L.bvo_relight_render_f64_px.argtypes = [C.POINTER(RelightScene), C.POINTER(PointLight),
+                                                C.c_uint32, C.POINTER(Camera), C.c_uint32,
+                                                C.c_uint32, f32p, C.c_uint32, u32p, f64p,
+                                                C.c_int]
         L.bvo_logf.restype = C.c_float
         L.bvo_logf.argtypes = [C.c_float]
         L.bvo_powf.restype = C.c_float
@@ -360,6 +384,33 @@ def psnr(image, reference, peak=1.0) -> float:
     return float("inf") if mse == 0.0 else 10.0 * np.log10(peak * peak / mse)
 
 
+def render_splats_pixels(model: OracleModel, cam, width, height, pixels, max_steps=1024,
+                         weight_threshold=1e-3, threads=0):
+    """render_splats at the listed pixel indices (y * width + x) only:
+    rgba [n, 4], steps [n]."""
+    px = np.ascontiguousarray(pixels, dtype=np.uint32)
+    rgba = np.zeros((len(px), 4), dtype=np.float32)
+    steps = np.zeros(len(px), dtype=np.uint32)
+    cs = camera_struct(cam)
+    lib().bvo_render_splats_px(C.byref(model.c), C.byref(cs), width, height, max_steps,
+                               weight_threshold, len(px), _ptr(px, u32p), _ptr(rgba, f32p),
+                               _ptr(steps, u32p), threads)
+    return rgba, steps
+
+
+def render_splats_f64_pixels(model: OracleModel, cam, width, height, pixels, max_steps=1024,
+                             weight_threshold=1e-3, threads=0):
+    """FP64 accuracy oracle of render_splats at the listed pixels: rgba [n, 4]
+    float64 (every quantity in double from the model's FP32 values)."""
+    px = np.ascontiguousarray(pixels, dtype=np.uint32)
+    rgba = np.zeros((len(px), 4), dtype=np.float64)
+    cs = camera_struct(cam)
+    lib().bvo_render_splats_f64_px(C.byref(model.c), C.byref(cs), width, height, max_steps,
+                                   float(weight_threshold), len(px), _ptr(px, u32p),
+                                   _ptr(rgba, f64p), threads)
+    return rgba
+
+
 def record_image(model: OracleModel, cams: Sequence, width, height, max_steps, starts=None,
                  threads=0):
     """Path-recorder rows for every pixel of every camera (PathRecordBuffers
@@ -399,10 +450,14 @@ def render_splats(model: OracleModel, cam, width, height, max_steps=1024, weight
 
 def forward_backward(model: OracleModel, cams: Sequence, width, height, max_steps=1024,
                      weight_threshold=0.0, max_dt=50.0, target=None, loss_kind=0,
-                     override=None, want_grads=True, threads=0, splats=False):
+                     override=None, want_grads=True, threads=0, splats=False, mask=None,
+                     want_mass=False):
     """FP64 training-contract oracle.  Returns dict(loss, rgb, d_density,
     d_sh, d_pos, d_radius).  splats: PowerFoam splat semantics instead of the
-    walk."""
+    walk.  mask ([views, H, W] bool): only those rays are traced and
+    contribute (the loss is still normalised over every ray of the batch).
+    want_mass: also return mass_density, mass_sh, mass_pos, mass_radius, the
+    per-entry FP32 error budget (units of 2^-24) of each gradient table."""
     n = model.n
     K3 = model.sh.size // max(n, 1)
     cam_arr = (Camera * len(cams))(*[camera_struct(c) for c in cams])
@@ -424,14 +479,29 @@ def forward_backward(model: OracleModel, cams: Sequence, width, height, max_step
         rad = None if rad is None else np.ascontiguousarray(rad, dtype=np.float64)
         keep = [pts, sh, rad]
         ov = ParamsF64(_ptr(pts, f64p), _ptr(sh, f64p), _ptr(rad, f64p))
-    loss = lib().bvo_forward_backward_ex(
+    mk = None
+    if mask is not None:
+        mk = np.ascontiguousarray(np.asarray(mask, dtype=bool).reshape(-1), dtype=np.uint8)
+        assert mk.size == len(cams) * width * height
+    mass = None
+    if want_mass and want_grads:
+        mass = dict(density=np.zeros(n), sh=np.zeros(n * K3), pos=np.zeros(n * 3),
+                    radius=np.zeros(n) if model.radii is not None else None)
+    gm = None if mass is None else GradMass(*[_ptr(mass[k], f64p)
+                                              for k in ("density", "sh", "pos", "radius")])
+    loss = lib().bvo_forward_backward_mx(
         C.byref(model.c), cam_arr, len(cams), width, height, max_steps, weight_threshold,
         max_dt, _ptr(tgt, f32p), loss_kind, C.byref(ov) if ov is not None else None,
         _ptr(rgb, f64p), _ptr(rgb32, f32p), _ptr(dd, f64p), _ptr(dsh, f64p), _ptr(dpos, f64p),
-        _ptr(drad, f64p), threads, int(splats))
+        _ptr(drad, f64p), threads, int(splats), _ptr(mk, C.POINTER(C.c_uint8)),
+        C.byref(gm) if gm is not None else None)
     del keep
-    return dict(loss=loss, rgb=rgb, rgb32=rgb32, d_density=dd, d_sh=dsh,
-                d_pos=None if dpos is None else dpos.reshape(n, 3), d_radius=drad)
+    out = dict(loss=loss, rgb=rgb, rgb32=rgb32, d_density=dd, d_sh=dsh,
+               d_pos=None if dpos is None else dpos.reshape(n, 3), d_radius=drad)
+    if mass is not None:
+        out.update(mass_density=mass["density"], mass_sh=mass["sh"],
+                   mass_pos=mass["pos"].reshape(n, 3), mass_radius=mass["radius"])
+    return out
 
 
 # --------------------------------------------------------------------------
@@ -544,6 +614,36 @@ def relight_render(scene: RelightOracleScene, lights, cam, width, height,
     return out, hits
 
 
+def relight_render_pixels(scene: RelightOracleScene, lights, cam, width, height, pixels,
+                          background=(0.0, 0.0, 0.0), threads=0):
+    """relight_render at the listed pixel indices (y * width + x) only."""
+    px = np.ascontiguousarray(pixels, dtype=np.uint32)
+    out = np.zeros((len(px), 4), np.float32)
+    hits = np.zeros(len(px), np.uint32)
+    bg = np.ascontiguousarray(background, np.float32)
+    arr = _lights(lights)
+    cs = camera_struct(cam)
+    lib().bvo_relight_render_px(C.byref(scene.c), arr, len(arr), C.byref(cs), width, height,
+                                _ptr(bg, f32p), len(px), _ptr(px, u32p), _ptr(out, f32p),
+                                _ptr(hits, u32p), threads)
+    return out, hits
+
+
+def relight_render_f64_pixels(scene: RelightOracleScene, lights, cam, width, height, pixels,
+                              background=(0.0, 0.0, 0.0), threads=0):
+    """FP64 accuracy oracle of relight_render at the listed pixels: rgba
+    [n, 4] float64."""
+    px = np.ascontiguousarray(pixels, dtype=np.uint32)
+    out = np.zeros((len(px), 4), np.float64)
+    bg = np.ascontiguousarray(background, np.float32)
+    arr = _lights(lights)
+    cs = camera_struct(cam)
+    lib().bvo_relight_render_f64_px(C.byref(scene.c), arr, len(arr), C.byref(cs), width, height,
+                                    _ptr(bg, f32p), len(px), _ptr(px, u32p), _ptr(out, f64p),
+                                    threads)
+    return out
+
+
 # --------------------------------------------------------------------------
 # Gaussian ray tracing with SH colour (trace.rs:695-773)
 # --------------------------------------------------------------------------
@@ -598,6 +698,21 @@ def gaussian_render(scene: GaussianOracleScene, cam, width, height, min_transmit
     lib().bvo_gaussian_render(C.byref(scene.c), C.byref(cs), width, height, scene.min_opacity,
                               float(min_transmittance), _ptr(bg, f32p), _ptr(out, f32p),
                               _ptr(hits, u32p), threads)
+    return out, hits
+
+
+def gaussian_render_pixels(scene: GaussianOracleScene, cam, width, height, pixels,
+                           min_transmittance=0.01, background=(0.0, 0.0, 0.0), threads=0):
+    """gaussian_render at the listed pixel indices (y * width + x) only."""
+    px = np.ascontiguousarray(pixels, dtype=np.uint32)
+    out = np.zeros((len(px), 4), np.float32)
+    hits = np.zeros(len(px), np.uint32)
+    bg = np.ascontiguousarray(background, np.float32)
+    cs = camera_struct(cam)
+    lib().bvo_gaussian_render_px(C.byref(scene.c), C.byref(cs), width, height,
+                                 scene.min_opacity, float(min_transmittance), _ptr(bg, f32p),
+                                 len(px), _ptr(px, u32p), _ptr(out, f32p), _ptr(hits, u32p),
+                                 threads)
     return out, hits
 
 

@@ -79,3 +79,24 @@ def test_generated_scene_is_valid():
     m = scenes.radfoam_ball(512, seed=3, sh_degree=1)
     assert bv.validate_model(m) is None
     assert 10.0 < m.mean_degree() < 20.0
+
+
+def test_noalloc_wrapper_rejects_bad_tensors():
+    """The Python mirror checks shapes, dtypes and placement before handing
+    device pointers to bv_containing_points_noalloc (no GPU needed)."""
+    torch = pytest.importorskip("torch")
+    q = np.zeros((4, 3), np.float32)
+    good_sites = torch.zeros((8, 4), dtype=torch.float32)
+    good_out = torch.zeros(4, dtype=torch.int32)
+    cases = [
+        (torch.zeros((8, 3), dtype=torch.float32), good_out, "shape"),
+        (torch.zeros((8, 4), dtype=torch.float64), good_out, "float32"),
+        (torch.zeros((4, 8), dtype=torch.float32).t(), good_out, "contiguous"),
+        (good_sites, torch.zeros(3, dtype=torch.int32), "at least 4"),
+        (good_sites, torch.zeros(4, dtype=torch.int64), "int32"),
+        (good_sites, good_out, "CUDA"),
+    ]
+    for sites, out, what in cases:
+        with pytest.raises(ValueError) as e:
+            bv.containing_points_noalloc(sites, q, out)
+        assert what in str(e.value), (what, str(e.value))

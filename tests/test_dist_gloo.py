@@ -18,6 +18,7 @@ torch = pytest.importorskip("torch")
 import torch.distributed as tdist  # noqa: E402
 import torch.multiprocessing as mp  # noqa: E402
 
+import blade_volume_b200 as bv  # noqa: E402
 from blade_volume_b200 import dist as bvdist  # noqa: E402
 from blade_volume_b200 import scenes  # noqa: E402
 from oracle import oracle as O  # noqa: E402
@@ -46,11 +47,19 @@ def worker(rank, port, out_dir):
                              timeout=__import__("datetime").timedelta(seconds=60))
     try:
         g = rank_grads(scene(), rank)
-        tables = {k: torch.from_numpy(np.ascontiguousarray(v).reshape(-1)) for k, v in g.items()}
+        # a plain dict of tables: packed into one bucket, one collective
+        tables = {k: torch.from_numpy(np.array(v, copy=True).reshape(-1)) for k, v in g.items()}
         bvdist.allreduce_grads(tables, tdist)
+        # a tracer's tables (views of one flat buffer): the buffer is reduced
+        flat = bv._grad_tables(len(g["d_density"]), len(g["d_sh"]) // len(g["d_density"]),
+                               False, device="cpu")
+        for k, v in g.items():
+            flat[k].copy_(torch.from_numpy(np.ascontiguousarray(v).reshape(-1)).float())
+        bvdist.allreduce_grads(flat, tdist)
         slowest = bvdist.max_over_ranks([10.0 + rank, 5.0 - rank], tdist, "cpu")
         np.savez(os.path.join(out_dir, f"rank{rank}.npz"), slowest=np.array(slowest),
-                 **{k: v.numpy() for k, v in tables.items()})
+                 **{k: v.numpy() for k, v in tables.items()},
+                 **{"flat_" + k: v.numpy() for k, v in flat.items()})
     finally:
         tdist.destroy_process_group()
 
@@ -73,5 +82,7 @@ def test_gradient_allreduce_across_two_gloo_ranks(tmp_path):
             total = sum(np.asarray(w[k]).reshape(-1) for w in want)
             assert np.abs(total).max() > 0
             np.testing.assert_allclose(got[k], total, rtol=1e-12, atol=1e-15)
+            np.testing.assert_allclose(got["flat_" + k], total.astype(np.float32), rtol=1e-6,
+                                       atol=1e-6 * np.abs(total).max())
     # the ranks rendered different views: their gradients differ
     assert not np.allclose(want[0]["d_density"], want[1]["d_density"])

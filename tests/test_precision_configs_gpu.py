@@ -1,0 +1,165 @@
+"""Per-configuration error of the device paths against FP64 oracles.
+
+Every quantity of the FP64 oracles is a double evaluated from the model's
+FP32 values (the walk: bvo_render_walk_f64; the splat: bvo_render_splats_f64_px;
+the relight: bvo_relight_render_f64_px; gradients: the training contract with
+every segment length and Jacobian re-derived in FP64 along the device's cell
+sequence).  Each test writes its figures to BV_PARITY_LOG (one JSON line,
+"kind": "precision") and holds them to the stated bars:
+
+* images: PSNR over RGB against the FP64 image;
+* gradients: relative error ||g - g64|| / ||g64|| per table, 1e-4 with FP32
+  storage and 2e-3 with BF16 SH storage (the FP64 oracle reads the
+  unrounded FP32 coefficients).
+"""
+
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import blade_volume_b200 as bv  # noqa: E402
+from blade_volume_b200 import dist as bvdist  # noqa: E402
+from blade_volume_b200 import scenes  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+from tests import scene_cache  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+SAMPLES = 2048
+
+
+def log(record):
+    record = dict(record, kind="precision")
+    path = os.environ.get("BV_PARITY_LOG")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps(record) + "\n")
+    print(json.dumps(record))
+
+
+def grad_errors(got, ref):
+    out = {}
+    for t in ("density", "sh", "pos", "radius"):
+        g, r = got.get("d_" + t), ref.get("d_" + t)
+        if g is None or r is None:
+            continue
+        g = np.asarray(g, np.float64).reshape(-1)
+        r = np.asarray(r, np.float64).reshape(-1)
+        nz = np.abs(r) > 0
+        out[t] = {"norm_rel": float(np.linalg.norm(g - r) / np.linalg.norm(r)),
+                  "median_rel": float(np.median(np.abs(g - r)[nz] / np.abs(r)[nz]))}
+    return out
+
+
+def f64_override(model, sh=None):
+    pts = model.points.astype(np.float64)
+    sh64 = (model.sh if sh is None else sh).astype(np.float64)
+    rad = None if model.radii is None else model.radii.astype(np.float64)
+    return pts, sh64, rad
+
+
+def test_config1_image_and_gradients_against_fp64():
+    """262,144 sites, SH 3, 8 x 512^2 (the benchmark workload)."""
+    model = scene_cache.radfoam_ball_262k()
+    cams = bvdist.rank_cameras(8, 0)
+    om = O.OracleModel.from_scene(model)
+    rec = {"config": "radfoam 262,144 sites, SH3 FP32, 8 x 512^2"}
+    for tb in (False, True):
+        t = bv.RadFoamGpuTracer(model, max_steps=1024, weight_threshold=1e-3)
+        t.set_tie_break(tb)
+        img = t.render(cams, 512, 512).cpu().numpy()
+        t.deinit()
+        f64 = np.stack([O.render_walk_f64(om, c, 512, 512, 1024, 1e-3)[0] for c in cams])
+        rec["psnr_tie_break" if tb else "psnr"] = O.psnr(img[..., :3], f64[..., :3])
+    # gradients: 2 of the 8 views keep the FP64 oracle to seconds
+    side = 512
+    target = np.random.default_rng(1).random((2, side, side, 3)).astype(np.float32)
+    t = bv.RadFoamGpuTracer(model)
+    grads = t.new_grads()
+    t.forward_backward(cams[:2], side, side, torch.from_numpy(target).cuda(), grads)
+    torch.cuda.synchronize()
+    got = {k: v.cpu().numpy() for k, v in grads.items()}
+    t.deinit()
+    ref = O.forward_backward(om, cams[:2], side, side, target=target,
+                             override=f64_override(model))
+    rec["gradients_2_views"] = grad_errors(got, ref)
+    log(rec)
+    assert rec["psnr"] > 60.0 and rec["psnr_tie_break"] >= rec["psnr"] - 0.5
+    for tab, e in rec["gradients_2_views"].items():
+        assert e["norm_rel"] <= 1e-4, (tab, e)
+
+
+def sample(views, width, height, seed):
+    rng = np.random.default_rng(seed)
+    return np.sort(rng.choice(views * width * height, SAMPLES, replace=False))
+
+
+def test_config2_splat_image_and_bf16_gradients_against_fp64():
+    """1,048,576-site mixture, SH 3 stored in BF16 on the device, 4 x 1024^2;
+    the FP64 oracles read the unrounded FP32 coefficients."""
+    model = scene_cache.powerfoam_1m(bf16=False)
+    dev_model = scene_cache.powerfoam_1m(bf16=True)
+    cams = bvdist.rank_cameras(4, 0)
+    om = O.OracleModel.from_scene(model)
+    W = H = 1024
+    px = sample(4, W, H, seed=21)
+    t = bv.PowerFoamSplatTracer(dev_model, max_steps=1024, weight_threshold=1e-3)
+    img = t.render(cams, W, H).cpu().numpy().reshape(4, -1, 4)
+    t.deinit()
+    got, ref = [], []
+    for v, cam in enumerate(cams):
+        sel = px[px // (W * H) == v] % (W * H)
+        got.append(img[v, sel])
+        ref.append(O.render_splats_f64_pixels(om, cam, W, H, sel, 1024, 1e-3))
+    got, ref = np.concatenate(got), np.concatenate(ref)
+    rec = {"config": "powerfoam 1,048,576 sites, SH3 BF16, 4 x 1024^2 (2,048 sampled rays)",
+           "psnr_splat": O.psnr(got[:, :3], ref[:, :3]),
+           "max_abs_err": float(np.abs(got - ref).max())}
+    # gradients of the sampled rays: full-size launch, dL/dC zero elsewhere
+    t = bv.PowerFoamSplatTracer(dev_model)
+    grads = t.new_grads()
+    rgb = torch.zeros((4, H, W, 3), dtype=torch.float32, device="cuda")
+    t.forward_backward(cams, W, H, torch.zeros_like(rgb), grads, rgb_out=rgb)
+    target = rgb.cpu().numpy()
+    target.reshape(-1, 3)[px] = np.random.default_rng(22).random((len(px), 3))
+    for g in grads.values():
+        g.zero_()
+    t.forward_backward(cams, W, H, torch.from_numpy(target).cuda(), grads)
+    torch.cuda.synchronize()
+    dev = {k: v.cpu().numpy() for k, v in grads.items()}
+    t.deinit()
+    mask = np.zeros(4 * W * H, bool)
+    mask[px] = True
+    g64 = O.forward_backward(om, cams, W, H, target=target, mask=mask, splats=True,
+                             override=f64_override(model))
+    rec["gradients_bf16_vs_fp64"] = grad_errors(dev, g64)
+    log(rec)
+    assert rec["psnr_splat"] > 40.0
+    for tab, e in rec["gradients_bf16_vs_fp64"].items():
+        assert e["norm_rel"] <= 2e-3, (tab, e)
+
+
+def test_config3_relight_against_fp64():
+    """1,000,000 Gaussians, 16 point lights, 1024 x 768 (2,048 sampled rays)."""
+    g, cam, lights = scenes.relight_workload(1_000_000)
+    t = bv.RelightTracer(g)
+    t.set_point_lights(lights)
+    img = t.render(cam, 1024, 768).cpu().numpy().reshape(-1, 4)
+    t.deinit()
+    px = sample(1, 1024, 768, seed=23)
+    ref = O.relight_render_f64_pixels(O.RelightOracleScene.from_scene(g), lights, cam, 1024,
+                                      768, px)
+    got = img[px].astype(np.float64)
+    peak = float(ref[:, :3].max())
+    rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-3)
+    rec = {"config": "relight 1,000,000 Gaussians, 16 lights, 1024 x 768 (2,048 sampled rays)",
+           "psnr_peak_scaled": O.psnr(got[:, :3], ref[:, :3], peak=peak), "peak": peak,
+           "max_rel_err": float(rel.max()), "p99_rel_err": float(np.quantile(rel, 0.99))}
+    log(rec)
+    # the reference's own GPU-vs-CPU point-light tolerance (relight_gpu_vs_cpu.rs:466)
+    assert rec["p99_rel_err"] <= 2e-3

@@ -6,8 +6,8 @@ record_powerfoam_splats_jacobians does (trace.rs:1421-1452) and evaluates the
 training contract on them in FP64 (its gradients are pinned by central
 differences in tests/test_train_oracle.py).  Bar, as for the walk: forward
 colours bit-exact against the oracle's FP32 restatement, the loss within
-1e-5 relative, every gradient table within 1e-4 of the oracle relative to the
-table's largest entry.
+1e-5 relative, every gradient entry within the element-wise bar of
+tests/gradcheck.py.
 """
 
 import math
@@ -20,6 +20,7 @@ torch = pytest.importorskip("torch")
 import blade_volume_b200 as bv  # noqa: E402
 from blade_volume_b200 import scenes  # noqa: E402
 from oracle import oracle as O  # noqa: E402
+from tests import gradcheck  # noqa: E402
 from tests.test_train_gpu import assert_table  # noqa: E402
 
 pytestmark = pytest.mark.gpu
@@ -46,6 +47,7 @@ def run_gpu(m, cams, target, repeat=1, interval_record=None, **kw):
         loss_out = t.forward_backward(cams, W, H, tg, grads, rgb_out=rgb, **kw)
     torch.cuda.synchronize()
     out = {k: v.cpu().numpy().astype(np.float64) for k, v in grads.items()}
+    out["d_pos"] = out["d_pos"].reshape(-1, 3)
     out["loss"] = float(loss_out.item())
     out["rgb"] = rgb.cpu().numpy()
     t.deinit()
@@ -57,12 +59,10 @@ def test_splat_gradients_match_fp64_oracle(bf16, radius_max):
     m, cams, target = case(bf16=bf16, radius_max=radius_max)
     g = run_gpu(m, cams, target)
     om = O.OracleModel.from_scene(m)
-    ref = O.forward_backward(om, cams, W, H, target=target, splats=True)
+    ref = O.forward_backward(om, cams, W, H, target=target, splats=True, want_mass=True)
     assert abs(g["loss"] - ref["loss"]) <= 1e-5 * ref["loss"]
     assert np.array_equal(g["rgb"].view(np.uint32), ref["rgb32"].view(np.uint32))
-    for k, name in (("d_density", "density"), ("d_sh", "sh"), ("d_radius", "radius")):
-        assert_table(name, g[k], ref[k])
-    assert_table("pos", g["d_pos"].reshape(-1, 3), ref["d_pos"])
+    assert len(gradcheck.check_all(g, ref, where=f"splat bf16={bf16} r={radius_max}")) == 4
 
 
 # The replay walks the forward's recorded intervals of a ray when they all
@@ -75,12 +75,10 @@ def test_interval_record_lengths_match_oracle(entries):
     m, cams, target = case(seed=8, n=3000)
     g = run_gpu(m, cams, target, interval_record=entries)
     om = O.OracleModel.from_scene(m)
-    ref = O.forward_backward(om, cams, W, H, target=target, splats=True)
+    ref = O.forward_backward(om, cams, W, H, target=target, splats=True, want_mass=True)
     assert abs(g["loss"] - ref["loss"]) <= 1e-5 * ref["loss"]
     assert np.array_equal(g["rgb"].view(np.uint32), ref["rgb32"].view(np.uint32))
-    for k, name in (("d_density", "density"), ("d_sh", "sh"), ("d_radius", "radius")):
-        assert_table(name, g[k], ref[k])
-    assert_table("pos", g["d_pos"].reshape(-1, 3), ref["d_pos"])
+    assert len(gradcheck.check_all(g, ref, where=f"splat record {entries}")) == 4
 
 
 def test_splat_training_settings_and_accumulation():
@@ -91,10 +89,10 @@ def test_splat_training_settings_and_accumulation():
         g = run_gpu(m, cams, target, loss=loss, max_dt=max_dt, weight_threshold=thr,
                     max_steps=steps)
         ref = O.forward_backward(om, cams, W, H, target=target, loss_kind=loss, max_dt=max_dt,
-                                 weight_threshold=thr, max_steps=steps, splats=True)
+                                 weight_threshold=thr, max_steps=steps, splats=True,
+                                 want_mass=True)
         assert abs(g["loss"] - ref["loss"]) <= 1e-5 * ref["loss"], (loss, max_dt, thr, steps)
-        assert_table("density", g["d_density"], ref["d_density"])
-        assert_table("sh", g["d_sh"], ref["d_sh"])
+        gradcheck.check_all(g, ref, where=f"splat loss {loss} max_dt {max_dt} thr {thr}")
     once = run_gpu(m, cams, target)
     twice = run_gpu(m, cams, target, repeat=2)
     for k in ("d_density", "d_sh", "d_pos", "d_radius"):

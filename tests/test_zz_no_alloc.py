@@ -49,3 +49,33 @@ def test_noalloc_rejects_more_than_32_queries():
     with pytest.raises(bv.BvError) as e:
         bv.containing_points_noalloc(sites, np.zeros((33, 3), np.float32), out)
     assert e.value.status == 1 and "32" in str(e.value)
+
+
+def test_noalloc_full_scratch_capacity_and_cross_block_ties():
+    """700,000 sites: the search runs its full 296 blocks, so the per-block
+    partials fill the whole fixed array.  Duplicated sites far apart in
+    index (so in different blocks) tie exactly; the lowest index must win.
+    Checked against the FP64 oracle's exhaustive search."""
+    from oracle import oracle as O
+
+    n = 700_000
+    rng = np.random.default_rng(5)
+    xyz = rng.uniform(-1.0, 1.0, (n, 3)).astype(np.float32)
+    radii = rng.uniform(0.0, 0.01, n).astype(np.float32)
+    for lo, hi in [(5, 650_001), (1_000, 420_000), (123_456, 699_999)]:
+        xyz[hi] = xyz[lo]
+        radii[hi] = radii[lo]
+    sites = torch.from_numpy(np.concatenate([xyz, radii[:, None]], axis=1)).cuda()
+    pts = np.concatenate([xyz, np.ones((n, 1), np.float32)], axis=1)
+    om = O.OracleModel(pts, np.zeros((n, 3), np.float32), 0, np.zeros(n + 1, np.uint32),
+                       np.zeros(0, np.uint32), radii)
+    out = torch.full((32,), -1, dtype=torch.int32, device="cuda")
+    for call in range(2):
+        q = rng.uniform(-1.1, 1.1, (32, 3)).astype(np.float32)
+        q[:3] = xyz[[5, 1_000, 123_456]]
+        bv.containing_points_noalloc(sites, q, out)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        want = np.array([O.containing_cell_f64(om, p) for p in q], dtype=np.int32)
+        assert np.array_equal(got, want), (call, got, want)
+        assert list(got[:3]) == [5, 1_000, 123_456]
