@@ -73,6 +73,7 @@ EXPORTED_SYMBOLS = [
     "bv_gaussian_tracer_enable_stats", "bv_gaussian_tracer_last_stats",
     "bv_radfoam_tracer_adam_step", "bv_radfoam_tracer_adam_steps", "bv_radfoam_tracer_read_model",
     "bv_powerfoam_splat_tracer_forward_backward",
+    "bv_radfoam_ply_info", "bv_radfoam_ply_read",
 ]
 DENSITY_IDENTITY, DENSITY_RELU, DENSITY_SOFTPLUS = 0, 1, 2
 SERVE_BATCHED, SERVE_PLAIN, SERVE_PLAIN_BATCH = 0, 1, 2
@@ -93,6 +94,11 @@ class ModelDesc(C.Structure):
                 ("radii", C.POINTER(C.c_float)), ("adjacency_offsets", C.POINTER(C.c_uint32)),
                 ("adjacency_neighbors", C.POINTER(C.c_uint32)), ("flags", C.c_uint32),
                 ("reserved", C.c_uint32)]
+
+
+class PlyInfo(C.Structure):
+    _fields_ = [("num_points", C.c_uint32), ("num_adjacency", C.c_uint32),
+                ("sh_degree", C.c_uint32), ("has_radii", C.c_uint32)]
 
 
 class CameraC(C.Structure):
@@ -216,6 +222,9 @@ def load_library(path: str = LIB_PATH):
     L.bv_last_error.restype = C.c_char_p
     L.bv_abi_version.restype = C.c_uint32
     L.bv_model_validate.argtypes = [C.POINTER(ModelDesc), C.c_char_p, C.c_size_t]
+    L.bv_radfoam_ply_info.argtypes = [C.c_char_p, C.POINTER(PlyInfo)]
+    L.bv_radfoam_ply_read.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]
     L.bv_radfoam_tracer_new.argtypes = [C.POINTER(ModelDesc), C.POINTER(TraceSettings),
                                         C.POINTER(C.c_void_p)]
     L.bv_radfoam_tracer_destroy.argtypes = [C.c_void_p]

@@ -49,9 +49,35 @@ namespace {
 #ifndef BV_SPLAT_SHARED_NUM
 #define BV_SPLAT_SHARED_NUM 1
 #endif
+// Window keys in shared memory (1) or registers (0).
+#ifndef BV_SPLAT_SMEM_WINDOW
+#define BV_SPLAT_SMEM_WINDOW 1
+#endif
 constexpr int kSplatBlock = 128;
 constexpr int kSplatWindow = BV_SPLAT_WINDOW;
 constexpr int kSplatStack = 80;  // > BVH depth, checked at tracer creation
+
+// The window of a splat kernel: SPLAT_WINDOW(Key) declares it (shared memory
+// per thread, or a register array), SPLAT_GATHER runs one pass into it and
+// SPLAT_KEY(i) reads key i.
+#if BV_SPLAT_SMEM_WINDOW
+#define SPLAT_WINDOW(KEY)                                                                      \
+    __shared__ float s_win_t[kSplatWindow * kSplatBlock];                                     \
+    __shared__ uint32_t s_win_idx[kSplatWindow * kSplatBlock];                                \
+    __shared__ uint32_t s_win_pos[kSplatWindow * kSplatBlock];                                \
+    __shared__ uint32_t s_win_aux[sizeof(KEY) == sizeof(WinKey2) ? kSplatWindow * kSplatBlock \
+                                                                  : 1];                       \
+    SmemWindow<kSplatWindow, KEY> win{s_win_t + threadIdx.x, s_win_idx + threadIdx.x,         \
+                                      s_win_pos + threadIdx.x,                                \
+                                      s_win_aux + (sizeof(KEY) == sizeof(WinKey2) ? threadIdx.x : 0), \
+                                      kSplatBlock}
+#define SPLAT_GATHER(...) win_gather_warp_smem<kSplatWindow, kSplatStack>(__VA_ARGS__, win, nodes_visited, hit)
+#define SPLAT_KEY(i) win.get(i)
+#else
+#define SPLAT_WINDOW(KEY) KEY buf[kSplatWindow]
+#define SPLAT_GATHER(...) win_gather_warp<kSplatWindow, kSplatStack>(__VA_ARGS__, buf, nodes_visited, hit)
+#define SPLAT_KEY(i) win_at(buf, i)
+#endif
 // Entry / exit plane of an interval as an offset in its Cech row (16 bits
 // each in the key; rows are at most 65,534 entries, checked at creation).
 constexpr uint32_t kNoPlane = 0xffffu;
@@ -351,17 +377,16 @@ splat_kernel(const __grid_constant__ SplatParams P) {
     auto hit = [&](uint32_t p, bool mine, float limit, auto &k) -> bool {
         return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, k, clipped);
     };
+    SPLAT_WINDOW(WinKey);
     for (;;) {
         const bool want = !finished;
         if (!__any_sync(0xffffffffu, want)) break;
-        WinKey buf[kSplatWindow];
-        const int count = win_gather_warp<kSplatWindow, kSplatStack>(
-            P.nodes, ray, depth, want, cursor_valid, cur_t, cur_cell, buf, nodes_visited, hit);
+        const int count = SPLAT_GATHER(P.nodes, ray, depth, want, cursor_valid, cur_t, cur_cell);
         if (!want) continue;
         // ---- composite the window in order (trace.rs:1490-1530)
 #pragma unroll 1
         for (int i = 0; i < count; ++i) {
-            const WinKey e = win_at(buf, i);
+            const WinKey e = SPLAT_KEY(i);
             if (T <= P.weight_threshold || steps >= P.max_steps) {
                 finished = true;
                 break;
@@ -384,9 +409,10 @@ splat_kernel(const __grid_constant__ SplatParams P) {
         if (count < kSplatWindow) {
             finished = true;
         } else {
+            const auto last = SPLAT_KEY(kSplatWindow - 1);
             cursor_valid = true;
-            cur_t = buf[kSplatWindow - 1].t;
-            cur_cell = buf[kSplatWindow - 1].idx;
+            cur_t = last.t;
+            cur_cell = last.idx;
         }
     }
     if (!active) return;
@@ -539,16 +565,15 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
     auto hit = [&](uint32_t p, bool mine, float limit, auto &k) -> bool {
         return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, k, clipped);
     };
+    SPLAT_WINDOW(WinKey2);
     for (;;) {
         const bool want = !finished;
         if (!__any_sync(0xffffffffu, want)) break;
-        WinKey2 buf[kSplatWindow];
-        const int count = win_gather_warp<kSplatWindow, kSplatStack>(
-            P.nodes, ray, depth, want, cursor_valid, cur_t, cur_cell, buf, nodes_visited, hit);
+        const int count = SPLAT_GATHER(P.nodes, ray, depth, want, cursor_valid, cur_t, cur_cell);
         if (!want) continue;
 #pragma unroll 1
         for (int i = 0; i < count; ++i) {
-            const WinKey2 e = win_at(buf, i);
+            const WinKey2 e = SPLAT_KEY(i);
             if (T <= P.weight_threshold || steps >= P.max_steps) {
                 finished = true;
                 break;
@@ -585,9 +610,10 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
         if (count < kSplatWindow) {
             finished = true;
         } else {
+            const auto last = SPLAT_KEY(kSplatWindow - 1);
             cursor_valid = true;
-            cur_t = buf[kSplatWindow - 1].t;
-            cur_cell = buf[kSplatWindow - 1].idx;
+            cur_t = last.t;
+            cur_cell = last.idx;
         }
     }
     // loss and dL/dC of the pixel (the walk's training epilogue)
@@ -835,16 +861,15 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
     auto hit = [&](uint32_t p, bool mine, float limit, auto &k) -> bool {
         return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, k, clipped);
     };
+    SPLAT_WINDOW(WinKey2);
     for (;;) {
         const bool want = !finished;
         if (!__any_sync(0xffffffffu, want)) break;
-        WinKey2 buf[kSplatWindow];
-        const int count = win_gather_warp<kSplatWindow, kSplatStack>(
-            P.nodes, ray, depth, want, cursor_valid, cur_t, cur_cell, buf, nodes_visited, hit);
+        const int count = SPLAT_GATHER(P.nodes, ray, depth, want, cursor_valid, cur_t, cur_cell);
         if (!want) continue;
 #pragma unroll 1
         for (int i = 0; i < count; ++i) {
-            const WinKey2 e = win_at(buf, i);
+            const WinKey2 e = SPLAT_KEY(i);
             if (T <= P.weight_threshold || steps >= P.max_steps) {
                 finished = true;
                 break;
@@ -866,9 +891,10 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
         if (count < kSplatWindow) {
             finished = true;
         } else {
+            const auto last = SPLAT_KEY(kSplatWindow - 1);
             cursor_valid = true;
-            cur_t = buf[kSplatWindow - 1].t;
-            cur_cell = buf[kSplatWindow - 1].idx;
+            cur_t = last.t;
+            cur_cell = last.idx;
         }
     }
 }

@@ -191,3 +191,110 @@ __device__ __forceinline__ Key win_at(const Key (&buf)[W], int i) {
 }
 
 }  // namespace bv
+
+namespace bv {
+
+// The window of win_gather_warp held in shared memory instead of registers
+// (the W keys are the bulk of a lane's registers; in shared memory they let
+// more warps stay resident).  Key i of thread tid sits at [i][tid] of each
+// field array, so the lanes of a warp touch consecutive words.
+template <int W, class Key>
+struct SmemWindow {
+    float *t;
+    uint32_t *idx, *pos, *aux;  // aux unused for WinKey
+    int stride;
+
+    __device__ __forceinline__ Key get(int i) const {
+        Key k;
+        k.t = t[i * stride];
+        k.idx = idx[i * stride];
+        k.pos = pos[i * stride];
+        get_aux(k, i);
+        return k;
+    }
+    __device__ __forceinline__ void set(int i, const Key &k) {
+        t[i * stride] = k.t;
+        idx[i * stride] = k.idx;
+        pos[i * stride] = k.pos;
+        set_aux(k, i);
+    }
+    __device__ __forceinline__ void get_aux(WinKey &, int) const {}
+    __device__ __forceinline__ void get_aux(WinKey2 &k, int i) const { k.aux = aux[i * stride]; }
+    __device__ __forceinline__ void set_aux(const WinKey &, int) {}
+    __device__ __forceinline__ void set_aux(const WinKey2 &k, int i) { aux[i * stride] = k.aux; }
+};
+
+// win_gather_warp with the window in shared memory: the same traversal,
+// pruning and key order, so a pass ends with the same window.  The
+// window's last key is mirrored in registers for the pruning tests.
+template <int W, int S, class Key, class Hit>
+__device__ __forceinline__ int win_gather_warp_smem(const BvhNode *__restrict__ nodes,
+                                                    const WinRay &ray, float t_end, bool want,
+                                                    bool cursor_valid, float cur_t,
+                                                    uint32_t cur_idx, SmemWindow<W, Key> &win,
+                                                    uint32_t &nodes_visited, Hit hit) {
+    const uint32_t lane = threadIdx.x & 31u;
+    int count = 0;
+    float last_t = __int_as_float(0x7f800000);
+    uint32_t last_idx = 0xffffffffu;
+    WarpStack<S> stack;
+    stack.push(0u, lane);
+    while (stack.sp > 0) {
+        const uint32_t ni = stack.pop();
+        const BvhNode nd = nodes[ni];
+        if (want) nodes_visited += 1;
+        float tn[2], tf[2];
+        bool ok[2];
+        const float4 lo[2] = {nd.l_lo, nd.r_lo}, hi[2] = {nd.l_hi, nd.r_hi};
+        const uint32_t cnts[2] = {__float_as_uint(nd.l_hi.w), __float_as_uint(nd.r_hi.w)};
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            ok[c] = want && cnts[c] != kBvhNoChild &&
+                    win_slab(lo[c], hi[c], ray, t_end, tn[c], tf[c]);
+            if (ok[c] && cursor_valid && tf[c] < cur_t) ok[c] = false;
+            if (ok[c] && count == W && tn[c] > last_t) ok[c] = false;
+        }
+        const uint32_t live0 = __ballot_sync(0xffffffffu, ok[0]);
+        const uint32_t live1 = __ballot_sync(0xffffffffu, ok[1]);
+        const uint32_t near1 = __ballot_sync(0xffffffffu, ok[0] && ok[1] && tn[1] < tn[0]);
+        const uint32_t near0 = __ballot_sync(0xffffffffu, ok[0] && ok[1] && !(tn[1] < tn[0]));
+        const int first = __popc(near1) > __popc(near0) ? 1 : 0;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int c = k == 0 ? 1 - first : first;
+            if ((c == 0 ? live0 : live1) == 0u) continue;
+            const uint32_t ref = __float_as_uint(c == 0 ? nd.l_lo.w : nd.r_lo.w);
+            const uint32_t cnt = cnts[c];
+            if (cnt == 0u) {
+                stack.push(ref, lane);
+                continue;
+            }
+            const bool mine = ok[c];
+            for (uint32_t p = ref; p < ref + cnt; ++p) {
+                Key nk;
+                nk.pos = p;
+                const float limit = count == W ? last_t : __int_as_float(0x7f800000);
+                if (!hit(p, mine, limit, nk)) continue;
+                if (cursor_valid && !win_less(cur_t, cur_idx, nk.t, nk.idx)) continue;
+                if (count == W && !win_less(nk.t, nk.idx, last_t, last_idx)) continue;
+                // insertion: shift the larger keys up one slot (the last one
+                // drops out of a full window)
+                int i = count < W ? count : W - 1;
+                while (i > 0) {
+                    const float ti = win.t[(i - 1) * win.stride];
+                    const uint32_t ii = win.idx[(i - 1) * win.stride];
+                    if (!win_less(nk.t, nk.idx, ti, ii)) break;
+                    win.set(i, win.get(i - 1));
+                    --i;
+                }
+                win.set(i, nk);
+                if (count < W) count += 1;
+                last_t = win.t[(count - 1) * win.stride];
+                last_idx = win.idx[(count - 1) * win.stride];
+            }
+        }
+    }
+    return count;
+}
+
+}  // namespace bv

@@ -468,6 +468,30 @@ bv_status bv_gaussian_tracer_dispatch(bv_gaussian_tracer *tracer, float *out_rgb
 bv_status bv_gaussian_tracer_enable_stats(bv_gaussian_tracer *tracer, uint32_t enabled);
 bv_status bv_gaussian_tracer_last_stats(bv_gaussian_tracer *tracer, bv_launch_stats *out);
 
+/* ---- RadFoam / PowerFoam PLY model files ----------------------------------
+ * The walk subset of blade_volume::io::load_radfoam / try_load
+ * (blade-volume/src/io/radfoam_ply.rs:1141-1213): PLY 1.0, binary
+ * little-endian or ASCII, elements `vertex` (x, y, z, density,
+ * adjacency_offset, blade_sh_dc_0..2 or red/green/blue preview DC,
+ * color_sh_<k>, optional radius) then `adjacency` (one uint per CSR entry),
+ * with the reference's ASCII row rules (comment and blank lines skipped,
+ * extra columns ignored, trailing data an error) and its CSR validation
+ * (:1111-1139).  Oriented-surface and detail properties are rejected
+ * (BV_ERR_INVALID_MODEL; the walk has no such terms).  Two calls: _info for
+ * the sizes, then _read into caller arrays points [n*4] (x, y, z, density),
+ * sh [n*3K] (K = (sh_degree+1)^2, [component][rgb]), offsets [n+1],
+ * neighbors [num_adjacency] and radii [n] (required when has_radii).  The
+ * arrays are a bv_model_desc's inputs.  Host only; no device is touched. */
+typedef struct bv_ply_info {
+    uint32_t num_points;
+    uint32_t num_adjacency;
+    uint32_t sh_degree;
+    uint32_t has_radii;
+} bv_ply_info;
+bv_status bv_radfoam_ply_info(const char *path, bv_ply_info *out);
+bv_status bv_radfoam_ply_read(const char *path, float *points, float *sh, uint32_t *offsets,
+                              uint32_t *neighbors, float *radii);
+
 /* ---- allocation-free start-cell search -----------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
  * hosts whose device memory is owned by their own pool (a renderer's frame

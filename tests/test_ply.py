@@ -1,6 +1,9 @@
 """RadFoam PLY reader/writer (blade_volume_b200.ply), the walk subset of the
 reference's loader (blade-volume/src/io/radfoam_ply.rs)."""
 
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -125,3 +128,49 @@ def test_rebuild_adjacency_after_moving_sites():
     p = scenes.powerfoam_mixture(300, seed=3, sh_degree=0, radius_max=0.2)
     fresh = scenes.rebuild_adjacency(p)
     assert np.array_equal(fresh.offsets, p.offsets) and np.array_equal(fresh.neighbors, p.neighbors)
+
+
+REFERENCE_FIXTURE = "/root/reference/blade-volume/tests/data/radfoam_tiny_ascii.ply"
+
+
+@pytest.mark.skipif(not os.path.exists(REFERENCE_FIXTURE),
+                    reason="the reference checkout is not present on this machine")
+def test_loads_the_reference_ascii_fixture():
+    """The reference's own fixture file (tests/data/radfoam_tiny_ascii.ply,
+    loaded by tests/radfoam_cpu_ref.rs:16-42): body comment lines, rows with
+    more columns than declared, preview colours.  Parsed points and CSR equal
+    the transcription in tests/golden/reference_cases.json, the SH rows are
+    the preview DC of grey 128 with zero rest, and the reference test's ray
+    traces to a finite colour with steps > 0."""
+    m = ply.load_radfoam_ply(REFERENCE_FIXTURE)
+    with open(os.path.join(os.path.dirname(__file__), "golden", "reference_cases.json")) as f:
+        cases = {c["name"]: c for c in json.load(f)["cases"]}
+    want = cases["cpu_ref_traces_without_nan_on_tiny_fixture"]["model"]
+    assert np.array_equal(m.points, np.asarray(want["points"], np.float32))
+    assert np.array_equal(m.offsets, np.asarray(want["offsets"], np.uint32))
+    assert np.array_equal(m.neighbors, np.asarray(want["neighbors"], np.uint32))
+    assert m.sh_degree == 1  # 9 color_sh_* rest coefficients declared
+    # preview DC of (128, 128, 128) (radfoam_ply.rs:722-726), SH rest all 0
+    dc = (np.float32(128) / np.float32(255.0) - np.float32(0.5)) / np.float32(0.2820948)
+    assert np.all(m.sh[:, :3] == dc) and np.all(m.sh[:, 3:] == 0.0)
+    assert bv.validate_model(m) is None
+    om = O.OracleModel.from_scene(m)
+    s = O.settings(max_steps=16, weight_threshold=1e-4, start_point=0, depth=100.0,
+                   eval_mode=O.EVAL_CONSTANT, constant_rgb=(1.0, 1.0, 1.0))
+    r = O.trace_one_ray(om, (0.5, 0.5, -1.0), (0.0, 0.0, 1.0), s)
+    assert all(np.isfinite(r.rgba[i]) for i in range(4)) and 0.0 <= r.rgba[3] <= 1.0
+    assert r.steps > 0
+
+
+def test_binary_and_ascii_files_read_alike(tmp_path):
+    """The C reader gives the same arrays for the binary and the ASCII form
+    of one model (floats written with repr, so they round-trip exactly)."""
+    m = scenes.powerfoam_mixture(400, seed=9, sh_degree=2, radius_max=0.2, bf16=False)
+    a, b = str(tmp_path / "m.bin.ply"), str(tmp_path / "m.txt.ply")
+    ply.save_radfoam_ply(m, a, binary=True)
+    ply.save_radfoam_ply(m, b, binary=False)
+    same_model(ply.load_radfoam_ply(a), ply.load_radfoam_ply(b))
+    with open(b, "a") as f:
+        f.write("7\n")
+    with pytest.raises(ply.PlyError, match="trailing"):
+        ply.load_radfoam_ply(b)
