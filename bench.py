@@ -693,11 +693,25 @@ def run_serving(args):
     clocks = sampler.stop()
     top = f"{rates[-1]:g}"
     b, p = out["batched"][top], out["plain"][top]
+
+    def hd_frames(mode):
+        """1920x1080 frame latencies (ms) of a mode at every rate."""
+        res = {}
+        for rate, r in out[mode].items():
+            d = r["per_resolution"].get("1920x1080", {})
+            res[rate] = {k: d.get(k, {}).get("p99_ms") for k in
+                         ("first_frame", "frame_interval", "frame")}
+        return res
     line = {"metric": "serving Mrays/s", "value": b["mrays_per_s"], "unit": "Mrays/s",
             "higher_is_better": True, "n_gpus": 1, "dtype": "f32", "data": "synthetic",
             "plain_value": p["mrays_per_s"],
             "plain_batch_value": out["plain_batch"][top]["mrays_per_s"],
             "vs_plain": b["mrays_per_s"] / p["mrays_per_s"] if p["mrays_per_s"] else None,
+            "fwdbwd_mrays_per_s": b["fwdbwd_mrays_per_s"],
+            "fwdbwd_vs_plain": (b["fwdbwd_mrays_per_s"] / p["fwdbwd_mrays_per_s"]
+                                if p["fwdbwd_mrays_per_s"] else None),
+            "p99_ms_1080p_batched": hd_frames("batched"),
+            "p99_ms_1080p_plain": hd_frames("plain"),
             "config": {"workload": "serving", "scene_sites": sites, "sh_degree": 3,
                        "resolutions": ["256x256", "512x512", "1280x720", "1920x1080"],
                        "views": "1-16", "fwdbwd_fraction": 0.1, "rates": rates,

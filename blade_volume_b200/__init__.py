@@ -34,7 +34,8 @@ LIB_PATH = os.environ.get("BV_B200_LIBRARY", os.path.join(HERE, "libbv_b200.so")
 BV_OK = 0
 STATUS_NAMES = {0: "BV_OK", 1: "BV_ERR_INVALID_ARGUMENT", 2: "BV_ERR_INVALID_MODEL",
                 3: "BV_ERR_CUDA", 4: "BV_ERR_OUT_OF_MEMORY", 5: "BV_ERR_CANDIDATE_OVERFLOW",
-                6: "BV_ERR_NOT_SUPPORTED", 7: "BV_ERR_NO_DEVICE", 8: "BV_ERR_TIMEOUT"}
+                6: "BV_ERR_NOT_SUPPORTED", 7: "BV_ERR_NO_DEVICE", 8: "BV_ERR_TIMEOUT",
+                9: "BV_ERR_CANCELLED"}
 MODEL_SH_BF16 = 0x1
 PATH_TRUNCATED = 0x80000000
 LOSS_L2, LOSS_L1 = 0, 1
@@ -57,7 +58,7 @@ EXPORTED_SYMBOLS = [
     "bv_relight_tracer_enable_stats", "bv_relight_tracer_last_stats",
     "bv_server_new", "bv_server_add_scene", "bv_server_scene_grads", "bv_server_start",
     "bv_server_submit", "bv_server_wait", "bv_server_stats_get", "bv_server_clock",
-    "bv_server_destroy",
+    "bv_server_destroy", "bv_server_cancel",
     "bv_powerfoam_splat_tracer_new", "bv_powerfoam_splat_tracer_destroy",
     "bv_powerfoam_splat_tracer_dispatch", "bv_powerfoam_splat_tracer_dispatch_batch",
     "bv_powerfoam_splat_tracer_validate_candidate_counts",
@@ -80,6 +81,7 @@ SERVE_BATCHED, SERVE_PLAIN, SERVE_PLAIN_BATCH = 0, 1, 2
 REQUEST_RENDER, REQUEST_FORWARD_BACKWARD = 0, 1
 SCENE_GRADIENTS = 0x1
 BV_ERR_TIMEOUT = 8
+BV_ERR_CANCELLED = 9
 
 
 class BvError(RuntimeError):
@@ -181,7 +183,8 @@ class ServerSettings(C.Structure):
                 ("max_batch_rays", C.c_uint32), ("max_batch_views", C.c_uint32),
                 ("slots", C.c_uint32), ("max_steps", C.c_uint32), ("weight_threshold", C.c_float),
                 ("max_train_rays", C.c_uint64), ("use_graphs", C.c_uint32),
-                ("reserved", C.c_uint32 * 3)]
+                ("train_chunk_rays", C.c_uint32), ("frame_period_us", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class RequestC(C.Structure):
@@ -204,7 +207,8 @@ class ServerStats(C.Structure):
                 ("graph_launches", C.c_uint64), ("kernel_launches", C.c_uint64),
                 ("arena_bytes", C.c_uint64), ("arena_peak_bytes", C.c_uint64),
                 ("resident_bytes", C.c_uint64), ("admission_waits", C.c_uint64),
-                ("busy_s", C.c_double)]
+                ("busy_s", C.c_double), ("arena_used_bytes", C.c_uint64),
+                ("requests_cancelled", C.c_uint64)]
 
 
 _lib = None
@@ -279,6 +283,7 @@ def load_library(path: str = LIB_PATH):
     L.bv_server_submit.argtypes = [C.c_void_p, C.POINTER(RequestC), C.POINTER(C.c_uint64)]
     L.bv_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(RequestResult)]
     L.bv_server_stats_get.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+    L.bv_server_cancel.argtypes = [C.c_void_p, C.c_uint64]
     L.bv_server_clock.argtypes = [C.c_void_p]
     L.bv_server_clock.restype = C.c_double
     L.bv_server_destroy.argtypes = [C.c_void_p]
@@ -911,7 +916,7 @@ class Server:
     def __init__(self, hbm_budget_bytes: int, mode: str = "batched", max_batch_rays: int = 0,
                  max_batch_views: int = 0, slots: int = 0, max_steps: int = 1024,
                  weight_threshold: float = 0.001, max_train_rays: int = 0,
-                 use_graphs: bool = True):
+                 use_graphs: bool = True, train_chunk_rays: int = 0, frame_period_us: int = 0):
         L = load_library()
         s = ServerSettings()
         s.hbm_budget_bytes = int(hbm_budget_bytes)
@@ -924,6 +929,8 @@ class Server:
         s.weight_threshold = weight_threshold
         s.max_train_rays = max_train_rays
         s.use_graphs = 1 if use_graphs else 0
+        s.train_chunk_rays = train_chunk_rays
+        s.frame_period_us = frame_period_us
         h = C.c_void_p()
         _check(L.bv_server_new(C.byref(s), C.byref(h)))
         self._h = h
@@ -996,6 +1003,11 @@ class Server:
         return dict(id=res.id, status=res.status, kind=res.kind, submit_s=res.submit_s,
                     admit_s=res.admit_s, start_s=res.start_s, done_s=res.done_s, rays=res.rays,
                     message=res.message.decode(errors="replace"))
+
+    def cancel(self, rid: int):
+        """bv_server_cancel: withdraw a request (wait() then reports status
+        BV_ERR_CANCELLED unless it had finished already)."""
+        _check(load_library().bv_server_cancel(self._h, rid))
 
     def stats(self) -> dict:
         st = ServerStats()

@@ -114,6 +114,8 @@ struct bv_tracer {
     uint32_t *step_rec = nullptr;      // training forward's step record, read by the replay
     size_t step_rec_capacity = 0;      // words
     uint32_t step_rec_steps = kExitRecSteps;  // recorded steps per ray
+    bool step_rec_owned = true;        // false: lent by a serving engine
+    uint32_t train_chunk = 0;          // work items per training launch pair (0: a whole group)
     int grid_forward = 0;
     int grid_train_fwd = 0;
     int grid_train_bwd = 0;
@@ -154,7 +156,7 @@ void free_tracer(bv_tracer *t) {
     cudaFree(t->faces);
     if (t->ray_state_owned) cudaFree(t->ray_state);
     cudaFree(t->site_grads);
-    cudaFree(t->step_rec);
+    if (t->step_rec_owned) cudaFree(t->step_rec);
     cudaFree(t->start_cells);
     cudaFree(t->work_counter);
     cudaFree(t->stats);
@@ -256,6 +258,18 @@ void bv::tracer_lend_ray_state(bv_tracer *t, RayState *buffer, size_t capacity) 
     t->ray_state = buffer;
     t->ray_state_capacity = capacity;
     t->ray_state_owned = false;
+}
+
+void bv::tracer_lend_step_record(bv_tracer *t, uint32_t *buffer, size_t words) {
+    if (t->step_rec_owned) cudaFree(t->step_rec);
+    t->step_rec = buffer;
+    t->step_rec_capacity = buffer ? words : 0;
+    t->step_rec_owned = false;
+}
+
+void bv::tracer_set_train_chunk(bv_tracer *t, uint32_t work_items) {
+    // whole 8x4 tiles, so that a chunk's rays keep their tile-major record lines
+    t->train_chunk = (work_items + kTileRays - 1) / kTileRays * kTileRays;
 }
 
 extern "C" {
@@ -528,7 +542,7 @@ bv_status bv_radfoam_tracer_set_tie_break(bv_tracer *t, uint32_t mode) {
 bv_status bv_radfoam_tracer_set_exit_record(bv_tracer *t, uint32_t steps) {
     if (!t) return fail(BV_ERR_INVALID_ARGUMENT, "null tracer");
     t->step_rec_steps = steps;
-    if (steps == 0) {
+    if (steps == 0 && t->step_rec_owned) {
         cudaFree(t->step_rec);
         t->step_rec = nullptr;
         t->step_rec_capacity = 0;
@@ -649,14 +663,15 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         BV_CUDA(cudaMalloc(&t->ray_state, sizeof(RayState) * chunk_rays), "cudaMalloc ray state");
         t->ray_state_capacity = chunk_rays;
     }
-    // step record: the first rec_steps steps of every ray, within
-    // kExitRecBytes; a tracer whose scratch is lent by a serving engine
-    // (which budgets its device memory itself) and any steps past the record
-    // replay the exit-face search and the SH evaluation instead
+    // step record: the first rec_steps steps of every ray of a launch, within
+    // kExitRecBytes (or the buffer a serving engine lends, which budgets its
+    // device memory itself); steps past the record replay the exit-face
+    // search and the SH evaluation instead
+    const size_t group_work =
+        (size_t)std::min<uint32_t>(n_cams, kMaxViewsPerLaunch) * padded_rays(width, height);
+    const size_t chunk_work = t->train_chunk ? std::min<size_t>(t->train_chunk, group_work) : group_work;
     uint32_t rec_steps = 0;
-    if (t->ray_state_owned) {
-        const size_t chunk_work =
-            (size_t)std::min<uint32_t>(n_cams, kMaxViewsPerLaunch) * padded_rays(width, height);
+    if (t->step_rec_owned) {
         const size_t fit = kExitRecBytes / (chunk_work * kStepRecWords * sizeof(uint32_t));
         rec_steps = (uint32_t)std::min<size_t>({(size_t)t->step_rec_steps, (size_t)ts->max_steps, fit});
         const size_t need = chunk_work * rec_steps * kStepRecWords;
@@ -672,6 +687,10 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
                 rec_steps = 0;
             }
         }
+    }
+    if (!t->step_rec_owned && t->step_rec) {
+        const size_t fit = t->step_rec_capacity / (chunk_work * kStepRecWords);
+        rec_steps = (uint32_t)std::min<size_t>({(size_t)t->step_rec_steps, (size_t)ts->max_steps, fit});
     }
     bv_status st = begin_timing(t, s);
     if (st != BV_OK) return st;
@@ -697,7 +716,6 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
             work += padded_rays(width, height);
         }
         const size_t off = (size_t)c0 * width * height;
-        p.total_work = work;
         p.start_cells = t->start_cells;
         p.work_counter = t->work_counter;
         p.target = target + 3 * off;
@@ -710,14 +728,19 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         p.stats = t->stats_enabled ? t->stats : nullptr;
         p.step_rec = rec_steps ? t->step_rec : nullptr;
         p.rec_steps = rec_steps;
-        BV_CUDA(cudaMemsetAsync(t->work_counter, 0, 2 * sizeof(uint32_t), s), "counter reset");
-        const int blocks_needed = std::max((int)((work + 255) / 256), 1);
-        BV_CUDA(launch_train_forward(p, std::min(t->grid_train_fwd, blocks_needed), s),
-                "training forward launch");
-        if (t->stats_enabled && c0 == 0) BV_CUDA(cudaEventRecord(t->ev[3], s), "event");
-        BV_CUDA(launch_train_backward(p, std::min(t->grid_train_bwd, blocks_needed), s),
-                "training backward launch");
-        t->last_launches += 3;
+        t->last_launches += 1;  // start cells
+        for (uint32_t b = 0; b < work; b += (uint32_t)chunk_work) {
+            p.work_begin = b;
+            p.total_work = std::min<uint32_t>((uint32_t)chunk_work, work - b);
+            BV_CUDA(cudaMemsetAsync(t->work_counter, 0, 2 * sizeof(uint32_t), s), "counter reset");
+            const int blocks_needed = std::max((int)((p.total_work + 255) / 256), 1);
+            BV_CUDA(launch_train_forward(p, std::min(t->grid_train_fwd, blocks_needed), s),
+                    "training forward launch");
+            if (t->stats_enabled && c0 == 0 && b == 0) BV_CUDA(cudaEventRecord(t->ev[3], s), "event");
+            BV_CUDA(launch_train_backward(p, std::min(t->grid_train_bwd, blocks_needed), s),
+                    "training backward launch");
+            t->last_launches += 2;
+        }
     }
     if (grads->d_positions_dev || grads->d_radii_dev) {
         BV_CUDA(launch_fold_site_grads(t->site_grads, t->n, grads->d_positions_dev,

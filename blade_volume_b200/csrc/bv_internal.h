@@ -110,6 +110,7 @@ struct TrainParams {
     unsigned long long *stats;
     uint32_t *step_rec;           // exit face + SH colour per (ray, step < rec_steps), or null
     uint32_t rec_steps;           // 0: the replay searches and evaluates every step
+    uint32_t work_begin;          // this launch covers work items [work_begin, +total_work)
     ViewDesc views[kMaxViewsPerLaunch];
 };
 
@@ -233,5 +234,13 @@ size_t tracer_device_bytes(const bv_tracer *t);
 // Hand the tracer a caller-owned ray-state buffer for bv_forward_backward
 // (chunks larger than capacity are refused instead of growing it).
 void tracer_lend_ray_state(bv_tracer *t, RayState *buffer, size_t capacity);
+// Hand the tracer a caller-owned step-record buffer (words) for
+// bv_forward_backward; the tracer never grows a lent record.
+void tracer_lend_step_record(bv_tracer *t, uint32_t *buffer, size_t words);
+// bv_forward_backward issues its forward and replay kernels over at most this
+// many work items (tile-padded rays) per launch pair, so that the launches
+// of one call stay short and other work on the device interleaves between
+// them (0: one launch pair per group of 32 views).  Results are the same.
+void tracer_set_train_chunk(bv_tracer *t, uint32_t work_items);
 
 }  // namespace bv

@@ -8,18 +8,23 @@
 // renders bit for bit as bv_radfoam_tracer_dispatch_batch renders it.
 //
 // One scheduler thread owns every CUDA call after bv_server_start.  Its loop:
+//   0. cancel: withdrawn requests drop their frames that are not launched;
 //   1. retire: batches whose frame copies have landed, forward+backward
 //      requests whose last copy has landed; a request whose outputs are all
 //      on the host is done and its device buffers go back to the arena;
 //   2. admit: pending requests in arrival order, while the head's buffers
 //      fit in the arena (the budget left after scenes and scratch);
 //   3. launch: while a batch slot is free and frames are waiting, pack
-//      frames in admission order (up to max_batch_rays rays and
+//      frames earliest-due first (frame k of a request is due k + 1 frame
+//      periods after its arrival; up to max_batch_rays rays and
 //      max_batch_views frames) into the slot's pinned table and replay the
 //      slot's graph: table upload, work-counter reset, start cells, walk.
 //      The slot's copy stream then moves each frame to its host buffer.
-// Slots run on their own streams, so one batch's tail overlaps the next
-// batch; forward+backward requests run on a further stream beside them.
+// Slots run on their own high-priority streams, so one batch's tail overlaps
+// the next batch and a frame's blocks are scheduled ahead of training work;
+// forward+backward requests run on a low-priority stream beside them, in
+// launch pairs of at most train_chunk_rays work items, each short enough
+// that waiting frames get the SMs between them.
 
 #include <cuda_runtime.h>
 
@@ -49,6 +54,11 @@ constexpr size_t kGranule = 256;
 constexpr uint32_t kDefaultBatchRays = 1u << 21;  // one 1920x1080 frame (2,073,600 rays)
 constexpr uint32_t kDefaultBatchViews = 256;
 constexpr uint64_t kDefaultTrainRays = 16ull * 1920 * 1080;
+constexpr uint32_t kDefaultTrainChunk = 1u << 19;
+constexpr uint32_t kDefaultFramePeriodUs = 16000;
+// Training step record of the serving engine: this many steps per ray of a
+// launch pair (the replay recomputes steps past it).
+constexpr uint32_t kServeRecSteps = 256;
 
 size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -118,6 +128,7 @@ class Arena {
     }
     size_t size() const { return size_; }
     size_t peak() const { return peak_; }
+    size_t used() const { return used_; }
 
   private:
     size_t size_ = 0, used_ = 0, peak_ = 0;
@@ -138,8 +149,13 @@ struct Request {
     int status = BV_OK;
     std::string message;
     bool done = false;
+    bool cancel = false;       // withdrawn: finish as soon as nothing of it is on the device
     cudaEvent_t ev = nullptr;  // forward+backward: last copy landed
 };
+
+// A frame waiting for a batch, ordered by due time (then submission order).
+using FrameKey = std::pair<double, uint64_t>;
+using FrameQueue = std::multimap<FrameKey, std::pair<Request *, uint32_t>>;
 
 struct Scene {
     bv_tracer *t = nullptr;
@@ -176,6 +192,7 @@ struct bv_server {
     void *arena_base = nullptr;
     Arena arena;
     RayState *ray_state = nullptr;
+    uint32_t *step_rec = nullptr;  // training step record lent to every scene's tracer
     size_t resident = 0;
     std::vector<Slot> slots;
     cudaStream_t train_stream = nullptr;
@@ -192,9 +209,11 @@ struct bv_server {
     std::string fatal;
     bv_server_stats st{};   // published copy, read under mu
     bv_server_stats wst{};  // scheduler's own counters
+    std::vector<uint64_t> cancels;  // ids withdrawn since the scheduler last looked
     std::thread worker;
     // scheduler thread only
-    std::deque<std::pair<Request *, uint32_t>> frames;
+    FrameQueue frames;
+    uint64_t frame_seq = 0;
     std::deque<Request *> train_inflight;
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
@@ -255,6 +274,7 @@ void publish(bv_server *sv) {
     o.admission_waits = w.admission_waits;
     o.busy_s = w.busy_s;
     o.arena_peak_bytes = sv->arena.peak();
+    o.arena_used_bytes = sv->arena.used();
 }
 
 void finish_request(bv_server *sv, Request *q, double t) {
@@ -265,10 +285,15 @@ void finish_request(bv_server *sv, Request *q, double t) {
     std::lock_guard<std::mutex> lk(sv->mu);
     q->t_done = t;
     q->done = true;
+    if (q->cancel && q->status == BV_OK) {
+        q->status = BV_ERR_CANCELLED;
+        q->message = "cancelled";
+    }
     if (q->status == BV_OK) {
         sv->st.requests_done += 1;
         sv->st.rays_done += q->rays;
     }
+    if (q->status == BV_ERR_CANCELLED) sv->st.requests_cancelled += 1;
     publish(sv);
     sv->cv_done.notify_all();
 }
@@ -302,8 +327,8 @@ bv_status launch_batch(bv_server *sv, Slot &sl) {
     const double t = sv->now();
     sl.frames.clear();
     while (!sv->frames.empty() && n < sv->s.max_batch_views) {
-        Request *q = sv->frames.front().first;
-        const uint32_t v = sv->frames.front().second;
+        Request *q = sv->frames.begin()->second.first;
+        const uint32_t v = sv->frames.begin()->second.second;
         const uint32_t w = q->r.width, hh = q->r.height;
         const uint32_t fr = tile_padded_rays(w, hh);
         if (n > 0 && (uint64_t)work + fr > sv->s.max_batch_rays) break;
@@ -314,7 +339,7 @@ bv_status launch_batch(bv_server *sv, Slot &sl) {
         row.out = reinterpret_cast<uint64_t>(q->out_dev + (size_t)v * w * hh);
         if (q->t_start < 0) q->t_start = t;
         sl.frames.emplace_back(q, v);
-        sv->frames.pop_front();
+        sv->frames.erase(sv->frames.begin());
         work += fr;
         ++n;
     }
@@ -407,6 +432,31 @@ void scheduler(bv_server *sv) {
     double busy_since = -1.0;
     for (;;) {
         bool progress = false;
+        // 0. withdrawn requests: drop their frames that are not launched
+        std::vector<uint64_t> cancels;
+        {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            cancels.swap(sv->cancels);
+        }
+        for (uint64_t id : cancels) {
+            Request *q = nullptr;
+            {
+                std::lock_guard<std::mutex> lk(sv->mu);
+                auto it = sv->live.find(id);
+                if (it != sv->live.end() && !it->second->done) q = it->second.get();
+            }
+            if (!q || q->r.kind != BV_REQUEST_RENDER || !q->has_mem) continue;
+            for (auto it = sv->frames.begin(); it != sv->frames.end();) {
+                if (it->second.first == q) {
+                    it = sv->frames.erase(it);
+                    q->frames_left -= 1;
+                } else {
+                    ++it;
+                }
+            }
+            if (q->frames_left == 0) finish_request(sv, q, sv->now());
+            progress = true;
+        }
         // 1. retire
         for (auto &sl : sv->slots) {
             if (!sl.busy) continue;
@@ -492,7 +542,10 @@ void scheduler(bv_server *sv) {
             }
             if (q->r.kind == BV_REQUEST_RENDER) {
                 q->frames_left = q->r.n_views;
-                for (uint32_t v = 0; v < q->r.n_views; ++v) sv->frames.emplace_back(q, v);
+                const double period = 1e-6 * sv->s.frame_period_us;
+                for (uint32_t v = 0; v < q->r.n_views; ++v)
+                    sv->frames.emplace(FrameKey(q->t_submit + period * (v + 1), sv->frame_seq++),
+                                       std::make_pair(q, v));
                 continue;
             }
             q->t_start = sv->now();
@@ -550,6 +603,7 @@ void free_server(bv_server *sv) {
     }
     if (sv->train_stream) cudaStreamDestroy(sv->train_stream);
     cudaFree(sv->ray_state);
+    cudaFree(sv->step_rec);
     cudaFree(sv->arena_base);
     delete sv;
 }
@@ -569,6 +623,8 @@ bv_status bv_server_new(const bv_server_settings *settings, bv_server **out) {
     if (s.slots == 0) s.slots = 2;
     if (s.max_steps == 0) s.max_steps = 1024;
     if (s.max_train_rays == 0) s.max_train_rays = kDefaultTrainRays;
+    if (s.train_chunk_rays == 0) s.train_chunk_rays = kDefaultTrainChunk;
+    if (s.frame_period_us == 0) s.frame_period_us = kDefaultFramePeriodUs;
     if (s.max_batch_views > (uint32_t)kMaxServeViews)
         return sfail(BV_ERR_INVALID_ARGUMENT, "max_batch_views above %d", kMaxServeViews);
     if (s.slots > 4) return sfail(BV_ERR_INVALID_ARGUMENT, "at most 4 batch slots");
@@ -657,10 +713,22 @@ bv_status bv_server_start(bv_server *sv) {
     resident += sizeof(RayState) * s.max_train_rays;
     for (auto &sc : sv->scenes) tracer_lend_ray_state(sc.t, sv->ray_state, s.max_train_rays);
     sv->table_bytes = sizeof(ServeHeader) + sizeof(ServeView) * s.max_batch_views;
+    // training step record, shared by the scenes' tracers (one training
+    // request runs at a time, on the training stream)
+    const size_t rec_words = (size_t)s.train_chunk_rays * kServeRecSteps * 4;
+    SV_CUDA(cudaMalloc(&sv->step_rec, rec_words * sizeof(uint32_t)), "training step record");
+    resident += rec_words * sizeof(uint32_t);
+    for (auto &sc : sv->scenes) {
+        tracer_lend_step_record(sc.t, sv->step_rec, rec_words);
+        tracer_set_train_chunk(sc.t, s.train_chunk_rays);
+    }
+    // frames on the highest stream priority, training on the lowest
+    int prio_low = 0, prio_high = 0;
+    SV_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high), "stream priorities");
     sv->slots.resize(s.slots);
     for (auto &sl : sv->slots) {
-        SV_CUDA(cudaStreamCreateWithFlags(&sl.compute, cudaStreamNonBlocking), "stream");
-        SV_CUDA(cudaStreamCreateWithFlags(&sl.copy, cudaStreamNonBlocking), "stream");
+        SV_CUDA(cudaStreamCreateWithPriority(&sl.compute, cudaStreamNonBlocking, prio_high), "stream");
+        SV_CUDA(cudaStreamCreateWithPriority(&sl.copy, cudaStreamNonBlocking, prio_high), "stream");
         SV_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), "event");
         SV_CUDA(cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming), "event");
         SV_CUDA(cudaHostAlloc(&sl.host_table, sv->table_bytes, cudaHostAllocDefault), "pinned table");
@@ -674,7 +742,7 @@ bv_status bv_server_start(bv_server *sv) {
         resident += 2 * sv->table_bytes + sizeof(uint32_t) * (1 + 2 * kMaxServeViews) +
                     sizeof(double) * kMaxServeViews * kServeStartBlocks;
     }
-    SV_CUDA(cudaStreamCreateWithFlags(&sv->train_stream, cudaStreamNonBlocking), "stream");
+    SV_CUDA(cudaStreamCreateWithPriority(&sv->train_stream, cudaStreamNonBlocking, prio_low), "stream");
     sv->resident = resident;
     if (resident >= s.hbm_budget_bytes)
         return sfail(BV_ERR_OUT_OF_MEMORY, "HBM budget %llu below the resident %zu bytes",
@@ -805,6 +873,31 @@ bv_status bv_server_wait(bv_server *sv, uint64_t id, double timeout_s, bv_reques
     out->rays = q->rays;
     std::snprintf(out->message, sizeof(out->message), "%s", q->message.c_str());
     sv->live.erase(it);
+    return BV_OK;
+}
+
+bv_status bv_server_cancel(bv_server *sv, uint64_t id) {
+    if (!sv) return sfail(BV_ERR_INVALID_ARGUMENT, "null server");
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->live.find(id);
+    if (it == sv->live.end()) return sfail(BV_ERR_INVALID_ARGUMENT, "unknown request %llu", (unsigned long long)id);
+    Request *q = it->second.get();
+    if (q->done || q->cancel) return BV_OK;
+    q->cancel = true;
+    auto p = std::find(sv->pending.begin(), sv->pending.end(), q);
+    if (p != sv->pending.end()) {  // not admitted: nothing of it is on the device
+        sv->pending.erase(p);
+        q->status = BV_ERR_CANCELLED;
+        q->message = "cancelled";
+        q->t_done = sv->now();
+        q->done = true;
+        sv->st.requests_cancelled += 1;
+        sv->cv_done.notify_all();
+        return BV_OK;
+    }
+    sv->cancels.push_back(id);
+    lk.unlock();
+    sv->cv_work.notify_one();
     return BV_OK;
 }
 

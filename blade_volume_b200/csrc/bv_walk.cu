@@ -479,7 +479,7 @@ train_forward_kernel(const __grid_constant__ TrainParams P) {
         uint32_t w;
         if (refill(P.work_counter, P.total_work, active, drained, w)) {
             uint32_t view, x, y;
-            if (work_item(P, w, view, x, y)) {
+            if (work_item(P, P.work_begin + w, view, x, y)) {
                 const ViewDesc &vd = P.views[view];
                 pix = pixel_index(P, view, x, y);
                 const bool ok = make_ray(vd, x, y, W.ray);
@@ -615,7 +615,7 @@ train_backward_kernel(const __grid_constant__ TrainParams P) {
         uint32_t w;
         if (refill(P.work_counter + 1, P.total_work, active, drained, w)) {
             uint32_t view, x, y;
-            if (work_item(P, w, view, x, y)) {
+            if (work_item(P, P.work_begin + w, view, x, y)) {
                 const ViewDesc &vd = P.views[view];
                 const size_t pix = pixel_index(P, view, x, y);
                 const bool ok = make_ray(vd, x, y, W.ray);

@@ -8,7 +8,11 @@ server's clock), waits for all of them and reports aggregate Mrays/s and
 p50/p99 latencies, each measured from the request's scheduled arrival:
   request      until every output of the request is on the host;
   first_frame  until its first frame (view) is on the host;
-  frame        until each frame is on the host (one sample per frame).
+  frame        until each frame is on the host (one sample per frame);
+  frame_interval  the time a viewer of the request waits for each frame: the
+               first frame from arrival, every later one from the frame
+               before it (frames in the order they landed).
+Forward+backward work is also summarised as Mrays/s over the stream's span.
 
 Host buffers: each resolution has one pinned output sink and one pinned
 target, shared by every request of that resolution (the outputs overwrite
@@ -136,7 +140,8 @@ def run_stream(server, specs: Sequence[RequestSpec], bufs: HostBuffers,
         rid = server.submit(spec.scene, spec.cameras, spec.width, spec.height,
                             frame_done=frame_done, **bufs.request_args(spec))
         sub.append((rid, spec, due, frame_done))
-    lat, frame_lat, first_lat = [], [], []
+    lat, frame_lat, first_lat, gaps = [], [], [], []
+    fwdbwd_rays = 0
     per_res: Dict[str, Dict[str, list]] = {}
     per_kind: Dict[str, list] = {"render": [], "fwdbwd": []}
     rays = 0
@@ -150,7 +155,10 @@ def run_stream(server, specs: Sequence[RequestSpec], bufs: HostBuffers,
         rays += spec.rays
         end = max(end, r["done_s"])
         key = f"{spec.width}x{spec.height}"
-        d = per_res.setdefault(key, dict(request=[], frame=[], first_frame=[]))
+        d = per_res.setdefault(key, dict(request=[], frame=[], first_frame=[],
+                                         frame_interval=[]))
+        if spec.fwdbwd:
+            fwdbwd_rays += spec.rays
         lat.append(r["done_s"] - due)
         d["request"].append(r["done_s"] - due)
         per_kind["fwdbwd" if spec.fwdbwd else "render"].append(r["done_s"] - due)
@@ -159,6 +167,10 @@ def run_stream(server, specs: Sequence[RequestSpec], bufs: HostBuffers,
         d["frame"].extend(f)
         first_lat.append(min(f))
         d["first_frame"].append(min(f))
+        landed = sorted(f)
+        g = [landed[0]] + [b - a for a, b in zip(landed, landed[1:])]
+        gaps.extend(g)
+        d["frame_interval"].extend(g)
     span = end - t0
     ms = 1e3
 
@@ -168,8 +180,9 @@ def run_stream(server, specs: Sequence[RequestSpec], bufs: HostBuffers,
 
     return dict(requests=len(specs), failures=failures, rays=rays, span_s=span,
                 mrays_per_s=rays / span / 1e6 if span > 0 else None,
+                fwdbwd_mrays_per_s=fwdbwd_rays / span / 1e6 if span > 0 else None,
                 request_latency=pct(lat), first_frame_latency=pct(first_lat),
-                frame_latency=pct(frame_lat),
+                frame_latency=pct(frame_lat), frame_interval=pct(gaps),
                 per_kind={k: pct(v) for k, v in per_kind.items()},
                 per_resolution={k: {m: pct(x) for m, x in v.items()}
                                 for k, v in sorted(per_res.items())},

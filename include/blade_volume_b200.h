@@ -46,6 +46,8 @@ typedef enum bv_status {
     BV_ERR_NO_DEVICE = 7,
     /* bv_server_wait: the request has not finished within the timeout */
     BV_ERR_TIMEOUT = 8,
+    /* a serving request withdrawn by bv_server_cancel */
+    BV_ERR_CANCELLED = 9,
 } bv_status;
 
 /* cudaStream_t; NULL selects the legacy default stream. */
@@ -524,12 +526,14 @@ bv_status bv_containing_points_noalloc(const float *sites_dev, uint32_t num_site
  *   - a request is admitted when its device buffers fit in the HBM budget
  *     left after the scenes and fixed scratch (first in, first admitted);
  *   - BV_SERVE_BATCHED: the frames (views) of all admitted render requests
- *     are packed into batches, each ONE start-cell launch plus ONE persistent
- *     traversal launch over every frame in it (any scene, any size), replayed
- *     from a captured CUDA graph; up to `slots` batches run concurrently on
- *     their own streams, and each frame is copied to the host as soon as its
- *     batch finishes.  Forward+backward requests run on a stream of their own
- *     beside the batches;
+ *     are packed into batches, earliest-due frame first, each ONE start-cell
+ *     launch plus ONE persistent traversal launch over every frame in it (any
+ *     scene, any size), replayed from a captured CUDA graph; up to `slots`
+ *     batches run concurrently on their own high-priority streams, and each
+ *     frame is copied to the host as soon as its batch finishes.
+ *     Forward+backward requests run on a low-priority stream of their own
+ *     beside the batches, in launch pairs of at most train_chunk_rays work
+ *     items with the training step record, so that frames interleave;
  *   - BV_SERVE_PLAIN: one request at a time through the tracer calls, one
  *     bv_radfoam_tracer_dispatch per view (the reference's tracer takes one
  *     camera per dispatch), or bv_forward_backward, then a synchronize: the
@@ -557,7 +561,13 @@ typedef struct bv_server_settings {
     float weight_threshold;     /* transmittance cut, e.g. 0.001 */
     uint64_t max_train_rays;    /* largest forward+backward chunk (<= 32 views); 0 = 16 x 1920 x 1080 */
     uint32_t use_graphs;        /* 1: replay captured graphs, 0: launch directly */
-    uint32_t reserved[3];
+    uint32_t train_chunk_rays;  /* forward+backward work per launch pair (tile-padded rays);
+                                   0 = 524,288: each pair lasts a few ms, so frames
+                                   interleave between them */
+    uint32_t frame_period_us;   /* frame k of a request is due (k + 1) periods after its
+                                   arrival; batches take the earliest-due frames first;
+                                   0 = 16,000 */
+    uint32_t reserved;
 } bv_server_settings;
 
 /* Scene flag: the server keeps gradient tables for the scene, into which
@@ -597,6 +607,8 @@ typedef struct bv_server_stats {
     uint64_t arena_bytes, arena_peak_bytes, resident_bytes;
     uint64_t admission_waits;     /* times the head request did not fit */
     double busy_s;                /* wall time with work on the device */
+    uint64_t arena_used_bytes;    /* request buffers held right now */
+    uint64_t requests_cancelled;
 } bv_server_stats;
 
 bv_status bv_server_new(const bv_server_settings *settings, bv_server **out);
@@ -616,6 +628,14 @@ bv_status bv_server_submit(bv_server *server, const bv_request *request, uint64_
  * forgotten.  BV_ERR_TIMEOUT if it has not finished, BV_ERR_INVALID_ARGUMENT
  * for an unknown id. */
 bv_status bv_server_wait(bv_server *server, uint64_t id, double timeout_s, bv_request_result *out);
+/* Withdraws request id.  A request not yet admitted finishes at once; an
+ * admitted render request drops its frames that have not been launched and
+ * finishes when its launched frames have landed; a forward+backward request
+ * already on the device finishes when its work ends.  Either way its device
+ * buffers go back to the arena, bv_server_wait reports BV_ERR_CANCELLED as
+ * the request's status, and its host outputs are incomplete.  BV_OK also
+ * for a request that had already finished (its status is then its own). */
+bv_status bv_server_cancel(bv_server *server, uint64_t id);
 bv_status bv_server_stats_get(bv_server *server, bv_server_stats *out);
 double bv_server_clock(const bv_server *server);
 /* Finishes queued work, stops the scheduler, frees everything. */

@@ -120,7 +120,11 @@ def test_same_alone_and_in_mix(models, reference_tracers):
         assert np.array_equal(bits(m), bits(a))
 
 
-def test_forward_backward_requests_in_the_mix(models, reference_tracers):
+@pytest.mark.parametrize("chunk", [0, 1024], ids=["one-launch-pair", "chunks-of-1024-rays"])
+def test_forward_backward_requests_in_the_mix(models, reference_tracers, chunk):
+    """chunk: the server's training launch pairs cover at most this many
+    work items (0: its default, larger than these requests), with the step
+    record lent by the server; the results are the tracer's own."""
     w, h = 48, 40
     cams = scenes.sphere_cameras(3, 3.0, 9, math.radians(55.0), w / h, 100.0)
     target = np.random.default_rng(2).random((3, h, w, 3)).astype(np.float32)
@@ -132,7 +136,7 @@ def test_forward_backward_requests_in_the_mix(models, reference_tracers):
     loss_ref = t.forward_backward(cams, w, h, tgt_dev, g_ref, rgb_out=rgb_ref,
                                   weight_threshold=0.0, max_dt=50.0)
     torch.cuda.synchronize()
-    server = new_server(models)
+    server = new_server(models, train_chunk_rays=chunk)
     try:
         renders = make_requests(len(models), 10, seed=3)
         ids = []
@@ -233,3 +237,46 @@ def test_rejects_bad_requests(models):
             server.wait(12345, 0.1)
     finally:
         server.close()
+
+
+def test_cancel_withdraws_requests_and_returns_their_arena_bytes(models, reference_tracers):
+    """Requests queued behind a small arena are withdrawn: each finishes with
+    BV_ERR_CANCELLED (or, if it had already finished, with its own status
+    and a correct image), the arena holds no bytes once everything is done,
+    and cancelling a finished request changes nothing."""
+    probe = new_server(models, budget=1 << 30)
+    resident = probe.stats()["resident_bytes"]
+    probe.close()
+    w = h = 256
+    frame = 4 * w * h * 16
+    server = new_server(models, budget=resident + 2 * frame + 4096)
+    try:
+        reqs = []
+        for i in range(10):
+            cams = scenes.sphere_cameras(4, 3.0, 40 + i, math.radians(55.0), 1.0, 100.0)
+            reqs.append(dict(scene=i % len(models), cams=cams, w=w, h=h))
+        outs, ids = [], []
+        for r in reqs:
+            out = np.zeros((4, h, w, 4), np.float32)
+            ids.append(server.submit(r["scene"], r["cams"], w, h, out=out))
+            outs.append(out)
+        for rid in ids[2:]:
+            server.cancel(rid)
+        results = [server.wait(rid, 120.0) for rid in ids]
+        st = server.stats()
+        done = server.submit(0, reqs[0]["cams"][:1], 8, 8, out=np.zeros((1, 8, 8, 4), np.float32))
+        res_done = server.wait(done, 60.0)
+        with pytest.raises(bv.BvError):
+            server.cancel(done)  # forgotten once waited for
+    finally:
+        server.close()
+    assert res_done["status"] == 0
+    statuses = [r["status"] for r in results]
+    assert set(statuses) <= {0, bv.BV_ERR_CANCELLED}, statuses
+    assert statuses[0] == 0 and statuses[1] == 0
+    assert statuses.count(bv.BV_ERR_CANCELLED) >= 4
+    assert st["requests_cancelled"] == statuses.count(bv.BV_ERR_CANCELLED)
+    assert st["arena_used_bytes"] == 0
+    for r, out, res in zip(reqs, outs, results):
+        if res["status"] == 0:
+            assert np.array_equal(bits(out), bits(expected(reference_tracers, r)))

@@ -45,7 +45,7 @@ def test_abi_struct_sizes():
     assert C.sizeof(bv.ServerSettings) == 56
     assert C.sizeof(bv.RequestC) == 112
     assert C.sizeof(bv.RequestResult) == 184
-    assert C.sizeof(bv.ServerStats) == 88
+    assert C.sizeof(bv.ServerStats) == 104
 
 
 def test_poisson_stream_statistics():
