@@ -44,6 +44,10 @@ constexpr int kWalkBlock = 256;
 #ifndef BV_REC_PREFETCH
 #define BV_REC_PREFETCH 1
 #endif
+// Exit search: skip the division of faces that provably cannot win (1).
+#ifndef BV_EXIT_DIV_SAVER
+#define BV_EXIT_DIV_SAVER 1
+#endif
 constexpr int kFaceUnroll = BV_FACE_UNROLL;
 
 
@@ -167,7 +171,7 @@ __device__ __forceinline__ bool find_exit(const DeviceModel &m, const Cell &c, c
             if (k + u < c.end) {
                 float num, dp;
                 if (face_exit_nd<BOUNDED>(c, ri2, site[u], ray, num, dp) &&
-                    (TIE || !quotient_not_below(num, dp, best))) {
+                    (TIE || !BV_EXIT_DIV_SAVER || !quotient_not_below(num, dp, best))) {
                     const float t = num / dp;
                     if (isfinite(t) && t > t0 && t < best) {
                         if (TIE) {

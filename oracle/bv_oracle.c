@@ -1231,15 +1231,22 @@ static void add_mass(const bvo_grad_mass *mass, const seg_eval_t *ev, const seg_
         egs += ge[ch] * fabs(D) + fabs(g[ch]) * eD;
     }
     if (mass->density) atomic_add_d(&mass->density[cell], ev->dt * egs + fabs(ev->dt * gs));
+    if (mass->count_density) atomic_add_d(&mass->count_density[cell], 1.0);
     const double ew = ev->Et * ev->alpha + ev->T + ev->w; /* budget of w = T alpha */
     if (mass->sh) {
         for (int ch = 0; ch < 3; ++ch) {
-            /* a colour within its rounding of 0 may clamp either way */
-            if (!(ev->cu[ch] > 0.0 || fabs(ev->cu[ch]) <= 64.0 * u32 * ev->csum[ch])) continue;
+            /* a colour within its FP32 rounding of 0 may clamp either way:
+             * then the whole term may be present on one side and absent on
+             * the other, an error of the term itself (|term| / 2^-24 in these
+             * units) */
+            const int near0 = fabs(ev->cu[ch]) <= 64.0 * u32 * ev->csum[ch];
+            if (!(ev->cu[ch] > 0.0 || near0)) continue;
             for (uint32_t mm = 0; mm < K; ++mm) {
+                const double term = fabs(g[ch] * ev->w * Y[mm]);
                 const double v = (ge[ch] * ev->w + fabs(g[ch]) * ew) * fabs(Y[mm]) +
-                                 fabs(g[ch] * ev->w * Y[mm]);
+                                 (near0 ? term / u32 : term);
                 atomic_add_d(&mass->sh[(size_t)cell * 3 * K + 3 * mm + ch], v);
+                if (mass->count_sh) atomic_add_d(&mass->count_sh[(size_t)cell * 3 * K + 3 * mm + ch], 1.0);
             }
         }
     }
@@ -1249,12 +1256,17 @@ static void add_mass(const bvo_grad_mass *mass, const seg_eval_t *ev, const seg_
         const double *js[3] = {ev->j_prev, ev->j_cur, ev->j_next};
         const double gdt = ev->sigma * gs, egdt = ev->sigma * egs + fabs(gdt);
         for (int r = 0; r < 3; ++r) {
-            if (want_pos && mass->pos)
-                for (int a = 0; a < 3; ++a)
-                    if (js[r][a] != 0.0)
-                        atomic_add_d(&mass->pos[3 * (size_t)who[r] + a], egdt * fabs(js[r][a]));
-            if (want_radius && mass->radius && js[r][3] != 0.0)
+            if (want_pos && mass->pos) {
+                for (int a = 0; a < 3; ++a) {
+                    if (js[r][a] == 0.0) continue;
+                    atomic_add_d(&mass->pos[3 * (size_t)who[r] + a], egdt * fabs(js[r][a]));
+                    if (mass->count_pos) atomic_add_d(&mass->count_pos[3 * (size_t)who[r] + a], 1.0);
+                }
+            }
+            if (want_radius && mass->radius && js[r][3] != 0.0) {
                 atomic_add_d(&mass->radius[who[r]], egdt * fabs(js[r][3]));
+                if (mass->count_radius) atomic_add_d(&mass->count_radius[who[r]], 1.0);
+            }
         }
     }
     for (int ch = 0; ch < 3; ++ch) Se[ch] += ew * ev->c[ch] + ev->w * ev->csum[ch];

@@ -199,12 +199,16 @@ double bvo_forward_backward_ex(const bvo_model *m, const bvo_camera *cams, uint3
  * transmittance product, 1 - alpha, the SH sum, dL/dC through the colour,
  * the suffix, the scatter), in units of 2^-24.  An FP32 implementation of
  * the contract then differs from the FP64 gradient by at most a small
- * multiple of 2^-24 times this mass.  Any table may be NULL. */
+ * multiple of 2^-24 times this mass, plus the error of summing the entry's
+ * terms in FP32 in any order, at most (count - 1) 2^-24 times the sum of
+ * their magnitudes (which the mass bounds); count_* holds each entry's
+ * number of terms.  Any table may be NULL. */
 typedef struct {
     double *density; /* [n] */
     double *sh;      /* [n*3K] */
     double *pos;     /* [n*3] */
     double *radius;  /* [n] */
+    double *count_density, *count_sh, *count_pos, *count_radius; /* same shapes */
 } bvo_grad_mass;
 
 /* bvo_forward_backward_ex restricted to the rays whose ray_mask byte is

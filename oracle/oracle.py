@@ -100,7 +100,9 @@ EVAL_OPACITY, EVAL_CONSTANT, EVAL_SH = 0, 1, 2
 
 
 class GradMass(C.Structure):
-    _fields_ = [("density", f64p), ("sh", f64p), ("pos", f64p), ("radius", f64p)]
+    _fields_ = [("density", f64p), ("sh", f64p), ("pos", f64p), ("radius", f64p),
+                ("count_density", f64p), ("count_sh", f64p), ("count_pos", f64p),
+                ("count_radius", f64p)]
 
 
 def lib():
@@ -457,7 +459,8 @@ def forward_backward(model: OracleModel, cams: Sequence, width, height, max_step
     walk.  mask ([views, H, W] bool): only those rays are traced and
     contribute (the loss is still normalised over every ray of the batch).
     want_mass: also return mass_density, mass_sh, mass_pos, mass_radius, the
-    per-entry FP32 error budget (units of 2^-24) of each gradient table."""
+    per-entry FP32 error budget (units of 2^-24) of each gradient table, and
+    count_<table>, the number of terms summed into each entry."""
     n = model.n
     K3 = model.sh.size // max(n, 1)
     cam_arr = (Camera * len(cams))(*[camera_struct(c) for c in cams])
@@ -484,11 +487,16 @@ def forward_backward(model: OracleModel, cams: Sequence, width, height, max_step
         mk = np.ascontiguousarray(np.asarray(mask, dtype=bool).reshape(-1), dtype=np.uint8)
         assert mk.size == len(cams) * width * height
     mass = None
+    tables = ("density", "sh", "pos", "radius")
     if want_mass and want_grads:
-        mass = dict(density=np.zeros(n), sh=np.zeros(n * K3), pos=np.zeros(n * 3),
-                    radius=np.zeros(n) if model.radii is not None else None)
-    gm = None if mass is None else GradMass(*[_ptr(mass[k], f64p)
-                                              for k in ("density", "sh", "pos", "radius")])
+        sizes = dict(density=n, sh=n * K3, pos=n * 3, radius=n)
+        mass = {}
+        for k in tables:
+            has = k != "radius" or model.radii is not None
+            mass[k] = np.zeros(sizes[k]) if has else None
+            mass["count_" + k] = np.zeros(sizes[k]) if has else None
+    gm = None if mass is None else GradMass(*[_ptr(mass[k], f64p) for k in tables],
+                                            *[_ptr(mass["count_" + k], f64p) for k in tables])
     loss = lib().bvo_forward_backward_mx(
         C.byref(model.c), cam_arr, len(cams), width, height, max_steps, weight_threshold,
         max_dt, _ptr(tgt, f32p), loss_kind, C.byref(ov) if ov is not None else None,
@@ -500,7 +508,9 @@ def forward_backward(model: OracleModel, cams: Sequence, width, height, max_step
                d_pos=None if dpos is None else dpos.reshape(n, 3), d_radius=drad)
     if mass is not None:
         out.update(mass_density=mass["density"], mass_sh=mass["sh"],
-                   mass_pos=mass["pos"].reshape(n, 3), mass_radius=mass["radius"])
+                   mass_pos=mass["pos"].reshape(n, 3), mass_radius=mass["radius"],
+                   count_density=mass["count_density"], count_sh=mass["count_sh"],
+                   count_pos=mass["count_pos"].reshape(n, 3), count_radius=mass["count_radius"])
     return out
 
 

