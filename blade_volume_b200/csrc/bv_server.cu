@@ -714,10 +714,17 @@ bv_status bv_server_start(bv_server *sv) {
     for (auto &sc : sv->scenes) tracer_lend_ray_state(sc.t, sv->ray_state, s.max_train_rays);
     sv->table_bytes = sizeof(ServeHeader) + sizeof(ServeView) * s.max_batch_views;
     // training step record, shared by the scenes' tracers (one training
-    // request runs at a time, on the training stream)
-    const size_t rec_words = (size_t)s.train_chunk_rays * kServeRecSteps * 4;
-    SV_CUDA(cudaMalloc(&sv->step_rec, rec_words * sizeof(uint32_t)), "training step record");
-    resident += rec_words * sizeof(uint32_t);
+    // request runs at a time, on the training stream): kServeRecSteps steps
+    // of every ray of a launch pair, within an eighth of the HBM budget (a
+    // smaller record holds fewer steps per ray; the replay recomputes the
+    // rest; below one step per ray there is none)
+    size_t rec_words = (size_t)s.train_chunk_rays * kServeRecSteps * 4;
+    rec_words = std::min<size_t>(rec_words, s.hbm_budget_bytes / 8 / sizeof(uint32_t));
+    if (rec_words < (size_t)s.train_chunk_rays * 4) rec_words = 0;
+    if (rec_words) {
+        SV_CUDA(cudaMalloc(&sv->step_rec, rec_words * sizeof(uint32_t)), "training step record");
+        resident += rec_words * sizeof(uint32_t);
+    }
     for (auto &sc : sv->scenes) {
         tracer_lend_step_record(sc.t, sv->step_rec, rec_words);
         tracer_set_train_chunk(sc.t, s.train_chunk_rays);

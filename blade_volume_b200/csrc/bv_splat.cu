@@ -53,6 +53,11 @@ namespace {
 #ifndef BV_SPLAT_SMEM_WINDOW
 #define BV_SPLAT_SMEM_WINDOW 1
 #endif
+// Cech-row clip: each chunk of a row staged in the warp's shared memory (1)
+// or broadcast lane to lane with shuffles (0).
+#ifndef BV_SPLAT_SMEM_ROWS
+#define BV_SPLAT_SMEM_ROWS 1
+#endif
 constexpr int kSplatBlock = 128;
 constexpr int kSplatWindow = BV_SPLAT_WINDOW;
 constexpr int kSplatStack = 80;  // > BVH depth, checked at tracer creation
@@ -189,6 +194,20 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
         // with the normal.
         const float num_own = dot3(fp.x - ray.ox, fp.y - ray.oy, fp.z - ray.oz, fn.x, fn.y, fn.z);
 #endif
+#if BV_SPLAT_SMEM_ROWS && BV_SPLAT_SHARED_NUM
+        // The chunk (numerator and normal of each entry) goes to the warp's
+        // slice of shared memory once; every lane that still clips then
+        // reads the entries it needs (broadcast reads) and leaves the row
+        // alone as soon as its interval is empty.
+        __shared__ float4 s_row[kSplatBlock];
+        float4 *row = s_row + (threadIdx.x & ~31u);
+        __syncwarp();
+        row[lane] = make_float4(num_own, fn.x, fn.y, fn.z);
+        __syncwarp();
+        for (uint32_t j = 0; j < n && !empty; ++j) {
+            const float4 e = row[j];
+            const float num = e.x, nx = e.y, ny = e.z, nz = e.w;
+#else
         for (uint32_t j = 0; j < n; ++j) {
 #if BV_SPLAT_SHARED_NUM
             const float num = __shfl_sync(0xffffffffu, num_own, j);
@@ -201,6 +220,7 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
             const float ny = __shfl_sync(0xffffffffu, fn.y, j);
             const float nz = __shfl_sync(0xffffffffu, fn.z, j);
             if (empty) continue;
+#endif
 #if !BV_SPLAT_SHARED_NUM
             const float rx = fx - ray.ox, ry = fy - ray.oy, rz = fz - ray.oz;
             const float num = dot3(rx, ry, rz, nx, ny, nz);

@@ -206,6 +206,38 @@ static void sh_basis_d(uint32_t deg, const double d[3], double Y[16]) {
     }
 }
 
+/* Magnitudes that an FP32 evaluation of each basis value rounds: the basis
+ * with every difference turned into a sum (3 zz - 1 -> 3 zz + 1, ...), so
+ * that a basis value near a zero of its polynomial carries the error of its
+ * unreduced terms (error-budget use only). */
+static void sh_basis_mag_d(uint32_t deg, const double d[3], double M[16]) {
+    const double x = fabs(d[0]), y = fabs(d[1]), z = fabs(d[2]);
+    const double xx = x * x, yy = y * y, zz = z * z;
+    for (int i = 0; i < 16; ++i) M[i] = 0.0;
+    M[0] = fabs((double)SH_C[0]);
+    if (deg >= 1) {
+        M[1] = fabs((double)SH_C[1]) * y;
+        M[2] = fabs((double)SH_C[2]) * z;
+        M[3] = fabs((double)SH_C[3]) * x;
+    }
+    if (deg >= 2) {
+        M[4] = fabs((double)SH_C[4]) * x * y;
+        M[5] = fabs((double)SH_C[5]) * y * z;
+        M[6] = fabs((double)SH_C[6]) * (3.0 * zz + 1.0);
+        M[7] = fabs((double)SH_C[7]) * x * z;
+        M[8] = fabs((double)SH_C[8]) * (xx + yy);
+    }
+    if (deg >= 3) {
+        M[9] = fabs((double)SH_C[9]) * y * (3.0 * xx + yy);
+        M[10] = fabs((double)SH_C[10]) * x * y * z;
+        M[11] = fabs((double)SH_C[11]) * y * (5.0 * zz + 1.0);
+        M[12] = fabs((double)SH_C[12]) * z * (5.0 * zz + 3.0);
+        M[13] = fabs((double)SH_C[13]) * x * (5.0 * zz + 1.0);
+        M[14] = fabs((double)SH_C[14]) * z * (xx + yy);
+        M[15] = fabs((double)SH_C[15]) * x * (xx + 3.0 * yy);
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* geometry kernels of the walk                                        */
 /* ------------------------------------------------------------------ */
@@ -1147,8 +1179,8 @@ typedef struct {
 } seg_eval_t;
 
 static void eval_segment(const dparams *P, uint32_t K, const double o[3], const double d[3],
-                         const double Y[16], const seg_t *sg, double depth, int use_f32_interval,
-                         seg_eval_t *ev) {
+                         const double Y[16], const double Ymag[16], const seg_t *sg, double depth,
+                         int use_f32_interval, seg_eval_t *ev) {
     memset(ev, 0, sizeof(*ev));
     double t_start = 0.0, t_end = 0.0;
     double jc[4], ja[4];
@@ -1197,7 +1229,7 @@ static void eval_segment(const dparams *P, uint32_t K, const double o[3], const 
         double acc = 0.0, mag = 0.5;
         for (uint32_t k = 0; k < K; ++k) {
             acc += Y[k] * c[3 * k + ch];
-            mag += fabs(Y[k] * c[3 * k + ch]);
+            mag += Ymag[k] * fabs(c[3 * k + ch]);
         }
         ev->cu[ch] = 0.5 + acc;
         ev->c[ch] = ev->cu[ch] > 0.0 ? ev->cu[ch] : 0.0;
@@ -1220,7 +1252,8 @@ static inline void atomic_add_d(double *p, double v) {
  * relative rounding of its operands' magnitudes, 1 - alpha carries one
  * rounding of 1, and an error budget propagates through every factor. */
 static void add_mass(const bvo_grad_mass *mass, const seg_eval_t *ev, const seg_t *sg,
-                     uint32_t cell, uint32_t K, const double Y[16], const double g[3],
+                     uint32_t cell, uint32_t K, const double Y[16], const double Ymag[16],
+                     const double g[3],
                      const double ge[3], const double S[3], double Se[3], double gs, double Tn,
                      float max_dt, int want_pos, int want_radius, double u32) {
     const double Etn = ev->Et * (1.0 - ev->alpha) + ev->T + Tn; /* budget of T_{k+1} */
@@ -1244,7 +1277,7 @@ static void add_mass(const bvo_grad_mass *mass, const seg_eval_t *ev, const seg_
             for (uint32_t mm = 0; mm < K; ++mm) {
                 const double term = fabs(g[ch] * ev->w * Y[mm]);
                 const double v = (ge[ch] * ev->w + fabs(g[ch]) * ew) * fabs(Y[mm]) +
-                                 (near0 ? term / u32 : term);
+                                 fabs(g[ch]) * ev->w * Ymag[mm] + (near0 ? term / u32 : term);
                 atomic_add_d(&mass->sh[(size_t)cell * 3 * K + 3 * mm + ch], v);
                 if (mass->count_sh) atomic_add_d(&mass->count_sh[(size_t)cell * 3 * K + 3 * mm + ch], 1.0);
             }
@@ -1367,6 +1400,8 @@ double bvo_forward_backward_mx(const bvo_model *m, const bvo_camera *cams, uint3
             if (out_rgb32)
                 for (int ch = 0; ch < 3; ++ch) out_rgb32[3 * (size_t)i + ch] = rgb32[ch];
             sh_basis_d(deg, d, Y);
+            double Ymag[16];
+            sh_basis_mag_d(deg, d, Ymag);
             double T = 1.0;
             /* FP32 error budget of the device's forward, in units of 2^-24:
              * Et bounds |T32 - T| before segment k (each 1 - alpha carries
@@ -1375,7 +1410,7 @@ double bvo_forward_backward_mx(const bvo_model *m, const bvo_camera *cams, uint3
             double Et = 0.0, Cerr[3] = {0.0, 0.0, 0.0};
             for (int k = 0; k < nseg; ++k) {
                 seg_eval_t *ev = &evs[k];
-                eval_segment(&P, K, o, d, Y, &segs[k], (double)cams[v].depth,
+                eval_segment(&P, K, o, d, Y, Ymag, &segs[k], (double)cams[v].depth,
                              override_params == NULL, ev);
                 double dt = ev->dt_raw;
                 if (dt < 0.0) dt = 0.0;
@@ -1433,7 +1468,7 @@ double bvo_forward_backward_mx(const bvo_model *m, const bvo_camera *cams, uint3
                 for (int ch = 0; ch < 3; ++ch) gs += g[ch] * (Tn * ev->c[ch] - S[ch]);
                 const uint32_t cell = segs[k].cell;
                 if (mass) {
-                    add_mass(mass, ev, segs + k, cell, K, Y, g, ge, S, Se, gs, Tn, max_dt,
+                    add_mass(mass, ev, segs + k, cell, K, Y, Ymag, g, ge, S, Se, gs, Tn, max_dt,
                              d_pos != NULL, d_radius != NULL, u32);
                 }
 #ifdef _OPENMP
