@@ -905,7 +905,7 @@ def main():
     #             16-byte step record, per ray 48 B of state, and the tables
     #             touched once (face table, sites, gradient tables read and
     #             written)
-    #   gather    the reference's per-step byte model: every face
+    #   gather    the reference layout's per-step byte model: every face
     #             gather, CSR row and SH row counted, most of them served by
     #             L1/L2; gathered bytes per second, not a bandwidth
     K = 16
