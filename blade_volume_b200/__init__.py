@@ -80,6 +80,7 @@ DENSITY_IDENTITY, DENSITY_RELU, DENSITY_SOFTPLUS = 0, 1, 2
 SERVE_BATCHED, SERVE_PLAIN, SERVE_PLAIN_BATCH = 0, 1, 2
 REQUEST_RENDER, REQUEST_FORWARD_BACKWARD = 0, 1
 SCENE_GRADIENTS = 0x1
+SERVE_NO_RECORD = 0xFFFFFFFF
 BV_ERR_TIMEOUT = 8
 BV_ERR_CANCELLED = 9
 
@@ -184,7 +185,7 @@ class ServerSettings(C.Structure):
                 ("slots", C.c_uint32), ("max_steps", C.c_uint32), ("weight_threshold", C.c_float),
                 ("max_train_rays", C.c_uint64), ("use_graphs", C.c_uint32),
                 ("train_chunk_rays", C.c_uint32), ("frame_period_us", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("train_record_steps", C.c_uint32)]
 
 
 class RequestC(C.Structure):
@@ -911,12 +912,15 @@ class Server:
     persistent traversal launch per batch (replayed CUDA graphs), or the
     plain one-request-at-a-time modes ("plain": one dispatch per view,
     "plain_batch": one dispatch over the request's views).  Host buffers passed to :meth:`submit`
-    are kept alive here until :meth:`wait` returns their request."""
+    are kept alive here until :meth:`wait` returns their request.
+    ``train_record_steps``: steps per ray of the training step record (1..256,
+    0 = the most that fits an eighth of the budget, None = no record)."""
 
     def __init__(self, hbm_budget_bytes: int, mode: str = "batched", max_batch_rays: int = 0,
                  max_batch_views: int = 0, slots: int = 0, max_steps: int = 1024,
                  weight_threshold: float = 0.001, max_train_rays: int = 0,
-                 use_graphs: bool = True, train_chunk_rays: int = 0, frame_period_us: int = 0):
+                 use_graphs: bool = True, train_chunk_rays: int = 0, frame_period_us: int = 0,
+                 train_record_steps: int = 0):
         L = load_library()
         s = ServerSettings()
         s.hbm_budget_bytes = int(hbm_budget_bytes)
@@ -931,6 +935,7 @@ class Server:
         s.use_graphs = 1 if use_graphs else 0
         s.train_chunk_rays = train_chunk_rays
         s.frame_period_us = frame_period_us
+        s.train_record_steps = SERVE_NO_RECORD if train_record_steps is None else train_record_steps
         h = C.c_void_p()
         _check(L.bv_server_new(C.byref(s), C.byref(h)))
         self._h = h

@@ -625,6 +625,8 @@ bv_status bv_server_new(const bv_server_settings *settings, bv_server **out) {
     if (s.max_train_rays == 0) s.max_train_rays = kDefaultTrainRays;
     if (s.train_chunk_rays == 0) s.train_chunk_rays = kDefaultTrainChunk;
     if (s.frame_period_us == 0) s.frame_period_us = kDefaultFramePeriodUs;
+    if (s.train_record_steps != BV_SERVE_NO_RECORD && s.train_record_steps > kServeRecSteps)
+        return sfail(BV_ERR_INVALID_ARGUMENT, "train_record_steps above %u", kServeRecSteps);
     if (s.max_batch_views > (uint32_t)kMaxServeViews)
         return sfail(BV_ERR_INVALID_ARGUMENT, "max_batch_views above %d", kMaxServeViews);
     if (s.slots > 4) return sfail(BV_ERR_INVALID_ARGUMENT, "at most 4 batch slots");
@@ -714,13 +716,18 @@ bv_status bv_server_start(bv_server *sv) {
     for (auto &sc : sv->scenes) tracer_lend_ray_state(sc.t, sv->ray_state, s.max_train_rays);
     sv->table_bytes = sizeof(ServeHeader) + sizeof(ServeView) * s.max_batch_views;
     // training step record, shared by the scenes' tracers (one training
-    // request runs at a time, on the training stream): kServeRecSteps steps
-    // of every ray of a launch pair, within an eighth of the HBM budget (a
-    // smaller record holds fewer steps per ray; the replay recomputes the
-    // rest; below one step per ray there is none)
-    size_t rec_words = (size_t)s.train_chunk_rays * kServeRecSteps * 4;
-    rec_words = std::min<size_t>(rec_words, s.hbm_budget_bytes / 8 / sizeof(uint32_t));
-    if (rec_words < (size_t)s.train_chunk_rays * 4) rec_words = 0;
+    // request runs at a time, on the training stream): train_record_steps
+    // steps of every ray of a launch pair (the replay recomputes the steps
+    // past them).  Automatic: kServeRecSteps within an eighth of the HBM
+    // budget, none below one step per ray.
+    size_t rec_words = 0;
+    if (s.train_record_steps == 0) {
+        rec_words = (size_t)s.train_chunk_rays * kServeRecSteps * 4;
+        rec_words = std::min<size_t>(rec_words, s.hbm_budget_bytes / 8 / sizeof(uint32_t));
+        if (rec_words < (size_t)s.train_chunk_rays * 4) rec_words = 0;
+    } else if (s.train_record_steps != BV_SERVE_NO_RECORD) {
+        rec_words = (size_t)s.train_chunk_rays * s.train_record_steps * 4;
+    }
     if (rec_words) {
         SV_CUDA(cudaMalloc(&sv->step_rec, rec_words * sizeof(uint32_t)), "training step record");
         resident += rec_words * sizeof(uint32_t);

@@ -12,7 +12,10 @@ p50/p99 latencies, each measured from the request's scheduled arrival:
   frame_interval  the time a viewer of the request waits for each frame: the
                first frame from arrival, every later one from the frame
                before it (frames in the order they landed).
-Forward+backward work is also summarised as Mrays/s over the stream's span.
+Frame figures cover render requests; a forward+backward request's colours
+land with its gradients, so it counts in request latency only.  Its work is
+summarised as Mrays/s over the stream's span and over the time from its
+first launch to its outputs (service Mrays/s).
 
 Host buffers: each resolution has one pinned output sink and one pinned
 target, shared by every request of that resolution (the outputs overwrite
@@ -142,7 +145,9 @@ def run_stream(server, specs: Sequence[RequestSpec], bufs: HostBuffers,
         sub.append((rid, spec, due, frame_done))
     lat, frame_lat, first_lat, gaps = [], [], [], []
     fwdbwd_rays = 0
+    fwdbwd_busy = 0.0
     per_res: Dict[str, Dict[str, list]] = {}
+    per_res_fb: Dict[str, list] = {}
     per_kind: Dict[str, list] = {"render": [], "fwdbwd": []}
     rays = 0
     end = t0
@@ -155,13 +160,17 @@ def run_stream(server, specs: Sequence[RequestSpec], bufs: HostBuffers,
         rays += spec.rays
         end = max(end, r["done_s"])
         key = f"{spec.width}x{spec.height}"
+        lat.append(r["done_s"] - due)
+        per_kind["fwdbwd" if spec.fwdbwd else "render"].append(r["done_s"] - due)
+        if spec.fwdbwd:
+            # a training request's colours land with its gradients: no frames
+            fwdbwd_rays += spec.rays
+            fwdbwd_busy += r["done_s"] - r["start_s"]
+            per_res_fb.setdefault(key, []).append(r["done_s"] - due)
+            continue
         d = per_res.setdefault(key, dict(request=[], frame=[], first_frame=[],
                                          frame_interval=[]))
-        if spec.fwdbwd:
-            fwdbwd_rays += spec.rays
-        lat.append(r["done_s"] - due)
         d["request"].append(r["done_s"] - due)
-        per_kind["fwdbwd" if spec.fwdbwd else "render"].append(r["done_s"] - due)
         f = [float(x) - due for x in frame_done]
         frame_lat.extend(f)
         d["frame"].extend(f)
@@ -181,9 +190,12 @@ def run_stream(server, specs: Sequence[RequestSpec], bufs: HostBuffers,
     return dict(requests=len(specs), failures=failures, rays=rays, span_s=span,
                 mrays_per_s=rays / span / 1e6 if span > 0 else None,
                 fwdbwd_mrays_per_s=fwdbwd_rays / span / 1e6 if span > 0 else None,
+                fwdbwd_service_mrays_per_s=(fwdbwd_rays / fwdbwd_busy / 1e6
+                                            if fwdbwd_busy > 0 else None),
                 request_latency=pct(lat), first_frame_latency=pct(first_lat),
                 frame_latency=pct(frame_lat), frame_interval=pct(gaps),
                 per_kind={k: pct(v) for k, v in per_kind.items()},
                 per_resolution={k: {m: pct(x) for m, x in v.items()}
                                 for k, v in sorted(per_res.items())},
+                per_resolution_fwdbwd={k: pct(v) for k, v in sorted(per_res_fb.items())},
                 offered_rate=len(specs) / specs[-1].arrival if specs else None)

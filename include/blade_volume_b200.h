@@ -567,8 +567,13 @@ typedef struct bv_server_settings {
     uint32_t frame_period_us;   /* frame k of a request is due (k + 1) periods after its
                                    arrival; batches take the earliest-due frames first;
                                    0 = 16,000 */
-    uint32_t reserved;
+    uint32_t train_record_steps;/* steps per ray held by the training step record (chunk x
+                                   steps x 16 B of HBM; a replay searches past them):
+                                   1..256 as given, 0 = the most of 256 that fits an eighth
+                                   of the budget, BV_SERVE_NO_RECORD = none */
 } bv_server_settings;
+
+#define BV_SERVE_NO_RECORD 0xffffffffu
 
 /* Scene flag: the server keeps gradient tables for the scene, into which
  * forward+backward requests that name no tables of their own accumulate. */

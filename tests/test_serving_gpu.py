@@ -120,11 +120,15 @@ def test_same_alone_and_in_mix(models, reference_tracers):
         assert np.array_equal(bits(m), bits(a))
 
 
-@pytest.mark.parametrize("chunk", [0, 1024], ids=["one-launch-pair", "chunks-of-1024-rays"])
-def test_forward_backward_requests_in_the_mix(models, reference_tracers, chunk):
+@pytest.mark.parametrize("chunk,rec", [(0, 0), (1024, 0), (1024, 3), (0, None)],
+                         ids=["one-launch-pair", "chunks-of-1024-rays", "3-step-record",
+                              "no-record"])
+def test_forward_backward_requests_in_the_mix(models, reference_tracers, chunk, rec):
     """chunk: the server's training launch pairs cover at most this many
-    work items (0: its default, larger than these requests), with the step
-    record lent by the server; the results are the tracer's own."""
+    work items (0: its default, larger than these requests); rec: the steps
+    per ray of the step record the server lends (0: automatic, 3: the replay
+    searches past the third step, None: it searches every step); the results
+    are the tracer's own."""
     w, h = 48, 40
     cams = scenes.sphere_cameras(3, 3.0, 9, math.radians(55.0), w / h, 100.0)
     target = np.random.default_rng(2).random((3, h, w, 3)).astype(np.float32)
@@ -136,7 +140,7 @@ def test_forward_backward_requests_in_the_mix(models, reference_tracers, chunk):
     loss_ref = t.forward_backward(cams, w, h, tgt_dev, g_ref, rgb_out=rgb_ref,
                                   weight_threshold=0.0, max_dt=50.0)
     torch.cuda.synchronize()
-    server = new_server(models, train_chunk_rays=chunk)
+    server = new_server(models, train_chunk_rays=chunk, train_record_steps=rec)
     try:
         renders = make_requests(len(models), 10, seed=3)
         ids = []
@@ -190,13 +194,14 @@ def test_scene_gradient_tables_accumulate(models):
 
 
 def test_admission_under_a_small_budget(models, reference_tracers):
-    probe = new_server(models, budget=1 << 30)
+    # no training step record: the resident bytes then do not depend on the budget
+    probe = new_server(models, budget=1 << 30, train_record_steps=None)
     resident = probe.stats()["resident_bytes"]
     probe.close()
     reqs = make_requests(len(models), 16, seed=21)
     biggest = max(len(r["cams"]) * r["w"] * r["h"] * 16 for r in reqs)
     arena_want = 2 * biggest + 4096
-    server = new_server(models, budget=resident + arena_want)
+    server = new_server(models, budget=resident + arena_want, train_record_steps=None)
     try:
         st0 = server.stats()
         assert st0["arena_bytes"] <= arena_want
@@ -237,6 +242,8 @@ def test_rejects_bad_requests(models):
             server.wait(12345, 0.1)
     finally:
         server.close()
+    with pytest.raises(bv.BvError):
+        bv.Server(1 << 30, train_record_steps=257)
 
 
 def test_cancel_withdraws_requests_and_returns_their_arena_bytes(models, reference_tracers):
