@@ -54,9 +54,19 @@ namespace {
 #define BV_SPLAT_SMEM_WINDOW 1
 #endif
 // Cech-row clip: each chunk of a row staged in the warp's shared memory (1)
-// or broadcast lane to lane with shuffles (0).
+// or broadcast lane to lane with shuffles (0); entries taken two per
+// iteration from shared memory (1) or one (0).
 #ifndef BV_SPLAT_SMEM_ROWS
 #define BV_SPLAT_SMEM_ROWS 1
+#endif
+#ifndef BV_SPLAT_CLIP_PAIRS
+#define BV_SPLAT_CLIP_PAIRS 0
+#endif
+// Training launches take tiles heaviest first (1), ordered by the time each
+// tile's forward took in the previous call over the same views, or in
+// launch order (0).
+#ifndef BV_SPLAT_TILE_ORDER
+#define BV_SPLAT_TILE_ORDER 1
 #endif
 constexpr int kSplatBlock = 128;
 constexpr int kSplatWindow = BV_SPLAT_WINDOW;
@@ -179,6 +189,40 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
     float face_near = 0.0f, face_far = depth;
     uint32_t near_k = kNoPlane, far_k = kNoPlane;
     bool empty = !need;
+    // One Cech entry (row offset k, numerator <f - o, n>, denominator
+    // <d, n>) applied to this lane's interval.  A plane whose quotient
+    // provably cannot tighten the interval is passed without dividing
+    // (clip_*_cannot_tighten); the planes that can are divided and compared,
+    // so the interval and the planes that bound it are the same bit for bit.
+    auto clip_entry = [&](float num, float den, uint32_t k) {
+        bool moved = false;
+        if (den > 1.0e-20f) {
+            if (!clip_far_cannot_tighten(num, den, face_far)) {
+                const float t = num / den;
+                if (t < face_far) {
+                    face_far = t;
+                    far_k = k;
+                    moved = true;
+                }
+            }
+        } else if (den < -1.0e-20f) {
+            if (!clip_near_cannot_tighten(num, den, face_near)) {
+                const float t = num / den;
+                if (t > face_near) {
+                    face_near = t;
+                    near_k = k;
+                    moved = true;
+                }
+            }
+        } else if (num < 0.0f) {
+            empty = true;
+        }
+        if (moved) {
+            const float st = sn > face_near ? sn : face_near;
+            const float en = sf < face_far ? sf : face_far;
+            if (en <= st) empty = true;
+        }
+    };
     for (uint32_t base = begin; base < end; base += 32u) {
         if (!__any_sync(0xffffffffu, !empty)) break;
         const uint32_t n = min(32u, end - base);
@@ -204,9 +248,24 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
         __syncwarp();
         row[lane] = make_float4(num_own, fn.x, fn.y, fn.z);
         __syncwarp();
+#if BV_SPLAT_CLIP_PAIRS
+        // two entries per iteration: both denominators are formed before
+        // either is applied, then they are applied in row order (the slot
+        // after the last entry is read but not applied; a lane past the
+        // row's end wrote zeros there)
+        for (uint32_t j = 0; j < n && !empty; j += 2u) {
+            const float4 e0 = row[j], e1 = row[min(j + 1u, 31u)];
+            const float den0 = dot3(ray.dx, ray.dy, ray.dz, e0.y, e0.z, e0.w);
+            const float den1 = dot3(ray.dx, ray.dy, ray.dz, e1.y, e1.z, e1.w);
+            clip_entry(e0.x, den0, base + j - begin);
+            if (j + 1u < n && !empty) clip_entry(e1.x, den1, base + j + 1u - begin);
+        }
+#else
         for (uint32_t j = 0; j < n && !empty; ++j) {
             const float4 e = row[j];
-            const float num = e.x, nx = e.y, ny = e.z, nz = e.w;
+            clip_entry(e.x, dot3(ray.dx, ray.dy, ray.dz, e.y, e.z, e.w), base + j - begin);
+        }
+#endif
 #else
         for (uint32_t j = 0; j < n; ++j) {
 #if BV_SPLAT_SHARED_NUM
@@ -220,44 +279,12 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
             const float ny = __shfl_sync(0xffffffffu, fn.y, j);
             const float nz = __shfl_sync(0xffffffffu, fn.z, j);
             if (empty) continue;
-#endif
 #if !BV_SPLAT_SHARED_NUM
-            const float rx = fx - ray.ox, ry = fy - ray.oy, rz = fz - ray.oz;
-            const float num = dot3(rx, ry, rz, nx, ny, nz);
+            const float num = dot3(fx - ray.ox, fy - ray.oy, fz - ray.oz, nx, ny, nz);
 #endif
-            const float den = dot3(ray.dx, ray.dy, ray.dz, nx, ny, nz);
-            // A plane whose quotient provably cannot tighten the interval is
-            // passed without dividing (clip_cannot_tighten); the planes
-            // that can are divided and compared as before, so the interval
-            // and the planes that bound it are the same bit for bit.
-            bool moved = false;
-            if (den > 1.0e-20f) {
-                if (!clip_far_cannot_tighten(num, den, face_far)) {
-                    const float t = num / den;
-                    if (t < face_far) {
-                        face_far = t;
-                        far_k = base + j - begin;
-                        moved = true;
-                    }
-                }
-            } else if (den < -1.0e-20f) {
-                if (!clip_near_cannot_tighten(num, den, face_near)) {
-                    const float t = num / den;
-                    if (t > face_near) {
-                        face_near = t;
-                        near_k = base + j - begin;
-                        moved = true;
-                    }
-                }
-            } else if (num < 0.0f) {
-                empty = true;
-            }
-            if (moved) {
-                const float st = sn > face_near ? sn : face_near;
-                const float en = sf < face_far ? sf : face_far;
-                if (en <= st) empty = true;
-            }
+            clip_entry(num, dot3(ray.dx, ray.dy, ray.dz, nx, ny, nz), base + j - begin);
         }
+#endif
     }
     if (empty) return false;
     float st = face_near, en = face_far;
@@ -468,7 +495,17 @@ struct SplatTrainParams {
     uint32_t rec_chunks;        // chunk ranks per tile; 0: the replay traverses every ray
     uint32_t rec_limit;         // intervals recorded per ray at most
     uint32_t pool_chunks;       // chunks in the pool
+    const uint32_t *tile_order; // [tiles] tile taken by warp slot i, or null: slot i takes tile i
+    uint32_t *tile_cost;        // [tiles] forward: the tile's duration in 64-cycle units, or null
 };
+
+// The work item of thread w: its warp slot's tile (tile_order, a permutation
+// of the launch's tiles, or the slot itself) and its lane.  Every per-ray
+// and per-tile index (pixel, ray state, interval record) follows from it, so
+// the order tiles are taken in changes no result.
+__device__ __forceinline__ uint32_t splat_train_item(const uint32_t *order, uint32_t w) {
+    return order ? (__ldg(order + (w >> 5)) << 5) | (w & 31u) : w;
+}
 
 // Interval record of the training forward, read back by the replay.  The
 // i-th composited interval of ray w (the cell, the raw interval length as
@@ -568,8 +605,10 @@ template <int DEG, bool BF16>
 __global__ void __launch_bounds__(kSplatBlock)
 splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
     const SplatParams &P = TP.base;
-    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-    if ((w & ~31u) >= P.total_work) return;
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((slot & ~31u) >= P.total_work) return;
+    const long long clock_begin = clock64();
+    const uint32_t w = splat_train_item(TP.tile_order, slot);
     const SplatLane L = splat_lane(P, w);
     const WinRay &ray = L.ray;
     const float depth = L.vd->depth;
@@ -668,6 +707,10 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
         atomicAdd(P.stats + 0, 1ull);
         atomicAdd(P.stats + 1, (unsigned long long)composited);
         atomicAdd(P.stats + 2, (unsigned long long)clipped);
+    }
+    if (TP.tile_cost && (threadIdx.x & 31u) == 0) {
+        const unsigned long long d = (unsigned long long)(clock64() - clock_begin) >> 6;
+        TP.tile_cost[w >> 5] = d > 0xffffffffull ? 0xffffffffu : (uint32_t)d;
     }
 }
 
@@ -821,8 +864,9 @@ __global__ void __launch_bounds__(kSplatBlock)
 splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
     const SplatParams &P = TP.base;
     constexpr int K = ShDims<DEG>::K;
-    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-    if ((w & ~31u) >= P.total_work) return;
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((slot & ~31u) >= P.total_work) return;
+    const uint32_t w = splat_train_item(TP.tile_order, slot);
     const SplatLane L = splat_lane(P, w);
     const WinRay &ray = L.ray;
     const float depth = L.vd->depth;
@@ -946,6 +990,56 @@ cudaError_t launch_splat_train(const SplatTrainParams &p, bool backward, cudaStr
     return cudaGetLastError();
 }
 
+// Heaviest-first tile order from the forward's tile durations: tiles go to
+// 32 classes by floor(log2(cost)) and the classes are laid out from the
+// heaviest down (the order inside a class is whatever the atomics give).
+// counts[0..31] per class, counts[32..63] the classes' fill cursors, both
+// zero on entry.
+constexpr int kOrderClasses = 32;
+
+__device__ __forceinline__ uint32_t order_class(uint32_t cost) {
+    return 31u - (uint32_t)__clz(cost | 1u);
+}
+
+__global__ void tile_cost_histogram_kernel(const uint32_t *__restrict__ cost, uint32_t tiles,
+                                           uint32_t *__restrict__ counts) {
+    __shared__ uint32_t h[kOrderClasses];
+    if (threadIdx.x < kOrderClasses) h[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < tiles; i += gridDim.x * blockDim.x)
+        atomicAdd(&h[order_class(cost[i])], 1u);
+    __syncthreads();
+    if (threadIdx.x < kOrderClasses && h[threadIdx.x]) atomicAdd(&counts[threadIdx.x], h[threadIdx.x]);
+}
+
+__global__ void tile_order_scatter_kernel(const uint32_t *__restrict__ cost, uint32_t tiles,
+                                          uint32_t *__restrict__ counts,
+                                          uint32_t *__restrict__ order) {
+    __shared__ uint32_t start[kOrderClasses];
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int c = kOrderClasses - 1; c >= 0; --c) {
+            start[c] = acc;
+            acc += counts[c];
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < tiles; i += gridDim.x * blockDim.x) {
+        const uint32_t c = order_class(cost[i]);
+        order[start[c] + atomicAdd(&counts[kOrderClasses + c], 1u)] = i;
+    }
+}
+
+cudaError_t launch_tile_order(const uint32_t *cost, uint32_t tiles, uint32_t *counts,
+                              uint32_t *order, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(counts, 0, 2 * kOrderClasses * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    const int blocks = (int)std::min<uint32_t>(296u, (tiles + 255u) / 256u);
+    tile_cost_histogram_kernel<<<blocks, 256, 0, s>>>(cost, tiles, counts);
+    tile_order_scatter_kernel<<<blocks, 256, 0, s>>>(cost, tiles, counts, order);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_splat(const SplatParams &p, cudaStream_t s) {
     const int blocks = (int)((p.total_work + kSplatBlock - 1) / kSplatBlock);
     if (blocks == 0) return cudaSuccess;
@@ -1016,6 +1110,14 @@ struct bv_splat_tracer {
     uint32_t *rec_demand = nullptr;    // pinned: the pool counter after the last forward
     cudaEvent_t rec_event = nullptr;   // that copy has landed
     uint32_t rec_entries = kSplatRecEntries;
+    // training tile order: the forward's duration of every tile of the last
+    // call (tile_cost), the heaviest-first order built from it (tile_order)
+    // and the views and size it holds for (order_valid: same call again)
+    uint32_t *tile_cost = nullptr, *tile_order = nullptr, *order_counts = nullptr;
+    size_t tile_capacity = 0;
+    std::vector<bv_camera> order_cams;
+    uint32_t order_w = 0, order_h = 0;
+    bool order_valid = false;
     float4 *site_grads = nullptr;    // [N], kept zero between calls
     void *sh = nullptr;
     unsigned long long *stats = nullptr;
@@ -1056,6 +1158,9 @@ void free_splat(bv_splat_tracer *t) {
     cudaFree(t->ray_state);
     cudaFree(t->rec_pool);
     cudaFree(t->rec_table);
+    cudaFree(t->tile_cost);
+    cudaFree(t->tile_order);
+    cudaFree(t->order_counts);
     cudaFreeHost(t->rec_demand);
     if (t->rec_event) cudaEventDestroy(t->rec_event);
     cudaFree(t->site_grads);
@@ -1469,6 +1574,37 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         }
         if (!ok) rec_chunks = 0;
     }
+    // heaviest-first tile order (calls of one launch): the forward times its
+    // tiles, the order is built from those times after the backward, and a
+    // later call over the same views and size takes its tiles in that order
+    bool time_tiles = false, use_order = false;
+    if (BV_SPLAT_TILE_ORDER && n_cams <= (uint32_t)kMaxViewsPerLaunch) {
+        time_tiles = true;
+        if (tiles > t->tile_capacity) {
+            cudaFree(t->tile_cost);
+            cudaFree(t->tile_order);
+            t->tile_cost = t->tile_order = nullptr;
+            t->tile_capacity = 0;
+            t->order_valid = false;
+            if (!t->order_counts &&
+                cudaMalloc(&t->order_counts, 2 * kOrderClasses * sizeof(uint32_t)) != cudaSuccess)
+                t->order_counts = nullptr;
+            if (t->order_counts && cudaMalloc(&t->tile_cost, tiles * sizeof(uint32_t)) == cudaSuccess &&
+                cudaMalloc(&t->tile_order, tiles * sizeof(uint32_t)) == cudaSuccess) {
+                t->tile_capacity = tiles;
+            } else {
+                (void)cudaGetLastError();  // no room: tiles in launch order
+                cudaFree(t->tile_cost);
+                cudaFree(t->tile_order);
+                t->tile_cost = t->tile_order = nullptr;
+                time_tiles = false;
+            }
+        }
+        use_order = time_tiles && t->order_valid && t->order_w == width && t->order_h == height &&
+                    t->order_cams.size() == n_cams &&
+                    std::memcmp(t->order_cams.data(), cams, n_cams * sizeof(bv_camera)) == 0;
+    }
+    t->order_valid = false;
     t->last_launches = 0;
     t->last_has_stats = t->stats_enabled;
     if (t->stats_enabled) {
@@ -1521,6 +1657,8 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
             p.rec_limit = std::min<uint32_t>(t->rec_entries, ts->max_steps);
             p.pool_chunks = (uint32_t)std::min<size_t>(t->rec_pool_chunks, 0xfffffff0u);
         }
+        p.tile_order = use_order ? t->tile_order : nullptr;
+        p.tile_cost = time_tiles ? t->tile_cost : nullptr;
         SP_CUDA(launch_splat_train(p, false, s), "splat training forward launch");
         if (rec_chunks) {
             SP_CUDA(cudaMemcpyAsync(t->rec_demand, p.rec_next, sizeof(uint32_t),
@@ -1530,6 +1668,15 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         p.base.stats = nullptr;
         SP_CUDA(launch_splat_train(p, true, s), "splat training backward launch");
         t->last_launches += 2;
+        if (time_tiles) {
+            SP_CUDA(launch_tile_order(t->tile_cost, (uint32_t)tiles, t->order_counts,
+                                      t->tile_order, s), "tile order");
+            t->last_launches += 2;
+            t->order_cams.assign(cams, cams + n_cams);
+            t->order_w = width;
+            t->order_h = height;
+            t->order_valid = true;
+        }
     }
     if (want_site) {
         SP_CUDA(launch_fold_site_grads(t->site_grads, t->n, grads->d_positions_dev,

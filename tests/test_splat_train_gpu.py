@@ -97,3 +97,35 @@ def test_splat_training_settings_and_accumulation():
     twice = run_gpu(m, cams, target, repeat=2)
     for k in ("d_density", "d_sh", "d_pos", "d_radius"):
         assert_table(k, twice[k], 2.0 * once[k], tol=1e-5)
+
+
+def test_repeated_calls_take_tiles_heaviest_first_with_the_same_results():
+    """A call over the same views and size as the one before takes its tiles
+    in the order of the previous forward's tile durations (two more launches
+    per call build that order); other views, or another size, go back to
+    launch order.  Every call is held to the oracle."""
+    m, cams, target = case(seed=5, n=3000)
+    other = scenes.sphere_cameras(3, 3.0, 11, math.radians(55.0), 1.0, 100.0)
+    om = O.OracleModel.from_scene(m)
+    refs = {}
+    t = bv.PowerFoamSplatTracer(m)
+    try:
+        tg = torch.from_numpy(target).cuda()
+        for i, views in enumerate([cams, cams, cams, other, cams]):
+            key = id(views)
+            if key not in refs:
+                refs[key] = O.forward_backward(om, views, W, H, target=target, splats=True,
+                                               want_mass=True)
+            ref = refs[key]
+            grads = t.new_grads()
+            rgb = torch.zeros((len(views), H, W, 3), dtype=torch.float32, device="cuda")
+            loss = t.forward_backward(views, W, H, tg, grads, rgb_out=rgb)
+            torch.cuda.synchronize()
+            assert t.last_stats().launches == 5  # forward, backward, order x 2, site fold
+            g = {k: v.cpu().numpy().astype(np.float64) for k, v in grads.items()}
+            g["d_pos"] = g["d_pos"].reshape(-1, 3)
+            assert abs(float(loss.item()) - ref["loss"]) <= 1e-5 * ref["loss"], i
+            assert np.array_equal(rgb.cpu().numpy().view(np.uint32), ref["rgb32"].view(np.uint32)), i
+            gradcheck.check_all(g, ref, where=f"tile order call {i}")
+    finally:
+        t.deinit()
