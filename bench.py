@@ -83,6 +83,8 @@ def parse():
                     help="serving: sites of the resident scenes (seeds 1, 2, ...)")
     ap.add_argument("--batch-rays", type=int, default=0, help="serving: rays per batch (0: default)")
     ap.add_argument("--slots", type=int, default=0, help="serving: batches in flight (0: default)")
+    ap.add_argument("--train-chunk", type=int, default=0,
+                    help="serving: forward+backward work items per launch pair (0: default)")
     args = ap.parse_args()
     splat = args.workload in ("splat", "powerfoam", "powerfoam_walk")
     if args.size is None:
@@ -264,16 +266,24 @@ def cpu_baseline(model, cams, width, height, steps=1, target=None):
                                       f"{d1:.2f} s"}}
 
 
-def cpu_image_baseline(render, width, height, what):
+def cpu_image_baseline(render, width, height, what, single=None):
     """Times one oracle render (all host cores) of a width x height image of
-    the workload's own camera: a spread sample of its rays."""
+    the workload's own camera, a spread sample of its rays, and one on a
+    single core of ``single`` (w, h) (default: the same image), as the
+    reference's single-threaded render_cpu loop runs."""
     t0 = time.perf_counter()
-    render(width, height)
+    render(width, height, 0)
     dt = time.perf_counter() - t0
     rays = width * height
+    sw, sh = single or (width, height)
+    t0 = time.perf_counter()
+    render(sw, sh, 1)
+    dt1 = time.perf_counter() - t0
     return {"value": rays / dt / 1e6, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
             "sample": f"{what}: {width}x{height} rays ({rays}) over the same field of view, "
-                      f"{dt:.2f} s"}
+                      f"{dt:.2f} s",
+            "single_core": {"value": sw * sh / dt1 / 1e6, "unit": UNIT, "cores": 1,
+                            "sample": f"{sw}x{sh} rays over the same field of view, {dt1:.2f} s"}}
 
 
 # Timed steps of the reference arm: each is the whole workload, about 10 s on
@@ -383,8 +393,9 @@ def run_secondary(args):
             from oracle import oracle as O
 
             osc = O.RelightOracleScene.from_scene(g)
-            cpu = cpu_image_baseline(lambda w, h: O.relight_render(osc, lights, cam, w, h), 32, 24,
-                                     "oracle relight (every particle tested per ray)")
+            cpu = cpu_image_baseline(lambda w, h, th: O.relight_render(osc, lights, cam, w, h,
+                                                                      threads=th), 32, 24,
+                                     "oracle relight (every particle tested per ray)", (16, 12))
         line = {"metric": "relight Mrays/s", "value": W * H / (ms * 1e-3) / 1e6, "unit": "Mrays/s",
                 "ms_per_step": ms, "steps": args.steps, "warmup": max(args.warmup, 3),
                 "dtype": "f32", "data": "synthetic",
@@ -426,8 +437,9 @@ def run_secondary(args):
             from oracle import oracle as O
 
             osc = O.GaussianOracleScene.from_scene(g)
-            cpu = cpu_image_baseline(lambda w, h: O.gaussian_render(osc, cam, w, h), 32, 24,
-                                     "oracle trace_gaussians (every particle tested per ray)")
+            cpu = cpu_image_baseline(lambda w, h, th: O.gaussian_render(osc, cam, w, h, threads=th),
+                                     32, 24, "oracle trace_gaussians (every particle tested per ray)",
+                                     (16, 12))
         line = {"metric": "gaussian Mrays/s", "value": W * H / (ms * 1e-3) / 1e6,
                 "unit": "Mrays/s", "ms_per_step": ms, "steps": args.steps,
                 "warmup": max(args.warmup, 3), "dtype": "f32", "data": "synthetic",
@@ -478,9 +490,9 @@ def run_secondary(args):
 
             om = O.OracleModel.from_scene(w.model)
             cpu = cpu_image_baseline(
-                lambda ww, hh: O.render_splats(om, w.cameras[0], ww, hh, w.max_steps,
-                                               w.weight_threshold), 16, 16,
-                "oracle trace_powerfoam_splats (every support tested per ray), view 0")
+                lambda ww, hh, th: O.render_splats(om, w.cameras[0], ww, hh, w.max_steps,
+                                                   w.weight_threshold, threads=th), 16, 16,
+                "oracle trace_powerfoam_splats (every support tested per ray), view 0", (8, 8))
         line = {"metric": "splat Mrays/s", "value": rays / (ms * 1e-3) / 1e6, "unit": "Mrays/s",
                 "ms_per_step": ms, "steps": args.steps, "warmup": max(args.warmup, 3),
                 "dtype": "f32 (SH bf16)", "data": "synthetic",
@@ -523,8 +535,9 @@ def run_secondary(args):
         from oracle import oracle as O
 
         om = O.OracleModel.from_scene(w.model)
-        cpu = cpu_image_baseline(lambda ww, hh: O.render_walk(om, w.cameras[0], ww, hh,
-                                                              w.max_steps, w.weight_threshold),
+        cpu = cpu_image_baseline(lambda ww, hh, th: O.render_walk(om, w.cameras[0], ww, hh,
+                                                                  w.max_steps, w.weight_threshold,
+                                                                  threads=th),
                                  w.width, w.height, "oracle trace_one_ray, the whole image")
     line = {"metric": "forward Mrays/s", "value": w.width * w.height / (ms * 1e-3) / 1e6,
             "unit": "Mrays/s", "ms_per_step": ms, "steps": args.steps,
@@ -619,11 +632,15 @@ def run_powerfoam_train(args):
     # table touched once: sites, density, BF16 SH rows, the CSR, the Cech
     # row faces (32 B per entry, splat semantics) or face table (32 B per
     # entry, walk), and the gradient tables read and written
+    # (the walk reads only the cells its rays cross: for it the tables
+    # count once, written by the gradient reset)
     n, m_edges = model.n, len(model.neighbors)
-    per_unit = 2 * 16 if walk else 2 * 24
-    alg = (st.steps * per_unit + rays * (2 * 48 + 12)
-           + n * (16 + 4 + 2 * 3 * K + 4) + m_edges * (32 + 4)
-           + 2 * n * (4 + 4 * 3 * K + 16))
+    grad_bytes = n * (4 + 4 * 3 * K + 16)
+    if walk:
+        alg = st.steps * 2 * 16 + rays * (2 * 48 + 12) + grad_bytes
+    else:
+        alg = (st.steps * 2 * 24 + rays * (2 * 48 + 12)
+               + n * (16 + 4 + 2 * 3 * K + 4) + m_edges * (32 + 4) + 2 * grad_bytes)
     peak, kind = peaks()
     cpu = None
     if not args.no_cpu_baseline:
@@ -641,8 +658,15 @@ def run_powerfoam_train(args):
         dt = time.perf_counter() - t0
         what = ("oracle walk fwd+bwd" if walk else
                 "oracle splat fwd+bwd (every support tested per ray)")
+        s1 = side // 4 if walk else side // 2
+        t0 = time.perf_counter()
+        O.forward_backward(om, cams[:1], s1, s1, MAX_STEPS, 0.0, MAX_DT,
+                           np.zeros((1, s1, s1, 3), np.float32), 0, splats=not walk, threads=1)
+        dt1 = time.perf_counter() - t0
         cpu = {"value": side * side / dt / 1e6, "unit": UNIT, "cores": os.cpu_count() or 1,
-               "kind": "port", "sample": f"{what}, view 0 at {side}x{side}, {dt:.2f} s"}
+               "kind": "port", "sample": f"{what}, view 0 at {side}x{side}, {dt:.2f} s",
+               "single_core": {"value": s1 * s1 / dt1 / 1e6, "unit": UNIT, "cores": 1,
+                               "sample": f"view 0 at {s1}x{s1}, {dt1:.2f} s"}}
     line = {"metric": METRIC, "value": rays / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": 1,
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -697,7 +721,7 @@ def run_serving(args):
     sampler.start()
     for mode in ("plain", "plain_batch", "batched"):
         srv = bv.Server(int(args.budget_gb * 1e9), mode=mode, max_batch_rays=args.batch_rays,
-                        slots=args.slots)
+                        slots=args.slots, train_chunk_rays=args.train_chunk)
         for m in models:
             srv.add_scene(m, gradients=True)
         srv.start()

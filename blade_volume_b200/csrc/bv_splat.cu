@@ -54,13 +54,14 @@ namespace {
 #define BV_SPLAT_SMEM_WINDOW 1
 #endif
 // Cech-row clip: each chunk of a row staged in the warp's shared memory (1)
-// or broadcast lane to lane with shuffles (0); entries taken two per
-// iteration from shared memory (1) or one (0).
+// or broadcast lane to lane with shuffles (0); entries read from shared
+// memory per iteration of the clip loop, 1, 2 or 4 (2: 30.3 -> 32.9 Mrays/s
+// for config-2 training, 23.8 -> 26.4 for its render).
 #ifndef BV_SPLAT_SMEM_ROWS
 #define BV_SPLAT_SMEM_ROWS 1
 #endif
-#ifndef BV_SPLAT_CLIP_PAIRS
-#define BV_SPLAT_CLIP_PAIRS 0
+#ifndef BV_SPLAT_CLIP_ILP
+#define BV_SPLAT_CLIP_ILP 2
 #endif
 // Training launches take tiles heaviest first (1), ordered by the time each
 // tile's forward took in the previous call over the same views, or in
@@ -126,8 +127,26 @@ struct SplatParams {
     uint32_t *max_candidates;      // counting pass: max over rays of the support hits
     unsigned long long *count_totals;  // counting pass: [2] support hits, their Cech row entries
     uint32_t count_only;
+    const uint32_t *tile_order;    // [tiles] tile taken by warp slot i, or null: slot i takes tile i
+    uint32_t *tile_cost;           // [tiles] the tile's duration in 64-cycle units, or null
     ViewDesc views[kMaxViewsPerLaunch];
 };
+
+// The work item of thread `slot`: its warp slot's tile (tile_order, a
+// permutation of the launch's tiles, or the slot itself) and its lane.
+// Every per-ray and per-tile index (pixel, ray state, interval record)
+// follows from it, so the order tiles are taken in changes no result.
+__device__ __forceinline__ uint32_t splat_item(const uint32_t *order, uint32_t slot) {
+    return order ? (__ldg(order + (slot >> 5)) << 5) | (slot & 31u) : slot;
+}
+
+// Lane 0 of a warp stores its tile's duration since `begin` (clock64).
+__device__ __forceinline__ void store_tile_cost(uint32_t *cost, uint32_t w, long long begin) {
+    if (cost && (threadIdx.x & 31u) == 0) {
+        const unsigned long long d = (unsigned long long)(clock64() - begin) >> 6;
+        cost[w >> 5] = d > 0xffffffffull ? 0xffffffffu : (uint32_t)d;
+    }
+}
 
 // Slab test for the counting pass (per-lane traversal).
 __device__ __forceinline__ bool slab(const float4 &lo, const float4 &hi, const WinRay &r, float t_end,
@@ -248,17 +267,24 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
         __syncwarp();
         row[lane] = make_float4(num_own, fn.x, fn.y, fn.z);
         __syncwarp();
-#if BV_SPLAT_CLIP_PAIRS
-        // two entries per iteration: both denominators are formed before
-        // either is applied, then they are applied in row order (the slot
-        // after the last entry is read but not applied; a lane past the
-        // row's end wrote zeros there)
-        for (uint32_t j = 0; j < n && !empty; j += 2u) {
-            const float4 e0 = row[j], e1 = row[min(j + 1u, 31u)];
-            const float den0 = dot3(ray.dx, ray.dy, ray.dz, e0.y, e0.z, e0.w);
-            const float den1 = dot3(ray.dx, ray.dy, ray.dz, e1.y, e1.z, e1.w);
-            clip_entry(e0.x, den0, base + j - begin);
-            if (j + 1u < n && !empty) clip_entry(e1.x, den1, base + j + 1u - begin);
+#if BV_SPLAT_CLIP_ILP > 1
+        // BV_SPLAT_CLIP_ILP entries per iteration: their denominators are
+        // formed before any is applied, then they are applied in row order
+        // (slots past the last entry are read but not applied; lanes past
+        // the row's end wrote zeros there, and the slot index stays below 32)
+        constexpr uint32_t kIlp = BV_SPLAT_CLIP_ILP;
+        for (uint32_t j = 0; j < n && !empty; j += kIlp) {
+            float4 e[kIlp];
+            float den[kIlp];
+#pragma unroll
+            for (uint32_t u = 0; u < kIlp; ++u) {
+                e[u] = row[min(j + u, 31u)];
+                den[u] = dot3(ray.dx, ray.dy, ray.dz, e[u].y, e[u].z, e[u].w);
+            }
+            clip_entry(e[0].x, den[0], base + j - begin);
+#pragma unroll
+            for (uint32_t u = 1; u < kIlp; ++u)
+                if (j + u < n && !empty) clip_entry(e[u].x, den[u], base + j + u - begin);
         }
 #else
         for (uint32_t j = 0; j < n && !empty; ++j) {
@@ -372,8 +398,10 @@ splat_kernel(const __grid_constant__ SplatParams P) {
     // A view's work is whole 8x4 tiles, so a warp is one tile of one view;
     // whole warps past the end leave together, lanes of a partial edge tile
     // stay (inactive) because the main pass is warp-cooperative.
-    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-    if ((w & ~31u) >= P.total_work) return;
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((slot & ~31u) >= P.total_work) return;
+    const long long clock_begin = clock64();
+    const uint32_t w = splat_item(P.tile_order, slot);
     const SplatLane L = splat_lane(P, w);
     const WinRay &ray = L.ray;
     const bool active = L.active;
@@ -462,13 +490,15 @@ splat_kernel(const __grid_constant__ SplatParams P) {
             cur_cell = last.idx;
         }
     }
-    if (!active) return;
-    *out = make_float4(ar, ag, ab, 1.0f - T);
-    if (P.stats) {
-        atomicAdd(P.stats + 0, 1ull);
-        atomicAdd(P.stats + 1, (unsigned long long)steps);
-        atomicAdd(P.stats + 2, (unsigned long long)clipped);
+    if (active) {
+        *out = make_float4(ar, ag, ab, 1.0f - T);
+        if (P.stats) {
+            atomicAdd(P.stats + 0, 1ull);
+            atomicAdd(P.stats + 1, (unsigned long long)steps);
+            atomicAdd(P.stats + 2, (unsigned long long)clipped);
+        }
     }
+    store_tile_cost(P.tile_cost, w, clock_begin);
 }
 
 // ---------------------------------------------------------------------------
@@ -495,17 +525,7 @@ struct SplatTrainParams {
     uint32_t rec_chunks;        // chunk ranks per tile; 0: the replay traverses every ray
     uint32_t rec_limit;         // intervals recorded per ray at most
     uint32_t pool_chunks;       // chunks in the pool
-    const uint32_t *tile_order; // [tiles] tile taken by warp slot i, or null: slot i takes tile i
-    uint32_t *tile_cost;        // [tiles] forward: the tile's duration in 64-cycle units, or null
 };
-
-// The work item of thread w: its warp slot's tile (tile_order, a permutation
-// of the launch's tiles, or the slot itself) and its lane.  Every per-ray
-// and per-tile index (pixel, ray state, interval record) follows from it, so
-// the order tiles are taken in changes no result.
-__device__ __forceinline__ uint32_t splat_train_item(const uint32_t *order, uint32_t w) {
-    return order ? (__ldg(order + (w >> 5)) << 5) | (w & 31u) : w;
-}
 
 // Interval record of the training forward, read back by the replay.  The
 // i-th composited interval of ray w (the cell, the raw interval length as
@@ -608,7 +628,7 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if ((slot & ~31u) >= P.total_work) return;
     const long long clock_begin = clock64();
-    const uint32_t w = splat_train_item(TP.tile_order, slot);
+    const uint32_t w = splat_item(P.tile_order, slot);
     const SplatLane L = splat_lane(P, w);
     const WinRay &ray = L.ray;
     const float depth = L.vd->depth;
@@ -708,10 +728,7 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
         atomicAdd(P.stats + 1, (unsigned long long)composited);
         atomicAdd(P.stats + 2, (unsigned long long)clipped);
     }
-    if (TP.tile_cost && (threadIdx.x & 31u) == 0) {
-        const unsigned long long d = (unsigned long long)(clock64() - clock_begin) >> 6;
-        TP.tile_cost[w >> 5] = d > 0xffffffffull ? 0xffffffffu : (uint32_t)d;
-    }
+    store_tile_cost(P.tile_cost, w, clock_begin);
 }
 
 // Gradient of one composited interval of the replay (cell, raw length,
@@ -866,7 +883,7 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
     constexpr int K = ShDims<DEG>::K;
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if ((slot & ~31u) >= P.total_work) return;
-    const uint32_t w = splat_train_item(TP.tile_order, slot);
+    const uint32_t w = splat_item(P.tile_order, slot);
     const SplatLane L = splat_lane(P, w);
     const WinRay &ray = L.ray;
     const float depth = L.vd->depth;
@@ -1040,6 +1057,58 @@ cudaError_t launch_tile_order(const uint32_t *cost, uint32_t tiles, uint32_t *co
     return cudaGetLastError();
 }
 
+// Heaviest-first scheduling of one kind of launch (render or training)
+// from frame to frame: a launch times its tiles into `cost`, the order is
+// built from those times after it, and the next launch of the same shape
+// (views, width, height: the same tiles) takes its tiles in that order.
+// Frames of a moving camera keep most of their heavy tiles where they were;
+// the order changes no result, only when each tile starts.
+struct TileScheduler {
+    uint32_t *cost = nullptr, *order = nullptr, *counts = nullptr;
+    size_t capacity = 0;
+    uint32_t views = 0, width = 0, height = 0;
+    bool valid = false;
+
+    void release() {
+        cudaFree(cost);
+        cudaFree(order);
+        cudaFree(counts);
+        cost = order = counts = nullptr;
+        capacity = 0;
+        valid = false;
+    }
+    // Before a launch of `tiles` tiles: whether it times them (buffers to
+    // hand) and the order to take them in (null: launch order).
+    bool begin(size_t tiles, uint32_t n_views, uint32_t w, uint32_t h, const uint32_t *&use) {
+        use = nullptr;
+        if (!BV_SPLAT_TILE_ORDER || n_views > (uint32_t)kMaxViewsPerLaunch) return false;
+        if (tiles > capacity) {
+            release();
+            if (cudaMalloc(&counts, 2 * kOrderClasses * sizeof(uint32_t)) != cudaSuccess ||
+                cudaMalloc(&cost, tiles * sizeof(uint32_t)) != cudaSuccess ||
+                cudaMalloc(&order, tiles * sizeof(uint32_t)) != cudaSuccess) {
+                (void)cudaGetLastError();  // no room: launch order
+                release();
+                return false;
+            }
+            capacity = tiles;
+        }
+        if (valid && views == n_views && width == w && height == h) use = order;
+        valid = false;
+        return true;
+    }
+    // After the launch (same stream): the order for the next one.
+    cudaError_t end(size_t tiles, uint32_t n_views, uint32_t w, uint32_t h, cudaStream_t s) {
+        const cudaError_t e = launch_tile_order(cost, (uint32_t)tiles, counts, order, s);
+        if (e != cudaSuccess) return e;
+        views = n_views;
+        width = w;
+        height = h;
+        valid = true;
+        return cudaSuccess;
+    }
+};
+
 cudaError_t launch_splat(const SplatParams &p, cudaStream_t s) {
     const int blocks = (int)((p.total_work + kSplatBlock - 1) / kSplatBlock);
     if (blocks == 0) return cudaSuccess;
@@ -1110,14 +1179,7 @@ struct bv_splat_tracer {
     uint32_t *rec_demand = nullptr;    // pinned: the pool counter after the last forward
     cudaEvent_t rec_event = nullptr;   // that copy has landed
     uint32_t rec_entries = kSplatRecEntries;
-    // training tile order: the forward's duration of every tile of the last
-    // call (tile_cost), the heaviest-first order built from it (tile_order)
-    // and the views and size it holds for (order_valid: same call again)
-    uint32_t *tile_cost = nullptr, *tile_order = nullptr, *order_counts = nullptr;
-    size_t tile_capacity = 0;
-    std::vector<bv_camera> order_cams;
-    uint32_t order_w = 0, order_h = 0;
-    bool order_valid = false;
+    TileScheduler render_order, train_order;  // heaviest-first tile orders
     float4 *site_grads = nullptr;    // [N], kept zero between calls
     void *sh = nullptr;
     unsigned long long *stats = nullptr;
@@ -1158,9 +1220,8 @@ void free_splat(bv_splat_tracer *t) {
     cudaFree(t->ray_state);
     cudaFree(t->rec_pool);
     cudaFree(t->rec_table);
-    cudaFree(t->tile_cost);
-    cudaFree(t->tile_order);
-    cudaFree(t->order_counts);
+    t->render_order.release();
+    t->train_order.release();
     cudaFreeHost(t->rec_demand);
     if (t->rec_event) cudaEventDestroy(t->rec_event);
     cudaFree(t->site_grads);
@@ -1206,8 +1267,17 @@ bv_status enqueue_splats(bv_splat_tracer *t, float4 *out, const bv_camera *cams,
         p.max_candidates = t->max_candidates;
         p.count_totals = t->count_totals;
         p.count_only = count_only ? 1u : 0u;
+        const size_t tiles = work / 32u;
+        bool time_tiles = false;
+        if (!count_only && n <= (uint32_t)kMaxViewsPerLaunch)
+            time_tiles = t->render_order.begin(tiles, nc, w, h, p.tile_order);
+        p.tile_cost = time_tiles ? t->render_order.cost : nullptr;
         SP_CUDA(launch_splat(p, s), "splat launch");
         t->last_launches += 1;
+        if (time_tiles) {
+            SP_CUDA(t->render_order.end(tiles, nc, w, h, s), "tile order");
+            t->last_launches += 2;
+        }
     }
     return BV_OK;
 }
@@ -1575,36 +1645,9 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         if (!ok) rec_chunks = 0;
     }
     // heaviest-first tile order (calls of one launch): the forward times its
-    // tiles, the order is built from those times after the backward, and a
-    // later call over the same views and size takes its tiles in that order
-    bool time_tiles = false, use_order = false;
-    if (BV_SPLAT_TILE_ORDER && n_cams <= (uint32_t)kMaxViewsPerLaunch) {
-        time_tiles = true;
-        if (tiles > t->tile_capacity) {
-            cudaFree(t->tile_cost);
-            cudaFree(t->tile_order);
-            t->tile_cost = t->tile_order = nullptr;
-            t->tile_capacity = 0;
-            t->order_valid = false;
-            if (!t->order_counts &&
-                cudaMalloc(&t->order_counts, 2 * kOrderClasses * sizeof(uint32_t)) != cudaSuccess)
-                t->order_counts = nullptr;
-            if (t->order_counts && cudaMalloc(&t->tile_cost, tiles * sizeof(uint32_t)) == cudaSuccess &&
-                cudaMalloc(&t->tile_order, tiles * sizeof(uint32_t)) == cudaSuccess) {
-                t->tile_capacity = tiles;
-            } else {
-                (void)cudaGetLastError();  // no room: tiles in launch order
-                cudaFree(t->tile_cost);
-                cudaFree(t->tile_order);
-                t->tile_cost = t->tile_order = nullptr;
-                time_tiles = false;
-            }
-        }
-        use_order = time_tiles && t->order_valid && t->order_w == width && t->order_h == height &&
-                    t->order_cams.size() == n_cams &&
-                    std::memcmp(t->order_cams.data(), cams, n_cams * sizeof(bv_camera)) == 0;
-    }
-    t->order_valid = false;
+    // tiles, the order is built from those times after the backward
+    const uint32_t *order = nullptr;
+    const bool time_tiles = t->train_order.begin(tiles, n_cams, width, height, order);
     t->last_launches = 0;
     t->last_has_stats = t->stats_enabled;
     if (t->stats_enabled) {
@@ -1657,8 +1700,8 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
             p.rec_limit = std::min<uint32_t>(t->rec_entries, ts->max_steps);
             p.pool_chunks = (uint32_t)std::min<size_t>(t->rec_pool_chunks, 0xfffffff0u);
         }
-        p.tile_order = use_order ? t->tile_order : nullptr;
-        p.tile_cost = time_tiles ? t->tile_cost : nullptr;
+        p.base.tile_order = order;
+        p.base.tile_cost = time_tiles ? t->train_order.cost : nullptr;
         SP_CUDA(launch_splat_train(p, false, s), "splat training forward launch");
         if (rec_chunks) {
             SP_CUDA(cudaMemcpyAsync(t->rec_demand, p.rec_next, sizeof(uint32_t),
@@ -1666,16 +1709,12 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
             SP_CUDA(cudaEventRecord(t->rec_event, s), "event");
         }
         p.base.stats = nullptr;
+        p.base.tile_cost = nullptr;
         SP_CUDA(launch_splat_train(p, true, s), "splat training backward launch");
         t->last_launches += 2;
         if (time_tiles) {
-            SP_CUDA(launch_tile_order(t->tile_cost, (uint32_t)tiles, t->order_counts,
-                                      t->tile_order, s), "tile order");
+            SP_CUDA(t->train_order.end(tiles, n_cams, width, height, s), "tile order");
             t->last_launches += 2;
-            t->order_cams.assign(cams, cams + n_cams);
-            t->order_w = width;
-            t->order_h = height;
-            t->order_valid = true;
         }
     }
     if (want_site) {

@@ -133,3 +133,26 @@ def test_stats_count_rays_and_intervals():
     _, steps = O.render_splats(O.OracleModel.from_scene(m), cam[0], 20, 20, 1024, 0.0)
     assert st.rays == 400 and st.steps == int(steps.sum()) and st.kernel_ms > 0
     t.deinit()
+
+
+def test_repeated_renders_take_tiles_heaviest_first_bit_exact():
+    """A dispatch of the same shape as the one before takes its tiles in the
+    order of the previous dispatch's tile durations (two more launches build
+    it); the image does not depend on that order, for the same cameras or
+    moved ones."""
+    m = scenes.powerfoam_mixture(3000, seed=4, radius_max=0.15)
+    cams = scenes.sphere_cameras(2, 3.0, 5, math.radians(55.0), 1.0, 100.0)
+    moved = scenes.sphere_cameras(2, 3.0, 6, math.radians(55.0), 1.0, 100.0)
+    om = O.OracleModel.from_scene(m)
+    t = bv.PowerFoamSplatTracer(m)
+    try:
+        for views in (cams, cams, moved, cams):
+            img = t.render(views, 48, 40)
+            torch.cuda.synchronize()
+            assert t.last_stats().launches == 3  # render, order x 2
+            got = img.cpu().numpy()
+            for v, cam in enumerate(views):
+                ref, _ = O.render_splats(om, cam, 48, 40)
+                assert np.array_equal(bits(got[v]), bits(ref)), v
+    finally:
+        t.deinit()

@@ -100,10 +100,10 @@ def test_splat_training_settings_and_accumulation():
 
 
 def test_repeated_calls_take_tiles_heaviest_first_with_the_same_results():
-    """A call over the same views and size as the one before takes its tiles
-    in the order of the previous forward's tile durations (two more launches
-    per call build that order); other views, or another size, go back to
-    launch order.  Every call is held to the oracle."""
+    """A call of the same shape (views, width, height) as the one before
+    takes its tiles in the order of the previous forward's tile durations
+    (two more launches per call build that order), whether its cameras are
+    the same or not.  Every call is held to the oracle."""
     m, cams, target = case(seed=5, n=3000)
     other = scenes.sphere_cameras(3, 3.0, 11, math.radians(55.0), 1.0, 100.0)
     om = O.OracleModel.from_scene(m)
