@@ -751,7 +751,7 @@ def run_serving(args):
         for rate, r in out[mode].items():
             d = r["per_resolution"].get("1920x1080", {})
             res[rate] = {k: d.get(k, {}).get("p99_ms") for k in
-                         ("first_frame", "frame_interval", "frame")}
+                         ("first_frame", "paced_frame", "frame_interval", "frame")}
         return res
     line = {"metric": "serving Mrays/s", "value": b["mrays_per_s"], "unit": "Mrays/s",
             "higher_is_better": True, "n_gpus": 1, "dtype": "f32", "data": "synthetic",

@@ -23,6 +23,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <thread>
+#include <utility>
 #include <vector>
 
 #include "bv_bvh.h"
@@ -46,6 +48,16 @@ namespace {
 #ifndef BV_MINB_SPLAT
 #define BV_MINB_SPLAT 4
 #endif
+// Resident blocks per SM asked of the training forward (0: no minimum; the
+// compiler then takes 80 registers, 6 blocks by registers and shared memory).
+#ifndef BV_MINB_SPLAT_TRAIN
+#define BV_MINB_SPLAT_TRAIN 0
+#endif
+#if BV_MINB_SPLAT_TRAIN
+#define SPLAT_TRAIN_BOUNDS __launch_bounds__(kSplatBlock, BV_MINB_SPLAT_TRAIN)
+#else
+#define SPLAT_TRAIN_BOUNDS __launch_bounds__(kSplatBlock)
+#endif
 #ifndef BV_SPLAT_SHARED_NUM
 #define BV_SPLAT_SHARED_NUM 1
 #endif
@@ -55,13 +67,19 @@ namespace {
 #endif
 // Cech-row clip: each chunk of a row staged in the warp's shared memory (1)
 // or broadcast lane to lane with shuffles (0); entries read from shared
-// memory per iteration of the clip loop, 1, 2 or 4 (2: 30.3 -> 32.9 Mrays/s
-// for config-2 training, 23.8 -> 26.4 for its render).
+// memory per iteration of the clip loop, 1, 2 or 4 (config-2 training
+// 30.4 / 32.7 / 33.2 Mrays/s, its render 23.8 / 26.4 / 27.3 before tile
+// ordering and 37.0 / 38.1 for 2 / 4 with it).
 #ifndef BV_SPLAT_SMEM_ROWS
 #define BV_SPLAT_SMEM_ROWS 1
 #endif
 #ifndef BV_SPLAT_CLIP_ILP
-#define BV_SPLAT_CLIP_ILP 2
+#define BV_SPLAT_CLIP_ILP 4
+#endif
+// Each Cech row's clip planes stored nearest to the site first (1), so that
+// a support the clip empties is left after fewer planes, or in CSR order (0).
+#ifndef BV_SPLAT_ROW_SORT
+#define BV_SPLAT_ROW_SORT 1
 #endif
 // Training launches take tiles heaviest first (1), ordered by the time each
 // tile's forward took in the previous call over the same views, or in
@@ -107,10 +125,15 @@ struct __align__(16) SplatPrim {
 // One Cech entry of a support's row: the clip plane's point f = s_i + shift n
 // and normal n = s_j - s_i (shift = 0.5 + 0.5 (r_i^2 - r_j^2) / max(|n|^2,
 // 1e-20)), formed on the host in the kernel's FP32 operation order
-// (trace.rs:1351-1389), so each ray evaluates only (f - o).n and d.n.
+// (trace.rs:1351-1389), so each ray evaluates only (f - o).n and d.n.  A
+// row's entries may be stored in any order (nearest plane first, see
+// BV_SPLAT_ROW_SORT): each carries its offset in the CSR row, which breaks
+// ties between planes at the same depth as the CSR order does, and its
+// neighbour.  Interval keys and records name an entry by its stored
+// position.
 struct __align__(16) SplatFace {
-    float4 point;   // f, 0
-    float4 normal;  // n, 0
+    float4 point;   // f, CSR offset in the row (uint bits)
+    float4 normal;  // n, neighbour j (uint bits)
 };
 
 struct SplatParams {
@@ -206,19 +229,28 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
                                                 float &dt, uint32_t &links) {
     const uint32_t lane = threadIdx.x & 31u;
     float face_near = 0.0f, face_far = depth;
-    uint32_t near_k = kNoPlane, far_k = kNoPlane;
+    uint32_t near_k = kNoPlane, far_k = kNoPlane;  // stored positions in the row
     bool empty = !need;
-    // One Cech entry (row offset k, numerator <f - o, n>, denominator
-    // <d, n>) applied to this lane's interval.  A plane whose quotient
-    // provably cannot tighten the interval is passed without dividing
-    // (clip_*_cannot_tighten); the planes that can are divided and compared,
-    // so the interval and the planes that bound it are the same bit for bit.
-    auto clip_entry = [&](float num, float den, uint32_t k) {
+    // CSR offset of the entry stored at position k (ties only: rare)
+    auto csr_offset = [&](uint32_t k) {
+        return __float_as_uint(__ldg(&P.row_faces[begin + k].point.w));
+    };
+    // One Cech entry (stored position k, CSR offset o, numerator <f - o, n>,
+    // denominator <d, n>) applied to this lane's interval.  The bounds are a
+    // min / max over the row; of planes at the same depth the one earliest
+    // in CSR order bounds the interval, as the reference's scan in CSR order
+    // keeps the first, whatever order the entries are taken in.  A plane
+    // whose quotient provably cannot reach the bound is passed without
+    // dividing (clip_*_cannot_tighten: the rounded quotient is then
+    // strictly beyond it, so no tie is passed either); the planes that can
+    // are divided and compared, so the interval and the planes that bound it
+    // are the same bit for bit.
+    auto clip_entry = [&](float num, float den, uint32_t k, uint32_t o) {
         bool moved = false;
         if (den > 1.0e-20f) {
             if (!clip_far_cannot_tighten(num, den, face_far)) {
                 const float t = num / den;
-                if (t < face_far) {
+                if (t < face_far || (t == face_far && far_k != kNoPlane && o < csr_offset(far_k))) {
                     face_far = t;
                     far_k = k;
                     moved = true;
@@ -227,7 +259,8 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
         } else if (den < -1.0e-20f) {
             if (!clip_near_cannot_tighten(num, den, face_near)) {
                 const float t = num / den;
-                if (t > face_near) {
+                if (t > face_near ||
+                    (t == face_near && near_k != kNoPlane && o < csr_offset(near_k))) {
                     face_near = t;
                     near_k = k;
                     moved = true;
@@ -263,9 +296,12 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
         // reads the entries it needs (broadcast reads) and leaves the row
         // alone as soon as its interval is empty.
         __shared__ float4 s_row[kSplatBlock];
+        __shared__ uint32_t s_row_off[kSplatBlock];
         float4 *row = s_row + (threadIdx.x & ~31u);
+        uint32_t *row_off = s_row_off + (threadIdx.x & ~31u);
         __syncwarp();
         row[lane] = make_float4(num_own, fn.x, fn.y, fn.z);
+        row_off[lane] = __float_as_uint(fp.w);
         __syncwarp();
 #if BV_SPLAT_CLIP_ILP > 1
         // BV_SPLAT_CLIP_ILP entries per iteration: their denominators are
@@ -281,15 +317,17 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
                 e[u] = row[min(j + u, 31u)];
                 den[u] = dot3(ray.dx, ray.dy, ray.dz, e[u].y, e[u].z, e[u].w);
             }
-            clip_entry(e[0].x, den[0], base + j - begin);
+            clip_entry(e[0].x, den[0], base + j - begin, row_off[j]);
 #pragma unroll
             for (uint32_t u = 1; u < kIlp; ++u)
-                if (j + u < n && !empty) clip_entry(e[u].x, den[u], base + j + u - begin);
+                if (j + u < n && !empty)
+                    clip_entry(e[u].x, den[u], base + j + u - begin, row_off[j + u]);
         }
 #else
         for (uint32_t j = 0; j < n && !empty; ++j) {
             const float4 e = row[j];
-            clip_entry(e.x, dot3(ray.dx, ray.dy, ray.dz, e.y, e.z, e.w), base + j - begin);
+            clip_entry(e.x, dot3(ray.dx, ray.dy, ray.dz, e.y, e.z, e.w), base + j - begin,
+                       row_off[j]);
         }
 #endif
 #else
@@ -304,11 +342,12 @@ __device__ __forceinline__ bool splat_clip_warp(const SplatParams &P, const WinR
             const float nx = __shfl_sync(0xffffffffu, fn.x, j);
             const float ny = __shfl_sync(0xffffffffu, fn.y, j);
             const float nz = __shfl_sync(0xffffffffu, fn.z, j);
+            const uint32_t o = __shfl_sync(0xffffffffu, __float_as_uint(fp.w), j);
             if (empty) continue;
 #if !BV_SPLAT_SHARED_NUM
             const float num = dot3(fx - ray.ox, fy - ray.oy, fz - ray.oz, nx, ny, nz);
 #endif
-            clip_entry(num, dot3(ray.dx, ray.dy, ray.dz, nx, ny, nz), base + j - begin);
+            clip_entry(num, dot3(ray.dx, ray.dy, ray.dz, nx, ny, nz), base + j - begin, o);
         }
 #endif
     }
@@ -593,9 +632,10 @@ __device__ __forceinline__ uint32_t rec_chunk_for_write(const SplatTrainParams &
 // the sphere clip, evaluated as splat_clip_warp evaluates them, and the
 // neighbours across them (the cell itself when none).
 __device__ __forceinline__ float splat_plane_t(const SplatTrainParams &TP, const WinRay &ray,
-                                               uint32_t k) {
+                                               uint32_t k, uint32_t &neighbour) {
     const float4 fp = __ldg(&TP.base.row_faces[k].point);
     const float4 fn = __ldg(&TP.base.row_faces[k].normal);
+    neighbour = __float_as_uint(fn.w);
     const float rx = fp.x - ray.ox, ry = fp.y - ray.oy, rz = fp.z - ray.oz;
     const float num = dot3(rx, ry, rz, fn.x, fn.y, fn.z);
     const float den = dot3(ray.dx, ray.dy, ray.dz, fn.x, fn.y, fn.z);
@@ -611,18 +651,12 @@ __device__ __forceinline__ void splat_planes_of(const SplatTrainParams &TP, cons
     face_near = 0.0f;
     face_far = depth;
     prev = next = cell;
-    if (nk != kNoPlane) {
-        face_near = splat_plane_t(TP, ray, b + nk);
-        prev = __ldg(TP.neighbors + b + nk);
-    }
-    if (fk != kNoPlane) {
-        face_far = splat_plane_t(TP, ray, b + fk);
-        next = __ldg(TP.neighbors + b + fk);
-    }
+    if (nk != kNoPlane) face_near = splat_plane_t(TP, ray, b + nk, prev);
+    if (fk != kNoPlane) face_far = splat_plane_t(TP, ray, b + fk, next);
 }
 
 template <int DEG, bool BF16>
-__global__ void __launch_bounds__(kSplatBlock)
+__global__ void SPLAT_TRAIN_BOUNDS
 splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
     const SplatParams &P = TP.base;
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1243,6 +1277,52 @@ uint16_t bf16_rne(float f) {
 }
 
 // Enqueues the splat kernel for the cameras (chunks of kMaxViewsPerLaunch).
+// The clip planes of rows [r0, r1) of the Cech CSR into `rows` (see
+// SplatFace), each row in BV_SPLAT_ROW_SORT order.
+void build_clip_rows_range(const bv_model_desc *md, uint32_t r0, uint32_t r1, SplatFace *rows) {
+    std::vector<std::pair<double, uint32_t>> order;
+    std::vector<SplatFace> faces;
+    for (uint32_t i = r0; i < r1; ++i) {
+        const float *si = md->points + 4 * (size_t)i;
+        const float ri = md->radii[i];
+        const uint32_t b = md->adjacency_offsets[i], e = md->adjacency_offsets[i + 1];
+        order.clear();
+        faces.resize(e - b);
+        for (uint32_t k = b; k < e; ++k) {
+            const uint32_t j = md->adjacency_neighbors[k];
+            const float *a = md->points + 4 * (size_t)j;
+            const float rj = md->radii[j];
+            const float nx = a[0] - si[0], ny = a[1] - si[1], nz = a[2] - si[2];
+            const float dsq = std::max((nx * nx + ny * ny) + nz * nz, 1.0e-20f);
+            const float shift = 0.5f + 0.5f * (ri * ri - rj * rj) / dsq;
+            SplatFace &f = faces[k - b];
+            uint32_t off = k - b;
+            float off_bits, nbr_bits;
+            std::memcpy(&off_bits, &off, 4);
+            std::memcpy(&nbr_bits, &j, 4);
+            f.point = make_float4(si[0] + shift * nx, si[1] + shift * ny, si[2] + shift * nz, off_bits);
+            f.normal = make_float4(nx, ny, nz, nbr_bits);
+            double key = BV_SPLAT_ROW_SORT ? (double)shift * std::sqrt((double)dsq) : 0.0;
+            if (!(key == key)) key = INFINITY;  // a NaN sorts last
+            order.emplace_back(key, off);
+        }
+        std::sort(order.begin(), order.end());
+        for (uint32_t p = 0; p < e - b; ++p) rows[b + p] = faces[order[p].second];
+    }
+}
+
+void build_clip_rows(const bv_model_desc *md, uint32_t n, SplatFace *rows) {
+    const uint32_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const uint32_t workers = std::min<uint32_t>(hw, std::max<uint32_t>(1u, n / 4096u));
+    std::vector<std::thread> pool;
+    for (uint32_t w = 0; w < workers; ++w) {
+        const uint32_t r0 = (uint32_t)((uint64_t)n * w / workers);
+        const uint32_t r1 = (uint32_t)((uint64_t)n * (w + 1) / workers);
+        pool.emplace_back(build_clip_rows_range, md, r0, r1, rows);
+    }
+    for (auto &th : pool) th.join();
+}
+
 bv_status enqueue_splats(bv_splat_tracer *t, float4 *out, const bv_camera *cams, uint32_t n,
                          uint32_t w, uint32_t h, bool count_only, cudaStream_t s) {
     for (uint32_t c0 = 0; c0 < n; c0 += kMaxViewsPerLaunch) {
@@ -1341,22 +1421,11 @@ bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *md, const bv_trace_
         prims[i].link = make_uint4(c, md->adjacency_offsets[c], md->adjacency_offsets[c + 1], 0u);
     }
     // clip planes of every Cech entry, FP32 in the per-ray order of
-    // powerfoam_splat_interval (this file is built with FP contraction off)
+    // powerfoam_splat_interval (this file is built with FP contraction off);
+    // each row stored nearest plane first (the plane's distance from the
+    // site, shift |n|; ties by CSR offset), over the host's threads
     std::vector<SplatFace> rows(std::max<uint32_t>(m_edges, 1));
-    for (uint32_t i = 0; i < n; ++i) {
-        const float *si = md->points + 4 * (size_t)i;
-        const float ri = md->radii[i];
-        for (uint32_t k = md->adjacency_offsets[i]; k < md->adjacency_offsets[i + 1]; ++k) {
-            const uint32_t j = md->adjacency_neighbors[k];
-            const float *a = md->points + 4 * (size_t)j;
-            const float rj = md->radii[j];
-            const float nx = a[0] - si[0], ny = a[1] - si[1], nz = a[2] - si[2];
-            const float dsq = std::max((nx * nx + ny * ny) + nz * nz, 1.0e-20f);
-            const float shift = 0.5f + 0.5f * (ri * ri - rj * rj) / dsq;
-            rows[k].point = make_float4(si[0] + shift * nx, si[1] + shift * ny, si[2] + shift * nz, 0.f);
-            rows[k].normal = make_float4(nx, ny, nz, 0.f);
-        }
-    }
+    build_clip_rows(md, n, rows.data());
     std::vector<float> dens(n);
     std::vector<float4> geom(n);
     for (uint32_t i = 0; i < n; ++i) {

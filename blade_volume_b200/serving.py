@@ -11,7 +11,11 @@ p50/p99 latencies, each measured from the request's scheduled arrival:
   frame        until each frame is on the host (one sample per frame);
   frame_interval  the time a viewer of the request waits for each frame: the
                first frame from arrival, every later one from the frame
-               before it (frames in the order they landed).
+               before it (frames in the order they landed);
+  paced_frame  a streamed request: frame k is asked for k frame periods
+               after arrival (the server's deadline for it is one period
+               later), and its latency runs from then until it is on the
+               host (negative when it landed ahead of being asked for).
 Frame figures cover render requests; a forward+backward request's colours
 land with its gradients, so it counts in request latency only.  Its work is
 summarised as Mrays/s over the stream's span and over the time from its
@@ -128,8 +132,10 @@ def percentile(values, q: float) -> Optional[float]:
 
 
 def run_stream(server, specs: Sequence[RequestSpec], bufs: HostBuffers,
-               timeout: float = 600.0) -> dict:
-    """Submit every request at its arrival time, wait for all, summarise."""
+               timeout: float = 600.0, frame_period_s: float = 0.016) -> dict:
+    """Submit every request at its arrival time, wait for all, summarise.
+    frame_period_s: the server's frame period (frame k of a request is asked
+    for k periods after its arrival)."""
     t0 = server.clock() + 0.01
     sub = []
     for spec in specs:
@@ -143,7 +149,7 @@ def run_stream(server, specs: Sequence[RequestSpec], bufs: HostBuffers,
         rid = server.submit(spec.scene, spec.cameras, spec.width, spec.height,
                             frame_done=frame_done, **bufs.request_args(spec))
         sub.append((rid, spec, due, frame_done))
-    lat, frame_lat, first_lat, gaps = [], [], [], []
+    lat, frame_lat, first_lat, gaps, paced_lat = [], [], [], [], []
     fwdbwd_rays = 0
     fwdbwd_busy = 0.0
     per_res: Dict[str, Dict[str, list]] = {}
@@ -169,7 +175,7 @@ def run_stream(server, specs: Sequence[RequestSpec], bufs: HostBuffers,
             per_res_fb.setdefault(key, []).append(r["done_s"] - due)
             continue
         d = per_res.setdefault(key, dict(request=[], frame=[], first_frame=[],
-                                         frame_interval=[]))
+                                         frame_interval=[], paced_frame=[]))
         d["request"].append(r["done_s"] - due)
         f = [float(x) - due for x in frame_done]
         frame_lat.extend(f)
@@ -180,6 +186,9 @@ def run_stream(server, specs: Sequence[RequestSpec], bufs: HostBuffers,
         g = [landed[0]] + [b - a for a, b in zip(landed, landed[1:])]
         gaps.extend(g)
         d["frame_interval"].extend(g)
+        paced = [x - k * frame_period_s for k, x in enumerate(f)]
+        paced_lat.extend(paced)
+        d["paced_frame"].extend(paced)
     span = end - t0
     ms = 1e3
 
@@ -194,6 +203,7 @@ def run_stream(server, specs: Sequence[RequestSpec], bufs: HostBuffers,
                                             if fwdbwd_busy > 0 else None),
                 request_latency=pct(lat), first_frame_latency=pct(first_lat),
                 frame_latency=pct(frame_lat), frame_interval=pct(gaps),
+                paced_frame_latency=pct(paced_lat),
                 per_kind={k: pct(v) for k, v in per_kind.items()},
                 per_resolution={k: {m: pct(x) for m, x in v.items()}
                                 for k, v in sorted(per_res.items())},

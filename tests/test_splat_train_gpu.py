@@ -129,3 +129,48 @@ def test_repeated_calls_take_tiles_heaviest_first_with_the_same_results():
             gradcheck.check_all(g, ref, where=f"tile order call {i}")
     finally:
         t.deinit()
+
+
+def test_planes_at_the_same_depth_bound_the_interval_in_csr_order():
+    """Site 0's Cech row holds site 1 (offset 0) and site 2 (offset 1).  Both
+    planes cross the ray z = -10 + t along the axis at t = 11 exactly (num /
+    den = 22 / 2 and 11 / 1 in FP32), so the exit plane of site 0's interval
+    is a tie, which the reference's scan in CSR order gives to site 1.  The
+    device stores the row nearest plane first (site 2's plane, 0.71 from the
+    site, before site 1's, at 1.0) and must still pick site 1: the gradient of
+    the exit plane's Jacobian lands on site 1's position."""
+    pts = np.array([[0, 0, 0, 2.0], [0, 0, 2, 1.5], [1, 0, 1, 1.0]], np.float32)
+    offsets = np.array([0, 2, 4, 6], np.uint32)
+    neighbors = np.array([1, 2, 0, 2, 0, 1], np.uint32)
+    sh = np.zeros((3, 3), np.float32)
+    sh[:, 0] = [1.0, 0.2, 0.6]
+    sh[:, 1] = [0.3, 1.0, 0.4]
+    sh[:, 2] = [0.5, 0.7, 1.0]
+    m = scenes.PointCloudModel(pts, sh, 0, offsets, neighbors, np.full(3, 1.2, np.float32))
+    # the tie, in the clip's own FP32 operations
+    o = np.float32(-10.0)
+    t1 = np.float32(np.float32(2.0) * (np.float32(1.0) - o)) / np.float32(2.0)
+    f2 = (np.float32(0.5), np.float32(0.5))
+    t2 = np.float32(f2[0] * np.float32(1.0) + (f2[1] - o) * np.float32(1.0)) / np.float32(1.0)
+    assert t1 == t2 == np.float32(11.0)
+    cam = scenes.looking_at((0.0, 0.0, -10.0), (0.0, 0.0, 1.0), math.radians(10.0), 1.0, 100.0)
+    target = np.zeros((1, 1, 1, 3), np.float32)
+    om = O.OracleModel.from_scene(m)
+    ref = O.forward_backward(om, [cam], 1, 1, target=target, splats=True, want_mass=True)
+    t = bv.PowerFoamSplatTracer(m)
+    try:
+        grads = t.new_grads()
+        rgb = torch.zeros((1, 1, 1, 3), dtype=torch.float32, device="cuda")
+        loss = t.forward_backward([cam], 1, 1, torch.from_numpy(target).cuda(), grads, rgb_out=rgb)
+        torch.cuda.synchronize()
+        g = {k: v.cpu().numpy().astype(np.float64) for k, v in grads.items()}
+    finally:
+        t.deinit()
+    g["d_pos"] = g["d_pos"].reshape(-1, 3)
+    assert np.array_equal(rgb.cpu().numpy().view(np.uint32), ref["rgb32"].view(np.uint32))
+    assert abs(float(loss.item()) - ref["loss"]) <= 1e-5 * ref["loss"]
+    # the exit plane is site 1's: site 2, across the tied plane, gets nothing
+    # (with site 2 first in the CSR row it would take the Jacobian instead)
+    ref_pos = ref["d_pos"].reshape(-1, 3)
+    assert ref_pos[1, 2] != 0 and not ref_pos[2].any()
+    gradcheck.check_all(g, ref, where="tied exit planes")
