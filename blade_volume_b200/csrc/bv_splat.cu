@@ -1226,6 +1226,12 @@ struct bv_splat_tracer {
     bool stats_enabled = false, last_has_stats = false;
     uint32_t last_launches = 0;
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    // every dispatch and training call: its end, and the stream it ran on
+    // (a call on another stream waits for it: the tile orders, ray state and
+    // interval record are the tracer's)
+    cudaEvent_t done = nullptr;
+    cudaStream_t work_stream = nullptr;
+    bool worked = false;
 
     DeviceModel model() const {
         DeviceModel m;
@@ -1266,6 +1272,7 @@ void free_splat(bv_splat_tracer *t) {
     cudaFree(t->count_totals);
     for (auto &e : t->ev)
         if (e) cudaEventDestroy(e);
+    if (t->done) cudaEventDestroy(t->done);
     delete t;
 }
 
@@ -1321,6 +1328,21 @@ void build_clip_rows(const bv_model_desc *md, uint32_t n, SplatFace *rows) {
         pool.emplace_back(build_clip_rows_range, md, r0, r1, rows);
     }
     for (auto &th : pool) th.join();
+}
+
+// Orders a call on stream s after the tracer's previous call when that ran
+// on another stream; marks the call's end afterwards.
+bv_status order_after_previous(bv_splat_tracer *t, cudaStream_t s) {
+    if (t->worked && t->work_stream != s)
+        SP_CUDA(cudaStreamWaitEvent(s, t->done, 0), "stream wait on the previous call");
+    return BV_OK;
+}
+
+bv_status mark_call_end(bv_splat_tracer *t, cudaStream_t s) {
+    SP_CUDA(cudaEventRecord(t->done, s), "event record");
+    t->work_stream = s;
+    t->worked = true;
+    return BV_OK;
 }
 
 bv_status enqueue_splats(bv_splat_tracer *t, float4 *out, const bv_camera *cams, uint32_t n,
@@ -1494,6 +1516,7 @@ bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *md, const bv_trace_
         SP_TRY(cudaMemcpy(t->sh, row.data(), row.size() * 4, cudaMemcpyHostToDevice), "upload sh");
     }
     for (auto &e : t->ev) SP_TRY(cudaEventCreate(&e), "cudaEventCreate");
+    SP_TRY(cudaEventCreateWithFlags(&t->done, cudaEventDisableTiming), "cudaEventCreate");
 #undef SP_TRY
     *out = t;
     return BV_OK;
@@ -1518,6 +1541,8 @@ bv_status bv_powerfoam_splat_tracer_dispatch_batch(bv_splat_tracer *t, float *ou
         if (st != BV_OK) return st;
     }
     cudaStream_t s = (cudaStream_t)stream;
+    bv_status st = order_after_previous(t, s);
+    if (st != BV_OK) return st;
     t->last_cams.assign(cams, cams + n_cams);
     t->last_w = width;
     t->last_h = height;
@@ -1528,11 +1553,11 @@ bv_status bv_powerfoam_splat_tracer_dispatch_batch(bv_splat_tracer *t, float *ou
         SP_CUDA(cudaMemsetAsync(t->stats, 0, 4 * sizeof(unsigned long long), s), "stats reset");
         SP_CUDA(cudaEventRecord(t->ev[0], s), "event");
     }
-    const bv_status st = enqueue_splats(t, reinterpret_cast<float4 *>(out_rgba_dev), cams, n_cams,
-                                        width, height, false, s);
+    st = enqueue_splats(t, reinterpret_cast<float4 *>(out_rgba_dev), cams, n_cams, width, height,
+                        false, s);
     if (st != BV_OK) return st;
     if (t->stats_enabled) SP_CUDA(cudaEventRecord(t->ev[1], s), "event");
-    return BV_OK;
+    return mark_call_end(t, s);
 }
 
 bv_status bv_powerfoam_splat_tracer_dispatch(bv_splat_tracer *t, float *out_rgba_dev,
@@ -1546,12 +1571,16 @@ bv_status bv_powerfoam_splat_tracer_candidate_stats(bv_splat_tracer *t, uint32_t
     if (!t || !max_hits) return sp_fail(BV_ERR_INVALID_ARGUMENT, "null argument");
     if (t->last_cams.empty()) return sp_fail(BV_ERR_INVALID_ARGUMENT, "no dispatch to count");
     cudaStream_t s = t->last_stream;
+    bv_status st = order_after_previous(t, s);
+    if (st != BV_OK) return st;
     SP_CUDA(cudaMemsetAsync(t->max_candidates, 0, sizeof(uint32_t), s), "counter reset");
     SP_CUDA(cudaMemsetAsync(t->count_totals, 0, 2 * sizeof(unsigned long long), s), "counter reset");
     const uint32_t launches = t->last_launches;
-    const bv_status st = enqueue_splats(t, nullptr, t->last_cams.data(), (uint32_t)t->last_cams.size(),
-                                        t->last_w, t->last_h, true, s);
+    st = enqueue_splats(t, nullptr, t->last_cams.data(), (uint32_t)t->last_cams.size(), t->last_w,
+                        t->last_h, true, s);
     t->last_launches = launches;
+    if (st != BV_OK) return st;
+    st = mark_call_end(t, s);
     if (st != BV_OK) return st;
     uint32_t h = 0;
     unsigned long long tot[2] = {0, 0};
@@ -1652,6 +1681,10 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         if (st != BV_OK) return st;
     }
     cudaStream_t s = (cudaStream_t)stream;
+    {
+        const bv_status st = order_after_previous(t, s);
+        if (st != BV_OK) return st;
+    }
     if (chunk_rays > t->ray_state_capacity) {
         cudaFree(t->ray_state);
         t->ray_state = nullptr;
@@ -1792,7 +1825,7 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         t->last_launches += 1;
     }
     if (t->stats_enabled) SP_CUDA(cudaEventRecord(t->ev[1], s), "event");
-    return BV_OK;
+    return mark_call_end(t, s);
 }
 
 }  // extern "C"

@@ -372,7 +372,13 @@ typedef struct bv_splat_tracer bv_splat_tracer;
 bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *model, const bv_trace_settings *settings,
                                         bv_splat_tracer **out);
 void bv_powerfoam_splat_tracer_destroy(bv_splat_tracer *tracer);
-/* Renders [height][width][4] float32 (RGB, alpha = 1 - transmittance). */
+/* Renders [height][width][4] float32 (RGB, alpha = 1 - transmittance).
+ * Dispatches and training calls time their 8x4-pixel tiles; a later call of
+ * the same shape (views, width, height) starts its tiles heaviest first by
+ * those times (two more small launches per call build the order).  The
+ * order changes no result.  A call on a different stream than the tracer's
+ * previous call is ordered after it (an event wait): the tile orders, ray
+ * state and interval record belong to the tracer. */
 bv_status bv_powerfoam_splat_tracer_dispatch(bv_splat_tracer *tracer, float *out_rgba_dev,
                                              const bv_camera *camera, uint32_t width, uint32_t height,
                                              bv_stream stream);

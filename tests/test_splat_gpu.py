@@ -156,3 +156,25 @@ def test_repeated_renders_take_tiles_heaviest_first_bit_exact():
                 assert np.array_equal(bits(got[v]), bits(ref)), v
     finally:
         t.deinit()
+
+
+def test_dispatches_on_two_streams_are_ordered():
+    """Three dispatches of one tracer of the same shape, on alternating
+    streams with no host synchronisation: each later one reads the tile
+    order the one before it writes, so it waits for it; every image matches
+    the oracle."""
+    m = scenes.powerfoam_mixture(3000, seed=7, radius_max=0.15)
+    cams = scenes.sphere_cameras(3, 3.0, 8, math.radians(55.0), 1.0, 100.0)
+    om = O.OracleModel.from_scene(m)
+    t = bv.PowerFoamSplatTracer(m)
+    try:
+        streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+        outs = [torch.empty((1, 40, 48, 4), dtype=torch.float32, device="cuda") for _ in cams]
+        for k, cam in enumerate(cams):
+            t.dispatch_batch(outs[k], [cam], (48, 40), stream=streams[k % 2])
+        torch.cuda.synchronize()
+        for k, cam in enumerate(cams):
+            ref, _ = O.render_splats(om, cam, 48, 40)
+            assert np.array_equal(bits(outs[k].cpu().numpy()[0]), bits(ref)), k
+    finally:
+        t.deinit()
