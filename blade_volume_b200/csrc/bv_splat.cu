@@ -49,9 +49,11 @@ namespace {
 #define BV_MINB_SPLAT 4
 #endif
 // Resident blocks per SM asked of the training forward (0: no minimum; the
-// compiler then takes 80 registers, 6 blocks by registers and shared memory).
+// compiler then takes 80 registers and spills, 6 blocks by registers and
+// shared memory; 5: 94 registers without spills, 50.6 vs 49.6 Mrays/s for
+// config-2 training; 4: 42.6).
 #ifndef BV_MINB_SPLAT_TRAIN
-#define BV_MINB_SPLAT_TRAIN 0
+#define BV_MINB_SPLAT_TRAIN 5
 #endif
 #if BV_MINB_SPLAT_TRAIN
 #define SPLAT_TRAIN_BOUNDS __launch_bounds__(kSplatBlock, BV_MINB_SPLAT_TRAIN)
