@@ -93,20 +93,28 @@ constexpr int kSplatBlock = 128;
 constexpr int kSplatWindow = BV_SPLAT_WINDOW;
 constexpr int kSplatStack = 80;  // > BVH depth, checked at tracer creation
 
+// Dynamic shared memory of a splat kernel's window: `fields` words per key
+// (3 for WinKey, 4 for WinKey2), kSplatWindow keys per thread.
+constexpr size_t splat_window_bytes(int fields) {
+    return (BV_SPLAT_SMEM_WINDOW ? (size_t)fields * kSplatWindow * kSplatBlock * 4u : 0u);
+}
+
 // The window of a splat kernel: SPLAT_WINDOW(Key) declares it (shared memory
 // per thread, or a register array), SPLAT_GATHER runs one pass into it and
 // SPLAT_KEY(i) reads key i.
 #if BV_SPLAT_SMEM_WINDOW
+// in dynamic shared memory (splat_window_bytes per block, set at launch), so
+// that windows of more than 20 keys fit: field f of key i of thread tid at
+// word (f W + i) 128 + tid
 #define SPLAT_WINDOW(KEY)                                                                      \
-    __shared__ float s_win_t[kSplatWindow * kSplatBlock];                                     \
-    __shared__ uint32_t s_win_idx[kSplatWindow * kSplatBlock];                                \
-    __shared__ uint32_t s_win_pos[kSplatWindow * kSplatBlock];                                \
-    __shared__ uint32_t s_win_aux[sizeof(KEY) == sizeof(WinKey2) ? kSplatWindow * kSplatBlock \
-                                                                  : 1];                       \
-    SmemWindow<kSplatWindow, KEY> win{s_win_t + threadIdx.x, s_win_idx + threadIdx.x,         \
-                                      s_win_pos + threadIdx.x,                                \
-                                      s_win_aux + (sizeof(KEY) == sizeof(WinKey2) ? threadIdx.x : 0), \
-                                      kSplatBlock}
+    extern __shared__ uint32_t s_win_dyn[];                                                   \
+    SmemWindow<kSplatWindow, KEY> win{                                                        \
+        reinterpret_cast<float *>(s_win_dyn) + threadIdx.x,                                   \
+        s_win_dyn + 1 * kSplatWindow * kSplatBlock + threadIdx.x,                             \
+        s_win_dyn + 2 * kSplatWindow * kSplatBlock + threadIdx.x,                             \
+        s_win_dyn + (sizeof(KEY) == sizeof(WinKey2) ? 3 * kSplatWindow * kSplatBlock + threadIdx.x \
+                                                    : 0),                                     \
+        kSplatBlock}
 #define SPLAT_GATHER(...) win_gather_warp_smem<kSplatWindow, kSplatStack>(__VA_ARGS__, win, nodes_visited, hit)
 #define SPLAT_KEY(i) win.get(i)
 #else
@@ -913,7 +921,7 @@ __device__ __forceinline__ void scatter_interval_warp(const SplatTrainParams &TP
 // overflow, or no record) gather the same windows in the same order again
 // and recompute each interval's colour.  Both feed splat_interval_grad.
 template <int DEG, bool BF16>
-__global__ void __launch_bounds__(kSplatBlock)
+__global__ void __launch_bounds__(kSplatBlock, 5)
 splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
     const SplatParams &P = TP.base;
     constexpr int K = ShDims<DEG>::K;
@@ -1016,31 +1024,42 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
     }
 }
 
-#define BV_SPLAT_SELECT(KERNEL, PARAMS, DEGREE, BF, BLOCKS, STREAM)                       \
-    do {                                                                                  \
-        switch ((int)(DEGREE) * 2 + ((BF) ? 1 : 0)) {                                     \
-            case 0: KERNEL<0, false><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;  \
-            case 1: KERNEL<0, true><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;   \
-            case 2: KERNEL<1, false><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;  \
-            case 3: KERNEL<1, true><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;   \
-            case 4: KERNEL<2, false><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;  \
-            case 5: KERNEL<2, true><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;   \
-            case 6: KERNEL<3, false><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;  \
-            case 7: KERNEL<3, true><<<BLOCKS, kSplatBlock, 0, STREAM>>>(PARAMS); break;   \
-            default: return cudaErrorInvalidValue;                                        \
-        }                                                                                 \
-    } while (0)
+// Launches KERNEL<DEG, BF16> with `smem` bytes of dynamic shared memory
+// (raising the kernel's limit first when that is above the default 48 KB).
+template <class K, class P>
+cudaError_t launch_with_smem(K kernel, int blocks, size_t smem, cudaStream_t s, const P &p) {
+    if (smem > (size_t)48 * 1024) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    kernel<<<blocks, kSplatBlock, smem, s>>>(p);
+    return cudaGetLastError();
+}
+
+#define BV_SPLAT_SELECT(KERNEL, PARAMS, DEGREE, BF, BLOCKS, SMEM, STREAM)                 \
+    switch ((int)(DEGREE) * 2 + ((BF) ? 1 : 0)) {                                         \
+        case 0: return launch_with_smem(KERNEL<0, false>, BLOCKS, SMEM, STREAM, PARAMS);  \
+        case 1: return launch_with_smem(KERNEL<0, true>, BLOCKS, SMEM, STREAM, PARAMS);   \
+        case 2: return launch_with_smem(KERNEL<1, false>, BLOCKS, SMEM, STREAM, PARAMS);  \
+        case 3: return launch_with_smem(KERNEL<1, true>, BLOCKS, SMEM, STREAM, PARAMS);   \
+        case 4: return launch_with_smem(KERNEL<2, false>, BLOCKS, SMEM, STREAM, PARAMS);  \
+        case 5: return launch_with_smem(KERNEL<2, true>, BLOCKS, SMEM, STREAM, PARAMS);   \
+        case 6: return launch_with_smem(KERNEL<3, false>, BLOCKS, SMEM, STREAM, PARAMS);  \
+        case 7: return launch_with_smem(KERNEL<3, true>, BLOCKS, SMEM, STREAM, PARAMS);   \
+        default: return cudaErrorInvalidValue;                                            \
+    }
 
 cudaError_t launch_splat_train(const SplatTrainParams &p, bool backward, cudaStream_t s) {
     const int blocks = (int)((p.base.total_work + kSplatBlock - 1) / kSplatBlock);
     if (blocks == 0) return cudaSuccess;
-    if (backward)
+    const size_t smem = splat_window_bytes(4);
+    if (backward) {
         BV_SPLAT_SELECT(splat_train_backward_kernel, p, p.base.m.sh_degree, p.base.m.sh_bf16,
-                        blocks, s);
-    else
-        BV_SPLAT_SELECT(splat_train_forward_kernel, p, p.base.m.sh_degree, p.base.m.sh_bf16,
-                        blocks, s);
-    return cudaGetLastError();
+                        blocks, smem, s);
+    }
+    BV_SPLAT_SELECT(splat_train_forward_kernel, p, p.base.m.sh_degree, p.base.m.sh_bf16, blocks,
+                    smem, s);
 }
 
 // Heaviest-first tile order from the forward's tile durations: tiles go to
@@ -1148,19 +1167,7 @@ struct TileScheduler {
 cudaError_t launch_splat(const SplatParams &p, cudaStream_t s) {
     const int blocks = (int)((p.total_work + kSplatBlock - 1) / kSplatBlock);
     if (blocks == 0) return cudaSuccess;
-    const int key = (int)p.m.sh_degree * 2 + (p.m.sh_bf16 ? 1 : 0);
-    switch (key) {
-        case 0: splat_kernel<0, false><<<blocks, kSplatBlock, 0, s>>>(p); break;
-        case 1: splat_kernel<0, true><<<blocks, kSplatBlock, 0, s>>>(p); break;
-        case 2: splat_kernel<1, false><<<blocks, kSplatBlock, 0, s>>>(p); break;
-        case 3: splat_kernel<1, true><<<blocks, kSplatBlock, 0, s>>>(p); break;
-        case 4: splat_kernel<2, false><<<blocks, kSplatBlock, 0, s>>>(p); break;
-        case 5: splat_kernel<2, true><<<blocks, kSplatBlock, 0, s>>>(p); break;
-        case 6: splat_kernel<3, false><<<blocks, kSplatBlock, 0, s>>>(p); break;
-        case 7: splat_kernel<3, true><<<blocks, kSplatBlock, 0, s>>>(p); break;
-        default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+    BV_SPLAT_SELECT(splat_kernel, p, p.m.sh_degree, p.m.sh_bf16, blocks, splat_window_bytes(3), s);
 }
 
 // ---------------------------------------------------------------------------
