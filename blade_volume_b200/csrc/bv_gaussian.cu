@@ -28,6 +28,7 @@
 
 #include "bv_device.cuh"
 #include "bv_internal.h"
+#include "bv_tile_order.cuh"
 #include "bv_window.cuh"
 
 namespace bv {
@@ -35,6 +36,11 @@ namespace {
 
 constexpr int kGaussBlock = 128;
 // resident blocks per SM requested from the register allocator
+// Tiles heaviest first by the previous dispatch's tile times (1) or in
+// launch order (0).
+#ifndef BV_GAUSS_TILE_ORDER
+#define BV_GAUSS_TILE_ORDER 1
+#endif
 #ifndef BV_MINB_GAUSS
 #define BV_MINB_GAUSS 4
 #endif
@@ -69,6 +75,8 @@ struct GaussianParams {
     float tan_half[2];
     float principal[2];
     uint32_t width, height, tiles_x, total_work;
+    const uint32_t *tile_order;  // [tiles] tile of warp slot i, or null (bv_tile_order.cuh)
+    uint32_t *tile_cost;         // [tiles] each tile's duration, or null
     float min_opacity, min_transmittance;
     float background[3];
 };
@@ -142,8 +150,10 @@ template <int DEG>
 __global__ void __launch_bounds__(kGaussBlock, BV_MINB_GAUSS) gaussian_kernel(const __grid_constant__ GaussianParams P) {
     // whole warps past the last tile leave together; lanes of a partial edge
     // tile stay (inactive) because the traversal is warp-cooperative
-    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-    if ((w & ~31u) >= P.total_work) return;
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((slot & ~31u) >= P.total_work) return;
+    const long long clock_begin = clock64();
+    const uint32_t w = tile_item(P.tile_order, slot);
     const uint32_t tile = w / 32u, in = w % 32u;
     const uint32_t x = (tile % P.tiles_x) * 8u + in % 8u;
     const uint32_t y = (tile / P.tiles_x) * 4u + in / 8u;
@@ -227,15 +237,17 @@ __global__ void __launch_bounds__(kGaussBlock, BV_MINB_GAUSS) gaussian_kernel(co
             cur_idx = buf[kWindow - 1].idx;
         }
     }
-    if (!active) return;
-    const size_t o = (size_t)y * P.width + x;
-    P.out[o] = make_float4(rad_r + T * P.background[0], rad_g + T * P.background[1],
-                           rad_b + T * P.background[2], 1.0f - T);
-    if (P.stats) {
-        atomicAdd(P.stats + 0, 1ull);
-        atomicAdd(P.stats + 1, (unsigned long long)hits_used);
-        atomicAdd(P.stats + 2, (unsigned long long)nodes_visited);
+    if (active) {
+        const size_t o = (size_t)y * P.width + x;
+        P.out[o] = make_float4(rad_r + T * P.background[0], rad_g + T * P.background[1],
+                               rad_b + T * P.background[2], 1.0f - T);
+        if (P.stats) {
+            atomicAdd(P.stats + 0, 1ull);
+            atomicAdd(P.stats + 1, (unsigned long long)hits_used);
+            atomicAdd(P.stats + 2, (unsigned long long)nodes_visited);
+        }
     }
+    store_tile_cost(P.tile_cost, w, clock_begin);
 }
 
 // The camera-origin terms of every particle for one view, with the
@@ -296,6 +308,7 @@ struct bv_gaussian_tracer {
     unsigned long long *stats = nullptr;
     bool stats_enabled = false, last_has_stats = false;
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    TileScheduler tile_sched;  // heaviest-first tile order between dispatches
     // The per-view origin table is rewritten by every dispatch: a dispatch on
     // another stream than the previous one first waits for the previous one.
     cudaEvent_t done = nullptr;
@@ -315,6 +328,7 @@ void free_gaussian(bv_gaussian_tracer *t) {
     if (!t) return;
     cudaFree(t->prims);
     cudaFree(t->local);
+    t->tile_sched.release();
     cudaFree(t->ids);
     cudaFree(t->nodes);
     cudaFree(t->sh);
@@ -553,7 +567,15 @@ bv_status bv_gaussian_tracer_dispatch(bv_gaussian_tracer *t, float *out_rgba_dev
     if (t->dispatched && t->last_stream != s && cudaStreamWaitEvent(s, t->done, 0) != cudaSuccess)
         return gfail(BV_ERR_CUDA, "stream wait on the previous dispatch failed");
     uint32_t launches = 0;
+    const size_t tiles = work / 32u;
+    const bool time_tiles =
+        t->tile_sched.begin(BV_GAUSS_TILE_ORDER, tiles, 1, width, height, p.tile_order);
+    p.tile_cost = time_tiles ? t->tile_sched.cost : nullptr;
     cudaError_t e = launch_gaussian(p, t->n_kept, t->sh_degree, s, launches);
+    if (e == cudaSuccess && time_tiles) {
+        e = t->tile_sched.end(tiles, 1, width, height, s);
+        launches += 2;
+    }
     if (e != cudaSuccess) {
         set_last_error(cudaGetErrorString(e));
         return BV_ERR_CUDA;

@@ -19,6 +19,7 @@
 
 #include "bv_device.cuh"
 #include "bv_relight.h"
+#include "bv_tile_order.cuh"
 #include "bv_window.cuh"
 
 namespace bv {
@@ -147,8 +148,10 @@ __global__ void BV_RELIGHT_BOUNDS
 relight_kernel(const __grid_constant__ RelightParams P) {
     // whole warps past the last tile leave together; lanes of a partial edge
     // tile stay (inactive) because the traversal is warp-cooperative
-    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-    if ((w & ~31u) >= P.total_work) return;
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((slot & ~31u) >= P.total_work) return;
+    const long long clock_begin = clock64();
+    const uint32_t w = tile_item(P.tile_order, slot);
     const uint32_t tile = w / 32u, in = w % 32u;
     const uint32_t x = (tile % P.tiles_x) * 8u + in % 8u;
     const uint32_t y = (tile / P.tiles_x) * 4u + in / 8u;
@@ -290,15 +293,17 @@ relight_kernel(const __grid_constant__ RelightParams P) {
         rad_b += T * (alpha * sc_b / wmax);
         T *= 1.0f - alpha;
     }
-    if (!active) return;
-    const size_t o = (size_t)y * P.width + x;
-    P.out[o] = make_float4(rad_r + T * P.background[0], rad_g + T * P.background[1],
-                           rad_b + T * P.background[2], 1.0f - T);
-    if (P.stats) {
-        atomicAdd(P.stats + 0, 1ull);
-        atomicAdd(P.stats + 1, (unsigned long long)hits_used);
-        atomicAdd(P.stats + 2, (unsigned long long)nodes_visited);
+    if (active) {
+        const size_t o = (size_t)y * P.width + x;
+        P.out[o] = make_float4(rad_r + T * P.background[0], rad_g + T * P.background[1],
+                               rad_b + T * P.background[2], 1.0f - T);
+        if (P.stats) {
+            atomicAdd(P.stats + 0, 1ull);
+            atomicAdd(P.stats + 1, (unsigned long long)hits_used);
+            atomicAdd(P.stats + 2, (unsigned long long)nodes_visited);
+        }
     }
+    store_tile_cost(P.tile_cost, w, clock_begin);
 }
 
 // The camera-origin terms of every particle for one view, with the

@@ -56,6 +56,8 @@ struct RelightParams {
     float tan_half[2];
     float principal[2];
     uint32_t width, height, tiles_x, total_work;
+    const uint32_t *tile_order;  // [tiles] tile of warp slot i, or null (bv_tile_order.cuh)
+    uint32_t *tile_cost;         // [tiles] each tile's duration, or null
     float background[3];
     uint32_t n_lights;
     RelightLight lights[kMaxRelightLights];

@@ -12,6 +12,13 @@
 
 #include "bv_internal.h"
 #include "bv_relight.h"
+#include "bv_tile_order.cuh"
+
+// Relight tiles heaviest first by the previous dispatch's tile times (1) or
+// in launch order (0).
+#ifndef BV_RELIGHT_TILE_ORDER
+#define BV_RELIGHT_TILE_ORDER 1
+#endif
 
 using namespace bv;
 
@@ -36,6 +43,7 @@ struct bv_relight_tracer {
     cudaStream_t last_stream = nullptr;
     bool dispatched = false;
     uint32_t last_launches = 0;
+    TileScheduler tile_sched;  // heaviest-first tile order between dispatches
 };
 
 namespace {
@@ -49,6 +57,7 @@ void free_relight(bv_relight_tracer *t) {
     if (!t) return;
     cudaFree(t->prims);
     cudaFree(t->local);
+    t->tile_sched.release();
     cudaFree(t->nodes);
     cudaFree(t->materials);
     cudaFree(t->stats);
@@ -298,7 +307,15 @@ bv_status bv_relight_tracer_dispatch(bv_relight_tracer *t, float *out_rgba_dev,
     if (t->dispatched && t->last_stream != s && cudaStreamWaitEvent(s, t->done, 0) != cudaSuccess)
         return rfail(BV_ERR_CUDA, "stream wait on the previous dispatch failed");
     uint32_t launches = 0;
+    const size_t tiles = work / 32u;
+    const bool time_tiles =
+        t->tile_sched.begin(BV_RELIGHT_TILE_ORDER, tiles, 1, width, height, p.tile_order);
+    p.tile_cost = time_tiles ? t->tile_sched.cost : nullptr;
     cudaError_t e = launch_relight(p, s, launches);
+    if (e == cudaSuccess && time_tiles) {
+        e = t->tile_sched.end(tiles, 1, width, height, s);
+        launches += 2;
+    }
     if (e != cudaSuccess) {
         set_last_error(cudaGetErrorString(e));
         return BV_ERR_CUDA;

@@ -166,9 +166,19 @@ struct Scene {
     size_t bytes = 0;
 };
 
+// A frame on its way to the host: its copy's event (the frame has landed
+// when it completes).
+struct Landing {
+    cudaEvent_t copied = nullptr;
+    Request *q = nullptr;
+    uint32_t view = 0;
+};
+
+// A batch slot: free again once its traversal is done (its frames' copies
+// run on, tracked as Landings, while the slot's next batch computes).
 struct Slot {
     cudaStream_t compute = nullptr, copy = nullptr;
-    cudaEvent_t done = nullptr, copied = nullptr;
+    cudaEvent_t done = nullptr;
     void *host_table = nullptr;  // pinned: ServeHeader + ServeView[max_views]
     void *dev_table = nullptr;
     uint32_t *counter = nullptr;
@@ -195,6 +205,8 @@ struct bv_server {
     uint32_t *step_rec = nullptr;  // training step record lent to every scene's tracer
     size_t resident = 0;
     std::vector<Slot> slots;
+    std::deque<Landing> landings;           // frame copies in flight
+    std::vector<cudaEvent_t> spare_events;  // their events, for reuse
     cudaStream_t train_stream = nullptr;
     ServeParams params{};
     int walk_grid = 0;
@@ -356,14 +368,30 @@ bv_status launch_batch(bv_server *sv, Slot &sl) {
     sv->wst.batches += 1;
     SV_CUDA(cudaEventRecord(sl.done, sl.compute), "event");
     SV_CUDA(cudaStreamWaitEvent(sl.copy, sl.done, 0), "stream wait");
+    // each frame lands on its own: one copy and one event per frame
     for (auto &f : sl.frames) {
         Request *q = f.first;
         const size_t px = (size_t)q->r.width * q->r.height;
         SV_CUDA(cudaMemcpyAsync(q->r.out_host + 4 * px * f.second, q->out_dev + px * f.second,
                                 px * sizeof(float4), cudaMemcpyDeviceToHost, sl.copy),
                 "frame copy");
+        Landing ld;
+        if (!sv->spare_events.empty()) {
+            ld.copied = sv->spare_events.back();
+            sv->spare_events.pop_back();
+        } else {
+            SV_CUDA(cudaEventCreateWithFlags(&ld.copied, cudaEventDisableTiming), "event");
+        }
+        ld.q = q;
+        ld.view = f.second;
+        const cudaError_t e = cudaEventRecord(ld.copied, sl.copy);
+        if (e != cudaSuccess) {
+            sv->spare_events.push_back(ld.copied);
+            return scuda(e, "event");
+        }
+        sv->landings.push_back(ld);
     }
-    SV_CUDA(cudaEventRecord(sl.copied, sl.copy), "event");
+    sl.frames.clear();
     sl.busy = true;
     return BV_OK;
 }
@@ -390,6 +418,8 @@ void fail_all(bv_server *sv, const std::string &why) {
         sl.busy = false;
         sl.frames.clear();
     }
+    for (auto &ld : sv->landings) sv->spare_events.push_back(ld.copied);
+    sv->landings.clear();
 }
 
 // Plain modes: the oldest request alone through the tracer calls, then a
@@ -457,24 +487,37 @@ void scheduler(bv_server *sv) {
             if (q->frames_left == 0) finish_request(sv, q, sv->now());
             progress = true;
         }
-        // 1. retire
+        // 1. retire: slots whose traversal is done, frames that landed
+        bool failed = false;
         for (auto &sl : sv->slots) {
             if (!sl.busy) continue;
-            const cudaError_t e = cudaEventQuery(sl.copied);
+            const cudaError_t e = cudaEventQuery(sl.done);
             if (e == cudaErrorNotReady) continue;
             if (e != cudaSuccess) {
                 fail_all(sv, std::string("batch: ") + cudaGetErrorString(e));
+                failed = true;
+                break;
+            }
+            sl.busy = false;
+            progress = true;
+        }
+        for (auto it = sv->landings.begin(); !failed && it != sv->landings.end();) {
+            const cudaError_t e = cudaEventQuery(it->copied);
+            if (e == cudaErrorNotReady) {
+                ++it;
+                continue;
+            }
+            if (e != cudaSuccess) {
+                fail_all(sv, std::string("frame copy: ") + cudaGetErrorString(e));
                 break;
             }
             const double t = sv->now();
-            for (auto &f : sl.frames) {
-                Request *q = f.first;
-                if (q->r.frame_done_host) q->r.frame_done_host[f.second] = t;
-                sv->wst.frames_done += 1;
-                if (--q->frames_left == 0) finish_request(sv, q, t);
-            }
-            sl.frames.clear();
-            sl.busy = false;
+            Request *q = it->q;
+            if (q->r.frame_done_host) q->r.frame_done_host[it->view] = t;
+            sv->wst.frames_done += 1;
+            if (--q->frames_left == 0) finish_request(sv, q, t);
+            sv->spare_events.push_back(it->copied);
+            it = sv->landings.erase(it);
             progress = true;
         }
         while (!sv->train_inflight.empty()) {
@@ -498,6 +541,7 @@ void scheduler(bv_server *sv) {
         {
             std::unique_lock<std::mutex> lk(sv->mu);
             const bool idle = sv->frames.empty() && sv->train_inflight.empty() &&
+                              sv->landings.empty() &&
                               std::none_of(sv->slots.begin(), sv->slots.end(),
                                            [](const Slot &s) { return s.busy; });
             if (idle && busy_since >= 0) {
@@ -584,12 +628,13 @@ void scheduler(bv_server *sv) {
 }
 
 void free_server(bv_server *sv) {
+    for (auto &ld : sv->landings) cudaEventDestroy(ld.copied);
+    for (cudaEvent_t e : sv->spare_events) cudaEventDestroy(e);
     for (auto &sl : sv->slots) {
         if (sl.exec) cudaGraphExecDestroy(sl.exec);
         if (sl.compute) cudaStreamDestroy(sl.compute);
         if (sl.copy) cudaStreamDestroy(sl.copy);
         if (sl.done) cudaEventDestroy(sl.done);
-        if (sl.copied) cudaEventDestroy(sl.copied);
         if (sl.host_table) cudaFreeHost(sl.host_table);
         cudaFree(sl.dev_table);
         cudaFree(sl.counter);
@@ -744,7 +789,6 @@ bv_status bv_server_start(bv_server *sv) {
         SV_CUDA(cudaStreamCreateWithPriority(&sl.compute, cudaStreamNonBlocking, prio_high), "stream");
         SV_CUDA(cudaStreamCreateWithPriority(&sl.copy, cudaStreamNonBlocking, prio_high), "stream");
         SV_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), "event");
-        SV_CUDA(cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming), "event");
         SV_CUDA(cudaHostAlloc(&sl.host_table, sv->table_bytes, cudaHostAllocDefault), "pinned table");
         std::memset(sl.host_table, 0, sv->table_bytes);
         SV_CUDA(cudaMalloc(&sl.dev_table, sv->table_bytes), "batch table");

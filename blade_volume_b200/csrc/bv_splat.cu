@@ -31,6 +31,7 @@
 #include "bv_device.cuh"
 #include "bv_internal.h"
 #include "bv_segment.cuh"
+#include "bv_tile_order.cuh"
 #include "bv_window.cuh"
 
 namespace bv {
@@ -165,21 +166,6 @@ struct SplatParams {
     ViewDesc views[kMaxViewsPerLaunch];
 };
 
-// The work item of thread `slot`: its warp slot's tile (tile_order, a
-// permutation of the launch's tiles, or the slot itself) and its lane.
-// Every per-ray and per-tile index (pixel, ray state, interval record)
-// follows from it, so the order tiles are taken in changes no result.
-__device__ __forceinline__ uint32_t splat_item(const uint32_t *order, uint32_t slot) {
-    return order ? (__ldg(order + (slot >> 5)) << 5) | (slot & 31u) : slot;
-}
-
-// Lane 0 of a warp stores its tile's duration since `begin` (clock64).
-__device__ __forceinline__ void store_tile_cost(uint32_t *cost, uint32_t w, long long begin) {
-    if (cost && (threadIdx.x & 31u) == 0) {
-        const unsigned long long d = (unsigned long long)(clock64() - begin) >> 6;
-        cost[w >> 5] = d > 0xffffffffull ? 0xffffffffu : (uint32_t)d;
-    }
-}
 
 // Slab test for the counting pass (per-lane traversal).
 __device__ __forceinline__ bool slab(const float4 &lo, const float4 &hi, const WinRay &r, float t_end,
@@ -450,7 +436,7 @@ splat_kernel(const __grid_constant__ SplatParams P) {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if ((slot & ~31u) >= P.total_work) return;
     const long long clock_begin = clock64();
-    const uint32_t w = splat_item(P.tile_order, slot);
+    const uint32_t w = tile_item(P.tile_order, slot);
     const SplatLane L = splat_lane(P, w);
     const WinRay &ray = L.ray;
     const bool active = L.active;
@@ -672,7 +658,7 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if ((slot & ~31u) >= P.total_work) return;
     const long long clock_begin = clock64();
-    const uint32_t w = splat_item(P.tile_order, slot);
+    const uint32_t w = tile_item(P.tile_order, slot);
     const SplatLane L = splat_lane(P, w);
     const WinRay &ray = L.ray;
     const float depth = L.vd->depth;
@@ -927,7 +913,7 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
     constexpr int K = ShDims<DEG>::K;
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if ((slot & ~31u) >= P.total_work) return;
-    const uint32_t w = splat_item(P.tile_order, slot);
+    const uint32_t w = tile_item(P.tile_order, slot);
     const SplatLane L = splat_lane(P, w);
     const WinRay &ray = L.ray;
     const float depth = L.vd->depth;
@@ -1061,108 +1047,6 @@ cudaError_t launch_splat_train(const SplatTrainParams &p, bool backward, cudaStr
     BV_SPLAT_SELECT(splat_train_forward_kernel, p, p.base.m.sh_degree, p.base.m.sh_bf16, blocks,
                     smem, s);
 }
-
-// Heaviest-first tile order from the forward's tile durations: tiles go to
-// 32 classes by floor(log2(cost)) and the classes are laid out from the
-// heaviest down (the order inside a class is whatever the atomics give).
-// counts[0..31] per class, counts[32..63] the classes' fill cursors, both
-// zero on entry.
-constexpr int kOrderClasses = 32;
-
-__device__ __forceinline__ uint32_t order_class(uint32_t cost) {
-    return 31u - (uint32_t)__clz(cost | 1u);
-}
-
-__global__ void tile_cost_histogram_kernel(const uint32_t *__restrict__ cost, uint32_t tiles,
-                                           uint32_t *__restrict__ counts) {
-    __shared__ uint32_t h[kOrderClasses];
-    if (threadIdx.x < kOrderClasses) h[threadIdx.x] = 0;
-    __syncthreads();
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < tiles; i += gridDim.x * blockDim.x)
-        atomicAdd(&h[order_class(cost[i])], 1u);
-    __syncthreads();
-    if (threadIdx.x < kOrderClasses && h[threadIdx.x]) atomicAdd(&counts[threadIdx.x], h[threadIdx.x]);
-}
-
-__global__ void tile_order_scatter_kernel(const uint32_t *__restrict__ cost, uint32_t tiles,
-                                          uint32_t *__restrict__ counts,
-                                          uint32_t *__restrict__ order) {
-    __shared__ uint32_t start[kOrderClasses];
-    if (threadIdx.x == 0) {
-        uint32_t acc = 0;
-        for (int c = kOrderClasses - 1; c >= 0; --c) {
-            start[c] = acc;
-            acc += counts[c];
-        }
-    }
-    __syncthreads();
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < tiles; i += gridDim.x * blockDim.x) {
-        const uint32_t c = order_class(cost[i]);
-        order[start[c] + atomicAdd(&counts[kOrderClasses + c], 1u)] = i;
-    }
-}
-
-cudaError_t launch_tile_order(const uint32_t *cost, uint32_t tiles, uint32_t *counts,
-                              uint32_t *order, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(counts, 0, 2 * kOrderClasses * sizeof(uint32_t), s);
-    if (e != cudaSuccess) return e;
-    const int blocks = (int)std::min<uint32_t>(296u, (tiles + 255u) / 256u);
-    tile_cost_histogram_kernel<<<blocks, 256, 0, s>>>(cost, tiles, counts);
-    tile_order_scatter_kernel<<<blocks, 256, 0, s>>>(cost, tiles, counts, order);
-    return cudaGetLastError();
-}
-
-// Heaviest-first scheduling of one kind of launch (render or training)
-// from frame to frame: a launch times its tiles into `cost`, the order is
-// built from those times after it, and the next launch of the same shape
-// (views, width, height: the same tiles) takes its tiles in that order.
-// Frames of a moving camera keep most of their heavy tiles where they were;
-// the order changes no result, only when each tile starts.
-struct TileScheduler {
-    uint32_t *cost = nullptr, *order = nullptr, *counts = nullptr;
-    size_t capacity = 0;
-    uint32_t views = 0, width = 0, height = 0;
-    bool valid = false;
-
-    void release() {
-        cudaFree(cost);
-        cudaFree(order);
-        cudaFree(counts);
-        cost = order = counts = nullptr;
-        capacity = 0;
-        valid = false;
-    }
-    // Before a launch of `tiles` tiles: whether it times them (buffers to
-    // hand) and the order to take them in (null: launch order).
-    bool begin(size_t tiles, uint32_t n_views, uint32_t w, uint32_t h, const uint32_t *&use) {
-        use = nullptr;
-        if (!BV_SPLAT_TILE_ORDER || n_views > (uint32_t)kMaxViewsPerLaunch) return false;
-        if (tiles > capacity) {
-            release();
-            if (cudaMalloc(&counts, 2 * kOrderClasses * sizeof(uint32_t)) != cudaSuccess ||
-                cudaMalloc(&cost, tiles * sizeof(uint32_t)) != cudaSuccess ||
-                cudaMalloc(&order, tiles * sizeof(uint32_t)) != cudaSuccess) {
-                (void)cudaGetLastError();  // no room: launch order
-                release();
-                return false;
-            }
-            capacity = tiles;
-        }
-        if (valid && views == n_views && width == w && height == h) use = order;
-        valid = false;
-        return true;
-    }
-    // After the launch (same stream): the order for the next one.
-    cudaError_t end(size_t tiles, uint32_t n_views, uint32_t w, uint32_t h, cudaStream_t s) {
-        const cudaError_t e = launch_tile_order(cost, (uint32_t)tiles, counts, order, s);
-        if (e != cudaSuccess) return e;
-        views = n_views;
-        width = w;
-        height = h;
-        valid = true;
-        return cudaSuccess;
-    }
-};
 
 cudaError_t launch_splat(const SplatParams &p, cudaStream_t s) {
     const int blocks = (int)((p.total_work + kSplatBlock - 1) / kSplatBlock);
@@ -1381,7 +1265,7 @@ bv_status enqueue_splats(bv_splat_tracer *t, float4 *out, const bv_camera *cams,
         const size_t tiles = work / 32u;
         bool time_tiles = false;
         if (!count_only && n <= (uint32_t)kMaxViewsPerLaunch)
-            time_tiles = t->render_order.begin(tiles, nc, w, h, p.tile_order);
+            time_tiles = t->render_order.begin(BV_SPLAT_TILE_ORDER, tiles, nc, w, h, p.tile_order);
         p.tile_cost = time_tiles ? t->render_order.cost : nullptr;
         SP_CUDA(launch_splat(p, s), "splat launch");
         t->last_launches += 1;
@@ -1758,7 +1642,7 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
     // heaviest-first tile order (calls of one launch): the forward times its
     // tiles, the order is built from those times after the backward
     const uint32_t *order = nullptr;
-    const bool time_tiles = t->train_order.begin(tiles, n_cams, width, height, order);
+    const bool time_tiles = t->train_order.begin(BV_SPLAT_TILE_ORDER, tiles, n_cams, width, height, order);
     t->last_launches = 0;
     t->last_has_stats = t->stats_enabled;
     if (t->stats_enabled) {

@@ -341,10 +341,13 @@ bv_status bv_relight_tracer_set_point_lights(bv_relight_tracer *tracer,
 bv_status bv_relight_tracer_set_background(bv_relight_tracer *tracer, const float rgb[3]);
 /* Renders width x height into out_rgba_dev ([h][w][4] float32): radiance +
  * transmittance * background, alpha = 1 - transmittance (relight.wgsl:747-780).
- * Two launches: each particle's camera-origin terms into the tracer's
- * per-view table, then the trace.  Because that table is rewritten by each
- * dispatch, a dispatch on a different stream than the tracer's previous one
- * is ordered after it (an event wait), so dispatches never overlap. */
+ * Four launches: each particle's camera-origin terms into the tracer's
+ * per-view table, the trace (its 8x4 tiles heaviest first by the previous
+ * dispatch's tile times when that had the same size; the order changes no
+ * result), and two small ones that order the tiles for the next dispatch.
+ * Because the tables are rewritten by each dispatch, a dispatch on a
+ * different stream than the tracer's previous one is ordered after it (an
+ * event wait), so dispatches never overlap. */
 bv_status bv_relight_tracer_dispatch(bv_relight_tracer *tracer, float *out_rgba_dev,
                                      const bv_camera *camera, uint32_t width, uint32_t height,
                                      bv_stream stream);
@@ -464,11 +467,14 @@ bv_status bv_gaussian_tracer_set_background(bv_gaussian_tracer *tracer, const fl
 /* particles kept (GaussianGpuCloud::num_points) */
 uint32_t bv_gaussian_tracer_num_points(const bv_gaussian_tracer *tracer);
 /* Renders width x height into out_rgba_dev ([h][w][4] float32):
- * (radiance + T * background, 1 - T).  Two launches: each particle's
- * camera-origin terms into the tracer's per-view table, then the trace.
- * Because that table is rewritten by each dispatch, a dispatch on a
- * different stream than the tracer's previous one is ordered after it (an
- * event wait), so dispatches never overlap. */
+ * (radiance + T * background, 1 - T).  Four launches: each particle's
+ * camera-origin terms into the tracer's per-view table, the trace (its 8x4
+ * tiles heaviest first by the previous dispatch's tile times when that had
+ * the same size; the order changes no result), and two small ones that
+ * order the tiles for the next dispatch.  Because the tables are rewritten
+ * by each dispatch, a dispatch on a different stream than the tracer's
+ * previous one is ordered after it (an event wait), so dispatches never
+ * overlap. */
 bv_status bv_gaussian_tracer_dispatch(bv_gaussian_tracer *tracer, float *out_rgba_dev,
                                       const bv_camera *camera, uint32_t width, uint32_t height,
                                       bv_stream stream);
