@@ -167,18 +167,23 @@ struct Scene {
 };
 
 // A frame on its way to the host: its copy's event (the frame has landed
-// when it completes).
+// when it completes) and the batch slot it came from.
 struct Landing {
     cudaEvent_t copied = nullptr;
     Request *q = nullptr;
     uint32_t view = 0;
+    uint32_t slot = 0;
 };
 
-// A batch slot: free again once its traversal is done (its frames' copies
-// run on, tracked as Landings, while the slot's next batch computes).
+// A batch slot: busy until its traversal is done and every frame of its
+// batch has landed.  (Freeing it when the traversal ends, with the copies
+// still running, lets batches be formed earlier from fewer queued frames:
+// measured worse for frame latency under load, 44 vs 27 ms p99 at 50 req/s.)
 struct Slot {
     cudaStream_t compute = nullptr, copy = nullptr;
     cudaEvent_t done = nullptr;
+    bool computing = false;
+    uint32_t copies = 0;  // frames of the batch not yet landed
     void *host_table = nullptr;  // pinned: ServeHeader + ServeView[max_views]
     void *dev_table = nullptr;
     uint32_t *counter = nullptr;
@@ -384,15 +389,18 @@ bv_status launch_batch(bv_server *sv, Slot &sl) {
         }
         ld.q = q;
         ld.view = f.second;
+        ld.slot = (uint32_t)(&sl - sv->slots.data());
         const cudaError_t e = cudaEventRecord(ld.copied, sl.copy);
         if (e != cudaSuccess) {
             sv->spare_events.push_back(ld.copied);
             return scuda(e, "event");
         }
         sv->landings.push_back(ld);
+        sl.copies += 1;
     }
     sl.frames.clear();
     sl.busy = true;
+    sl.computing = true;
     return BV_OK;
 }
 
@@ -415,7 +423,8 @@ void fail_all(bv_server *sv, const std::string &why) {
     sv->frames.clear();
     sv->train_inflight.clear();
     for (auto &sl : sv->slots) {
-        sl.busy = false;
+        sl.busy = sl.computing = false;
+        sl.copies = 0;
         sl.frames.clear();
     }
     for (auto &ld : sv->landings) sv->spare_events.push_back(ld.copied);
@@ -487,10 +496,11 @@ void scheduler(bv_server *sv) {
             if (q->frames_left == 0) finish_request(sv, q, sv->now());
             progress = true;
         }
-        // 1. retire: slots whose traversal is done, frames that landed
+        // 1. retire: traversals that are done, frames that landed, slots
+        // with both
         bool failed = false;
         for (auto &sl : sv->slots) {
-            if (!sl.busy) continue;
+            if (!sl.computing) continue;
             const cudaError_t e = cudaEventQuery(sl.done);
             if (e == cudaErrorNotReady) continue;
             if (e != cudaSuccess) {
@@ -498,7 +508,7 @@ void scheduler(bv_server *sv) {
                 failed = true;
                 break;
             }
-            sl.busy = false;
+            sl.computing = false;
             progress = true;
         }
         for (auto it = sv->landings.begin(); !failed && it != sv->landings.end();) {
@@ -516,10 +526,13 @@ void scheduler(bv_server *sv) {
             if (q->r.frame_done_host) q->r.frame_done_host[it->view] = t;
             sv->wst.frames_done += 1;
             if (--q->frames_left == 0) finish_request(sv, q, t);
+            sv->slots[it->slot].copies -= 1;
             sv->spare_events.push_back(it->copied);
             it = sv->landings.erase(it);
             progress = true;
         }
+        for (auto &sl : sv->slots)
+            if (sl.busy && !sl.computing && sl.copies == 0) sl.busy = false;
         while (!sv->train_inflight.empty()) {
             Request *q = sv->train_inflight.front();
             const cudaError_t e = cudaEventQuery(q->ev);
