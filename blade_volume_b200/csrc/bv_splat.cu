@@ -8,9 +8,9 @@
 // sorted_powerfoam_splat_intervals :1391-1411, trace_powerfoam_splats
 // :1456-1546 (the reference's GPU path, gpu/powerfoam_splat.rs:51-343,
 // records bounded candidate rows and sorts them).  Here a BVH over the
-// support spheres is walked front to back in windows of kSplatWindow
-// intervals: a pass keeps the kSplatWindow smallest (t, cell) keys above the
-// cursor, pruning boxes and spheres that end at or before the cursor or
+// support spheres is walked front to back in windows of W intervals (32
+// for the render, 20 for training): a pass keeps the W smallest (t, cell)
+// keys above the cursor, pruning boxes and spheres that end at or before the cursor or
 // start after the window's last key, so there is no per-ray candidate
 // scratch and no capacity to overflow.  The order equals the full sort, so
 // the image is the oracle's bit for bit (-fmad=false; every expression is
@@ -38,13 +38,20 @@ namespace bv {
 namespace {
 
 // Tuning knobs (measured on B200, 1M-site mixture at 4 x 1024^2): keys per
-// lane per window pass (8 and 12 were slower than 16: more passes over the
-// BVH) and the resident blocks per SM requested for the render kernel (4:
-// 128 registers, 19.4 Mrays/s; without the bound 162 registers, 16.3).  The
-// training kernels keep the allocator's choice (capping them at 128
-// registers spills and is no faster).
+// lane per window pass, for the render (12-byte keys) and for training
+// (16-byte keys with the interval's plane offsets).  A larger window means
+// fewer passes over the BVH and fewer supports clipped again in the next
+// pass, most of all for the heavy tiles, against fewer resident blocks:
+// render 16 / 24 / 28 / 32 keys 47.7 / 55.7 / 58.0 / 59.6 Mrays/s; training
+// 16 / 20 / 24 / 28 / 32 keys 51.0 / 54.3 / 48.9 / 40.4 / 41.6 (20 keys
+// still fit 5 blocks per SM, 24 and more only 4 or 3).  And the resident
+// blocks per SM requested for the render kernel (4: 128 registers, 19.4
+// Mrays/s; without the bound 162 registers, 16.3).
 #ifndef BV_SPLAT_WINDOW
-#define BV_SPLAT_WINDOW 16
+#define BV_SPLAT_WINDOW 32
+#endif
+#ifndef BV_SPLAT_TRAIN_WINDOW
+#define BV_SPLAT_TRAIN_WINDOW 20
 #endif
 #ifndef BV_MINB_SPLAT
 #define BV_MINB_SPLAT 4
@@ -91,36 +98,39 @@ namespace {
 #define BV_SPLAT_TILE_ORDER 1
 #endif
 constexpr int kSplatBlock = 128;
-constexpr int kSplatWindow = BV_SPLAT_WINDOW;
+constexpr int kSplatWindow = BV_SPLAT_WINDOW;            // render
+constexpr int kSplatTrainWindow = BV_SPLAT_TRAIN_WINDOW;  // training forward and replay
 constexpr int kSplatStack = 80;  // > BVH depth, checked at tracer creation
 
 // Dynamic shared memory of a splat kernel's window: `fields` words per key
-// (3 for WinKey, 4 for WinKey2), kSplatWindow keys per thread.
-constexpr size_t splat_window_bytes(int fields) {
-    return (BV_SPLAT_SMEM_WINDOW ? (size_t)fields * kSplatWindow * kSplatBlock * 4u : 0u);
+// (3 for WinKey, 4 for WinKey2), `keys` keys per thread.
+constexpr size_t splat_window_bytes(int fields, int keys) {
+    return (BV_SPLAT_SMEM_WINDOW ? (size_t)fields * keys * kSplatBlock * 4u : 0u);
 }
 
-// The window of a splat kernel: SPLAT_WINDOW(Key) declares it (shared memory
-// per thread, or a register array), SPLAT_GATHER runs one pass into it and
-// SPLAT_KEY(i) reads key i.
+// The window of a splat kernel: SPLAT_WINDOW(Key, W) declares it (W keys
+// per thread in shared memory, or a register array), SPLAT_GATHER runs one
+// pass into it and SPLAT_KEY(i) reads key i.
 #if BV_SPLAT_SMEM_WINDOW
 // in dynamic shared memory (splat_window_bytes per block, set at launch), so
 // that windows of more than 20 keys fit: field f of key i of thread tid at
 // word (f W + i) 128 + tid
-#define SPLAT_WINDOW(KEY)                                                                      \
-    extern __shared__ uint32_t s_win_dyn[];                                                   \
-    SmemWindow<kSplatWindow, KEY> win{                                                        \
-        reinterpret_cast<float *>(s_win_dyn) + threadIdx.x,                                   \
-        s_win_dyn + 1 * kSplatWindow * kSplatBlock + threadIdx.x,                             \
-        s_win_dyn + 2 * kSplatWindow * kSplatBlock + threadIdx.x,                             \
-        s_win_dyn + (sizeof(KEY) == sizeof(WinKey2) ? 3 * kSplatWindow * kSplatBlock + threadIdx.x \
-                                                    : 0),                                     \
+#define SPLAT_WINDOW(KEY, W)                                                      \
+    constexpr int kWin = (W);                                                     \
+    extern __shared__ uint32_t s_win_dyn[];                                       \
+    SmemWindow<kWin, KEY> win{                                                    \
+        reinterpret_cast<float *>(s_win_dyn) + threadIdx.x,                       \
+        s_win_dyn + 1 * kWin * kSplatBlock + threadIdx.x,                         \
+        s_win_dyn + 2 * kWin * kSplatBlock + threadIdx.x,                         \
+        s_win_dyn + (sizeof(KEY) == sizeof(WinKey2) ? 3 * kWin * kSplatBlock + threadIdx.x : 0), \
         kSplatBlock}
-#define SPLAT_GATHER(...) win_gather_warp_smem<kSplatWindow, kSplatStack>(__VA_ARGS__, win, nodes_visited, hit)
+#define SPLAT_GATHER(...) win_gather_warp_smem<kWin, kSplatStack>(__VA_ARGS__, win, nodes_visited, hit)
 #define SPLAT_KEY(i) win.get(i)
 #else
-#define SPLAT_WINDOW(KEY) KEY buf[kSplatWindow]
-#define SPLAT_GATHER(...) win_gather_warp<kSplatWindow, kSplatStack>(__VA_ARGS__, buf, nodes_visited, hit)
+#define SPLAT_WINDOW(KEY, W)  \
+    constexpr int kWin = (W); \
+    KEY buf[kWin]
+#define SPLAT_GATHER(...) win_gather_warp<kWin, kSplatStack>(__VA_ARGS__, buf, nodes_visited, hit)
 #define SPLAT_KEY(i) win_at(buf, i)
 #endif
 // Entry / exit plane of an interval as an offset in its Cech row (16 bits
@@ -487,7 +497,7 @@ splat_kernel(const __grid_constant__ SplatParams P) {
     auto hit = [&](uint32_t p, bool mine, float limit, auto &k) -> bool {
         return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, k, clipped);
     };
-    SPLAT_WINDOW(WinKey);
+    SPLAT_WINDOW(WinKey, kSplatWindow);
     for (;;) {
         const bool want = !finished;
         if (!__any_sync(0xffffffffu, want)) break;
@@ -516,10 +526,10 @@ splat_kernel(const __grid_constant__ SplatParams P) {
             T *= 1.0f - alpha;
         }
         if (finished) continue;
-        if (count < kSplatWindow) {
+        if (count < kWin) {
             finished = true;
         } else {
-            const auto last = SPLAT_KEY(kSplatWindow - 1);
+            const auto last = SPLAT_KEY(kWin - 1);
             cursor_valid = true;
             cur_t = last.t;
             cur_cell = last.idx;
@@ -674,7 +684,7 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
     auto hit = [&](uint32_t p, bool mine, float limit, auto &k) -> bool {
         return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, k, clipped);
     };
-    SPLAT_WINDOW(WinKey2);
+    SPLAT_WINDOW(WinKey2, kSplatTrainWindow);
     for (;;) {
         const bool want = !finished;
         if (!__any_sync(0xffffffffu, want)) break;
@@ -716,10 +726,10 @@ splat_train_forward_kernel(const __grid_constant__ SplatTrainParams TP) {
             composited += 1;
         }
         if (finished) continue;
-        if (count < kSplatWindow) {
+        if (count < kWin) {
             finished = true;
         } else {
-            const auto last = SPLAT_KEY(kSplatWindow - 1);
+            const auto last = SPLAT_KEY(kWin - 1);
             cursor_valid = true;
             cur_t = last.t;
             cur_cell = last.idx;
@@ -972,7 +982,7 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
     auto hit = [&](uint32_t p, bool mine, float limit, auto &k) -> bool {
         return splat_hit(P, ray, depth, cursor_valid, cur_t, p, mine, limit, k, clipped);
     };
-    SPLAT_WINDOW(WinKey2);
+    SPLAT_WINDOW(WinKey2, kSplatTrainWindow);
     for (;;) {
         const bool want = !finished;
         if (!__any_sync(0xffffffffu, want)) break;
@@ -999,10 +1009,10 @@ splat_train_backward_kernel(const __grid_constant__ SplatTrainParams TP) {
             scatter_interval<DEG>(TP, Y, cell, G);
         }
         if (finished) continue;
-        if (count < kSplatWindow) {
+        if (count < kWin) {
             finished = true;
         } else {
-            const auto last = SPLAT_KEY(kSplatWindow - 1);
+            const auto last = SPLAT_KEY(kWin - 1);
             cursor_valid = true;
             cur_t = last.t;
             cur_cell = last.idx;
@@ -1040,7 +1050,7 @@ cudaError_t launch_with_smem(K kernel, int blocks, size_t smem, cudaStream_t s, 
 cudaError_t launch_splat_train(const SplatTrainParams &p, bool backward, cudaStream_t s) {
     const int blocks = (int)((p.base.total_work + kSplatBlock - 1) / kSplatBlock);
     if (blocks == 0) return cudaSuccess;
-    const size_t smem = splat_window_bytes(4);
+    const size_t smem = splat_window_bytes(4, kSplatTrainWindow);
     if (backward) {
         BV_SPLAT_SELECT(splat_train_backward_kernel, p, p.base.m.sh_degree, p.base.m.sh_bf16,
                         blocks, smem, s);
@@ -1052,7 +1062,8 @@ cudaError_t launch_splat_train(const SplatTrainParams &p, bool backward, cudaStr
 cudaError_t launch_splat(const SplatParams &p, cudaStream_t s) {
     const int blocks = (int)((p.total_work + kSplatBlock - 1) / kSplatBlock);
     if (blocks == 0) return cudaSuccess;
-    BV_SPLAT_SELECT(splat_kernel, p, p.m.sh_degree, p.m.sh_bf16, blocks, splat_window_bytes(3), s);
+    BV_SPLAT_SELECT(splat_kernel, p, p.m.sh_degree, p.m.sh_bf16, blocks,
+                    splat_window_bytes(3, kSplatWindow), s);
 }
 
 // ---------------------------------------------------------------------------
