@@ -507,7 +507,7 @@ def run_secondary(args):
                              "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
                              "traffic": None, "peak_source": kind,
                              "achieved_is": GATHER_NOTE},
-                "gpu_launches": args.steps, "clocks": clocks}
+                "gpu_launches": max(int(st.launches), 1) * args.steps, "clocks": clocks}
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -688,7 +688,7 @@ def run_powerfoam_train(args):
                          "achieved_is": "compulsory bytes per step / step time",
                          "alg_bytes_per_step": alg, "gather_bytes_per_step": gather,
                          "gather_gbs": gather / (ms * 1e-3) / 1e9},
-            "gpu_launches": 3 * args.steps, "clocks": clocks}
+            "gpu_launches": max(int(st.launches), 1) * args.steps, "clocks": clocks}
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
