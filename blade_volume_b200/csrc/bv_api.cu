@@ -15,6 +15,13 @@
 #include <vector>
 
 #include "bv_internal.h"
+#include "bv_tile_order.cuh"
+
+// Training takes its tiles heaviest first by the previous call's tile times
+// (1) or in launch order (0).
+#ifndef BV_WALK_TILE_ORDER
+#define BV_WALK_TILE_ORDER 1
+#endif
 
 using namespace bv;
 
@@ -116,6 +123,7 @@ struct bv_tracer {
     uint32_t step_rec_steps = kExitRecSteps;  // recorded steps per ray
     bool step_rec_owned = true;        // false: lent by a serving engine
     uint32_t train_chunk = 0;          // work items per training launch pair (0: a whole group)
+    TileScheduler train_order;         // heaviest-first tile order between training calls
     int grid_forward = 0;
     int grid_train_fwd = 0;
     int grid_train_bwd = 0;
@@ -149,6 +157,7 @@ namespace {
 
 void free_tracer(bv_tracer *t) {
     if (!t) return;
+    t->train_order.release();
     cudaFree(t->geom);
     cudaFree(t->density);
     cudaFree(t->sh);
@@ -692,6 +701,13 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         const size_t fit = t->step_rec_capacity / (chunk_work * kStepRecWords);
         rec_steps = (uint32_t)std::min<size_t>({(size_t)t->step_rec_steps, (size_t)ts->max_steps, fit});
     }
+    // heaviest-first tiles (calls of one launch pair): the forward times its
+    // tiles, the order for the next call of the same shape is built after it
+    const uint32_t *order = nullptr;
+    const size_t order_tiles = group_work / 32u;
+    const bool time_tiles = n_cams <= (uint32_t)kMaxViewsPerLaunch && chunk_work == group_work &&
+                            t->train_order.begin(BV_WALK_TILE_ORDER, order_tiles, n_cams, width,
+                                                 height, order);
     bv_status st = begin_timing(t, s);
     if (st != BV_OK) return st;
     BV_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), s), "loss reset");
@@ -728,6 +744,8 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         p.stats = t->stats_enabled ? t->stats : nullptr;
         p.step_rec = rec_steps ? t->step_rec : nullptr;
         p.rec_steps = rec_steps;
+        p.tile_order = order;
+        p.tile_cost = time_tiles ? t->train_order.cost : nullptr;
         t->last_launches += 1;  // start cells
         for (uint32_t b = 0; b < work; b += (uint32_t)chunk_work) {
             p.work_begin = b;
@@ -748,6 +766,10 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         t->last_launches += 1;
     }
     if (t->stats_enabled) BV_CUDA(cudaEventRecord(t->ev[2], s), "event");
+    if (time_tiles) {
+        BV_CUDA(t->train_order.end(order_tiles, n_cams, width, height, s), "tile order");
+        t->last_launches += 2;
+    }
     t->start_point_pending = true;
     t->last_train = true;
     return BV_OK;

@@ -111,6 +111,8 @@ struct TrainParams {
     uint32_t *step_rec;           // exit face + SH colour per (ray, step < rec_steps), or null
     uint32_t rec_steps;           // 0: the replay searches and evaluates every step
     uint32_t work_begin;          // this launch covers work items [work_begin, +total_work)
+    const uint32_t *tile_order;   // [tiles] tile of dispensed tile i, or null (bv_tile_order.cuh)
+    uint32_t *tile_cost;          // [tiles] forward: each tile's duration, or null
     ViewDesc views[kMaxViewsPerLaunch];
 };
 

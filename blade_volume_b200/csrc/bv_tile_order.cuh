@@ -26,6 +26,8 @@ __device__ __forceinline__ uint32_t tile_item(const uint32_t *order, uint32_t sl
     return order ? (__ldg(order + (slot >> 5)) << 5) | (slot & 31u) : slot;
 }
 
+constexpr uint32_t kNoTile = 0xffffffffu;
+
 // Lane 0 of a warp stores its tile's duration since `begin` (clock64).
 __device__ __forceinline__ void store_tile_cost(uint32_t *cost, uint32_t w, long long begin) {
     if (cost && (threadIdx.x & 31u) == 0) {

@@ -20,6 +20,7 @@
 #include "bv_internal.h"
 #include "bv_device.cuh"
 #include "bv_segment.cuh"
+#include "bv_tile_order.cuh"
 
 namespace bv {
 namespace {
@@ -479,11 +480,20 @@ train_forward_kernel(const __grid_constant__ TrainParams P) {
     size_t pix = 0;
     float loss_acc = 0.f;
     uint32_t n_rays = 0, n_steps = 0, n_faces = 0;
+    // the warp's current tile and when it took it (tile times for the next
+    // call's heaviest-first order)
+    uint32_t tile_id = kNoTile;
+    long long tile_begin = 0;
     for (;;) {
+        if (P.tile_cost && tile_id != kNoTile && __ballot_sync(kFull, active) == 0) {
+            store_tile_cost(P.tile_cost, tile_id << 5, tile_begin);
+            tile_id = kNoTile;
+        }
         uint32_t w;
         if (refill(P.work_counter, P.total_work, active, drained, w)) {
             uint32_t view, x, y;
-            if (work_item(P, P.work_begin + w, view, x, y)) {
+            const uint32_t item = tile_item(P.tile_order, w);
+            if (work_item(P, P.work_begin + item, view, x, y)) {
                 const ViewDesc &vd = P.views[view];
                 pix = pixel_index(P, view, x, y);
                 const bool ok = make_ray(vd, x, y, W.ray);
@@ -493,11 +503,18 @@ train_forward_kernel(const __grid_constant__ TrainParams P) {
                 W.T = 1.f;
                 W.depth = ok ? vd.depth : -1.0f;  // a failed direction records nothing
                 W.steps = 0;
-                W.work = w;
+                W.work = item;
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch) Ch[ch] = Cl[ch] = 0.f;
                 active = true;
                 n_rays += 1;
+            }
+        }
+        if (P.tile_cost && tile_id == kNoTile) {
+            const unsigned act = __ballot_sync(kFull, active);
+            if (act) {
+                tile_id = __shfl_sync(kFull, W.work >> 5, __ffs(act) - 1);
+                tile_begin = clock64();
             }
         }
         if (__ballot_sync(kFull, active) == 0) {
@@ -619,7 +636,8 @@ train_backward_kernel(const __grid_constant__ TrainParams P) {
         uint32_t w;
         if (refill(P.work_counter + 1, P.total_work, active, drained, w)) {
             uint32_t view, x, y;
-            if (work_item(P, P.work_begin + w, view, x, y)) {
+            const uint32_t item = tile_item(P.tile_order, w);
+            if (work_item(P, P.work_begin + item, view, x, y)) {
                 const ViewDesc &vd = P.views[view];
                 const size_t pix = pixel_index(P, view, x, y);
                 const bool ok = make_ray(vd, x, y, W.ray);
@@ -630,7 +648,7 @@ train_backward_kernel(const __grid_constant__ TrainParams P) {
                 W.T = 1.f;
                 W.depth = ok ? vd.depth : -1.0f;
                 W.steps = 0;
-                W.work = w;
+                W.work = item;
                 const RayState st = P.ray_state[pix];
                 Ch[0] = st.c_hi.x;
                 Ch[1] = st.c_hi.y;
