@@ -18,7 +18,8 @@
 #include "bv_tile_order.cuh"
 
 // Training takes its tiles heaviest first by the previous call's tile times
-// (1) or in launch order (0).
+// in the forward and the replay (1), in the replay only (2), or in launch
+// order (0).
 #ifndef BV_WALK_TILE_ORDER
 #define BV_WALK_TILE_ORDER 1
 #endif
@@ -744,7 +745,7 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         p.stats = t->stats_enabled ? t->stats : nullptr;
         p.step_rec = rec_steps ? t->step_rec : nullptr;
         p.rec_steps = rec_steps;
-        p.tile_order = order;
+        p.tile_order = BV_WALK_TILE_ORDER == 1 ? order : nullptr;  // 2: the replay only
         p.tile_cost = time_tiles ? t->train_order.cost : nullptr;
         t->last_launches += 1;  // start cells
         for (uint32_t b = 0; b < work; b += (uint32_t)chunk_work) {
@@ -755,8 +756,10 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
             BV_CUDA(launch_train_forward(p, std::min(t->grid_train_fwd, blocks_needed), s),
                     "training forward launch");
             if (t->stats_enabled && c0 == 0 && b == 0) BV_CUDA(cudaEventRecord(t->ev[3], s), "event");
+            p.tile_order = order;
             BV_CUDA(launch_train_backward(p, std::min(t->grid_train_bwd, blocks_needed), s),
                     "training backward launch");
+            p.tile_order = BV_WALK_TILE_ORDER == 1 ? order : nullptr;
             t->last_launches += 2;
         }
     }

@@ -43,6 +43,11 @@ __device__ __forceinline__ void store_tile_cost(uint32_t *cost, uint32_t w, long
 // zero on entry.
 constexpr int kOrderClasses = 32;
 
+// Stable order inside a class (1) or the order the atomics give (0).
+#ifndef BV_TILE_ORDER_STABLE
+#define BV_TILE_ORDER_STABLE 1
+#endif
+
 __device__ __forceinline__ uint32_t order_class(uint32_t cost) {
     return 31u - (uint32_t)__clz(cost | 1u);
 }
@@ -76,17 +81,110 @@ __global__ void tile_order_scatter_kernel(const uint32_t *__restrict__ cost, uin
     }
 }
 
+// The same order, stable: inside a class the tiles keep their launch order,
+// so tiles that run at the same time stay neighbours on screen and share
+// cache lines.  Block b of kOrderBlocks takes a contiguous range of tiles:
+// pass 1 counts each class in each block, pass 2 (one warp) turns the counts
+// into each (block, class) start, pass 3 ranks the tiles of a block within
+// their class in order (a warp's tiles of one class through a match mask,
+// the warps of a 1024-tile chunk through a per-class prefix).  `counts`
+// holds kOrderBlocks x kOrderClasses words.
+constexpr int kOrderBlocks = 148;
+constexpr int kOrderThreads = 1024;
+
+__device__ __forceinline__ void order_block_range(uint32_t tiles, uint32_t &lo, uint32_t &hi) {
+    const uint32_t per = (tiles + gridDim.x - 1) / gridDim.x;
+    lo = min(tiles, blockIdx.x * per);
+    hi = min(tiles, lo + per);
+}
+
+__global__ void __launch_bounds__(kOrderThreads)
+tile_class_count_kernel(const uint32_t *__restrict__ cost, uint32_t tiles,
+                        uint32_t *__restrict__ counts) {
+    __shared__ uint32_t h[kOrderClasses];
+    if (threadIdx.x < kOrderClasses) h[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t lo, hi;
+    order_block_range(tiles, lo, hi);
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&h[order_class(cost[i])], 1u);
+    __syncthreads();
+    if (threadIdx.x < kOrderClasses) counts[blockIdx.x * kOrderClasses + threadIdx.x] = h[threadIdx.x];
+}
+
+// One warp: lane c owns class c.  counts[b][c] becomes the first position
+// of block b's tiles of class c (classes from the heaviest, 31, down).
+__global__ void tile_class_offsets_kernel(uint32_t *__restrict__ counts, uint32_t blocks) {
+    const uint32_t c = threadIdx.x;
+    uint32_t total = 0;
+    for (uint32_t b = 0; b < blocks; ++b) total += counts[b * kOrderClasses + c];
+    // exclusive sum over the heavier classes c + 1 .. 31
+    __shared__ uint32_t tot[kOrderClasses];
+    tot[c] = total;
+    __syncwarp();
+    uint32_t above = 0;
+    for (uint32_t k = c + 1; k < (uint32_t)kOrderClasses; ++k) above += tot[k];
+    uint32_t run = above;
+    for (uint32_t b = 0; b < blocks; ++b) {
+        const uint32_t n = counts[b * kOrderClasses + c];
+        counts[b * kOrderClasses + c] = run;
+        run += n;
+    }
+}
+
+__global__ void __launch_bounds__(kOrderThreads)
+tile_class_scatter_kernel(const uint32_t *__restrict__ cost, uint32_t tiles,
+                          const uint32_t *__restrict__ offsets, uint32_t *__restrict__ order) {
+    __shared__ uint32_t next[kOrderClasses];                       // next free position per class
+    __shared__ uint32_t warp_n[kOrderThreads / 32][kOrderClasses];  // class counts per warp
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (threadIdx.x < kOrderClasses) next[threadIdx.x] = offsets[blockIdx.x * kOrderClasses + threadIdx.x];
+    uint32_t lo, hi;
+    order_block_range(tiles, lo, hi);
+    for (uint32_t base = lo; base < hi; base += blockDim.x) {
+        for (uint32_t k = threadIdx.x; k < (kOrderThreads / 32) * kOrderClasses; k += blockDim.x)
+            (&warp_n[0][0])[k] = 0;
+        __syncthreads();
+        const uint32_t i = base + threadIdx.x;
+        const bool have = i < hi;
+        const uint32_t c = have ? order_class(cost[i]) : kOrderClasses;  // kOrderClasses: none
+        const unsigned peers = __match_any_sync(0xffffffffu, c);
+        const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+        if (have && rank == 0) warp_n[warp][c] = __popc(peers);
+        __syncthreads();
+        if (have) {
+            uint32_t before = 0;  // this class's tiles in the chunk's earlier warps
+            for (uint32_t v = 0; v < warp; ++v) before += warp_n[v][c];
+            order[next[c] + before + rank] = i;
+        }
+        __syncthreads();
+        if (threadIdx.x < kOrderClasses) {
+            uint32_t n = 0;
+            for (uint32_t v = 0; v < kOrderThreads / 32; ++v) n += warp_n[v][threadIdx.x];
+            next[threadIdx.x] += n;
+        }
+        __syncthreads();
+    }
+}
+
 cudaError_t launch_tile_order(const uint32_t *cost, uint32_t tiles, uint32_t *counts,
                               uint32_t *order, cudaStream_t s) {
+#if BV_TILE_ORDER_STABLE
+    tile_class_count_kernel<<<kOrderBlocks, kOrderThreads, 0, s>>>(cost, tiles, counts);
+    tile_class_offsets_kernel<<<1, 32, 0, s>>>(counts, kOrderBlocks);
+    tile_class_scatter_kernel<<<kOrderBlocks, kOrderThreads, 0, s>>>(cost, tiles, counts, order);
+    return cudaGetLastError();
+#else
     cudaError_t e = cudaMemsetAsync(counts, 0, 2 * kOrderClasses * sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
     const int blocks = (int)std::min<uint32_t>(296u, (tiles + 255u) / 256u);
     tile_cost_histogram_kernel<<<blocks, 256, 0, s>>>(cost, tiles, counts);
     tile_order_scatter_kernel<<<blocks, 256, 0, s>>>(cost, tiles, counts, order);
     return cudaGetLastError();
+#endif
 }
 
-// Heaviest-first scheduling of one kind of launch from frame to frame: a launch times its tiles into `cost`, the order is
+// Heaviest-first scheduling of one kind of launch from frame to frame: a
+// launch times its tiles into `cost`, the order is
 // built from those times after it, and the next launch of the same shape
 // (views, width, height: the same tiles) takes its tiles in that order.
 // Frames of a moving camera keep most of their heavy tiles where they were;
@@ -113,7 +211,7 @@ struct TileScheduler {
         if (!enabled || n_views > (uint32_t)kMaxViewsPerLaunch) return false;
         if (tiles > capacity) {
             release();
-            if (cudaMalloc(&counts, 2 * kOrderClasses * sizeof(uint32_t)) != cudaSuccess ||
+            if (cudaMalloc(&counts, kOrderBlocks * kOrderClasses * sizeof(uint32_t)) != cudaSuccess ||
                 cudaMalloc(&cost, tiles * sizeof(uint32_t)) != cudaSuccess ||
                 cudaMalloc(&order, tiles * sizeof(uint32_t)) != cudaSuccess) {
                 (void)cudaGetLastError();  // no room: launch order

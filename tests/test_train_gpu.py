@@ -203,3 +203,35 @@ def test_rays_longer_than_the_step_record():
     assert abs(got_loss - ref["loss"]) <= 1e-5 * ref["loss"]
     assert np.array_equal(got_rgb.view(np.uint32), ref["rgb32"].view(np.uint32))
     gradcheck.check_all(g, ref, where="slab, rays of 348-400 steps")
+
+
+def test_repeated_calls_take_tiles_heaviest_first_with_the_same_results():
+    """A call of the same shape as the one before takes its tiles in the
+    order of the previous forward's tile times (two more launches per call
+    build the order), for the same cameras or others; each call's colours
+    are the oracle's bit for bit and its gradients within the element-wise
+    bar."""
+    m, cams, target = case("plain", seed=9, n=3000)
+    other = scenes.sphere_cameras(3, 3.0, 21, math.radians(55.0), 1.0, 100.0)
+    om = O.OracleModel.from_scene(m)
+    refs = {}
+    t = bv.RadFoamGpuTracer(m)
+    try:
+        tg = torch.from_numpy(target).cuda()
+        for i, views in enumerate([cams, cams, other, cams]):
+            if id(views) not in refs:
+                refs[id(views)] = O.forward_backward(om, views, W, H, target=target,
+                                                     want_mass=True)
+            ref = refs[id(views)]
+            grads = t.new_grads()
+            rgb = torch.zeros((len(views), H, W, 3), dtype=torch.float32, device="cuda")
+            loss = t.forward_backward(views, W, H, tg, grads, max_dt=50.0, weight_threshold=0.0,
+                                      rgb_out=rgb)
+            torch.cuda.synchronize()
+            g = {k: v.cpu().numpy().astype(np.float64) for k, v in grads.items()}
+            g["d_pos"] = g["d_pos"].reshape(-1, 3)
+            assert np.array_equal(rgb.cpu().numpy().view(np.uint32), ref["rgb32"].view(np.uint32)), i
+            assert abs(float(loss.item()) - ref["loss"]) <= 1e-5 * ref["loss"], i
+            gradcheck.check_all(g, ref, where=f"walk tile order call {i}")
+    finally:
+        t.deinit()
