@@ -19,9 +19,14 @@
 
 // Training takes its tiles heaviest first by the previous call's tile times
 // in the forward and the replay (1), in the replay only (2), or in launch
-// order (0).
+// order (0).  Measured on the headline (262,144 sites, 8 x 512^2): the
+// forward keeps launch order faster (8.21 vs 8.65 ms: neighbouring tiles
+// share cells in L1/L2), the replay takes the order with classes in no
+// particular screen order faster (8.05 vs 9.04 ms in launch order, 8.64
+// with classes in launch order: concurrent tiles from all over the screen
+// scatter their gradient atomics into different cells).
 #ifndef BV_WALK_TILE_ORDER
-#define BV_WALK_TILE_ORDER 1
+#define BV_WALK_TILE_ORDER 2
 #endif
 
 using namespace bv;
@@ -124,7 +129,7 @@ struct bv_tracer {
     uint32_t step_rec_steps = kExitRecSteps;  // recorded steps per ray
     bool step_rec_owned = true;        // false: lent by a serving engine
     uint32_t train_chunk = 0;          // work items per training launch pair (0: a whole group)
-    TileScheduler train_order;         // heaviest-first tile order between training calls
+    TileScheduler train_order;         // heaviest-first tiles between training calls (unstable)
     int grid_forward = 0;
     int grid_train_fwd = 0;
     int grid_train_bwd = 0;
@@ -372,6 +377,7 @@ bv_status bv_radfoam_tracer_new(const bv_model_desc *md, const bv_trace_settings
     BV_CUDA(cudaGetDevice(&device), "cudaGetDevice");
 
     bv_tracer *t = new bv_tracer();
+    t->train_order.stable = false;
     t->device = device;
     t->n = md->num_points;
     t->m_edges = md->adjacency_offsets[md->num_points];
@@ -771,7 +777,7 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
     if (t->stats_enabled) BV_CUDA(cudaEventRecord(t->ev[2], s), "event");
     if (time_tiles) {
         BV_CUDA(t->train_order.end(order_tiles, n_cams, width, height, s), "tile order");
-        t->last_launches += 2;
+        t->last_launches += t->train_order.order_launches();
     }
     t->start_point_pending = true;
     t->last_train = true;

@@ -574,7 +574,7 @@ bv_status bv_gaussian_tracer_dispatch(bv_gaussian_tracer *t, float *out_rgba_dev
     cudaError_t e = launch_gaussian(p, t->n_kept, t->sh_degree, s, launches);
     if (e == cudaSuccess && time_tiles) {
         e = t->tile_sched.end(tiles, 1, width, height, s);
-        launches += 2;
+        launches += t->tile_sched.order_launches();
     }
     if (e != cudaSuccess) {
         set_last_error(cudaGetErrorString(e));

@@ -314,7 +314,7 @@ bv_status bv_relight_tracer_dispatch(bv_relight_tracer *t, float *out_rgba_dev,
     cudaError_t e = launch_relight(p, s, launches);
     if (e == cudaSuccess && time_tiles) {
         e = t->tile_sched.end(tiles, 1, width, height, s);
-        launches += 2;
+        launches += t->tile_sched.order_launches();
     }
     if (e != cudaSuccess) {
         set_last_error(cudaGetErrorString(e));

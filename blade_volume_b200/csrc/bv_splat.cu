@@ -1283,7 +1283,7 @@ bv_status enqueue_splats(bv_splat_tracer *t, float4 *out, const bv_camera *cams,
         t->last_launches += 1;
         if (time_tiles) {
             SP_CUDA(t->render_order.end(tiles, nc, w, h, s), "tile order");
-            t->last_launches += 2;
+            t->last_launches += t->render_order.order_launches();
         }
     }
     return BV_OK;
@@ -1721,7 +1721,7 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         t->last_launches += 2;
         if (time_tiles) {
             SP_CUDA(t->train_order.end(tiles, n_cams, width, height, s), "tile order");
-            t->last_launches += 2;
+            t->last_launches += t->train_order.order_launches();
         }
     }
     if (want_site) {

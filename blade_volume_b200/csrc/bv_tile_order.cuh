@@ -43,10 +43,7 @@ __device__ __forceinline__ void store_tile_cost(uint32_t *cost, uint32_t w, long
 // zero on entry.
 constexpr int kOrderClasses = 32;
 
-// Stable order inside a class (1) or the order the atomics give (0).
-#ifndef BV_TILE_ORDER_STABLE
-#define BV_TILE_ORDER_STABLE 1
-#endif
+
 
 __device__ __forceinline__ uint32_t order_class(uint32_t cost) {
     return 31u - (uint32_t)__clz(cost | 1u);
@@ -166,21 +163,24 @@ tile_class_scatter_kernel(const uint32_t *__restrict__ cost, uint32_t tiles,
     }
 }
 
+// stable: the order above, or classes in the order the atomics give (tiles
+// running at the same time then come from anywhere on screen, which spreads
+// the walk replay's gradient atomics: measured faster there).  Three
+// launches when stable, two otherwise.
 cudaError_t launch_tile_order(const uint32_t *cost, uint32_t tiles, uint32_t *counts,
-                              uint32_t *order, cudaStream_t s) {
-#if BV_TILE_ORDER_STABLE
-    tile_class_count_kernel<<<kOrderBlocks, kOrderThreads, 0, s>>>(cost, tiles, counts);
-    tile_class_offsets_kernel<<<1, 32, 0, s>>>(counts, kOrderBlocks);
-    tile_class_scatter_kernel<<<kOrderBlocks, kOrderThreads, 0, s>>>(cost, tiles, counts, order);
-    return cudaGetLastError();
-#else
+                              uint32_t *order, bool stable, cudaStream_t s) {
+    if (stable) {
+        tile_class_count_kernel<<<kOrderBlocks, kOrderThreads, 0, s>>>(cost, tiles, counts);
+        tile_class_offsets_kernel<<<1, 32, 0, s>>>(counts, kOrderBlocks);
+        tile_class_scatter_kernel<<<kOrderBlocks, kOrderThreads, 0, s>>>(cost, tiles, counts, order);
+        return cudaGetLastError();
+    }
     cudaError_t e = cudaMemsetAsync(counts, 0, 2 * kOrderClasses * sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
     const int blocks = (int)std::min<uint32_t>(296u, (tiles + 255u) / 256u);
     tile_cost_histogram_kernel<<<blocks, 256, 0, s>>>(cost, tiles, counts);
     tile_order_scatter_kernel<<<blocks, 256, 0, s>>>(cost, tiles, counts, order);
     return cudaGetLastError();
-#endif
 }
 
 // Heaviest-first scheduling of one kind of launch from frame to frame: a
@@ -194,6 +194,9 @@ struct TileScheduler {
     size_t capacity = 0;
     uint32_t views = 0, width = 0, height = 0;
     bool valid = false;
+    bool stable = true;  // launch order kept inside a cost class (launch_tile_order)
+
+    uint32_t order_launches() const { return stable ? 3u : 2u; }
 
     void release() {
         cudaFree(cost);
@@ -226,7 +229,7 @@ struct TileScheduler {
     }
     // After the launch (same stream): the order for the next one.
     cudaError_t end(size_t tiles, uint32_t n_views, uint32_t w, uint32_t h, cudaStream_t s) {
-        const cudaError_t e = launch_tile_order(cost, (uint32_t)tiles, counts, order, s);
+        const cudaError_t e = launch_tile_order(cost, (uint32_t)tiles, counts, order, stable, s);
         if (e != cudaSuccess) return e;
         views = n_views;
         width = w;

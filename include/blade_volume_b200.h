@@ -213,10 +213,15 @@ typedef struct bv_grads {
  * target_rgb_dev [n][height][width][3]; loss_dev receives the scalar loss
  * (float, overwritten); rgb_out_dev (may be NULL) the rendered colours
  * [n][height][width][3].  Two walk launches: the forward kernel walks
- * every ray and forms its loss gradient dL/dC; the replay kernel walks the
- * same path again, recomputing transmittance, and scatters the parameter
- * gradients.  Only per-ray state (colour and dL/dC, 48 bytes) passes between
- * them; no per-sample state is stored. */
+ * every ray, forms its loss gradient dL/dC and records each step's exit face
+ * and colour (the tracer's step record, up to its set number of steps per
+ * ray); the replay kernel walks the same path again from that record,
+ * recomputing transmittance, and scatters the parameter gradients (steps
+ * past the record search and evaluate again).  Per ray, the colour and
+ * dL/dC (48 bytes) pass between them.  The forward also times its 8x4
+ * tiles, and two small launches order them so that the replay of the next
+ * call of the same shape takes them heaviest first; the order changes no
+ * result. */
 bv_status bv_forward_backward(bv_tracer *tracer, const bv_camera *cameras, uint32_t n_cameras,
                               uint32_t width, uint32_t height, const float *target_rgb_dev,
                               const bv_train_settings *settings, const bv_grads *grads,
@@ -341,10 +346,10 @@ bv_status bv_relight_tracer_set_point_lights(bv_relight_tracer *tracer,
 bv_status bv_relight_tracer_set_background(bv_relight_tracer *tracer, const float rgb[3]);
 /* Renders width x height into out_rgba_dev ([h][w][4] float32): radiance +
  * transmittance * background, alpha = 1 - transmittance (relight.wgsl:747-780).
- * Four launches: each particle's camera-origin terms into the tracer's
+ * Five launches: each particle's camera-origin terms into the tracer's
  * per-view table, the trace (its 8x4 tiles heaviest first by the previous
  * dispatch's tile times when that had the same size; the order changes no
- * result), and two small ones that order the tiles for the next dispatch.
+ * result), and three small ones that order the tiles for the next dispatch.
  * Because the tables are rewritten by each dispatch, a dispatch on a
  * different stream than the tracer's previous one is ordered after it (an
  * event wait), so dispatches never overlap. */
@@ -378,7 +383,7 @@ void bv_powerfoam_splat_tracer_destroy(bv_splat_tracer *tracer);
 /* Renders [height][width][4] float32 (RGB, alpha = 1 - transmittance).
  * Dispatches and training calls time their 8x4-pixel tiles; a later call of
  * the same shape (views, width, height) starts its tiles heaviest first by
- * those times (two more small launches per call build the order).  The
+ * those times (three more small launches per call build the order).  The
  * order changes no result.  A call on a different stream than the tracer's
  * previous call is ordered after it (an event wait): the tile orders, ray
  * state and interval record belong to the tracer. */
@@ -467,10 +472,10 @@ bv_status bv_gaussian_tracer_set_background(bv_gaussian_tracer *tracer, const fl
 /* particles kept (GaussianGpuCloud::num_points) */
 uint32_t bv_gaussian_tracer_num_points(const bv_gaussian_tracer *tracer);
 /* Renders width x height into out_rgba_dev ([h][w][4] float32):
- * (radiance + T * background, 1 - T).  Four launches: each particle's
+ * (radiance + T * background, 1 - T).  Five launches: each particle's
  * camera-origin terms into the tracer's per-view table, the trace (its 8x4
  * tiles heaviest first by the previous dispatch's tile times when that had
- * the same size; the order changes no result), and two small ones that
+ * the same size; the order changes no result), and three small ones that
  * order the tiles for the next dispatch.  Because the tables are rewritten
  * by each dispatch, a dispatch on a different stream than the tracer's
  * previous one is ordered after it (an event wait), so dispatches never

@@ -142,7 +142,7 @@ def test_dispatches_on_two_streams_are_ordered():
     t.enable_stats(True)
     t.dispatch(out[0], cams[0], (48, 36), stream=s1)
     t.dispatch(out[1], cams[1], (48, 36), stream=s2)
-    assert t.last_stats().launches == 4  # origin terms, trace, tile order x 2
+    assert t.last_stats().launches == 5  # origin terms, trace, tile order x 3
     torch.cuda.synchronize()
     for k in range(2):
         ref, _ = O.relight_render(osc, lights, cams[k], 48, 36, (0.0, 0.0, 0.0))

@@ -137,7 +137,7 @@ def test_stats_count_rays_and_intervals():
 
 def test_repeated_renders_take_tiles_heaviest_first_bit_exact():
     """A dispatch of the same shape as the one before takes its tiles in the
-    order of the previous dispatch's tile durations (two more launches build
+    order of the previous dispatch's tile durations (three more launches build
     it); the image does not depend on that order, for the same cameras or
     moved ones."""
     m = scenes.powerfoam_mixture(3000, seed=4, radius_max=0.15)
@@ -149,7 +149,7 @@ def test_repeated_renders_take_tiles_heaviest_first_bit_exact():
         for views in (cams, cams, moved, cams):
             img = t.render(views, 48, 40)
             torch.cuda.synchronize()
-            assert t.last_stats().launches == 3  # render, order x 2
+            assert t.last_stats().launches == 4  # render, tile order x 3
             got = img.cpu().numpy()
             for v, cam in enumerate(views):
                 ref, _ = O.render_splats(om, cam, 48, 40)

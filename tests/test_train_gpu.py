@@ -207,7 +207,7 @@ def test_rays_longer_than_the_step_record():
 
 def test_repeated_calls_take_tiles_heaviest_first_with_the_same_results():
     """A call of the same shape as the one before takes its tiles in the
-    order of the previous forward's tile times (two more launches per call
+    order of the previous forward's tile times, in its replay (two more launches per call
     build the order), for the same cameras or others; each call's colours
     are the oracle's bit for bit and its gradients within the element-wise
     bar."""
