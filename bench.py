@@ -1028,7 +1028,9 @@ def main():
                     "train_backward_kernel": {"ms": kms_b,
                                               "gather_gbs": gather_bytes / (kms_b * 1e-3) / 1e9},
                     "adam (4 kernels)": {"ms": opt_ms, "alg_gbs": adam_bytes / (opt_ms * 1e-3) / 1e9}},
-        "gpu_launches": 8 * args.steps,
+        # the forward+backward's launches (start cells, forward, replay, site
+        # fold, tile order) and the Adam step's four
+        "gpu_launches": (int(st.launches) + 4) * args.steps,
         "clocks": clocks,
     }
     if cpu is not None:
