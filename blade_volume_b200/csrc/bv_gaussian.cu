@@ -50,7 +50,15 @@ constexpr int kGaussBlock = 128;
 #ifndef BV_GAUSS_LOCAL
 #define BV_GAUSS_LOCAL 1
 #endif
-constexpr int kWindow = 16;
+// Window keys per lane, in registers (BV_GAUSS_SMEM_WINDOW 0) or in dynamic
+// shared memory (1).
+#ifndef BV_GAUSS_WINDOW
+#define BV_GAUSS_WINDOW 16
+#endif
+#ifndef BV_GAUSS_SMEM_WINDOW
+#define BV_GAUSS_SMEM_WINDOW 0
+#endif
+constexpr int kWindow = BV_GAUSS_WINDOW;
 constexpr int kStack = 64;
 
 // One particle in BVH leaf order, 48 B: all a candidate test reads.
@@ -193,18 +201,23 @@ __global__ void __launch_bounds__(kGaussBlock, BV_MINB_GAUSS) gaussian_kernel(co
         id = __ldg(&P.ids[p]);
         return true;
     };
+#if BV_GAUSS_SMEM_WINDOW
+    TRACE_WINDOW_DECL(BV_GAUSS_SMEM_WINDOW, kWindow, kGaussBlock);
+#endif
     for (;;) {
         const bool want = !finished && T > P.min_transmittance;
         if (!__any_sync(0xffffffffu, want)) break;
-        WinKey buf[kWindow];
-        const int count = win_gather_warp<kWindow, kStack>(P.nodes, ray, P.depth, want,
-                                                           cursor_valid, cur_t, cur_idx, buf,
-                                                           nodes_visited, hit);
+#if !BV_GAUSS_SMEM_WINDOW
+        TRACE_WINDOW_DECL(BV_GAUSS_SMEM_WINDOW, kWindow, kGaussBlock);
+#endif
+        const int count = TRACE_WINDOW_PASS(BV_GAUSS_SMEM_WINDOW, kWindow, kStack, P.nodes, ray,
+                                            P.depth, want, cursor_valid, cur_t, cur_idx,
+                                            nodes_visited, hit);
         if (!want) continue;
 #pragma unroll 1
         for (int i = 0; i < count; ++i) {
             if (T <= P.min_transmittance) break;
-            const WinKey h = win_at(buf, i);
+            const WinKey h = TRACE_WINDOW_KEY(BV_GAUSS_SMEM_WINDOW, kWindow, i);
             float tt, a;
             response(P, h.pos, ray, tt, a);
             float coef[ShDims<DEG>::N];
@@ -233,8 +246,9 @@ __global__ void __launch_bounds__(kGaussBlock, BV_MINB_GAUSS) gaussian_kernel(co
             finished = true;
         } else {
             cursor_valid = true;
-            cur_t = buf[kWindow - 1].t;
-            cur_idx = buf[kWindow - 1].idx;
+            const WinKey last = TRACE_WINDOW_KEY(BV_GAUSS_SMEM_WINDOW, kWindow, kWindow - 1);
+            cur_t = last.t;
+            cur_idx = last.idx;
         }
     }
     if (active) {
@@ -282,12 +296,17 @@ cudaError_t launch_gaussian(const GaussianParams &p, uint32_t n, uint32_t deg, c
     const int blocks = (int)((p.total_work + kGaussBlock - 1) / kGaussBlock);
     if (blocks == 0) return cudaSuccess;
     launches += 1;
-    switch (deg) {
-        case 0: gaussian_kernel<0><<<blocks, kGaussBlock, 0, s>>>(p); break;
-        case 1: gaussian_kernel<1><<<blocks, kGaussBlock, 0, s>>>(p); break;
-        case 2: gaussian_kernel<2><<<blocks, kGaussBlock, 0, s>>>(p); break;
-        default: gaussian_kernel<3><<<blocks, kGaussBlock, 0, s>>>(p); break;
+    const size_t smem = BV_GAUSS_SMEM_WINDOW ? (size_t)3 * kWindow * kGaussBlock * 4u : 0u;
+    void (*kernel)(GaussianParams) = deg == 0   ? gaussian_kernel<0>
+                                     : deg == 1 ? gaussian_kernel<1>
+                                     : deg == 2 ? gaussian_kernel<2>
+                                                : gaussian_kernel<3>;
+    if (smem > (size_t)32 * 1024) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
     }
+    kernel<<<blocks, kGaussBlock, smem, s>>>(p);
     return cudaGetLastError();
 }
 

@@ -33,7 +33,15 @@ constexpr int kRelightBlock = 128;
 #else
 #define BV_RELIGHT_BOUNDS __launch_bounds__(kRelightBlock)
 #endif
-constexpr int kWindow = 16;
+// Window keys per lane, in registers (BV_RELIGHT_SMEM_WINDOW 0) or in
+// dynamic shared memory (1).
+#ifndef BV_RELIGHT_WINDOW
+#define BV_RELIGHT_WINDOW 16
+#endif
+#ifndef BV_RELIGHT_SMEM_WINDOW
+#define BV_RELIGHT_SMEM_WINDOW 0
+#endif
+constexpr int kWindow = BV_RELIGHT_WINDOW;
 
 // qrot (common.wgsl:386-390)
 __device__ __forceinline__ float3 qrot(float4 q, float vx, float vy, float vz) {
@@ -197,13 +205,19 @@ relight_kernel(const __grid_constant__ RelightParams P) {
     };
 
     bool finished = !active;
+#if BV_RELIGHT_SMEM_WINDOW
+    TRACE_WINDOW_DECL(BV_RELIGHT_SMEM_WINDOW, kWindow, kRelightBlock);
+#endif
     for (;;) {
         // ---- gather the next window of keys above the cursor (whole warp)
         const bool want = !finished;
         if (!__any_sync(0xffffffffu, want)) break;
-        WinKey buf[kWindow];
-        const int count = win_gather_warp<kWindow, kRelightStack>(
-            P.nodes, ray, t_end, want, cursor_valid, cur_t, cur_idx, buf, nodes_visited, hit);
+#if !BV_RELIGHT_SMEM_WINDOW
+        TRACE_WINDOW_DECL(BV_RELIGHT_SMEM_WINDOW, kWindow, kRelightBlock);
+#endif
+        const int count =
+            TRACE_WINDOW_PASS(BV_RELIGHT_SMEM_WINDOW, kWindow, kRelightStack, P.nodes, ray, t_end,
+                              want, cursor_valid, cur_t, cur_idx, nodes_visited, hit);
         if (!want) continue;
         if (count == 0) {
             finished = true;
@@ -212,7 +226,7 @@ relight_kernel(const __grid_constant__ RelightParams P) {
         // ---- composite the window in order (trace_blended :693-728)
 #pragma unroll 1
         for (int i = 0; i < count; ++i) {
-            const WinKey h = win_at(buf, i);
+            const WinKey h = TRACE_WINDOW_KEY(BV_RELIGHT_SMEM_WINDOW, kWindow, i);
             if (!group || h.t > limit) {
                 if (group) {
                     const float a_sum = fminf(1.0f, sum_w);
@@ -280,8 +294,9 @@ relight_kernel(const __grid_constant__ RelightParams P) {
             continue;
         }
         cursor_valid = true;
-        cur_t = buf[kWindow - 1].t;
-        cur_idx = buf[kWindow - 1].idx;
+        const WinKey last = TRACE_WINDOW_KEY(BV_RELIGHT_SMEM_WINDOW, kWindow, kWindow - 1);
+        cur_t = last.t;
+        cur_idx = last.idx;
     }
     if (group && !stopped) {
         const float a_sum = fminf(1.0f, sum_w);
@@ -336,7 +351,14 @@ cudaError_t launch_relight(const RelightParams &p, cudaStream_t s, uint32_t &lau
         launches += 1;
     }
 #endif
-    relight_kernel<<<blocks, kRelightBlock, 0, s>>>(p);
+    const size_t smem = BV_RELIGHT_SMEM_WINDOW ? (size_t)3 * kWindow * kRelightBlock * 4u : 0u;
+    if (smem > (size_t)32 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(relight_kernel,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    relight_kernel<<<blocks, kRelightBlock, smem, s>>>(p);
     launches += 1;
     return cudaGetLastError();
 }

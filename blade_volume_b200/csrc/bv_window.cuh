@@ -297,4 +297,27 @@ __device__ __forceinline__ int win_gather_warp_smem(const BvhNode *__restrict__ 
     return count;
 }
 
+// A tracer's window of W 12-byte keys per thread of a BLOCK-thread block:
+// in registers (SMEM 0) or in dynamic shared memory (SMEM 1, 12 W BLOCK
+// bytes set at launch).  TRACE_WINDOW_DECL declares what lives across
+// passes, TRACE_WINDOW_GATHER runs one pass, TRACE_WINDOW_KEY(i) reads key i.
+#define TRACE_WINDOW_DECL_1(W, BLOCK)                                              \
+    extern __shared__ uint32_t s_trace_win[];                                     \
+    SmemWindow<W, WinKey> trace_win{reinterpret_cast<float *>(s_trace_win) + threadIdx.x, \
+                                    s_trace_win + 1 * (W) * (BLOCK) + threadIdx.x,     \
+                                    s_trace_win + 2 * (W) * (BLOCK) + threadIdx.x,     \
+                                    s_trace_win, (BLOCK)}
+#define TRACE_WINDOW_PASS_1(W, S, NODES, RAY, TEND, WANT, CV, CT, CI, NV, HIT) \
+    win_gather_warp_smem<W, S>(NODES, RAY, TEND, WANT, CV, CT, CI, trace_win, NV, HIT)
+#define TRACE_WINDOW_KEY_1(W, i) trace_win.get(i)
+#define TRACE_WINDOW_DECL_0(W, BLOCK) WinKey trace_buf[W]
+#define TRACE_WINDOW_PASS_0(W, S, NODES, RAY, TEND, WANT, CV, CT, CI, NV, HIT) \
+    win_gather_warp<W, S>(NODES, RAY, TEND, WANT, CV, CT, CI, trace_buf, NV, HIT)
+#define TRACE_WINDOW_KEY_0(W, i) win_at(trace_buf, i)
+#define TRACE_CAT_(a, b) a##b
+#define TRACE_CAT(a, b) TRACE_CAT_(a, b)
+#define TRACE_WINDOW_DECL(SMEM, W, BLOCK) TRACE_CAT(TRACE_WINDOW_DECL_, SMEM)(W, BLOCK)
+#define TRACE_WINDOW_PASS(SMEM, ...) TRACE_CAT(TRACE_WINDOW_PASS_, SMEM)(__VA_ARGS__)
+#define TRACE_WINDOW_KEY(SMEM, W, i) TRACE_CAT(TRACE_WINDOW_KEY_, SMEM)(W, i)
+
 }  // namespace bv
