@@ -34,12 +34,14 @@ constexpr int kRelightBlock = 128;
 #define BV_RELIGHT_BOUNDS __launch_bounds__(kRelightBlock)
 #endif
 // Window keys per lane, in registers (BV_RELIGHT_SMEM_WINDOW 0) or in
-// dynamic shared memory (1).
+// dynamic shared memory (1).  Measured (1M Gaussians, 16 lights, 1024 x
+// 768): 16 keys in registers 62.3 Mrays/s, in shared memory 16 / 24 / 32
+// keys 61.8 / 65.4 / 64.9 (303 -> 251 nodes per ray at 24 keys).
 #ifndef BV_RELIGHT_WINDOW
-#define BV_RELIGHT_WINDOW 16
+#define BV_RELIGHT_WINDOW 24
 #endif
 #ifndef BV_RELIGHT_SMEM_WINDOW
-#define BV_RELIGHT_SMEM_WINDOW 0
+#define BV_RELIGHT_SMEM_WINDOW 1
 #endif
 constexpr int kWindow = BV_RELIGHT_WINDOW;
 
