@@ -73,6 +73,8 @@ def parse():
                          "the request loop, batched against plain")
     ap.add_argument("--splat-sites", type=int, default=1048576,
                     help="splat: sites of the PowerFoam mixture")
+    ap.add_argument("--lights", type=int, default=16,
+                    help="relight: point lights used (the first n of the scene's 16)")
     ap.add_argument("--gaussians", type=int, default=1000000,
                     help="relight / gaussian: particles of the Gaussian mixture scene")
     ap.add_argument("--rates", default="5,10,25,50,200,2000",
@@ -369,6 +371,7 @@ def run_secondary(args):
     sampler = ClockSampler(0)
     if args.workload == "relight":
         g, cam, lights = scenes.relight_workload(args.gaussians)
+        lights = lights[:args.lights]
         W, H = 1024, 768
         tr = bv.RelightTracer(g)
         tr.set_point_lights(lights)
@@ -401,7 +404,7 @@ def run_secondary(args):
                 "dtype": "f32", "data": "synthetic",
                 "config": {"workload": "gaussian relight", "gaussians": g.n,
                            "kept": tr.num_particles, "width": W, "height": H,
-                           "lights": len(lights), "window": 16},
+                           "lights": len(lights), "window": 24},
                 "hits_per_ray": hits / (W * H), "nodes_per_ray": st.faces / (W * H),
                 "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak,
                              "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
@@ -445,7 +448,7 @@ def run_secondary(args):
                 "warmup": max(args.warmup, 3), "dtype": "f32", "data": "synthetic",
                 "config": {"workload": "gaussian sh trace", "gaussians": g.n,
                            "kept": tr.num_points, "sh_degree": 3, "width": W, "height": H,
-                           "min_opacity": 0.01, "min_transmittance": 0.01, "window": 16},
+                           "min_opacity": 0.01, "min_transmittance": 0.01, "window": 24},
                 "hits_per_ray": hits / (W * H), "nodes_per_ray": st.faces / (W * H),
                 "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak,
                              "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
