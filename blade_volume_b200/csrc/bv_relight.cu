@@ -44,6 +44,19 @@ constexpr int kRelightBlock = 128;
 #define BV_RELIGHT_SMEM_WINDOW 1
 #endif
 constexpr int kWindow = BV_RELIGHT_WINDOW;
+// Shading of a window's hits spread over the warp (1): in rounds of
+// BV_RELIGHT_SPREAD_KEYS keys per lane, the warp's hits are shaded one per
+// lane whoever's ray they are on, into shared memory, and each lane then
+// composites its own in order; or each lane shades its own hits (0).  The
+// lanes of a tile hold different numbers of hits, so shading in place runs
+// the 16 lights in a third of the lanes.
+#ifndef BV_RELIGHT_SPREAD
+#define BV_RELIGHT_SPREAD 0
+#endif
+#ifndef BV_RELIGHT_SPREAD_KEYS
+#define BV_RELIGHT_SPREAD_KEYS 4
+#endif
+constexpr int kSpread = BV_RELIGHT_SPREAD_KEYS;
 
 // qrot (common.wgsl:386-390)
 __device__ __forceinline__ float3 qrot(float4 q, float vx, float vy, float vz) {
@@ -154,6 +167,27 @@ __device__ __forceinline__ void shade_light(const RelightLight &L, float px, flo
     ab += outb;
 }
 
+// The 16-light shading of one hit at depth t of a ray with direction d
+// from the camera origin: relight.wgsl's trace_blended body for one hit
+// (the normal faces the viewer), summed over the lights in order.
+__device__ __forceinline__ void shade_hit(const RelightParams &P, uint32_t pos, float t, float dx,
+                                          float dy, float dz, float &sr, float &sg, float &sb) {
+    const float ptx = P.origin[0] + t * dx, pty = P.origin[1] + t * dy, ptz = P.origin[2] + t * dz;
+    const float4 nr = __ldg(&P.prims[pos].normal_radius);
+    float nx = nr.x, ny = nr.y, nz = nr.z;
+    if (dot3(nx, ny, nz, dx, dy, dz) > 0.0f) {
+        nx = -nx;
+        ny = -ny;
+        nz = -nz;
+    }
+    const uint32_t mat = __ldg(&P.prims[pos].ids.y);
+    const float4 m0 = __ldg(&P.materials[mat].a);
+    const float4 m1 = __ldg(&P.materials[mat].b);
+    sr = sg = sb = 0.f;
+    for (uint32_t l = 0; l < P.n_lights; ++l)
+        shade_light(P.lights[l], ptx, pty, ptz, nx, ny, nz, -dx, -dy, -dz, m0, m1, sr, sg, sb);
+}
+
 __global__ void BV_RELIGHT_BOUNDS
 relight_kernel(const __grid_constant__ RelightParams P) {
     // whole warps past the last tile leave together; lanes of a partial edge
@@ -189,6 +223,21 @@ relight_kernel(const __grid_constant__ RelightParams P) {
         ray.iz = win_inverse(ray.dz);
     }
     const float t_end = P.depth;
+#if BV_RELIGHT_SPREAD
+#if !BV_RELIGHT_SMEM_WINDOW
+#error "spread shading reads other lanes' window keys from shared memory"
+#endif
+    // per warp: each lane's ray direction, the first job of each lane in a
+    // round, and each lane's shaded keys of the round
+    __shared__ float s_dir[kRelightBlock / 32][32][3];
+    __shared__ int s_first[kRelightBlock / 32][32];
+    __shared__ float s_shade[kRelightBlock / 32][32][kSpread][3];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    s_dir[warp][lane][0] = ray.dx;
+    s_dir[warp][lane][1] = ray.dy;
+    s_dir[warp][lane][2] = ray.dz;
+    __syncwarp();
+#endif
 
     float rad_r = 0.f, rad_g = 0.f, rad_b = 0.f, T = 1.0f;
     bool group = false, stopped = false;
@@ -220,6 +269,91 @@ relight_kernel(const __grid_constant__ RelightParams P) {
         const int count =
             TRACE_WINDOW_PASS(BV_RELIGHT_SMEM_WINDOW, kWindow, kRelightStack, P.nodes, ray, t_end,
                               want, cursor_valid, cur_t, cur_idx, nodes_visited, hit);
+#if BV_RELIGHT_SPREAD
+        // ---- shade and composite the window in rounds of kSpread keys per
+        // lane (trace_blended :693-728): the round's hits of all lanes are
+        // shaded one per lane, then each lane composites its own in order
+        {
+            const int cnt = (want && count > 0) ? count : 0;
+            const int n_max = __reduce_max_sync(0xffffffffu, cnt);
+            bool lane_done = cnt == 0;
+            for (int i0 = 0; i0 < n_max; i0 += kSpread) {
+                const int mine = lane_done ? 0 : max(0, min(cnt - i0, kSpread));
+                int incl = mine;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if ((int)lane >= o) incl += v;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                s_first[warp][lane] = incl - mine;
+                __syncwarp();
+                for (int j = (int)lane; j < total; j += 32) {
+                    // owner: the last lane whose first job is at or before j
+                    int lo = 0, hi = 31;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (s_first[warp][mid] <= j)
+                            lo = mid;
+                        else
+                            hi = mid - 1;
+                    }
+                    const int kk = j - s_first[warp][lo];
+                    const uint32_t otid = (warp << 5) + (uint32_t)lo;
+                    const uint32_t key = (uint32_t)(i0 + kk) * kRelightBlock + otid;
+                    const float t = __uint_as_float(s_trace_win[key]);
+                    const uint32_t pos = s_trace_win[2u * kWindow * kRelightBlock + key];
+                    shade_hit(P, pos, t, s_dir[warp][lo][0], s_dir[warp][lo][1], s_dir[warp][lo][2],
+                              s_shade[warp][lo][kk][0], s_shade[warp][lo][kk][1],
+                              s_shade[warp][lo][kk][2]);
+                }
+                __syncwarp();
+#pragma unroll 1
+                for (int kk = 0; kk < mine; ++kk) {
+                    const WinKey h = TRACE_WINDOW_KEY(BV_RELIGHT_SMEM_WINDOW, kWindow, i0 + kk);
+                    if (!group || h.t > limit) {
+                        if (group) {
+                            const float a_sum = fminf(1.0f, sum_w);
+                            const float a_union = 1.0f - group_T;
+                            const float alpha = a_union * (1.0f - 0.75f) + a_sum * 0.75f;
+                            const float wmax = fmaxf(sum_w, 1.0e-6f);
+                            rad_r += T * (alpha * sc_r / wmax);
+                            rad_g += T * (alpha * sc_g / wmax);
+                            rad_b += T * (alpha * sc_b / wmax);
+                            T *= 1.0f - alpha;
+                            group = false;
+                            if (T <= 0.003f) {
+                                stopped = true;
+                                lane_done = true;
+                                break;
+                            }
+                        }
+                        group = true;
+                        limit = h.t + 0.5f * __ldg(&P.prims[h.pos].normal_radius.w);
+                        sc_r = sc_g = sc_b = 0.f;
+                        sum_w = 0.f;
+                        group_T = 1.f;
+                    }
+                    float tt, a;
+                    intersect(P.prims, P.local, h.pos, ray, t_end, tt, a);
+                    hits_used += 1;
+                    const float sr = s_shade[warp][lane][kk][0], sg = s_shade[warp][lane][kk][1],
+                                sb = s_shade[warp][lane][kk][2];
+                    sc_r += a * sr;
+                    sc_g += a * sg;
+                    sc_b += a * sb;
+                    sum_w += a;
+                    group_T *= 1.0f - a;
+                }
+                __syncwarp();
+            }
+        }
+        if (!want) continue;
+        if (count == 0) {
+            finished = true;
+            continue;
+        }
+#else
         if (!want) continue;
         if (count == 0) {
             finished = true;
@@ -276,6 +410,7 @@ relight_kernel(const __grid_constant__ RelightParams P) {
             sum_w += a;
             group_T *= 1.0f - a;
         }
+#endif
         if (stopped) {
             finished = true;
             continue;
