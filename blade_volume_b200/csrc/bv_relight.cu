@@ -49,9 +49,14 @@ constexpr int kWindow = BV_RELIGHT_WINDOW;
 // lane whoever's ray they are on, into shared memory, and each lane then
 // composites its own in order; or each lane shades its own hits (0).  The
 // lanes of a tile hold different numbers of hits, so shading in place runs
-// the 16 lights in a third of the lanes.
+// the 16 lights in a third of the lanes (10.6 of 32 active per instruction).
+// Measured (1M Gaussians, 16 lights, 1024 x 768): in place 65.0 Mrays/s;
+// spread with 24-key windows and 4 / 2 keys per round 82.1 / 80.7, with
+// 20- and 16-key windows 76.3 / 71.2.  A hit's shading is the same
+// expression in whichever lane evaluates it, so the image is unchanged bit
+// for bit.
 #ifndef BV_RELIGHT_SPREAD
-#define BV_RELIGHT_SPREAD 0
+#define BV_RELIGHT_SPREAD 1
 #endif
 #ifndef BV_RELIGHT_SPREAD_KEYS
 #define BV_RELIGHT_SPREAD_KEYS 4
