@@ -35,10 +35,12 @@ constexpr int kRelightBlock = 128;
 #endif
 // Window keys per lane, in registers (BV_RELIGHT_SMEM_WINDOW 0) or in
 // dynamic shared memory (1).  Measured (1M Gaussians, 16 lights, 1024 x
-// 768): 16 keys in registers 62.3 Mrays/s, in shared memory 16 / 24 / 32
-// keys 61.8 / 65.4 / 64.9 (303 -> 251 nodes per ray at 24 keys).
+// 768), shading in place: 16 keys in registers 62.3 Mrays/s, in shared
+// memory 16 / 24 / 32 keys 61.8 / 65.4 / 64.9 (303 -> 251 nodes per ray at
+// 24 keys); shading spread over the warp (below): 16 / 20 / 24 / 28 / 32
+// keys 71.2 / 76.3 / 82.1-83.3 / 93.4 / 92.2.
 #ifndef BV_RELIGHT_WINDOW
-#define BV_RELIGHT_WINDOW 24
+#define BV_RELIGHT_WINDOW 28
 #endif
 #ifndef BV_RELIGHT_SMEM_WINDOW
 #define BV_RELIGHT_SMEM_WINDOW 1
@@ -50,9 +52,9 @@ constexpr int kWindow = BV_RELIGHT_WINDOW;
 // composites its own in order; or each lane shades its own hits (0).  The
 // lanes of a tile hold different numbers of hits, so shading in place runs
 // the 16 lights in a third of the lanes (10.6 of 32 active per instruction).
-// Measured (1M Gaussians, 16 lights, 1024 x 768): in place 65.0 Mrays/s;
-// spread with 24-key windows and 4 / 2 keys per round 82.1 / 80.7, with
-// 20- and 16-key windows 76.3 / 71.2.  A hit's shading is the same
+// Measured (1M Gaussians, 16 lights, 1024 x 768, 24-key windows): in place
+// 65.0 Mrays/s; spread with 2 / 4 / 8 keys per round 80.7 / 82.1 / 83.4.
+// A hit's shading is the same
 // expression in whichever lane evaluates it, so the image is unchanged bit
 // for bit.
 #ifndef BV_RELIGHT_SPREAD
