@@ -53,10 +53,9 @@ constexpr int kWindow = BV_RELIGHT_WINDOW;
 // lanes of a tile hold different numbers of hits, so shading in place runs
 // the 16 lights in a third of the lanes (10.6 of 32 active per instruction).
 // Measured (1M Gaussians, 16 lights, 1024 x 768, 24-key windows): in place
-// 65.0 Mrays/s; spread with 2 / 4 / 8 keys per round 80.7 / 82.1 / 83.4.
-// A hit's shading is the same
-// expression in whichever lane evaluates it, so the image is unchanged bit
-// for bit.
+// 65.0 Mrays/s; spread with 2 / 4 / 8 keys per shading round 80.7 / 82.1 /
+// 83.4.  A hit's shading is the same expression in whichever lane evaluates
+// it, so the image is unchanged bit for bit.
 #ifndef BV_RELIGHT_SPREAD
 #define BV_RELIGHT_SPREAD 1
 #endif
