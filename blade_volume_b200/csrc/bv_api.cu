@@ -28,6 +28,11 @@
 #ifndef BV_WALK_TILE_ORDER
 #define BV_WALK_TILE_ORDER 2
 #endif
+// The forward's own order (mode 2): tiles heaviest first in classes of
+// floor(log2(time)) >> shift, launch order inside a class; -1: launch order.
+#ifndef BV_WALK_FWD_ORDER_SHIFT
+#define BV_WALK_FWD_ORDER_SHIFT -1
+#endif
 
 using namespace bv;
 
@@ -378,6 +383,7 @@ bv_status bv_radfoam_tracer_new(const bv_model_desc *md, const bv_trace_settings
 
     bv_tracer *t = new bv_tracer();
     t->train_order.stable = false;
+    t->train_order.second_shift = BV_WALK_FWD_ORDER_SHIFT;
     t->device = device;
     t->n = md->num_points;
     t->m_edges = md->adjacency_offsets[md->num_points];
@@ -751,7 +757,8 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
         p.stats = t->stats_enabled ? t->stats : nullptr;
         p.step_rec = rec_steps ? t->step_rec : nullptr;
         p.rec_steps = rec_steps;
-        p.tile_order = BV_WALK_TILE_ORDER == 1 ? order : nullptr;  // 2: the replay only
+        // mode 2: the replay takes `order`, the forward its own second order
+        p.tile_order = BV_WALK_TILE_ORDER == 1 ? order : t->train_order.second(order);
         p.tile_cost = time_tiles ? t->train_order.cost : nullptr;
         t->last_launches += 1;  // start cells
         for (uint32_t b = 0; b < work; b += (uint32_t)chunk_work) {
@@ -762,10 +769,11 @@ bv_status bv_forward_backward(bv_tracer *t, const bv_camera *cams, uint32_t n_ca
             BV_CUDA(launch_train_forward(p, std::min(t->grid_train_fwd, blocks_needed), s),
                     "training forward launch");
             if (t->stats_enabled && c0 == 0 && b == 0) BV_CUDA(cudaEventRecord(t->ev[3], s), "event");
+            const uint32_t *fwd_order = p.tile_order;
             p.tile_order = order;
             BV_CUDA(launch_train_backward(p, std::min(t->grid_train_bwd, blocks_needed), s),
                     "training backward launch");
-            p.tile_order = BV_WALK_TILE_ORDER == 1 ? order : nullptr;
+            p.tile_order = fwd_order;
             t->last_launches += 2;
         }
     }

@@ -45,8 +45,11 @@ constexpr int kOrderClasses = 32;
 
 
 
-__device__ __forceinline__ uint32_t order_class(uint32_t cost) {
-    return 31u - (uint32_t)__clz(cost | 1u);
+// The class of a tile time: floor(log2(cost)) >> shift (shift 0: classes a
+// factor of 2 apart; larger shifts merge them, so that fewer, wider classes
+// keep more tiles in launch order).
+__device__ __forceinline__ uint32_t order_class(uint32_t cost, uint32_t shift = 0) {
+    return (31u - (uint32_t)__clz(cost | 1u)) >> shift;
 }
 
 __global__ void tile_cost_histogram_kernel(const uint32_t *__restrict__ cost, uint32_t tiles,
@@ -96,14 +99,15 @@ __device__ __forceinline__ void order_block_range(uint32_t tiles, uint32_t &lo, 
 }
 
 __global__ void __launch_bounds__(kOrderThreads)
-tile_class_count_kernel(const uint32_t *__restrict__ cost, uint32_t tiles,
+tile_class_count_kernel(const uint32_t *__restrict__ cost, uint32_t tiles, uint32_t shift,
                         uint32_t *__restrict__ counts) {
     __shared__ uint32_t h[kOrderClasses];
     if (threadIdx.x < kOrderClasses) h[threadIdx.x] = 0;
     __syncthreads();
     uint32_t lo, hi;
     order_block_range(tiles, lo, hi);
-    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&h[order_class(cost[i])], 1u);
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
+        atomicAdd(&h[order_class(cost[i], shift)], 1u);
     __syncthreads();
     if (threadIdx.x < kOrderClasses) counts[blockIdx.x * kOrderClasses + threadIdx.x] = h[threadIdx.x];
 }
@@ -129,7 +133,7 @@ __global__ void tile_class_offsets_kernel(uint32_t *__restrict__ counts, uint32_
 }
 
 __global__ void __launch_bounds__(kOrderThreads)
-tile_class_scatter_kernel(const uint32_t *__restrict__ cost, uint32_t tiles,
+tile_class_scatter_kernel(const uint32_t *__restrict__ cost, uint32_t tiles, uint32_t shift,
                           const uint32_t *__restrict__ offsets, uint32_t *__restrict__ order) {
     __shared__ uint32_t next[kOrderClasses];                       // next free position per class
     __shared__ uint32_t warp_n[kOrderThreads / 32][kOrderClasses];  // class counts per warp
@@ -143,7 +147,7 @@ tile_class_scatter_kernel(const uint32_t *__restrict__ cost, uint32_t tiles,
         __syncthreads();
         const uint32_t i = base + threadIdx.x;
         const bool have = i < hi;
-        const uint32_t c = have ? order_class(cost[i]) : kOrderClasses;  // kOrderClasses: none
+        const uint32_t c = have ? order_class(cost[i], shift) : kOrderClasses;  // none
         const unsigned peers = __match_any_sync(0xffffffffu, c);
         const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
         if (have && rank == 0) warp_n[warp][c] = __popc(peers);
@@ -168,11 +172,12 @@ tile_class_scatter_kernel(const uint32_t *__restrict__ cost, uint32_t tiles,
 // the walk replay's gradient atomics: measured faster there).  Three
 // launches when stable, two otherwise.
 cudaError_t launch_tile_order(const uint32_t *cost, uint32_t tiles, uint32_t *counts,
-                              uint32_t *order, bool stable, cudaStream_t s) {
+                              uint32_t *order, bool stable, uint32_t shift, cudaStream_t s) {
     if (stable) {
-        tile_class_count_kernel<<<kOrderBlocks, kOrderThreads, 0, s>>>(cost, tiles, counts);
+        tile_class_count_kernel<<<kOrderBlocks, kOrderThreads, 0, s>>>(cost, tiles, shift, counts);
         tile_class_offsets_kernel<<<1, 32, 0, s>>>(counts, kOrderBlocks);
-        tile_class_scatter_kernel<<<kOrderBlocks, kOrderThreads, 0, s>>>(cost, tiles, counts, order);
+        tile_class_scatter_kernel<<<kOrderBlocks, kOrderThreads, 0, s>>>(cost, tiles, shift, counts,
+                                                                        order);
         return cudaGetLastError();
     }
     cudaError_t e = cudaMemsetAsync(counts, 0, 2 * kOrderClasses * sizeof(uint32_t), s);
@@ -195,14 +200,21 @@ struct TileScheduler {
     uint32_t views = 0, width = 0, height = 0;
     bool valid = false;
     bool stable = true;  // launch order kept inside a cost class (launch_tile_order)
+    // an optional second order from the same tile times (second_shift >= 0):
+    // stable, classes floor(log2(cost)) >> second_shift
+    int second_shift = -1;
+    uint32_t *order2 = nullptr;
 
-    uint32_t order_launches() const { return stable ? 3u : 2u; }
+    uint32_t order_launches() const {
+        return (stable ? 3u : 2u) + (second_shift >= 0 ? 3u : 0u);
+    }
 
     void release() {
         cudaFree(cost);
         cudaFree(order);
+        cudaFree(order2);
         cudaFree(counts);
-        cost = order = counts = nullptr;
+        cost = order = order2 = counts = nullptr;
         capacity = 0;
         valid = false;
     }
@@ -216,7 +228,9 @@ struct TileScheduler {
             release();
             if (cudaMalloc(&counts, kOrderBlocks * kOrderClasses * sizeof(uint32_t)) != cudaSuccess ||
                 cudaMalloc(&cost, tiles * sizeof(uint32_t)) != cudaSuccess ||
-                cudaMalloc(&order, tiles * sizeof(uint32_t)) != cudaSuccess) {
+                cudaMalloc(&order, tiles * sizeof(uint32_t)) != cudaSuccess ||
+                (second_shift >= 0 &&
+                 cudaMalloc(&order2, tiles * sizeof(uint32_t)) != cudaSuccess)) {
                 (void)cudaGetLastError();  // no room: launch order
                 release();
                 return false;
@@ -227,9 +241,14 @@ struct TileScheduler {
         valid = false;
         return true;
     }
-    // After the launch (same stream): the order for the next one.
+    // The second order for the next launch of the shape begin() was given
+    // (null: launch order); call after begin().
+    const uint32_t *second(const uint32_t *first) const { return first ? order2 : nullptr; }
+    // After the launch (same stream): the order(s) for the next one.
     cudaError_t end(size_t tiles, uint32_t n_views, uint32_t w, uint32_t h, cudaStream_t s) {
-        const cudaError_t e = launch_tile_order(cost, (uint32_t)tiles, counts, order, stable, s);
+        cudaError_t e = launch_tile_order(cost, (uint32_t)tiles, counts, order, stable, 0u, s);
+        if (e == cudaSuccess && second_shift >= 0)
+            e = launch_tile_order(cost, (uint32_t)tiles, counts, order2, true, (uint32_t)second_shift, s);
         if (e != cudaSuccess) return e;
         views = n_views;
         width = w;
