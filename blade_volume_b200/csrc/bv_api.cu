@@ -30,6 +30,10 @@
 #endif
 // The forward's own order (mode 2): tiles heaviest first in classes of
 // floor(log2(time)) >> shift, launch order inside a class; -1: launch order.
+// Measured on the headline: the forward takes 8.24 ms in launch order and
+// 8.54 / 8.51 / 8.37 ms with shifts 0 / 1 / 2 (coarser classes keep more
+// tiles in launch order; neighbouring tiles sharing cells in L1/L2 is worth
+// more than the heavy tiles starting first).
 #ifndef BV_WALK_FWD_ORDER_SHIFT
 #define BV_WALK_FWD_ORDER_SHIFT -1
 #endif
