@@ -97,6 +97,12 @@ namespace {
 #ifndef BV_SPLAT_TILE_ORDER
 #define BV_SPLAT_TILE_ORDER 1
 #endif
+// Training: one stable order for the forward and the replay (0), or the
+// replay on an unstable order of the same times, whose concurrent tiles
+// from all over the screen spread the gradient atomics (1).
+#ifndef BV_SPLAT_SPLIT_ORDER
+#define BV_SPLAT_SPLIT_ORDER 0
+#endif
 constexpr int kSplatBlock = 128;
 constexpr int kSplatWindow = BV_SPLAT_WINDOW;            // render
 constexpr int kSplatTrainWindow = BV_SPLAT_TRAIN_WINDOW;  // training forward and replay
@@ -1362,6 +1368,10 @@ bv_status bv_powerfoam_splat_tracer_new(const bv_model_desc *md, const bv_trace_
     }
 
     bv_splat_tracer *t = new bv_splat_tracer();
+    if (BV_SPLAT_SPLIT_ORDER) {
+        t->train_order.stable = false;
+        t->train_order.second_shift = 0;
+    }
     t->n = n;
     t->m_edges = m_edges;
     t->sh_degree = deg;
@@ -1707,7 +1717,9 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
             p.rec_limit = std::min<uint32_t>(t->rec_entries, ts->max_steps);
             p.pool_chunks = (uint32_t)std::min<size_t>(t->rec_pool_chunks, 0xfffffff0u);
         }
-        p.base.tile_order = order;
+        // split orders: the forward takes the stable second order, the replay
+        // the first (unstable) one
+        p.base.tile_order = BV_SPLAT_SPLIT_ORDER ? t->train_order.second(order) : order;
         p.base.tile_cost = time_tiles ? t->train_order.cost : nullptr;
         SP_CUDA(launch_splat_train(p, false, s), "splat training forward launch");
         if (rec_chunks) {
@@ -1717,6 +1729,7 @@ bv_status bv_powerfoam_splat_tracer_forward_backward(
         }
         p.base.stats = nullptr;
         p.base.tile_cost = nullptr;
+        p.base.tile_order = order;
         SP_CUDA(launch_splat_train(p, true, s), "splat training backward launch");
         t->last_launches += 2;
         if (time_tiles) {
