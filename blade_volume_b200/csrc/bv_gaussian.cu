@@ -53,7 +53,7 @@ constexpr int kGaussBlock = 128;
 // Window keys per lane, in registers (BV_GAUSS_SMEM_WINDOW 0) or in dynamic
 // shared memory (1).  Measured (1M particles, 1024 x 768): 16 keys in
 // registers 91.4 Mrays/s (128 registers), in shared memory 16 / 20 / 24 /
-// 28 / 32 keys 95.0 / 106.9 / 105.2-105.4 / 98.0 / 96.8 (96 registers; 24
+// 28 / 32 keys 95.0 / 104.9-106.9 / 104.7-105.4 / 98.0 / 96.8 (96 registers; 24
 // keys make most rays one pass over the BVH, 416 -> 355 nodes per ray).
 #ifndef BV_GAUSS_WINDOW
 #define BV_GAUSS_WINDOW 24

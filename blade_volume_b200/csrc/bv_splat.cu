@@ -42,7 +42,8 @@ namespace {
 // (16-byte keys with the interval's plane offsets).  A larger window means
 // fewer passes over the BVH and fewer supports clipped again in the next
 // pass, most of all for the heavy tiles, against fewer resident blocks:
-// render 16 / 24 / 28 / 32 keys 47.7 / 55.7 / 58.0 / 59.6 Mrays/s; training
+// render 16 / 24 / 28 / 32 / 40 keys 47.7 / 55.7 / 58.0 / 59.6 / 54.5 Mrays/s
+// (with the stable tile order: 32 keys 64.1, 40 keys 54.5); training
 // 16 / 20 / 24 / 28 / 32 keys 51.0 / 54.3 / 48.9 / 40.4 / 41.6 (20 keys
 // still fit 5 blocks per SM, 24 and more only 4 or 3).  And the resident
 // blocks per SM requested for the render kernel (4: 128 registers, 19.4
