@@ -71,3 +71,57 @@ def test_percentile():
     v = list(range(1, 101))
     assert serving.percentile(v, 50) == pytest.approx(50.5)
     assert serving.percentile(v, 99) == pytest.approx(99.01)
+
+
+class _FakeServer:
+    """Stands in for bv.Server on the host: a clock that advances 1 ms per
+    read, frames that land 4 ms after submission plus one 16 ms period per
+    frame, and training requests that run 50 ms."""
+
+    def __init__(self):
+        self.now = 100.0
+        self.reqs = {}
+
+    def clock(self):
+        self.now += 1e-3
+        return self.now
+
+    def submit(self, scene, cams, w, h, out=None, target=None, loss=None, frame_done=None):
+        rid = len(self.reqs)
+        t = self.now
+        if target is None:
+            frame_done[:] = t + 0.004 + 0.016 * np.arange(len(frame_done))
+            done = float(frame_done[-1])
+        else:
+            frame_done[:] = t + 0.05
+            done = t + 0.05
+        self.reqs[rid] = dict(status=0, start_s=t, done_s=done)
+        return rid
+
+    def wait(self, rid, timeout):
+        return self.reqs[rid]
+
+
+class _FakeBuffers:
+    def request_args(self, spec):
+        return dict(target=np.zeros(1)) if spec.fwdbwd else dict(out=np.zeros(1))
+
+
+def test_run_stream_paces_frames_and_keeps_training_out_of_frame_figures():
+    cams = []
+    specs = [serving.RequestSpec(arrival=0.002 * i, scene=0, width=1920, height=1080,
+                                 views=4, fwdbwd=(i % 3 == 2), cameras=cams)
+             for i in range(9)]
+    r = serving.run_stream(_FakeServer(), specs, _FakeBuffers(), frame_period_s=0.016)
+    hd = r["per_resolution"]["1920x1080"]
+    # 6 render requests of 4 frames; the 3 training requests are not frames
+    assert hd["frame"]["n"] == 24 and hd["first_frame"]["n"] == 6
+    assert r["per_resolution_fwdbwd"]["1920x1080"]["n"] == 3
+    # each frame lands 4 ms after its request was submitted plus k periods:
+    # paced latency is that 4 ms plus the submission's lag behind arrival
+    assert 3.9 < hd["paced_frame"]["p50_ms"] < 8.0
+    assert hd["paced_frame"]["p99_ms"] < 8.0
+    assert hd["frame"]["p99_ms"] > 48.0  # the last frames, 3 periods later
+    # training work: 3 x 4 x 1080p rays over 50 ms each
+    want = 3 * 4 * 1920 * 1080 / (3 * 0.05) / 1e6
+    assert abs(r["fwdbwd_service_mrays_per_s"] - want) < 1e-6 * want
