@@ -63,6 +63,16 @@ constexpr int kGaussBlock = 128;
 #endif
 constexpr int kWindow = BV_GAUSS_WINDOW;
 constexpr int kStack = 64;
+// Each window's hits evaluated (alpha and SH colour) spread over the warp in
+// rounds of BV_GAUSS_SPREAD_KEYS keys per lane, then composited by their own
+// lane in order (1), or each lane evaluates its own hits (0).
+#ifndef BV_GAUSS_SPREAD
+#define BV_GAUSS_SPREAD 0
+#endif
+#ifndef BV_GAUSS_SPREAD_KEYS
+#define BV_GAUSS_SPREAD_KEYS 4
+#endif
+constexpr int kGSpread = BV_GAUSS_SPREAD_KEYS;
 
 // One particle in BVH leaf order, 48 B: all a candidate test reads.
 struct __align__(16) GaussShPrim {
@@ -157,6 +167,30 @@ __device__ __forceinline__ bool response(const GaussianParams &P, uint32_t pos, 
     return true;
 }
 
+// Alpha and clamped SH colour of a windowed hit (the key's particle passed
+// response() for this ray when it was gathered, so it passes again).
+template <int DEG>
+__device__ __forceinline__ void hit_colour(const GaussianParams &P, uint32_t pos, const WinRay &r,
+                                           float &a, float &cr, float &cg, float &cb) {
+    float tt;
+    a = 0.f;
+    response(P, pos, r, tt, a);
+    float coef[ShDims<DEG>::N];
+    const float4 *row = reinterpret_cast<const float4 *>(P.sh + (size_t)pos * P.sh_stride);
+#pragma unroll
+    for (int qd = 0; qd < (ShDims<DEG>::N + 3) / 4; ++qd) {
+        const float4 v = __ldg(row + qd);
+        const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if (qd * 4 + e < ShDims<DEG>::N) coef[qd * 4 + e] = vv[e];
+    }
+    eval_sh<DEG>(coef, r.dx, r.dy, r.dz, cr, cg, cb);
+    cr = fmaxf(cr, 0.0f);
+    cg = fmaxf(cg, 0.0f);
+    cb = fmaxf(cb, 0.0f);
+}
+
 template <int DEG>
 __global__ void __launch_bounds__(kGaussBlock, BV_MINB_GAUSS) gaussian_kernel(const __grid_constant__ GaussianParams P) {
     // whole warps past the last tile leave together; lanes of a partial edge
@@ -192,6 +226,19 @@ __global__ void __launch_bounds__(kGaussBlock, BV_MINB_GAUSS) gaussian_kernel(co
         ray.iz = win_inverse(ray.dz);
     }
 
+#if BV_GAUSS_SPREAD
+#if !BV_GAUSS_SMEM_WINDOW
+#error "spread evaluation reads other lanes' window keys from shared memory"
+#endif
+    __shared__ float s_gdir[kGaussBlock / 32][32][3];
+    __shared__ int s_gfirst[kGaussBlock / 32][32];
+    __shared__ float4 s_ghit[kGaussBlock / 32][32][kGSpread];  // alpha, colour
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    s_gdir[warp][lane][0] = ray.dx;
+    s_gdir[warp][lane][1] = ray.dy;
+    s_gdir[warp][lane][2] = ray.dz;
+    __syncwarp();
+#endif
     float rad_r = 0.f, rad_g = 0.f, rad_b = 0.f, T = 1.0f;
     bool cursor_valid = false, finished = !active;
     float cur_t = 0.f;
@@ -216,28 +263,71 @@ __global__ void __launch_bounds__(kGaussBlock, BV_MINB_GAUSS) gaussian_kernel(co
         const int count = TRACE_WINDOW_PASS(BV_GAUSS_SMEM_WINDOW, kWindow, kStack, P.nodes, ray,
                                             P.depth, want, cursor_valid, cur_t, cur_idx,
                                             nodes_visited, hit);
+#if BV_GAUSS_SPREAD
+        // rounds of kGSpread keys per lane: the round's hits of all lanes are
+        // evaluated one per lane, then each lane composites its own in order
+        {
+            const int cnt = want ? count : 0;
+            const int n_max = __reduce_max_sync(0xffffffffu, cnt);
+            bool lane_done = cnt == 0 || T <= P.min_transmittance;
+            for (int i0 = 0; i0 < n_max; i0 += kGSpread) {
+                const int mine = lane_done ? 0 : max(0, min(cnt - i0, kGSpread));
+                int incl = mine;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if ((int)lane >= o) incl += v;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                s_gfirst[warp][lane] = incl - mine;
+                __syncwarp();
+                for (int j = (int)lane; j < total; j += 32) {
+                    int lo = 0, hi = 31;  // owner: the last lane whose first job is at or before j
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (s_gfirst[warp][mid] <= j)
+                            lo = mid;
+                        else
+                            hi = mid - 1;
+                    }
+                    const int kk = j - s_gfirst[warp][lo];
+                    const uint32_t key = (uint32_t)(i0 + kk) * kGaussBlock + (warp << 5) + (uint32_t)lo;
+                    WinRay r = ray;
+                    r.dx = s_gdir[warp][lo][0];
+                    r.dy = s_gdir[warp][lo][1];
+                    r.dz = s_gdir[warp][lo][2];
+                    float a, cr, cg, cb;
+                    hit_colour<DEG>(P, s_trace_win[2u * kWindow * kGaussBlock + key], r, a, cr, cg, cb);
+                    s_ghit[warp][lo][kk] = make_float4(a, cr, cg, cb);
+                }
+                __syncwarp();
+#pragma unroll 1
+                for (int kk = 0; kk < mine; ++kk) {
+                    if (T <= P.min_transmittance) {
+                        lane_done = true;
+                        break;
+                    }
+                    const float4 hc = s_ghit[warp][lane][kk];
+                    const float a = hc.x;
+                    const float wt = a * T;
+                    rad_r += wt * hc.y;
+                    rad_g += wt * hc.z;
+                    rad_b += wt * hc.w;
+                    T *= 1.0f - a;
+                    hits_used += 1;
+                }
+                __syncwarp();
+            }
+        }
+        if (!want) continue;
+#else
         if (!want) continue;
 #pragma unroll 1
         for (int i = 0; i < count; ++i) {
             if (T <= P.min_transmittance) break;
             const WinKey h = TRACE_WINDOW_KEY(BV_GAUSS_SMEM_WINDOW, kWindow, i);
-            float tt, a;
-            response(P, h.pos, ray, tt, a);
-            float coef[ShDims<DEG>::N];
-            const float4 *row = reinterpret_cast<const float4 *>(P.sh + (size_t)h.pos * P.sh_stride);
-#pragma unroll
-            for (int qd = 0; qd < (ShDims<DEG>::N + 3) / 4; ++qd) {
-                const float4 v = __ldg(row + qd);
-                const float vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                for (int e = 0; e < 4; ++e)
-                    if (qd * 4 + e < ShDims<DEG>::N) coef[qd * 4 + e] = vv[e];
-            }
-            float cr, cg, cb;
-            eval_sh<DEG>(coef, ray.dx, ray.dy, ray.dz, cr, cg, cb);
-            cr = fmaxf(cr, 0.0f);
-            cg = fmaxf(cg, 0.0f);
-            cb = fmaxf(cb, 0.0f);
+            float a, cr, cg, cb;
+            hit_colour<DEG>(P, h.pos, ray, a, cr, cg, cb);
             const float wt = a * T;
             rad_r += wt * cr;
             rad_g += wt * cg;
@@ -245,6 +335,7 @@ __global__ void __launch_bounds__(kGaussBlock, BV_MINB_GAUSS) gaussian_kernel(co
             T *= 1.0f - a;
             hits_used += 1;
         }
+#endif
         if (count < kWindow) {
             finished = true;
         } else {
