@@ -75,7 +75,9 @@ constexpr int kStack = 64;
 #ifndef BV_GAUSS_SPREAD_KEYS
 #define BV_GAUSS_SPREAD_KEYS 4
 #endif
+#if BV_GAUSS_SPREAD
 constexpr int kGSpread = BV_GAUSS_SPREAD_KEYS;
+#endif
 
 // One particle in BVH leaf order, 48 B: all a candidate test reads.
 struct __align__(16) GaussShPrim {
